@@ -1,0 +1,321 @@
+"""Benchmark: one-fill, one-factorisation port solve of the 16x16 dipole array.
+
+Workload (one "step"): the 16 x 16 planar array of half-wave dipoles at
+300 MHz (41 segments each, degree 2, 10,496 unknowns, 256 ports, seeded
++-1 % length jitter), solved for every port: Galerkin fill, LU, solve of all
+256 port columns, Y = B^T X.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--precision fp64|mixed]
+
+Prints ONE JSON line on rank 0.  ``value`` is device-timed throughput with the
+inputs resident in HBM (solves per second over all ranks); ``e2e`` is the
+same metric through the public ``BSplineSolver(...).compute_port_solution()``
+call, host tables in and coefficients + Y out.  Under torchrun each rank
+solves its own replica ("replicas only": a single dense solve does not shard).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "sweep pts/s & fill+LU time, mixed+batched vs FP64 GPU at |ΔZin|/|Zin|≤1e-6"
+UNIT = "pts/s"
+WORKLOAD = "dipole_array_16x16_300MHz_41seg_d2_256port"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--nx", type=int, default=16)
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi sampling of SM clock and throttle reasons during a region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        import statistics
+
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+# ------------------------------------------------------------ reference
+def cpu_baseline_sample(kw):
+    """The reference's own CPU kernels (oracle/_ref) + LAPACK on a bounded
+    sample: a quarter of the observer rows, and the LU of their leading
+    block, extrapolated to the full workload."""
+    from oracle import ref_baseline
+
+    r = ref_baseline.time_sample(kw, row_fraction=0.25)
+    t = r["fill_s"] + r["solve_s"]
+    return {
+        "value": 1.0 / t,
+        "unit": UNIT,
+        "cores": r["threads"],
+        "kind": "reference",
+        "sample": (f"reference C++ fill kernels on {r['rows']}/{r['n_seg']} observer rows "
+                   f"(x{r['n_seg'] / r['rows']:.1f}) + LAPACK zgetrf/zgetrs on the leading "
+                   f"{r['lu_block']} block with {r['n_ports']} rhs (x(n/{r['lu_block']})^3 / ^2); "
+                   f"est. fill {r['fill_s']:.2f} s + solve {r['solve_s']:.2f} s"),
+        "fill_s": r["fill_s"],
+        "solve_s": r["solve_s"],
+    }
+
+
+def run_reference(args, kw):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    for _ in range(args.warmup):
+        cpu_baseline_sample(kw)
+    vals = []
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        vals.append(cpu_baseline_sample(kw))
+    wall = time.perf_counter() - t0
+    per_step = sum(1.0 / v["value"] for v in vals) / len(vals)
+    value = 1.0 / per_step
+    base = vals[-1]
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": per_step * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "complex128",
+        "data": "synthetic (seeded dipole array)",
+        "config": {"workload": WORKLOAD, "n_unknowns": base.get("n_basis", 10496), "ports": 256,
+                   "parallelism": "host threads"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": base["cores"], "kind": "reference",
+                         "sample": base["sample"]},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "wall_s": wall,
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ b200
+def run_b200(args, kw):
+    import numpy as np
+    import torch
+
+    import momwire_b200
+    from momwire_b200 import _lib
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+        pg = dist
+    lib = _lib.load()
+
+    solver = momwire_b200.BSplineSolver(**kw, precision=args.precision, device=local)
+    buf = solver._alloc()
+    stream = torch.cuda.current_stream(dev)
+    st = stream.cuda_stream
+
+    def step():
+        solver._device_solve(buf, st)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    solver._check_info(buf)
+
+    n0 = lib.mw_launch_count()
+    _lib.profile_enable(True)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    ms = e0.elapsed_time(e1)
+    launches = (lib.mw_launch_count() - n0) // max(args.steps, 1)
+    prof = _lib.profile_read()
+    _lib.profile_enable(False)
+    if pg:
+        t = torch.tensor([ms], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_step = ms / args.steps
+    value = world * args.steps / (ms / 1e3)
+
+    # correctness of what was timed: the 16x16 golden Y when available
+    y_dev = buf["Y"][: buf["n_p"], : buf["n_p"]].cpu().numpy().T
+    golden = ROOT / "tests" / "golden" / "array16x16.npz"
+    y_err = None
+    if golden.exists() and args.nx == 16:
+        g = np.load(golden)
+        y_err = float(np.max(np.abs(y_dev - g["y"])) / np.max(np.abs(g["y"])))
+
+    # e2e through the public API: host tables in, coefficients + Y out
+    e2e_ms = []
+    h2d = d2h = 0
+    for i in range(args.e2e_steps + 1):
+        s = momwire_b200.BSplineSolver(**kw, precision=args.precision, device=local)
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        sol = s.compute_port_solution()
+        b.record(stream)
+        torch.cuda.synchronize()
+        if i:  # first call is warm-up
+            e2e_ms.append(a.elapsed_time(b))
+        h2d, d2h = s.last_stats["h2d_bytes"], s.last_stats["d2h_bytes"]
+    e2e_step = sum(e2e_ms) / len(e2e_ms)
+    if pg:
+        t = torch.tensor([e2e_step], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_step = float(t.item())
+
+    # roofline of the dominant kernel class
+    peaks = {}
+    try:
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except OSError:
+        pass
+    dom = max(prof.items(), key=lambda kv: kv[1][1]) if prof else None
+    roof = None
+    if dom:
+        name, (cnt, tms, fl, by) = dom
+        achieved = fl / (tms / 1e3) / 1e12
+        # FP64 work has no measured peak in MEASURED_PEAKS.json: the nominal
+        # B200 FP64 rate is the denominator there.
+        fp64_nominal = 37.0
+        roof = {"kernel": name, "bound": "fp64", "achieved": achieved, "peak": fp64_nominal, "unit": "TFLOP/s",
+                "frac": achieved / fp64_nominal, "traffic": None, "launches_per_step": cnt / args.steps,
+                "avg_launch_ms": tms / cnt, "peak_source": "nominal B200 FP64 (no FP64 entry in MEASURED_PEAKS)"}
+    breakdown = {k: {"launches": v[0] / args.steps, "ms_per_step": v[1] / args.steps,
+                     "tflops": (v[2] / (v[1] / 1e3) / 1e12) if v[1] > 0 and v[2] > 0 else None}
+                 for k, v in prof.items()}
+
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_step,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "complex128" if args.precision == "fp64" else "complex64+fp64-refine",
+        "data": "synthetic (seeded dipole array)",
+        "config": {"workload": WORKLOAD, "n_unknowns": buf["n"], "ports": buf["n_p"], "precision": args.precision,
+                   "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (Z = 1.76 GB per step)"},
+        "e2e": {"value": world * 1e3 / e2e_step, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "ms_per_step": e2e_step},
+        "gpu_launches": int(launches),
+        "roofline": roof,
+        "kernels": breakdown,
+        "clocks": clocks.summary(),
+        "y_rel_err_vs_reference": y_err,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_sample(kw)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.destroy_process_group()
+
+
+def main():
+    args = parse()
+    from momwire_b200.workloads import dipole_array
+
+    kw = dipole_array(args.nx, args.nx)
+    if args.impl == "reference":
+        run_reference(args, kw)
+    else:
+        run_b200(args, kw)
+
+
+if __name__ == "__main__":
+    main()

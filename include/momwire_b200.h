@@ -1,0 +1,251 @@
+/*
+ * momwire_b200 — C ABI of the B200 (sm_100a) dense-solve path for momwire's
+ * B-spline Galerkin thin-wire solver.
+ *
+ * Every entry point takes plain pointers and sizes.  Pointers marked
+ * "device" must be device memory of the current CUDA device; the caller
+ * owns every buffer.  `stream` is a cudaStream_t passed as void* (NULL =
+ * the legacy default stream).  All calls are asynchronous on `stream`
+ * unless stated otherwise and return an mw_status (0 = success).
+ *
+ * The reference (momwire 0.37.0) reaches the same work through its
+ * pybind11 module `momwire._accelerators` and scipy's LAPACK; each
+ * declaration cites the reference interface it replaces
+ * (paths relative to the momwire source tree, src/momwire/).
+ *
+ * Matrix layout: complex values are interleaved (re, im) pairs of the
+ * element type.  Dense matrices are column-major with a leading dimension
+ * (the layout scipy.linalg.solve factors in place, bspline.py:2432).
+ */
+#ifndef MOMWIRE_B200_H
+#define MOMWIRE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t mw_status;
+
+#define MW_OK             0
+#define MW_ERR_INVALID   -1  /* bad argument (size, pointer, degree)        */
+#define MW_ERR_CUDA      -2  /* a CUDA runtime call failed                  */
+#define MW_ERR_CANCELLED -3  /* the host cancel flag was raised             */
+#define MW_ERR_TIMEOUT   -4  /* a bounded device wait gave up               */
+#define MW_ERR_SINGULAR  -5  /* exact zero pivot (LAPACK info > 0)          */
+#define MW_ERR_WORKSPACE -6  /* workspace smaller than the size query asked */
+
+/* Library version (major*10000 + minor*100 + patch). */
+int32_t mw_version(void);
+
+/* Human-readable text for the last error raised on this host thread. */
+const char* mw_last_error(void);
+
+/* Number of kernels this library has launched in this process (a running
+ * host-side count; the difference across a region counts its launches). */
+int64_t mw_launch_count(void);
+
+/* Optional per-kernel-class timing with CUDA events recorded around each
+ * launch on its own stream (for roofline figures).  Classes: 0 same-edge
+ * table, 1 fill, 2 image fill, 3 LU panel, 4 row swaps, 5 triangular solve
+ * block, 6 complex128 GEMM, 7 tensor-core complex GEMM, 8 refinement,
+ * 9 other.  mw_profile_enable(1) clears the counters and starts recording;
+ * mw_profile_read synchronises the recorded events and returns the launch
+ * count, summed device time and the algorithmic flops / bytes of a class. */
+void mw_profile_enable(int32_t on);
+int32_t mw_profile_read(int32_t cls, int64_t* launches, double* total_ms,
+                        double* flops, double* bytes);
+
+/* Ground models served by the fill (bspline.py:182-287 ground kwargs). */
+#define MW_GROUND_NONE        0  /* free space                              */
+#define MW_GROUND_PEC         1  /* perfect image, ground_eps=None          */
+#define MW_GROUND_REFL        2  /* ground_model="refl-coef" (Fresnel)      */
+#define MW_GROUND_SOMM_IMAGE  3  /* ground_model="sommerfeld": C2 image     */
+
+/* Phi-term image-charge weighting for MW_GROUND_REFL
+ * (_ground_refl.py:243-269, ground_phi_mode). */
+#define MW_PHI_RHO_V   0
+#define MW_PHI_IMAGE   1
+#define MW_PHI_NORMAL  2
+#define MW_PHI_BLEND   3
+
+/*
+ * Segment geometry of one structure, all device pointers.
+ * Segments are numbered wire by wire, edge by edge (bspline.py:988-1093).
+ */
+typedef struct mw_segments {
+    int32_t        n_seg;
+    const double*  seg_l;        /* (n_seg, 3) segment start points          */
+    const double*  seg_r;        /* (n_seg, 3) segment end points            */
+    const double*  tangent;      /* (n_seg, 3) unit tangents                 */
+    const double*  radius;       /* (n_seg)    wire radius of each segment   */
+    const int32_t* edge;         /* (n_seg)    straight edge of each segment */
+    const int32_t* pos_in_edge;  /* (n_seg)    index along that edge         */
+    const int32_t* ek_group;     /* (n_seg) coaxial labels, or NULL (EK off) */
+    const int32_t* ek_group_img; /* (n_seg) labels of the mirrored sources
+                                    from the joint real+image scan, or NULL  */
+} mw_segments;
+
+/*
+ * Uniform straight edges: the unit of the same-edge analytic split.
+ * Table entry (edge e, delta = j - i) lives at row table_off[e] + delta +
+ * n_in_edge[e] - 1 of a (rows, d+1, d+1) complex128 table.
+ */
+typedef struct mw_edges {
+    int32_t        n_edge;
+    const int32_t* n_in_edge;   /* (n_edge) segments per edge (device)      */
+    const int64_t* table_off;   /* (n_edge) first table row (device)        */
+    const double*  h;           /* (n_edge) segment length (device)         */
+    const double*  radius;      /* (n_edge) radius (device)                 */
+    int64_t        table_rows;  /* sum over edges of 2*n_in_edge - 1        */
+    int32_t        max_n;       /* max n_in_edge                            */
+} mw_edges;
+
+/*
+ * Basis tables (bspline.py:1216-1414): basis m has d+1 wings; wing a lies
+ * on segment supp[m*(d+1)+a] (-1 = padded wing) with monomial coefficients
+ * polys[(m*(d+1)+a)*(d+1)+p] of u^p, u the local arc length.
+ *
+ * Tiles: the fill works on tiles of consecutive bases.  Tile t covers
+ * bases [tile_first[t], tile_first[t]+tile_nb[t]) whose wings touch the
+ * tile_ns[t] segments listed at tile_seg[t*max_tile_seg ...]; loc[m*(d+1)+a]
+ * is the position of wing (m,a)'s segment in its own tile's list (-1 for a
+ * padded wing).  Built on the host by momwire_b200._tables.
+ */
+typedef struct mw_basis {
+    int32_t        degree;       /* 1 or 2                                  */
+    int32_t        n_basis;
+    const int32_t* supp;         /* (n_basis, d+1) device                   */
+    const double*  polys;        /* (n_basis, d+1, d+1) device              */
+    int32_t        n_tile;
+    int32_t        max_tile_basis;  /* <= 16                                */
+    int32_t        max_tile_seg;    /* <= MW_MAX_TILE_SEG                   */
+    const int32_t* tile_first;   /* (n_tile) device                         */
+    const int32_t* tile_nb;      /* (n_tile) device                         */
+    const int32_t* tile_ns;      /* (n_tile) device                         */
+    const int32_t* tile_seg;     /* (n_tile, max_tile_seg) device           */
+    const int32_t* loc;          /* (n_basis, d+1) device                   */
+} mw_basis;
+
+#define MW_MAX_TILE_BASIS 16
+#define MW_MAX_TILE_SEG   24
+
+/* Physical parameters of one frequency (bspline.py:343-346, 151-152). */
+typedef struct mw_freq {
+    double k;        /* wavenumber  = omega / c                             */
+    double omega;    /* angular frequency                                   */
+    double eps0;     /* 8.8541878188e-12 (the solver's own constants)       */
+    double mu0;      /* 1.25663706127e-6                                    */
+} mw_freq;
+
+/* Ground description for the image fill (_ground_spec.py:90-126). */
+typedef struct mw_ground {
+    int32_t model;        /* MW_GROUND_*                                    */
+    int32_t phi_mode;     /* MW_PHI_* (MW_GROUND_REFL only)                 */
+    double  ground_z;
+    double  eps_re, eps_im;  /* complex relative permittivity eps~(omega)    */
+} mw_ground;
+
+/*
+ * Same-edge Toeplitz table: static (closed-kernel 1/R, + EK correction)
+ * plus smooth (exp(-jkR)-1)/R moments for every uniform edge and every
+ * offset delta.  Replaces seg_seg_static_moments_bspline_uniform[_ek]
+ * (_accelerators.cpp:2954/2959, called from _bspline_kernels.py:333) and
+ * seg_seg_reg_moments_bspline_swept[_ek] (_accelerators.cpp:330/339,
+ * called from _bspline_kernels.py:480).
+ * out: (edges->table_rows, d+1, d+1) complex128, device.
+ */
+mw_status mw_same_edge_table(const mw_edges* edges, int32_t degree,
+                             int32_t n_qp, int32_t extended_kernel,
+                             double k, double* out, void* stream);
+
+/*
+ * Off-edge moment tensor J[p][P][i][j] over two segment sets (real
+ * sources, or sources mirrored through z = ground_z when mirror != 0).
+ * Replaces seg_seg_full_moments_bspline[_ek] (_accelerators.cpp:2683/2740,
+ * called from _bspline_kernels.py:599).  Used by the parity tests; the
+ * product fill never materialises J.
+ * seg_i / seg_j: segment sets (device); groups_i/groups_j may be NULL.
+ * out: (d+1, d+1, n_i, n_j) complex128, device.
+ */
+mw_status mw_offedge_moments(const mw_segments* seg_i, const mw_segments* seg_j,
+                             int32_t degree, int32_t n_qp, double k,
+                             int32_t mirror, double ground_z,
+                             const int32_t* groups_i, const int32_t* groups_j,
+                             double* out, void* stream);
+
+/*
+ * Fused Galerkin fill: Z = j w mu sum (t.t) C J C + (1/(j w eps)) sum C' J C'
+ * over every basis pair, with same-edge pairs taken from `table` (from
+ * mw_same_edge_table at the same k) and every other pair by n_qp x n_qp
+ * Gauss-Legendre quadrature of exp(-jkR)/(4 pi R).  Writes all of Z.
+ * Replaces _compute_Z_operator's free-space part: _build_J_blocks +
+ * assemble_Z_bspline (bspline.py:2222-2348, _accelerators.cpp:1767) and
+ * the chunked route _compute_Z_dense_chunked + assemble_Z_bspline_windowed
+ * (bspline.py:2386-2550, _accelerators.cpp:1447).
+ * Z: complex128 column-major (n_basis x n_basis, leading dim ldz), device.
+ * Z32 (optional, may be NULL): complex64 copy written in the same pass
+ * (leading dim ldz32), for the mixed-precision factorisation.
+ */
+mw_status mw_fill_z(const mw_segments* seg, const mw_basis* basis,
+                    const double* table, const mw_edges* edges,
+                    const mw_freq* freq, int32_t n_qp,
+                    double* Z, int64_t ldz, float* Z32, int64_t ldz32,
+                    void* stream);
+
+/*
+ * Ground image: Z -= weighted Galerkin assembly over mirrored sources
+ * (PEC mirror tangent dot; Fresnel w_A/w_Phi per segment pair; or the
+ * Sommerfeld C2-scaled exact image).  Replaces _accumulate_Z_image_chunked
+ * (bspline.py:2552-2661) with assemble_Z_bspline_weighted_windowed
+ * (_accelerators.cpp:1612) and the weight producers of
+ * _potential_ground.py:711-810.  Z32 as for mw_fill_z (may be NULL; when
+ * given it is overwritten with the updated Z).
+ */
+mw_status mw_fill_z_image(const mw_segments* seg, const mw_basis* basis,
+                          const mw_ground* ground, const mw_freq* freq,
+                          int32_t n_qp, double* Z, int64_t ldz,
+                          float* Z32, int64_t ldz32, void* stream);
+
+/*
+ * Workspace (bytes, device) needed by mw_zgetrf / mw_cgetrf for order n.
+ */
+size_t mw_getrf_workspace_size(int64_t n);
+
+/*
+ * In-place LU with partial pivoting of a complex128 column-major matrix,
+ * P A = L U, pivots 1-based as LAPACK zgetrf (ipiv device, length n).
+ * Replaces LAPACK zgetrf inside scipy.linalg.solve (bspline.py:2979).
+ * `info` (device, 1 int32) receives LAPACK's info (0, or j+1 for an exact
+ * zero pivot U(j,j)).  `cancel` (host-mapped or device int32, may be NULL)
+ * is polled between panels; a raised flag returns MW_ERR_CANCELLED.
+ */
+mw_status mw_zgetrf(int64_t n, double* A, int64_t lda, int32_t* ipiv,
+                    int32_t* info, void* workspace, size_t workspace_bytes,
+                    const volatile int32_t* cancel, void* stream);
+
+/*
+ * Solve A X = B with the factors of mw_zgetrf (LAPACK zgetrs, 'N'), B
+ * overwritten by X: (n x nrhs, leading dim ldb), complex128, device.
+ * Replaces the zgetrs half of scipy.linalg.solve (bspline.py:2979).
+ */
+mw_status mw_zgetrs(int64_t n, int64_t nrhs, const double* LU, int64_t lda,
+                    const int32_t* ipiv, double* B, int64_t ldb, void* stream);
+
+/*
+ * C = alpha * op(A) * op(B) + beta * C for complex128 column-major
+ * matrices, op = 'N' or 'T' (transA/transB 0/1).  Used for the KCL Schur
+ * step and Y = B^T X (bspline.py:2984-2989, 4179).
+ */
+mw_status mw_zgemm(int32_t transA, int32_t transB, int64_t m, int64_t n, int64_t k,
+                   double alpha_re, double alpha_im, const double* A, int64_t lda,
+                   const double* B, int64_t ldb, double beta_re, double beta_im,
+                   double* C, int64_t ldc, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MOMWIRE_B200_H */

@@ -1,0 +1,167 @@
+"""ctypes binding of ``libmomwire_b200.so`` (the C ABI in include/momwire_b200.h).
+
+The library is loaded from ``momwire_b200/lib/`` (built in-tree by
+``python -m momwire_b200.build``).  Loading fails loudly: there is no CPU
+fallback behind this module.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "lib" / "libmomwire_b200.so"
+
+MW_OK = 0
+MW_ERR_INVALID = -1
+MW_ERR_CUDA = -2
+MW_ERR_CANCELLED = -3
+MW_ERR_TIMEOUT = -4
+MW_ERR_SINGULAR = -5
+MW_ERR_WORKSPACE = -6
+
+MW_GROUND_NONE = 0
+MW_GROUND_PEC = 1
+MW_GROUND_REFL = 2
+MW_GROUND_SOMM_IMAGE = 3
+
+PHI_MODES = {"rho_v": 0, "image": 1, "normal": 2, "blend": 3}
+
+vp = C.c_void_p
+i32, i64, f64, sz = C.c_int32, C.c_int64, C.c_double, C.c_size_t
+
+
+class Segments(C.Structure):
+    _fields_ = [
+        ("n_seg", i32),
+        ("seg_l", vp),
+        ("seg_r", vp),
+        ("tangent", vp),
+        ("radius", vp),
+        ("edge", vp),
+        ("pos_in_edge", vp),
+        ("ek_group", vp),
+        ("ek_group_img", vp),
+    ]
+
+
+class Edges(C.Structure):
+    _fields_ = [
+        ("n_edge", i32),
+        ("n_in_edge", vp),
+        ("table_off", vp),
+        ("h", vp),
+        ("radius", vp),
+        ("table_rows", i64),
+        ("max_n", i32),
+    ]
+
+
+class BasisT(C.Structure):
+    _fields_ = [
+        ("degree", i32),
+        ("n_basis", i32),
+        ("supp", vp),
+        ("polys", vp),
+        ("n_tile", i32),
+        ("max_tile_basis", i32),
+        ("max_tile_seg", i32),
+        ("tile_first", vp),
+        ("tile_nb", vp),
+        ("tile_ns", vp),
+        ("tile_seg", vp),
+        ("loc", vp),
+    ]
+
+
+class Freq(C.Structure):
+    _fields_ = [("k", f64), ("omega", f64), ("eps0", f64), ("mu0", f64)]
+
+
+class Ground(C.Structure):
+    _fields_ = [
+        ("model", i32),
+        ("phi_mode", i32),
+        ("ground_z", f64),
+        ("eps_re", f64),
+        ("eps_im", f64),
+    ]
+
+
+# name -> (restype, argtypes)
+_SIGS = {
+    "mw_version": (i32, []),
+    "mw_last_error": (C.c_char_p, []),
+    "mw_launch_count": (i64, []),
+    "mw_profile_enable": (None, [i32]),
+    "mw_profile_read": (i32, [i32, C.POINTER(i64), C.POINTER(f64), C.POINTER(f64), C.POINTER(f64)]),
+    "mw_same_edge_table": (i32, [C.POINTER(Edges), i32, i32, i32, f64, vp, vp]),
+    "mw_offedge_moments": (i32, [C.POINTER(Segments), C.POINTER(Segments), i32, i32, f64, i32, f64, vp, vp, vp, vp]),
+    "mw_fill_z": (i32, [C.POINTER(Segments), C.POINTER(BasisT), vp, C.POINTER(Edges), C.POINTER(Freq), i32, vp, i64, vp, i64, vp]),
+    "mw_fill_z_image": (i32, [C.POINTER(Segments), C.POINTER(BasisT), C.POINTER(Ground), C.POINTER(Freq), i32, vp, i64, vp, i64, vp]),
+    "mw_getrf_workspace_size": (sz, [i64]),
+    "mw_zgetrf": (i32, [i64, vp, i64, vp, vp, vp, sz, vp, vp]),
+    "mw_zgetrs": (i32, [i64, i64, vp, i64, vp, vp, i64, vp]),
+    "mw_zgemm": (i32, [i32, i32, i64, i64, i64, f64, f64, vp, i64, vp, i64, f64, f64, vp, i64, vp]),
+}
+
+EXPORTED = tuple(_SIGS)
+
+PROFILE_CLASSES = ("same_edge_table", "fill", "fill_image", "lu_panel", "laswp", "trsm", "zgemm",
+                   "cgemm_tc", "refine", "misc")
+
+
+def profile_enable(on=True):
+    load().mw_profile_enable(1 if on else 0)
+
+
+def profile_read():
+    """{class name: (launches, total_ms, flops, bytes)} since profile_enable."""
+    lib = load()
+    out = {}
+    for i, name in enumerate(PROFILE_CLASSES):
+        n, ms, fl, by = i64(), f64(), f64(), f64()
+        lib.mw_profile_read(i, C.byref(n), C.byref(ms), C.byref(fl), C.byref(by))
+        if n.value:
+            out[name] = (int(n.value), float(ms.value), float(fl.value), float(by.value))
+    return out
+
+_lib = None
+
+
+class NativeError(RuntimeError):
+    """A call into libmomwire_b200 returned a non-zero status."""
+
+    def __init__(self, name, status, text):
+        super().__init__(f"{name} failed with status {status}: {text}")
+        self.status = status
+
+
+def load():
+    """Load (once) and return the native library; raises if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = os.environ.get("MOMWIRE_B200_LIB", str(LIB_PATH))
+    if not Path(path).exists():
+        raise ImportError(
+            f"momwire_b200 native library not found at {path}; build it with "
+            "`python -m momwire_b200.build` (there is no CPU fallback)"
+        )
+    lib = C.CDLL(path)
+    for name, (res, args) in _SIGS.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def call(name, *args):
+    """Invoke an mw_* entry point and raise NativeError on a bad status."""
+    lib = load()
+    st = getattr(lib, name)(*args)
+    if st != MW_OK:
+        raise NativeError(name, st, lib.mw_last_error().decode(errors="replace"))
+    return st

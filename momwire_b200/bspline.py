@@ -1,0 +1,894 @@
+"""B200-native drop-in for momwire's ``BSplineSolver`` dense-solve path.
+
+Same constructor keywords, the same ``feeds=`` / ``junction_ports=`` /
+``node_gaps=`` port surface and the same ``PortSolution`` result as the
+reference (``bspline.py:332``, ``:511``, ``:4053``).  Host code here builds
+the O(N) tables (geometry, basis, ports) and drives the native library
+``libmomwire_b200.so`` through its C ABI; torch tensors serve only as
+device buffers.  The fill and the factorisation run on the GPU:
+
+* ``precision="fp64"`` (default): complex128 fill and complex128 LU --
+  the plain drop-in, matching the reference to ~1e-10;
+* ``precision="mixed"``: complex64 factorisation on the tensor cores with
+  FP64 iterative refinement against the FP64 fill.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from contextlib import contextmanager
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from . import _tables as T
+from ._port_solution import PortSolution
+
+
+class SolveAborted(Exception):
+    """Solve was cancelled via a :class:`CancelToken`; no result was produced."""
+
+
+class CancelToken:
+    """One-shot cancellation flag shared with a solve (same surface as the
+    reference's ``_cancel.CancelToken``).  The factorisation polls it
+    between panels; the host polls it at phase seams."""
+
+    def __init__(self):
+        self._flag = np.zeros(1, dtype=np.int32)
+
+    def cancel(self):
+        self._flag[0] = 1
+
+    @property
+    def cancelled(self):
+        return bool(self._flag[0])
+
+    def raise_if_cancelled(self):
+        if self._flag[0]:
+            raise SolveAborted()
+
+    @property
+    def ptr(self):
+        return self._flag.ctypes.data
+
+
+@dataclass(frozen=True)
+class _SplineBasis:
+    """Opaque ``PortSolution.basis`` payload (reference ``bspline.py:288``)."""
+
+    geom: object
+    supp_seg: object
+    polys: object
+    wire_knots: object
+    wire_basis_global: object
+    n_poly: int
+
+
+def _torch():
+    import torch
+
+    if not torch.cuda.is_available():
+        raise RuntimeError("momwire_b200 needs a CUDA device (B200); none is visible")
+    return torch
+
+
+class _DeviceTables:
+    """Device copies of the k-independent tables plus their C structs."""
+
+    def __init__(self, solver, geom: T.Geometry, basis: T.Basis, tiles: T.Tiles, ek, dev):
+        torch = _torch()
+        self.keep = []
+        self.h2d_bytes = 0
+
+        def up(a, dtype):
+            t = torch.from_numpy(np.ascontiguousarray(a, dtype=dtype)).to(dev)
+            self.keep.append(t)
+            self.h2d_bytes += t.numel() * t.element_size()
+            return t
+
+        self.seg_l = up(geom.seg_l, np.float64)
+        self.seg_r = up(geom.seg_r, np.float64)
+        self.tan = up(geom.tangents, np.float64)
+        self.rad = up(geom.radius, np.float64)
+        self.edge = up(geom.edge, np.int32)
+        self.pos = up(geom.pos_in_edge, np.int32)
+        self.grp = up(ek[0], np.int32) if ek is not None else None
+        self.grp_img = up(ek[1], np.int32) if (ek is not None and ek[1] is not None) else None
+        self.seg = _lib.Segments(
+            geom.n,
+            self.seg_l.data_ptr(),
+            self.seg_r.data_ptr(),
+            self.tan.data_ptr(),
+            self.rad.data_ptr(),
+            self.edge.data_ptr(),
+            self.pos.data_ptr(),
+            self.grp.data_ptr() if self.grp is not None else None,
+            self.grp_img.data_ptr() if self.grp_img is not None else None,
+        )
+        off, rows = T.edge_table_offsets(geom.edge_n)
+        self.e_n = up(geom.edge_n, np.int32)
+        self.e_off = up(off, np.int64)
+        self.e_h = up(geom.edge_h, np.float64)
+        self.e_r = up(geom.edge_radius, np.float64)
+        self.table_rows = rows
+        self.edges = _lib.Edges(
+            len(geom.edge_n),
+            self.e_n.data_ptr(),
+            self.e_off.data_ptr(),
+            self.e_h.data_ptr(),
+            self.e_r.data_ptr(),
+            rows,
+            int(geom.edge_n.max()),
+        )
+        self.supp = up(basis.supp, np.int32)
+        self.polys = up(basis.polys, np.float64)
+        self.t_first = up(tiles.first, np.int32)
+        self.t_nb = up(tiles.nb, np.int32)
+        self.t_ns = up(tiles.ns, np.int32)
+        self.t_seg = up(tiles.seg, np.int32)
+        self.loc = up(tiles.loc, np.int32)
+        self.basis = _lib.BasisT(
+            basis.degree,
+            basis.n,
+            self.supp.data_ptr(),
+            self.polys.data_ptr(),
+            len(tiles.first),
+            tiles.max_basis,
+            tiles.max_seg,
+            self.t_first.data_ptr(),
+            self.t_nb.data_ptr(),
+            self.t_ns.data_ptr(),
+            self.t_seg.data_ptr(),
+            self.loc.data_ptr(),
+        )
+
+
+class BSplineSolver:
+    """Degree-d B-spline Galerkin MoM on multi-wire polylines with
+    junctions, filled and factorised on a B200.
+
+    Keyword arguments follow the reference constructor (``bspline.py:511-548``).
+    Served: degree 1-2, reduced or extended thin-wire kernel, free space,
+    PEC image and reflection-coefficient ground, point/segment feeds,
+    junctions, junction ports and node gaps, per-wire radii.  Additional:
+
+    precision : "fp64" (default) or "mixed".
+    device : CUDA device index or torch.device (default: current device).
+    """
+
+    eps = 8.8541878188e-12
+    mu = 1.25663706127e-6
+
+    def __init__(
+        self,
+        *,
+        wires,
+        n_per_edge_per_wire=None,
+        degree=2,
+        feed_wire_index=0,
+        feed_arclength=None,
+        feeds=None,
+        feed_model="point",
+        feed_smoothing_factor=None,
+        junctions=None,
+        junction_ports=None,
+        node_gaps=None,
+        n_qp_pair=4,
+        n_qp_source=16,
+        extended_kernel=False,
+        wavelength=22,
+        halfdriver_factor=0.962,
+        wire_radius=0.0005,
+        wire_conductivity=None,
+        insulation_radius=None,
+        insulation_eps_r=None,
+        nsegs=101,
+        ground_z=None,
+        ground_eps=None,
+        ground_phi_mode="normal",
+        ground_model="refl-coef",
+        n_qp_sommerfeld=3,
+        use_singular_enrichment=False,
+        swept_mem_mb=256,
+        cancel=None,
+        precision="fp64",
+        device=None,
+    ):
+        self._cancel = cancel
+        if degree < 1:
+            raise ValueError(f"degree must be >= 1, got {degree}")
+        if degree > 2:
+            raise NotImplementedError(
+                "degree > 2 needs scripts/derive_bspline_static_moments.py "
+                "to be re-run with a larger MAX_D"
+            )
+        if not wires:
+            raise ValueError("wires must be non-empty")
+        if use_singular_enrichment:
+            raise NotImplementedError("use_singular_enrichment is outside the B200 dense path")
+        if wire_conductivity is not None or insulation_radius is not None or insulation_eps_r is not None:
+            raise NotImplementedError("distributed wire loading is outside the B200 dense path")
+        if precision not in ("fp64", "mixed"):
+            raise ValueError(f"precision must be 'fp64' or 'mixed', got {precision!r}")
+        self.precision = precision
+        self.degree = int(degree)
+        self.wavelength = wavelength
+        self.halfdriver_factor = halfdriver_factor
+        self.wire_radius = wire_radius
+        self.nsegs = nsegs
+        self.ground_z = ground_z
+        if ground_eps is not None and ground_z is None:
+            raise ValueError("ground_eps requires ground_z to be set")
+        if ground_phi_mode not in _lib.PHI_MODES:
+            raise ValueError(
+                f"ground_phi_mode must be one of {tuple(_lib.PHI_MODES)}, got {ground_phi_mode!r}"
+            )
+        self.ground_eps = ground_eps
+        self.ground_phi_mode = ground_phi_mode
+        if ground_model not in ("refl-coef", "sommerfeld"):
+            raise ValueError(f"ground_model must be 'refl-coef' or 'sommerfeld', got {ground_model!r}")
+        if ground_model == "sommerfeld" and ground_eps is None:
+            raise ValueError("ground_model='sommerfeld' requires ground_eps")
+        self.ground_model = ground_model
+        self.n_qp_sommerfeld = int(n_qp_sommerfeld)
+        self.extended_kernel = bool(extended_kernel)
+        self.swept_mem_mb = int(swept_mem_mb)
+        if self.swept_mem_mb < 1:
+            raise ValueError(f"swept_mem_mb must be >= 1, got {swept_mem_mb}")
+        if feed_model not in ("point", "segment"):
+            raise ValueError(f"feed_model must be 'point' or 'segment', got {feed_model!r}")
+        if feed_model == "segment" and feed_smoothing_factor is not None:
+            raise ValueError(
+                "feed_model='segment' and feed_smoothing_factor are mutually "
+                "exclusive — both replace the point drive with a spread one"
+            )
+        self.feed_model = feed_model
+        self.feed_smoothing_factor = feed_smoothing_factor
+        self.n_qp_source = int(n_qp_source)
+
+        self.c = 1 / np.sqrt(self.eps * self.mu)
+        self.freq = self.c / self.wavelength
+        self.omega = 2 * np.pi * self.freq
+        self.k = self.omega / self.c
+        self.halfdriver = self.halfdriver_factor * self.wavelength / 4
+
+        self.wires_polylines = [np.asarray(w, dtype=float) for w in wires]
+        for i, pl in enumerate(self.wires_polylines):
+            if pl.ndim != 2 or pl.shape[0] < 2 or pl.shape[1] != 3:
+                raise ValueError(f"wire {i}: polyline must be (M, 3) with M >= 2")
+        n_w = len(self.wires_polylines)
+        if self.ground_eps is not None and self.ground_model == "refl-coef":
+            touching = self._contact_ends()
+            if touching:
+                where = ", ".join(f"wire {w} {kind}" for w, kind in touching)
+                raise NotImplementedError(
+                    f"{where} lies in the ground plane: ground contact is refused "
+                    "under ground_model='refl-coef' (use ground_model='sommerfeld')"
+                )
+        r = np.asarray(wire_radius, dtype=float)
+        if r.ndim == 0:
+            r = np.full(n_w, float(r))
+        elif r.shape != (n_w,):
+            raise ValueError(
+                f"wire_radius: expected a scalar or a length-{n_w} sequence "
+                f"(one entry per wire), got shape {r.shape}"
+            )
+        if not np.all(np.isfinite(r)) or np.any(r <= 0.0):
+            raise ValueError(f"wire_radius entries must be positive and finite, got {r}")
+        self._radius_per_wire = r
+
+        if n_per_edge_per_wire is None:
+            n_per_edge_per_wire = [None] * n_w
+        if len(n_per_edge_per_wire) != n_w:
+            raise ValueError(f"n_per_edge_per_wire length {len(n_per_edge_per_wire)} != n_wires {n_w}")
+        self.n_per_edge_per_wire = []
+        for i, (pl, npe) in enumerate(zip(self.wires_polylines, n_per_edge_per_wire)):
+            n_edges_w = pl.shape[0] - 1
+            if npe is None:
+                npe = self.nsegs
+            if np.isscalar(npe):
+                npe = [int(npe)] * n_edges_w
+            npe = list(npe)
+            if len(npe) != n_edges_w:
+                raise ValueError(f"wire {i}: n_per_edge length {len(npe)} != n_edges {n_edges_w}")
+            self.n_per_edge_per_wire.append(npe)
+
+        if feeds is None:
+            if not (0 <= feed_wire_index < n_w):
+                raise ValueError(f"feed_wire_index {feed_wire_index} out of range")
+            self.feeds = [(int(feed_wire_index), feed_arclength, 1.0 + 0.0j)]
+        else:
+            if len(feeds) == 0 and not junction_ports and not node_gaps:
+                raise ValueError("feeds must contain at least one entry")
+            norm = []
+            for i, f in enumerate(feeds):
+                if len(f) != 3:
+                    raise ValueError(f"feeds[{i}]: expected (wire_index, arclength, voltage), got {f!r}")
+                w_i, arc_i, v_i = f
+                if not (0 <= w_i < n_w):
+                    raise ValueError(f"feeds[{i}]: wire_index {w_i} out of range [0, {n_w})")
+                arc_i = None if arc_i is None else float(arc_i)
+                norm.append((int(w_i), arc_i, complex(v_i)))
+            self.feeds = norm
+        self.feed_wire_index = self.feeds[0][0] if self.feeds else None
+        self.feed_arclength = self.feeds[0][1] if self.feeds else None
+        self.n_qp_pair = int(n_qp_pair)
+        if not (1 <= self.n_qp_pair <= 8):
+            raise ValueError(f"n_qp_pair must be in [1, 8], got {n_qp_pair}")
+
+        self.junctions = []
+        if junctions is not None:
+            for j, jw in enumerate(junctions):
+                if len(jw) < 1:
+                    raise ValueError(f"junction {j}: need >= 1 wire-end")
+                normalized = []
+                for w, end in jw:
+                    if not (0 <= w < n_w):
+                        raise ValueError(f"junction {j}: wire_idx {w} out of range [0, {n_w})")
+                    if end not in ("start", "end"):
+                        raise ValueError(f"junction {j}: end must be 'start' or 'end', got {end!r}")
+                    normalized.append((int(w), end))
+                self.junctions.append(normalized)
+            self._check_junction_coincidence()
+
+        self.junction_ports = []
+        if junction_ports is not None:
+            seen = set()
+            for p in junction_ports:
+                if isinstance(p, (int, np.integer)):
+                    j_idx, volt = int(p), 0j
+                else:
+                    j_idx, volt = int(p[0]), complex(p[1])
+                if not (0 <= j_idx < len(self.junctions)):
+                    raise ValueError(
+                        f"junction_ports: junction index {j_idx} out of range [0, {len(self.junctions)})"
+                    )
+                if j_idx in seen:
+                    raise ValueError(f"junction_ports: junction {j_idx} listed twice")
+                seen.add(j_idx)
+                self.junction_ports.append((j_idx, volt))
+
+        self.node_gaps = []
+        if node_gaps is not None:
+            end_to_junction = {m: j for j, jw in enumerate(self.junctions) for m in jw}
+            seen_m, seen_j = set(), set()
+            ported = {j for j, _v in self.junction_ports}
+            for i, g in enumerate(node_gaps):
+                if len(g) != 3:
+                    raise ValueError(
+                        f"node_gaps[{i}]: expected (wire_index, 'start'|'end', voltage), got {g!r}"
+                    )
+                w_i, end_i, v_i = g
+                if not (0 <= w_i < n_w):
+                    raise ValueError(f"node_gaps[{i}]: wire_index {w_i} out of range [0, {n_w})")
+                if end_i not in ("start", "end"):
+                    raise ValueError(f"node_gaps[{i}]: end must be 'start' or 'end', got {end_i!r}")
+                member = (int(w_i), end_i)
+                j_idx = end_to_junction.get(member)
+                if j_idx is None:
+                    raise ValueError(
+                        f"node_gaps[{i}]: wire {w_i} {end_i!r} is not a member of any junction group — a "
+                        "series node gap lives at a junction; for a feed inside a wire use feeds="
+                    )
+                if len(self.junctions[j_idx]) < 2:
+                    raise ValueError(
+                        f"node_gaps[{i}]: junction {j_idx} has a single member — there is no "
+                        "through-current path to be in series with (a lone-end attachment is junction_ports=)"
+                    )
+                if member in seen_m:
+                    raise ValueError(f"node_gaps[{i}]: wire {w_i} {end_i!r} listed twice")
+                if j_idx in seen_j:
+                    raise ValueError(
+                        f"node_gaps[{i}]: junction {j_idx} already carries a node gap — one series gap per junction"
+                    )
+                if j_idx in ported:
+                    raise ValueError(
+                        f"node_gaps[{i}]: junction {j_idx} is also a junction port — the shunt and series "
+                        "ports of one node cannot be driven together yet"
+                    )
+                seen_m.add(member)
+                seen_j.add(j_idx)
+                self.node_gaps.append((int(w_i), end_i, complex(v_i)))
+
+        self._device = device
+        self._cached_geometry = None
+        self._cached_basis = None
+        self._cached_tiles = None
+        self._cached_dev = None
+        self._cached_ek = None
+        self.last_stats = {}
+
+    # ------------------------------------------------------------------ misc
+    def _checkpoint(self):
+        if self._cancel is not None:
+            self._cancel.raise_if_cancelled()
+
+    def _contact_ends(self):
+        """``_ground_spec.contact_ends`` (reference ``_ground_spec.py:156``)."""
+        if self.ground_z is None:
+            return ()
+        out = []
+        for i, pl in enumerate(self.wires_polylines):
+            tol = T.touch_tol(pl)
+            if abs(float(pl[0, 2]) - self.ground_z) <= tol:
+                out.append((i, "start"))
+            if abs(float(pl[-1, 2]) - self.ground_z) <= tol:
+                out.append((i, "end"))
+        return tuple(sorted(out))
+
+    def _check_junction_coincidence(self):
+        """``_wire_spec.check_junction_coincidence`` (reference ``_wire_spec.py:62``)."""
+        for j, group in enumerate(self.junctions):
+            anchors, lens = [], []
+            for w, end in group:
+                pl = self.wires_polylines[w]
+                npe = self.n_per_edge_per_wire[w]
+                if end == "start":
+                    anchor, edge, count = pl[0], pl[1] - pl[0], npe[0]
+                else:
+                    anchor, edge, count = pl[-1], pl[-1] - pl[-2], npe[-1]
+                anchors.append(anchor)
+                lens.append(float(np.linalg.norm(edge)) / max(int(count), 1))
+            tol = max(1e-5, 1e-3 * min(lens))
+            w0, e0 = group[0]
+            for (w, e), a in zip(group[1:], anchors[1:]):
+                dist = float(np.linalg.norm(a - anchors[0]))
+                if dist > tol:
+                    raise ValueError(
+                        f"junction {j}: wire {w} {e!r} is {dist:.6g} from wire {w0} {e0!r} "
+                        f"(tolerance {tol:.3g}) — junction members must coincide"
+                    )
+
+    def _set_k(self, kk):
+        self.k = float(kk)
+        self.omega = self.k * self.c
+        self.wavelength = self.c / (self.omega / (2 * np.pi))
+
+    @contextmanager
+    def _k_restored(self):
+        saved = (self.k, self.wavelength, self.omega)
+        try:
+            yield
+        finally:
+            self.k, self.wavelength, self.omega = saved
+
+    # ------------------------------------------------------------ topology
+    def _wire_endpoint_status(self):
+        """``bspline.py:1108-1150``."""
+        n_w = len(self.wires_polylines)
+        st = ["free"] * n_w
+        en = ["free"] * n_w
+        for j, jw in enumerate(self.junctions):
+            for w, end in jw:
+                if end == "start":
+                    st[w] = j
+                else:
+                    en[w] = j
+        gz = self.ground_z
+        if gz is not None:
+            for w, pl in enumerate(self.wires_polylines):
+                tol = T.touch_tol(pl)
+                if float(pl[:, 2].min()) < gz - tol:
+                    raise ValueError(
+                        f"wire {w} dips below the ground plane "
+                        f"(min z = {pl[:, 2].min():.6g} < ground_z = {gz:g})"
+                    )
+                at = np.abs(pl[:, 2] - gz) <= tol
+                if np.any(at[:-1] & at[1:]):
+                    raise ValueError(
+                        f"wire {w} has an edge lying in the ground plane "
+                        "(both endpoints at ground_z) — degenerate over a conducting ground"
+                    )
+                if st[w] == "free" and at[0]:
+                    st[w] = "ground"
+                if en[w] == "free" and at[-1]:
+                    en[w] = "ground"
+        return st, en
+
+    def _grounded_junctions(self):
+        """``bspline.py:1152-1169``."""
+        gz = self.ground_z
+        if gz is None or not self.junctions:
+            return frozenset()
+        out = set()
+        for j, jw in enumerate(self.junctions):
+            w, end = jw[0]
+            pl = self.wires_polylines[w]
+            pt = pl[0] if end == "start" else pl[-1]
+            if abs(pt[2] - gz) <= T.touch_tol(pl):
+                out.add(j)
+        return frozenset(out)
+
+    def _geometry(self) -> T.Geometry:
+        if self._cached_geometry is None:
+            self._cached_geometry = T.build_geometry(
+                self.wires_polylines, self.n_per_edge_per_wire, self._radius_per_wire
+            )
+        return self._cached_geometry
+
+    def _basis(self) -> T.Basis:
+        if self._cached_basis is None:
+            st, en = self._wire_endpoint_status()
+            self._cached_basis = T.build_basis(
+                self._geometry(), self.degree, st, en, len(self.junctions), self._grounded_junctions()
+            )
+        return self._cached_basis
+
+    def _ek(self):
+        if not self.extended_kernel:
+            return None
+        if self._cached_ek is None:
+            self._cached_ek = T.ek_labels(self._geometry(), self.ground_z)
+        return self._cached_ek
+
+    def _torch_device(self):
+        torch = _torch()
+        if self._device is None:
+            return torch.device("cuda", torch.cuda.current_device())
+        if isinstance(self._device, int):
+            return torch.device("cuda", self._device)
+        return torch.device(self._device)
+
+    def _dev_tables(self) -> _DeviceTables:
+        if self._cached_dev is None:
+            geom, basis = self._geometry(), self._basis()
+            if self._cached_tiles is None:
+                self._cached_tiles = T.build_tiles(basis.supp)
+            self._cached_dev = _DeviceTables(self, geom, basis, self._cached_tiles, self._ek(), self._torch_device())
+        return self._cached_dev
+
+    # --------------------------------------------------------------- ports
+    def _split_kcl_ports(self, kcl_A):
+        """``bspline.py:1171-1214``."""
+        if not self.junction_ports:
+            return kcl_A, np.zeros((0, kcl_A.shape[1])), np.zeros(0, dtype=np.complex128)
+        grounded = self._grounded_junctions()
+        row_of, row = {}, 0
+        for j in range(len(self.junctions)):
+            if j not in grounded:
+                row_of[j] = row
+                row += 1
+        port_rows = []
+        for j_idx, _v in self.junction_ports:
+            if j_idx in grounded:
+                raise ValueError(
+                    f"junction {j_idx} is both grounded and a junction port — a grounded node's "
+                    "voltage is pinned by the ground image, so it cannot also be a driven port"
+                )
+            port_rows.append(row_of[j_idx])
+        keep = [r for r in range(kcl_A.shape[0]) if r not in set(port_rows)]
+        port_V = np.array([v for _j, v in self.junction_ports], dtype=np.complex128)
+        return kcl_A[keep, :], kcl_A[port_rows, :], port_V
+
+    def _source_vector(self, w, s_f):
+        """Galerkin drive column of one gap feed (``bspline.py:2806-2942``):
+        point (v_m = Phi_m(s_f)), segment-wide gap, or cos^2 bump."""
+        geom, basis = self._geometry(), self._basis()
+        d = self.degree
+        arc = geom.wire_arc[w]
+        knots = basis.knots[w]
+        if self.feed_smoothing_factor is None and self.feed_model == "point":
+            vals = T.basis_values(knots, d, [s_f])[0]
+        elif self.feed_model == "segment":
+            s = int(np.searchsorted(arc, s_f, side="right")) - 1
+            s = max(0, min(s, len(arc) - 2))
+            lo, hi = float(arc[s]), float(arc[s + 1])
+            xg, wg = T.gauss_legendre(self.n_qp_source)
+            t = 0.5 * (hi + lo) + 0.5 * (hi - lo) * xg
+            vals = T.basis_values(knots, d, t).T @ ((0.5 * (hi - lo) * wg) / (hi - lo))
+        else:
+            h = np.diff(arc)
+            s = int(np.searchsorted(arc, s_f, side="right")) - 1
+            s = max(0, min(s, len(h) - 1))
+            width = float(self.feed_smoothing_factor) * float(h[s])
+            half = width / 2.0
+            lo, hi = max(0.0, s_f - half), min(float(arc[-1]), s_f + half)
+            if lo >= hi:
+                raise ValueError("feed_smoothing_factor too large for wire — bump doesn't fit")
+            xg, wg = T.gauss_legendre(self.n_qp_source)
+            t = 0.5 * (hi + lo) + 0.5 * (hi - lo) * xg
+            wts = 0.5 * (hi - lo) * wg
+            delta = t - s_f
+            g = np.where(np.abs(delta) < half, (2.0 / width) * np.cos(np.pi * delta / width) ** 2, 0.0)
+            vals = np.einsum("qj,q,q->j", T.basis_values(knots, d, t), g, wts)
+        v = np.zeros(basis.n, dtype=np.complex128)
+        for j, _kind, _jn, _end, mg in basis.kept[w]:
+            v[mg] = vals[j]
+        return v
+
+    def _node_gap_columns(self):
+        """``bspline.py:3784-3818``."""
+        basis = self._basis()
+        cols = np.zeros((basis.n, len(self.node_gaps)))
+        volts = np.zeros(len(self.node_gaps), dtype=np.complex128)
+        if not self.node_gaps:
+            return cols, volts
+        grounded = self._grounded_junctions()
+        e2j = {m: j for j, jw in enumerate(self.junctions) for m in jw}
+        for p, (w, end, v) in enumerate(self.node_gaps):
+            j = e2j[(w, end)]
+            if j in grounded:
+                raise ValueError(
+                    f"node_gaps[{p}]: junction {j} is grounded — a series gap between a wire and the "
+                    "ground stake is not supported"
+                )
+            for _jl, kind, jn, en, mg in basis.kept[w]:
+                if kind == "dir" and jn == j and en == end:
+                    cols[mg, p] = 1.0 if end == "start" else -1.0
+            volts[p] = v
+        return cols, volts
+
+    def _port_columns(self):
+        """(B, kcl_con) with ports [feeds | junction ports | node gaps]
+        (``bspline.py:3841-3867``)."""
+        geom, basis = self._geometry(), self._basis()
+        B = np.zeros((basis.n, len(self.feeds)), dtype=np.complex128)
+        for i, (w, arc_i, _v) in enumerate(self.feeds):
+            s_f = arc_i if arc_i is not None else geom.wire_arc[w][-1] / 2.0
+            B[:, i] = self._source_vector(w, s_f)
+        kcl_con, port_A, _pv = self._split_kcl_ports(basis.kcl_A)
+        gap, _gv = self._node_gap_columns()
+        return np.hstack([B, port_A.T.astype(np.complex128), gap.astype(np.complex128)]), kcl_con
+
+    def _port_count(self):
+        return len(self.feeds) + len(self.junction_ports) + len(self.node_gaps)
+
+    # ----------------------------------------------------------- device
+    def _ground_struct(self):
+        if self.ground_z is None:
+            return None
+        g = _lib.Ground()
+        g.ground_z = float(self.ground_z)
+        if self.ground_eps is None:
+            g.model = _lib.MW_GROUND_PEC
+            return g
+        et = T.eps_tilde(self.ground_eps, self.omega, self.eps)
+        g.eps_re, g.eps_im = et.real, et.imag
+        if self.ground_model == "sommerfeld":
+            raise NotImplementedError("ground_model='sommerfeld' is not served yet")
+        g.model = _lib.MW_GROUND_REFL
+        g.phi_mode = _lib.PHI_MODES[self.ground_phi_mode]
+        return g
+
+    def _alloc(self):
+        """Device buffers of one solve at this geometry (reused across calls
+        by the benchmark): Z, the same-edge table, the port right-hand sides
+        [B | kcl_con^T], LU workspace, pivots, status and Y."""
+        torch = _torch()
+        dev = self._torch_device()
+        dt = self._dev_tables()
+        n = self._basis().n
+        nm = self.degree + 1
+        B, kcl_con = self._port_columns()
+        n_p, n_c = B.shape[1], kcl_con.shape[0]
+        rhs_host = np.hstack([B, kcl_con.T.astype(np.complex128)]) if n_c else B
+        lib = _lib.load()
+        buf = {
+            "n": n,
+            "n_p": n_p,
+            "n_c": n_c,
+            "Z": torch.empty((n, n), dtype=torch.complex128, device=dev),
+            "table": torch.empty((max(dt.table_rows, 1), nm, nm), dtype=torch.complex128, device=dev),
+            # column-major (n x m) right-hand sides live in an (m, n) tensor
+            "RHS0": torch.from_numpy(np.ascontiguousarray(rhs_host.T)).to(dev),
+            "B": torch.from_numpy(np.ascontiguousarray(B.T)).to(dev),
+            "ws": torch.empty(lib.mw_getrf_workspace_size(n), dtype=torch.uint8, device=dev),
+            "ipiv": torch.empty(max(n, 1), dtype=torch.int32, device=dev),
+            "info": torch.zeros(2, dtype=torch.int32, device=dev),
+            "Y": torch.empty((max(n_p, 1), max(n_p, 1)), dtype=torch.complex128, device=dev),
+            "kcl": kcl_con,
+        }
+        buf["RHS"] = torch.empty_like(buf["RHS0"])
+        if n_c:
+            buf["A"] = torch.from_numpy(np.ascontiguousarray(kcl_con.astype(np.complex128).T)).to(dev)
+            buf["S"] = torch.empty((n_c, n_c), dtype=torch.complex128, device=dev)
+            buf["AW"] = torch.empty((max(n_p, 1), n_c), dtype=torch.complex128, device=dev)
+            buf["ws_c"] = torch.empty(lib.mw_getrf_workspace_size(n_c), dtype=torch.uint8, device=dev)
+            buf["ipiv_c"] = torch.empty(n_c, dtype=torch.int32, device=dev)
+            buf["info_c"] = torch.zeros(2, dtype=torch.int32, device=dev)
+            buf["W"] = torch.empty((max(n_p, 1), n), dtype=torch.complex128, device=dev)
+        buf["h2d_bytes"] = int(buf["RHS0"].numel() * 16 + buf["B"].numel() * 16 + dt.h2d_bytes +
+                               (buf["A"].numel() * 16 if n_c else 0))
+        return buf
+
+    def _fill_device(self, buf, stream):
+        """Fill buf["Z"] (complex128, column-major) at the current k."""
+        dt = self._dev_tables()
+        d = self.degree
+        n = buf["n"]
+        table = buf["table"]
+        _lib.call("mw_same_edge_table", C.byref(dt.edges), d, self.n_qp_pair, int(self.extended_kernel),
+                  float(self.k), table.data_ptr(), stream)
+        fr = _lib.Freq(float(self.k), float(self.omega), float(self.eps), float(self.mu))
+        Z = buf["Z"]
+        _lib.call("mw_fill_z", C.byref(dt.seg), C.byref(dt.basis), table.data_ptr(), C.byref(dt.edges),
+                  C.byref(fr), self.n_qp_pair, Z.data_ptr(), n, None, n, stream)
+        g = self._ground_struct()
+        if g is not None:
+            _lib.call("mw_fill_z_image", C.byref(dt.seg), C.byref(dt.basis), C.byref(g), C.byref(fr),
+                      self.n_qp_pair, Z.data_ptr(), n, None, n, stream)
+
+    def _lu_solve(self, A, n, ws, ipiv, info, rhs, nrhs, stream):
+        """zgetrf(A) in place then zgetrs on rhs (both column-major, ld n)."""
+        cancel = C.c_void_p(self._cancel.ptr) if self._cancel is not None else None
+        try:
+            _lib.call("mw_zgetrf", n, A.data_ptr(), n, ipiv.data_ptr(), info.data_ptr(), ws.data_ptr(),
+                      ws.numel(), cancel, stream)
+        except _lib.NativeError as e:
+            if e.status == _lib.MW_ERR_CANCELLED:
+                raise SolveAborted() from e
+            raise
+        if nrhs:
+            _lib.call("mw_zgetrs", n, nrhs, A.data_ptr(), n, ipiv.data_ptr(), rhs.data_ptr(), n, stream)
+
+    def _device_solve(self, buf, stream):
+        """The whole device pipeline of compute_port_solution: fill, LU,
+        solve all port columns, KCL Schur step, Y = B^T X.  Returns the
+        device tensor holding X (column-major, n x n_p)."""
+        n, n_p, n_c = buf["n"], buf["n_p"], buf["n_c"]
+        self._fill_device(buf, stream)
+        buf["RHS"].copy_(buf["RHS0"], non_blocking=True)
+        self._lu_solve(buf["Z"], n, buf["ws"], buf["ipiv"], buf["info"], buf["RHS"], n_p + n_c, stream)
+        X = buf["RHS"]
+        if n_c:
+            # Lam = (A Xc)^-1 (A W); X <- W - Xc Lam   (bspline.py:2980-2989)
+            A, S, AW = buf["A"], buf["S"], buf["AW"]
+            Wd, Xc = X[:n_p], X[n_p:]
+            _lib.call("mw_zgemm", 0, 0, n_c, n_c, n, 1.0, 0.0, A.data_ptr(), n_c, Xc.data_ptr(), n, 0.0, 0.0,
+                      S.data_ptr(), n_c, stream)
+            if n_p:
+                _lib.call("mw_zgemm", 0, 0, n_c, n_p, n, 1.0, 0.0, A.data_ptr(), n_c, Wd.data_ptr(), n, 0.0, 0.0,
+                          AW.data_ptr(), n_c, stream)
+            self._lu_solve(S, n_c, buf["ws_c"], buf["ipiv_c"], buf["info_c"], AW, n_p, stream)
+            W = buf["W"][:n_p]
+            W.copy_(Wd, non_blocking=True)
+            if n_p:
+                _lib.call("mw_zgemm", 0, 0, n, n_p, n_c, -1.0, 0.0, Xc.data_ptr(), n, AW.data_ptr(), n_c, 1.0,
+                          0.0, W.data_ptr(), n, stream)
+            X = W
+        if n_p:
+            _lib.call("mw_zgemm", 1, 0, n_p, n_p, n, 1.0, 0.0, buf["B"].data_ptr(), n, X.data_ptr(), n, 0.0, 0.0,
+                      buf["Y"].data_ptr(), n_p, stream)
+        return X
+
+    def _check_info(self, buf):
+        infos = [buf["info"]] + ([buf["info_c"]] if buf["n_c"] else [])
+        for inf in infos:
+            v = inf.cpu().numpy()
+            if v[1] != 0:
+                raise RuntimeError(f"LU panel barrier timed out (device status {int(v[1])})")
+            if v[0] > 0:
+                raise np.linalg.LinAlgError("Matrix is singular.")
+
+    def _compute_Z_operator(self, *_unused):
+        """Host copy of Z (numpy complex128) -- for tests and for callers of
+        the reference's private helper of the same name."""
+        torch = _torch()
+        buf = self._alloc()
+        st = torch.cuda.current_stream(buf["Z"].device).cuda_stream
+        self._fill_device(buf, st)
+        return buf["Z"].cpu().numpy().T.copy()
+
+    def compute_port_solution(self) -> PortSolution:
+        """Solve every port from ONE fill and ONE factorisation
+        (``bspline.py:4053-4179``)."""
+        torch = _torch()
+        self._checkpoint()
+        geom, basis = self._geometry(), self._basis()
+        buf = self._alloc()
+        st = torch.cuda.current_stream(buf["Z"].device).cuda_stream
+        X = self._device_solve(buf, st)
+        n_p = buf["n_p"]
+        Xh = X.cpu().numpy().T.copy()
+        Yh = buf["Y"][:n_p, :n_p].cpu().numpy().T.copy() if n_p else np.zeros((0, 0), dtype=np.complex128)
+        self._check_info(buf)
+        self.last_stats = {"h2d_bytes": buf["h2d_bytes"], "d2h_bytes": int(Xh.nbytes + Yh.nbytes + 16)}
+        return PortSolution(
+            y=Yh,
+            coeffs=Xh,
+            port_currents=Yh,
+            basis=_SplineBasis(geom, basis.supp, basis.polys, basis.knots, basis.kept, basis.n),
+        )
+
+    def compute_y_matrix(self) -> np.ndarray:
+        """Short-circuit admittance matrix (``bspline.py:4019``)."""
+        return self.compute_port_solution().y
+
+    def compute_impedance(self):
+        """Drive-point impedance(s) for the configured voltages and the
+        solved coefficients (``bspline.py:3919-4017``)."""
+        sol = self.compute_port_solution()
+        _kcl, _pa, port_V = self._split_kcl_ports(self._basis().kcl_A)
+        _gap, gap_V = self._node_gap_columns()
+        volts = np.concatenate([np.array([v for _w, _a, v in self.feeds], dtype=np.complex128), port_V, gap_V])
+        coeffs = sol.coeffs @ volts
+        B, _ = self._port_columns()
+        currents = B.T @ coeffs
+        z = volts / currents
+        return (z[0] if len(volts) == 1 else z), coeffs
+
+    # --------------------------------------------------------------- sweeps
+    def compute_port_solution_swept(self, k_array):
+        """One ``PortSolution`` per wavenumber (``_port_solution.py:127``)."""
+        out = []
+        with self._k_restored():
+            for kk in np.asarray(k_array, dtype=float):
+                self._checkpoint()
+                self._set_k(kk)
+                out.append(self.compute_port_solution())
+        return out
+
+    def compute_y_matrix_swept(self, k_array) -> np.ndarray:
+        """(n_k, n_ports, n_ports) Y matrices (``_port_solution.py:142``)."""
+        k_array = np.asarray(k_array, dtype=float)
+        n_p = self._port_count()
+        out = np.zeros((k_array.shape[0], n_p, n_p), dtype=np.complex128)
+        for i, sol in enumerate(self.compute_port_solution_swept(k_array)):
+            out[i] = sol.y
+        return out
+
+    def compute_impedance_swept(self, k_array):
+        """Per-k drive-point impedance (``bspline.py:4479``)."""
+        out = []
+        with self._k_restored():
+            for kk in np.asarray(k_array, dtype=float):
+                self._set_k(kk)
+                out.append(self.compute_impedance()[0])
+        return np.asarray(out)
+
+    # -------------------------------------------------------------- readout
+    def currents_at_knots(self, coeffs, s_array=None):
+        """Per-wire complex current at every mesh knot, or at the given arc
+        positions (``bspline.py:4586-4685``)."""
+        coeffs = np.asarray(coeffs)
+        geom, basis = self._geometry(), self._basis()
+        d = self.degree
+        out = []
+        for w in range(len(self.wires_polylines)):
+            knots = basis.knots[w]
+            if s_array is None:
+                s = np.clip(geom.wire_arc[w], knots[0], knots[-1])
+            else:
+                s = np.clip(np.asarray(s_array[w], dtype=np.float64), knots[0], knots[-1])
+            c = np.zeros(len(knots) - d - 1, dtype=np.complex128)
+            for j, _k, _jn, _e, mg in basis.kept[w]:
+                c[j] = coeffs[mg]
+            out.append(T.basis_values(knots, d, s) @ c if s.size else np.zeros(0, dtype=np.complex128))
+        return out
+
+    def element_currents(self, coeffs, subdiv: int = 1):
+        """(mid, moment, nodes, delta) per mesh element
+        (reference ``_element_currents.py:33-120``)."""
+        subdiv = int(subdiv)
+        if subdiv < 1:
+            raise ValueError(f"subdiv must be >= 1, got {subdiv}")
+        coeffs = np.asarray(coeffs)
+        if coeffs.ndim != 1:
+            raise ValueError(
+                "element_currents takes ONE solution vector; got coeffs with "
+                f"shape {coeffs.shape}. For a multi-port solution pass a single "
+                "column, e.g. compute_port_solution().coeffs[:, j]."
+            )
+        fine, arcs = [], []
+        for pl, npe in zip(self.wires_polylines, self.n_per_edge_per_wire):
+            parts = []
+            for i, n_e in enumerate(npe):
+                seg = np.linspace(pl[i], pl[i + 1], n_e * subdiv + 1)
+                parts.append(seg if i == 0 else seg[1:])
+            knots = np.vstack(parts)
+            fine.append(knots)
+            step = np.linalg.norm(knots[1:] - knots[:-1], axis=1)
+            arcs.append(np.concatenate([[0.0], np.cumsum(step)]))
+        currents = self.currents_at_knots(coeffs, None if subdiv == 1 else arcs)
+        mids, moments, nodes, deltas = [], [], [], []
+        for knots, cur in zip(fine, currents):
+            cur = np.asarray(cur)
+            element = 0.5 * (cur[1:] + cur[:-1])
+            mids.append(0.5 * (knots[1:] + knots[:-1]))
+            moments.append(element[:, None] * (knots[1:] - knots[:-1]))
+            nodes.append(knots)
+            zero = np.zeros(1, dtype=np.complex128)
+            deltas.append(np.concatenate([zero, element]) - np.concatenate([element, zero]))
+        return (np.concatenate(mids), np.concatenate(moments), np.concatenate(nodes), np.concatenate(deltas))

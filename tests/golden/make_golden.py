@@ -1,0 +1,103 @@
+"""Generate golden vectors by running the reference momwire itself.
+
+Run in a container that has the reference source tree (default
+/root/reference) and its native kernels built by ``make -C oracle``:
+
+    python tests/golden/make_golden.py [--ref /root/reference] [--big]
+
+The reference package is copied to a temporary directory together with the
+compiled ``_accelerators`` module, imported from there, and every case in
+``tests/golden/cases.py`` is solved with ``BSplineSolver``.  Outputs are
+small ``.npz`` files next to this script.  ``--big`` adds the 16x16 dipole
+array (10,496 unknowns, 256 ports; ~30 s on 8 cores), stored as Y plus a
+seeded sample of Z entries and per-column checksums of the coefficients.
+"""
+
+from __future__ import annotations
+
+import argparse
+import glob
+import os
+import shutil
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REPO = HERE.parent.parent
+sys.path.insert(0, str(HERE))
+
+from cases import BIG_CASES, CASES, SAMPLED  # noqa: E402
+
+
+def import_reference(ref_root: Path):
+    tmp = Path(tempfile.mkdtemp(prefix="momwire_ref_"))
+    shutil.copytree(ref_root / "src" / "momwire", tmp / "momwire")
+    so = glob.glob(str(REPO / "oracle" / "_ref" / "_accelerators*.so"))
+    if not so:
+        raise SystemExit("build the reference kernels first: make -C oracle")
+    shutil.copy(so[0], tmp / "momwire")
+    sys.path.insert(0, str(tmp))
+    import momwire  # noqa: E402
+
+    if not momwire.accelerated:
+        raise SystemExit("reference accelerator failed to load")
+    return momwire
+
+
+def solve_case(momwire, kw, sample_seed=None):
+    s = momwire.BSplineSolver(**kw)
+    geom = s._build_geometry()
+    supp, polys, kcl, wk, wbg = s._build_basis_polynomials(geom)
+    t0 = time.perf_counter()
+    Z = s._compute_Z_operator(geom, supp, polys)
+    t_fill = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    sol = s.compute_port_solution()
+    t_all = time.perf_counter() - t0
+    out = {"y": sol.y, "t_fill": t_fill, "t_solve_total": t_all}
+    n = Z.shape[0]
+    if sample_seed is None:
+        out["Z"] = Z
+        out["coeffs"] = sol.coeffs
+        cur = s.currents_at_knots(sol.coeffs[:, 0])
+        out["currents0"] = np.concatenate(cur)
+    else:
+        rng = np.random.default_rng(sample_seed)
+        ii = rng.integers(0, n, 4096)
+        jj = rng.integers(0, n, 4096)
+        d = np.arange(min(n, 512))
+        ii = np.concatenate([ii, d, d[1:], d[:-1]])
+        jj = np.concatenate([jj, d, d[:-1], d[1:]])
+        out["z_i"] = ii
+        out["z_j"] = jj
+        out["z_v"] = Z[ii, jj]
+        out["coeff_colsum"] = sol.coeffs.sum(axis=0)
+        out["coeff_colnorm"] = np.linalg.norm(sol.coeffs, axis=0)
+        out["coeffs_first_rows"] = sol.coeffs[:64]
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--big", action="store_true")
+    ap.add_argument("--only", default=None)
+    args = ap.parse_args()
+    momwire = import_reference(Path(args.ref))
+    todo = dict(CASES)
+    if args.big:
+        todo.update(BIG_CASES)
+    for name, kw in todo.items():
+        if args.only and name != args.only:
+            continue
+        out = solve_case(momwire, kw(), sample_seed=1234 if name in SAMPLED else None)
+        np.savez_compressed(HERE / f"{name}.npz", **out)
+        print(f"{name}: y[0,0]={out['y'][0, 0]:.12g} fill={out['t_fill']:.3f}s", flush=True)
+
+
+if __name__ == "__main__":
+    main()

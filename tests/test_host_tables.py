@@ -1,0 +1,74 @@
+"""Host-side tables of momwire_b200 against the oracle's restatement:
+geometry, basis support and polynomials, KCL rows, port columns, tiles."""
+
+import numpy as np
+import pytest
+
+from cases import CASES
+from oracle import bspline_oracle as O
+
+import momwire_b200
+from momwire_b200 import _tables as T
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_tables_match_oracle(name):
+    kw = CASES[name]()
+    s = momwire_b200.BSplineSolver(**kw)
+    sp = O.make_spec(**kw)
+    og = O.build_geometry(sp)
+    ob = O.build_basis(sp, og)
+    g, b = s._geometry(), s._basis()
+    assert np.array_equal(g.seg_l, og["seg_l"]) and np.array_equal(g.seg_r, og["seg_r"])
+    np.testing.assert_allclose(g.tangents, og["tangents"], rtol=0, atol=1e-15)
+    assert np.array_equal(np.where(b.supp < 0, 0, b.supp), ob.supp_seg)
+    np.testing.assert_allclose(b.polys, ob.polys, rtol=1e-12, atol=1e-12 * np.abs(ob.polys).max())
+    assert np.array_equal(b.kcl_A, ob.kcl_A)
+    B, kcl = s._port_columns()
+    Bo, kclo = O.port_columns(sp, og, ob)
+    np.testing.assert_allclose(B, Bo, rtol=1e-13, atol=1e-14)
+    assert np.array_equal(kcl, kclo)
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_tiles_cover_every_wing(name):
+    s = momwire_b200.BSplineSolver(**CASES[name]())
+    b = s._basis()
+    t = T.build_tiles(b.supp)
+    assert t.max_basis <= T.MAX_TILE_BASIS and t.max_seg <= T.MAX_TILE_SEG
+    assert int(t.nb.sum()) == b.n
+    for ti in range(len(t.first)):
+        for m in range(t.first[ti], t.first[ti] + t.nb[ti]):
+            for a in range(b.supp.shape[1]):
+                if b.supp[m, a] < 0:
+                    assert t.loc[m, a] == -1
+                else:
+                    assert t.seg[ti, t.loc[m, a]] == b.supp[m, a]
+
+
+def test_ek_labels_match_oracle():
+    kw = CASES["d2_ek_monopole_pec"]()
+    s = momwire_b200.BSplineSolver(**kw)
+    sp = O.make_spec(**kw)
+    og = O.build_geometry(sp)
+    lab, lab_img = s._ek()
+    ol, oli = O.ek_labels(sp, og, True)
+    assert np.array_equal(lab, ol) and np.array_equal(lab_img, oli)
+
+
+def test_constructor_validation_messages():
+    w = [np.array([[0, 0, 0.0], [0, 0, 1.0]])]
+    with pytest.raises(ValueError, match="degree must be >= 1"):
+        momwire_b200.BSplineSolver(wires=w, degree=0)
+    with pytest.raises(NotImplementedError, match="degree > 2"):
+        momwire_b200.BSplineSolver(wires=w, degree=3)
+    with pytest.raises(ValueError, match="ground_eps requires ground_z"):
+        momwire_b200.BSplineSolver(wires=w, ground_eps=(13, 0.005))
+    with pytest.raises(ValueError, match="feeds\\[0\\]: wire_index 3 out of range"):
+        momwire_b200.BSplineSolver(wires=w, feeds=[(3, None, 1.0)])
+    with pytest.raises(ValueError, match="wire_radius entries must be positive"):
+        momwire_b200.BSplineSolver(wires=w, wire_radius=-1.0)
+    with pytest.raises(ValueError, match="junction_ports: junction index 0 out of range"):
+        momwire_b200.BSplineSolver(wires=w, junction_ports=[0])
+    with pytest.raises(NotImplementedError, match="ground plane"):
+        momwire_b200.BSplineSolver(wires=w, ground_z=0.0, ground_eps=(13, 0.005))

@@ -59,10 +59,14 @@ def test_array16x16_matches_reference(cuda_device):
 def test_port_invariants_junction_port(cuda_device):
     """Reference test_port_solution.py: columns satisfy the KCL rows, Y is
     symmetric, superposition equals the configured drive."""
-    s = momwire_b200.BSplineSolver(**CASES["d2_junction_port"]())
+    s = momwire_b200.BSplineSolver(**CASES["d2_junction"]())
     sol = s.compute_port_solution()
     kcl, _pa, _pv = s._split_kcl_ports(s._basis().kcl_A)
+    assert kcl.shape[0] == 1
     assert np.abs(kcl @ sol.coeffs).max() < 1e-10 * np.abs(sol.coeffs).max()
+    s = momwire_b200.BSplineSolver(**CASES["d2_junction_port"]())
+    sol = s.compute_port_solution()
+    assert sol.y.shape == (2, 2)
     assert rel_err(sol.y, sol.y.T) < 1e-9
     z, coeffs = s.compute_impedance()
     assert np.allclose(coeffs, sol.coeffs @ np.array([1.0, 0.0]))

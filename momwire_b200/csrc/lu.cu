@@ -66,6 +66,7 @@ struct PanelArgs {
     int64_t n;
     int64_t j0;
     int jb;
+    int rcap;  // slab leading dimension (rows per CTA)
     int32_t* ipiv;
     int32_t* info;
     PanelWs* ws;
@@ -77,84 +78,129 @@ struct PanelArgs {
     cd* cur_row;
 };
 
-__global__ void __launch_bounds__(kPanelThreads) panel_kernel(PanelArgs P) {
-    const int G = gridDim.x;
-    const int g = blockIdx.x;
-    const int tid = threadIdx.x;
-    const int64_t m = P.n - P.j0;  // rows of the panel
-    const int64_t per = (m + G - 1) / G;
-    const int64_t r0 = P.j0 + g * per;
-    const int64_t r1 = min(P.n, r0 + per);
-    const int jb = P.jb;
-    cd* A = P.A;
-    const int64_t lda = P.lda;
+// Block-wide argmax of (value, row): larger value wins, smaller row on ties.
+__device__ __forceinline__ void argmax_merge(double& v, int64_t& i, double v2, int64_t i2) {
+    if (v2 > v || (v2 == v && i2 < i)) {
+        v = v2;
+        i = i2;
+    }
+}
 
-    __shared__ double s_val[kPanelThreads];
-    __shared__ int64_t s_idx[kPanelThreads];
+__device__ void block_argmax(double& v, int64_t& i, double* s_v, int64_t* s_i) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        double v2 = __shfl_xor_sync(0xffffffffu, v, off);
+        int64_t i2 = __shfl_xor_sync(0xffffffffu, i, off);
+        argmax_merge(v, i, v2, i2);
+    }
+    if (lane == 0) {
+        s_v[warp] = v;
+        s_i[warp] = i;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        const int nw = blockDim.x >> 5;
+        v = lane < nw ? s_v[lane] : -1.0;
+        i = lane < nw ? s_i[lane] : INT64_MAX;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            double v2 = __shfl_xor_sync(0xffffffffu, v, off);
+            int64_t i2 = __shfl_xor_sync(0xffffffffu, i, off);
+            argmax_merge(v, i, v2, i2);
+        }
+        if (lane == 0) {
+            s_v[0] = v;
+            s_i[0] = i;
+        }
+    }
+    __syncthreads();
+    v = s_v[0];
+    i = s_i[0];
+    __syncthreads();
+}
+
+// Panel factorisation of rows [j0, n) x columns [j0, j0+jb).  Each CTA keeps
+// its contiguous row slab of the panel in shared memory for the whole panel
+// (column-major, leading dimension rcap) and writes it back at the end.
+__global__ void __launch_bounds__(kPanelThreads) panel_kernel(PanelArgs P) {
+    extern __shared__ cd slab[];
+    __shared__ double s_v[kPanelThreads / 32];
+    __shared__ int64_t s_i[kPanelThreads / 32];
     __shared__ cd s_piv[kNB];
     __shared__ cd s_cur[kNB];
     __shared__ int64_t s_p;
     __shared__ double s_pv;
+    __shared__ int s_bg;
+
+    const int G = gridDim.x;
+    const int g = blockIdx.x;
+    const int tid = threadIdx.x;
+    const int64_t m = P.n - P.j0;
+    const int64_t per = (m + G - 1) / G;
+    const int64_t r0 = P.j0 + g * per;
+    const int64_t r1 = min(P.n, r0 + per);
+    const int R = (int)max((int64_t)0, r1 - r0);
+    const int rcap = P.rcap;
+    const int jb = P.jb;
+    cd* A = P.A;
+    const int64_t lda = P.lda;
+
+    for (int idx = tid; idx < R * jb; idx += blockDim.x) {
+        int i = idx % R, x = idx / R;
+        slab[x * rcap + i] = A[(r0 + i) + (P.j0 + x) * lda];
+    }
+    __syncthreads();
 
     for (int jj = 0; jj < jb; ++jj) {
         const int64_t c = P.j0 + jj;
         const int buf = jj & 1;
-        // 1. local argmax of |re|+|im| in column c over rows >= c
+        const int i0 = (int)max((int64_t)0, c - r0);  // first local row >= c
+        // 1. local argmax of |re| + |im| in column c
         double best = -1.0;
         int64_t bidx = INT64_MAX;
-        for (int64_t r = max(r0, c) + tid; r < r1; r += blockDim.x) {
-            double v = cabs1(A[r + c * lda]);
-            if (v > best || (v == best && r < bidx)) { best = v; bidx = r; }
-        }
-        s_val[tid] = best;
-        s_idx[tid] = bidx;
-        __syncthreads();
-        for (int off = blockDim.x / 2; off > 0; off >>= 1) {
-            if (tid < off) {
-                double v2 = s_val[tid + off];
-                int64_t i2 = s_idx[tid + off];
-                if (v2 > s_val[tid] || (v2 == s_val[tid] && i2 < s_idx[tid])) {
-                    s_val[tid] = v2;
-                    s_idx[tid] = i2;
-                }
-            }
-            __syncthreads();
-        }
-        // 2. publish candidate (value, index, row) and, for the owner of
-        //    row c, the current row c
+        for (int i = i0 + tid; i < R; i += blockDim.x) argmax_merge(best, bidx, cabs1(slab[jj * rcap + i]), r0 + i);
+        block_argmax(best, bidx, s_v, s_i);
+        // 2. publish the candidate and (owner of row c) the current row c
         if (tid == 0) {
-            P.slot_val[buf * G + g] = s_val[0];
-            P.slot_idx[buf * G + g] = s_idx[0];
+            P.slot_val[buf * G + g] = best;
+            P.slot_idx[buf * G + g] = bidx;
         }
-        int64_t cand = s_idx[0];
-        if (cand != INT64_MAX) {
+        if (bidx != INT64_MAX)
             for (int x = tid; x < jb; x += blockDim.x)
-                P.slot_row[((size_t)buf * G + g) * kNB + x] = A[cand + (P.j0 + x) * lda];
-        }
-        if (c >= r0 && c < r1) {
-            for (int x = tid; x < jb; x += blockDim.x) P.cur_row[buf * kNB + x] = A[c + (P.j0 + x) * lda];
-        }
+                P.slot_row[((size_t)buf * G + g) * kNB + x] = slab[x * rcap + (int)(bidx - r0)];
+        if (c >= r0 && c < r1)
+            for (int x = tid; x < jb; x += blockDim.x) P.cur_row[buf * kNB + x] = slab[x * rcap + (int)(c - r0)];
         // 3. one barrier per column
         if (!grid_sync_bounded(P.ws, (unsigned)(jj + 1) * G)) return;
-        // 4. global pivot (largest value, smallest index on ties)
-        if (tid == 0) {
+        // 4. global pivot from the G candidates (warp 0)
+        if (tid < 32) {
             double bv = -1.0;
             int64_t bi = INT64_MAX;
             int bg = 0;
-            for (int x = 0; x < G; ++x) {
+            for (int x = tid; x < G; x += 32) {
                 double v = __ldcg(&P.slot_val[buf * G + x]);
                 int64_t i = (int64_t)__ldcg(reinterpret_cast<const long long*>(&P.slot_idx[buf * G + x]));
                 if (i == INT64_MAX) continue;
                 if (v > bv || (v == bv && i < bi)) { bv = v; bi = i; bg = x; }
             }
-            s_p = bi;
-            s_pv = bv;
-            if (g == 0) P.ipiv[c] = (int32_t)(bi + 1);
-            s_val[0] = (double)bg;
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                double v2 = __shfl_xor_sync(0xffffffffu, bv, off);
+                int64_t i2 = __shfl_xor_sync(0xffffffffu, bi, off);
+                int g2 = __shfl_xor_sync(0xffffffffu, bg, off);
+                if (v2 > bv || (v2 == bv && i2 < bi)) { bv = v2; bi = i2; bg = g2; }
+            }
+            if (tid == 0) {
+                s_p = bi;
+                s_pv = bv;
+                s_bg = bg;
+                if (g == 0) P.ipiv[c] = (int32_t)(bi + 1);
+            }
         }
         __syncthreads();
         const int64_t p = s_p;
-        const int bg = (int)s_val[0];
+        const int bg = s_bg;
         for (int x = tid; x < jb; x += blockDim.x) {
             // L2-coherent loads: these slots were written by other CTAs
             double2 a = __ldcg(reinterpret_cast<const double2*>(P.slot_row) + ((size_t)buf * G + bg) * kNB + x);
@@ -163,38 +209,36 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel(PanelArgs P) {
             s_cur[x] = cd{b.x, b.y};
         }
         __syncthreads();
-        // 5. swap rows c <-> p inside the panel columns
+        // 5. swap rows c <-> p inside the slab
         if (p != c) {
             if (c >= r0 && c < r1)
-                for (int x = tid; x < jb; x += blockDim.x) A[c + (P.j0 + x) * lda] = s_piv[x];
+                for (int x = tid; x < jb; x += blockDim.x) slab[x * rcap + (int)(c - r0)] = s_piv[x];
             if (p >= r0 && p < r1)
-                for (int x = tid; x < jb; x += blockDim.x) A[p + (P.j0 + x) * lda] = s_cur[x];
+                for (int x = tid; x < jb; x += blockDim.x) slab[x * rcap + (int)(p - r0)] = s_cur[x];
         }
         __syncthreads();
-        // 6. scale the column below the pivot and rank-1 update the panel
-        const cd piv = s_piv[jj];
-        const bool zero = (s_pv == 0.0);
-        if (zero) {
+        // 6. scale below the pivot, then rank-1 update of the panel
+        if (s_pv == 0.0) {
             if (g == 0 && tid == 0 && P.info[0] == 0) P.info[0] = (int32_t)(c + 1);
             continue;  // LAPACK: no scaling, no update for an exact zero pivot
         }
-        const cd inv = cdiv(cd{1.0, 0.0}, piv);
-        const int ncol = jb - jj - 1;
-        const int64_t rs = max(r0, c + 1);
-        const int64_t nr = r1 - rs;
+        const int is = (int)max((int64_t)0, c + 1 - r0);
+        const int nr = R - is;
         if (nr > 0) {
-            for (int64_t r = rs + tid; r < r1; r += blockDim.x) {
-                cd l = A[r + c * lda] * inv;
-                A[r + c * lda] = l;
-                for (int x = 0; x < ncol; ++x) {
-                    int64_t col = c + 1 + x;
-                    cd u = s_piv[jj + 1 + x];
-                    cd a = A[r + col * lda];
-                    A[r + col * lda] = a - l * u;
-                }
+            const cd inv = cdiv(cd{1.0, 0.0}, s_piv[jj]);
+            for (int i = is + tid; i < R; i += blockDim.x) slab[jj * rcap + i] = slab[jj * rcap + i] * inv;
+            __syncthreads();
+            const int ncol = jb - jj - 1;
+            for (int idx = tid; idx < nr * ncol; idx += blockDim.x) {
+                int i = is + idx % nr, x = jj + 1 + idx / nr;
+                slab[x * rcap + i] = slab[x * rcap + i] - slab[jj * rcap + i] * s_piv[x];
             }
         }
         __syncthreads();
+    }
+    for (int idx = tid; idx < R * jb; idx += blockDim.x) {
+        int i = idx % R, x = idx / R;
+        A[(r0 + i) + (P.j0 + x) * lda] = slab[x * rcap + i];
     }
 }
 
@@ -359,18 +403,80 @@ mw_status zgemm_launch(bool ta, bool tb, int64_t m, int64_t n, int64_t k, cd alp
     return MW_OK;
 }
 
-static int panel_grid(int64_t m) {
-    static int sms = 0, per_sm = 0;
+constexpr size_t kPanelSmemMax = 200 * 1024;  // slab bytes per CTA
+
+static int panel_sms() {
+    static int sms = 0;
     if (sms == 0) {
         int dev = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, panel_kernel, kPanelThreads, 0);
-        if (per_sm < 1) per_sm = 1;
+        cudaFuncSetAttribute(panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPanelSmemMax);
+        if (sms < 1) sms = 1;
     }
+    return sms;
+}
+
+static size_t ws_layout(int G, size_t* off_val, size_t* off_idx, size_t* off_row, size_t* off_cur);
+
+// Factor the panel rows [j0, n) x columns [j0, j0+jb) with partial pivoting.
+// One cooperative launch when every CTA's row slab fits in shared memory;
+// otherwise split the columns in two and recurse (left half, then update and
+// factor the right half, then apply the right half's swaps to the left).
+static mw_status panel_factor(cd* A, int64_t lda, int64_t n, int64_t j0, int jb, int32_t* ipiv, int32_t* info,
+                              char* ws, cudaStream_t st) {
+    const int sms = panel_sms();
+    const int64_t m = n - j0;
     int64_t want = (m + 31) / 32;  // at least 32 rows per CTA
-    int64_t g = want < (int64_t)sms ? want : (int64_t)sms;
-    return (int)(g < 1 ? 1 : g);
+    int G = (int)(want < sms ? want : sms);
+    if (G < 1) G = 1;
+    const int64_t per = (m + G - 1) / G;
+    const size_t smem = (size_t)per * jb * sizeof(cd);
+    if (smem > kPanelSmemMax) {
+        MW_REQUIRE(jb > 1, "matrix too large for the panel kernel (%lld rows per CTA)", (long long)per);
+        const int h = jb / 2;
+        mw_status s = panel_factor(A, lda, n, j0, h, ipiv, info, ws, st);
+        if (s != MW_OK) return s;
+        laswp_kernel<<<(unsigned)((jb - h + 127) / 128), 128, 0, st>>>(A, lda, j0 + h, jb - h, ipiv, j0, j0 + h);
+        trsm_kernel<false><<<(unsigned)((jb - h + 31) / 32), 256, kTrsmSmem, st>>>(
+            A + j0 + j0 * lda, lda, A + j0 + (j0 + h) * lda, lda, h, jb - h);
+        count_launch(2);
+        s = zgemm_launch(false, false, m - h, jb - h, h, cd{-1.0, 0.0}, A + (j0 + h) + j0 * lda, lda,
+                         A + j0 + (j0 + h) * lda, lda, cd{1.0, 0.0}, A + (j0 + h) + (j0 + h) * lda, lda, st);
+        if (s != MW_OK) return s;
+        s = panel_factor(A, lda, n, j0 + h, jb - h, ipiv, info, ws, st);
+        if (s != MW_OK) return s;
+        laswp_kernel<<<(unsigned)((h + 127) / 128), 128, 0, st>>>(A, lda, j0, h, ipiv, j0 + h, j0 + jb);
+        count_launch();
+        MW_CHECK_CUDA(cudaGetLastError());
+        return MW_OK;
+    }
+    size_t ov, oi, orow, ocur;
+    ws_layout(G, &ov, &oi, &orow, &ocur);
+    PanelWs* pws = reinterpret_cast<PanelWs*>(ws);
+    // reset the barrier counter only; the error word stays sticky
+    MW_CHECK_CUDA(cudaMemsetAsync(&pws->counter, 0, sizeof(unsigned int), st));
+    PanelArgs P;
+    P.A = A;
+    P.lda = lda;
+    P.n = n;
+    P.j0 = j0;
+    P.jb = jb;
+    P.rcap = (int)per;
+    P.ipiv = ipiv;
+    P.info = info;
+    P.ws = pws;
+    P.slot_val = reinterpret_cast<double*>(ws + ov);
+    P.slot_idx = reinterpret_cast<int64_t*>(ws + oi);
+    P.slot_row = reinterpret_cast<cd*>(ws + orow);
+    P.cur_row = reinterpret_cast<cd*>(ws + ocur);
+    void* args[] = {&P};
+    {
+        ProfileScope ps(PC_PANEL, st, 4.0 * (double)m * jb * jb, 32.0 * (double)m * jb);
+        MW_CHECK_CUDA(cudaLaunchCooperativeKernel((void*)panel_kernel, dim3(G), dim3(kPanelThreads), args, smem, st));
+    }
+    count_launch();
+    return MW_OK;
 }
 
 static size_t ws_layout(int G, size_t* off_val, size_t* off_idx, size_t* off_row, size_t* off_cur) {
@@ -417,31 +523,10 @@ extern "C" mw_status mw_zgetrf(int64_t n, double* Ad, int64_t lda, int32_t* ipiv
             return MW_ERR_CANCELLED;
         }
         int jb = (int)((n - j0) < kNB ? (n - j0) : kNB);
-        int G = panel_grid(n - j0);
-        size_t ov, oi, orow, ocur;
-        ws_layout(G, &ov, &oi, &orow, &ocur);
-        // reset the barrier counter only; the error word stays sticky
-        MW_CHECK_CUDA(cudaMemsetAsync(&pws->counter, 0, sizeof(unsigned int), st));
-        PanelArgs P;
-        P.A = A;
-        P.lda = lda;
-        P.n = n;
-        P.j0 = j0;
-        P.jb = jb;
-        P.ipiv = ipiv;
-        P.info = info;
-        P.ws = reinterpret_cast<PanelWs*>(ws);
-        P.slot_val = reinterpret_cast<double*>(ws + ov);
-        P.slot_idx = reinterpret_cast<int64_t*>(ws + oi);
-        P.slot_row = reinterpret_cast<cd*>(ws + orow);
-        P.cur_row = reinterpret_cast<cd*>(ws + ocur);
-        void* args[] = {&P};
         {
-            ProfileScope ps(PC_PANEL, st, 4.0 * (double)(n - j0) * jb * jb, 32.0 * (double)(n - j0) * jb);
-            MW_CHECK_CUDA(
-                cudaLaunchCooperativeKernel((void*)panel_kernel, dim3(G), dim3(kPanelThreads), args, 0, st));
+            mw_status s = panel_factor(A, lda, n, j0, jb, ipiv, info, ws, st);
+            if (s != MW_OK) return s;
         }
-        count_launch();
         int64_t left = j0, right = n - j0 - jb;
         if (left > 0) {
             ProfileScope ps(PC_LASWP, st, 0.0, 64.0 * (double)jb * left);

@@ -210,6 +210,30 @@ mw_status mw_fill_z_image(const mw_segments* seg, const mw_basis* basis,
                           float* Z32, int64_t ldz32, void* stream);
 
 /*
+ * mw_fill_z for callers that cannot allocate device memory -- no
+ * counterpart in the reference (its fills run on the host).  Some hosts
+ * own every device allocation (a plugin given only its input and output
+ * buffers by a process with its own memory pool, or a binding with no
+ * route to cudaMalloc); for them the same-edge scratch table that
+ * mw_fill_z takes from the caller lives here in a fixed device array that
+ * the library holds from load until exit.  This call allocates nothing.
+ * Writes the same Z as mw_same_edge_table + mw_fill_z (Z32 not written).
+ * Limits: at most mw_fill_z_noalloc_capacity(degree) table rows (32768 at
+ * degree 2, 81920 at degree 1; a structure needs the sum over its straight
+ * edges of 2*n_segments - 1), otherwise MW_ERR_WORKSPACE.  All calls share
+ * the array, so calls that overlap on the GPU race: serialise them.  The
+ * first call on a device looks up the array's device address; make it
+ * before any stream capture.
+ */
+mw_status mw_fill_z_noalloc(const mw_segments* seg, const mw_basis* basis,
+                            const mw_edges* edges, const mw_freq* freq,
+                            int32_t n_qp, int32_t extended_kernel,
+                            double* Z, int64_t ldz, void* stream);
+
+/* Table rows mw_fill_z_noalloc can hold at this degree (0 if invalid). */
+size_t mw_fill_z_noalloc_capacity(int32_t degree);
+
+/*
  * Workspace (bytes, device) needed by mw_zgetrf / mw_cgetrf for order n.
  */
 size_t mw_getrf_workspace_size(int64_t n);

@@ -100,6 +100,8 @@ _SIGS = {
     "mw_offedge_moments": (i32, [C.POINTER(Segments), C.POINTER(Segments), i32, i32, f64, i32, f64, vp, vp, vp, vp]),
     "mw_fill_z": (i32, [C.POINTER(Segments), C.POINTER(BasisT), vp, C.POINTER(Edges), C.POINTER(Freq), i32, vp, i64, vp, i64, vp]),
     "mw_fill_z_image": (i32, [C.POINTER(Segments), C.POINTER(BasisT), C.POINTER(Ground), C.POINTER(Freq), i32, vp, i64, vp, i64, vp]),
+    "mw_fill_z_noalloc": (i32, [C.POINTER(Segments), C.POINTER(BasisT), C.POINTER(Edges), C.POINTER(Freq), i32, i32, vp, i64, vp]),
+    "mw_fill_z_noalloc_capacity": (sz, [i32]),
     "mw_getrf_workspace_size": (sz, [i64]),
     "mw_zgetrf": (i32, [i64, vp, i64, vp, vp, vp, sz, vp, vp]),
     "mw_zgetrs": (i32, [i64, i64, vp, i64, vp, vp, i64, vp]),

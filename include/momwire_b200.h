@@ -234,6 +234,23 @@ mw_status mw_fill_z_noalloc(const mw_segments* seg, const mw_basis* basis,
 size_t mw_fill_z_noalloc_capacity(int32_t degree);
 
 /*
+ * Tensor-core complex update C -= A B for complex64 column-major matrices
+ * (A m x k, B k x n, C m x n), on tcgen05 (kind::tf32) with the 3xTF32
+ * split (hi*hi + hi*lo + lo*hi) and fp32 accumulation in TMEM: the
+ * trailing update of the mixed-precision factorisation.  The fp64 path of
+ * the reference has no counterpart (its LAPACK zgetrf runs in complex128,
+ * bspline.py:2979).  `workspace` (device) holds the packed operand planes:
+ * mw_cgemm_tc_workspace_size(m, n, k) bytes.  `status` (device int32) is
+ * set to MW_ERR_TIMEOUT if a bounded device wait gave up (left untouched
+ * otherwise; the caller zeroes it).
+ */
+size_t mw_cgemm_tc_workspace_size(int64_t m, int64_t n, int64_t k);
+mw_status mw_cgemm_tc_sub(int64_t m, int64_t n, int64_t k,
+                          const float* A, int64_t lda, const float* B, int64_t ldb,
+                          float* C, int64_t ldc, void* workspace,
+                          size_t workspace_bytes, int32_t* status, void* stream);
+
+/*
  * Workspace (bytes, device) needed by mw_zgetrf / mw_cgetrf for order n.
  */
 size_t mw_getrf_workspace_size(int64_t n);
@@ -257,6 +274,43 @@ mw_status mw_zgetrf(int64_t n, double* A, int64_t lda, int32_t* ipiv,
  */
 mw_status mw_zgetrs(int64_t n, int64_t nrhs, const double* LU, int64_t lda,
                     const int32_t* ipiv, double* B, int64_t ldb, void* stream);
+
+/*
+ * complex64 LU with partial pivoting (same conventions as mw_zgetrf),
+ * trailing updates on the tensor cores (mw_cgemm_tc_sub), and the matching
+ * triangular solve.  The factorisation of the mixed-precision path; its
+ * fp64 counterpart in the reference is LAPACK zgetrf/zgetrs
+ * (bspline.py:2979).  Workspace: mw_cgetrf_workspace_size(n, nrhs_max)
+ * bytes, nrhs_max the widest right-hand side later passed to mw_cgetrs.
+ * info[1] receives MW_ERR_TIMEOUT if a bounded device wait gave up.
+ */
+size_t mw_cgetrf_workspace_size(int64_t n, int64_t nrhs_max);
+mw_status mw_cgetrf(int64_t n, float* A, int64_t lda, int32_t* ipiv,
+                    int32_t* info, void* workspace, size_t workspace_bytes,
+                    int64_t nrhs_max, const volatile int32_t* cancel, void* stream);
+mw_status mw_cgetrs(int64_t n, int64_t nrhs, const float* LU, int64_t lda,
+                    const int32_t* ipiv, float* B, int64_t ldb, void* workspace,
+                    size_t workspace_bytes, void* stream);
+
+/*
+ * Mixed-precision drop-in for the complex128 solve of
+ * _solve_with_kcl_ports (bspline.py:2971-2989): factor Z32 (a complex64
+ * copy of Z, overwritten by its LU) with mw_cgetrf, then refine
+ * X <- X + LU32 \ (B - Z X) with the residual in FP64 against Z until the
+ * largest per-column correction ||dX||_inf / ||X||_inf is <= tol, or
+ * max_iter corrections.  X (n x nrhs, complex128) receives the solution.
+ * *iterations / *last_correction (host pointers, may be NULL) report the
+ * refinement.  Synchronises `stream` once per refinement step.  Returns
+ * MW_ERR_SINGULAR if tol was not reached.
+ */
+size_t mw_zgesv_mixed_workspace_size(int64_t n, int64_t nrhs);
+mw_status mw_zgesv_mixed(int64_t n, int64_t nrhs, const double* Z, int64_t ldz,
+                         float* Z32, int64_t ldz32, int32_t* ipiv,
+                         const double* B, int64_t ldb, double* X, int64_t ldx,
+                         double tol, int32_t max_iter, void* workspace,
+                         size_t workspace_bytes, int32_t* info,
+                         int32_t* iterations, double* last_correction,
+                         const volatile int32_t* cancel, void* stream);
 
 /*
  * C = alpha * op(A) * op(B) + beta * C for complex128 column-major

@@ -102,6 +102,14 @@ _SIGS = {
     "mw_fill_z_image": (i32, [C.POINTER(Segments), C.POINTER(BasisT), C.POINTER(Ground), C.POINTER(Freq), i32, vp, i64, vp, i64, vp]),
     "mw_fill_z_noalloc": (i32, [C.POINTER(Segments), C.POINTER(BasisT), C.POINTER(Edges), C.POINTER(Freq), i32, i32, vp, i64, vp]),
     "mw_fill_z_noalloc_capacity": (sz, [i32]),
+    "mw_cgemm_tc_workspace_size": (sz, [i64, i64, i64]),
+    "mw_cgemm_tc_sub": (i32, [i64, i64, i64, vp, i64, vp, i64, vp, i64, vp, sz, vp, vp]),
+    "mw_cgetrf_workspace_size": (sz, [i64, i64]),
+    "mw_cgetrf": (i32, [i64, vp, i64, vp, vp, vp, sz, i64, vp, vp]),
+    "mw_cgetrs": (i32, [i64, i64, vp, i64, vp, vp, i64, vp, sz, vp]),
+    "mw_zgesv_mixed_workspace_size": (sz, [i64, i64]),
+    "mw_zgesv_mixed": (i32, [i64, i64, vp, i64, vp, i64, vp, vp, i64, vp, i64, f64, i32, vp, sz, vp,
+                             C.POINTER(i32), C.POINTER(f64), vp, vp]),
     "mw_getrf_workspace_size": (sz, [i64]),
     "mw_zgetrf": (i32, [i64, vp, i64, vp, vp, vp, sz, vp, vp]),
     "mw_zgetrs": (i32, [i64, i64, vp, i64, vp, vp, i64, vp]),

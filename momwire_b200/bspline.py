@@ -213,6 +213,12 @@ class BSplineSolver:
         if precision not in ("fp64", "mixed"):
             raise ValueError(f"precision must be 'fp64' or 'mixed', got {precision!r}")
         self.precision = precision
+        # mixed: stop refining once the largest relative correction of any
+        # port column is below this (the remaining error is then ~ kappa *
+        # 6e-8 times smaller still)
+        self.mixed_tol = 1e-7
+        self.mixed_max_iter = 10
+        self.last_refinement = None
         self.degree = int(degree)
         self.wavelength = wavelength
         self.halfdriver_factor = halfdriver_factor
@@ -681,6 +687,10 @@ class BSplineSolver:
             "kcl": kcl_con,
         }
         buf["RHS"] = torch.empty_like(buf["RHS0"])
+        if self.precision == "mixed":
+            m = n_p + n_c
+            buf["Z32"] = torch.empty((n, n), dtype=torch.complex64, device=dev)
+            buf["ws_mix"] = torch.empty(lib.mw_zgesv_mixed_workspace_size(n, m), dtype=torch.uint8, device=dev)
         if n_c:
             buf["A"] = torch.from_numpy(np.ascontiguousarray(kcl_con.astype(np.complex128).T)).to(dev)
             buf["S"] = torch.empty((n_c, n_c), dtype=torch.complex128, device=dev)
@@ -703,12 +713,13 @@ class BSplineSolver:
                   float(self.k), table.data_ptr(), stream)
         fr = _lib.Freq(float(self.k), float(self.omega), float(self.eps), float(self.mu))
         Z = buf["Z"]
+        z32 = buf["Z32"].data_ptr() if "Z32" in buf else None
         _lib.call("mw_fill_z", C.byref(dt.seg), C.byref(dt.basis), table.data_ptr(), C.byref(dt.edges),
-                  C.byref(fr), self.n_qp_pair, Z.data_ptr(), n, None, n, stream)
+                  C.byref(fr), self.n_qp_pair, Z.data_ptr(), n, z32, n, stream)
         g = self._ground_struct()
         if g is not None:
             _lib.call("mw_fill_z_image", C.byref(dt.seg), C.byref(dt.basis), C.byref(g), C.byref(fr),
-                      self.n_qp_pair, Z.data_ptr(), n, None, n, stream)
+                      self.n_qp_pair, Z.data_ptr(), n, z32, n, stream)
 
     def _lu_solve(self, A, n, ws, ipiv, info, rhs, nrhs, stream):
         """zgetrf(A) in place then zgetrs on rhs (both column-major, ld n)."""
@@ -729,8 +740,24 @@ class BSplineSolver:
         device tensor holding X (column-major, n x n_p)."""
         n, n_p, n_c = buf["n"], buf["n_p"], buf["n_c"]
         self._fill_device(buf, stream)
-        buf["RHS"].copy_(buf["RHS0"], non_blocking=True)
-        self._lu_solve(buf["Z"], n, buf["ws"], buf["ipiv"], buf["info"], buf["RHS"], n_p + n_c, stream)
+        if self.precision == "mixed":
+            # complex64 tensor-core LU + FP64 refinement against Z
+            m = n_p + n_c
+            it, corr = C.c_int32(0), C.c_double(0.0)
+            cancel = C.c_void_p(self._cancel.ptr) if self._cancel is not None else None
+            try:
+                _lib.call("mw_zgesv_mixed", n, m, buf["Z"].data_ptr(), n, buf["Z32"].data_ptr(), n,
+                          buf["ipiv"].data_ptr(), buf["RHS0"].data_ptr(), n, buf["RHS"].data_ptr(), n,
+                          float(self.mixed_tol), int(self.mixed_max_iter), buf["ws_mix"].data_ptr(),
+                          buf["ws_mix"].numel(), buf["info"].data_ptr(), C.byref(it), C.byref(corr), cancel, stream)
+            except _lib.NativeError as e:
+                if e.status == _lib.MW_ERR_CANCELLED:
+                    raise SolveAborted() from e
+                raise
+            self.last_refinement = {"iterations": int(it.value), "last_correction": float(corr.value)}
+        else:
+            buf["RHS"].copy_(buf["RHS0"], non_blocking=True)
+            self._lu_solve(buf["Z"], n, buf["ws"], buf["ipiv"], buf["info"], buf["RHS"], n_p + n_c, stream)
         X = buf["RHS"]
         if n_c:
             # Lam = (A Xc)^-1 (A W); X <- W - Xc Lam   (bspline.py:2980-2989)

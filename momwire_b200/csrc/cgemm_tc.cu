@@ -1,0 +1,460 @@
+// Tensor-core complex update C -= A B for the mixed-precision LU (sm_100a).
+//
+// C is complex64, column-major.  The product is carried out as the real GEMM
+//     C_real (2m x n)  -=  Ahat (2m x 2k) * Breal (2k x n)
+// where C_real interleaves re/im down each column (the memory of C itself),
+// Ahat holds each complex a as the 2x2 block [[re, -im], [im, re]] and
+// Breal interleaves re/im of B down each column.  Every fp32 operand is split
+// as x = hi + lo with hi = tf32(x), and the MMA sums hi*hi + hi*lo + lo*hi
+// ("3xTF32"), which keeps fp32-level accuracy at tensor-core rate.
+//
+// Kernel structure (one persistent CTA per SM, 192 threads):
+//   warp 0      producer: cp.async.bulk copies of pre-tiled operand stages
+//               into a 2-deep shared-memory ring (mbarrier complete_tx);
+//   warp 1      allocates 512 TMEM columns; one lane issues tcgen05.mma
+//               (M=128, N=256, K=8, kind::tf32) into one of two TMEM
+//               accumulators and commits to mbarriers;
+//   warps 2..5  epilogue: tcgen05.ld the accumulator, C -= D with coalesced
+//               loads/stores, then hand the accumulator back.
+// Operands are packed by the two pack kernels below into the shared-memory
+// image of a K-major, no-swizzle UMMA tile: [block][stage][chunk][row][4],
+// so each stage block is one contiguous bulk copy.
+// Every wait is bounded; on a timeout the kernel records MW_ERR_TIMEOUT,
+// lets each role finish without further work, and frees its TMEM.
+#include <cstdint>
+
+#include "common.cuh"
+
+namespace mw {
+
+constexpr int TC_M = 128;                           // real rows per tile
+constexpr int TC_N = 256;                           // columns per tile
+constexpr int TC_KS = 32;                           // real K per stage
+constexpr int TC_STAGES = 2;
+constexpr int TC_A_BYTES = TC_M * TC_KS * 4;        // 16 KB per plane
+constexpr int TC_B_BYTES = TC_N * TC_KS * 4;        // 32 KB per plane
+constexpr int TC_STAGE_BYTES = 2 * TC_A_BYTES + 2 * TC_B_BYTES;
+constexpr int TC_THREADS = 192;
+constexpr uint32_t TC_TMEM_COLS = 512;              // two 256-column accumulators
+constexpr long long TC_SPIN_LIMIT = 1ll << 26;
+
+struct TcArgs {
+    const float* a_hi;
+    const float* a_lo;
+    const float* b_hi;
+    const float* b_lo;
+    float* C;          // complex64 column-major, viewed as floats
+    int64_t ldc;       // in complex elements
+    int64_t m_real;    // 2 * complex rows
+    int64_t n;         // columns
+    int n_mb, n_nb, n_ks;
+    int* err;
+};
+
+// ------------------------------------------------------------ PTX helpers
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait; returns false (and raises the error word) on a timeout or
+// when another role has already given up.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
+    for (long long it = 0; it < TC_SPIN_LIMIT; ++it) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if ((it & 1023) == 1023 && *(volatile int*)err) return false;
+    }
+    atomicExch(err, MW_ERR_TIMEOUT);
+    return false;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// K-major, no-swizzle UMMA shared-memory descriptor: 8-row core matrices of
+// 16-byte rows; `lbo` = byte distance between the two 16-byte K halves of
+// one MMA step, `sbo` = byte distance between successive 8-row groups.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+    d |= (uint64_t)1 << 46;  // descriptor version for sm_100
+    // base offset 0, lbo mode 0, layout type 0 (no swizzle)
+    return d;
+}
+
+// Instruction descriptor: D f32, A/B tf32, both K-major, M x N.
+__host__ __device__ constexpr uint32_t idesc_tf32(int M, int N) {
+    return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(da), "l"(db), "r"(idesc), "r"(acc)
+        : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float v[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// ---------------------------------------------------------------- kernel
+__global__ void __launch_bounds__(TC_THREADS, 1) cgemm_tc_kernel(TcArgs P) {
+    extern __shared__ __align__(1024) uint8_t tc_smem[];
+    __shared__ __align__(8) uint64_t bar_full[TC_STAGES], bar_empty[TC_STAGES];
+    __shared__ __align__(8) uint64_t bar_accf[2], bar_acce[2], bar_done;
+    __shared__ uint32_t s_tmem;
+
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const int n_tiles = P.n_mb * P.n_nb;
+    int* err = P.err;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < TC_STAGES; ++s) {
+            mbar_init(&bar_full[s], 1);
+            mbar_init(&bar_empty[s], 1);
+        }
+        for (int a = 0; a < 2; ++a) {
+            mbar_init(&bar_accf[a], 1);
+            mbar_init(&bar_acce[a], 4);
+        }
+        mbar_init(&bar_done, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                     "r"(TC_TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = s_tmem;
+
+    if (warp == 0) {
+        // ------------------------------------------------ producer
+        if (lane == 0) {
+            int slot = 0;
+            uint32_t ph_empty[TC_STAGES];
+            uint32_t issued[TC_STAGES] = {};
+            for (int s = 0; s < TC_STAGES; ++s) ph_empty[s] = 1;
+            bool dead = false;
+            for (int t = blockIdx.x; t < n_tiles && !dead; t += gridDim.x) {
+                const int mb = t % P.n_mb, nb = t / P.n_mb;
+                for (int ks = 0; ks < P.n_ks; ++ks) {
+                    if (!mbar_wait(&bar_empty[slot], ph_empty[slot], err)) { dead = true; break; }
+                    ph_empty[slot] ^= 1;
+                    uint8_t* st = tc_smem + (size_t)slot * TC_STAGE_BYTES;
+                    const size_t ao = ((size_t)mb * P.n_ks + ks) * (TC_A_BYTES / 4);
+                    const size_t bo = ((size_t)nb * P.n_ks + ks) * (TC_B_BYTES / 4);
+                    mbar_expect_tx(&bar_full[slot], TC_STAGE_BYTES);
+                    bulk_g2s(st, P.a_hi + ao, TC_A_BYTES, &bar_full[slot]);
+                    bulk_g2s(st + TC_A_BYTES, P.a_lo + ao, TC_A_BYTES, &bar_full[slot]);
+                    bulk_g2s(st + 2 * TC_A_BYTES, P.b_hi + bo, TC_B_BYTES, &bar_full[slot]);
+                    bulk_g2s(st + 2 * TC_A_BYTES + TC_B_BYTES, P.b_lo + bo, TC_B_BYTES, &bar_full[slot]);
+                    issued[slot] += 1;
+                    slot = (slot + 1) % TC_STAGES;
+                }
+            }
+            // drain: the last copy issued into each slot must have landed
+            // before the CTA exits (the k-th fill of a slot completes phase
+            // k-1 of its full barrier); bounded, and independent of the MMA
+            // side so that it also ends when another role gave up
+            for (int s = 0; s < TC_STAGES; ++s) {
+                if (issued[s] == 0) continue;
+                for (long long it = 0; it < TC_SPIN_LIMIT; ++it)
+                    if (mbar_try_wait(&bar_full[s], (issued[s] - 1) & 1)) break;
+            }
+        }
+        __syncwarp();
+    } else if (warp == 1) {
+        // ------------------------------------------------ MMA issuer
+        if (lane == 0) {
+            const uint32_t idesc = idesc_tf32(TC_M, TC_N);
+            int slot = 0;
+            uint32_t ph_full[TC_STAGES] = {};
+            uint32_t ph_acce[2] = {1, 1};
+            bool dead = false;
+            int lt = 0;
+            for (int t = blockIdx.x; t < n_tiles && !dead; t += gridDim.x, ++lt) {
+                const int acc = lt & 1;
+                if (!mbar_wait(&bar_acce[acc], ph_acce[acc], err)) { dead = true; break; }
+                ph_acce[acc] ^= 1;
+                tc_fence_after();
+                const uint32_t tmem_d = tmem_base + acc * TC_N;
+                for (int ks = 0; ks < P.n_ks; ++ks) {
+                    if (!mbar_wait(&bar_full[slot], ph_full[slot], err)) { dead = true; break; }
+                    ph_full[slot] ^= 1;
+                    tc_fence_after();
+                    const uint32_t st = smem_u32(tc_smem + (size_t)slot * TC_STAGE_BYTES);
+                    const uint32_t a_hi = st, a_lo = st + TC_A_BYTES;
+                    const uint32_t b_hi = st + 2 * TC_A_BYTES, b_lo = b_hi + TC_B_BYTES;
+#pragma unroll
+                    for (int kk = 0; kk < TC_KS / 8; ++kk) {
+                        // one MMA step = two 16-byte K chunks
+                        const uint32_t ao = kk * 2 * (TC_M * 16), bo = kk * 2 * (TC_N * 16);
+                        const uint64_t dah = umma_desc(a_hi + ao, TC_M * 16, 128);
+                        const uint64_t dal = umma_desc(a_lo + ao, TC_M * 16, 128);
+                        const uint64_t dbh = umma_desc(b_hi + bo, TC_N * 16, 128);
+                        const uint64_t dbl = umma_desc(b_lo + bo, TC_N * 16, 128);
+                        const uint32_t first = (ks == 0 && kk == 0) ? 0u : 1u;
+                        mma_tf32(tmem_d, dah, dbh, idesc, first);
+                        mma_tf32(tmem_d, dah, dbl, idesc, 1u);
+                        mma_tf32(tmem_d, dal, dbh, idesc, 1u);
+                    }
+                    mma_commit(&bar_empty[slot]);  // stage reusable once these MMAs finish
+                    slot = (slot + 1) % TC_STAGES;
+                }
+                if (!dead) mma_commit(&bar_accf[acc]);
+            }
+            // teardown: no MMA may still be reading shared memory or writing
+            // TMEM when the CTA frees them (commit tracks all prior MMAs)
+            mma_commit(&bar_done);
+            for (long long it = 0; it < TC_SPIN_LIMIT; ++it)
+                if (mbar_try_wait(&bar_done, 0)) break;
+        }
+        __syncwarp();
+    } else {
+        // ------------------------------------------------ epilogue (warps 2..5)
+        const int quad = warp & 3;  // TMEM lane quadrant this warp may access
+        uint32_t ph_accf[2] = {0, 0};
+        bool dead = false;
+        int lt = 0;
+        for (int t = blockIdx.x; t < n_tiles && !dead; t += gridDim.x, ++lt) {
+            const int acc = lt & 1;
+            const int mb = t % P.n_mb, nb = t / P.n_mb;
+            bool ok = true;
+            if (lane == 0) ok = mbar_wait(&bar_accf[acc], ph_accf[acc], err);
+            ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+            if (!ok) { dead = true; break; }
+            ph_accf[acc] ^= 1;
+            tc_fence_after();
+            const int64_t r = (int64_t)mb * TC_M + quad * 32 + lane;  // real row
+            const uint32_t taddr = tmem_base + ((uint32_t)(quad * 32) << 16) + acc * TC_N;
+            for (int c0 = 0; c0 < TC_N; c0 += 16) {
+                float v[16];
+                tmem_ld16(taddr + c0, v);
+                const int64_t col0 = (int64_t)nb * TC_N + c0;
+                if (r < P.m_real) {
+#pragma unroll
+                    for (int e = 0; e < 16; ++e) {
+                        const int64_t col = col0 + e;
+                        if (col < P.n) {
+                            float* cp = P.C + r + col * 2 * P.ldc;
+                            *cp = *cp - v[e];
+                        }
+                    }
+                }
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&bar_acce[acc]);
+        }
+    }
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(TC_TMEM_COLS)
+                     : "memory");
+    }
+}
+
+// -------------------------------------------------------------- packing
+__device__ __forceinline__ float tf32_hi(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
+}
+
+// Ahat (2m x 2k, from complex A at A + (i + l*lda)) packed as
+// [mb][ks][chunk 8][row 128][4]; zero beyond (2m, 2k).
+__global__ void pack_a_kernel(const cf* __restrict__ A, int64_t lda, int64_t m, int64_t k, int n_mb, int n_ks,
+                              float* __restrict__ hi, float* __restrict__ lo) {
+    const int64_t total = (int64_t)n_mb * n_ks * 8 * TC_M;  // float4 slots
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
+        const int row = (int)(q % TC_M);
+        int64_t rest = q / TC_M;
+        const int ch = (int)(rest % 8);
+        rest /= 8;
+        const int ks = (int)(rest % n_ks);
+        const int mb = (int)(rest / n_ks);
+        const int64_t rho = (int64_t)mb * TC_M + row;  // real row
+        const int64_t kap0 = (int64_t)ks * TC_KS + ch * 4;
+        float4 vh, vl;
+        float* ph = &vh.x;
+        float* pl = &vl.x;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const int64_t kap = kap0 + e;
+            float x = 0.f;
+            if (rho < 2 * m && kap < 2 * k) {
+                const cf a = A[(rho >> 1) + (kap >> 1) * lda];
+                const int t = (int)(rho & 1), s = (int)(kap & 1);
+                x = (t == 0) ? (s == 0 ? a.re : -a.im) : (s == 0 ? a.im : a.re);
+            }
+            const float h = tf32_hi(x);
+            ph[e] = h;
+            pl[e] = x - h;
+        }
+        reinterpret_cast<float4*>(hi)[q] = vh;
+        reinterpret_cast<float4*>(lo)[q] = vl;
+    }
+}
+
+// Breal^T (n x 2k, from complex B at B + (l + j*ldb)) packed as
+// [nb][ks][chunk 8][row 256][4]; zero beyond (n, 2k).
+__global__ void pack_b_kernel(const cf* __restrict__ B, int64_t ldb, int64_t k, int64_t n, int n_nb, int n_ks,
+                              float* __restrict__ hi, float* __restrict__ lo) {
+    const int64_t total = (int64_t)n_nb * n_ks * 8 * TC_N;
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
+        const int row = (int)(q % TC_N);
+        int64_t rest = q / TC_N;
+        const int ch = (int)(rest % 8);
+        rest /= 8;
+        const int ks = (int)(rest % n_ks);
+        const int nb = (int)(rest / n_ks);
+        const int64_t j = (int64_t)nb * TC_N + row;
+        const int64_t kap0 = (int64_t)ks * TC_KS + ch * 4;
+        float4 vh, vl;
+        float* ph = &vh.x;
+        float* pl = &vl.x;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const int64_t kap = kap0 + e;
+            float x = 0.f;
+            if (j < n && kap < 2 * k) {
+                const cf b = B[(kap >> 1) + j * ldb];
+                x = (kap & 1) ? b.im : b.re;
+            }
+            const float h = tf32_hi(x);
+            ph[e] = h;
+            pl[e] = x - h;
+        }
+        reinterpret_cast<float4*>(hi)[q] = vh;
+        reinterpret_cast<float4*>(lo)[q] = vl;
+    }
+}
+
+size_t tc_pack_a_bytes(int64_t m, int64_t k) {
+    int64_t n_mb = (2 * m + TC_M - 1) / TC_M, n_ks = (2 * k + TC_KS - 1) / TC_KS;
+    return (size_t)n_mb * n_ks * TC_A_BYTES;
+}
+size_t tc_pack_b_bytes(int64_t k, int64_t n) {
+    int64_t n_nb = (n + TC_N - 1) / TC_N, n_ks = (2 * k + TC_KS - 1) / TC_KS;
+    return (size_t)n_nb * n_ks * TC_B_BYTES;
+}
+
+// C (m x n, complex64 col-major) -= A (m x k) B (k x n), via packed planes
+// in `ws` (layout: a_hi | a_lo | b_hi | b_lo, each 1 KB aligned).
+mw_status cgemm_tc_update(int64_t m, int64_t n, int64_t k, const cf* A, int64_t lda, const cf* B, int64_t ldb, cf* C,
+                          int64_t ldc, void* ws, size_t ws_bytes, int* err, cudaStream_t st) {
+    if (m <= 0 || n <= 0 || k <= 0) return MW_OK;
+    const int n_mb = (int)((2 * m + TC_M - 1) / TC_M);
+    const int n_nb = (int)((n + TC_N - 1) / TC_N);
+    const int n_ks = (int)((2 * k + TC_KS - 1) / TC_KS);
+    const size_t ab = tc_pack_a_bytes(m, k), bb = tc_pack_b_bytes(k, n);
+    auto al = [](size_t x) { return (x + 1023) & ~size_t(1023); };
+    MW_REQUIRE(2 * al(ab) + 2 * al(bb) <= ws_bytes, "tensor-core GEMM workspace too small");
+    char* w = static_cast<char*>(ws);
+    float* a_hi = reinterpret_cast<float*>(w);
+    float* a_lo = reinterpret_cast<float*>(w + al(ab));
+    float* b_hi = reinterpret_cast<float*>(w + 2 * al(ab));
+    float* b_lo = reinterpret_cast<float*>(w + 2 * al(ab) + al(bb));
+    {
+        ProfileScope ps(PC_MISC, st);
+        int64_t qa = (int64_t)n_mb * n_ks * 8 * TC_M, qb = (int64_t)n_nb * n_ks * 8 * TC_N;
+        pack_a_kernel<<<(unsigned)((qa + 255) / 256), 256, 0, st>>>(A, lda, m, k, n_mb, n_ks, a_hi, a_lo);
+        pack_b_kernel<<<(unsigned)((qb + 255) / 256), 256, 0, st>>>(B, ldb, k, n, n_nb, n_ks, b_hi, b_lo);
+        count_launch(2);
+    }
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        MW_CHECK_CUDA(cudaFuncSetAttribute(cgemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           TC_STAGES * TC_STAGE_BYTES));
+    }
+    TcArgs P{a_hi, a_lo, b_hi, b_lo, reinterpret_cast<float*>(C), ldc, 2 * m, n, n_mb, n_nb, n_ks, err};
+    const int tiles = n_mb * n_nb;
+    const int grid = tiles < sms ? tiles : sms;
+    {
+        ProfileScope ps(PC_CGEMM_TC, st, 8.0 * (double)m * n * k, 8.0 * 2.0 * (double)m * n);
+        cgemm_tc_kernel<<<grid, TC_THREADS, TC_STAGES * TC_STAGE_BYTES, st>>>(P);
+    }
+    MW_CHECK_CUDA(cudaGetLastError());
+    count_launch();
+    return MW_OK;
+}
+
+size_t cgemm_tc_workspace(int64_t m, int64_t n, int64_t k) {
+    auto al = [](size_t x) { return (x + 1023) & ~size_t(1023); };
+    return 2 * al(tc_pack_a_bytes(m, k)) + 2 * al(tc_pack_b_bytes(k, n));
+}
+
+}  // namespace mw
+
+using namespace mw;
+
+extern "C" size_t mw_cgemm_tc_workspace_size(int64_t m, int64_t n, int64_t k) { return cgemm_tc_workspace(m, n, k); }
+
+extern "C" mw_status mw_cgemm_tc_sub(int64_t m, int64_t n, int64_t k, const float* A, int64_t lda, const float* B,
+                                     int64_t ldb, float* C, int64_t ldc, void* workspace, size_t workspace_bytes,
+                                     int32_t* status, void* stream) {
+    MW_REQUIRE(m >= 0 && n >= 0 && k >= 0, "negative size");
+    MW_REQUIRE(A && B && C && workspace && status, "NULL argument");
+    MW_REQUIRE(lda >= m && ldb >= k && ldc >= m, "leading dimension too small");
+    return cgemm_tc_update(m, n, k, reinterpret_cast<const cf*>(A), lda, reinterpret_cast<const cf*>(B), ldb,
+                           reinterpret_cast<cf*>(C), ldc, workspace, workspace_bytes, status, as_stream(stream));
+}

@@ -33,6 +33,26 @@ __host__ __device__ __forceinline__ cd cdiv(cd a, cd b) {
         return cd{(a.re * r + a.im) / den, (a.im * r - a.re) / den};
     }
 }
+__host__ __device__ __forceinline__ cf operator+(cf a, cf b) { return cf{a.re + b.re, a.im + b.im}; }
+__host__ __device__ __forceinline__ cf operator-(cf a, cf b) { return cf{a.re - b.re, a.im - b.im}; }
+__host__ __device__ __forceinline__ cf operator*(cf a, cf b) {
+    return cf{a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+}
+__host__ __device__ __forceinline__ cf cdiv(cf a, cf b) {
+    if (fabsf(b.re) >= fabsf(b.im)) {
+        float r = b.im / b.re, den = b.re + b.im * r;
+        return cf{(a.re + a.im * r) / den, (a.im - a.re * r) / den};
+    } else {
+        float r = b.re / b.im, den = b.re * r + b.im;
+        return cf{(a.re * r + a.im) / den, (a.im * r - a.re) / den};
+    }
+}
+__host__ __device__ __forceinline__ double cabs1(cd z) { return fabs(z.re) + fabs(z.im); }
+__host__ __device__ __forceinline__ double cabs1(cf z) { return (double)fabsf(z.re) + (double)fabsf(z.im); }
+template <class T> __host__ __device__ __forceinline__ T cone();
+template <> __host__ __device__ __forceinline__ cd cone<cd>() { return cd{1.0, 0.0}; }
+template <> __host__ __device__ __forceinline__ cf cone<cf>() { return cf{1.0f, 0.0f}; }
+
 // Principal square root (branch cut on the negative real axis; Im >= 0
 // except that -0 imaginary input maps to the lower half, like numpy).
 __host__ __device__ __forceinline__ cd csqrt_p(cd z) {

@@ -1,15 +1,18 @@
-// Dense complex128 LU with partial pivoting and triangular solves (sm_100a).
+// Dense complex LU with partial pivoting and triangular solves (sm_100a).
 //
 // Replaces LAPACK zgetrf/zgetrs reached through scipy.linalg.solve in
-// momwire (bspline.py:2971-2989).  Right-looking blocked algorithm:
-//   panel   : one cooperative kernel per NB-column panel; the rows are split
-//             over all SMs, one bounded grid barrier per column; pivot
-//             candidates and their rows travel through double-buffered
-//             slots so a column costs exactly one barrier;
+// momwire (bspline.py:2971-2989).  Right-looking blocked algorithm, generic
+// in the element type (complex128 for the plain path, complex64 for the
+// mixed-precision path):
+//   panel   : one cooperative kernel per panel; rows split over all SMs,
+//             each CTA's row slab kept in shared memory for the whole panel,
+//             one bounded grid barrier per column; pivot candidates and their
+//             rows travel through double-buffered slots; panels whose slabs
+//             would not fit are split in two and recursed;
 //   laswp   : row interchanges outside the panel;
 //   trsm    : U12 = L11^-1 A12 with L11 staged in shared memory;
-//   gemm    : A22 -= L21 U12, register-tiled complex FP64 (4 DFMA per
-//             complex multiply-add), the bulk of the (8/3) n^3 flops.
+//   update  : A22 -= L21 U12 -- complex128: register-tiled FP64 GEMM;
+//             complex64: tcgen05 tensor cores, 3xTF32 (cgemm_tc.cu).
 // Pivot choice follows LAPACK's izamax: max |re| + |im|, first index wins.
 #include <cstdio>
 
@@ -17,7 +20,12 @@
 
 namespace mw {
 
-constexpr int kNB = 64;          // panel width
+// tensor-core update (cgemm_tc.cu)
+mw_status cgemm_tc_update(int64_t m, int64_t n, int64_t k, const cf* A, int64_t lda, const cf* B, int64_t ldb, cf* C,
+                          int64_t ldc, void* ws, size_t ws_bytes, int* err, cudaStream_t st);
+size_t cgemm_tc_workspace(int64_t m, int64_t n, int64_t k);
+
+constexpr int kNB = 64;  // panel width
 constexpr int kPanelThreads = 256;
 
 struct PanelWs {
@@ -44,12 +52,12 @@ __device__ bool grid_sync_bounded(PanelWs* ws, unsigned int target) {
         long long spins = 0;
         while (ld_acquire(&ws->counter) < target) {
             if (ws->err) { ok = 0; break; }
-            if (++spins > (1ll << 24)) {
+            if (++spins > (1ll << 25)) {
                 atomicExch(&ws->err, MW_ERR_TIMEOUT);
                 ok = 0;
                 break;
             }
-            __nanosleep(64);
+            __nanosleep(20);
         }
         __threadfence();
         s_ok = ok;
@@ -58,10 +66,17 @@ __device__ bool grid_sync_bounded(PanelWs* ws, unsigned int target) {
     return s_ok != 0;
 }
 
-__device__ __forceinline__ double cabs1(cd z) { return fabs(z.re) + fabs(z.im); }
+__device__ __forceinline__ cd ldcg_c(const cd* p) {
+    double2 v = __ldcg(reinterpret_cast<const double2*>(p));
+    return cd{v.x, v.y};
+}
+__device__ __forceinline__ cf ldcg_c(const cf* p) {
+    float2 v = __ldcg(reinterpret_cast<const float2*>(p));
+    return cf{v.x, v.y};
+}
 
 struct PanelArgs {
-    cd* A;
+    void* A;
     int64_t lda;
     int64_t n;
     int64_t j0;
@@ -70,15 +85,14 @@ struct PanelArgs {
     int32_t* ipiv;
     int32_t* info;
     PanelWs* ws;
-    // slot buffers, double buffered: [2][G] values, [2][G] indices,
-    // [2][G][jb] candidate rows, [2][jb] current row
+    // double-buffered slots: [2][G] values, [2][G] indices, [2][G][kNB]
+    // candidate rows, [2][kNB] current row
     double* slot_val;
     int64_t* slot_idx;
-    cd* slot_row;
-    cd* cur_row;
+    void* slot_row;
+    void* cur_row;
 };
 
-// Block-wide argmax of (value, row): larger value wins, smaller row on ties.
 __device__ __forceinline__ void argmax_merge(double& v, int64_t& i, double v2, int64_t i2) {
     if (v2 > v || (v2 == v && i2 < i)) {
         v = v2;
@@ -86,6 +100,7 @@ __device__ __forceinline__ void argmax_merge(double& v, int64_t& i, double v2, i
     }
 }
 
+// Block-wide argmax of (value, row): larger value wins, smaller row on ties.
 __device__ void block_argmax(double& v, int64_t& i, double* s_v, int64_t* s_i) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -123,12 +138,14 @@ __device__ void block_argmax(double& v, int64_t& i, double* s_v, int64_t* s_i) {
 // Panel factorisation of rows [j0, n) x columns [j0, j0+jb).  Each CTA keeps
 // its contiguous row slab of the panel in shared memory for the whole panel
 // (column-major, leading dimension rcap) and writes it back at the end.
+template <class T>
 __global__ void __launch_bounds__(kPanelThreads) panel_kernel(PanelArgs P) {
-    extern __shared__ cd slab[];
+    extern __shared__ __align__(16) unsigned char panel_smem[];
+    T* slab = reinterpret_cast<T*>(panel_smem);
     __shared__ double s_v[kPanelThreads / 32];
     __shared__ int64_t s_i[kPanelThreads / 32];
-    __shared__ cd s_piv[kNB];
-    __shared__ cd s_cur[kNB];
+    __shared__ T s_piv[kNB];
+    __shared__ T s_cur[kNB];
     __shared__ int64_t s_p;
     __shared__ double s_pv;
     __shared__ int s_bg;
@@ -143,7 +160,9 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel(PanelArgs P) {
     const int R = (int)max((int64_t)0, r1 - r0);
     const int rcap = P.rcap;
     const int jb = P.jb;
-    cd* A = P.A;
+    T* A = static_cast<T*>(P.A);
+    T* slot_row = static_cast<T*>(P.slot_row);
+    T* cur_row = static_cast<T*>(P.cur_row);
     const int64_t lda = P.lda;
 
     for (int idx = tid; idx < R * jb; idx += blockDim.x) {
@@ -168,9 +187,9 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel(PanelArgs P) {
         }
         if (bidx != INT64_MAX)
             for (int x = tid; x < jb; x += blockDim.x)
-                P.slot_row[((size_t)buf * G + g) * kNB + x] = slab[x * rcap + (int)(bidx - r0)];
+                slot_row[((size_t)buf * G + g) * kNB + x] = slab[x * rcap + (int)(bidx - r0)];
         if (c >= r0 && c < r1)
-            for (int x = tid; x < jb; x += blockDim.x) P.cur_row[buf * kNB + x] = slab[x * rcap + (int)(c - r0)];
+            for (int x = tid; x < jb; x += blockDim.x) cur_row[buf * kNB + x] = slab[x * rcap + (int)(c - r0)];
         // 3. one barrier per column
         if (!grid_sync_bounded(P.ws, (unsigned)(jj + 1) * G)) return;
         // 4. global pivot from the G candidates (warp 0)
@@ -203,10 +222,8 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel(PanelArgs P) {
         const int bg = s_bg;
         for (int x = tid; x < jb; x += blockDim.x) {
             // L2-coherent loads: these slots were written by other CTAs
-            double2 a = __ldcg(reinterpret_cast<const double2*>(P.slot_row) + ((size_t)buf * G + bg) * kNB + x);
-            double2 b = __ldcg(reinterpret_cast<const double2*>(P.cur_row) + buf * kNB + x);
-            s_piv[x] = cd{a.x, a.y};
-            s_cur[x] = cd{b.x, b.y};
+            s_piv[x] = ldcg_c(slot_row + ((size_t)buf * G + bg) * kNB + x);
+            s_cur[x] = ldcg_c(cur_row + buf * kNB + x);
         }
         __syncthreads();
         // 5. swap rows c <-> p inside the slab
@@ -225,7 +242,7 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel(PanelArgs P) {
         const int is = (int)max((int64_t)0, c + 1 - r0);
         const int nr = R - is;
         if (nr > 0) {
-            const cd inv = cdiv(cd{1.0, 0.0}, s_piv[jj]);
+            const T inv = cdiv(cone<T>(), s_piv[jj]);
             for (int i = is + tid; i < R; i += blockDim.x) slab[jj * rcap + i] = slab[jj * rcap + i] * inv;
             __syncthreads();
             const int ncol = jb - jj - 1;
@@ -242,15 +259,16 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel(PanelArgs P) {
     }
 }
 
-__global__ void laswp_kernel(cd* A, int64_t lda, int64_t col0, int64_t ncols, const int32_t* ipiv, int64_t k1,
+template <class T>
+__global__ void laswp_kernel(T* A, int64_t lda, int64_t col0, int64_t ncols, const int32_t* ipiv, int64_t k1,
                              int64_t k2) {
     int64_t col = col0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (col >= col0 + ncols) return;
-    cd* a = A + col * lda;
+    T* a = A + col * lda;
     for (int64_t i = k1; i < k2; ++i) {
         int64_t p = ipiv[i] - 1;
         if (p != i) {
-            cd t = a[i];
+            T t = a[i];
             a[i] = a[p];
             a[p] = t;
         }
@@ -259,18 +277,17 @@ __global__ void laswp_kernel(cd* A, int64_t lda, int64_t col0, int64_t ncols, co
 
 // X (jb x ncols, leading dim ldx) <- L^-1 X with L unit lower (jb x jb),
 // or U^-1 X with U upper non-unit.  32 columns per CTA.
-template <bool UPPER>
-__global__ void __launch_bounds__(256) trsm_kernel(const cd* T, int64_t ldt, cd* X, int64_t ldx, int jb,
-                                                   int64_t ncols) {
-    extern __shared__ cd trsm_smem[];
-    cd(*sT)[kNB + 1] = reinterpret_cast<cd(*)[kNB + 1]>(trsm_smem);
-    cd(*sX)[33] = reinterpret_cast<cd(*)[33]>(trsm_smem + kNB * (kNB + 1));
+template <class T, bool UPPER>
+__global__ void __launch_bounds__(256) trsm_kernel(const T* Tm, int64_t ldt, T* X, int64_t ldx, int jb, int64_t ncols) {
+    extern __shared__ __align__(16) unsigned char trsm_smem[];
+    T(*sT)[kNB + 1] = reinterpret_cast<T(*)[kNB + 1]>(trsm_smem);
+    T(*sX)[33] = reinterpret_cast<T(*)[33]>(trsm_smem + sizeof(T) * kNB * (kNB + 1));
     const int tid = threadIdx.x;
     const int64_t c0 = blockIdx.x * 32;
     const int nc = (int)((ncols - c0) < 32 ? (ncols - c0) : 32);
     for (int i = tid; i < jb * jb; i += blockDim.x) {
         int r = i % jb, cc = i / jb;
-        sT[r][cc] = T[r + cc * ldt];
+        sT[r][cc] = Tm[r + cc * ldt];
     }
     for (int i = tid; i < jb * nc; i += blockDim.x) {
         int r = i % jb, cc = i / jb;
@@ -302,52 +319,120 @@ __global__ void __launch_bounds__(256) trsm_kernel(const cd* T, int64_t ldt, cd*
     }
 }
 
-// C = alpha op(A) op(B) + beta C, complex128, column-major.
-// 128 x 64 output tile per CTA, 256 threads, 8 x 4 complex per thread,
-// K staged through shared memory 8 at a time.
+template <class T>
+constexpr size_t trsm_smem_bytes() {
+    return sizeof(T) * (kNB * (kNB + 1) + kNB * 33);
+}
+
+template <class T>
+static mw_status trsm_setup() {
+    static bool done = false;
+    if (!done) {
+        MW_CHECK_CUDA(cudaFuncSetAttribute(trsm_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)trsm_smem_bytes<T>()));
+        MW_CHECK_CUDA(cudaFuncSetAttribute(trsm_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)trsm_smem_bytes<T>()));
+        done = true;
+    }
+    return MW_OK;
+}
+
+template <class T, bool UPPER>
+static void trsm_launch(const T* Tm, int64_t ldt, T* X, int64_t ldx, int jb, int64_t ncols, cudaStream_t st) {
+    ProfileScope ps(PC_TRSM, st, 4.0 * (double)jb * jb * ncols, 2.0 * sizeof(T) * (double)jb * ncols);
+    trsm_kernel<T, UPPER><<<(unsigned)((ncols + 31) / 32), 256, trsm_smem_bytes<T>(), st>>>(Tm, ldt, X, ldx, jb,
+                                                                                            ncols);
+    count_launch();
+}
+
+template <class T>
+static void laswp_launch(T* A, int64_t lda, int64_t col0, int64_t ncols, const int32_t* ipiv, int64_t k1, int64_t k2,
+                         cudaStream_t st) {
+    if (ncols <= 0) return;
+    ProfileScope ps(PC_LASWP, st, 0.0, 4.0 * sizeof(T) * (double)(k2 - k1) * ncols);
+    laswp_kernel<T><<<(unsigned)((ncols + 127) / 128), 128, 0, st>>>(A, lda, col0, ncols, ipiv, k1, k2);
+    count_launch();
+}
+
+// --------------------------------------------------------------- FP64 GEMM
+// C = alpha op(A) op(B) + beta C, complex128, column-major.  128 x 64 tile
+// per CTA, 256 threads, 8 x 4 complex per thread; K staged 8 at a time
+// through a two-slot shared-memory ring with register prefetch of the next
+// slice while the current one is consumed.
 constexpr int GM = 128, GN = 64, GK = 8;
+constexpr size_t kZgemmSmem = sizeof(cd) * 2 * (GK * (GM + 1) + GK * (GN + 1));
 
 template <bool TA, bool TB>
 __global__ void __launch_bounds__(256) zgemm_kernel(int64_t m, int64_t n, int64_t k, cd alpha, const cd* __restrict__ A,
                                                     int64_t lda, const cd* __restrict__ B, int64_t ldb, cd beta,
                                                     cd* __restrict__ C, int64_t ldc) {
-    __shared__ cd sA[GK][GM + 1];
-    __shared__ cd sB[GK][GN + 1];
+    extern __shared__ __align__(16) unsigned char zg_smem[];
+    cd* sA0 = reinterpret_cast<cd*>(zg_smem);             // [2][GK][GM+1]
+    cd* sB0 = sA0 + 2 * GK * (GM + 1);                     // [2][GK][GN+1]
     const int tid = threadIdx.x;
     const int64_t m0 = blockIdx.x * (int64_t)GM, n0 = blockIdx.y * (int64_t)GN;
     const int tx = tid % 16, ty = tid / 16;  // rows tx + 16*i, cols ty + 16*j
+    constexpr int LA = GM * GK / 256, LB = GK * GN / 256;
     cd acc[8][4];
 #pragma unroll
     for (int i = 0; i < 8; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) acc[i][j] = cd{0.0, 0.0};
 
-    for (int64_t k0 = 0; k0 < k; k0 += GK) {
-        // stage A tile (GM x GK) and B tile (GK x GN)
-        for (int i = tid; i < GM * GK; i += 256) {
+    cd ra[LA], rb[LB];
+    auto fetch = [&](int64_t k0) {
+#pragma unroll
+        for (int u = 0; u < LA; ++u) {
+            int i = tid + u * 256;
             int r = TA ? i / GK : i % GM;
             int kk = TA ? i % GK : i / GM;
             int64_t gr = m0 + r, gk = k0 + kk;
-            cd v{0.0, 0.0};
-            if (gr < m && gk < k) v = TA ? A[gk + gr * lda] : A[gr + gk * lda];
-            sA[kk][r] = v;
+            ra[u] = (gr < m && gk < k) ? (TA ? A[gk + gr * lda] : A[gr + gk * lda]) : cd{0.0, 0.0};
         }
-        for (int i = tid; i < GK * GN; i += 256) {
+#pragma unroll
+        for (int u = 0; u < LB; ++u) {
+            int i = tid + u * 256;
             int kk = TB ? i / GN : i % GK;
             int cc = TB ? i % GN : i / GK;
             int64_t gk = k0 + kk, gc = n0 + cc;
-            cd v{0.0, 0.0};
-            if (gk < k && gc < n) v = TB ? B[gc + gk * ldb] : B[gk + gc * ldb];
-            sB[kk][cc] = v;
+            rb[u] = (gk < k && gc < n) ? (TB ? B[gc + gk * ldb] : B[gk + gc * ldb]) : cd{0.0, 0.0};
         }
-        __syncthreads();
+    };
+    auto stash = [&](int slot) {
+        cd* sA = sA0 + slot * GK * (GM + 1);
+        cd* sB = sB0 + slot * GK * (GN + 1);
+#pragma unroll
+        for (int u = 0; u < LA; ++u) {
+            int i = tid + u * 256;
+            int r = TA ? i / GK : i % GM;
+            int kk = TA ? i % GK : i / GM;
+            sA[kk * (GM + 1) + r] = ra[u];
+        }
+#pragma unroll
+        for (int u = 0; u < LB; ++u) {
+            int i = tid + u * 256;
+            int kk = TB ? i / GN : i % GK;
+            int cc = TB ? i % GN : i / GK;
+            sB[kk * (GN + 1) + cc] = rb[u];
+        }
+    };
+
+    fetch(0);
+    stash(0);
+    __syncthreads();
+    int slot = 0;
+    for (int64_t k0 = 0; k0 < k; k0 += GK) {
+        const bool more = k0 + GK < k;
+        if (more) fetch(k0 + GK);
+        const cd* sA = sA0 + slot * GK * (GM + 1);
+        const cd* sB = sB0 + slot * GK * (GN + 1);
 #pragma unroll
         for (int kk = 0; kk < GK; ++kk) {
             cd a[8], b[4];
 #pragma unroll
-            for (int i = 0; i < 8; ++i) a[i] = sA[kk][tx + 16 * i];
+            for (int i = 0; i < 8; ++i) a[i] = sA[kk * (GM + 1) + tx + 16 * i];
 #pragma unroll
-            for (int j = 0; j < 4; ++j) b[j] = sB[kk][ty + 16 * j];
+            for (int j = 0; j < 4; ++j) b[j] = sB[kk * (GN + 1) + ty + 16 * j];
 #pragma unroll
             for (int i = 0; i < 8; ++i)
 #pragma unroll
@@ -358,7 +443,9 @@ __global__ void __launch_bounds__(256) zgemm_kernel(int64_t m, int64_t n, int64_
                     acc[i][j].im = fma(a[i].im, b[j].re, acc[i][j].im);
                 }
         }
+        if (more) stash(slot ^ 1);
         __syncthreads();
+        slot ^= 1;
     }
     const bool beta_zero = (beta.re == 0.0 && beta.im == 0.0);
 #pragma unroll
@@ -377,77 +464,112 @@ __global__ void __launch_bounds__(256) zgemm_kernel(int64_t m, int64_t n, int64_
     }
 }
 
-constexpr size_t kTrsmSmem = sizeof(cd) * (kNB * (kNB + 1) + kNB * 33);
-
-static mw_status trsm_setup() {
-    static bool done = false;
-    if (!done) {
-        MW_CHECK_CUDA(cudaFuncSetAttribute(trsm_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsmSmem));
-        MW_CHECK_CUDA(cudaFuncSetAttribute(trsm_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsmSmem));
-        done = true;
-    }
-    return MW_OK;
-}
-
 mw_status zgemm_launch(bool ta, bool tb, int64_t m, int64_t n, int64_t k, cd alpha, const cd* A, int64_t lda,
                        const cd* B, int64_t ldb, cd beta, cd* C, int64_t ldc, cudaStream_t st) {
     if (m <= 0 || n <= 0) return MW_OK;
+    static bool attr = false;
+    if (!attr) {
+        MW_CHECK_CUDA(cudaFuncSetAttribute(zgemm_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)kZgemmSmem));
+        MW_CHECK_CUDA(cudaFuncSetAttribute(zgemm_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)kZgemmSmem));
+        MW_CHECK_CUDA(cudaFuncSetAttribute(zgemm_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)kZgemmSmem));
+        MW_CHECK_CUDA(cudaFuncSetAttribute(zgemm_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)kZgemmSmem));
+        attr = true;
+    }
     dim3 grid((unsigned)((m + GM - 1) / GM), (unsigned)((n + GN - 1) / GN));
     ProfileScope ps(PC_ZGEMM, st, 8.0 * (double)m * n * k, 16.0 * ((double)m * k + (double)k * n + 2.0 * m * n));
-    if (!ta && !tb) zgemm_kernel<false, false><<<grid, 256, 0, st>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
-    else if (ta && !tb) zgemm_kernel<true, false><<<grid, 256, 0, st>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
-    else if (!ta && tb) zgemm_kernel<false, true><<<grid, 256, 0, st>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
-    else zgemm_kernel<true, true><<<grid, 256, 0, st>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+    if (!ta && !tb) zgemm_kernel<false, false><<<grid, 256, kZgemmSmem, st>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+    else if (ta && !tb) zgemm_kernel<true, false><<<grid, 256, kZgemmSmem, st>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+    else if (!ta && tb) zgemm_kernel<false, true><<<grid, 256, kZgemmSmem, st>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+    else zgemm_kernel<true, true><<<grid, 256, kZgemmSmem, st>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
     MW_CHECK_CUDA(cudaGetLastError());
     count_launch();
     return MW_OK;
 }
 
+// --------------------------------------------------------------- driver
 constexpr size_t kPanelSmemMax = 200 * 1024;  // slab bytes per CTA
 
+template <class T>
 static int panel_sms() {
     static int sms = 0;
     if (sms == 0) {
         int dev = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaFuncSetAttribute(panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPanelSmemMax);
+        cudaFuncSetAttribute(panel_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPanelSmemMax);
         if (sms < 1) sms = 1;
     }
     return sms;
 }
 
-static size_t ws_layout(int G, size_t* off_val, size_t* off_idx, size_t* off_row, size_t* off_cur);
+static size_t ws_layout(int G, size_t* off_val, size_t* off_idx, size_t* off_row, size_t* off_cur) {
+    size_t o = 256;  // PanelWs + padding
+    *off_val = o;
+    o += sizeof(double) * 2 * G;
+    o = (o + 255) & ~size_t(255);
+    *off_idx = o;
+    o += sizeof(int64_t) * 2 * G;
+    o = (o + 255) & ~size_t(255);
+    *off_row = o;
+    o += sizeof(cd) * 2 * (size_t)G * kNB;
+    o = (o + 255) & ~size_t(255);
+    *off_cur = o;
+    o += sizeof(cd) * 2 * kNB;
+    return (o + 255) & ~size_t(255);
+}
+
+constexpr int kMaxPanelGrid = 1024;
+
+// Trailing update C -= A B of a block (type-specific engine).
+struct Updater {
+    // complex64 only: tensor-core workspace
+    void* tc_ws = nullptr;
+    size_t tc_ws_bytes = 0;
+    int* tc_err = nullptr;
+};
+
+static mw_status block_update(const cd* A, int64_t lda, const cd* B, int64_t ldb, cd* C, int64_t ldc, int64_t m,
+                              int64_t n, int64_t k, const Updater&, cudaStream_t st) {
+    return zgemm_launch(false, false, m, n, k, cd{-1.0, 0.0}, A, lda, B, ldb, cd{1.0, 0.0}, C, ldc, st);
+}
+
+static mw_status block_update(const cf* A, int64_t lda, const cf* B, int64_t ldb, cf* C, int64_t ldc, int64_t m,
+                              int64_t n, int64_t k, const Updater& u, cudaStream_t st) {
+    return cgemm_tc_update(m, n, k, A, lda, B, ldb, C, ldc, u.tc_ws, u.tc_ws_bytes, u.tc_err, st);
+}
 
 // Factor the panel rows [j0, n) x columns [j0, j0+jb) with partial pivoting.
 // One cooperative launch when every CTA's row slab fits in shared memory;
 // otherwise split the columns in two and recurse (left half, then update and
 // factor the right half, then apply the right half's swaps to the left).
-static mw_status panel_factor(cd* A, int64_t lda, int64_t n, int64_t j0, int jb, int32_t* ipiv, int32_t* info,
-                              char* ws, cudaStream_t st) {
-    const int sms = panel_sms();
+template <class T>
+static mw_status panel_factor(T* A, int64_t lda, int64_t n, int64_t j0, int jb, int32_t* ipiv, int32_t* info, char* ws,
+                              const Updater& up, cudaStream_t st) {
+    const int sms = panel_sms<T>();
     const int64_t m = n - j0;
     int64_t want = (m + 31) / 32;  // at least 32 rows per CTA
     int G = (int)(want < sms ? want : sms);
+    if (G > kMaxPanelGrid) G = kMaxPanelGrid;
     if (G < 1) G = 1;
     const int64_t per = (m + G - 1) / G;
-    const size_t smem = (size_t)per * jb * sizeof(cd);
+    const size_t smem = (size_t)per * jb * sizeof(T);
     if (smem > kPanelSmemMax) {
         MW_REQUIRE(jb > 1, "matrix too large for the panel kernel (%lld rows per CTA)", (long long)per);
         const int h = jb / 2;
-        mw_status s = panel_factor(A, lda, n, j0, h, ipiv, info, ws, st);
+        mw_status s = panel_factor<T>(A, lda, n, j0, h, ipiv, info, ws, up, st);
         if (s != MW_OK) return s;
-        laswp_kernel<<<(unsigned)((jb - h + 127) / 128), 128, 0, st>>>(A, lda, j0 + h, jb - h, ipiv, j0, j0 + h);
-        trsm_kernel<false><<<(unsigned)((jb - h + 31) / 32), 256, kTrsmSmem, st>>>(
-            A + j0 + j0 * lda, lda, A + j0 + (j0 + h) * lda, lda, h, jb - h);
-        count_launch(2);
-        s = zgemm_launch(false, false, m - h, jb - h, h, cd{-1.0, 0.0}, A + (j0 + h) + j0 * lda, lda,
-                         A + j0 + (j0 + h) * lda, lda, cd{1.0, 0.0}, A + (j0 + h) + (j0 + h) * lda, lda, st);
+        laswp_launch<T>(A, lda, j0 + h, jb - h, ipiv, j0, j0 + h, st);
+        trsm_launch<T, false>(A + j0 + j0 * lda, lda, A + j0 + (j0 + h) * lda, lda, h, jb - h, st);
+        s = block_update(A + (j0 + h) + j0 * lda, lda, A + j0 + (j0 + h) * lda, lda, A + (j0 + h) + (j0 + h) * lda,
+                         lda, m - h, jb - h, h, up, st);
         if (s != MW_OK) return s;
-        s = panel_factor(A, lda, n, j0 + h, jb - h, ipiv, info, ws, st);
+        s = panel_factor<T>(A, lda, n, j0 + h, jb - h, ipiv, info, ws, up, st);
         if (s != MW_OK) return s;
-        laswp_kernel<<<(unsigned)((h + 127) / 128), 128, 0, st>>>(A, lda, j0, h, ipiv, j0 + h, j0 + jb);
-        count_launch();
+        laswp_launch<T>(A, lda, j0, h, ipiv, j0 + h, j0 + jb, st);
         MW_CHECK_CUDA(cudaGetLastError());
         return MW_OK;
     }
@@ -468,89 +590,46 @@ static mw_status panel_factor(cd* A, int64_t lda, int64_t n, int64_t j0, int jb,
     P.ws = pws;
     P.slot_val = reinterpret_cast<double*>(ws + ov);
     P.slot_idx = reinterpret_cast<int64_t*>(ws + oi);
-    P.slot_row = reinterpret_cast<cd*>(ws + orow);
-    P.cur_row = reinterpret_cast<cd*>(ws + ocur);
+    P.slot_row = ws + orow;
+    P.cur_row = ws + ocur;
     void* args[] = {&P};
     {
-        ProfileScope ps(PC_PANEL, st, 4.0 * (double)m * jb * jb, 32.0 * (double)m * jb);
-        MW_CHECK_CUDA(cudaLaunchCooperativeKernel((void*)panel_kernel, dim3(G), dim3(kPanelThreads), args, smem, st));
+        ProfileScope ps(PC_PANEL, st, 4.0 * (double)m * jb * jb, 2.0 * sizeof(T) * (double)m * jb);
+        MW_CHECK_CUDA(
+            cudaLaunchCooperativeKernel((void*)panel_kernel<T>, dim3(G), dim3(kPanelThreads), args, smem, st));
     }
     count_launch();
     return MW_OK;
 }
 
-static size_t ws_layout(int G, size_t* off_val, size_t* off_idx, size_t* off_row, size_t* off_cur) {
-    size_t o = 256;  // PanelWs + padding
-    *off_val = o;
-    o += sizeof(double) * 2 * G;
-    o = (o + 255) & ~size_t(255);
-    *off_idx = o;
-    o += sizeof(int64_t) * 2 * G;
-    o = (o + 255) & ~size_t(255);
-    *off_row = o;
-    o += sizeof(cd) * 2 * (size_t)G * kNB;
-    o = (o + 255) & ~size_t(255);
-    *off_cur = o;
-    o += sizeof(cd) * 2 * kNB;
-    return (o + 255) & ~size_t(255);
-}
-
-}  // namespace mw
-
-using namespace mw;
-
-extern "C" size_t mw_getrf_workspace_size(int64_t n) {
-    size_t a, b, c, d;
-    (void)n;
-    return ws_layout(1024, &a, &b, &c, &d);  // enough for any grid up to 1024 CTAs
-}
-
-extern "C" mw_status mw_zgetrf(int64_t n, double* Ad, int64_t lda, int32_t* ipiv, int32_t* info, void* workspace,
-                               size_t workspace_bytes, const volatile int32_t* cancel, void* stream) {
-    MW_REQUIRE(n >= 0 && lda >= (n > 0 ? n : 1), "bad n/lda");
-    MW_REQUIRE(Ad && ipiv && info && workspace, "NULL argument");
-    MW_REQUIRE(workspace_bytes >= mw_getrf_workspace_size(n), "workspace too small");
-    cudaStream_t st = as_stream(stream);
-    cd* A = reinterpret_cast<cd*>(Ad);
-    char* ws = reinterpret_cast<char*>(workspace);
+// Right-looking blocked LU of an n x n column-major matrix.
+template <class T>
+static mw_status getrf(int64_t n, T* A, int64_t lda, int32_t* ipiv, int32_t* info, char* ws,
+                       const volatile int32_t* cancel, const Updater& up, cudaStream_t st) {
     MW_CHECK_CUDA(cudaMemsetAsync(info, 0, 2 * sizeof(int32_t), st));
     MW_CHECK_CUDA(cudaMemsetAsync(ws, 0, sizeof(PanelWs), st));
-    { mw_status s0 = trsm_setup(); if (s0 != MW_OK) return s0; }
+    {
+        mw_status s0 = trsm_setup<T>();
+        if (s0 != MW_OK) return s0;
+    }
     PanelWs* pws = reinterpret_cast<PanelWs*>(ws);
     for (int64_t j0 = 0; j0 < n; j0 += kNB) {
         if (cancel && *cancel) {
             set_error("factorisation cancelled");
             return MW_ERR_CANCELLED;
         }
-        int jb = (int)((n - j0) < kNB ? (n - j0) : kNB);
-        {
-            mw_status s = panel_factor(A, lda, n, j0, jb, ipiv, info, ws, st);
-            if (s != MW_OK) return s;
-        }
-        int64_t left = j0, right = n - j0 - jb;
-        if (left > 0) {
-            ProfileScope ps(PC_LASWP, st, 0.0, 64.0 * (double)jb * left);
-            laswp_kernel<<<(unsigned)((left + 127) / 128), 128, 0, st>>>(A, lda, 0, left, ipiv, j0, j0 + jb);
-            count_launch();
-        }
+        const int jb = (int)((n - j0) < kNB ? (n - j0) : kNB);
+        mw_status s = panel_factor<T>(A, lda, n, j0, jb, ipiv, info, ws, up, st);
+        if (s != MW_OK) return s;
+        const int64_t left = j0, right = n - j0 - jb;
+        laswp_launch<T>(A, lda, 0, left, ipiv, j0, j0 + jb, st);
         if (right > 0) {
-            {
-                ProfileScope ps(PC_LASWP, st, 0.0, 64.0 * (double)jb * right);
-                laswp_kernel<<<(unsigned)((right + 127) / 128), 128, 0, st>>>(A, lda, j0 + jb, right, ipiv, j0,
-                                                                             j0 + jb);
-            }
-            cd* A11 = A + j0 + j0 * lda;
-            cd* A12 = A + j0 + (j0 + jb) * lda;
-            {
-                ProfileScope ps(PC_TRSM, st, 4.0 * (double)jb * jb * right, 32.0 * (double)jb * right);
-                trsm_kernel<false><<<(unsigned)((right + 31) / 32), 256, kTrsmSmem, st>>>(A11, lda, A12, lda, jb,
-                                                                                         right);
-            }
-            count_launch(2);  // laswp + trsm
-            cd* A21 = A + (j0 + jb) + j0 * lda;
-            cd* A22 = A + (j0 + jb) + (j0 + jb) * lda;
-            mw_status s = zgemm_launch(false, false, right, right, jb, cd{-1.0, 0.0}, A21, lda, A12, lda,
-                                       cd{1.0, 0.0}, A22, lda, st);
+            laswp_launch<T>(A, lda, j0 + jb, right, ipiv, j0, j0 + jb, st);
+            T* A11 = A + j0 + j0 * lda;
+            T* A12 = A + j0 + (j0 + jb) * lda;
+            trsm_launch<T, false>(A11, lda, A12, lda, jb, right, st);
+            s = block_update(A + (j0 + jb) + j0 * lda, lda, A12, lda, A + (j0 + jb) + (j0 + jb) * lda, lda, right, right,
+                             jb, up, st);
             if (s != MW_OK) return s;
         }
         MW_CHECK_CUDA(cudaGetLastError());
@@ -560,45 +639,117 @@ extern "C" mw_status mw_zgetrf(int64_t n, double* Ad, int64_t lda, int32_t* ipiv
     return MW_OK;
 }
 
-extern "C" mw_status mw_zgetrs(int64_t n, int64_t nrhs, const double* LUd, int64_t lda, const int32_t* ipiv,
-                               double* Bd, int64_t ldb, void* stream) {
-    MW_REQUIRE(n >= 0 && nrhs >= 0 && lda >= (n > 0 ? n : 1) && ldb >= (n > 0 ? n : 1), "bad sizes");
-    MW_REQUIRE(LUd && ipiv && Bd, "NULL argument");
-    if (n == 0 || nrhs == 0) return MW_OK;
-    cudaStream_t st = as_stream(stream);
-    const cd* LU = reinterpret_cast<const cd*>(LUd);
-    cd* B = reinterpret_cast<cd*>(Bd);
+// Solve A X = B from the factors (forward with unit L, back with U).
+template <class T>
+static mw_status getrs(int64_t n, int64_t nrhs, const T* LU, int64_t lda, const int32_t* ipiv, T* B, int64_t ldb,
+                       const Updater& up, cudaStream_t st) {
     {
-        mw_status s0 = trsm_setup();
+        mw_status s0 = trsm_setup<T>();
         if (s0 != MW_OK) return s0;
     }
-    laswp_kernel<<<(unsigned)((nrhs + 127) / 128), 128, 0, st>>>(B, ldb, 0, nrhs, ipiv, 0, n);
-    count_launch();
-    unsigned cb = (unsigned)((nrhs + 31) / 32);
+    laswp_launch<T>(B, ldb, 0, nrhs, ipiv, 0, n, st);
     for (int64_t j0 = 0; j0 < n; j0 += kNB) {
-        int jb = (int)((n - j0) < kNB ? (n - j0) : kNB);
-        trsm_kernel<false><<<cb, 256, kTrsmSmem, st>>>(LU + j0 + j0 * lda, lda, B + j0, ldb, jb, nrhs);
-        count_launch();
-        int64_t rest = n - j0 - jb;
+        const int jb = (int)((n - j0) < kNB ? (n - j0) : kNB);
+        trsm_launch<T, false>(LU + j0 + j0 * lda, lda, B + j0, ldb, jb, nrhs, st);
+        const int64_t rest = n - j0 - jb;
         if (rest > 0) {
-            mw_status s = zgemm_launch(false, false, rest, nrhs, jb, cd{-1.0, 0.0}, LU + (j0 + jb) + j0 * lda, lda,
-                                       B + j0, ldb, cd{1.0, 0.0}, B + j0 + jb, ldb, st);
+            mw_status s = block_update(LU + (j0 + jb) + j0 * lda, lda, B + j0, ldb, B + j0 + jb, ldb, rest, nrhs, jb,
+                                       up, st);
             if (s != MW_OK) return s;
         }
     }
-    int64_t last = ((n - 1) / kNB) * kNB;
+    const int64_t last = ((n - 1) / kNB) * kNB;
     for (int64_t j0 = last; j0 >= 0; j0 -= kNB) {
-        int jb = (int)((n - j0) < kNB ? (n - j0) : kNB);
-        trsm_kernel<true><<<cb, 256, kTrsmSmem, st>>>(LU + j0 + j0 * lda, lda, B + j0, ldb, jb, nrhs);
-        count_launch();
+        const int jb = (int)((n - j0) < kNB ? (n - j0) : kNB);
+        trsm_launch<T, true>(LU + j0 + j0 * lda, lda, B + j0, ldb, jb, nrhs, st);
         if (j0 > 0) {
-            mw_status s = zgemm_launch(false, false, j0, nrhs, jb, cd{-1.0, 0.0}, LU + j0 * lda, lda, B + j0, ldb,
-                                       cd{1.0, 0.0}, B, ldb, st);
+            mw_status s = block_update(LU + j0 * lda, lda, B + j0, ldb, B, ldb, j0, nrhs, jb, up, st);
             if (s != MW_OK) return s;
         }
     }
     MW_CHECK_CUDA(cudaGetLastError());
     return MW_OK;
+}
+
+static size_t panel_ws_bytes() {
+    size_t a, b, c, d;
+    return ws_layout(kMaxPanelGrid, &a, &b, &c, &d);
+}
+
+// Workspace of the complex64 path: panel slots, then the tensor-core
+// operand planes for the largest update (m = n, n = n, k = kNB), then the
+// device status word.
+static size_t cgetrf_ws_bytes(int64_t n, int64_t nrhs_max) {
+    int64_t w = n > nrhs_max ? n : nrhs_max;
+    return panel_ws_bytes() + 1024 + cgemm_tc_workspace(n, w, kNB) + 256;
+}
+
+static Updater tc_updater(char* ws, size_t ws_bytes, int64_t n, int64_t nrhs_max) {
+    Updater u;
+    size_t p = (panel_ws_bytes() + 1023) & ~size_t(1023);
+    int64_t w = n > nrhs_max ? n : nrhs_max;
+    u.tc_ws = ws + p;
+    u.tc_ws_bytes = cgemm_tc_workspace(n, w, kNB);
+    u.tc_err = reinterpret_cast<int*>(ws + p + ((u.tc_ws_bytes + 255) & ~size_t(255)));
+    (void)ws_bytes;
+    return u;
+}
+
+}  // namespace mw
+
+using namespace mw;
+
+extern "C" size_t mw_getrf_workspace_size(int64_t n) {
+    (void)n;
+    return panel_ws_bytes();
+}
+
+extern "C" mw_status mw_zgetrf(int64_t n, double* Ad, int64_t lda, int32_t* ipiv, int32_t* info, void* workspace,
+                               size_t workspace_bytes, const volatile int32_t* cancel, void* stream) {
+    MW_REQUIRE(n >= 0 && lda >= (n > 0 ? n : 1), "bad n/lda");
+    MW_REQUIRE(Ad && ipiv && info && workspace, "NULL argument");
+    MW_REQUIRE(workspace_bytes >= mw_getrf_workspace_size(n), "workspace too small");
+    return getrf<cd>(n, reinterpret_cast<cd*>(Ad), lda, ipiv, info, static_cast<char*>(workspace), cancel, Updater{},
+                     as_stream(stream));
+}
+
+extern "C" mw_status mw_zgetrs(int64_t n, int64_t nrhs, const double* LUd, int64_t lda, const int32_t* ipiv,
+                               double* Bd, int64_t ldb, void* stream) {
+    MW_REQUIRE(n >= 0 && nrhs >= 0 && lda >= (n > 0 ? n : 1) && ldb >= (n > 0 ? n : 1), "bad sizes");
+    MW_REQUIRE(LUd && ipiv && Bd, "NULL argument");
+    if (n == 0 || nrhs == 0) return MW_OK;
+    return getrs<cd>(n, nrhs, reinterpret_cast<const cd*>(LUd), lda, ipiv, reinterpret_cast<cd*>(Bd), ldb, Updater{},
+                     as_stream(stream));
+}
+
+extern "C" size_t mw_cgetrf_workspace_size(int64_t n, int64_t nrhs_max) { return cgetrf_ws_bytes(n, nrhs_max); }
+
+extern "C" mw_status mw_cgetrf(int64_t n, float* Ad, int64_t lda, int32_t* ipiv, int32_t* info, void* workspace,
+                               size_t workspace_bytes, int64_t nrhs_max, const volatile int32_t* cancel, void* stream) {
+    MW_REQUIRE(n >= 0 && lda >= (n > 0 ? n : 1) && nrhs_max >= 0, "bad n/lda");
+    MW_REQUIRE(Ad && ipiv && info && workspace, "NULL argument");
+    MW_REQUIRE(workspace_bytes >= cgetrf_ws_bytes(n, nrhs_max), "workspace too small");
+    char* ws = static_cast<char*>(workspace);
+    Updater up = tc_updater(ws, workspace_bytes, n, nrhs_max);
+    cudaStream_t st = as_stream(stream);
+    MW_CHECK_CUDA(cudaMemsetAsync(up.tc_err, 0, sizeof(int), st));
+    mw_status s = getrf<cf>(n, reinterpret_cast<cf*>(Ad), lda, ipiv, info, ws, cancel, up, st);
+    if (s != MW_OK) return s;
+    // fold a tensor-core timeout into info[1] (barrier timeouts already there)
+    MW_CHECK_CUDA(cudaMemcpyAsync(info + 1, up.tc_err, sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
+    return MW_OK;
+}
+
+extern "C" mw_status mw_cgetrs(int64_t n, int64_t nrhs, const float* LUd, int64_t lda, const int32_t* ipiv, float* Bd,
+                               int64_t ldb, void* workspace, size_t workspace_bytes, void* stream) {
+    MW_REQUIRE(n >= 0 && nrhs >= 0 && lda >= (n > 0 ? n : 1) && ldb >= (n > 0 ? n : 1), "bad sizes");
+    MW_REQUIRE(LUd && ipiv && Bd && workspace, "NULL argument");
+    MW_REQUIRE(workspace_bytes >= cgetrf_ws_bytes(n, nrhs), "workspace too small");
+    if (n == 0 || nrhs == 0) return MW_OK;
+    char* ws = static_cast<char*>(workspace);
+    Updater up = tc_updater(ws, workspace_bytes, n, nrhs);
+    return getrs<cf>(n, nrhs, reinterpret_cast<const cf*>(LUd), lda, ipiv, reinterpret_cast<cf*>(Bd), ldb, up,
+                     as_stream(stream));
 }
 
 extern "C" mw_status mw_zgemm(int32_t transA, int32_t transB, int64_t m, int64_t n, int64_t k, double alpha_re,
@@ -607,6 +758,6 @@ extern "C" mw_status mw_zgemm(int32_t transA, int32_t transB, int64_t m, int64_t
     MW_REQUIRE(m >= 0 && n >= 0 && k >= 0, "negative size");
     MW_REQUIRE(A && B && C, "NULL argument");
     return zgemm_launch(transA != 0, transB != 0, m, n, k, cd{alpha_re, alpha_im}, reinterpret_cast<const cd*>(A),
-                        lda, reinterpret_cast<const cd*>(B), ldb, cd{beta_re, beta_im}, reinterpret_cast<cd*>(C),
-                        ldc, as_stream(stream));
+                        lda, reinterpret_cast<const cd*>(B), ldb, cd{beta_re, beta_im}, reinterpret_cast<cd*>(C), ldc,
+                        as_stream(stream));
 }

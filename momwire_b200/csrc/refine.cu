@@ -1,0 +1,168 @@
+// Mixed-precision solve with FP64 iterative refinement (sm_100a).
+//
+// Solves Z X = B (complex128) from a complex64 LU of the same matrix:
+//   X0 = LU32 \ B;  repeat  R = B - Z X (FP64),  C = LU32 \ R,  X += C
+// until max over columns of ||C||_inf / ||X||_inf <= tol.  The factors come
+// from mw_cgetrf (tensor-core trailing updates, 3xTF32); the residual uses
+// the FP64 Z.  The reference solves in complex128 LAPACK
+// (bspline.py:2971-2989); this path adds nothing to its algebra.
+#include <cmath>
+#include <vector>
+
+#include "common.cuh"
+
+namespace mw {
+mw_status zgemm_launch(bool ta, bool tb, int64_t m, int64_t n, int64_t k, cd alpha, const cd* A, int64_t lda,
+                       const cd* B, int64_t ldb, cd beta, cd* C, int64_t ldc, cudaStream_t st);
+
+__global__ void to_c64_kernel(const cd* __restrict__ src, int64_t lds, cf* __restrict__ dst, int64_t ldd, int64_t n,
+                              int64_t ncol) {
+    const int64_t total = n * ncol;
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = q % n, j = q / n;
+        const cd v = src[i + j * lds];
+        dst[i + j * ldd] = cf{(float)v.re, (float)v.im};
+    }
+}
+
+// X += C (widened), and per-column max-abs of C and of the new X.
+__global__ void accumulate_kernel(const cf* __restrict__ C, int64_t ldc, cd* __restrict__ X, int64_t ldx, int64_t n,
+                                  double* __restrict__ cmax, double* __restrict__ xmax) {
+    const int64_t j = blockIdx.y;
+    double mc = 0.0, mx = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const cf c = C[i + j * ldc];
+        cd x = X[i + j * ldx];
+        x.re += (double)c.re;
+        x.im += (double)c.im;
+        X[i + j * ldx] = x;
+        mc = fmax(mc, fabs((double)c.re) + fabs((double)c.im));
+        mx = fmax(mx, fabs(x.re) + fabs(x.im));
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        mc = fmax(mc, __shfl_xor_sync(0xffffffffu, mc, off));
+        mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        // non-negative doubles order like their bit patterns
+        atomicMax(reinterpret_cast<unsigned long long*>(cmax + j), (unsigned long long)__double_as_longlong(mc));
+        atomicMax(reinterpret_cast<unsigned long long*>(xmax + j), (unsigned long long)__double_as_longlong(mx));
+    }
+}
+
+__global__ void copy_c128_kernel(const cd* __restrict__ src, int64_t lds, cd* __restrict__ dst, int64_t ldd, int64_t n,
+                                 int64_t ncol) {
+    const int64_t total = n * ncol;
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = q % n, j = q / n;
+        dst[i + j * ldd] = src[i + j * lds];
+    }
+}
+
+static unsigned grid_for(int64_t total) {
+    int64_t b = (total + 255) / 256;
+    return (unsigned)(b < 4096 ? (b < 1 ? 1 : b) : 4096);
+}
+
+}  // namespace mw
+
+using namespace mw;
+
+extern "C" size_t mw_cgetrf_workspace_size(int64_t n, int64_t nrhs_max);
+extern "C" mw_status mw_cgetrf(int64_t n, float* A, int64_t lda, int32_t* ipiv, int32_t* info, void* workspace,
+                               size_t workspace_bytes, int64_t nrhs_max, const volatile int32_t* cancel, void* stream);
+extern "C" mw_status mw_cgetrs(int64_t n, int64_t nrhs, const float* LU, int64_t lda, const int32_t* ipiv, float* B,
+                               int64_t ldb, void* workspace, size_t workspace_bytes, void* stream);
+
+static size_t al256(size_t x) { return (x + 255) & ~size_t(255); }
+
+extern "C" size_t mw_zgesv_mixed_workspace_size(int64_t n, int64_t nrhs) {
+    return al256(mw_cgetrf_workspace_size(n, nrhs)) + al256((size_t)n * nrhs * 16) + al256((size_t)n * nrhs * 8) +
+           al256((size_t)nrhs * 16);
+}
+
+extern "C" mw_status mw_zgesv_mixed(int64_t n, int64_t nrhs, const double* Z, int64_t ldz, float* Z32, int64_t ldz32,
+                                    int32_t* ipiv, const double* B, int64_t ldb, double* X, int64_t ldx, double tol,
+                                    int32_t max_iter, void* workspace, size_t workspace_bytes, int32_t* info,
+                                    int32_t* iterations, double* last_correction, const volatile int32_t* cancel,
+                                    void* stream) {
+    MW_REQUIRE(n >= 1 && nrhs >= 1 && ldz >= n && ldz32 >= n && ldb >= n && ldx >= n, "bad sizes");
+    MW_REQUIRE(Z && Z32 && ipiv && B && X && workspace && info, "NULL argument");
+    MW_REQUIRE(max_iter >= 0, "max_iter < 0");
+    MW_REQUIRE(workspace_bytes >= mw_zgesv_mixed_workspace_size(n, nrhs), "workspace too small");
+    cudaStream_t st = as_stream(stream);
+    char* w = static_cast<char*>(workspace);
+    const size_t lu_ws = mw_cgetrf_workspace_size(n, nrhs);
+    void* ws_lu = w;
+    cd* R = reinterpret_cast<cd*>(w + al256(lu_ws));
+    cf* R32 = reinterpret_cast<cf*>(w + al256(lu_ws) + al256((size_t)n * nrhs * 16));
+    double* norms = reinterpret_cast<double*>(w + al256(lu_ws) + al256((size_t)n * nrhs * 16) +
+                                              al256((size_t)n * nrhs * 8));
+    const cd* Zc = reinterpret_cast<const cd*>(Z);
+    const cd* Bc = reinterpret_cast<const cd*>(B);
+    cd* Xc = reinterpret_cast<cd*>(X);
+    const int64_t tot = n * nrhs;
+
+    mw_status s = mw_cgetrf(n, Z32, ldz32, ipiv, info, ws_lu, lu_ws, nrhs, cancel, stream);
+    if (s != MW_OK) return s;
+    int32_t hinfo[2] = {0, 0};
+    MW_CHECK_CUDA(cudaMemcpyAsync(hinfo, info, sizeof(hinfo), cudaMemcpyDeviceToHost, st));
+    MW_CHECK_CUDA(cudaStreamSynchronize(st));
+    if (hinfo[1] != 0) {
+        set_error("factorisation: a bounded device wait timed out");
+        return MW_ERR_TIMEOUT;
+    }
+    if (hinfo[0] > 0) {
+        set_error("exact zero pivot at column %d", hinfo[0]);
+        return MW_ERR_SINGULAR;
+    }
+    // X = 0, R = B
+    MW_CHECK_CUDA(cudaMemsetAsync(norms, 0, sizeof(double) * 2 * nrhs, st));
+    for (int64_t j = 0; j < nrhs; ++j) MW_CHECK_CUDA(cudaMemsetAsync(Xc + j * ldx, 0, sizeof(cd) * n, st));
+    copy_c128_kernel<<<grid_for(tot), 256, 0, st>>>(Bc, ldb, R, n, n, nrhs);
+    count_launch();
+    double corr = INFINITY;
+    int it = 0;
+    std::vector<double> hn(2 * nrhs);
+    for (;; ++it) {
+        if (cancel && *cancel) {
+            set_error("solve cancelled");
+            return MW_ERR_CANCELLED;
+        }
+        {
+            ProfileScope ps(PC_REFINE, st, 0.0, 24.0 * (double)tot);
+            to_c64_kernel<<<grid_for(tot), 256, 0, st>>>(R, n, R32, n, n, nrhs);
+            count_launch();
+        }
+        s = mw_cgetrs(n, nrhs, Z32, ldz32, ipiv, reinterpret_cast<float*>(R32), n, ws_lu, lu_ws, stream);
+        if (s != MW_OK) return s;
+        MW_CHECK_CUDA(cudaMemsetAsync(norms, 0, sizeof(double) * 2 * nrhs, st));
+        {
+            ProfileScope ps(PC_REFINE, st, 2.0 * (double)tot, 40.0 * (double)tot);
+            dim3 g((unsigned)((n + 255) / 256 < 64 ? (n + 255) / 256 : 64), (unsigned)nrhs);
+            accumulate_kernel<<<g, 256, 0, st>>>(R32, n, Xc, ldx, n, norms, norms + nrhs);
+            count_launch();
+        }
+        MW_CHECK_CUDA(cudaMemcpyAsync(hn.data(), norms, sizeof(double) * 2 * nrhs, cudaMemcpyDeviceToHost, st));
+        MW_CHECK_CUDA(cudaStreamSynchronize(st));
+        corr = 0.0;
+        for (int64_t j = 0; j < nrhs; ++j) {
+            double xm = hn[nrhs + j];
+            double r = xm > 0.0 ? hn[j] / xm : (hn[j] > 0.0 ? INFINITY : 0.0);
+            if (!(r <= corr)) corr = r;  // NaN-propagating max
+        }
+        if (corr <= tol || it >= max_iter) break;
+        // R = B - Z X   (FP64)
+        copy_c128_kernel<<<grid_for(tot), 256, 0, st>>>(Bc, ldb, R, n, n, nrhs);
+        count_launch();
+        s = zgemm_launch(false, false, n, nrhs, n, cd{-1.0, 0.0}, Zc, ldz, Xc, ldx, cd{1.0, 0.0}, R, n, st);
+        if (s != MW_OK) return s;
+    }
+    if (iterations) *iterations = it;
+    if (last_correction) *last_correction = corr;
+    if (!(corr <= tol)) {
+        set_error("iterative refinement did not reach tol %.3g in %d steps (last correction %.3g)", tol, it, corr);
+        return MW_ERR_SINGULAR;
+    }
+    return MW_OK;
+}

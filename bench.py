@@ -44,6 +44,13 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--nx", type=int, default=16)
+    ap.add_argument("--micro", default=None, choices=["cgemm_tc"], help="kernel microbenchmark instead")
+    ap.add_argument("--m", type=int, default=8192)
+    ap.add_argument("--k", type=int, default=64)
+    ap.add_argument("--workload", default="array", choices=["array", "yagi_sweep"])
+    ap.add_argument("--n-struct", type=int, default=512)
+    ap.add_argument("--fp64-structs", type=int, default=4)
+    ap.add_argument("--fp64-kstep", type=int, default=4)
     return ap.parse_args()
 
 
@@ -318,8 +325,98 @@ def run_b200(args, kw):
         pg.destroy_process_group()
 
 
+def run_micro(args):
+    """Kernel microbenchmark: C (m x m complex64) -= A (m x k) B (k x m)
+    through mw_cgemm_tc_sub, timed with CUDA events."""
+    import torch
+
+    from momwire_b200 import _lib
+
+    m, k = args.m, args.k
+    dev = torch.device("cuda", 0)
+    A = torch.randn(k, m, dtype=torch.complex64, device=dev)  # column-major (m x k)
+    B = torch.randn(m, k, dtype=torch.complex64, device=dev)  # column-major (k x m)
+    Cm = torch.randn(m, m, dtype=torch.complex64, device=dev)
+    wsb = _lib.load().mw_cgemm_tc_workspace_size(m, m, k)
+    ws = torch.empty(wsb, dtype=torch.uint8, device=dev)
+    status = torch.zeros(1, dtype=torch.int32, device=dev)
+
+    def run():
+        _lib.call("mw_cgemm_tc_sub", m, m, k, A.data_ptr(), m, B.data_ptr(), k, Cm.data_ptr(), m, ws.data_ptr(), wsb,
+                  status.data_ptr(), None)
+
+    run()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        run()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    print(json.dumps({"micro": "cgemm_tc", "m": m, "n": m, "k": k, "ms": ms,
+                      "tflops_algorithmic": 8.0 * m * m * k / (ms / 1e3) / 1e12, "status": int(status.item())}))
+
+
+def run_sweep(args):
+    """The batched-sweep workload: seeded Yagis, 64 frequencies each,
+    25.2-30.8 MHz.  Mixed + batched over all structures (device-timed per
+    structure with CUDA events, summed), against the plain FP64 GPU path
+    (per-frequency complex128 solves) on the first --fp64-structs
+    structures, extrapolated per solve."""
+    import numpy as np
+    import torch
+
+    import momwire_b200
+    from momwire_b200.workloads import yagi_sweep
+
+    structs, ks = yagi_sweep(n_structures=args.n_struct, n_freq=64, seed=0)
+    stream = torch.cuda.current_stream()
+
+    def timed(fn):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        out = fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return out, a.elapsed_time(b)
+
+    # warm-up (library init, kernels)
+    momwire_b200.BSplineSolver(**structs[0], precision="mixed").compute_y_matrix_swept(ks[:4])
+    total_ms, iters, max_err = 0.0, 0, 0.0
+    ys = []
+    for kw in structs:
+        s = momwire_b200.BSplineSolver(**kw, precision="mixed")
+        y, ms = timed(lambda: s.compute_y_matrix_swept(ks))
+        total_ms += ms
+        iters = max(iters, s.last_refinement["iterations"])
+        ys.append(y)
+    mixed_pts = len(structs) * len(ks) / (total_ms / 1e3)
+    fp64_ms, n_fp64 = 0.0, 0
+    for i, kw in enumerate(structs[: args.fp64_structs]):
+        s = momwire_b200.BSplineSolver(**kw)
+        sub = ks[:: args.fp64_kstep]
+        y, ms = timed(lambda: s.compute_y_matrix_swept(sub))
+        fp64_ms += ms
+        n_fp64 += len(sub)
+        z64 = 1.0 / y[:, 0, 0]
+        zmx = 1.0 / ys[i][:: args.fp64_kstep, 0, 0]
+        max_err = max(max_err, float(np.max(np.abs(zmx - z64) / np.abs(z64))))
+    fp64_pts = n_fp64 / (fp64_ms / 1e3)
+    print(json.dumps({"workload": f"yagi_sweep_{len(structs)}x64", "mixed_batched_pts_per_s": mixed_pts,
+                      "mixed_total_s": total_ms / 1e3, "fp64_per_k_pts_per_s": fp64_pts,
+                      "fp64_sample_solves": n_fp64, "speedup": mixed_pts / fp64_pts,
+                      "max_rel_dZin_vs_fp64": max_err, "max_refinement_iterations": iters}), flush=True)
+
+
 def main():
     args = parse()
+    if args.micro:
+        run_micro(args)
+        return
+    if args.workload == "yagi_sweep":
+        run_sweep(args)
+        return
     from momwire_b200.workloads import dipole_array
 
     kw = dipole_array(args.nx, args.nx)

@@ -313,6 +313,45 @@ mw_status mw_zgesv_mixed(int64_t n, int64_t nrhs, const double* Z, int64_t ldz,
                          const volatile int32_t* cancel, void* stream);
 
 /*
+ * Frequency-batched fill: Z_b (and Z32_b when Z32 != NULL) for n_k
+ * wavenumbers k_dev[b] / omega_dev[b] (device arrays), free space or a PEC
+ * ground (pec_ground != 0), in two launches.  `table` (device) holds
+ * n_k same-edge tables: n_k * edges->table_rows * (d+1)^2 complex128.
+ * Matrices are z_stride (z32_stride) complex elements apart.  Replaces the
+ * k-batched reference fill seg_seg_full_moments_bspline_swept +
+ * assemble_Z_bspline_swept (_accelerators.cpp:2711, :1922; driven by
+ * bspline.py:4283-4439).
+ */
+mw_status mw_fill_z_batch(const mw_segments* seg, const mw_basis* basis,
+                          const mw_edges* edges, int32_t n_k, const double* k_dev,
+                          const double* omega_dev, double eps0, double mu0,
+                          int32_t n_qp, int32_t extended_kernel, double ground_z,
+                          int32_t pec_ground, double* table, double* Z, int64_t ldz,
+                          int64_t z_stride, float* Z32, int64_t ldz32,
+                          int64_t z32_stride, void* stream);
+
+/*
+ * Batched mixed-precision solve of `batch` same-order systems Z_b X_b = B_b
+ * (complex128, n x nrhs; B shared when b_stride == 0): complex64 LU of Z32_b
+ * (overwritten) with one CTA per matrix panel and the batched tensor-core
+ * update, then FP64 refinement of every X_b against Z_b until the largest
+ * relative correction over the batch is <= tol.  X is batch x n x nrhs,
+ * contiguous.  The reference's counterpart is the stacked complex128
+ * numpy.linalg.solve of _solve_with_kcl_swept_ports (bspline.py:3017).
+ * Strides count complex elements.  n <= 1600 (the complex64 panel of 16
+ * columns, 128 n bytes, must fit in 200 KB of shared memory).
+ */
+size_t mw_zgesv_mixed_batched_workspace_size(int32_t n, int32_t nrhs, int32_t batch);
+mw_status mw_zgesv_mixed_batched(int32_t n, int32_t nrhs, int32_t batch,
+                                 const double* Z, int64_t ldz, int64_t z_stride,
+                                 float* Z32, int64_t ldz32, int64_t z32_stride,
+                                 int32_t* ipiv, int32_t* info, const double* B,
+                                 int64_t ldb, int64_t b_stride, double* X, double tol,
+                                 int32_t max_iter, void* workspace,
+                                 size_t workspace_bytes, int32_t* iterations,
+                                 double* last_correction, void* stream);
+
+/*
  * C = alpha * op(A) * op(B) + beta * C for complex128 column-major
  * matrices, op = 'N' or 'T' (transA/transB 0/1).  Used for the KCL Schur
  * step and Y = B^T X (bspline.py:2984-2989, 4179).

@@ -848,12 +848,87 @@ class BSplineSolver:
         return out
 
     def compute_y_matrix_swept(self, k_array) -> np.ndarray:
-        """(n_k, n_ports, n_ports) Y matrices (``_port_solution.py:142``)."""
+        """(n_k, n_ports, n_ports) Y matrices (``_port_solution.py:142``).
+
+        With ``precision="mixed"`` on free space or a PEC ground and no KCL
+        constraint rows, every frequency of a chunk is filled in one batched
+        launch and factorised together (``_swept_batched``); otherwise each
+        k takes the single-solve path."""
         k_array = np.asarray(k_array, dtype=float)
+        if self._swept_batched_available():
+            return self._swept_batched(k_array)
         n_p = self._port_count()
         out = np.zeros((k_array.shape[0], n_p, n_p), dtype=np.complex128)
         for i, sol in enumerate(self.compute_port_solution_swept(k_array)):
             out[i] = sol.y
+        return out
+
+    def _swept_batched_available(self):
+        """Batched route: mixed precision, free space or PEC image (finite
+        grounds carry per-k weight tables), no KCL rows left after the port
+        split, order within the batched panel's limit."""
+        if self.precision != "mixed" or self.ground_eps is not None:
+            return False
+        kcl, _pa, _pv = self._split_kcl_ports(self._basis().kcl_A)
+        return kcl.shape[0] == 0 and self._basis().n <= 1600
+
+    def _fill_batched(self, ks, stream):
+        """(Z, Z32): device (n_k, n, n) complex128 / complex64 stacks, each
+        matrix column-major (Z[b].T is the matrix at ks[b]), from one
+        batched fill launch."""
+        torch = _torch()
+        dev = self._torch_device()
+        dt = self._dev_tables()
+        n, d = self._basis().n, self.degree
+        nk = len(ks)
+        kb = torch.from_numpy(np.asarray(ks, dtype=np.float64)).to(dev)
+        ob = torch.from_numpy(np.asarray(ks, dtype=np.float64) * self.c).to(dev)
+        table = torch.empty((nk, max(dt.table_rows, 1), d + 1, d + 1), dtype=torch.complex128, device=dev)
+        Z = torch.empty((nk, n, n), dtype=torch.complex128, device=dev)
+        Z32 = torch.empty((nk, n, n), dtype=torch.complex64, device=dev)
+        pec = 1 if self.ground_z is not None else 0
+        _lib.call("mw_fill_z_batch", C.byref(dt.seg), C.byref(dt.basis), C.byref(dt.edges), nk, kb.data_ptr(),
+                  ob.data_ptr(), float(self.eps), float(self.mu), self.n_qp_pair, int(self.extended_kernel),
+                  float(self.ground_z or 0.0), pec, table.data_ptr(), Z.data_ptr(), n, n * n, Z32.data_ptr(), n,
+                  n * n, stream)
+        return Z, Z32
+
+    def _swept_batched(self, k_array, mem_budget_bytes=16 << 30):
+        """Chunked batched sweep: per chunk of frequencies, one batched fill
+        (Z in complex128 and complex64) and one batched mixed solve with FP64
+        refinement; Y_k = B^T X_k."""
+        torch = _torch()
+        dev = self._torch_device()
+        dt = self._dev_tables()
+        basis = self._basis()
+        n, d = basis.n, self.degree
+        B, _kcl = self._port_columns()
+        n_p = B.shape[1]
+        per_k = n * n * (16 + 8) + dt.table_rows * (d + 1) ** 2 * 16 + n * n_p * 48 + n * 4
+        chunk = int(max(1, min(len(k_array), 65535, mem_budget_bytes // max(per_k, 1))))
+        st = torch.cuda.current_stream(dev).cuda_stream
+        lib = _lib.load()
+        Bd = torch.from_numpy(np.ascontiguousarray(B.T)).to(dev)  # column-major n x n_p
+        out = np.zeros((len(k_array), n_p, n_p), dtype=np.complex128)
+        iters = []
+        for c0 in range(0, len(k_array), chunk):
+            ks = np.asarray(k_array[c0 : c0 + chunk], dtype=np.float64)
+            nk = len(ks)
+            Z, Z32 = self._fill_batched(ks, st)
+            X = torch.empty((nk, n_p, n), dtype=torch.complex128, device=dev)
+            ipiv = torch.empty((nk, n), dtype=torch.int32, device=dev)
+            info = torch.zeros(nk, dtype=torch.int32, device=dev)
+            wsb = lib.mw_zgesv_mixed_batched_workspace_size(n, n_p, nk)
+            ws = torch.empty(wsb, dtype=torch.uint8, device=dev)
+            it, corr = C.c_int32(0), C.c_double(0.0)
+            _lib.call("mw_zgesv_mixed_batched", n, n_p, nk, Z.data_ptr(), n, n * n, Z32.data_ptr(), n, n * n,
+                      ipiv.data_ptr(), info.data_ptr(), Bd.data_ptr(), n, 0, X.data_ptr(), float(self.mixed_tol),
+                      int(self.mixed_max_iter), ws.data_ptr(), wsb, C.byref(it), C.byref(corr), st)
+            iters.append(int(it.value))
+            Xh = X.cpu().numpy()  # (nk, n_p, n): X_k^T
+            out[c0 : c0 + nk] = np.einsum("kpn,nq->kqp", Xh, B)
+            del Z, Z32, X, ws
+        self.last_refinement = {"iterations": max(iters) if iters else 0, "chunks": len(iters)}
         return out
 
     def compute_impedance_swept(self, k_array):

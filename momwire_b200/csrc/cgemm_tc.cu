@@ -49,6 +49,11 @@ struct TcArgs {
     int64_t n;         // columns
     int n_mb, n_nb, n_ks;
     int* err;
+    // batch of independent updates: strides between consecutive C
+    // matrices (floats) and packed operand planes (floats)
+    int batch;
+    int64_t c_stride;
+    int64_t a_pstride, b_pstride;
 };
 
 // ------------------------------------------------------------ PTX helpers
@@ -156,7 +161,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) cgemm_tc_kernel(TcArgs P) {
 
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
-    const int n_tiles = P.n_mb * P.n_nb;
+    const int per_mat = P.n_mb * P.n_nb;
+    const int n_tiles = per_mat * (P.batch > 0 ? P.batch : 1);
     int* err = P.err;
 
     if (threadIdx.x == 0) {
@@ -191,13 +197,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1) cgemm_tc_kernel(TcArgs P) {
             for (int s = 0; s < TC_STAGES; ++s) ph_empty[s] = 1;
             bool dead = false;
             for (int t = blockIdx.x; t < n_tiles && !dead; t += gridDim.x) {
-                const int mb = t % P.n_mb, nb = t / P.n_mb;
+                const int bt = t / per_mat, tr = t - bt * per_mat;
+                const int mb = tr % P.n_mb, nb = tr / P.n_mb;
                 for (int ks = 0; ks < P.n_ks; ++ks) {
                     if (!mbar_wait(&bar_empty[slot], ph_empty[slot], err)) { dead = true; break; }
                     ph_empty[slot] ^= 1;
                     uint8_t* st = tc_smem + (size_t)slot * TC_STAGE_BYTES;
-                    const size_t ao = ((size_t)mb * P.n_ks + ks) * (TC_A_BYTES / 4);
-                    const size_t bo = ((size_t)nb * P.n_ks + ks) * (TC_B_BYTES / 4);
+                    const size_t ao = (size_t)bt * P.a_pstride + ((size_t)mb * P.n_ks + ks) * (TC_A_BYTES / 4);
+                    const size_t bo = (size_t)bt * P.b_pstride + ((size_t)nb * P.n_ks + ks) * (TC_B_BYTES / 4);
                     mbar_expect_tx(&bar_full[slot], TC_STAGE_BYTES);
                     bulk_g2s(st, P.a_hi + ao, TC_A_BYTES, &bar_full[slot]);
                     bulk_g2s(st + TC_A_BYTES, P.a_lo + ao, TC_A_BYTES, &bar_full[slot]);
@@ -273,7 +280,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) cgemm_tc_kernel(TcArgs P) {
         int lt = 0;
         for (int t = blockIdx.x; t < n_tiles && !dead; t += gridDim.x, ++lt) {
             const int acc = lt & 1;
-            const int mb = t % P.n_mb, nb = t / P.n_mb;
+            const int bt = t / per_mat, tr = t - bt * per_mat;
+            const int mb = tr % P.n_mb, nb = tr / P.n_mb;
             bool ok = true;
             if (lane == 0) ok = mbar_wait(&bar_accf[acc], ph_accf[acc], err);
             ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
@@ -282,20 +290,22 @@ __global__ void __launch_bounds__(TC_THREADS, 1) cgemm_tc_kernel(TcArgs P) {
             tc_fence_after();
             const int64_t r = (int64_t)mb * TC_M + quad * 32 + lane;  // real row
             const uint32_t taddr = tmem_base + ((uint32_t)(quad * 32) << 16) + acc * TC_N;
-            for (int c0 = 0; c0 < TC_N; c0 += 16) {
-                float v[16];
+            // 32 columns per round: all loads of C issue before any store so
+            // that they overlap (a store may alias the next load otherwise)
+            for (int c0 = 0; c0 < TC_N; c0 += 32) {
+                float v[32], old[32];
                 tmem_ld16(taddr + c0, v);
+                tmem_ld16(taddr + c0 + 16, v + 16);
                 const int64_t col0 = (int64_t)nb * TC_N + c0;
-                if (r < P.m_real) {
+                const bool row_ok = r < P.m_real;
+                float* cbase = P.C + (int64_t)bt * P.c_stride + r + col0 * 2 * P.ldc;
+                const int64_t cstep = 2 * P.ldc;
 #pragma unroll
-                    for (int e = 0; e < 16; ++e) {
-                        const int64_t col = col0 + e;
-                        if (col < P.n) {
-                            float* cp = P.C + r + col * 2 * P.ldc;
-                            *cp = *cp - v[e];
-                        }
-                    }
-                }
+                for (int e = 0; e < 32; ++e)
+                    old[e] = (row_ok && col0 + e < P.n) ? __ldcs(cbase + e * cstep) : 0.f;
+#pragma unroll
+                for (int e = 0; e < 32; ++e)
+                    if (row_ok && col0 + e < P.n) __stcs(cbase + e * cstep, old[e] - v[e]);
             }
             tc_fence_before();
             __syncwarp();
@@ -320,8 +330,11 @@ __device__ __forceinline__ float tf32_hi(float x) {
 // Ahat (2m x 2k, from complex A at A + (i + l*lda)) packed as
 // [mb][ks][chunk 8][row 128][4]; zero beyond (2m, 2k).
 __global__ void pack_a_kernel(const cf* __restrict__ A, int64_t lda, int64_t m, int64_t k, int n_mb, int n_ks,
-                              float* __restrict__ hi, float* __restrict__ lo) {
+                              float* __restrict__ hi, float* __restrict__ lo, int64_t a_stride, int64_t p_stride) {
     const int64_t total = (int64_t)n_mb * n_ks * 8 * TC_M;  // float4 slots
+    A += blockIdx.y * a_stride;  // batch entry
+    hi += blockIdx.y * p_stride;
+    lo += blockIdx.y * p_stride;
     for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
         const int row = (int)(q % TC_M);
         int64_t rest = q / TC_M;
@@ -355,8 +368,11 @@ __global__ void pack_a_kernel(const cf* __restrict__ A, int64_t lda, int64_t m, 
 // Breal^T (n x 2k, from complex B at B + (l + j*ldb)) packed as
 // [nb][ks][chunk 8][row 256][4]; zero beyond (n, 2k).
 __global__ void pack_b_kernel(const cf* __restrict__ B, int64_t ldb, int64_t k, int64_t n, int n_nb, int n_ks,
-                              float* __restrict__ hi, float* __restrict__ lo) {
+                              float* __restrict__ hi, float* __restrict__ lo, int64_t b_stride, int64_t p_stride) {
     const int64_t total = (int64_t)n_nb * n_ks * 8 * TC_N;
+    B += blockIdx.y * b_stride;  // batch entry
+    hi += blockIdx.y * p_stride;
+    lo += blockIdx.y * p_stride;
     for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
         const int row = (int)(q % TC_N);
         int64_t rest = q / TC_N;
@@ -395,27 +411,31 @@ size_t tc_pack_b_bytes(int64_t k, int64_t n) {
     return (size_t)n_nb * n_ks * TC_B_BYTES;
 }
 
-// C (m x n, complex64 col-major) -= A (m x k) B (k x n), via packed planes
-// in `ws` (layout: a_hi | a_lo | b_hi | b_lo, each 1 KB aligned).
-mw_status cgemm_tc_update(int64_t m, int64_t n, int64_t k, const cf* A, int64_t lda, const cf* B, int64_t ldb, cf* C,
-                          int64_t ldc, void* ws, size_t ws_bytes, int* err, cudaStream_t st) {
-    if (m <= 0 || n <= 0 || k <= 0) return MW_OK;
+// Batched: C_b (m x n, complex64 col-major) -= A_b (m x k) B_b (k x n) for
+// b < batch, matrices `sa`, `sb`, `sc` complex elements apart; packed
+// planes in `ws` (a_hi | a_lo | b_hi | b_lo, each 1 KB aligned, batch-major).
+mw_status cgemm_tc_update_batched(int64_t m, int64_t n, int64_t k, int batch, const cf* A, int64_t lda, int64_t sa,
+                                  const cf* B, int64_t ldb, int64_t sb, cf* C, int64_t ldc, int64_t sc, void* ws,
+                                  size_t ws_bytes, int* err, cudaStream_t st) {
+    if (m <= 0 || n <= 0 || k <= 0 || batch <= 0) return MW_OK;
     const int n_mb = (int)((2 * m + TC_M - 1) / TC_M);
     const int n_nb = (int)((n + TC_N - 1) / TC_N);
     const int n_ks = (int)((2 * k + TC_KS - 1) / TC_KS);
     const size_t ab = tc_pack_a_bytes(m, k), bb = tc_pack_b_bytes(k, n);
     auto al = [](size_t x) { return (x + 1023) & ~size_t(1023); };
-    MW_REQUIRE(2 * al(ab) + 2 * al(bb) <= ws_bytes, "tensor-core GEMM workspace too small");
+    MW_REQUIRE(2 * al(ab * batch) + 2 * al(bb * batch) <= ws_bytes, "tensor-core GEMM workspace too small");
+    MW_REQUIRE(batch <= 65535, "batch too large");
     char* w = static_cast<char*>(ws);
     float* a_hi = reinterpret_cast<float*>(w);
-    float* a_lo = reinterpret_cast<float*>(w + al(ab));
-    float* b_hi = reinterpret_cast<float*>(w + 2 * al(ab));
-    float* b_lo = reinterpret_cast<float*>(w + 2 * al(ab) + al(bb));
+    float* a_lo = reinterpret_cast<float*>(w + al(ab * batch));
+    float* b_hi = reinterpret_cast<float*>(w + 2 * al(ab * batch));
+    float* b_lo = reinterpret_cast<float*>(w + 2 * al(ab * batch) + al(bb * batch));
     {
         ProfileScope ps(PC_MISC, st);
         int64_t qa = (int64_t)n_mb * n_ks * 8 * TC_M, qb = (int64_t)n_nb * n_ks * 8 * TC_N;
-        pack_a_kernel<<<(unsigned)((qa + 255) / 256), 256, 0, st>>>(A, lda, m, k, n_mb, n_ks, a_hi, a_lo);
-        pack_b_kernel<<<(unsigned)((qb + 255) / 256), 256, 0, st>>>(B, ldb, k, n, n_nb, n_ks, b_hi, b_lo);
+        dim3 ga((unsigned)((qa + 255) / 256), (unsigned)batch), gb((unsigned)((qb + 255) / 256), (unsigned)batch);
+        pack_a_kernel<<<ga, 256, 0, st>>>(A, lda, m, k, n_mb, n_ks, a_hi, a_lo, sa, (int64_t)(ab / 4));
+        pack_b_kernel<<<gb, 256, 0, st>>>(B, ldb, k, n, n_nb, n_ks, b_hi, b_lo, sb, (int64_t)(bb / 4));
         count_launch(2);
     }
     static int sms = 0;
@@ -426,16 +446,28 @@ mw_status cgemm_tc_update(int64_t m, int64_t n, int64_t k, const cf* A, int64_t 
         MW_CHECK_CUDA(cudaFuncSetAttribute(cgemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            TC_STAGES * TC_STAGE_BYTES));
     }
-    TcArgs P{a_hi, a_lo, b_hi, b_lo, reinterpret_cast<float*>(C), ldc, 2 * m, n, n_mb, n_nb, n_ks, err};
-    const int tiles = n_mb * n_nb;
-    const int grid = tiles < sms ? tiles : sms;
+    TcArgs P{a_hi, a_lo, b_hi, b_lo, reinterpret_cast<float*>(C), ldc, 2 * m, n, n_mb, n_nb, n_ks, err,
+             batch,    2 * sc, (int64_t)(ab / 4), (int64_t)(bb / 4)};
+    const int64_t tiles = (int64_t)n_mb * n_nb * batch;
+    MW_REQUIRE(tiles < (1ll << 31), "too many tiles");
+    const int grid = tiles < sms ? (int)tiles : sms;
     {
-        ProfileScope ps(PC_CGEMM_TC, st, 8.0 * (double)m * n * k, 8.0 * 2.0 * (double)m * n);
+        ProfileScope ps(PC_CGEMM_TC, st, 8.0 * (double)m * n * k * batch, 8.0 * 2.0 * (double)m * n * batch);
         cgemm_tc_kernel<<<grid, TC_THREADS, TC_STAGES * TC_STAGE_BYTES, st>>>(P);
     }
     MW_CHECK_CUDA(cudaGetLastError());
     count_launch();
     return MW_OK;
+}
+
+mw_status cgemm_tc_update(int64_t m, int64_t n, int64_t k, const cf* A, int64_t lda, const cf* B, int64_t ldb, cf* C,
+                          int64_t ldc, void* ws, size_t ws_bytes, int* err, cudaStream_t st) {
+    return cgemm_tc_update_batched(m, n, k, 1, A, lda, 0, B, ldb, 0, C, ldc, 0, ws, ws_bytes, err, st);
+}
+
+size_t cgemm_tc_workspace_batched(int64_t m, int64_t n, int64_t k, int batch) {
+    auto al = [](size_t x) { return (x + 1023) & ~size_t(1023); };
+    return 2 * al(tc_pack_a_bytes(m, k) * batch) + 2 * al(tc_pack_b_bytes(k, n) * batch);
 }
 
 size_t cgemm_tc_workspace(int64_t m, int64_t n, int64_t k) {

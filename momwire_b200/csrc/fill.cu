@@ -144,10 +144,14 @@ template <int D, bool EK>
 __global__ void same_edge_table_kernel(int n_edge, const int32_t* __restrict__ n_in_edge,
                                        const int64_t* __restrict__ table_off,
                                        const double* __restrict__ hs, const double* __restrict__ radii,
-                                       int64_t rows, double k, GLParams gl, double* __restrict__ out) {
+                                       int64_t rows, double k0, GLParams gl, double* __restrict__ out,
+                                       const double* __restrict__ kb, int64_t out_stride) {
     constexpr int NM = D + 1;
     int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (row >= rows) return;
+    // frequency batch: blockIdx.y selects k and the output table
+    const double k = kb ? kb[blockIdx.y] : k0;
+    out += blockIdx.y * out_stride;
     // edge owning this row: last e with table_off[e] <= row
     int lo = 0, hi = n_edge - 1;
     while (lo < hi) {
@@ -384,6 +388,12 @@ struct FillArgs {
     int64_t ldz;
     float* Z32;
     int64_t ldz32;
+    // frequency batch (blockIdx.z): per-entry k / omega (NULL = the scalars
+    // above) and the strides between consecutive tables and matrices
+    const double* kb;
+    const double* omegab;
+    int64_t table_stride, z_stride, z32_stride;
+    int nbatch;
 };
 
 template <int D, bool IMAGE, bool EK>
@@ -402,6 +412,13 @@ __global__ void __launch_bounds__(256) fill_kernel(FillArgs A, GLParams gl) {
     const int ns_r = A.basis.tile_ns[tr], ns_c = A.basis.tile_ns[tc];
     const int nb_r = A.basis.tile_nb[tr], nb_c = A.basis.tile_nb[tc];
     const int fb_r = A.basis.tile_first[tr], fb_c = A.basis.tile_first[tc];
+    const int bz = blockIdx.z;
+    const double kz = A.kb ? A.kb[bz] : A.k;
+    const double omz = A.omegab ? A.omegab[bz] : A.omega;
+    const double* table = A.table ? A.table + bz * A.table_stride : nullptr;
+    // z_stride / z32_stride count complex elements (two scalars each)
+    double* Zb = A.Z + 2 * bz * A.z_stride;
+    float* Z32b = A.Z32 ? A.Z32 + 2 * bz * A.z32_stride : nullptr;
 
     double* s_row = smem;                               // SMAX * SD
     double* s_col = s_row + SMAX * SD;                  // SMAX * SD
@@ -470,9 +487,9 @@ __global__ void __launch_bounds__(256) fill_kernel(FillArgs A, GLParams gl) {
             double acc_re = 0;  // silence unused warnings
             (void)acc_re;
             cd Jt[NM][NM];
-            pair_row<D, EK>(s_row + li * SD, s_col + lj * SD, nq, lane4, A.k, ek_on, Jt);
+            pair_row<D, EK>(s_row + li * SD, s_col + lj * SD, nq, lane4, kz, ek_on, Jt);
             cd Jt2[NM][NM];
-            pair_row<D, EK>(s_row + li * SD, s_col + lj * SD, nq, lane4 + 4, A.k, ek_on, Jt2);
+            pair_row<D, EK>(s_row + li * SD, s_col + lj * SD, nq, lane4 + 4, kz, ek_on, Jt2);
 #pragma unroll
             for (int p = 0; p < NM; ++p)
 #pragma unroll
@@ -490,7 +507,7 @@ __global__ void __launch_bounds__(256) fill_kernel(FillArgs A, GLParams gl) {
                 if (lane4 == 0) {
                     int e = s_edge_r[li];
                     int64_t row = A.e_off[e] + (s_pos_c[lj] - s_pos_r[li]) + A.e_n[e] - 1;
-                    const double* src = A.table + row * NMM * 2;
+                    const double* src = table + row * NMM * 2;
 #pragma unroll
                     for (int x = 0; x < NMM * 2; ++x) dst[x] = src[x];
                 }
@@ -530,8 +547,8 @@ __global__ void __launch_bounds__(256) fill_kernel(FillArgs A, GLParams gl) {
     __syncthreads();
 
     // ---- phase B: Galerkin contraction into the Z tile
-    const double wmu = A.omega * A.mu0;
-    const double inv_weps = 1.0 / (A.omega * A.eps0);
+    const double wmu = omz * A.mu0;
+    const double inv_weps = 1.0 / (omz * A.eps0);
     for (int pp = tid; pp < TB * TB; pp += blockDim.x) {
         int mi = pp % TB, ni = pp / TB;
         if (mi >= nb_r || ni >= nb_c) continue;
@@ -590,15 +607,15 @@ __global__ void __launch_bounds__(256) fill_kernel(FillArgs A, GLParams gl) {
         double zre = -wmu * zA.im + inv_weps * zP.im;
         double zim = wmu * zA.re - inv_weps * zP.re;
         int64_t m = fb_r + mi, n = fb_c + ni;
-        double* zp = A.Z + m * 2 + n * A.ldz * 2;
+        double* zp = Zb + m * 2 + n * A.ldz * 2;
         if (IMAGE) {
             zre = zp[0] - zre;
             zim = zp[1] - zim;
         }
         zp[0] = zre;
         zp[1] = zim;
-        if (A.Z32) {
-            float* z32 = A.Z32 + m * 2 + n * A.ldz32 * 2;
+        if (Z32b) {
+            float* z32 = Z32b + m * 2 + n * A.ldz32 * 2;
             z32[0] = (float)zre;
             z32[1] = (float)zim;
         }
@@ -688,10 +705,11 @@ static mw_status launch_fill(const FillArgs& A, const GLParams& gl, cudaStream_t
     size_t smem = fill_smem_bytes(D, IMAGE, gl.nq, A.basis.max_tile_seg, A.basis.max_tile_basis);
     auto kern = fill_kernel<D, IMAGE, EK>;
     MW_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    dim3 grid(A.basis.n_tile, A.basis.n_tile);
+    const int nbz = A.nbatch > 0 ? A.nbatch : 1;
+    dim3 grid(A.basis.n_tile, A.basis.n_tile, nbz);
     double nb = A.basis.n_basis;
-    ProfileScope ps(IMAGE ? PC_FILL_IMAGE : PC_FILL, st, fill_flops(D, gl.nq, A.seg.n_seg, nb),
-                    nb * nb * (16.0 + (A.Z32 ? 8.0 : 0.0)) * (IMAGE ? 2.0 : 1.0));
+    ProfileScope ps(IMAGE ? PC_FILL_IMAGE : PC_FILL, st, nbz * fill_flops(D, gl.nq, A.seg.n_seg, nb),
+                    nbz * nb * nb * (16.0 + (A.Z32 ? 8.0 : 0.0)) * (IMAGE ? 2.0 : 1.0));
     kern<<<grid, 256, smem, st>>>(A, gl);
     MW_CHECK_CUDA(cudaGetLastError());
     count_launch();
@@ -728,7 +746,7 @@ extern "C" mw_status mw_same_edge_table(const mw_edges* edges, int32_t degree, i
 #define MW_TBL(DD, EE)                                                                                 \
     same_edge_table_kernel<DD, EE><<<(unsigned)blocks, threads, 0, st>>>(                                \
         edges->n_edge, edges->n_in_edge, edges->table_off, edges->h, edges->radius, edges->table_rows, k, \
-        gl, out)
+        gl, out, nullptr, 0)
     if (degree == 1) { if (extended_kernel) MW_TBL(1, true); else MW_TBL(1, false); }
     else             { if (extended_kernel) MW_TBL(2, true); else MW_TBL(2, false); }
 #undef MW_TBL
@@ -817,4 +835,63 @@ extern "C" mw_status mw_fill_z_image(const mw_segments* seg, const mw_basis* bas
     cudaStream_t st = as_stream(stream);
     if (basis->degree == 1) return ek ? launch_fill<1, true, true>(A, gl, st) : launch_fill<1, true, false>(A, gl, st);
     return ek ? launch_fill<2, true, true>(A, gl, st) : launch_fill<2, true, false>(A, gl, st);
+}
+
+extern "C" mw_status mw_fill_z_batch(const mw_segments* seg, const mw_basis* basis, const mw_edges* edges,
+                                     int32_t n_k, const double* k_dev, const double* omega_dev, double eps0,
+                                     double mu0, int32_t n_qp, int32_t extended_kernel, double ground_z,
+                                     int32_t pec_ground, double* table, double* Z, int64_t ldz, int64_t z_stride,
+                                     float* Z32, int64_t ldz32, int64_t z32_stride, void* stream) {
+    MW_REQUIRE(seg && basis && edges && k_dev && omega_dev && table && Z, "NULL argument");
+    MW_REQUIRE(n_k >= 1 && n_k <= 65535, "n_k out of range (%d)", n_k);
+    mw_status s = check_common(basis, n_qp);
+    if (s != MW_OK) return s;
+    MW_REQUIRE(ldz >= basis->n_basis && z_stride >= ldz * basis->n_basis, "bad Z layout");
+    MW_REQUIRE(Z32 == nullptr || (ldz32 >= basis->n_basis && z32_stride >= ldz32 * basis->n_basis), "bad Z32 layout");
+    const int d = basis->degree;
+    const int64_t tstride = edges->table_rows * (d + 1) * (d + 1) * 2;
+    GLParams gl = make_gl(n_qp);
+    cudaStream_t st = as_stream(stream);
+    if (edges->table_rows > 0) {
+        ProfileScope ps(PC_TABLE, st);
+        const int threads = 128;
+        dim3 grid((unsigned)((edges->table_rows + threads - 1) / threads), (unsigned)n_k);
+        const bool ek = extended_kernel != 0;
+        if (d == 1) {
+            if (ek) same_edge_table_kernel<1, true><<<grid, threads, 0, st>>>(edges->n_edge, edges->n_in_edge, edges->table_off, edges->h, edges->radius, edges->table_rows, 0.0, gl, table, k_dev, tstride);
+            else same_edge_table_kernel<1, false><<<grid, threads, 0, st>>>(edges->n_edge, edges->n_in_edge, edges->table_off, edges->h, edges->radius, edges->table_rows, 0.0, gl, table, k_dev, tstride);
+        } else {
+            if (ek) same_edge_table_kernel<2, true><<<grid, threads, 0, st>>>(edges->n_edge, edges->n_in_edge, edges->table_off, edges->h, edges->radius, edges->table_rows, 0.0, gl, table, k_dev, tstride);
+            else same_edge_table_kernel<2, false><<<grid, threads, 0, st>>>(edges->n_edge, edges->n_in_edge, edges->table_off, edges->h, edges->radius, edges->table_rows, 0.0, gl, table, k_dev, tstride);
+        }
+        MW_CHECK_CUDA(cudaGetLastError());
+        count_launch();
+    }
+    FillArgs A{};
+    A.seg = *seg;
+    A.basis = *basis;
+    A.table = table;
+    A.e_n = edges->n_in_edge;
+    A.e_off = edges->table_off;
+    A.eps0 = eps0;
+    A.mu0 = mu0;
+    A.Z = Z;
+    A.ldz = ldz;
+    A.Z32 = Z32;
+    A.ldz32 = ldz32;
+    A.kb = k_dev;
+    A.omegab = omega_dev;
+    A.table_stride = tstride;
+    A.z_stride = z_stride;
+    A.z32_stride = z32_stride;
+    A.nbatch = n_k;
+    const bool ek = seg->ek_group != nullptr;
+    s = (d == 1) ? (ek ? launch_fill<1, false, true>(A, gl, st) : launch_fill<1, false, false>(A, gl, st))
+                 : (ek ? launch_fill<2, false, true>(A, gl, st) : launch_fill<2, false, false>(A, gl, st));
+    if (s != MW_OK || !pec_ground) return s;
+    MW_REQUIRE(!ek || seg->ek_group_img != nullptr, "EK image fill needs ek_group_img labels");
+    A.ground.model = MW_GROUND_PEC;
+    A.ground.ground_z = ground_z;
+    return (d == 1) ? (ek ? launch_fill<1, true, true>(A, gl, st) : launch_fill<1, true, false>(A, gl, st))
+                    : (ek ? launch_fill<2, true, true>(A, gl, st) : launch_fill<2, true, false>(A, gl, st));
 }

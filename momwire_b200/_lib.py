@@ -89,6 +89,25 @@ class Ground(C.Structure):
     ]
 
 
+class SommGrid(C.Structure):
+    _fields_ = [
+        ("n_region", i32),
+        ("n_r", i32 * 6),
+        ("n_th", i32 * 6),
+        ("offset", i64 * 6),
+        ("r0", f64 * 6),
+        ("dr", f64 * 6),
+        ("th0", f64 * 6),
+        ("dth", f64 * 6),
+        ("r1_max", f64),
+        ("r_break", f64),
+        ("th_split", f64),
+        ("r_near", f64),
+        ("value_scale", f64),
+        ("vals", vp),
+    ]
+
+
 # name -> (restype, argtypes)
 _SIGS = {
     "mw_version": (i32, []),
@@ -119,12 +138,18 @@ _SIGS = {
     "mw_zgetrf": (i32, [i64, vp, i64, vp, vp, vp, sz, vp, vp]),
     "mw_zgetrs": (i32, [i64, i64, vp, i64, vp, vp, i64, vp]),
     "mw_zgemm": (i32, [i32, i32, i64, i64, i64, f64, f64, vp, i64, vp, i64, f64, f64, vp, i64, vp]),
+    "mw_somm_surfaces_workspace_size": (sz, []),
+    "mw_somm_surfaces": (i32, [i64, vp, vp, vp, vp, f64, f64, f64, f64, f64, f64, vp, vp, vp]),
+    "mw_somm_field_proj": (i32, [i64, vp, vp, i64, vp, vp, f64, f64, C.POINTER(SommGrid), vp, vp]),
+    "mw_somm_remainder_q": (i32, [C.POINTER(Segments), C.POINTER(BasisT), C.POINTER(SommGrid), i32, f64, f64, vp,
+                                  i64, vp, i64, vp]),
+    "mw_max_image_distance": (i32, [i32, vp, vp, f64, vp, vp]),
 }
 
 EXPORTED = tuple(_SIGS)
 
 PROFILE_CLASSES = ("same_edge_table", "fill", "fill_image", "lu_panel", "laswp", "trsm", "zgemm",
-                   "cgemm_tc", "refine", "misc")
+                   "cgemm_tc", "refine", "misc", "somm_grid", "somm_q")
 
 
 def profile_enable(on=True):

@@ -23,6 +23,7 @@ import numpy as np
 
 from . import _lib
 from . import _tables as T
+from . import sommerfeld as somm
 from ._port_solution import PortSolution
 
 
@@ -653,7 +654,8 @@ class BSplineSolver:
         et = T.eps_tilde(self.ground_eps, self.omega, self.eps)
         g.eps_re, g.eps_im = et.real, et.imag
         if self.ground_model == "sommerfeld":
-            raise NotImplementedError("ground_model='sommerfeld' is not served yet")
+            g.model = _lib.MW_GROUND_SOMM_IMAGE  # C2 = (eps~-1)/(eps~+1) image
+            return g
         g.model = _lib.MW_GROUND_REFL
         g.phi_mode = _lib.PHI_MODES[self.ground_phi_mode]
         return g
@@ -720,6 +722,28 @@ class BSplineSolver:
         if g is not None:
             _lib.call("mw_fill_z_image", C.byref(dt.seg), C.byref(dt.basis), C.byref(g), C.byref(fr),
                       self.n_qp_pair, Z.data_ptr(), n, z32, n, stream)
+        if self._is_sommerfeld():
+            grid = self._somm_grid(stream)
+            _lib.call("mw_somm_remainder_q", C.byref(dt.seg), C.byref(dt.basis), C.byref(grid),
+                      self.n_qp_sommerfeld, float(self.ground_z), float(self.k), Z.data_ptr(), n, z32, n, stream)
+
+    def _is_sommerfeld(self):
+        return self.ground_z is not None and self.ground_eps is not None and self.ground_model == "sommerfeld"
+
+    def _somm_grid(self, stream):
+        """``mw_somm_grid`` of the remainder grid at the current k
+        (``bspline.py:1781-1789``, ``:1859-1862``): the cached
+        wavelength-normalised master for (bucketed eps~, r1 bucket), viewed
+        at this k, omega and mu."""
+        dt = self._dev_tables()
+        dev = self._torch_device()
+        if getattr(self, "_somm_r1", None) is None:
+            self._somm_r1 = somm.max_image_distance(dt.seg.seg_l, dt.seg.seg_r, dt.seg.n_seg, self.ground_z, dev,
+                                                    stream)
+        et = T.eps_tilde(self.ground_eps, self.omega, self.eps)
+        master = somm.get_master(et, self.k, self._somm_r1, dev, stream)
+        self._somm_master = master
+        return master.view(self.k, self.omega, self.mu)
 
     def _lu_solve(self, A, n, ws, ipiv, info, rhs, nrhs, stream):
         """zgetrf(A) in place then zgetrs on rhs (both column-major, ld n)."""

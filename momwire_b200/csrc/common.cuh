@@ -108,7 +108,9 @@ enum ProfileClass {
     PC_CGEMM_TC = 7,
     PC_REFINE = 8,
     PC_MISC = 9,
-    PC_COUNT = 10
+    PC_SOMM_GRID = 10,
+    PC_SOMM_Q = 11,
+    PC_COUNT = 12
 };
 
 struct ProfileScope {

@@ -69,6 +69,7 @@ class Spec:
     ground_eps: object = None
     ground_phi_mode: str = "normal"
     ground_model: str = "refl-coef"
+    n_qp_sommerfeld: int = 3
 
     @property
     def k(self):
@@ -102,6 +103,7 @@ def make_spec(
     ground_eps=None,
     ground_phi_mode="normal",
     ground_model="refl-coef",
+    n_qp_sommerfeld=3,
 ):
     """Build a :class:`Spec` from BSplineSolver-style kwargs
     (``bspline.py:402-637``: per-edge counts, feeds, junction ports)."""
@@ -149,6 +151,7 @@ def make_spec(
         ground_eps=ground_eps,
         ground_phi_mode=ground_phi_mode,
         ground_model=ground_model,
+        n_qp_sommerfeld=int(n_qp_sommerfeld),
     )
 
 
@@ -672,19 +675,36 @@ def image_weights(spec, geom, omega):
     return wA, wP
 
 
-def compute_Z(spec, geom=None, basis=None):
-    """Free-space (+ image) Z for one k (``bspline.py:3702-3776``).
-    The Sommerfeld remainder is not part of this oracle."""
+def sommerfeld_grid(spec, geom, master_values=None):
+    """The remainder grid a Sommerfeld solve interpolates
+    (``bspline.py:1781-1789``, ``1861-1862``)."""
+    from oracle import sommerfeld_oracle as so
+
+    r1_max = so.max_image_distance(geom["seg_l"], geom["seg_r"], spec.ground_z)
+    et = eps_tilde(spec.ground_eps, spec.omega)
+    return so.get_grid(et, spec.k, r1_max, spec.omega, MU0, master_values=master_values)
+
+
+def compute_Z(spec, geom=None, basis=None, somm_master_values=None):
+    """Free-space (+ image) Z for one k (``bspline.py:3702-3776``).  For the
+    Sommerfeld ground the C2 image and the remainder block Q are summed
+    before the one subtraction (``_potential_ground.py:524-527``);
+    ``somm_master_values`` supplies the grid master's tables."""
     geom = geom or build_geometry(spec)
     basis = basis or build_basis(spec, geom)
     k, om = spec.k, spec.omega
     t = geom["tangents"]
     Z = assemble(fill_J(spec, geom, k), basis, om, (t @ t.T).astype(np.complex128))
     if spec.ground_z is not None:
-        if spec.ground_eps is not None and spec.ground_model == "sommerfeld":
-            raise NotImplementedError("Sommerfeld remainder is outside this oracle")
         wA, wP = image_weights(spec, geom, om)
-        Z -= assemble(fill_J_image(spec, geom, k), basis, om, wA, wP)
+        img = assemble(fill_J_image(spec, geom, k), basis, om, wA, wP)
+        if spec.ground_eps is not None and spec.ground_model == "sommerfeld":
+            from oracle import sommerfeld_oracle as so
+
+            grid = sommerfeld_grid(spec, geom, somm_master_values)
+            img = img + so.remainder_Q(geom, basis.supp_seg, basis.polys, spec.degree, spec.n_qp_sommerfeld,
+                                       spec.ground_z, k, grid)
+        Z -= img
     return Z
 
 
@@ -753,12 +773,12 @@ def solve_ports(Z, B, kcl_con):
     return W - X @ Lam
 
 
-def port_solution(spec):
+def port_solution(spec, somm_master_values=None):
     """``compute_port_solution`` (``bspline.py:4053-4179``): returns
     (Y, coeffs, Z, geom, basis)."""
     geom = build_geometry(spec)
     basis = build_basis(spec, geom)
-    Z = compute_Z(spec, geom, basis)
+    Z = compute_Z(spec, geom, basis, somm_master_values)
     B, kcl = port_columns(spec, geom, basis)
     X = solve_ports(Z, B, kcl)
     return B.T @ X, X, Z, geom, basis

@@ -40,6 +40,33 @@ def dipole_array(nx, ny, nseg=41, f=300e6, seed=0):
     return dict(wires=wires, nsegs=nseg, degree=2, wire_radius=0.5e-3, wavelength=lam, feeds=feeds)
 
 
+LAM_SOMM = C_LIGHT / 28.47e6  # 10 m band
+
+
+def somm_dipole(height_wl, ground_eps, degree, nseg):
+    """Horizontal 0.48-wavelength dipole at the given height over a
+    Sommerfeld ground, centre-fed."""
+    L, z = 0.48 * LAM_SOMM, height_wl * LAM_SOMM
+    return dict(wires=[np.array([[0.0, -L / 2, z], [0.0, L / 2, z]])], nsegs=nseg, degree=degree,
+                wavelength=LAM_SOMM, wire_radius=5e-4, ground_z=0.0, ground_eps=ground_eps,
+                ground_model="sommerfeld")
+
+
+def somm_ground_plane():
+    """Quarter-wave vertical with four sloping quarter-wave radials joined at
+    a feed point 0.05 wavelength above a Sommerfeld ground."""
+    lam = LAM_SOMM
+    base = np.array([0.0, 0.0, 0.05 * lam])
+    wires = [np.array([base, base + [0, 0, 0.25 * lam]])]
+    for ang in (0.0, 0.5 * np.pi, np.pi, 1.5 * np.pi):
+        tip = base + 0.25 * lam * np.array([0.95 * np.cos(ang), 0.95 * np.sin(ang), 0.0]) + [0, 0, -0.04 * lam]
+        wires.append(np.array([base, tip]))
+    return dict(wires=wires, nsegs=7, degree=2, wavelength=lam, wire_radius=1e-3, ground_z=0.0,
+                ground_eps=(5.0, 0.001), ground_model="sommerfeld",
+                junctions=[[(0, "start"), (1, "start"), (2, "start"), (3, "start"), (4, "start")]],
+                feeds=[(0, 0.05, 1.0)])
+
+
 def _star():
     return [
         np.array([[0.0, 0.0, 0.0], [0.0, 0.0, 5.0]]),
@@ -96,7 +123,24 @@ CASES = {
         wires=[np.array([[0.0, 0.0, -HD], [0.0, 0.0, HD]]), np.array([[3.0, 0.0, -HD], [3.0, 0.0, HD]])],
         nsegs=20, degree=1, feeds=[(0, None, 1.0), (1, None, 1.0 + 0.5j)]),
     "array4x4": lambda: dipole_array(4, 4),
+    # Sommerfeld ground (ground_model="sommerfeld"): remainder grid + C2 image
+    "d2_somm_dipole": lambda: somm_dipole(0.1, (10.0, 0.002), degree=2, nseg=21),
+    "d1_somm_dipole_low": lambda: somm_dipole(0.03, (13.0, 0.005), degree=1, nseg=20),
+    "d2_somm_sea": lambda: somm_dipole(0.05, (81.0, 4.0), degree=2, nseg=15),
+    "d2_somm_radials": lambda: somm_ground_plane(),
+    "d2_somm_contact": lambda: dict(
+        wires=[np.array([[0, 0, 0.0], [0, 0, 0.24 * LAM_SOMM]])], nsegs=12, degree=2, wavelength=LAM_SOMM,
+        wire_radius=1e-3, ground_z=0.0, ground_eps=(15.0, 0.01), ground_model="sommerfeld", feeds=[(0, 0.2, 1.0)]),
+    "d2_somm_far_pair": lambda: dict(
+        wires=[np.array([[0, -0.24 * LAM_SOMM, 0.1 * LAM_SOMM], [0, 0.24 * LAM_SOMM, 0.1 * LAM_SOMM]]),
+               np.array([[4.5 * LAM_SOMM, -0.24 * LAM_SOMM, 0.1 * LAM_SOMM],
+                         [4.5 * LAM_SOMM, 0.24 * LAM_SOMM, 0.1 * LAM_SOMM]])],
+        nsegs=11, degree=2, wavelength=LAM_SOMM, wire_radius=1e-3, ground_z=0.0, ground_eps=(10.0, 0.002),
+        ground_model="sommerfeld", feeds=[(0, None, 1.0), (1, None, 1.0)]),
 }
+
+# Sommerfeld-ground cases whose fixtures also carry the grid master tables.
+SOMMERFELD = {name for name in CASES if "_somm_" in name}
 
 # Cases stored as Y plus a seeded sample of Z entries (full Z would be large).
 SAMPLED = {"array4x4", "array16x16"}

@@ -30,7 +30,7 @@ HERE = Path(__file__).resolve().parent
 REPO = HERE.parent.parent
 sys.path.insert(0, str(HERE))
 
-from cases import BIG_CASES, CASES, SAMPLED  # noqa: E402
+from cases import BIG_CASES, CASES, SAMPLED, SOMMERFELD  # noqa: E402
 
 
 def import_reference(ref_root: Path):
@@ -48,7 +48,24 @@ def import_reference(ref_root: Path):
     return momwire
 
 
-def solve_case(momwire, kw, sample_seed=None):
+def somm_master(momwire, s, geom):
+    """The wavelength-normalised grid master the reference's solve used,
+    as region tables vals_<i> (4, n_r, n_th) plus its key."""
+    from momwire import _ground_refl, _sommerfeld
+
+    eps_t = _ground_refl.eps_tilde(s.ground_eps, s.omega, s.eps)
+    r1 = _sommerfeld.max_image_distance(geom["seg_l"], geom["seg_r"], s.ground_z)
+    lam = 2.0 * np.pi / s.k
+    r1b = _sommerfeld._somm_r1_bucket_wl(min(r1 / lam, _sommerfeld._SOMM_R1_CAP_LAMBDA))
+    eb = _sommerfeld._somm_eps_bucket(complex(eps_t))
+    master = _sommerfeld._NORM_CACHE[(eb, r1b)]
+    out = {"somm_eps_b": np.complex128(eb), "somm_r1b_wl": np.float64(r1b), "somm_n_region": len(master._regions)}
+    for i, reg in enumerate(master._regions):
+        out[f"somm_vals_{i}"] = reg["vals"]
+    return out
+
+
+def solve_case(momwire, kw, sample_seed=None, somm=False):
     s = momwire.BSplineSolver(**kw)
     geom = s._build_geometry()
     supp, polys, kcl, wk, wbg = s._build_basis_polynomials(geom)
@@ -59,6 +76,8 @@ def solve_case(momwire, kw, sample_seed=None):
     sol = s.compute_port_solution()
     t_all = time.perf_counter() - t0
     out = {"y": sol.y, "t_fill": t_fill, "t_solve_total": t_all}
+    if somm:
+        out.update(somm_master(momwire, s, geom))
     n = Z.shape[0]
     if sample_seed is None:
         out["Z"] = Z
@@ -94,7 +113,7 @@ def main():
     for name, kw in todo.items():
         if args.only and name != args.only:
             continue
-        out = solve_case(momwire, kw(), sample_seed=1234 if name in SAMPLED else None)
+        out = solve_case(momwire, kw(), sample_seed=1234 if name in SAMPLED else None, somm=name in SOMMERFELD)
         np.savez_compressed(HERE / f"{name}.npz", **out)
         print(f"{name}: y[0,0]={out['y'][0, 0]:.12g} fill={out['t_fill']:.3f}s", flush=True)
 

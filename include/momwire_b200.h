@@ -400,6 +400,12 @@ mw_status mw_somm_surfaces(int64_t n_nodes, const double* r1, const double* rho,
                            double eps_im, double k2, double omega, double mu,
                            double rtol, double* out, void* workspace, void* stream);
 
+/* As mw_somm_surfaces with a permittivity per node (device arrays). */
+mw_status mw_somm_surfaces_eps(int64_t n_nodes, const double* r1, const double* rho,
+                               const double* h, const double* theta, const double* eps_re,
+                               const double* eps_im, double k2, double omega, double mu,
+                               double rtol, double* out, void* workspace, void* stream);
+
 /*
  * out[m * n_src + n] = t_obs[m] . F(obs[m], src[n]) . t_src[n] (complex128)
  * for points (n, 3) and unit tangents (n, 3) on the device: the projected
@@ -429,6 +435,37 @@ mw_status mw_somm_remainder_q(const mw_segments* seg, const mw_basis* basis,
  */
 mw_status mw_max_image_distance(int32_t n_seg, const double* seg_l, const double* seg_r,
                                 double ground_z, double* out, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Learned Sommerfeld surrogate (no reference counterpart: the reference
+ * tabulates the remainder surfaces by quadrature, _sommerfeld.py:648-813)
+ *
+ * A 5 -> 128 -> 128 -> 128 -> 128 -> 8 MLP with GELU.  Parameters are one
+ * flat FP32 vector of mw_mlp_param_count() entries, layer by layer
+ * [W_l (out x in, row-major), b_l]; the forward pass uses a BF16 copy of it
+ * (mw_mlp_to_bf16) with FP32 accumulation.  Inputs are 5 normalised
+ * features per row, outputs 8 (Re/Im of the four surfaces, scaled).
+ * ------------------------------------------------------------------------ */
+int32_t mw_mlp_param_count(void);
+size_t mw_mlp_train_workspace_size(int32_t batch);
+mw_status mw_mlp_to_bf16(const float* params, void* params_bf16, void* stream);
+/* FP32 forward of the training numerics: Y (n x 8) from X (n x 5). */
+mw_status mw_mlp_forward(int32_t n, const float* X, const void* params_bf16, const float* params,
+                         float* Y, void* workspace, size_t workspace_bytes, void* stream);
+/* Gradient of the mean squared error against T (n x 8), and the loss. */
+mw_status mw_mlp_grad(int32_t n, const float* X, const float* T, const void* params_bf16,
+                      const float* params, float* grad, float* loss, void* workspace,
+                      size_t workspace_bytes, void* stream);
+/* One Adam step (bias-corrected, step >= 1) on a batch; *loss += batch loss.
+ * rows != NULL: the batch is rows X[rows[i]], T[rows[i]] of a larger set. */
+mw_status mw_mlp_train_step(int32_t n, const float* X, const float* T, const int64_t* rows, float* params,
+                            void* params_bf16, float* adam_m, float* adam_v, int32_t step,
+                            float lr, float beta1, float beta2, float eps, float* loss,
+                            void* workspace, size_t workspace_bytes, void* stream);
+/* Tensor-core (tcgen05, BF16 weights, hi/lo BF16 activations) inference;
+ * *err (device) is set non-zero if a bounded wait timed out. */
+mw_status mw_mlp_infer(int64_t n, const float* X, const void* params_bf16, const float* params,
+                       float* Y, int32_t* err, void* stream);
 
 #ifdef __cplusplus
 }

@@ -140,10 +140,19 @@ _SIGS = {
     "mw_zgemm": (i32, [i32, i32, i64, i64, i64, f64, f64, vp, i64, vp, i64, f64, f64, vp, i64, vp]),
     "mw_somm_surfaces_workspace_size": (sz, []),
     "mw_somm_surfaces": (i32, [i64, vp, vp, vp, vp, f64, f64, f64, f64, f64, f64, vp, vp, vp]),
+    "mw_somm_surfaces_eps": (i32, [i64, vp, vp, vp, vp, vp, vp, f64, f64, f64, f64, vp, vp, vp]),
     "mw_somm_field_proj": (i32, [i64, vp, vp, i64, vp, vp, f64, f64, C.POINTER(SommGrid), vp, vp]),
     "mw_somm_remainder_q": (i32, [C.POINTER(Segments), C.POINTER(BasisT), C.POINTER(SommGrid), i32, f64, f64, vp,
                                   i64, vp, i64, vp]),
     "mw_max_image_distance": (i32, [i32, vp, vp, f64, vp, vp]),
+    "mw_mlp_param_count": (i32, []),
+    "mw_mlp_train_workspace_size": (sz, [i32]),
+    "mw_mlp_to_bf16": (i32, [vp, vp, vp]),
+    "mw_mlp_forward": (i32, [i32, vp, vp, vp, vp, vp, sz, vp]),
+    "mw_mlp_grad": (i32, [i32, vp, vp, vp, vp, vp, vp, vp, sz, vp]),
+    "mw_mlp_train_step": (i32, [i32, vp, vp, vp, vp, vp, vp, vp, i32, C.c_float, C.c_float, C.c_float, C.c_float,
+                                vp, vp, sz, vp]),
+    "mw_mlp_infer": (i32, [i64, vp, vp, vp, vp, vp, vp]),
 }
 
 EXPORTED = tuple(_SIGS)

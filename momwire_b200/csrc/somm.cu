@@ -60,6 +60,7 @@ struct WarpRule {
 struct SurfArgs {
     int64_t n;
     const double *r1, *rho, *h, *theta;
+    const double *eps_re, *eps_im;  // per-node eps~, or NULL: eps_t for all
     cd eps_t;
     double k2, omega, mu, rtol;
     double2* out;  // (n, 4) complex
@@ -77,8 +78,8 @@ __global__ void __launch_bounds__(128) somm_surfaces_kernel(SurfArgs A, GL24 gl)
         node = __shfl_sync(0xffffffffu, node, 0);
         if (node >= (unsigned long long)A.n) break;
         cd s[4];
-        somm::surfaces(rule, A.eps_t, A.k2, A.omega, A.mu, A.r1[node], A.rho[node], A.h[node], A.theta[node], A.rtol,
-                       s);
+        const cd et = A.eps_re ? cd{A.eps_re[node], A.eps_im[node]} : A.eps_t;
+        somm::surfaces(rule, et, A.k2, A.omega, A.mu, A.r1[node], A.rho[node], A.h[node], A.theta[node], A.rtol, s);
         if (lane < 4) A.out[node * 4 + lane] = make_double2(s[lane].re, s[lane].im);
     }
 }
@@ -443,15 +444,16 @@ using namespace mw;
 
 extern "C" size_t mw_somm_surfaces_workspace_size(void) { return 256; }
 
-extern "C" mw_status mw_somm_surfaces(int64_t n_nodes, const double* r1, const double* rho, const double* h,
-                                      const double* theta, double eps_re, double eps_im, double k2, double omega,
-                                      double mu, double rtol, double* out, void* workspace, void* stream) {
+static mw_status launch_surfaces(int64_t n_nodes, const double* r1, const double* rho, const double* h,
+                                 const double* theta, const double* eps_re_v, const double* eps_im_v, double eps_re,
+                                 double eps_im, double k2, double omega, double mu, double rtol, double* out,
+                                 void* workspace, void* stream) {
     MW_REQUIRE(n_nodes >= 0, "n_nodes must be >= 0");
     if (n_nodes == 0) return MW_OK;
     MW_REQUIRE(r1 && rho && h && theta && out && workspace, "NULL argument");
     MW_REQUIRE(k2 > 0.0 && rtol > 0.0, "k2 and rtol must be positive");
     cudaStream_t st = as_stream(stream);
-    SurfArgs A{n_nodes, r1, rho, h, theta, cd{eps_re, eps_im}, k2, omega, mu, rtol,
+    SurfArgs A{n_nodes, r1, rho, h, theta, eps_re_v, eps_im_v, cd{eps_re, eps_im}, k2, omega, mu, rtol,
                reinterpret_cast<double2*>(out), reinterpret_cast<unsigned long long*>(workspace)};
     MW_CHECK_CUDA(cudaMemsetAsync(workspace, 0, sizeof(unsigned long long), st));
     int dev = 0, sms = 148;
@@ -465,6 +467,22 @@ extern "C" mw_status mw_somm_surfaces(int64_t n_nodes, const double* r1, const d
     MW_CHECK_CUDA(cudaGetLastError());
     count_launch();
     return MW_OK;
+}
+
+extern "C" mw_status mw_somm_surfaces(int64_t n_nodes, const double* r1, const double* rho, const double* h,
+                                      const double* theta, double eps_re, double eps_im, double k2, double omega,
+                                      double mu, double rtol, double* out, void* workspace, void* stream) {
+    return launch_surfaces(n_nodes, r1, rho, h, theta, nullptr, nullptr, eps_re, eps_im, k2, omega, mu, rtol, out,
+                           workspace, stream);
+}
+
+extern "C" mw_status mw_somm_surfaces_eps(int64_t n_nodes, const double* r1, const double* rho, const double* h,
+                                          const double* theta, const double* eps_re, const double* eps_im, double k2,
+                                          double omega, double mu, double rtol, double* out, void* workspace,
+                                          void* stream) {
+    MW_REQUIRE(eps_re && eps_im, "NULL eps arrays");
+    return launch_surfaces(n_nodes, r1, rho, h, theta, eps_re, eps_im, 0.0, 0.0, k2, omega, mu, rtol, out, workspace,
+                           stream);
 }
 
 extern "C" mw_status mw_somm_field_proj(int64_t n_obs, const double* obs, const double* t_obs, int64_t n_src,

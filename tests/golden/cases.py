@@ -139,12 +139,51 @@ CASES = {
         ground_model="sommerfeld", feeds=[(0, None, 1.0), (1, None, 1.0)]),
 }
 
+CASES["d2_somm_plate8"] = lambda: wire_grid_plate(n_cells=8, size=10.0, n_jports=3)
+
 # Sommerfeld-ground cases whose fixtures also carry the grid master tables.
 SOMMERFELD = {name for name in CASES if "_somm_" in name}
 
 # Cases stored as Y plus a seeded sample of Z entries (full Z would be large).
-SAMPLED = {"array4x4", "array16x16"}
+SAMPLED = {"array4x4", "array16x16", "plate64_somm"}
+
+def wire_grid_plate(n_cells=64, size=10.0, z=2.0, mono_len=10.0, mono_segs=10, n_jports=7, seed=0,
+                    ground=(13.0, 5e-3), f=14.1e6):
+    """(n_cells+1)^2-node square wire grid (2 segments per cell edge, radius
+    1 mm) at height z over a Sommerfeld ground, a vertical monopole from the
+    centre node fed at its base segment, and n_jports seeded junction ports
+    at grid nodes other than the centre."""
+    m = n_cells + 1
+    step = size / n_cells
+    xy = lambda i, j: (-size / 2 + i * step, -size / 2 + j * step, z)  # noqa: E731
+    wires, nodes = [], {}
+    for j in range(m):
+        for i in range(n_cells):  # x-directed wire (i, j) -> (i + 1, j)
+            wires.append(np.array([xy(i, j), xy(i + 1, j)]))
+            nodes.setdefault((i, j), []).append((len(wires) - 1, "start"))
+            nodes.setdefault((i + 1, j), []).append((len(wires) - 1, "end"))
+    for i in range(m):
+        for j in range(n_cells):  # y-directed wire (i, j) -> (i, j + 1)
+            wires.append(np.array([xy(i, j), xy(i, j + 1)]))
+            nodes.setdefault((i, j), []).append((len(wires) - 1, "start"))
+            nodes.setdefault((i, j + 1), []).append((len(wires) - 1, "end"))
+    c = (n_cells // 2, n_cells // 2)
+    cx, cy, _ = xy(*c)
+    wires.append(np.array([(cx, cy, z), (cx, cy, z + mono_len)]))
+    mono = len(wires) - 1
+    nodes[c].append((mono, "start"))
+    keys = sorted(nodes)
+    junctions = [nodes[k] for k in keys]
+    rng = np.random.default_rng(seed)
+    cand = [i for i, k in enumerate(keys) if k != c]
+    jports = sorted(int(x) for x in rng.choice(cand, size=n_jports, replace=False))
+    npe = [2] * (len(wires) - 1) + [mono_segs]
+    return dict(wires=wires, n_per_edge_per_wire=npe, degree=2, wire_radius=1e-3, wavelength=C_LIGHT / f,
+                junctions=junctions, junction_ports=jports, feeds=[(mono, 0.5 * mono_len / mono_segs, 1.0)],
+                ground_z=0.0, ground_eps=ground, ground_model="sommerfeld")
+
 
 BIG_CASES = {
     "array16x16": lambda: dipole_array(16, 16),
+    "plate64_somm": lambda: wire_grid_plate(),
 }

@@ -72,28 +72,31 @@ def solve_case(momwire, kw, sample_seed=None, somm=False):
     t0 = time.perf_counter()
     Z = s._compute_Z_operator(geom, supp, polys)
     t_fill = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    sol = s.compute_port_solution()
-    t_all = time.perf_counter() - t0
-    out = {"y": sol.y, "t_fill": t_fill, "t_solve_total": t_all}
-    if somm:
-        out.update(somm_master(momwire, s, geom))
     n = Z.shape[0]
-    if sample_seed is None:
-        out["Z"] = Z
-        out["coeffs"] = sol.coeffs
-        cur = s.currents_at_knots(sol.coeffs[:, 0])
-        out["currents0"] = np.concatenate(cur)
-    else:
+    samples = None
+    if sample_seed is not None:
+        # big cases: keep a seeded sample of Z and free it before the solve
         rng = np.random.default_rng(sample_seed)
         ii = rng.integers(0, n, 4096)
         jj = rng.integers(0, n, 4096)
         d = np.arange(min(n, 512))
         ii = np.concatenate([ii, d, d[1:], d[:-1]])
         jj = np.concatenate([jj, d, d[:-1], d[1:]])
-        out["z_i"] = ii
-        out["z_j"] = jj
-        out["z_v"] = Z[ii, jj]
+        samples = (ii, jj, Z[ii, jj].copy())
+        del Z
+    t0 = time.perf_counter()
+    sol = s.compute_port_solution()
+    t_all = time.perf_counter() - t0
+    out = {"y": sol.y, "t_fill": t_fill, "t_solve_total": t_all}
+    if somm:
+        out.update(somm_master(momwire, s, geom))
+    if sample_seed is None:
+        out["Z"] = Z
+        out["coeffs"] = sol.coeffs
+        cur = s.currents_at_knots(sol.coeffs[:, 0])
+        out["currents0"] = np.concatenate(cur)
+    else:
+        out["z_i"], out["z_j"], out["z_v"] = samples
         out["coeff_colsum"] = sol.coeffs.sum(axis=0)
         out["coeff_colnorm"] = np.linalg.norm(sol.coeffs, axis=0)
         out["coeffs_first_rows"] = sol.coeffs[:64]

@@ -467,6 +467,20 @@ mw_status mw_mlp_train_step(int32_t n, const float* X, const float* T, const int
 mw_status mw_mlp_infer(int64_t n, const float* X, const void* params_bf16, const float* params,
                        float* Y, int32_t* err, void* stream);
 
+/*
+ * Z -= Q with the four surfaces predicted by the surrogate instead of
+ * interpolated from a grid (mw_somm_remainder_q's contract otherwise).
+ * struct_features: the three per-structure inputs (normalised log|eps~|,
+ * arg eps~, log f); value_scale: output scale x (omega mu)/(omega0 mu0).
+ * Every node pair must lie in the surrogate's domain (the caller checks).
+ */
+mw_status mw_somm_remainder_q_mlp(const mw_segments* seg, const mw_basis* basis,
+                                  const void* params_bf16, const float* params,
+                                  const float* struct_features, double wavelength,
+                                  double value_scale, int32_t n_qp, double ground_z, double k,
+                                  double* Z, int64_t ldz, float* Z32, int64_t ldz32,
+                                  int32_t* err, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -153,6 +153,8 @@ _SIGS = {
     "mw_mlp_train_step": (i32, [i32, vp, vp, vp, vp, vp, vp, vp, i32, C.c_float, C.c_float, C.c_float, C.c_float,
                                 vp, vp, sz, vp]),
     "mw_mlp_infer": (i32, [i64, vp, vp, vp, vp, vp, vp]),
+    "mw_somm_remainder_q_mlp": (i32, [C.POINTER(Segments), C.POINTER(BasisT), vp, vp, vp, f64, f64, i32, f64, f64, vp,
+                                      i64, vp, i64, vp, vp]),
 }
 
 EXPORTED = tuple(_SIGS)

@@ -11,6 +11,12 @@ device buffers.  The fill and the factorisation run on the GPU:
   the plain drop-in, matching the reference to ~1e-10;
 * ``precision="mixed"``: complex64 factorisation on the tensor cores with
   FP64 iterative refinement against the FP64 fill.
+
+For ``ground_model="sommerfeld"`` the remainder surfaces come from the
+reference's quadrature grid (``sommerfeld_method="grid"``, the default and
+the drop-in) or from the learned surrogate (``"surrogate"``), which falls
+back to the grid outside its domain or when a quadrature spot check of the
+structure misses ``SURROGATE_BOUND``.
 """
 
 from __future__ import annotations
@@ -24,6 +30,7 @@ import numpy as np
 from . import _lib
 from . import _tables as T
 from . import sommerfeld as somm
+from . import surrogate as sur
 from ._port_solution import PortSolution
 
 
@@ -196,6 +203,7 @@ class BSplineSolver:
         cancel=None,
         precision="fp64",
         device=None,
+        sommerfeld_method="grid",
     ):
         self._cancel = cancel
         if degree < 1:
@@ -214,6 +222,10 @@ class BSplineSolver:
         if precision not in ("fp64", "mixed"):
             raise ValueError(f"precision must be 'fp64' or 'mixed', got {precision!r}")
         self.precision = precision
+        if sommerfeld_method not in ("grid", "surrogate"):
+            raise ValueError(f"sommerfeld_method must be 'grid' or 'surrogate', got {sommerfeld_method!r}")
+        self.sommerfeld_method = sommerfeld_method
+        self.last_sommerfeld = None
         # mixed: stop refining once the largest relative correction of any
         # port column is below this (the remaining error is then ~ kappa *
         # 6e-8 times smaller still)
@@ -723,9 +735,58 @@ class BSplineSolver:
             _lib.call("mw_fill_z_image", C.byref(dt.seg), C.byref(dt.basis), C.byref(g), C.byref(fr),
                       self.n_qp_pair, Z.data_ptr(), n, z32, n, stream)
         if self._is_sommerfeld():
-            grid = self._somm_grid(stream)
-            _lib.call("mw_somm_remainder_q", C.byref(dt.seg), C.byref(dt.basis), C.byref(grid),
-                      self.n_qp_sommerfeld, float(self.ground_z), float(self.k), Z.data_ptr(), n, z32, n, stream)
+            use, info = self._surrogate_check(stream) if self.sommerfeld_method == "surrogate" else (None, {})
+            if use is not None:
+                feats = np.ascontiguousarray(info.pop("struct_features"), dtype=np.float32)
+                vscale = sur.SCALE * (self.omega * self.mu) / (sur.OMEGA_REF * sur.MU0_GRID)
+                _lib.call("mw_somm_remainder_q_mlp", C.byref(dt.seg), C.byref(dt.basis), use.pbf.data_ptr(),
+                          use.p32.data_ptr(), feats.ctypes.data, float(self.wavelength), float(vscale),
+                          self.n_qp_sommerfeld, float(self.ground_z), float(self.k), Z.data_ptr(), n, z32, n,
+                          use.err.data_ptr(), stream)
+                self.last_sommerfeld = dict(info, method="surrogate")
+            else:
+                grid = self._somm_grid(stream)
+                _lib.call("mw_somm_remainder_q", C.byref(dt.seg), C.byref(dt.basis), C.byref(grid),
+                          self.n_qp_sommerfeld, float(self.ground_z), float(self.k), Z.data_ptr(), n, z32, n, stream)
+                self.last_sommerfeld = dict(info, method="grid")
+
+    def _surrogate_check(self, stream):
+        """(model, info) when the surrogate may serve this structure at this
+        k, else (None, info with the reason): the weights must exist, eps~
+        and f and every Gauss-node pair must lie in the training domain, and
+        the largest error of a quadrature spot check on sampled node pairs
+        must be within SURROGATE_BOUND (of the surfaces' scale)."""
+        model = sur.get_model(self._torch_device())
+        if model is None:
+            return None, {"reason": "no surrogate weights"}
+        et = complex(T.eps_tilde(self.ground_eps, self.omega, self.eps))
+        f = self.omega / (2.0 * np.pi)
+        lam = self.wavelength
+        geom = self._geometry()
+        q = self.n_qp_sommerfeld
+        tq = 0.5 * (np.polynomial.legendre.leggauss(q)[0] + 1.0)
+        nodes = (geom.seg_l[:, None, :] + tq[None, :, None] * (geom.seg_r - geom.seg_l)[:, None, :]).reshape(-1, 3)
+        zmin = float(nodes[:, 2].min()) - self.ground_z
+        r1_max = float(somm.max_image_distance(self._dev_tables().seg.seg_l, self._dev_tables().seg.seg_r,
+                                               self._dev_tables().seg.n_seg, self.ground_z, self._torch_device(),
+                                               stream)) / 1.001
+        ok = sur.in_domain(np.array([0.0, 0.0]), np.array([2.0 * zmin / lam, sur.H_MIN_WL]), np.array([et, et]),
+                           np.array([f, f]))
+        if not (ok.all() and r1_max / lam <= sur.R1_MAX_WL):
+            return None, {"reason": "outside the surrogate domain"}
+        rng = np.random.default_rng(1234)
+        a = rng.integers(0, nodes.shape[0], sur.SPOT_PAIRS)
+        b = rng.integers(0, nodes.shape[0], sur.SPOT_PAIRS)
+        d = nodes[a] - nodes[b]
+        rho = np.hypot(d[:, 0], d[:, 1]) / lam
+        h = ((nodes[a, 2] - self.ground_z) + (nodes[b, 2] - self.ground_z)) / lam
+        err = float(sur.spot_check(model, rho, h, et, f))
+        info = {"spot_max_err": err, "struct_features": sur.features(0.0, 1.0, et, f)[2:5]}
+        if not err <= sur.SURROGATE_BOUND:
+            info.pop("struct_features")
+            info["reason"] = "spot check over the bound"
+            return None, info
+        return model, info
 
     def _is_sommerfeld(self):
         return self.ground_z is not None and self.ground_eps is not None and self.ground_model == "sommerfeld"

@@ -30,6 +30,7 @@
 #include <cstdint>
 
 #include "common.cuh"
+#include "somm_proj.cuh"
 #include "tc_common.cuh"
 
 namespace mw {
@@ -455,6 +456,182 @@ __global__ void __launch_bounds__(MI_THREADS, 1) mlp_infer_tc_kernel(int64_t n, 
     mlp_tc_end(c);
 }
 
+// ------------------------------------------- surrogate remainder block Q
+// Q[m, n] = sum over node pairs f_m(q) F(q, r) f_n(r), F the projected
+// remainder field with the four surfaces predicted by the MLP.  Persistent
+// CTAs walk the (row tile, column tile) pairs of the fill's basis tiling;
+// per tile pair the node pairs go through the tensor-core MLP 128 at a time,
+// and each thread adds its pair's field, weighted by the basis values at the
+// two nodes, into a shared 16 x 16 tile of Q.
+constexpr int SQ_MAX_NQ = 8;
+constexpr int SQ_MAX_NODES = MW_MAX_TILE_SEG * SQ_MAX_NQ;  // 192
+
+struct SqArgs {
+    mw_segments seg;
+    mw_basis basis;
+    const __nv_bfloat16* pb;
+    const float* pf;
+    float fe2, fe3, fe4;      // per-structure features (|eps|, arg eps, f)
+    double inv_lambda;        // 1 / wavelength
+    double vscale;            // SCALE (omega mu) / (omega0 mu0)
+    double tiny;              // rho below which the azimuth degenerates
+    double gz, k;
+    int nq;
+    double tq[SQ_MAX_NQ], wq[SQ_MAX_NQ];
+    double* Z;
+    int64_t ldz;
+    float* Z32;
+    int64_t ldz32;
+    int* err;
+};
+
+struct SqNode {
+    double x, y, z;
+    double f[3];  // basis values x Gauss weight at this node, per wing slot
+    int m[3];     // local basis index of each slot (-1: none)
+};
+
+template <int D>
+__device__ void sq_stage_nodes(const SqArgs& A, int tile, int ns, SqNode* nodes, double* tang) {
+    constexpr int NM = D + 1;
+    const int nq = A.nq;
+    const int SMAX = A.basis.max_tile_seg, TB = A.basis.max_tile_basis;
+    const int nb = A.basis.tile_nb[tile], fb = A.basis.tile_first[tile];
+    for (int q = threadIdx.x; q < ns * nq; q += blockDim.x) {
+        const int li = q / nq, iq = q - li * nq;
+        const int s = A.basis.tile_seg[(size_t)tile * SMAX + li];
+        const double* l = A.seg.seg_l + 3 * s;
+        const double* r = A.seg.seg_r + 3 * s;
+        const double dx = r[0] - l[0], dy = r[1] - l[1], dz = r[2] - l[2];
+        const double L = sqrt(dx * dx + dy * dy + dz * dz);
+        const double t = A.tq[iq];
+        SqNode nd;
+        nd.x = l[0] + t * dx;
+        nd.y = l[1] + t * dy;
+        nd.z = l[2] + t * dz;
+        double wpow[NM];
+        double wp = L * A.wq[iq];
+        const double u = L * t;
+        for (int p = 0; p < NM; ++p) {
+            wpow[p] = wp;
+            wp *= u;
+        }
+        int slot = 0;
+        for (int i = 0; i < 3; ++i) {
+            nd.m[i] = -1;
+            nd.f[i] = 0.0;
+        }
+        for (int mi = 0; mi < nb && slot < 3; ++mi)
+            for (int a = 0; a < NM; ++a)
+                if (A.basis.loc[(size_t)(fb + mi) * NM + a] == li && slot < 3) {
+                    const double* C = A.basis.polys + ((size_t)(fb + mi) * NM + a) * NM;
+                    double v = 0.0;
+                    for (int p = 0; p < NM; ++p) v += C[p] * wpow[p];
+                    nd.m[slot] = mi;
+                    nd.f[slot] = v;
+                    ++slot;
+                }
+        nodes[q] = nd;
+    }
+    for (int i = threadIdx.x; i < ns; i += blockDim.x) {
+        const int s = A.basis.tile_seg[(size_t)tile * SMAX + i];
+        for (int c = 0; c < 3; ++c) tang[3 * i + c] = A.seg.tangent[3 * s + c];
+    }
+    (void)TB;
+}
+
+template <int D>
+__global__ void __launch_bounds__(MI_THREADS, 1) somm_q_mlp_kernel(SqArgs A) {
+    extern __shared__ __align__(1024) uint8_t sq_smem[];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ uint32_t tmem_slot;
+    SqNode* nodes_r = reinterpret_cast<SqNode*>(sq_smem + MI_SMEM);
+    SqNode* nodes_c = nodes_r + SQ_MAX_NODES;
+    double* tang_r = reinterpret_cast<double*>(nodes_c + SQ_MAX_NODES);
+    double* tang_c = tang_r + 3 * MW_MAX_TILE_SEG;
+    double* Qs = tang_c + 3 * MW_MAX_TILE_SEG;  // MW_MAX_TILE_BASIS^2 complex
+    mlp_tc_stage(sq_smem, A.pb, A.pf);
+    MlpTc c;
+    mlp_tc_begin(c, sq_smem, &bar, &tmem_slot);
+    const int nt = A.basis.n_tile;
+    const int TB = A.basis.max_tile_basis;
+    const int nq = A.nq;
+    bool alive = true;
+    for (int64_t tp = blockIdx.x; tp < (int64_t)nt * nt && alive; tp += gridDim.x) {
+        const int tr = (int)(tp / nt), tc = (int)(tp - (int64_t)tr * nt);
+        const int ns_r = A.basis.tile_ns[tr], ns_c = A.basis.tile_ns[tc];
+        __syncthreads();  // previous tile's readers are done with the staging
+        sq_stage_nodes<D>(A, tr, ns_r, nodes_r, tang_r);
+        sq_stage_nodes<D>(A, tc, ns_c, nodes_c, tang_c);
+        for (int i = threadIdx.x; i < TB * TB * 2; i += blockDim.x) Qs[i] = 0.0;
+        __syncthreads();
+        const int nr = ns_r * nq, ncn = ns_c * nq;
+        const int npair = nr * ncn;
+        for (int p0 = 0; p0 < npair; p0 += MI_ROWS) {
+            const int p = p0 + threadIdx.x;
+            const bool valid = p < npair;
+            const int ir = valid ? p / ncn : 0, ic = valid ? p - ir * ncn : 0;
+            const SqNode& o = nodes_r[ir];
+            const SqNode& sn = nodes_c[ic];
+            const PairGeom g = pair_geom(A.gz, o.x, o.y, o.z, sn.x, sn.y, sn.z);
+            float x[MLP_IN], y[MLP_OUT];
+            const double r1w = fmin(g.r1 * A.inv_lambda, 4.0);
+            x[0] = (float)(2.0 * sqrt(r1w / 4.0) - 1.0);
+            x[1] = (float)(4.0 * g.theta / kPi - 1.0);
+            x[2] = A.fe2;
+            x[3] = A.fe3;
+            x[4] = A.fe4;
+            if (!mlp_tc_tile(c, x, y, A.err)) {
+                alive = false;
+                break;
+            }
+            if (valid) {
+                cd surf[4];
+#pragma unroll
+                for (int s = 0; s < 4; ++s) surf[s] = cd{(double)y[2 * s], (double)y[2 * s + 1]};
+                const int li = ir / nq, lj = ic / nq;
+                const double* to = tang_r + 3 * li;
+                const double* tsv = tang_c + 3 * lj;
+                const SrcTangent ts = split_tangent(tsv[0], tsv[1], tsv[2]);
+                const cd F = project_surfaces(g, surf, A.k, A.vscale, A.tiny, to[0], to[1], to[2], ts);
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    const int mi = o.m[a];
+                    if (mi < 0) continue;
+#pragma unroll
+                    for (int b = 0; b < 3; ++b) {
+                        const int ni = sn.m[b];
+                        if (ni < 0) continue;
+                        const double w = o.f[a] * sn.f[b];
+                        atomicAdd(&Qs[2 * (mi * TB + ni)], w * F.re);
+                        atomicAdd(&Qs[2 * (mi * TB + ni) + 1], w * F.im);
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        const int nb_r = A.basis.tile_nb[tr], nb_c = A.basis.tile_nb[tc];
+        const int fb_r = A.basis.tile_first[tr], fb_c = A.basis.tile_first[tc];
+        for (int q = threadIdx.x; q < nb_r * nb_c; q += blockDim.x) {
+            const int mi = q % nb_r, ni = q / nb_r;
+            const int64_t m = fb_r + mi, n = fb_c + ni;
+            double* zp = A.Z + 2 * (m + n * A.ldz);
+            const double zr = zp[0] - Qs[2 * (mi * TB + ni)], zi = zp[1] - Qs[2 * (mi * TB + ni) + 1];
+            zp[0] = zr;
+            zp[1] = zi;
+            if (A.Z32) {
+                float* z32 = A.Z32 + 2 * (m + n * A.ldz32);
+                z32[0] = (float)zr;
+                z32[1] = (float)zi;
+            }
+        }
+    }
+    mlp_tc_end(c);
+}
+
+constexpr size_t SQ_SMEM = MI_SMEM + 2 * SQ_MAX_NODES * sizeof(SqNode) + 6 * MW_MAX_TILE_SEG * sizeof(double) +
+                           2 * MW_MAX_TILE_BASIS * MW_MAX_TILE_BASIS * sizeof(double);
+
 }  // namespace mw
 
 using namespace mw;
@@ -551,6 +728,64 @@ extern "C" mw_status mw_mlp_infer(int64_t n, const float* X, const void* params_
     const int grid = (int)(tiles < sms ? tiles : sms);
     mlp_infer_tc_kernel<<<grid, MI_THREADS, MI_SMEM, st>>>(n, X, reinterpret_cast<const __nv_bfloat16*>(params_bf16),
                                                            params, Y, err);
+    MW_CHECK_CUDA(cudaGetLastError());
+    count_launch();
+    return MW_OK;
+}
+
+extern "C" mw_status mw_somm_remainder_q_mlp(const mw_segments* seg, const mw_basis* basis, const void* params_bf16,
+                                             const float* params, const float* struct_features,
+                                             double wavelength, double value_scale, int32_t n_qp, double ground_z,
+                                             double k, double* Z, int64_t ldz, float* Z32, int64_t ldz32,
+                                             int32_t* err, void* stream) {
+    MW_REQUIRE(seg && basis && params_bf16 && params && struct_features && Z && err, "NULL argument");
+    MW_REQUIRE(basis->degree == 1 || basis->degree == 2, "degree must be 1 or 2");
+    MW_REQUIRE(n_qp >= 1 && n_qp <= SQ_MAX_NQ, "n_qp_sommerfeld must be in [1, %d]", SQ_MAX_NQ);
+    MW_REQUIRE(basis->max_tile_seg >= 1 && basis->max_tile_seg <= MW_MAX_TILE_SEG &&
+                   basis->max_tile_basis >= 1 && basis->max_tile_basis <= MW_MAX_TILE_BASIS && basis->n_tile >= 1,
+               "bad basis tiling");
+    MW_REQUIRE(wavelength > 0.0, "wavelength must be positive");
+    cudaStream_t st = as_stream(stream);
+    SqArgs A{};
+    A.seg = *seg;
+    A.basis = *basis;
+    A.pb = reinterpret_cast<const __nv_bfloat16*>(params_bf16);
+    A.pf = params;
+    A.fe2 = struct_features[0];
+    A.fe3 = struct_features[1];
+    A.fe4 = struct_features[2];
+    A.inv_lambda = 1.0 / wavelength;
+    A.vscale = value_scale;
+    A.tiny = 1e-12 * 4.0 * wavelength;  // the grid path's 1e-12 r1_max at a 4-wavelength grid
+    A.gz = ground_z;
+    A.k = k;
+    A.nq = n_qp;
+    const double *t, *w;
+    gauss_legendre01(n_qp, &t, &w);
+    for (int i = 0; i < n_qp; ++i) {
+        A.tq[i] = t[i];
+        A.wq[i] = w[i];
+    }
+    A.Z = Z;
+    A.ldz = ldz;
+    A.Z32 = Z32;
+    A.ldz32 = ldz32;
+    A.err = err;
+    int dev = 0, sms = 148;
+    MW_CHECK_CUDA(cudaGetDevice(&dev));
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int64_t pairs = (int64_t)basis->n_tile * basis->n_tile;
+    const int grid = (int)(pairs < sms ? pairs : sms);
+    ProfileScope ps(PC_SOMM_Q, st);
+    if (basis->degree == 1) {
+        MW_CHECK_CUDA(cudaFuncSetAttribute(somm_q_mlp_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)SQ_SMEM));
+        somm_q_mlp_kernel<1><<<grid, MI_THREADS, SQ_SMEM, st>>>(A);
+    } else {
+        MW_CHECK_CUDA(cudaFuncSetAttribute(somm_q_mlp_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)SQ_SMEM));
+        somm_q_mlp_kernel<2><<<grid, MI_THREADS, SQ_SMEM, st>>>(A);
+    }
     MW_CHECK_CUDA(cudaGetLastError());
     count_launch();
     return MW_OK;

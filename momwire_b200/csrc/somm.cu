@@ -25,6 +25,7 @@
 
 #include "common.cuh"
 #include "somm_math.cuh"
+#include "somm_proj.cuh"
 
 namespace mw {
 
@@ -93,104 +94,6 @@ static GL24 make_gl24() {
         g.w[i] = 2.0 * w[i];
     }
     return g;
-}
-
-// ------------------------------------------------------- field projection
-struct GridDev {
-    int n_region;
-    int n_r[6], n_th[6];
-    int64_t off[6];
-    double r0[6], dr[6], th0[6], dth[6];
-    double r1_max, r_break, th_split, r_near, tiny, vscale;
-    const double2* vals;  // (nodes, 4) complex
-};
-
-__device__ __forceinline__ void lagrange4(double u, double w[4]) {
-    const double u0 = u, u1 = u - 1.0, u2 = u - 2.0, u3 = u - 3.0;
-    w[0] = -u1 * u2 * u3 / 6.0;
-    w[1] = u0 * u2 * u3 / 2.0;
-    w[2] = -u0 * u1 * u3 / 2.0;
-    w[3] = u0 * u1 * u2 / 6.0;
-}
-
-// Source tangent split into horizontal unit (ux, uy), horizontal magnitude
-// and vertical part (_sommerfeld.py:985-990).
-struct SrcTangent {
-    double ux, uy, th, tz;
-};
-__host__ __device__ __forceinline__ SrcTangent split_tangent(double tx, double ty, double tz) {
-    SrcTangent s;
-    s.th = hypot(tx, ty);
-    const bool safe = s.th > 1e-12;
-    s.ux = safe ? tx / s.th : 1.0;
-    s.uy = safe ? ty / s.th : 0.0;
-    s.tz = tz;
-    return s;
-}
-
-// t_obs . F(obs, src) . t_src: 4x4 Lagrange interpolation of the four
-// surfaces at (R1, theta) of the image geometry, then eqs 143-147.
-__device__ __forceinline__ cd proj_one(const GridDev& G, double gz, double k, double ox, double oy, double oz,
-                                       double tox, double toy, double toz, double sx, double sy, double sz,
-                                       const SrcTangent& ts) {
-    const double dx = ox - sx, dy = oy - sy;
-    const double rho = hypot(dx, dy);
-    const double hh = (oz - gz) + (sz - gz);
-    const double r1 = sqrt(rho * rho + hh * hh);
-    double theta = atan2(hh, rho);
-    theta = fmin(fmax(theta, 0.0), 0.5 * kPi);
-    const double r1c = fmin(r1, G.r1_max);
-    const int reg = (r1c <= G.r_break) ? (theta <= G.th_split ? 0 : 1)
-                                       : (r1c <= G.r_near ? (theta <= G.th_split ? 2 : 3)
-                                                          : (theta <= G.th_split ? 4 : 5));
-    const double fr = (r1c - G.r0[reg]) / G.dr[reg];
-    const double ft = (theta - G.th0[reg]) / G.dth[reg];
-    int i0 = (int)floor(fr) - 1, j0 = (int)floor(ft) - 1;
-    i0 = min(max(i0, 0), G.n_r[reg] - 4);
-    j0 = min(max(j0, 0), G.n_th[reg] - 4);
-    double wr[4], wt[4];
-    lagrange4(fr - i0, wr);
-    lagrange4(ft - j0, wt);
-    const double2* V = G.vals + (G.off[reg] + (int64_t)i0 * G.n_th[reg] + j0) * 4;
-    cd surf[4];
-#pragma unroll
-    for (int s = 0; s < 4; ++s) surf[s] = cd{0.0, 0.0};
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        const double2* row = V + (int64_t)i * G.n_th[reg] * 4;
-        cd rs[4];
-#pragma unroll
-        for (int s = 0; s < 4; ++s) rs[s] = cd{0.0, 0.0};
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-#pragma unroll
-            for (int s = 0; s < 4; ++s) {
-                const double2 v = __ldg(row + j * 4 + s);
-                rs[s].re += v.x * wt[j];
-                rs[s].im += v.y * wt[j];
-            }
-        }
-#pragma unroll
-        for (int s = 0; s < 4; ++s) {
-            surf[s].re += rs[s].re * wr[i];
-            surf[s].im += rs[s].im * wr[i];
-        }
-    }
-    double sn, cs;
-    sincos(k * r1, &sn, &cs);
-    const double ir = G.vscale / r1;  // surfaces scaled to this frequency
-    const cd g{cs * ir, -sn * ir};
-    const bool safe_r = rho > G.tiny;
-    const double inv_rho = safe_r ? 1.0 / rho : 0.0;
-    const double dhx = safe_r ? dx * inv_rho : ts.ux;
-    const double dhy = safe_r ? dy * inv_rho : ts.uy;
-    const double cphi = ts.ux * dhx + ts.uy * dhy;
-    const double sphi = ts.ux * dhy - ts.uy * dhx;
-    const cd e_rho = g * cd{ts.tz * surf[0].re + ts.th * cphi * surf[2].re, ts.tz * surf[0].im + ts.th * cphi * surf[2].im};
-    const cd e_phi = g * cd{ts.th * sphi * surf[3].re, ts.th * sphi * surf[3].im};
-    const cd e_z = g * cd{ts.tz * surf[1].re - ts.th * cphi * surf[0].re, ts.tz * surf[1].im - ts.th * cphi * surf[0].im};
-    const double ax = tox * dhx + toy * dhy, ay = toy * dhx - tox * dhy;
-    return cd{ax * e_rho.re + ay * e_phi.re + toz * e_z.re, ax * e_rho.im + ay * e_phi.im + toz * e_z.im};
 }
 
 __global__ void field_proj_kernel(GridDev G, double gz, double k, int64_t n_obs, const double* __restrict__ obs,

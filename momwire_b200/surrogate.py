@@ -46,6 +46,14 @@ F_HZ = (2.5e6, 35e6)
 
 WEIGHTS_PATH = Path(__file__).resolve().parent / "data" / "somm_mlp.npz"
 
+# spot check: node pairs sampled per structure and the largest accepted
+# |surrogate - quadrature| / SCALE over them
+SPOT_PAIRS = 64
+SURROGATE_BOUND = 2e-2
+# drive-point impedance agreement with the quadrature-grid path that the
+# shipped weights are tested to (|dZin| / |Zin| on seeded structures)
+ZIN_TOL = 1e-2
+
 
 def _torch():
     import torch
@@ -262,3 +270,22 @@ def he_init(seed):
         parts.append((rng.standard_normal(i * n) * math.sqrt(2.0 / i)).astype(np.float32))
         parts.append(np.zeros(n, dtype=np.float32))
     return np.concatenate(parts)
+
+
+_MODELS: dict = {}
+
+
+def get_model(device):
+    """The shipped surrogate on `device` (loaded once), or None without
+    weights."""
+    key = getattr(device, "index", None)
+    if key not in _MODELS:
+        _MODELS[key] = Surrogate.load(device) if WEIGHTS_PATH.exists() else None
+    return _MODELS[key]
+
+
+def spot_check(model, rho_wl, h_wl, eps, f_hz):
+    """Largest |surrogate - quadrature| / SCALE over the given queries."""
+    q = quadrature_surfaces(rho_wl, h_wl, np.full(np.shape(rho_wl), eps), model.device)
+    p = model.surfaces(rho_wl, h_wl, eps, f_hz)
+    return float((p - q).abs().max()) / SCALE

@@ -46,20 +46,22 @@ __device__ bool grid_sync_bounded(PanelWs* ws, unsigned int target) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
-        __threadfence();
-        atomicAdd(&ws->counter, 1u);
+        // the release add publishes every write the CTA made before the
+        // __syncthreads above (cumulativity); the acquire loads order the
+        // reads that follow the barrier
+        asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(&ws->counter) : "memory");
         int ok = 1;
         long long spins = 0;
         while (ld_acquire(&ws->counter) < target) {
-            if (ws->err) { ok = 0; break; }
-            if (++spins > (1ll << 25)) {
-                atomicExch(&ws->err, MW_ERR_TIMEOUT);
-                ok = 0;
-                break;
+            if ((++spins & 255) == 0) {
+                if (*(volatile int*)&ws->err) { ok = 0; break; }
+                if (spins > (1ll << 26)) {
+                    atomicExch(&ws->err, MW_ERR_TIMEOUT);
+                    ok = 0;
+                    break;
+                }
             }
-            __nanosleep(20);
         }
-        __threadfence();
         s_ok = ok;
     }
     __syncthreads();
@@ -148,7 +150,6 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel(PanelArgs P) {
     __shared__ T s_cur[kNB];
     __shared__ int64_t s_p;
     __shared__ double s_pv;
-    __shared__ int s_bg;
 
     const int G = gridDim.x;
     const int g = blockIdx.x;
@@ -213,43 +214,38 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel(PanelArgs P) {
             if (tid == 0) {
                 s_p = bi;
                 s_pv = bv;
-                s_bg = bg;
                 if (g == 0) P.ipiv[c] = (int32_t)(bi + 1);
+            }
+            bg = __shfl_sync(0xffffffffu, bg, 0);
+            // the same warp fetches the pivot row and the current row (L2-
+            // coherent loads: other CTAs wrote them)
+            for (int x = tid; x < jb; x += 32) {
+                s_piv[x] = ldcg_c(slot_row + ((size_t)buf * G + bg) * kNB + x);
+                s_cur[x] = ldcg_c(cur_row + buf * kNB + x);
             }
         }
         __syncthreads();
         const int64_t p = s_p;
-        const int bg = s_bg;
-        for (int x = tid; x < jb; x += blockDim.x) {
-            // L2-coherent loads: these slots were written by other CTAs
-            s_piv[x] = ldcg_c(slot_row + ((size_t)buf * G + bg) * kNB + x);
-            s_cur[x] = ldcg_c(cur_row + buf * kNB + x);
-        }
-        __syncthreads();
-        // 5. swap rows c <-> p inside the slab
-        if (p != c) {
-            if (c >= r0 && c < r1)
-                for (int x = tid; x < jb; x += blockDim.x) slab[x * rcap + (int)(c - r0)] = s_piv[x];
-            if (p >= r0 && p < r1)
-                for (int x = tid; x < jb; x += blockDim.x) slab[x * rcap + (int)(p - r0)] = s_cur[x];
-        }
-        __syncthreads();
-        // 6. scale below the pivot, then rank-1 update of the panel
-        if (s_pv == 0.0) {
-            if (g == 0 && tid == 0 && P.info[0] == 0) P.info[0] = (int32_t)(c + 1);
-            continue;  // LAPACK: no scaling, no update for an exact zero pivot
-        }
-        const int is = (int)max((int64_t)0, c + 1 - r0);
-        const int nr = R - is;
-        if (nr > 0) {
-            const T inv = cdiv(cone<T>(), s_piv[jj]);
-            for (int i = is + tid; i < R; i += blockDim.x) slab[jj * rcap + i] = slab[jj * rcap + i] * inv;
-            __syncthreads();
-            const int ncol = jb - jj - 1;
-            for (int idx = tid; idx < nr * ncol; idx += blockDim.x) {
-                int i = is + idx % nr, x = jj + 1 + idx / nr;
-                slab[x * rcap + i] = slab[x * rcap + i] - slab[jj * rcap + i] * s_piv[x];
+        if (s_pv == 0.0 && g == 0 && tid == 0 && P.info[0] == 0) P.info[0] = (int32_t)(c + 1);
+        // 5-6. rows in the threads: the owners of rows c and p swap them;
+        // every row below c is scaled by the pivot and updated with the
+        // pivot row (LAPACK: an exact zero pivot is neither divided by nor
+        // applied)
+        const bool apply = s_pv != 0.0;
+        const T inv = apply ? cdiv(cone<T>(), s_piv[jj]) : cone<T>();
+        for (int i = i0 + tid; i < R; i += blockDim.x) {
+            const int64_t gr = r0 + i;
+            if (gr == c) {
+                if (p != c)
+                    for (int x = 0; x < jb; ++x) slab[x * rcap + i] = s_piv[x];
+                continue;
             }
+            if (gr == p && p != c)
+                for (int x = 0; x < jb; ++x) slab[x * rcap + i] = s_cur[x];
+            if (!apply) continue;
+            const T l = slab[jj * rcap + i] * inv;
+            slab[jj * rcap + i] = l;
+            for (int x = jj + 1; x < jb; ++x) slab[x * rcap + i] = slab[x * rcap + i] - l * s_piv[x];
         }
         __syncthreads();
     }

@@ -296,11 +296,13 @@ mw_status mw_cgetrs(int64_t n, int64_t nrhs, const float* LU, int64_t lda,
  * Mixed-precision drop-in for the complex128 solve of
  * _solve_with_kcl_ports (bspline.py:2971-2989): factor Z32 (a complex64
  * copy of Z, overwritten by its LU) with mw_cgetrf, then refine
- * X <- X + LU32 \ (B - Z X) with the residual in FP64 against Z until the
- * largest per-column correction ||dX||_inf / ||X||_inf is <= tol, or
- * max_iter corrections.  X (n x nrhs, complex128) receives the solution.
- * *iterations / *last_correction (host pointers, may be NULL) report the
- * refinement.  Synchronises `stream` once per refinement step.  Returns
+ * X <- X + LU32 \ (B - Z X) with the residual in FP64 against Z until, in
+ * every column, the correction r = ||dX||_inf / ||X||_inf -- or, once
+ * successive corrections contract by q = r / r_prev <= 1/2, the error
+ * estimated to remain after it, r q -- is <= tol, or max_iter corrections.
+ * X (n x nrhs, complex128) receives the solution.  *iterations /
+ * *last_correction (host pointers, may be NULL) report the refinement
+ * (last_correction: the largest controlling value above).  Synchronises `stream` once per refinement step.  Returns
  * MW_ERR_SINGULAR if tol was not reached.
  */
 size_t mw_zgesv_mixed_workspace_size(int64_t n, int64_t nrhs);
@@ -334,8 +336,8 @@ mw_status mw_fill_z_batch(const mw_segments* seg, const mw_basis* basis,
  * Batched mixed-precision solve of `batch` same-order systems Z_b X_b = B_b
  * (complex128, n x nrhs; B shared when b_stride == 0): complex64 LU of Z32_b
  * (overwritten) with one CTA per matrix panel and the batched tensor-core
- * update, then FP64 refinement of every X_b against Z_b until the largest
- * relative correction over the batch is <= tol.  X is batch x n x nrhs,
+ * update, then FP64 refinement of every X_b against Z_b with the stopping
+ * rule of mw_zgesv_mixed applied to every matrix of the batch.  X is batch x n x nrhs,
  * contiguous.  The reference's counterpart is the stacked complex128
  * numpy.linalg.solve of _solve_with_kcl_swept_ports (bspline.py:3017).
  * Strides count complex elements.  n <= 1600 (the complex64 panel of 16

@@ -380,7 +380,7 @@ extern "C" mw_status mw_zgesv_mixed_batched(int32_t n, int32_t nrhs, int32_t bat
     for (int b = 0; b < batch; ++b)
         MW_CHECK_CUDA(cudaMemcpy2DAsync(w.R + (int64_t)b * per, sizeof(cd) * n, Bc + (int64_t)b * b_stride,
                                         sizeof(cd) * ldb, sizeof(cd) * n, nrhs, cudaMemcpyDeviceToDevice, st));
-    std::vector<double> hn(2 * (size_t)batch);
+    std::vector<double> hn(2 * (size_t)batch), prev((size_t)batch, 0.0);
     std::vector<int32_t> hinfo(batch);
     double corr = INFINITY;
     int it = 0;
@@ -413,11 +413,16 @@ extern "C" mw_status mw_zgesv_mixed_batched(int32_t n, int32_t nrhs, int32_t bat
                     return MW_ERR_SINGULAR;
                 }
         }
+        // as mw_zgesv_mixed: the relative correction, or once corrections
+        // contract (q <= 1/2) the error estimated to remain, r q
         corr = 0.0;
         for (int b = 0; b < batch; ++b) {
             const double xm = hn[batch + b];
             const double r = xm > 0.0 ? hn[b] / xm : (hn[b] > 0.0 ? INFINITY : 0.0);
-            if (!(r <= corr)) corr = r;
+            double v = r;
+            if (it > 0 && prev[b] > 0.0 && r <= 0.5 * prev[b]) v = fmin(r, r * (r / prev[b]));
+            prev[b] = r;
+            if (!(v <= corr)) corr = v;
         }
         if (corr <= tol || it >= max_iter) break;
         {

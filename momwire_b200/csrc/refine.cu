@@ -2,7 +2,9 @@
 //
 // Solves Z X = B (complex128) from a complex64 LU of the same matrix:
 //   X0 = LU32 \ B;  repeat  R = B - Z X (FP64),  C = LU32 \ R,  X += C
-// until max over columns of ||C||_inf / ||X||_inf <= tol.  The factors come
+// until, for every column, the relative correction r = ||C||_inf / ||X||_inf
+// or -- once successive corrections contract by q = r / r_prev <= 1/2 -- the
+// error estimated to remain after it, r q, is <= tol.  The factors come
 // from mw_cgetrf (tensor-core trailing updates, 3xTF32); the residual uses
 // the FP64 Z.  The reference solves in complex128 LAPACK
 // (bspline.py:2971-2989); this path adds nothing to its algebra.
@@ -123,7 +125,7 @@ extern "C" mw_status mw_zgesv_mixed(int64_t n, int64_t nrhs, const double* Z, in
     count_launch();
     double corr = INFINITY;
     int it = 0;
-    std::vector<double> hn(2 * nrhs);
+    std::vector<double> hn(2 * nrhs), prev(nrhs, 0.0);
     for (;; ++it) {
         if (cancel && *cancel) {
             set_error("solve cancelled");
@@ -145,11 +147,18 @@ extern "C" mw_status mw_zgesv_mixed(int64_t n, int64_t nrhs, const double* Z, in
         }
         MW_CHECK_CUDA(cudaMemcpyAsync(hn.data(), norms, sizeof(double) * 2 * nrhs, cudaMemcpyDeviceToHost, st));
         MW_CHECK_CUDA(cudaStreamSynchronize(st));
+        // per column: the relative correction r, and once two corrections
+        // are known and contract (ratio q = r / r_prev <= 1/2), the error
+        // left after this one, about r q; the controlling value is the
+        // smaller of the two, maximised over the columns
         corr = 0.0;
         for (int64_t j = 0; j < nrhs; ++j) {
             double xm = hn[nrhs + j];
             double r = xm > 0.0 ? hn[j] / xm : (hn[j] > 0.0 ? INFINITY : 0.0);
-            if (!(r <= corr)) corr = r;  // NaN-propagating max
+            double v = r;
+            if (it > 0 && prev[j] > 0.0 && r <= 0.5 * prev[j]) v = fmin(r, r * (r / prev[j]));
+            prev[j] = r;
+            if (!(v <= corr)) corr = v;  // NaN-propagating max
         }
         if (corr <= tol || it >= max_iter) break;
         // R = B - Z X   (FP64)

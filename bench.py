@@ -6,13 +6,18 @@ Workload (one "step"): the 16 x 16 planar array of half-wave dipoles at
 256 port columns, Y = B^T X.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                    [--precision fp64|mixed]
+                    [--precision mixed|fp64] [--workload array|yagi_sweep|somm]
 
 Prints ONE JSON line on rank 0.  ``value`` is device-timed throughput with the
-inputs resident in HBM (solves per second over all ranks); ``e2e`` is the
-same metric through the public ``BSplineSolver(...).compute_port_solution()``
-call, host tables in and coefficients + Y out.  Under torchrun each rank
-solves its own replica ("replicas only": a single dense solve does not shard).
+inputs resident in HBM (solves per second over all ranks) of the default
+mixed-precision path (complex64 tensor-core LU + FP64 refinement against the
+FP64 fill); ``fp64_ms_per_step`` times the plain complex128 path on the same
+workload; ``e2e`` is the same metric through the public
+``BSplineSolver(...).compute_port_solution()`` call, host tables in and
+coefficients + Y out.  ``sweep`` adds the batched frequency sweep of seeded
+Yagis (64 frequencies each), sharded over the ranks.  Under torchrun each
+rank solves its own replica of the array ("replicas only": a single dense
+solve does not shard) and its shard of the sweep.
 """
 
 from __future__ import annotations
@@ -40,14 +45,17 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
+    ap.add_argument("--fp64-steps", type=int, default=2, help="steps of the FP64 path timed beside a mixed run")
+    ap.add_argument("--sweep-structs", type=int, default=16,
+                    help="Yagis per rank in the sweep part of the line (0: none)")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--nx", type=int, default=16)
     ap.add_argument("--micro", default=None, choices=["cgemm_tc"], help="kernel microbenchmark instead")
     ap.add_argument("--m", type=int, default=8192)
     ap.add_argument("--k", type=int, default=64)
-    ap.add_argument("--workload", default="array", choices=["array", "yagi_sweep"])
+    ap.add_argument("--workload", default="array", choices=["array", "yagi_sweep", "somm"])
     ap.add_argument("--n-struct", type=int, default=512)
     ap.add_argument("--fp64-structs", type=int, default=4)
     ap.add_argument("--fp64-kstep", type=int, default=4)
@@ -261,6 +269,29 @@ def run_b200(args, kw):
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         e2e_step = float(t.item())
 
+    # the plain FP64 path on the same workload, for the mixed-vs-FP64 ratio
+    fp64_ms = None
+    if args.precision == "mixed" and args.fp64_steps > 0:
+        s64 = momwire_b200.BSplineSolver(**kw, precision="fp64", device=local)
+        b64 = s64._alloc()
+        s64._device_solve(b64, st)
+        torch.cuda.synchronize()
+        if pg:
+            pg.barrier()
+        e0.record(stream)
+        for _ in range(args.fp64_steps):
+            s64._device_solve(b64, st)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        fp64_ms = e0.elapsed_time(e1) / args.fp64_steps
+        if pg:
+            t = torch.tensor([fp64_ms], device=dev)
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            fp64_ms = float(t.item())
+        del s64, b64
+
+    sweep_part = run_sweep_part(args, rank, world, local, pg) if args.sweep_structs > 0 else None
+
     # roofline of the dominant kernel class
     peaks = {}
     try:
@@ -316,6 +347,9 @@ def run_b200(args, kw):
         "kernels": breakdown,
         "clocks": clocks.summary(),
         "y_rel_err_vs_reference": y_err,
+        "fp64_ms_per_step": fp64_ms,
+        "speedup_vs_fp64": (fp64_ms / ms_step) if fp64_ms else None,
+        "sweep": sweep_part,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample(kw)
@@ -356,6 +390,95 @@ def run_micro(args):
     ms = e0.elapsed_time(e1) / args.steps
     print(json.dumps({"micro": "cgemm_tc", "m": m, "n": m, "k": k, "ms": ms,
                       "tflops_algorithmic": 8.0 * m * m * k / (ms / 1e3) / 1e12, "status": int(status.item())}))
+
+
+def run_sweep_part(args, rank, world, local, pg):
+    """Sweep part of the headline line: world x --sweep-structs seeded Yagis
+    at 64 frequencies, sharded over the ranks (LPT on n^3), each rank's
+    shard device-timed; pts/s = all solves / the slowest rank.  Rank 0 also
+    times the plain FP64 GPU path on a sample (2 structures, every 8th
+    frequency) and compares drive-point impedances."""
+    import numpy as np
+    import torch
+
+    import momwire_b200
+    from momwire_b200 import sweep
+    from momwire_b200.workloads import yagi_sweep
+
+    structs, ks = yagi_sweep(n_structures=args.sweep_structs * world, n_freq=64, seed=0)
+    parts = sweep.partition([sweep.structure_cost(k) for k in structs], world)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    fn = sweep.mixed_sweep_fn(local)
+    fn(structs[parts[rank][0]], ks[:4])  # warm-up
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    local_y = sweep.solve_shard(structs, ks, parts[rank], fn)
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b)
+    if pg:
+        t = torch.tensor([ms], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+    ys = sweep.gather(local_y)
+    out = {"workload": f"yagi_sweep_{len(structs)}x64", "solves": len(structs) * len(ks),
+           "pts_per_s": len(structs) * len(ks) / (ms / 1e3), "ms": ms, "sharding": f"LPT x{world}"}
+    if rank == 0:
+        sub = ks[::8]
+        f_ms, n64, err = 0.0, 0, 0.0
+        for i in range(min(2, len(structs))):
+            s = momwire_b200.BSplineSolver(**structs[i], device=local)
+            a.record(stream)
+            y = s.compute_y_matrix_swept(sub)
+            b.record(stream)
+            torch.cuda.synchronize()
+            f_ms += a.elapsed_time(b)
+            n64 += len(sub)
+            z64, zmx = 1.0 / y[:, 0, 0], 1.0 / ys[i][::8, 0, 0]
+            err = max(err, float(np.max(np.abs(zmx - z64) / np.abs(z64))))
+        out.update(fp64_pts_per_s=n64 / (f_ms / 1e3), max_rel_dZin_vs_fp64=err)
+        out["speedup_vs_fp64"] = out["pts_per_s"] / out["fp64_pts_per_s"]
+    return out
+
+
+def run_somm(args):
+    """The Sommerfeld-ground workload: seeded structures (dipole, monopole +
+    radials, inverted V) over random grounds and frequencies, each solved
+    cold through the public API on the quadrature-grid path and on the
+    surrogate path; solves per second and the impedance agreement."""
+    import numpy as np
+    import torch
+
+    import momwire_b200
+    from momwire_b200 import sommerfeld as P
+    from momwire_b200.workloads import somm_structures
+
+    structs = somm_structures(args.n_struct, seed=0)
+    for m in ("grid", "surrogate"):
+        momwire_b200.BSplineSolver(**structs[0], sommerfeld_method=m).compute_impedance()
+    res, z = {}, {}
+    for m in ("grid", "surrogate"):
+        P.clear_cache()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        zs, used = [], 0
+        for kw in structs:
+            s = momwire_b200.BSplineSolver(**kw, sommerfeld_method=m)
+            zs.append(s.compute_impedance()[0])
+            used += s.last_sommerfeld["method"] == "surrogate"
+        torch.cuda.synchronize()
+        res[m] = (time.perf_counter() - t0, used)
+        z[m] = np.array(zs)
+    err = np.abs(z["surrogate"] - z["grid"]) / np.abs(z["grid"])
+    print(json.dumps({"workload": f"somm_structures_{len(structs)}", "grid_pts_per_s": len(structs) / res["grid"][0],
+                      "surrogate_pts_per_s": len(structs) / res["surrogate"][0],
+                      "speedup": res["grid"][0] / res["surrogate"][0], "surrogate_used": res["surrogate"][1],
+                      "max_rel_dZin_vs_grid": float(err.max()), "median_rel_dZin_vs_grid": float(np.median(err)),
+                      "timing": "wall clock per cold structure, host + device"}), flush=True)
 
 
 def run_sweep(args):
@@ -416,6 +539,9 @@ def main():
         return
     if args.workload == "yagi_sweep":
         run_sweep(args)
+        return
+    if args.workload == "somm":
+        run_somm(args)
         return
     from momwire_b200.workloads import dipole_array
 

@@ -354,6 +354,16 @@ mw_status mw_zgesv_mixed_batched(int32_t n, int32_t nrhs, int32_t batch,
                                  double* last_correction, void* stream);
 
 /*
+ * out (ld x ncols complex128, column-major) = 0, then out[rows[q], cols[q]]
+ * += vals[q] for the nnz entries (device arrays; vals interleaved re/im).
+ * Builds the sparse port right-hand sides [B | kcl_con^T] and the KCL rows
+ * on the device (the dense host matrices of bspline.py:3841-3867 are mostly
+ * zeros: a few basis functions per feed, a few +-1 per junction).
+ */
+mw_status mw_scatter_c128(int64_t ld, int64_t ncols, int64_t nnz, const int64_t* rows,
+                          const int64_t* cols, const double* vals, double* out, void* stream);
+
+/*
  * C = alpha * op(A) * op(B) + beta * C for complex128 column-major
  * matrices, op = 'N' or 'T' (transA/transB 0/1).  Used for the KCL Schur
  * step and Y = B^T X (bspline.py:2984-2989, 4179).

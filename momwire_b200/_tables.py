@@ -13,6 +13,7 @@ import math
 from dataclasses import dataclass
 
 import numpy as np
+import scipy.sparse
 
 MAX_TILE_BASIS = 16
 MAX_TILE_SEG = 24
@@ -147,7 +148,7 @@ class Basis:
     degree: int
     supp: np.ndarray  # (n_b, d+1) int32, -1 = padded wing
     polys: np.ndarray  # (n_b, d+1, d+1)
-    kcl_A: np.ndarray  # (n_c, n_b)
+    kcl_A: "scipy.sparse.csr_matrix"  # (n_c, n_b) KCL rows, entries +-1
     knots: list  # per wire
     kept: list  # per wire: list of (j_local, kind, junction, end, m_global)
 
@@ -212,10 +213,15 @@ def build_basis(geom: Geometry, degree, start_status, end_status, n_junctions, g
         poly_all.append(poly)
         m += nk
     rows = [j for j in range(n_junctions) if j not in grounded]
-    kcl = np.zeros((len(rows), m))
+    ri, ci, vi = [], [], []
     for r, j in enumerate(rows):
         for mg, sg in jdirs[j]:
-            kcl[r, mg] = sg
+            ri.append(r)
+            ci.append(mg)
+            vi.append(sg)
+    # sparse: a few +-1 per junction row (4,225 x 33,280 dense would be 1.1 GB)
+    kcl = scipy.sparse.csr_matrix((np.asarray(vi, dtype=np.float64), (np.asarray(ri, dtype=np.int64),
+                                   np.asarray(ci, dtype=np.int64))), shape=(len(rows), m))
     return Basis(
         degree=d,
         supp=np.ascontiguousarray(np.concatenate(supp_all, axis=0)),

@@ -26,6 +26,7 @@ from contextlib import contextmanager
 from dataclasses import dataclass
 
 import numpy as np
+import scipy.sparse
 
 from . import _lib
 from . import _tables as T
@@ -562,7 +563,7 @@ class BSplineSolver:
     def _split_kcl_ports(self, kcl_A):
         """``bspline.py:1171-1214``."""
         if not self.junction_ports:
-            return kcl_A, np.zeros((0, kcl_A.shape[1])), np.zeros(0, dtype=np.complex128)
+            return kcl_A, scipy.sparse.csr_matrix((0, kcl_A.shape[1])), np.zeros(0, dtype=np.complex128)
         grounded = self._grounded_junctions()
         row_of, row = {}, 0
         for j in range(len(self.junctions)):
@@ -581,9 +582,10 @@ class BSplineSolver:
         port_V = np.array([v for _j, v in self.junction_ports], dtype=np.complex128)
         return kcl_A[keep, :], kcl_A[port_rows, :], port_V
 
-    def _source_vector(self, w, s_f):
-        """Galerkin drive column of one gap feed (``bspline.py:2806-2942``):
-        point (v_m = Phi_m(s_f)), segment-wide gap, or cos^2 bump."""
+    def _source_entries(self, w, s_f):
+        """Nonzeros (basis indices, values) of the Galerkin drive column of
+        one gap feed (``bspline.py:2806-2942``): point (v_m = Phi_m(s_f)),
+        segment-wide gap, or cos^2 bump."""
         geom, basis = self._geometry(), self._basis()
         d = self.degree
         arc = geom.wire_arc[w]
@@ -612,9 +614,16 @@ class BSplineSolver:
             delta = t - s_f
             g = np.where(np.abs(delta) < half, (2.0 / width) * np.cos(np.pi * delta / width) ** 2, 0.0)
             vals = np.einsum("qj,q,q->j", T.basis_values(knots, d, t), g, wts)
-        v = np.zeros(basis.n, dtype=np.complex128)
-        for j, _kind, _jn, _end, mg in basis.kept[w]:
-            v[mg] = vals[j]
+        idx = np.array([mg for j, _kind, _jn, _end, mg in basis.kept[w] if vals[j] != 0.0], dtype=np.int64)
+        val = np.array([vals[j] for j, _kind, _jn, _end, _mg in basis.kept[w] if vals[j] != 0.0],
+                       dtype=np.complex128)
+        return idx, val
+
+    def _source_vector(self, w, s_f):
+        """Dense drive column of one gap feed (see ``_source_entries``)."""
+        v = np.zeros(self._basis().n, dtype=np.complex128)
+        idx, val = self._source_entries(w, s_f)
+        v[idx] = val
         return v
 
     def _node_gap_columns(self):
@@ -649,7 +658,32 @@ class BSplineSolver:
             B[:, i] = self._source_vector(w, s_f)
         kcl_con, port_A, _pv = self._split_kcl_ports(basis.kcl_A)
         gap, _gv = self._node_gap_columns()
-        return np.hstack([B, port_A.T.astype(np.complex128), gap.astype(np.complex128)]), kcl_con
+        return np.hstack([B, port_A.T.toarray().astype(np.complex128), gap.astype(np.complex128)]), kcl_con
+
+    def _port_entries(self):
+        """(rows, cols, vals, n_p): the nonzeros of the port matrix B of
+        ``_port_columns`` in coordinate form (feeds, junction-port KCL rows,
+        node gaps)."""
+        geom, basis = self._geometry(), self._basis()
+        rs, cs, vs = [], [], []
+        for i, (w, arc_i, _v) in enumerate(self.feeds):
+            s_f = arc_i if arc_i is not None else geom.wire_arc[w][-1] / 2.0
+            idx, val = self._source_entries(w, s_f)
+            rs.append(idx)
+            cs.append(np.full(idx.size, i, dtype=np.int64))
+            vs.append(val)
+        _kcl, port_A, _pv = self._split_kcl_ports(basis.kcl_A)
+        pa = port_A.tocoo()
+        rs.append(pa.col.astype(np.int64))
+        cs.append(pa.row.astype(np.int64) + len(self.feeds))
+        vs.append(pa.data.astype(np.complex128))
+        gap, _gv = self._node_gap_columns()
+        gr, gc = np.nonzero(gap)
+        rs.append(gr.astype(np.int64))
+        cs.append(gc.astype(np.int64) + len(self.feeds) + port_A.shape[0])
+        vs.append(gap[gr, gc].astype(np.complex128))
+        n_p = len(self.feeds) + port_A.shape[0] + gap.shape[1]
+        return np.concatenate(rs), np.concatenate(cs), np.concatenate(vs), n_p
 
     def _port_count(self):
         return len(self.feeds) + len(self.junction_ports) + len(self.node_gaps)
@@ -681,10 +715,27 @@ class BSplineSolver:
         dt = self._dev_tables()
         n = self._basis().n
         nm = self.degree + 1
-        B, kcl_con = self._port_columns()
-        n_p, n_c = B.shape[1], kcl_con.shape[0]
-        rhs_host = np.hstack([B, kcl_con.T.astype(np.complex128)]) if n_c else B
+        # port columns and KCL rows are a few nonzeros each: upload them in
+        # coordinate form and scatter [B | kcl_con^T], B and kcl_con on the
+        # device
+        pr, pc, pv, n_p = self._port_entries()
+        kcl_con = self._split_kcl_ports(self._basis().kcl_A)[0].tocoo()
+        n_c = kcl_con.shape[0]
+        kr, kc = kcl_con.row.astype(np.int64), kcl_con.col.astype(np.int64)
+        kv = kcl_con.data.astype(np.complex128)
+        rr, rc, rv = np.concatenate([pr, kc]), np.concatenate([pc, kr + n_p]), np.concatenate([pv, kv])
+        host = [pr, pc, np.ascontiguousarray(pv).view(np.float64), kr, kc, np.ascontiguousarray(kv).view(np.float64),
+                rr, rc, np.ascontiguousarray(rv).view(np.float64)]
+        ent = [torch.from_numpy(np.ascontiguousarray(a)).to(dev) for a in host]
         lib = _lib.load()
+        st = torch.cuda.current_stream(dev).cuda_stream
+        m = n_p + n_c
+        rhs0 = torch.empty((max(m, 1), n), dtype=torch.complex128, device=dev)
+        Bd = torch.empty((max(n_p, 1), n), dtype=torch.complex128, device=dev)
+        _lib.call("mw_scatter_c128", n, n_p, pr.size, ent[0].data_ptr(), ent[1].data_ptr(), ent[2].data_ptr(),
+                  Bd.data_ptr(), st)
+        _lib.call("mw_scatter_c128", n, m, rr.size, ent[6].data_ptr(), ent[7].data_ptr(), ent[8].data_ptr(),
+                  rhs0.data_ptr(), st)
         buf = {
             "n": n,
             "n_p": n_p,
@@ -692,8 +743,9 @@ class BSplineSolver:
             "Z": torch.empty((n, n), dtype=torch.complex128, device=dev),
             "table": torch.empty((max(dt.table_rows, 1), nm, nm), dtype=torch.complex128, device=dev),
             # column-major (n x m) right-hand sides live in an (m, n) tensor
-            "RHS0": torch.from_numpy(np.ascontiguousarray(rhs_host.T)).to(dev),
-            "B": torch.from_numpy(np.ascontiguousarray(B.T)).to(dev),
+            "RHS0": rhs0,
+            "B": Bd,
+            "entries": ent,
             "ws": torch.empty(lib.mw_getrf_workspace_size(n), dtype=torch.uint8, device=dev),
             "ipiv": torch.empty(max(n, 1), dtype=torch.int32, device=dev),
             "info": torch.zeros(2, dtype=torch.int32, device=dev),
@@ -706,15 +758,17 @@ class BSplineSolver:
             buf["Z32"] = torch.empty((n, n), dtype=torch.complex64, device=dev)
             buf["ws_mix"] = torch.empty(lib.mw_zgesv_mixed_workspace_size(n, m), dtype=torch.uint8, device=dev)
         if n_c:
-            buf["A"] = torch.from_numpy(np.ascontiguousarray(kcl_con.astype(np.complex128).T)).to(dev)
+            # kcl_con (n_c x n, column-major, ld n_c)
+            buf["A"] = torch.empty((n, n_c), dtype=torch.complex128, device=dev)
+            _lib.call("mw_scatter_c128", n_c, n, kr.size, ent[3].data_ptr(), ent[4].data_ptr(), ent[5].data_ptr(),
+                      buf["A"].data_ptr(), st)
             buf["S"] = torch.empty((n_c, n_c), dtype=torch.complex128, device=dev)
             buf["AW"] = torch.empty((max(n_p, 1), n_c), dtype=torch.complex128, device=dev)
             buf["ws_c"] = torch.empty(lib.mw_getrf_workspace_size(n_c), dtype=torch.uint8, device=dev)
             buf["ipiv_c"] = torch.empty(n_c, dtype=torch.int32, device=dev)
             buf["info_c"] = torch.zeros(2, dtype=torch.int32, device=dev)
             buf["W"] = torch.empty((max(n_p, 1), n), dtype=torch.complex128, device=dev)
-        buf["h2d_bytes"] = int(buf["RHS0"].numel() * 16 + buf["B"].numel() * 16 + dt.h2d_bytes +
-                               (buf["A"].numel() * 16 if n_c else 0))
+        buf["h2d_bytes"] = int(sum(a.nbytes for a in host) + dt.h2d_bytes)
         return buf
 
     def _fill_device(self, buf, stream):
@@ -916,8 +970,9 @@ class BSplineSolver:
         _gap, gap_V = self._node_gap_columns()
         volts = np.concatenate([np.array([v for _w, _a, v in self.feeds], dtype=np.complex128), port_V, gap_V])
         coeffs = sol.coeffs @ volts
-        B, _ = self._port_columns()
-        currents = B.T @ coeffs
+        pr, pc, pv, n_p = self._port_entries()
+        Bs = scipy.sparse.csr_matrix((pv, (pr, pc)), shape=(self._basis().n, n_p))
+        currents = Bs.T @ coeffs
         z = volts / currents
         return (z[0] if len(volts) == 1 else z), coeffs
 

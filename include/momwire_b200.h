@@ -298,7 +298,8 @@ mw_status mw_cgetrs(int64_t n, int64_t nrhs, const float* LU, int64_t lda,
  * copy of Z, overwritten by its LU) with mw_cgetrf, then refine
  * X <- X + LU32 \ (B - Z X) with the residual in FP64 against Z until, in
  * every column, the correction r = ||dX||_inf / ||X||_inf -- or, once
- * successive corrections contract by q = r / r_prev <= 1/2, the error
+ * successive corrections contract by q = r / r_prev <= 1/2 (the initial
+ * solve from X = 0 counting as a correction of 1), the error
  * estimated to remain after it, r q -- is <= tol, or max_iter corrections.
  * X (n x nrhs, complex128) receives the solution.  *iterations /
  * *last_correction (host pointers, may be NULL) report the refinement

@@ -25,7 +25,9 @@ mw_status cgemm_tc_update(int64_t m, int64_t n, int64_t k, const cf* A, int64_t 
                           int64_t ldc, void* ws, size_t ws_bytes, int* err, cudaStream_t st);
 size_t cgemm_tc_workspace(int64_t m, int64_t n, int64_t k);
 
-constexpr int kNB = 64;  // panel width
+constexpr int kNB = 64;         // triangular-solve block (and getrs block)
+constexpr int kOuterNB = 128;   // getrf block: panel width and trailing-update k
+constexpr int kPanelMaxJb = 128;
 constexpr int kPanelThreads = 256;
 
 struct PanelWs {
@@ -87,8 +89,8 @@ struct PanelArgs {
     int32_t* ipiv;
     int32_t* info;
     PanelWs* ws;
-    // double-buffered slots: [2][G] values, [2][G] indices, [2][G][kNB]
-    // candidate rows, [2][kNB] current row
+    // double-buffered slots: [2][G] values, [2][G] indices,
+    // [2][G][kPanelMaxJb] candidate rows, [2][kPanelMaxJb] current row
     double* slot_val;
     int64_t* slot_idx;
     void* slot_row;
@@ -146,8 +148,8 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel(PanelArgs P) {
     T* slab = reinterpret_cast<T*>(panel_smem);
     __shared__ double s_v[kPanelThreads / 32];
     __shared__ int64_t s_i[kPanelThreads / 32];
-    __shared__ T s_piv[kNB];
-    __shared__ T s_cur[kNB];
+    __shared__ T s_piv[kPanelMaxJb];
+    __shared__ T s_cur[kPanelMaxJb];
     __shared__ int64_t s_p;
     __shared__ double s_pv;
 
@@ -188,9 +190,9 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel(PanelArgs P) {
         }
         if (bidx != INT64_MAX)
             for (int x = tid; x < jb; x += blockDim.x)
-                slot_row[((size_t)buf * G + g) * kNB + x] = slab[x * rcap + (int)(bidx - r0)];
+                slot_row[((size_t)buf * G + g) * kPanelMaxJb + x] = slab[x * rcap + (int)(bidx - r0)];
         if (c >= r0 && c < r1)
-            for (int x = tid; x < jb; x += blockDim.x) cur_row[buf * kNB + x] = slab[x * rcap + (int)(c - r0)];
+            for (int x = tid; x < jb; x += blockDim.x) cur_row[buf * kPanelMaxJb + x] = slab[x * rcap + (int)(c - r0)];
         // 3. one barrier per column
         if (!grid_sync_bounded(P.ws, (unsigned)(jj + 1) * G)) return;
         // 4. global pivot from the G candidates (warp 0)
@@ -220,8 +222,8 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel(PanelArgs P) {
             // the same warp fetches the pivot row and the current row (L2-
             // coherent loads: other CTAs wrote them)
             for (int x = tid; x < jb; x += 32) {
-                s_piv[x] = ldcg_c(slot_row + ((size_t)buf * G + bg) * kNB + x);
-                s_cur[x] = ldcg_c(cur_row + buf * kNB + x);
+                s_piv[x] = ldcg_c(slot_row + ((size_t)buf * G + bg) * kPanelMaxJb + x);
+                s_cur[x] = ldcg_c(cur_row + buf * kPanelMaxJb + x);
             }
         }
         __syncthreads();
@@ -692,10 +694,10 @@ static size_t ws_layout(int G, size_t* off_val, size_t* off_idx, size_t* off_row
     o += sizeof(int64_t) * 2 * G;
     o = (o + 255) & ~size_t(255);
     *off_row = o;
-    o += sizeof(cd) * 2 * (size_t)G * kNB;
+    o += sizeof(cd) * 2 * (size_t)G * kPanelMaxJb;
     o = (o + 255) & ~size_t(255);
     *off_cur = o;
-    o += sizeof(cd) * 2 * kNB;
+    o += sizeof(cd) * 2 * kPanelMaxJb;
     return (o + 255) & ~size_t(255);
 }
 
@@ -719,6 +721,24 @@ static mw_status block_update(const cf* A, int64_t lda, const cf* B, int64_t ldb
     return cgemm_tc_update(m, n, k, A, lda, B, ldb, C, ldc, u.tc_ws, u.tc_ws_bytes, u.tc_err, st);
 }
 
+// X <- L^-1 X for a unit lower triangle of any order: kNB-row diagonal
+// blocks by the warp-per-column kernel, the rest of X updated in between.
+template <class T>
+static mw_status trsm_lower_blocked(const T* L, int64_t ldl, T* X, int64_t ldx, int jb, int64_t ncols,
+                                    const Updater& up, cudaStream_t st) {
+    for (int b0 = 0; b0 < jb; b0 += kNB) {
+        const int bb = (jb - b0) < kNB ? (jb - b0) : kNB;
+        trsm_launch<T, false>(L + b0 + (int64_t)b0 * ldl, ldl, X + b0, ldx, bb, ncols, st);
+        const int rest = jb - b0 - bb;
+        if (rest > 0) {
+            mw_status s = block_update(L + (b0 + bb) + (int64_t)b0 * ldl, ldl, X + b0, ldx, X + b0 + bb, ldx, rest,
+                                       ncols, bb, up, st);
+            if (s != MW_OK) return s;
+        }
+    }
+    return MW_OK;
+}
+
 // Factor the panel rows [j0, n) x columns [j0, j0+jb) with partial pivoting.
 // One cooperative launch when every CTA's row slab fits in shared memory;
 // otherwise split the columns in two and recurse (left half, then update and
@@ -736,7 +756,9 @@ static mw_status panel_factor(T* A, int64_t lda, int64_t n, int64_t j0, int jb, 
     if (G < 1) G = 1;
     const int64_t per = (m + G - 1) / G;
     const size_t smem = (size_t)per * jb * sizeof(T);
-    if (smem > kPanelSmemMax) {
+    // panels wider than kNB are factored as two halves (the per-column
+    // rank-1 work stays kNB wide; the halves meet in one small update)
+    if (smem > kPanelSmemMax || jb > kNB) {
         MW_REQUIRE(jb > 1, "matrix too large for the panel kernel (%lld rows per CTA)", (long long)per);
         const int h = jb / 2;
         mw_status s = panel_factor<T>(A, lda, n, j0, h, ipiv, info, ws, up, st);
@@ -792,12 +814,12 @@ static mw_status getrf(int64_t n, T* A, int64_t lda, int32_t* ipiv, int32_t* inf
         if (s0 != MW_OK) return s0;
     }
     PanelWs* pws = reinterpret_cast<PanelWs*>(ws);
-    for (int64_t j0 = 0; j0 < n; j0 += kNB) {
+    for (int64_t j0 = 0; j0 < n; j0 += kOuterNB) {
         if (cancel && *cancel) {
             set_error("factorisation cancelled");
             return MW_ERR_CANCELLED;
         }
-        const int jb = (int)((n - j0) < kNB ? (n - j0) : kNB);
+        const int jb = (int)((n - j0) < kOuterNB ? (n - j0) : kOuterNB);
         mw_status s = panel_factor<T>(A, lda, n, j0, jb, ipiv, info, ws, up, st);
         if (s != MW_OK) return s;
         const int64_t left = j0, right = n - j0 - jb;
@@ -806,7 +828,7 @@ static mw_status getrf(int64_t n, T* A, int64_t lda, int32_t* ipiv, int32_t* inf
             laswp_launch<T>(A, lda, j0 + jb, right, ipiv, j0, j0 + jb, st);
             T* A11 = A + j0 + j0 * lda;
             T* A12 = A + j0 + (j0 + jb) * lda;
-            trsm_launch<T, false>(A11, lda, A12, lda, jb, right, st);
+            trsm_lower_blocked<T>(A11, lda, A12, lda, jb, right, up, st);
             s = block_update(A + (j0 + jb) + j0 * lda, lda, A12, lda, A + (j0 + jb) + (j0 + jb) * lda, lda, right, right,
                              jb, up, st);
             if (s != MW_OK) return s;
@@ -856,11 +878,11 @@ static size_t panel_ws_bytes() {
 }
 
 // Workspace of the complex64 path: panel slots, then the tensor-core
-// operand planes for the largest update (m = n, n = n, k = kNB), then the
+// operand planes for the largest update (m = n, n = n, k = kOuterNB), then the
 // device status word.
 static size_t cgetrf_ws_bytes(int64_t n, int64_t nrhs_max) {
     int64_t w = n > nrhs_max ? n : nrhs_max;
-    return panel_ws_bytes() + 1024 + cgemm_tc_workspace(n, w, kNB) + 256;
+    return panel_ws_bytes() + 1024 + cgemm_tc_workspace(n, w, kOuterNB) + 256;
 }
 
 static Updater tc_updater(char* ws, size_t ws_bytes, int64_t n, int64_t nrhs_max) {
@@ -868,7 +890,7 @@ static Updater tc_updater(char* ws, size_t ws_bytes, int64_t n, int64_t nrhs_max
     size_t p = (panel_ws_bytes() + 1023) & ~size_t(1023);
     int64_t w = n > nrhs_max ? n : nrhs_max;
     u.tc_ws = ws + p;
-    u.tc_ws_bytes = cgemm_tc_workspace(n, w, kNB);
+    u.tc_ws_bytes = cgemm_tc_workspace(n, w, kOuterNB);
     u.tc_err = reinterpret_cast<int*>(ws + p + ((u.tc_ws_bytes + 255) & ~size_t(255)));
     (void)ws_bytes;
     return u;

@@ -147,10 +147,13 @@ extern "C" mw_status mw_zgesv_mixed(int64_t n, int64_t nrhs, const double* Z, in
         }
         MW_CHECK_CUDA(cudaMemcpyAsync(hn.data(), norms, sizeof(double) * 2 * nrhs, cudaMemcpyDeviceToHost, st));
         MW_CHECK_CUDA(cudaStreamSynchronize(st));
-        // per column: the relative correction r, and once two corrections
-        // are known and contract (ratio q = r / r_prev <= 1/2), the error
-        // left after this one, about r q; the controlling value is the
-        // smaller of the two, maximised over the columns
+        // per column: the relative correction r, and once corrections
+        // contract (q = r / r_prev <= 1/2), the error left after this one,
+        // about r q.  The initial solve counts as the first correction: it
+        // starts from X = 0, so its error was the whole solution (r = 1) and
+        // the first refinement correction r_1 measures the contraction
+        // itself.  The controlling value is the smaller of r and r q,
+        // maximised over the columns.
         corr = 0.0;
         for (int64_t j = 0; j < nrhs; ++j) {
             double xm = hn[nrhs + j];

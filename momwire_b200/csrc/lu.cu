@@ -612,7 +612,7 @@ mw_status zgemm_launch_simt(bool ta, bool tb, int64_t m, int64_t n, int64_t k, c
 mw_status zgemm_launch(bool ta, bool tb, int64_t m, int64_t n, int64_t k, cd alpha, const cd* A, int64_t lda,
                        const cd* B, int64_t ldb, cd beta, cd* C, int64_t ldc, cudaStream_t st) {
     if (m <= 0 || n <= 0) return MW_OK;
-    if (k <= 256) return zgemm_launch_simt(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, st);
+    if (k < 128) return zgemm_launch_simt(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, st);
     {
         static bool attr = false;
         if (!attr) {

@@ -290,10 +290,12 @@ __device__ __forceinline__ void pair_row(const double* si, const double* sj, int
         double dy = yi - sj[r * 3 + 1];
         double dz = zi - sj[r * 3 + 2];
         double R2 = dx * dx + dy * dy + dz * dz + a2;
-        double R = sqrt(R2);
+        // one reciprocal square root serves both R and 1/R
+        double iR = rsqrt(R2);
+        double R = R2 * iR;
         double s, c;
         sincos(k * R, &s, &c);
-        double g = kInv4Pi / R;
+        double g = kInv4Pi * iR;
         cd G = cd{c * g, -s * g};
         if (EK && ek_on) G = G * ek_factor(R, a, k);
 #pragma unroll

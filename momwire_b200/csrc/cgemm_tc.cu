@@ -320,7 +320,7 @@ size_t tc_pack_b_bytes(int64_t k, int64_t n) {
 // planes in `ws` (a_hi | a_lo | b_hi | b_lo, each 1 KB aligned, batch-major).
 mw_status cgemm_tc_update_batched(int64_t m, int64_t n, int64_t k, int batch, const cf* A, int64_t lda, int64_t sa,
                                   const cf* B, int64_t ldb, int64_t sb, cf* C, int64_t ldc, int64_t sc, void* ws,
-                                  size_t ws_bytes, int* err, cudaStream_t st) {
+                                  size_t ws_bytes, int* err, cudaStream_t st, int max_ctas) {
     if (m <= 0 || n <= 0 || k <= 0 || batch <= 0) return MW_OK;
     const int n_mb = (int)((2 * m + TC_M - 1) / TC_M);
     const int n_nb = (int)((n + TC_N - 1) / TC_N);
@@ -354,7 +354,8 @@ mw_status cgemm_tc_update_batched(int64_t m, int64_t n, int64_t k, int batch, co
              batch,    2 * sc, (int64_t)(ab / 4), (int64_t)(bb / 4)};
     const int64_t tiles = (int64_t)n_mb * n_nb * batch;
     MW_REQUIRE(tiles < (1ll << 31), "too many tiles");
-    const int grid = tiles < sms ? (int)tiles : sms;
+    const int cap = (max_ctas > 0 && max_ctas < sms) ? max_ctas : sms;  // CTAs (= SMs) this update may hold
+    const int grid = tiles < cap ? (int)tiles : cap;
     {
         ProfileScope ps(PC_CGEMM_TC, st, 8.0 * (double)m * n * k * batch, 8.0 * 2.0 * (double)m * n * batch);
         cgemm_tc_kernel<<<grid, TC_THREADS, TC_STAGES * TC_STAGE_BYTES, st>>>(P);
@@ -365,8 +366,8 @@ mw_status cgemm_tc_update_batched(int64_t m, int64_t n, int64_t k, int batch, co
 }
 
 mw_status cgemm_tc_update(int64_t m, int64_t n, int64_t k, const cf* A, int64_t lda, const cf* B, int64_t ldb, cf* C,
-                          int64_t ldc, void* ws, size_t ws_bytes, int* err, cudaStream_t st) {
-    return cgemm_tc_update_batched(m, n, k, 1, A, lda, 0, B, ldb, 0, C, ldc, 0, ws, ws_bytes, err, st);
+                          int64_t ldc, void* ws, size_t ws_bytes, int* err, cudaStream_t st, int max_ctas) {
+    return cgemm_tc_update_batched(m, n, k, 1, A, lda, 0, B, ldb, 0, C, ldc, 0, ws, ws_bytes, err, st, max_ctas);
 }
 
 size_t cgemm_tc_workspace_batched(int64_t m, int64_t n, int64_t k, int batch) {
@@ -392,5 +393,5 @@ extern "C" mw_status mw_cgemm_tc_sub(int64_t m, int64_t n, int64_t k, const floa
     MW_REQUIRE(A && B && C && workspace && status, "NULL argument");
     MW_REQUIRE(lda >= m && ldb >= k && ldc >= m, "leading dimension too small");
     return cgemm_tc_update(m, n, k, reinterpret_cast<const cf*>(A), lda, reinterpret_cast<const cf*>(B), ldb,
-                           reinterpret_cast<cf*>(C), ldc, workspace, workspace_bytes, status, as_stream(stream));
+                           reinterpret_cast<cf*>(C), ldc, workspace, workspace_bytes, status, as_stream(stream), 0);
 }

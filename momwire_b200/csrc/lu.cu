@@ -22,7 +22,7 @@ namespace mw {
 
 // tensor-core update (cgemm_tc.cu)
 mw_status cgemm_tc_update(int64_t m, int64_t n, int64_t k, const cf* A, int64_t lda, const cf* B, int64_t ldb, cf* C,
-                          int64_t ldc, void* ws, size_t ws_bytes, int* err, cudaStream_t st);
+                          int64_t ldc, void* ws, size_t ws_bytes, int* err, cudaStream_t st, int max_ctas);
 size_t cgemm_tc_workspace(int64_t m, int64_t n, int64_t k);
 
 constexpr int kNB = 64;         // triangular-solve block (and getrs block)
@@ -705,10 +705,11 @@ constexpr int kMaxPanelGrid = 1024;
 
 // Trailing update C -= A B of a block (type-specific engine).
 struct Updater {
-    // complex64 only: tensor-core workspace
+    // complex64 only: tensor-core workspace and the CTAs an update may hold
     void* tc_ws = nullptr;
     size_t tc_ws_bytes = 0;
     int* tc_err = nullptr;
+    int max_ctas = 0;
 };
 
 static mw_status block_update(const cd* A, int64_t lda, const cd* B, int64_t ldb, cd* C, int64_t ldc, int64_t m,
@@ -718,7 +719,7 @@ static mw_status block_update(const cd* A, int64_t lda, const cd* B, int64_t ldb
 
 static mw_status block_update(const cf* A, int64_t lda, const cf* B, int64_t ldb, cf* C, int64_t ldc, int64_t m,
                               int64_t n, int64_t k, const Updater& u, cudaStream_t st) {
-    return cgemm_tc_update(m, n, k, A, lda, B, ldb, C, ldc, u.tc_ws, u.tc_ws_bytes, u.tc_err, st);
+    return cgemm_tc_update(m, n, k, A, lda, B, ldb, C, ldc, u.tc_ws, u.tc_ws_bytes, u.tc_err, st, u.max_ctas);
 }
 
 // X <- L^-1 X for a unit lower triangle of any order: kNB-row diagonal
@@ -745,13 +746,14 @@ static mw_status trsm_lower_blocked(const T* L, int64_t ldl, T* X, int64_t ldx, 
 // factor the right half, then apply the right half's swaps to the left).
 template <class T>
 static mw_status panel_factor(T* A, int64_t lda, int64_t n, int64_t j0, int jb, int32_t* ipiv, int32_t* info, char* ws,
-                              const Updater& up, cudaStream_t st) {
+                              const Updater& up, cudaStream_t st, int grid_cap = 0) {
     const int sms = panel_sms<T>();
     const int64_t m = n - j0;
     // fewer, fatter CTAs: the per-column grid barrier costs grow with the
     // number of participants, the per-CTA work is small either way
     int64_t want = (m + 127) / 128;  // at least 128 rows per CTA
     int G = (int)(want < sms ? want : sms);
+    if (grid_cap > 0 && G > grid_cap) G = grid_cap;
     if (G > kMaxPanelGrid) G = kMaxPanelGrid;
     if (G < 1) G = 1;
     const int64_t per = (m + G - 1) / G;
@@ -761,14 +763,14 @@ static mw_status panel_factor(T* A, int64_t lda, int64_t n, int64_t j0, int jb, 
     if (smem > kPanelSmemMax || jb > kNB) {
         MW_REQUIRE(jb > 1, "matrix too large for the panel kernel (%lld rows per CTA)", (long long)per);
         const int h = jb / 2;
-        mw_status s = panel_factor<T>(A, lda, n, j0, h, ipiv, info, ws, up, st);
+        mw_status s = panel_factor<T>(A, lda, n, j0, h, ipiv, info, ws, up, st, grid_cap);
         if (s != MW_OK) return s;
         laswp_launch<T>(A, lda, j0 + h, jb - h, ipiv, j0, j0 + h, st);
         trsm_launch<T, false>(A + j0 + j0 * lda, lda, A + j0 + (j0 + h) * lda, lda, h, jb - h, st);
         s = block_update(A + (j0 + h) + j0 * lda, lda, A + j0 + (j0 + h) * lda, lda, A + (j0 + h) + (j0 + h) * lda,
                          lda, m - h, jb - h, h, up, st);
         if (s != MW_OK) return s;
-        s = panel_factor<T>(A, lda, n, j0 + h, jb - h, ipiv, info, ws, up, st);
+        s = panel_factor<T>(A, lda, n, j0 + h, jb - h, ipiv, info, ws, up, st, grid_cap);
         if (s != MW_OK) return s;
         laswp_launch<T>(A, lda, j0, h, ipiv, j0 + h, j0 + jb, st);
         MW_CHECK_CUDA(cudaGetLastError());
@@ -840,6 +842,114 @@ static mw_status getrf(int64_t n, T* A, int64_t lda, int32_t* ipiv, int32_t* inf
     return MW_OK;
 }
 
+// ------------------------------------------------------------ look-ahead
+// Right-looking LU with a look-ahead of one block for the complex64 path.
+// The factorisation splits into two streams:
+//   main   panel j (<= kLaPanelCtas CTAs), then the update of block j+1's
+//          columns only (a narrow GEMM on as many CTAs), so that panel j+1
+//          can start at once; the panels' row swaps on the columns left of
+//          them are applied at the end, in panel order (the trail stream
+//          still reads the previous panel's rows while the next one runs);
+//   trail  the row swaps, triangular solve and tensor-core update of every
+//          column right of block j+1, on the remaining SMs.
+// Panel j waits only for trail j-2 (the last update that touched its
+// columns), so each panel runs under the previous block's big update.  The
+// two streams use separate packed-operand workspaces; events order them.
+constexpr int kLaPanelCtas = 32;
+
+struct AuxStreams {
+    cudaStream_t trail = nullptr;
+    cudaEvent_t ev_main = nullptr;  // main -> trail
+    cudaEvent_t ev_trail[4] = {};   // trail j -> main (ring)
+};
+
+static mw_status aux_streams(AuxStreams** out) {
+    static AuxStreams per_dev[64];
+    int dev = 0;
+    MW_CHECK_CUDA(cudaGetDevice(&dev));
+    MW_REQUIRE(dev >= 0 && dev < 64, "device index out of range");
+    AuxStreams& a = per_dev[dev];
+    if (!a.trail) {
+        MW_CHECK_CUDA(cudaStreamCreateWithFlags(&a.trail, cudaStreamNonBlocking));
+        MW_CHECK_CUDA(cudaEventCreateWithFlags(&a.ev_main, cudaEventDisableTiming));
+        for (auto& e : a.ev_trail) MW_CHECK_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    *out = &a;
+    return MW_OK;
+}
+
+template <class T>
+static mw_status getrf_lookahead(int64_t n, T* A, int64_t lda, int32_t* ipiv, int32_t* info, char* ws,
+                                 const volatile int32_t* cancel, const Updater& up_main, const Updater& up_trail,
+                                 cudaStream_t st) {
+    MW_CHECK_CUDA(cudaMemsetAsync(info, 0, 2 * sizeof(int32_t), st));
+    MW_CHECK_CUDA(cudaMemsetAsync(ws, 0, sizeof(PanelWs), st));
+    {
+        mw_status s0 = trsm_setup<T>();
+        if (s0 != MW_OK) return s0;
+    }
+    AuxStreams* ax = nullptr;
+    {
+        mw_status s0 = aux_streams(&ax);
+        if (s0 != MW_OK) return s0;
+    }
+    cudaStream_t tr = ax->trail;
+    PanelWs* pws = reinterpret_cast<PanelWs*>(ws);
+    const int64_t nb = (n + kOuterNB - 1) / kOuterNB;
+    // the trail stream starts after everything already queued on st
+    MW_CHECK_CUDA(cudaEventRecord(ax->ev_main, st));
+    MW_CHECK_CUDA(cudaStreamWaitEvent(tr, ax->ev_main, 0));
+    for (int64_t j = 0; j < nb; ++j) {
+        if (cancel && *cancel) {
+            // let the trail stream finish what it was given before returning
+            MW_CHECK_CUDA(cudaStreamSynchronize(tr));
+            set_error("factorisation cancelled");
+            return MW_ERR_CANCELLED;
+        }
+        const int64_t j0 = j * kOuterNB;
+        const int jb = (int)((n - j0) < kOuterNB ? (n - j0) : kOuterNB);
+        if (j >= 2) MW_CHECK_CUDA(cudaStreamWaitEvent(st, ax->ev_trail[(j - 2) & 3], 0));
+        mw_status s = panel_factor<T>(A, lda, n, j0, jb, ipiv, info, ws, up_main, st, kLaPanelCtas);
+        if (s != MW_OK) return s;
+        MW_CHECK_CUDA(cudaEventRecord(ax->ev_main, st));
+        // (the swaps of panel j on the columns left of it wait until the
+        // end: trail j-1 may still be reading those rows of panel j-1)
+        const int64_t c1 = j0 + jb;                                       // next block
+        const int64_t jbn = (n - c1) < kOuterNB ? (n - c1) : kOuterNB;
+        const int64_t c2 = c1 + jbn;                                      // rest
+        if (jbn > 0) {
+            if (j >= 1) MW_CHECK_CUDA(cudaStreamWaitEvent(st, ax->ev_trail[(j - 1) & 3], 0));
+            laswp_launch<T>(A, lda, c1, jbn, ipiv, j0, j0 + jb, st);
+            s = trsm_lower_blocked<T>(A + j0 + j0 * lda, lda, A + j0 + c1 * lda, lda, jb, jbn, up_main, st);
+            if (s != MW_OK) return s;
+            s = block_update(A + c1 + j0 * lda, lda, A + j0 + c1 * lda, lda, A + c1 + c1 * lda, lda, n - c1, jbn, jb,
+                             up_main, st);
+            if (s != MW_OK) return s;
+        }
+        // trail: everything right of the next block, after panel j
+        MW_CHECK_CUDA(cudaStreamWaitEvent(tr, ax->ev_main, 0));
+        if (n - c2 > 0) {
+            laswp_launch<T>(A, lda, c2, n - c2, ipiv, j0, j0 + jb, tr);
+            s = trsm_lower_blocked<T>(A + j0 + j0 * lda, lda, A + j0 + c2 * lda, lda, jb, n - c2, up_trail, tr);
+            if (s != MW_OK) return s;
+            s = block_update(A + c1 + j0 * lda, lda, A + j0 + c2 * lda, lda, A + c1 + c2 * lda, lda, n - c1, n - c2,
+                             jb, up_trail, tr);
+            if (s != MW_OK) return s;
+        }
+        MW_CHECK_CUDA(cudaEventRecord(ax->ev_trail[j & 3], tr));
+        MW_CHECK_CUDA(cudaGetLastError());
+    }
+    if (nb > 0) MW_CHECK_CUDA(cudaStreamWaitEvent(st, ax->ev_trail[(nb - 1) & 3], 0));
+    // every panel's row swaps on the columns left of it, in panel order
+    for (int64_t j = 1; j < nb; ++j) {
+        const int64_t j0 = j * kOuterNB;
+        const int jb = (int)((n - j0) < kOuterNB ? (n - j0) : kOuterNB);
+        laswp_launch<T>(A, lda, 0, j0, ipiv, j0, j0 + jb, st);
+    }
+    MW_CHECK_CUDA(cudaMemcpyAsync(info + 1, &pws->err, sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
+    return MW_OK;
+}
+
 // Solve A X = B from the factors (forward with unit L, back with U).
 template <class T>
 static mw_status getrs(int64_t n, int64_t nrhs, const T* LU, int64_t lda, const int32_t* ipiv, T* B, int64_t ldb,
@@ -882,7 +992,10 @@ static size_t panel_ws_bytes() {
 // device status word.
 static size_t cgetrf_ws_bytes(int64_t n, int64_t nrhs_max) {
     int64_t w = n > nrhs_max ? n : nrhs_max;
-    return panel_ws_bytes() + 1024 + cgemm_tc_workspace(n, w, kOuterNB) + 256;
+    // panel slots | trail-stream operand planes | status word | main-stream
+    // operand planes (updates at most kOuterNB columns wide)
+    return panel_ws_bytes() + 1024 + ((cgemm_tc_workspace(n, w, kOuterNB) + 255) & ~size_t(255)) + 256 +
+           cgemm_tc_workspace(n, kOuterNB, kOuterNB) + 1024;
 }
 
 static Updater tc_updater(char* ws, size_t ws_bytes, int64_t n, int64_t nrhs_max) {
@@ -893,6 +1006,20 @@ static Updater tc_updater(char* ws, size_t ws_bytes, int64_t n, int64_t nrhs_max
     u.tc_ws_bytes = cgemm_tc_workspace(n, w, kOuterNB);
     u.tc_err = reinterpret_cast<int*>(ws + p + ((u.tc_ws_bytes + 255) & ~size_t(255)));
     (void)ws_bytes;
+    return u;
+}
+
+// The main-stream updater of the look-ahead factorisation: its own operand
+// planes (after the trail region and the status word), the shared status
+// word, and the panel's CTA budget.
+static Updater tc_updater_main(char* ws, int64_t n, int64_t nrhs_max) {
+    Updater t = tc_updater(ws, 0, n, nrhs_max);
+    Updater u;
+    char* base = static_cast<char*>(t.tc_ws) + ((t.tc_ws_bytes + 255) & ~size_t(255)) + 256;
+    u.tc_ws = reinterpret_cast<void*>((reinterpret_cast<uintptr_t>(base) + 1023) & ~uintptr_t(1023));
+    u.tc_ws_bytes = cgemm_tc_workspace(n, kOuterNB, kOuterNB);
+    u.tc_err = t.tc_err;
+    u.max_ctas = kLaPanelCtas;
     return u;
 }
 
@@ -932,9 +1059,11 @@ extern "C" mw_status mw_cgetrf(int64_t n, float* Ad, int64_t lda, int32_t* ipiv,
     MW_REQUIRE(workspace_bytes >= cgetrf_ws_bytes(n, nrhs_max), "workspace too small");
     char* ws = static_cast<char*>(workspace);
     Updater up = tc_updater(ws, workspace_bytes, n, nrhs_max);
+    Updater up_main = tc_updater_main(ws, n, nrhs_max);
+    up.max_ctas = panel_sms<cf>() - kLaPanelCtas;  // the trail stream leaves the panel its SMs
     cudaStream_t st = as_stream(stream);
     MW_CHECK_CUDA(cudaMemsetAsync(up.tc_err, 0, sizeof(int), st));
-    mw_status s = getrf<cf>(n, reinterpret_cast<cf*>(Ad), lda, ipiv, info, ws, cancel, up, st);
+    mw_status s = getrf_lookahead<cf>(n, reinterpret_cast<cf*>(Ad), lda, ipiv, info, ws, cancel, up_main, up, st);
     if (s != MW_OK) return s;
     // fold a tensor-core timeout into info[1] (barrier timeouts already there)
     MW_CHECK_CUDA(cudaMemcpyAsync(info + 1, up.tc_err, sizeof(int32_t), cudaMemcpyDeviceToDevice, st));

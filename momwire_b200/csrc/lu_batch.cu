@@ -22,7 +22,7 @@ namespace mw {
 
 mw_status cgemm_tc_update_batched(int64_t m, int64_t n, int64_t k, int batch, const cf* A, int64_t lda, int64_t sa,
                                   const cf* B, int64_t ldb, int64_t sb, cf* C, int64_t ldc, int64_t sc, void* ws,
-                                  size_t ws_bytes, int* err, cudaStream_t st);
+                                  size_t ws_bytes, int* err, cudaStream_t st, int max_ctas);
 size_t cgemm_tc_workspace_batched(int64_t m, int64_t n, int64_t k, int batch);
 
 constexpr int kBNB = 16;       // panel width of the batched factorisation
@@ -304,7 +304,7 @@ static mw_status cgetrf_batched(int n, int batch, cf* A, int64_t lda, int64_t st
             count_launch(2);
             mw_status s = cgemm_tc_update_batched(right, right, jb, batch, A + (j0 + jb) + (int64_t)j0 * lda, lda,
                                                   stride, A12, lda, stride, A + (j0 + jb) + (int64_t)(j0 + jb) * lda,
-                                                  lda, stride, w.tc, w.tc_bytes, w.tc_err, st);
+                                                  lda, stride, w.tc, w.tc_bytes, w.tc_err, st, 0);
             if (s != MW_OK) return s;
         }
         MW_CHECK_CUDA(cudaGetLastError());

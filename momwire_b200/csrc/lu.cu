@@ -498,8 +498,13 @@ __global__ void __launch_bounds__(256, 1) zgemm_dmma_kernel(int64_t m, int64_t n
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int wm = warp & 3, wn = warp >> 2;
     const int gid = lane >> 2, tig = lane & 3;
-    const int64_t m0 = blockIdx.x * (int64_t)DM_M, n0 = blockIdx.y * (int64_t)DM_N;
     constexpr int LA = DM_M * DM_K / 256, LB = DM_K * DM_N / 256;
+    // persistent over the output tiles (the grid may be capped to leave SMs
+    // to a concurrent kernel)
+    const int64_t n_mt = (m + DM_M - 1) / DM_M;
+    const int64_t n_tiles = n_mt * ((n + DM_N - 1) / DM_N);
+    for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+    const int64_t m0 = (tile % n_mt) * DM_M, n0 = (tile / n_mt) * DM_N;
     double cr[4][4][2], ci[4][4][2];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
@@ -600,6 +605,7 @@ __global__ void __launch_bounds__(256, 1) zgemm_dmma_kernel(int64_t m, int64_t n
                 *cp = v;
             }
     }
+    }  // tiles
 }
 
 mw_status zgemm_launch_simt(bool ta, bool tb, int64_t m, int64_t n, int64_t k, cd alpha, const cd* A, int64_t lda,
@@ -610,7 +616,7 @@ mw_status zgemm_launch_simt(bool ta, bool tb, int64_t m, int64_t n, int64_t k, c
 // K, epilogue-bound), the DMMA kernel on long-K products such as the
 // refinement residual Z X (14.4 vs 9.6 TFLOP/s).
 mw_status zgemm_launch(bool ta, bool tb, int64_t m, int64_t n, int64_t k, cd alpha, const cd* A, int64_t lda,
-                       const cd* B, int64_t ldb, cd beta, cd* C, int64_t ldc, cudaStream_t st) {
+                       const cd* B, int64_t ldb, cd beta, cd* C, int64_t ldc, cudaStream_t st, int max_ctas) {
     if (m <= 0 || n <= 0) return MW_OK;
     if (k < 128) return zgemm_launch_simt(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, st);
     {
@@ -626,7 +632,10 @@ mw_status zgemm_launch(bool ta, bool tb, int64_t m, int64_t n, int64_t k, cd alp
                                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDmmaSmem));
             attr = true;
         }
-        dim3 grid((unsigned)((m + DM_M - 1) / DM_M), (unsigned)((n + DM_N - 1) / DM_N));
+        // one CTA per SM (register-bound); a cap leaves SMs to other work
+        int64_t tiles = ((m + DM_M - 1) / DM_M) * ((n + DM_N - 1) / DM_N);
+        if (max_ctas > 0 && tiles > max_ctas) tiles = max_ctas;
+        dim3 grid((unsigned)tiles);
         ProfileScope ps(PC_ZGEMM, st, 8.0 * (double)m * n * k, 16.0 * ((double)m * k + (double)k * n + 2.0 * m * n));
         if (!ta && !tb)
             zgemm_dmma_kernel<false, false><<<grid, 256, kDmmaSmem, st>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
@@ -713,8 +722,8 @@ struct Updater {
 };
 
 static mw_status block_update(const cd* A, int64_t lda, const cd* B, int64_t ldb, cd* C, int64_t ldc, int64_t m,
-                              int64_t n, int64_t k, const Updater&, cudaStream_t st) {
-    return zgemm_launch(false, false, m, n, k, cd{-1.0, 0.0}, A, lda, B, ldb, cd{1.0, 0.0}, C, ldc, st);
+                              int64_t n, int64_t k, const Updater& u, cudaStream_t st) {
+    return zgemm_launch(false, false, m, n, k, cd{-1.0, 0.0}, A, lda, B, ldb, cd{1.0, 0.0}, C, ldc, st, u.max_ctas);
 }
 
 static mw_status block_update(const cf* A, int64_t lda, const cf* B, int64_t ldb, cf* C, int64_t ldc, int64_t m,
@@ -843,7 +852,7 @@ static mw_status getrf(int64_t n, T* A, int64_t lda, int32_t* ipiv, int32_t* inf
 }
 
 // ------------------------------------------------------------ look-ahead
-// Right-looking LU with a look-ahead of one block for the complex64 path.
+// Right-looking LU with a look-ahead of one block (both precisions).
 // The factorisation splits into two streams:
 //   main   panel j (<= kLaPanelCtas CTAs), then the update of block j+1's
 //          columns only (a narrow GEMM on as many CTAs), so that panel j+1
@@ -1037,8 +1046,11 @@ extern "C" mw_status mw_zgetrf(int64_t n, double* Ad, int64_t lda, int32_t* ipiv
     MW_REQUIRE(n >= 0 && lda >= (n > 0 ? n : 1), "bad n/lda");
     MW_REQUIRE(Ad && ipiv && info && workspace, "NULL argument");
     MW_REQUIRE(workspace_bytes >= mw_getrf_workspace_size(n), "workspace too small");
-    return getrf<cd>(n, reinterpret_cast<cd*>(Ad), lda, ipiv, info, static_cast<char*>(workspace), cancel, Updater{},
-                     as_stream(stream));
+    Updater up_main, up_trail;
+    up_main.max_ctas = kLaPanelCtas;
+    up_trail.max_ctas = panel_sms<cd>() - kLaPanelCtas;
+    return getrf_lookahead<cd>(n, reinterpret_cast<cd*>(Ad), lda, ipiv, info, static_cast<char*>(workspace), cancel,
+                               up_main, up_trail, as_stream(stream));
 }
 
 extern "C" mw_status mw_zgetrs(int64_t n, int64_t nrhs, const double* LUd, int64_t lda, const int32_t* ipiv,
@@ -1089,5 +1101,5 @@ extern "C" mw_status mw_zgemm(int32_t transA, int32_t transB, int64_t m, int64_t
     MW_REQUIRE(A && B && C, "NULL argument");
     return zgemm_launch(transA != 0, transB != 0, m, n, k, cd{alpha_re, alpha_im}, reinterpret_cast<const cd*>(A),
                         lda, reinterpret_cast<const cd*>(B), ldb, cd{beta_re, beta_im}, reinterpret_cast<cd*>(C), ldc,
-                        as_stream(stream));
+                        as_stream(stream), 0);
 }

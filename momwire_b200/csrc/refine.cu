@@ -15,7 +15,7 @@
 
 namespace mw {
 mw_status zgemm_launch(bool ta, bool tb, int64_t m, int64_t n, int64_t k, cd alpha, const cd* A, int64_t lda,
-                       const cd* B, int64_t ldb, cd beta, cd* C, int64_t ldc, cudaStream_t st);
+                       const cd* B, int64_t ldb, cd beta, cd* C, int64_t ldc, cudaStream_t st, int max_ctas);
 
 __global__ void to_c64_kernel(const cd* __restrict__ src, int64_t lds, cf* __restrict__ dst, int64_t ldd, int64_t n,
                               int64_t ncol) {
@@ -167,7 +167,7 @@ extern "C" mw_status mw_zgesv_mixed(int64_t n, int64_t nrhs, const double* Z, in
         // R = B - Z X   (FP64)
         copy_c128_kernel<<<grid_for(tot), 256, 0, st>>>(Bc, ldb, R, n, n, nrhs);
         count_launch();
-        s = zgemm_launch(false, false, n, nrhs, n, cd{-1.0, 0.0}, Zc, ldz, Xc, ldx, cd{1.0, 0.0}, R, n, st);
+        s = zgemm_launch(false, false, n, nrhs, n, cd{-1.0, 0.0}, Zc, ldz, Xc, ldx, cd{1.0, 0.0}, R, n, st, 0);
         if (s != MW_OK) return s;
     }
     if (iterations) *iterations = it;

@@ -55,7 +55,7 @@ def parse():
     ap.add_argument("--micro", default=None, choices=["cgemm_tc"], help="kernel microbenchmark instead")
     ap.add_argument("--m", type=int, default=8192)
     ap.add_argument("--k", type=int, default=64)
-    ap.add_argument("--workload", default="array", choices=["array", "yagi_sweep", "somm"])
+    ap.add_argument("--workload", default="array", choices=["array", "yagi_sweep", "somm", "plate"])
     ap.add_argument("--n-struct", type=int, default=512)
     ap.add_argument("--fp64-structs", type=int, default=4)
     ap.add_argument("--fp64-kstep", type=int, default=4)
@@ -481,6 +481,50 @@ def run_somm(args):
                       "timing": "wall clock per cold structure, host + device"}), flush=True)
 
 
+def run_plate(args):
+    """The combined large case: 64x64-cell wire-grid plate (2 segments per
+    wire) at 2 m over a Sommerfeld ground (13, 5e-3) with a 10 m monopole
+    from its centre, 14.1 MHz, 8 ports (33,290 unknowns, 4,218 KCL rows).
+    One warm-up and --steps timed solves per precision through the public
+    API (device events around compute_port_solution), and the drive-point
+    impedances of the mixed path against the FP64 path."""
+    import numpy as np
+    import torch
+
+    import momwire_b200
+    from momwire_b200 import _lib
+
+    sys.path.insert(0, str(ROOT / "tests" / "golden"))
+    from cases import wire_grid_plate
+
+    kw = wire_grid_plate()
+    stream = torch.cuda.current_stream()
+    out, ys = {}, {}
+    for prec in ("fp64", "mixed"):
+        s = momwire_b200.BSplineSolver(**kw, precision=prec)
+        s.compute_port_solution()
+        torch.cuda.synchronize()
+        _lib.profile_enable(True)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(args.steps):
+            sol = s.compute_port_solution()
+        b.record(stream)
+        torch.cuda.synchronize()
+        prof = _lib.profile_read()
+        _lib.profile_enable(False)
+        out[prec] = {"ms_per_step": a.elapsed_time(b) / args.steps,
+                     "kernels_ms": {k: round(v[1] / args.steps, 1) for k, v in prof.items()}}
+        ys[prec] = sol.y
+    z64, zmx = 1.0 / np.diag(ys["fp64"]), 1.0 / np.diag(ys["mixed"])
+    print(json.dumps({"workload": "plate64_sommerfeld_33290_unknowns", "n_unknowns": int(s._basis().n), "ports": 8,
+                      "fp64": out["fp64"], "mixed": out["mixed"],
+                      "speedup_mixed_vs_fp64": out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"],
+                      "max_rel_dZin_mixed_vs_fp64": float(np.max(np.abs(zmx - z64) / np.abs(z64))),
+                      "timing": "device events around compute_port_solution (host tables, h2d, d2h included)"}),
+          flush=True)
+
+
 def run_sweep(args):
     """The batched-sweep workload: seeded Yagis, 64 frequencies each,
     25.2-30.8 MHz.  Mixed + batched over all structures (device-timed per
@@ -542,6 +586,9 @@ def main():
         return
     if args.workload == "somm":
         run_somm(args)
+        return
+    if args.workload == "plate":
+        run_plate(args)
         return
     from momwire_b200.workloads import dipole_array
 

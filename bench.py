@@ -49,6 +49,7 @@ def parse():
     ap.add_argument("--fp64-steps", type=int, default=2, help="steps of the FP64 path timed beside a mixed run")
     ap.add_argument("--sweep-structs", type=int, default=16,
                     help="Yagis per rank in the sweep part of the line (0: none)")
+    ap.add_argument("--sweep-workers", type=int, default=4, help="host threads (one CUDA stream each) per rank")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--nx", type=int, default=16)
@@ -416,7 +417,7 @@ def run_sweep_part(args, rank, world, local, pg):
         pg.barrier()
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     a.record(stream)
-    local_y = sweep.solve_shard(structs, ks, parts[rank], fn)
+    local_y = sweep.solve_shard(structs, ks, parts[rank], fn, workers=args.sweep_workers, device=local)
     b.record(stream)
     torch.cuda.synchronize()
     ms = a.elapsed_time(b)
@@ -426,7 +427,8 @@ def run_sweep_part(args, rank, world, local, pg):
         ms = float(t.item())
     ys = sweep.gather(local_y)
     out = {"workload": f"yagi_sweep_{len(structs)}x64", "solves": len(structs) * len(ks),
-           "pts_per_s": len(structs) * len(ks) / (ms / 1e3), "ms": ms, "sharding": f"LPT x{world}"}
+           "pts_per_s": len(structs) * len(ks) / (ms / 1e3), "ms": ms, "sharding": f"LPT x{world}",
+           "workers_per_rank": args.sweep_workers}
     if rank == 0:
         sub = ks[::8]
         f_ms, n64, err = 0.0, 0, 0.0

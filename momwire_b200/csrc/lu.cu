@@ -872,8 +872,10 @@ struct AuxStreams {
     cudaEvent_t ev_trail[4] = {};   // trail j -> main (ring)
 };
 
+// one set per host thread and device: concurrent factorisations from
+// different threads never share the trail stream or its events
 static mw_status aux_streams(AuxStreams** out) {
-    static AuxStreams per_dev[64];
+    static thread_local AuxStreams per_dev[64];
     int dev = 0;
     MW_CHECK_CUDA(cudaGetDevice(&dev));
     MW_REQUIRE(dev >= 0 && dev < 64, "device index out of range");

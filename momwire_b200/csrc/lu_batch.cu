@@ -398,11 +398,13 @@ extern "C" mw_status mw_zgesv_mixed_batched(int32_t n, int32_t nrhs, int32_t bat
             count_launch();
         }
         MW_CHECK_CUDA(cudaMemcpyAsync(hn.data(), w.norms, sizeof(double) * 2 * batch, cudaMemcpyDeviceToHost, st));
-        if (it == 0) MW_CHECK_CUDA(cudaMemcpyAsync(hinfo.data(), info, sizeof(int32_t) * batch, cudaMemcpyDeviceToHost, st));
+        int tce = 0;
+        if (it == 0) {
+            MW_CHECK_CUDA(cudaMemcpyAsync(hinfo.data(), info, sizeof(int32_t) * batch, cudaMemcpyDeviceToHost, st));
+            MW_CHECK_CUDA(cudaMemcpyAsync(&tce, w.tc_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+        }
         MW_CHECK_CUDA(cudaStreamSynchronize(st));
         if (it == 0) {
-            int tce = 0;
-            MW_CHECK_CUDA(cudaMemcpy(&tce, w.tc_err, sizeof(int), cudaMemcpyDeviceToHost));
             if (tce != 0) {
                 set_error("batched factorisation: a bounded device wait timed out");
                 return MW_ERR_TIMEOUT;

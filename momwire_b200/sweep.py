@@ -56,9 +56,37 @@ def structure_cost(kw):
     return float(n) ** 3
 
 
-def solve_shard(structs, ks, indices, solve_fn):
-    """{structure index: solve_fn(kw, ks)} over this rank's indices."""
-    return {i: solve_fn(structs[i], ks) for i in indices}
+def solve_shard(structs, ks, indices, solve_fn, workers=1, device=None):
+    """{structure index: solve_fn(kw, ks)} over this rank's indices.
+
+    With workers > 1 the structures run on that many host threads, each
+    issuing to its own CUDA stream, so that one structure's host work and
+    small kernels overlap another's (a batched solve of one structure holds
+    only a CTA per matrix during its panels)."""
+    if workers <= 1:
+        return {i: solve_fn(structs[i], ks) for i in indices}
+    import concurrent.futures as cf
+
+    import torch
+
+    dev = torch.device("cuda", device if device is not None else torch.cuda.current_device())
+    streams = [torch.cuda.Stream(device=dev) for _ in range(workers)]
+    slot = {}
+
+    def run(i):
+        import threading
+
+        tid = threading.get_ident()
+        if tid not in slot:
+            slot[tid] = streams[len(slot) % workers]
+        with torch.cuda.device(dev), torch.cuda.stream(slot[tid]):
+            out = solve_fn(structs[i], ks)
+            torch.cuda.current_stream().synchronize()
+        return i, out
+
+    with cf.ThreadPoolExecutor(max_workers=workers) as ex:
+        res = dict(ex.map(run, indices))
+    return {i: res[i] for i in indices}
 
 
 def gather(local, group=None):

@@ -49,7 +49,7 @@ def parse():
     ap.add_argument("--fp64-steps", type=int, default=2, help="steps of the FP64 path timed beside a mixed run")
     ap.add_argument("--sweep-structs", type=int, default=16,
                     help="Yagis per rank in the sweep part of the line (0: none)")
-    ap.add_argument("--sweep-workers", type=int, default=4, help="host threads (one CUDA stream each) per rank")
+    ap.add_argument("--sweep-workers", type=int, default=8, help="host threads (one CUDA stream each) per rank")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--nx", type=int, default=16)

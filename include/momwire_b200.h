@@ -341,11 +341,12 @@ mw_status mw_fill_z_batch(const mw_segments* seg, const mw_basis* basis,
  * rule of mw_zgesv_mixed applied to every matrix of the batch.  X is batch x n x nrhs,
  * contiguous.  The reference's counterpart is the stacked complex128
  * numpy.linalg.solve of _solve_with_kcl_swept_ports (bspline.py:3017).
- * Strides count complex elements.  n <= 1600 (the complex64 panel of 16
- * columns, 128 n bytes, must fit in 200 KB of shared memory).
+ * Strides count complex elements.  panel_width: columns per batched panel
+ * (8, 16 or 32; 0 = 16) -- the n x panel_width complex64 panel must fit in
+ * 200 KB of shared memory (n <= 1600 at 16 columns).
  */
 size_t mw_zgesv_mixed_batched_workspace_size(int32_t n, int32_t nrhs, int32_t batch);
-mw_status mw_zgesv_mixed_batched(int32_t n, int32_t nrhs, int32_t batch,
+mw_status mw_zgesv_mixed_batched(int32_t n, int32_t nrhs, int32_t batch, int32_t panel_width,
                                  const double* Z, int64_t ldz, int64_t z_stride,
                                  float* Z32, int64_t ldz32, int64_t z32_stride,
                                  int32_t* ipiv, int32_t* info, const double* B,

@@ -132,8 +132,8 @@ _SIGS = {
     "mw_fill_z_batch": (i32, [C.POINTER(Segments), C.POINTER(BasisT), C.POINTER(Edges), i32, vp, vp, f64, f64, i32,
                               i32, f64, i32, vp, vp, i64, i64, vp, i64, i64, vp]),
     "mw_zgesv_mixed_batched_workspace_size": (sz, [i32, i32, i32]),
-    "mw_zgesv_mixed_batched": (i32, [i32, i32, i32, vp, i64, i64, vp, i64, i64, vp, vp, vp, i64, i64, vp, f64, i32,
-                                     vp, sz, C.POINTER(i32), C.POINTER(f64), vp]),
+    "mw_zgesv_mixed_batched": (i32, [i32, i32, i32, i32, vp, i64, i64, vp, i64, i64, vp, vp, vp, i64, i64, vp, f64,
+                                     i32, vp, sz, C.POINTER(i32), C.POINTER(f64), vp]),
     "mw_getrf_workspace_size": (sz, [i64]),
     "mw_zgetrf": (i32, [i64, vp, i64, vp, vp, vp, sz, vp, vp]),
     "mw_zgetrs": (i32, [i64, i64, vp, i64, vp, vp, i64, vp]),

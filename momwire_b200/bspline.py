@@ -30,6 +30,7 @@ import scipy.sparse
 
 from . import _lib
 from . import _tables as T
+from . import autotune
 from . import sommerfeld as somm
 from . import surrogate as sur
 from ._port_solution import PortSolution
@@ -1033,10 +1034,39 @@ class BSplineSolver:
                   n * n, stream)
         return Z, Z32
 
+    def _batched_panel_width(self, ks):
+        """Columns per batched panel step for this order: the autotuner's
+        cached choice for (n bucket, degree, ground), timed on a short sweep
+        of this structure the first time the bucket is met."""
+        if getattr(self, "_panel_width", None):
+            return self._panel_width
+        torch = _torch()
+        ground = "free" if self.ground_z is None else "pec"
+        ks = np.asarray(ks, dtype=np.float64)
+        probe = np.linspace(ks.min(), ks.max(), min(len(ks), 16))
+
+        def time_width(w):
+            self._panel_width = w
+            try:
+                self._swept_batched(probe)  # warm-up
+                st = torch.cuda.current_stream(self._torch_device())
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(st)
+                self._swept_batched(probe)
+                b.record(st)
+                b.synchronize()
+                return a.elapsed_time(b)
+            finally:
+                self._panel_width = None
+
+        self._panel_width = autotune.choose(self._basis().n, self.degree, ground, time_width)
+        return self._panel_width
+
     def _swept_batched(self, k_array, mem_budget_bytes=16 << 30):
         """Chunked batched sweep: per chunk of frequencies, one batched fill
         (Z in complex128 and complex64) and one batched mixed solve with FP64
         refinement; Y_k = B^T X_k."""
+        pw = self._batched_panel_width(k_array)
         torch = _torch()
         dev = self._torch_device()
         dt = self._dev_tables()
@@ -1061,7 +1091,8 @@ class BSplineSolver:
             wsb = lib.mw_zgesv_mixed_batched_workspace_size(n, n_p, nk)
             ws = torch.empty(wsb, dtype=torch.uint8, device=dev)
             it, corr = C.c_int32(0), C.c_double(0.0)
-            _lib.call("mw_zgesv_mixed_batched", n, n_p, nk, Z.data_ptr(), n, n * n, Z32.data_ptr(), n, n * n,
+            _lib.call("mw_zgesv_mixed_batched", n, n_p, nk, int(pw), Z.data_ptr(), n,
+                      n * n, Z32.data_ptr(), n, n * n,
                       ipiv.data_ptr(), info.data_ptr(), Bd.data_ptr(), n, 0, X.data_ptr(), float(self.mixed_tol),
                       int(self.mixed_max_iter), ws.data_ptr(), wsb, C.byref(it), C.byref(corr), st)
             iters.append(int(it.value))

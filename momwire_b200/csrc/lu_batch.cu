@@ -5,7 +5,7 @@
 // numpy.linalg.solve over the k axis) factorises one small complex matrix per
 // frequency.  Here a whole batch of same-order matrices (one structure at
 // many frequencies) is factorised together in complex64:
-//   panel   one CTA per matrix, the panel (rows j0..n, 16 columns) resident
+//   panel   one CTA per matrix, the panel (rows j0..n, 8-32 columns) resident
 //           in shared memory; pivot search, swap, scale and rank-1 update
 //           synchronise with __syncthreads only;
 //   update  the batched tcgen05 3xTF32 update of cgemm_tc.cu over all
@@ -25,7 +25,8 @@ mw_status cgemm_tc_update_batched(int64_t m, int64_t n, int64_t k, int batch, co
                                   size_t ws_bytes, int* err, cudaStream_t st, int max_ctas);
 size_t cgemm_tc_workspace_batched(int64_t m, int64_t n, int64_t k, int batch);
 
-constexpr int kBNB = 16;       // panel width of the batched factorisation
+constexpr int kBNB = 16;       // default panel width of the batched factorisation
+constexpr int kBNBMax = 32;    // widest panel the workspace is sized for
 constexpr int kBSB = 64;       // block size of the batched triangular solves
 constexpr int kBThreads = 256;
 
@@ -92,12 +93,11 @@ __global__ void __launch_bounds__(kBThreads) panel1_kernel(cf* A, int64_t lda, i
             continue;
         }
         const cf inv = cdiv(cf{1.f, 0.f}, slab[jj * m + jj]);
-        for (int i = jj + 1 + tid; i < m; i += blockDim.x) slab[jj * m + i] = slab[jj * m + i] * inv;
-        __syncthreads();
-        const int nr = m - jj - 1, nc = jb - jj - 1;
-        for (int q = tid; q < nr * nc; q += blockDim.x) {
-            const int i = jj + 1 + q % nr, x = jj + 1 + q / nr;
-            slab[x * m + i] = slab[x * m + i] - slab[jj * m + i] * slab[x * m + jj];
+        // rows in the threads: scale the multiplier and update its row
+        for (int i = jj + 1 + tid; i < m; i += blockDim.x) {
+            const cf l = slab[jj * m + i] * inv;
+            slab[jj * m + i] = l;
+            for (int x = jj + 1; x < jb; ++x) slab[x * m + i] = slab[x * m + i] - l * slab[x * m + jj];
         }
         __syncthreads();
     }
@@ -251,7 +251,7 @@ struct BatchWs {
 };
 
 static size_t batch_ws_bytes(int n, int nrhs, int batch) {
-    return al256(cgemm_tc_workspace_batched(n, n, kBNB, batch)) + 256 + al256((size_t)batch * n * nrhs * 16) +
+    return al256(cgemm_tc_workspace_batched(n, n, kBNBMax, batch)) + 256 + al256((size_t)batch * n * nrhs * 16) +
            al256((size_t)batch * n * nrhs * 8) + al256((size_t)batch * 16);
 }
 
@@ -259,7 +259,7 @@ static BatchWs batch_ws(void* ws, int n, int nrhs, int batch) {
     char* w = static_cast<char*>(ws);
     BatchWs b;
     b.tc = w;
-    b.tc_bytes = cgemm_tc_workspace_batched(n, n, kBNB, batch);
+    b.tc_bytes = cgemm_tc_workspace_batched(n, n, kBNBMax, batch);
     w += al256(b.tc_bytes);
     b.tc_err = reinterpret_cast<int*>(w);
     w += 256;
@@ -272,16 +272,16 @@ static BatchWs batch_ws(void* ws, int n, int nrhs, int batch) {
 }
 
 static mw_status cgetrf_batched(int n, int batch, cf* A, int64_t lda, int64_t stride, int32_t* ipiv, int32_t* info,
-                                const BatchWs& w, cudaStream_t st) {
-    const size_t slab_max = (size_t)n * kBNB * sizeof(cf);
-    MW_REQUIRE(slab_max <= 200 * 1024, "order %d too large for the batched panel", n);
+                                const BatchWs& w, int pw, cudaStream_t st) {
+    const size_t slab_max = (size_t)n * pw * sizeof(cf);
+    MW_REQUIRE(slab_max <= 200 * 1024, "order %d too large for a batched panel of %d columns", n, pw);
     static bool attr = false;
     if (!attr) {
         MW_CHECK_CUDA(cudaFuncSetAttribute(panel1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
         attr = true;
     }
-    for (int j0 = 0; j0 < n; j0 += kBNB) {
-        const int jb = (n - j0) < kBNB ? (n - j0) : kBNB;
+    for (int j0 = 0; j0 < n; j0 += pw) {
+        const int jb = (n - j0) < pw ? (n - j0) : pw;
         {
             ProfileScope ps(PC_PANEL, st, 4.0 * (double)(n - j0) * jb * jb * batch);
             panel1_kernel<<<batch, kBThreads, (size_t)(n - j0) * jb * sizeof(cf), st>>>(A, lda, stride, n, j0, jb,
@@ -353,7 +353,8 @@ extern "C" size_t mw_zgesv_mixed_batched_workspace_size(int32_t n, int32_t nrhs,
     return batch_ws_bytes(n, nrhs, batch);
 }
 
-extern "C" mw_status mw_zgesv_mixed_batched(int32_t n, int32_t nrhs, int32_t batch, const double* Z, int64_t ldz,
+extern "C" mw_status mw_zgesv_mixed_batched(int32_t n, int32_t nrhs, int32_t batch, int32_t panel_width,
+                                            const double* Z, int64_t ldz,
                                             int64_t z_stride, float* Z32, int64_t ldz32, int64_t z32_stride,
                                             int32_t* ipiv, int32_t* info, const double* B, int64_t ldb,
                                             int64_t b_stride, double* X, double tol, int32_t max_iter, void* workspace,
@@ -368,7 +369,9 @@ extern "C" mw_status mw_zgesv_mixed_batched(int32_t n, int32_t nrhs, int32_t bat
     MW_CHECK_CUDA(cudaMemsetAsync(info, 0, sizeof(int32_t) * batch, st));
     MW_CHECK_CUDA(cudaMemsetAsync(w.tc_err, 0, sizeof(int), st));
     cf* Z32c = reinterpret_cast<cf*>(Z32);
-    mw_status s = cgetrf_batched(n, batch, Z32c, ldz32, z32_stride, ipiv, info, w, st);
+    const int pw = panel_width > 0 ? panel_width : kBNB;
+    MW_REQUIRE(pw == 8 || pw == 16 || pw == 32, "panel_width must be 8, 16 or 32 (got %d)", pw);
+    mw_status s = cgetrf_batched(n, batch, Z32c, ldz32, z32_stride, ipiv, info, w, pw, st);
     if (s != MW_OK) return s;
     const int64_t per = (int64_t)n * nrhs;
     const int64_t tot = per * batch;

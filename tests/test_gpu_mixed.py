@@ -118,3 +118,18 @@ def test_mixed_array16x16(cuda_device):
     assert zin_err <= 1e-6, zin_err
     assert rel_err(sol.y, g["y"]) < 1e-6
     assert s.last_refinement["iterations"] <= 4
+
+
+@pytest.mark.parametrize("width", [8, 16, 32])
+def test_batched_sweep_panel_widths(width, cuda_device):
+    """Every panel width the autotuner may pick gives the same sweep."""
+    kw = CASES["d2_pec"]()
+    s64 = momwire_b200.BSplineSolver(**kw)
+    ks = np.linspace(0.9, 1.1, 5) * s64.k
+    y64 = s64.compute_y_matrix_swept(ks)
+    smx = momwire_b200.BSplineSolver(**kw, precision="mixed")
+    smx._panel_width = width
+    ymx = smx.compute_y_matrix_swept(ks)
+    for i in range(len(ks)):
+        z64, zmx = _zin(y64[i]), _zin(ymx[i])
+        assert np.max(np.abs(zmx - z64) / np.abs(z64)) <= 1e-6

@@ -15,6 +15,7 @@
 //             complex64: tcgen05 tensor cores, 3xTF32 (cgemm_tc.cu).
 // Pivot choice follows LAPACK's izamax: max |re| + |im|, first index wins.
 #include <cstdio>
+#include <type_traits>
 
 #include "common.cuh"
 
@@ -246,6 +247,152 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel(PanelArgs P) {
                 for (int x = 0; x < jb; ++x) slab[x * rcap + i] = s_cur[x];
             if (!apply) continue;
             const T l = slab[jj * rcap + i] * inv;
+            slab[jj * rcap + i] = l;
+            for (int x = jj + 1; x < jb; ++x) slab[x * rcap + i] = slab[x * rcap + i] - l * s_piv[x];
+        }
+        __syncthreads();
+    }
+    for (int idx = tid; idx < R * jb; idx += blockDim.x) {
+        int i = idx % R, x = idx / R;
+        A[(r0 + i) + (P.j0 + x) * lda] = slab[x * rcap + i];
+    }
+}
+
+// Complex64 panel with one exchange word per CTA and column.  Each CTA
+// publishes its candidate as a single 64-bit word
+//     [seq 8 | float(|re|+|im|) bits 32 | 2^24-1 - (row - j0) 24]
+// with a release store after its candidate row; every CTA's warp 0 polls
+// the G words (acquire), keeps the largest key -- largest value, then
+// smallest row, LAPACK's rule at float resolution -- and fetches that row.
+// Two dependent L2 round trips per column, no atomics.  The key's float
+// rounding can only change the choice between candidates within one float
+// ulp of each other, which the FP64 refinement of the mixed path absorbs.
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__global__ void __launch_bounds__(kPanelThreads) panel_kernel_c64(PanelArgs P) {
+    extern __shared__ __align__(16) unsigned char panel_smem[];
+    cf* slab = reinterpret_cast<cf*>(panel_smem);
+    __shared__ double s_v[kPanelThreads / 32];
+    __shared__ int64_t s_i[kPanelThreads / 32];
+    __shared__ cf s_piv[kPanelMaxJb];
+    __shared__ cf s_cur[kPanelMaxJb];
+    __shared__ int64_t s_p;
+    __shared__ int s_zero, s_ok;
+
+    const int G = gridDim.x;
+    const int g = blockIdx.x;
+    const int tid = threadIdx.x;
+    const int64_t m = P.n - P.j0;
+    const int64_t per = (m + G - 1) / G;
+    const int64_t r0 = P.j0 + g * per;
+    const int64_t r1 = min(P.n, r0 + per);
+    const int R = (int)max((int64_t)0, r1 - r0);
+    const int rcap = P.rcap;
+    const int jb = P.jb;
+    cf* A = static_cast<cf*>(P.A);
+    cf* slot_row = static_cast<cf*>(P.slot_row);
+    cf* cur_row = static_cast<cf*>(P.cur_row);
+    unsigned long long* words = reinterpret_cast<unsigned long long*>(P.slot_idx);  // [2][G]
+    const int64_t lda = P.lda;
+
+    for (int idx = tid; idx < R * jb; idx += blockDim.x) {
+        int i = idx % R, x = idx / R;
+        slab[x * rcap + i] = A[(r0 + i) + (P.j0 + x) * lda];
+    }
+    __syncthreads();
+
+    for (int jj = 0; jj < jb; ++jj) {
+        const int64_t c = P.j0 + jj;
+        const int buf = jj & 1;
+        // 1..255, never the 0 the slots are cleared to; a stale word in a
+        // slot is at most jb + 2 columns old, so it never matches
+        const unsigned long long seq = (unsigned long long)((c + 1) % 255 + 1);
+        const int i0 = (int)max((int64_t)0, c - r0);
+        double best = -1.0;
+        int64_t bidx = INT64_MAX;
+        for (int i = i0 + tid; i < R; i += blockDim.x) argmax_merge(best, bidx, cabs1(slab[jj * rcap + i]), r0 + i);
+        block_argmax(best, bidx, s_v, s_i);
+        if (bidx != INT64_MAX)
+            for (int x = tid; x < jb; x += blockDim.x)
+                slot_row[((size_t)buf * G + g) * kPanelMaxJb + x] = slab[x * rcap + (int)(bidx - r0)];
+        if (c >= r0 && c < r1)
+            for (int x = tid; x < jb; x += blockDim.x) cur_row[buf * kPanelMaxJb + x] = slab[x * rcap + (int)(c - r0)];
+        __syncthreads();
+        if (tid == 0) {
+            unsigned long long key = 0;  // no candidate: loses to every row
+            if (bidx != INT64_MAX) {
+                const unsigned int fb = __float_as_uint((float)best);
+                key = ((unsigned long long)fb << 24) | (unsigned long long)(0xFFFFFFll - (bidx - P.j0));
+            }
+            st_release_u64(words + (size_t)buf * G + g, (seq << 56) | key);
+        }
+        if (tid < 32) {
+            unsigned long long bk = 0;
+            int bg = 0, ok = 1;
+            for (int x = tid; x < G; x += 32) {
+                unsigned long long w;
+                long long spins = 0;
+                while (((w = ld_acquire_u64(words + (size_t)buf * G + x)) >> 56) != seq) {
+                    if ((++spins & 1023) == 0 && (spins > (1ll << 26) || *(volatile int*)&P.ws->err)) {
+                        atomicExch(&P.ws->err, MW_ERR_TIMEOUT);
+                        ok = 0;
+                        break;
+                    }
+                }
+                if (!ok) break;
+                const unsigned long long key = w & 0x00FFFFFFFFFFFFFFull;
+                if (key > bk) {
+                    bk = key;
+                    bg = x;
+                }
+            }
+            ok = __all_sync(0xffffffffu, ok);
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                const unsigned long long k2 = __shfl_xor_sync(0xffffffffu, bk, off);
+                const int g2 = __shfl_xor_sync(0xffffffffu, bg, off);
+                if (k2 > bk || (k2 == bk && g2 < bg)) {
+                    bk = k2;
+                    bg = g2;
+                }
+            }
+            const int64_t p = P.j0 + (0xFFFFFFll - (int64_t)(bk & 0xFFFFFFull));
+            if (tid == 0) {
+                s_ok = ok;
+                s_p = p;
+                s_zero = ((bk >> 24) & 0xFFFFFFFFull) == 0ull;  // |pivot| == 0
+                if (g == 0 && ok) P.ipiv[c] = (int32_t)(p + 1);
+            }
+            if (ok)
+                for (int x = tid; x < jb; x += 32) {
+                    s_piv[x] = ldcg_c(slot_row + ((size_t)buf * G + bg) * kPanelMaxJb + x);
+                    s_cur[x] = ldcg_c(cur_row + buf * kPanelMaxJb + x);
+                }
+        }
+        __syncthreads();
+        if (!s_ok) return;  // a wait gave up: the error word is set
+        const int64_t p = s_p;
+        if (s_zero && g == 0 && tid == 0 && P.info[0] == 0) P.info[0] = (int32_t)(c + 1);
+        const bool apply = !s_zero;
+        const cf inv = apply ? cdiv(cone<cf>(), s_piv[jj]) : cone<cf>();
+        for (int i = i0 + tid; i < R; i += blockDim.x) {
+            const int64_t gr = r0 + i;
+            if (gr == c) {
+                if (p != c)
+                    for (int x = 0; x < jb; ++x) slab[x * rcap + i] = s_piv[x];
+                continue;
+            }
+            if (gr == p && p != c)
+                for (int x = 0; x < jb; ++x) slab[x * rcap + i] = s_cur[x];
+            if (!apply) continue;
+            const cf l = slab[jj * rcap + i] * inv;
             slab[jj * rcap + i] = l;
             for (int x = jj + 1; x < jb; ++x) slab[x * rcap + i] = slab[x * rcap + i] - l * s_piv[x];
         }
@@ -689,6 +836,7 @@ static int panel_sms() {
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         cudaFuncSetAttribute(panel_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPanelSmemMax);
+        cudaFuncSetAttribute(panel_kernel_c64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPanelSmemMax);
         if (sms < 1) sms = 1;
     }
     return sms;
@@ -786,7 +934,9 @@ static mw_status panel_factor(T* A, int64_t lda, int64_t n, int64_t j0, int jb, 
         return MW_OK;
     }
     size_t ov, oi, orow, ocur;
-    ws_layout(G, &ov, &oi, &orow, &ocur);
+    // fixed offsets (sized for the largest grid): a CTA's exchange slot stays
+    // at one address for the whole factorisation
+    ws_layout(kMaxPanelGrid, &ov, &oi, &orow, &ocur);
     PanelWs* pws = reinterpret_cast<PanelWs*>(ws);
     // reset the barrier counter only; the error word stays sticky
     MW_CHECK_CUDA(cudaMemsetAsync(&pws->counter, 0, sizeof(unsigned int), st));
@@ -807,8 +957,8 @@ static mw_status panel_factor(T* A, int64_t lda, int64_t n, int64_t j0, int jb, 
     void* args[] = {&P};
     {
         ProfileScope ps(PC_PANEL, st, 4.0 * (double)m * jb * jb, 2.0 * sizeof(T) * (double)m * jb);
-        MW_CHECK_CUDA(
-            cudaLaunchCooperativeKernel((void*)panel_kernel<T>, dim3(G), dim3(kPanelThreads), args, smem, st));
+        void* kern = std::is_same<T, cf>::value ? (void*)panel_kernel_c64 : (void*)panel_kernel<T>;
+        MW_CHECK_CUDA(cudaLaunchCooperativeKernel(kern, dim3(G), dim3(kPanelThreads), args, smem, st));
     }
     count_launch();
     return MW_OK;
@@ -820,6 +970,11 @@ static mw_status getrf(int64_t n, T* A, int64_t lda, int32_t* ipiv, int32_t* inf
                        const volatile int32_t* cancel, const Updater& up, cudaStream_t st) {
     MW_CHECK_CUDA(cudaMemsetAsync(info, 0, 2 * sizeof(int32_t), st));
     MW_CHECK_CUDA(cudaMemsetAsync(ws, 0, sizeof(PanelWs), st));
+    {
+        size_t ov, oi, orow, ocur;
+        ws_layout(kMaxPanelGrid, &ov, &oi, &orow, &ocur);
+        MW_CHECK_CUDA(cudaMemsetAsync(ws + oi, 0, sizeof(int64_t) * 2 * kMaxPanelGrid, st));
+    }
     {
         mw_status s0 = trsm_setup<T>();
         if (s0 != MW_OK) return s0;
@@ -895,6 +1050,12 @@ static mw_status getrf_lookahead(int64_t n, T* A, int64_t lda, int32_t* ipiv, in
                                  cudaStream_t st) {
     MW_CHECK_CUDA(cudaMemsetAsync(info, 0, 2 * sizeof(int32_t), st));
     MW_CHECK_CUDA(cudaMemsetAsync(ws, 0, sizeof(PanelWs), st));
+    {
+        // the panel exchange words start cleared (no stale sequence number)
+        size_t ov, oi, orow, ocur;
+        ws_layout(kMaxPanelGrid, &ov, &oi, &orow, &ocur);
+        MW_CHECK_CUDA(cudaMemsetAsync(ws + oi, 0, sizeof(int64_t) * 2 * kMaxPanelGrid, st));
+    }
     {
         mw_status s0 = trsm_setup<T>();
         if (s0 != MW_OK) return s0;

@@ -48,56 +48,51 @@ class Geometry:
 
 def build_geometry(wires, npe, radius_per_wire) -> Geometry:
     """Uniform segments on every polyline edge: knots by linspace between
-    the edge's anchors, h = |edge| / n (``bspline.py:1027-1050``)."""
-    sl, sr, tg, hh, rr, ed, pe = [], [], [], [], [], [], []
-    e_first, e_n, e_h, e_r = [], [], [], []
-    w_first, w_n, w_arc = [], [], []
-    off = 0
-    e_idx = 0
-    for w, (pl, counts) in enumerate(zip(wires, npe)):
-        start = off
-        hw = []
-        for e in range(pl.shape[0] - 1):
-            p0, p1 = pl[e], pl[e + 1]
-            vec = p1 - p0
-            L = float(np.linalg.norm(vec))
-            if L < 1e-15:
-                raise ValueError(f"wire {w} edge {e} has zero length")
-            n = int(counts[e])
-            t = np.linspace(0.0, 1.0, n + 1)
-            pts = (1 - t[:, None]) * p0[None, :] + t[:, None] * p1[None, :]
-            sl.append(pts[:-1])
-            sr.append(pts[1:])
-            tg.append(np.tile(vec / L, (n, 1)))
-            h = L / n
-            hh.append(np.full(n, h))
-            hw.append(np.full(n, h))
-            rr.append(np.full(n, float(radius_per_wire[w])))
-            ed.append(np.full(n, e_idx, dtype=np.int32))
-            pe.append(np.arange(n, dtype=np.int32))
-            e_first.append(off)
-            e_n.append(n)
-            e_h.append(h)
-            e_r.append(float(radius_per_wire[w]))
-            e_idx += 1
-            off += n
-        w_first.append(start)
-        w_n.append(off - start)
-        w_arc.append(np.concatenate([[0.0], np.cumsum(np.concatenate(hw))]))
+    the edge's anchors, h = |edge| / n (``bspline.py:1027-1050``).  All
+    edges of all wires are laid out in one pass."""
+    p0 = np.concatenate([np.asarray(pl, dtype=np.float64)[:-1] for pl in wires], axis=0)
+    p1 = np.concatenate([np.asarray(pl, dtype=np.float64)[1:] for pl in wires], axis=0)
+    e_n = np.concatenate([np.asarray(c, dtype=np.int64).reshape(-1) for c in npe])
+    e_wire = np.concatenate([np.full(len(pl) - 1, w, dtype=np.int64) for w, pl in enumerate(wires)])
+    if e_n.shape[0] != p0.shape[0]:
+        raise ValueError("one segment count per polyline edge is needed")
+    vec = p1 - p0
+    L = np.sqrt((vec[:, None, :] @ vec[:, :, None])[:, 0, 0])  # same dot as a per-edge norm
+    if (L < 1e-15).any():
+        e = int(np.argmax(L < 1e-15))
+        w = int(e_wire[e])
+        first_edge = int(np.argmax(e_wire == w))
+        raise ValueError(f"wire {w} edge {e - first_edge} has zero length")
+    E = e_n.shape[0]
+    e_first = np.concatenate(([0], np.cumsum(e_n)[:-1]))
+    N = int(e_n.sum())
+    edge = np.repeat(np.arange(E), e_n)
+    pos = np.arange(N) - e_first[edge]
+    step = 1.0 / e_n[edge]
+    tl = pos * step
+    tr = np.where(pos + 1 == e_n[edge], 1.0, (pos + 1) * step)
+    seg_l = (1 - tl)[:, None] * p0[edge] + tl[:, None] * p1[edge]
+    seg_r = (1 - tr)[:, None] * p0[edge] + tr[:, None] * p1[edge]
+    e_h = L / e_n
+    radius_e = np.asarray([float(radius_per_wire[w]) for w in range(len(wires))], dtype=np.float64)[e_wire]
+    h = e_h[edge]
+    w_n = np.bincount(e_wire, weights=e_n, minlength=len(wires)).astype(np.int64)
+    w_first = np.concatenate(([0], np.cumsum(w_n)[:-1])).astype(np.int64)
+    w_arc = [np.concatenate([[0.0], np.cumsum(h[f : f + n])]) for f, n in zip(w_first.tolist(), w_n.tolist())]
     return Geometry(
-        seg_l=np.ascontiguousarray(np.vstack(sl)),
-        seg_r=np.ascontiguousarray(np.vstack(sr)),
-        tangents=np.ascontiguousarray(np.vstack(tg)),
-        h=np.concatenate(hh),
-        radius=np.concatenate(rr),
-        edge=np.concatenate(ed),
-        pos_in_edge=np.concatenate(pe),
-        edge_first=np.asarray(e_first, dtype=np.int32),
-        edge_n=np.asarray(e_n, dtype=np.int32),
-        edge_h=np.asarray(e_h, dtype=np.float64),
-        edge_radius=np.asarray(e_r, dtype=np.float64),
-        wire_first=np.asarray(w_first, dtype=np.int64),
-        wire_n=np.asarray(w_n, dtype=np.int64),
+        seg_l=np.ascontiguousarray(seg_l),
+        seg_r=np.ascontiguousarray(seg_r),
+        tangents=np.ascontiguousarray((vec / L[:, None])[edge]),
+        h=h,
+        radius=radius_e[edge],
+        edge=edge.astype(np.int32),
+        pos_in_edge=pos.astype(np.int32),
+        edge_first=e_first.astype(np.int32),
+        edge_n=e_n.astype(np.int32),
+        edge_h=e_h,
+        edge_radius=radius_e,
+        wire_first=w_first,
+        wire_n=w_n,
         wire_arc=w_arc,
     )
 
@@ -128,6 +123,25 @@ def _span_values(knots, d, span, x):
     return N
 
 
+def point_values(knots_list, d, wires, xs):
+    """Values of the d+1 active bases at one point per entry (wire w_i, arc
+    position x_i): (vals (n, d+1), first active local basis index (n,)).
+    Same span rule as ``basis_values``; one batched Cox-de Boor evaluation
+    over 2d-knot windows."""
+    n = len(xs)
+    K = np.empty((n, 2 * d))
+    first = np.empty(n, dtype=np.int64)
+    for i, (w, x) in enumerate(zip(wires, xs)):
+        kn = knots_list[w]
+        n_b = len(kn) - d - 1
+        sp = min(max(int(np.searchsorted(kn, x, side="right")) - 1, d), n_b - 1)
+        K[i] = kn[sp + 1 - d : sp + d + 1]
+        first[i] = sp - d
+    span = np.arange(n) * (2 * d) + (d - 1)
+    vals = _span_values(K.ravel(), d, span, np.asarray(xs, dtype=np.float64))
+    return vals.reshape(n, d + 1), first
+
+
 def basis_values(knots, d, x):
     """(len(x), n_basis) values of every basis of a clamped knot vector
     (right-open spans; the final knot belongs to the last non-empty span)."""
@@ -143,6 +157,58 @@ def basis_values(knots, d, x):
     return out
 
 
+class KeptBases:
+    """Per wire, the list of kept bases as (j_local, kind, junction, end,
+    m_global) tuples (kind "int" interior, "dir" held by a junction, "gnd"
+    held by the ground), built on first access of a wire."""
+
+    def __init__(self, ends, n_b, m_first):
+        self._ends = ends
+        self._n_b = [int(x) for x in n_b]
+        self._m_first = [int(x) for x in m_first]
+        self._cache = {}
+
+    def __len__(self):
+        return len(self._ends)
+
+    def __getitem__(self, w):
+        if w < 0:
+            w += len(self)
+        if not 0 <= w < len(self):
+            raise IndexError(w)
+        out = self._cache.get(w)
+        if out is None:
+            es, ee = self._ends[w]
+            n_b, m = self._n_b[w], self._m_first[w]
+            out = []
+            if es is not None:
+                out.append((0, es[0], es[1], "start", m))
+            base = m + len(out) - 1
+            out.extend((j, "int", None, None, base + j) for j in range(1, n_b - 1))
+            if ee is not None:
+                out.append((n_b - 1, ee[0], ee[1], "end", m + len(out)))
+            self._cache[w] = out
+        return out
+
+    def __iter__(self):
+        return (self[w] for w in range(len(self)))
+
+    def global_index(self, w, j):
+        """Global basis index of local basis j of wire w (arrays of equal
+        shape); -1 where that basis is not kept (a free end)."""
+        w = np.asarray(w, dtype=np.int64)
+        j = np.asarray(j, dtype=np.int64)
+        has_s = np.array([e[0] is not None for e in self._ends], dtype=np.int64)[w]
+        has_e = np.array([e[1] is not None for e in self._ends], dtype=np.int64)[w]
+        n_b = np.asarray(self._n_b, dtype=np.int64)[w]
+        m = np.asarray(self._m_first, dtype=np.int64)[w] + j - 1 + has_s
+        ok = ((j > 0) | (has_s == 1)) & ((j < n_b - 1) | (has_e == 1)) & (j >= 0) & (j < n_b)
+        return np.where(ok, m, -1)
+
+    def __eq__(self, other):
+        return len(self) == len(other) and all(a == b for a, b in zip(self, other))
+
+
 @dataclass
 class Basis:
     degree: int
@@ -150,7 +216,7 @@ class Basis:
     polys: np.ndarray  # (n_b, d+1, d+1)
     kcl_A: "scipy.sparse.csr_matrix"  # (n_c, n_b) KCL rows, entries +-1
     knots: list  # per wire
-    kept: list  # per wire: list of (j_local, kind, junction, end, m_global)
+    kept: KeptBases  # per wire: list of (j_local, kind, junction, end, m_global)
 
     @property
     def n(self) -> int:
@@ -161,57 +227,70 @@ def build_basis(geom: Geometry, degree, start_status, end_status, n_junctions, g
     """Clamped knot vector per wire; keep interior bases plus the value-1
     end basis at junction / ground ends; per-wing monomial coefficients in
     local arc length from values at d+1 uniform points (the reference's
-    design-matrix + Vandermonde step, ``bspline.py:1318-1414``)."""
+    design-matrix + Vandermonde step, ``bspline.py:1318-1414``).
+
+    The per-segment coefficients of all wires come from one batched
+    evaluation: segment s of a wire reads the knots at spans s+1-d .. s+d,
+    which in the clamped vector are the wire's arc positions at indices
+    clip(s+t, 0, n_w) for t in 1-d .. d."""
     d = int(degree)
-    supp_all, poly_all, knots_all, kept_all = [], [], [], []
+    n_wires = len(geom.wire_first)
+    wire_n = np.asarray(geom.wire_n, dtype=np.int64)
+    firsts = np.asarray(geom.wire_first, dtype=np.int64)
+    arcs = geom.wire_arc
+    knots_all = [np.concatenate([np.zeros(d), arc, np.full(d, arc[-1])]) for arc in arcs]
+    # ---- per-segment coefficients [segment, active basis c (= j - s), power p]
+    n_seg = int(wire_n.sum())
+    garc = np.concatenate(arcs)
+    arc_off = np.concatenate(([0], np.cumsum(wire_n + 1)[:-1]))
+    seg_wire = np.repeat(np.arange(n_wires), wire_n)
+    s_loc = np.arange(n_seg) - np.repeat(firsts - firsts[0], wire_n)
+    t = np.arange(1 - d, d + 1)
+    win = np.clip(s_loc[:, None] + t[None, :], 0, wire_n[seg_wire][:, None]) + arc_off[seg_wire][:, None]
+    K = garc[win]  # (n_seg, 2d) knots of spans s+1-d .. s+d
+    a0 = garc[arc_off[seg_wire] + s_loc]
+    hs = garc[arc_off[seg_wire] + s_loc + 1] - a0
+    unit = np.linspace(0.0, 1.0, d + 1)
+    us = hs[:, None] * unit[None, :]  # (n_seg, d+1) local sample points
+    span = np.repeat(np.arange(n_seg) * (2 * d) + (d - 1), d + 1)
+    vals = _span_values(K.ravel(), d, span, (a0[:, None] + us).ravel()).reshape(n_seg, d + 1, d + 1)
+    # Vandermonde V[s] = U diag(h_s^p) with U[sample, p] = unit^p, so
+    # V[s]^-1 vals[s] = diag(h_s^-p) U^-1 vals[s]
+    Uinv = np.linalg.inv(unit[:, None] ** np.arange(d + 1)[None, :])
+    coef = np.einsum("pq,sqc->scp", Uinv, vals) * hs[:, None, None] ** -np.arange(d + 1)[None, None, :]
+    # ---- kept bases: interior bases, plus end bases a junction / ground holds
+    def end_kind(status):
+        if status == "ground":
+            return ("gnd", None)
+        if status != "free":
+            return ("dir", status)
+        return None
+
+    ends = [(end_kind(start_status[w]), end_kind(end_status[w])) for w in range(n_wires)]
+    has_s = np.fromiter((e[0] is not None for e in ends), dtype=np.int64, count=n_wires)
+    has_e = np.fromiter((e[1] is not None for e in ends), dtype=np.int64, count=n_wires)
+    n_kept = (wire_n + d - 2) + has_s + has_e
+    m_first = np.concatenate(([0], np.cumsum(n_kept)[:-1])).astype(np.int64)
+    m = int(n_kept.sum())
     jdirs = {j: [] for j in range(n_junctions)}
-    m = 0
-    for w in range(len(geom.wire_first)):
-        arc = geom.wire_arc[w]
-        n_w = int(geom.wire_n[w])
-        first = int(geom.wire_first[w])
-        knots = np.concatenate([np.zeros(d), arc, np.full(d, arc[-1])])
-        knots_all.append(knots)
-        n_b = n_w + d
-        kept = []
-        if start_status[w] == "ground":
-            kept.append((0, "gnd", None, "start"))
-        elif start_status[w] != "free":
-            kept.append((0, "dir", start_status[w], "start"))
-        kept.extend((j, "int", None, None) for j in range(1, n_b - 1))
-        if end_status[w] == "ground":
-            kept.append((n_b - 1, "gnd", None, "end"))
-        elif end_status[w] != "free":
-            kept.append((n_b - 1, "dir", end_status[w], "end"))
-        # per-segment coefficients of the active bases, shape (n_w, d+1, d+1):
-        # [segment, active basis c (= j - s), power p]
-        hs = np.diff(arc)
-        unit = np.linspace(0.0, 1.0, d + 1)
-        us = hs[:, None] * unit[None, :]  # (n_w, d+1) local sample points
-        spans = np.arange(n_w) + d
-        vals = _span_values(knots, d, np.repeat(spans, d + 1), (arc[:-1, None] + us).ravel())
-        vals = vals.reshape(n_w, d + 1, d + 1)  # [s, sample, c]
-        V = us[:, :, None] ** np.arange(d + 1)[None, None, :]  # [s, sample, p]
-        coef = np.linalg.solve(V, vals)  # [s, p, c]
-        coef = np.transpose(coef, (0, 2, 1))  # [s, c, p]
-        js = np.array([k[0] for k in kept], dtype=np.int64)
-        nk = len(kept)
-        supp = np.full((nk, d + 1), -1, dtype=np.int32)
-        poly = np.zeros((nk, d + 1, d + 1))
-        lo = np.maximum(0, js - d)  # first wing of basis j
-        hi = np.minimum(n_w, js + 1)  # one past its last wing
-        for a in range(d + 1):
-            s = lo + a
-            ok = s < hi
-            supp[ok, a] = first + s[ok]
-            poly[ok, a, :] = coef[s[ok], (js - s)[ok], :]
-        for idx, (j, kind, junc, end) in enumerate(kept):
-            if kind == "dir":
-                jdirs[junc].append((m + idx, 1.0 if end == "start" else -1.0))
-        kept_all.append([(j, kind, junc, end, m + idx) for idx, (j, kind, junc, end) in enumerate(kept)])
-        supp_all.append(supp)
-        poly_all.append(poly)
-        m += nk
+    for w, (es, ee) in enumerate(ends):
+        if es is not None and es[0] == "dir":
+            jdirs[es[1]].append((int(m_first[w]), 1.0))
+        if ee is not None and ee[0] == "dir":
+            jdirs[ee[1]].append((int(m_first[w] + n_kept[w] - 1), -1.0))
+    bw = np.repeat(np.arange(n_wires), n_kept)
+    # local basis index: 1 - has_start at a wire's first kept basis, +1 after
+    js = np.arange(m) - np.repeat(m_first, n_kept) + np.repeat(1 - has_s, n_kept)
+    supp = np.full((m, d + 1), -1, dtype=np.int32)
+    poly = np.zeros((m, d + 1, d + 1))
+    lo = np.maximum(0, js - d)  # first wing of basis j
+    hi = np.minimum(wire_n[bw], js + 1)  # one past its last wing
+    for a in range(d + 1):
+        sl = lo + a
+        ok = sl < hi
+        gs = firsts[bw[ok]] + sl[ok]
+        supp[ok, a] = gs
+        poly[ok, a, :] = coef[gs - firsts[0], (js - sl)[ok], :]
     rows = [j for j in range(n_junctions) if j not in grounded]
     ri, ci, vi = [], [], []
     for r, j in enumerate(rows):
@@ -224,11 +303,11 @@ def build_basis(geom: Geometry, degree, start_status, end_status, n_junctions, g
                                    np.asarray(ci, dtype=np.int64))), shape=(len(rows), m))
     return Basis(
         degree=d,
-        supp=np.ascontiguousarray(np.concatenate(supp_all, axis=0)),
-        polys=np.ascontiguousarray(np.concatenate(poly_all, axis=0)),
+        supp=supp,
+        polys=poly,
         kcl_A=kcl,
         knots=knots_all,
-        kept=kept_all,
+        kept=KeptBases(ends, wire_n + d, m_first),
     )
 
 
@@ -252,16 +331,18 @@ def build_tiles(supp: np.ndarray, max_basis=MAX_TILE_BASIS, max_seg=MAX_TILE_SEG
     """Greedy split of the basis list into runs of consecutive bases whose
     wings touch at most ``max_seg`` distinct segments."""
     n_b = supp.shape[0]
+    rows = [[x for x in r if x >= 0] for r in supp.tolist()]
     firsts, nbs, segs = [], [], []
     m = 0
     while m < n_b:
         cur = set()
         cnt = 0
         while m + cnt < n_b and cnt < max_basis:
-            s = {int(x) for x in supp[m + cnt] if x >= 0}
-            if len(cur | s) > max_seg:
+            row = rows[m + cnt]
+            new = {x for x in row if x not in cur}
+            if len(cur) + len(new) > max_seg:
                 break
-            cur |= s
+            cur |= new
             cnt += 1
         if cnt == 0:
             raise ValueError("a single basis touches more segments than a tile holds")
@@ -270,23 +351,30 @@ def build_tiles(supp: np.ndarray, max_basis=MAX_TILE_BASIS, max_seg=MAX_TILE_SEG
         segs.append(sorted(cur))
         m += cnt
     T = len(firsts)
-    used = max(len(s) for s in segs) if segs else 1
+    ns = np.asarray([len(s) for s in segs], dtype=np.int64)
+    used = int(ns.max()) if T else 1
     seg_arr = np.full((T, used), -1, dtype=np.int32)
     loc = np.full(supp.shape, -1, dtype=np.int32)
-    for t, (f, c, s) in enumerate(zip(firsts, nbs, segs)):
-        seg_arr[t, : len(s)] = s
-        pos = {v: i for i, v in enumerate(s)}
-        for mm in range(f, f + c):
-            for a in range(supp.shape[1]):
-                if supp[mm, a] >= 0:
-                    loc[mm, a] = pos[int(supp[mm, a])]
+    if T:
+        # every tile's sorted segment list, keyed by (tile, segment), is one
+        # sorted array; a basis' local slot is its key's rank within its tile
+        flat = np.fromiter((x for s in segs for x in s), dtype=np.int64, count=int(ns.sum()))
+        tile_of_flat = np.repeat(np.arange(T), ns)
+        start = np.concatenate(([0], np.cumsum(ns)[:-1]))
+        seg_arr[tile_of_flat, np.arange(flat.size) - start[tile_of_flat]] = flat
+        stride = int(max(flat.max(), supp.max())) + 1
+        keys = tile_of_flat * stride + flat
+        tile_of_basis = np.repeat(np.arange(T), np.asarray(nbs))
+        want = tile_of_basis[:, None] * stride + supp.astype(np.int64)
+        pos = np.searchsorted(keys, want) - start[tile_of_basis][:, None]
+        loc[:] = np.where(supp >= 0, pos, -1)
     return Tiles(
         first=np.asarray(firsts, dtype=np.int32),
         nb=np.asarray(nbs, dtype=np.int32),
-        ns=np.asarray([len(s) for s in segs], dtype=np.int32),
+        ns=ns.astype(np.int32),
         seg=seg_arr,
         loc=loc,
-        max_basis=int(max(nbs)),
+        max_basis=int(max(nbs)) if nbs else 1,
         max_seg=int(used),
     )
 

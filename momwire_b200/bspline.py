@@ -579,7 +579,8 @@ class BSplineSolver:
                     "voltage is pinned by the ground image, so it cannot also be a driven port"
                 )
             port_rows.append(row_of[j_idx])
-        keep = [r for r in range(kcl_A.shape[0]) if r not in set(port_rows)]
+        port_set = set(port_rows)
+        keep = [r for r in range(kcl_A.shape[0]) if r not in port_set]
         port_V = np.array([v for _j, v in self.junction_ports], dtype=np.complex128)
         return kcl_A[keep, :], kcl_A[port_rows, :], port_V
 
@@ -667,12 +668,24 @@ class BSplineSolver:
         node gaps)."""
         geom, basis = self._geometry(), self._basis()
         rs, cs, vs = [], [], []
-        for i, (w, arc_i, _v) in enumerate(self.feeds):
-            s_f = arc_i if arc_i is not None else geom.wire_arc[w][-1] / 2.0
-            idx, val = self._source_entries(w, s_f)
-            rs.append(idx)
-            cs.append(np.full(idx.size, i, dtype=np.int64))
-            vs.append(val)
+        ws = [w for w, _a, _v in self.feeds]
+        sfs = [a if a is not None else geom.wire_arc[w][-1] / 2.0 for w, a, _v in self.feeds]
+        if self.feeds and self.feed_smoothing_factor is None and self.feed_model == "point":
+            # all point feeds in one batched evaluation: v_m = Phi_m(s_f)
+            d = self.degree
+            vals, first = T.point_values(basis.knots, d, ws, sfs)
+            wi = np.repeat(np.asarray(ws, dtype=np.int64), d + 1)
+            mg = basis.kept.global_index(wi, (first[:, None] + np.arange(d + 1)[None, :]).ravel())
+            keep = (mg >= 0) & (vals.ravel() != 0.0)
+            rs.append(mg[keep])
+            cs.append(np.repeat(np.arange(len(ws), dtype=np.int64), d + 1)[keep])
+            vs.append(vals.ravel()[keep].astype(np.complex128))
+        else:
+            for i, (w, s_f) in enumerate(zip(ws, sfs)):
+                idx, val = self._source_entries(w, s_f)
+                rs.append(idx)
+                cs.append(np.full(idx.size, i, dtype=np.int64))
+                vs.append(val)
         _kcl, port_A, _pv = self._split_kcl_ports(basis.kcl_A)
         pa = port_A.tocoo()
         rs.append(pa.col.astype(np.int64))

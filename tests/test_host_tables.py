@@ -51,6 +51,64 @@ def test_tiles_cover_every_wing(name):
                     assert t.seg[ti, t.loc[m, a]] == b.supp[m, a]
 
 
+def _greedy_tiles(supp, max_basis, max_seg):
+    """Plain set-based statement of the greedy tiling."""
+    out, m = [], 0
+    while m < supp.shape[0]:
+        cur, cnt = set(), 0
+        while m + cnt < supp.shape[0] and cnt < max_basis:
+            s = {int(x) for x in supp[m + cnt] if x >= 0}
+            if len(cur | s) > max_seg:
+                break
+            cur |= s
+            cnt += 1
+        out.append((m, cnt, sorted(cur)))
+        m += cnt
+    return out
+
+
+@pytest.mark.parametrize("name", ["d1_dipole20", "d2_junction", "d2_mixed_radius_kink", "d2_somm_plate8"])
+@pytest.mark.parametrize("limits", [(16, 24), (5, 7), (3, 4)])
+def test_tiles_are_the_greedy_split(name, limits):
+    b = momwire_b200.BSplineSolver(**CASES[name]())._basis()
+    t = T.build_tiles(b.supp, *limits)
+    want = _greedy_tiles(b.supp, *limits)
+    assert len(want) == len(t.first)
+    for ti, (f, c, segs) in enumerate(want):
+        assert (t.first[ti], t.nb[ti], t.ns[ti]) == (f, c, len(segs))
+        assert list(t.seg[ti, : len(segs)]) == segs
+
+
+@pytest.mark.parametrize("name", ["d1_dipole20", "d2_junction", "d2_ek_monopole_pec", "d2_somm_plate8"])
+def test_kept_index_and_point_values(name):
+    """The per-wire kept-basis lists, their vectorised global index, and
+    the batched point evaluation against ``basis_values``."""
+    s = momwire_b200.BSplineSolver(**CASES[name]())
+    g, b = s._geometry(), s._basis()
+    d = b.degree
+    m = 0
+    for w in range(len(b.kept)):
+        kept = b.kept[w]
+        n_b = len(b.knots[w]) - d - 1
+        assert [k[4] for k in kept] == list(range(m, m + len(kept)))
+        gi = b.kept.global_index(np.full(n_b, w), np.arange(n_b))
+        want = np.full(n_b, -1)
+        for j, _k, _jn, _e, mg in kept:
+            want[j] = mg
+        assert np.array_equal(gi, want)
+        m += len(kept)
+    assert m == b.n
+    rng = np.random.default_rng(3)
+    ws = rng.integers(0, len(b.kept), 40)
+    xs = np.array([rng.uniform(0, g.wire_arc[w][-1]) for w in ws])
+    xs[:3] = [g.wire_arc[ws[0]][0], g.wire_arc[ws[1]][-1], g.wire_arc[ws[2]][1]]
+    vals, first = T.point_values(b.knots, d, ws, xs)
+    for i, (w, x) in enumerate(zip(ws, xs)):
+        full = T.basis_values(b.knots[w], d, [x])[0]
+        assert np.array_equal(full[first[i] : first[i] + d + 1], vals[i])
+        assert np.count_nonzero(np.delete(full, np.arange(first[i], first[i] + d + 1))) == 0
+
+
 def test_ek_labels_match_oracle():
     kw = CASES["d2_ek_monopole_pec"]()
     s = momwire_b200.BSplineSolver(**kw)

@@ -366,6 +366,25 @@ mw_status mw_scatter_c128(int64_t ld, int64_t ncols, int64_t nnz, const int64_t*
                           const int64_t* cols, const double* vals, double* out, void* stream);
 
 /*
+ * Distributed series wire loading (bspline.py:2732-2760, _apply_loading;
+ * _wire_loading.py series_impedance_per_wire): for every matrix b of a
+ * batch, Z_b[rows[q], cols[q]] += zw[b * n_wires + wire[q]] * vals[q].
+ * The nnz entries are the coalesced same-wire basis-overlap Gram (unique
+ * (row, col) pairs, vals real, wire the wire both bases lie on); zw holds
+ * each matrix's per-wire series impedance Z'_w(omega) (complex128, Ohm/m).
+ * Z is column-major complex128 with leading dimension ldz and z_stride
+ * complex elements between matrices; Z32 (optional, complex64, ld32,
+ * z32_stride) receives the rounded updated values, so a mixed-precision
+ * copy written by the fill stays the rounded Z.  All arrays are device
+ * memory.  Entries out of range are skipped and counted into *bad
+ * (optional device int32).
+ */
+mw_status mw_add_loading(int64_t n, int32_t batch, int64_t nnz, const int64_t* rows, const int64_t* cols,
+                         const double* vals, const int32_t* wire, const double* zw, int32_t n_wires, double* Z,
+                         int64_t ldz, int64_t z_stride, float* Z32, int64_t ld32, int64_t z32_stride, int32_t* bad,
+                         void* stream);
+
+/*
  * C = alpha * op(A) * op(B) + beta * C for complex128 column-major
  * matrices, op = 'N' or 'T' (transA/transB 0/1).  Used for the KCL Schur
  * step and Y = B^T X (bspline.py:2984-2989, 4179).

@@ -31,6 +31,7 @@ import scipy.sparse
 from . import _lib
 from . import _tables as T
 from . import autotune
+from . import loading as wl
 from . import sommerfeld as somm
 from . import surrogate as sur
 from ._port_solution import PortSolution
@@ -219,8 +220,6 @@ class BSplineSolver:
             raise ValueError("wires must be non-empty")
         if use_singular_enrichment:
             raise NotImplementedError("use_singular_enrichment is outside the B200 dense path")
-        if wire_conductivity is not None or insulation_radius is not None or insulation_eps_r is not None:
-            raise NotImplementedError("distributed wire loading is outside the B200 dense path")
         if precision not in ("fp64", "mixed"):
             raise ValueError(f"precision must be 'fp64' or 'mixed', got {precision!r}")
         self.precision = precision
@@ -299,6 +298,13 @@ class BSplineSolver:
         if not np.all(np.isfinite(r)) or np.any(r <= 0.0):
             raise ValueError(f"wire_radius entries must be positive and finite, got {r}")
         self._radius_per_wire = r
+        # distributed series loading (bspline.py:715-728): None when off
+        self._loading = wl.configure(n_w, r, wire_conductivity, insulation_radius, insulation_eps_r)
+        self.wire_conductivity = None if self._loading is None else self._loading.conductivity
+        self.insulation_radius = None if self._loading is None else self._loading.insulation_radius
+        self.insulation_eps_r = None if self._loading is None else self._loading.insulation_eps_r
+        self._cached_loading = None
+        self._cached_loading_dev = None
 
         if n_per_edge_per_wire is None:
             n_per_edge_per_wire = [None] * n_w
@@ -817,6 +823,76 @@ class BSplineSolver:
                 _lib.call("mw_somm_remainder_q", C.byref(dt.seg), C.byref(dt.basis), C.byref(grid),
                           self.n_qp_sommerfeld, float(self.ground_z), float(self.k), Z.data_ptr(), n, z32, n, stream)
                 self.last_sommerfeld = dict(info, method="grid")
+        # distributed series wire loading, added once to the final Z
+        self._loading_device(Z, buf.get("Z32"), [self.omega], stream)
+
+    # ------------------------------------------------------------ loading
+    def _loading_tables(self) -> wl.LoadingGram:
+        if self._cached_loading is None:
+            self._cached_loading = wl.loading_gram(self._geometry(), self._basis())
+        return self._cached_loading
+
+    def _loading_gram(self):
+        """(rows, cols, vals, wire_of_nnz) triplets of the same-wire
+        basis-overlap Gram, one per shared segment (``bspline.py:2667-2731``)."""
+        g = self._loading_tables()
+        return g.rows, g.cols, g.vals, g.wire
+
+    def _apply_loading(self, Z, omega=None):
+        """Add the loading term into a host Z (n, n) or stack (n_k, n, n) in
+        place; a no-op when no loading is configured (``bspline.py:2732-2760``).
+        The device fill applies the same term through ``mw_add_loading``."""
+        if self._loading is None:
+            return Z
+        g = self._loading_tables()
+        zw = self._loading.z_wire(self.omega if omega is None else omega)
+        if Z.ndim == 2:
+            np.add.at(Z, (g.rows, g.cols), zw[g.wire] * g.vals)
+        else:
+            data = zw[g.wire, :].T * g.vals[None, :]
+            for ki in range(Z.shape[0]):
+                np.add.at(Z[ki], (g.rows, g.cols), data[ki])
+        return Z
+
+    def wire_loss_power(self, coeffs, omega=None):
+        """Ohmic power in the wire metal from a solve's coefficients:
+        P = 1/2 sum_w Re Z'_w (c^H S_w c); returns (total W, per-wire W)
+        (``bspline.py:2782-2806``).  Insulation is reactive and adds nothing."""
+        per_wire = np.zeros(len(self.wires_polylines), dtype=np.float64)
+        if self._loading is None:
+            return 0.0, per_wire
+        g = self._loading_tables()
+        c = np.asarray(coeffs)[: self._basis().n]
+        r_w = np.real(self._loading.z_wire(self.omega if omega is None else omega))
+        contrib = 0.5 * r_w[g.wire] * np.real(np.conj(c[g.rows]) * c[g.cols]) * g.vals
+        np.add.at(per_wire, g.wire, contrib)
+        return float(per_wire.sum()), per_wire
+
+    def _loading_device(self, Z, Z32, omegas, stream):
+        """Z_b += sum_w Z'_w(omega_b) S_w on the device for a stack of
+        column-major matrices (Z: (n_k, n, n) or (n, n) tensor; Z32 its
+        complex64 mirror or None)."""
+        if self._loading is None:
+            return
+        torch = _torch()
+        dev = self._torch_device()
+        n = self._basis().n
+        if self._cached_loading_dev is None:
+            g = self._loading_tables()
+            self._cached_loading_dev = (
+                torch.from_numpy(g.u_rows.astype(np.int64)).to(dev),
+                torch.from_numpy(g.u_cols.astype(np.int64)).to(dev),
+                torch.from_numpy(g.u_vals.astype(np.float64)).to(dev),
+                torch.from_numpy(g.u_wire.astype(np.int32)).to(dev),
+            )
+        rows, cols, vals, wire = self._cached_loading_dev
+        omegas = np.atleast_1d(np.asarray(omegas, dtype=np.float64))
+        zw = np.ascontiguousarray(self._loading.z_wire(omegas).T)  # (batch, n_wires)
+        zt = torch.from_numpy(zw).to(dev)
+        batch = omegas.size
+        _lib.call("mw_add_loading", n, batch, rows.numel(), rows.data_ptr(), cols.data_ptr(), vals.data_ptr(),
+                  wire.data_ptr(), zt.data_ptr(), zw.shape[1], Z.data_ptr(), n, n * n,
+                  Z32.data_ptr() if Z32 is not None else None, n, n * n, None, stream)
 
     def _surrogate_check(self, stream):
         """(model, info) when the surrogate may serve this structure at this
@@ -933,10 +1009,13 @@ class BSplineSolver:
                       buf["Y"].data_ptr(), n_p, stream)
         return X
 
-    def _check_info(self, buf):
-        infos = [buf["info"]] + ([buf["info_c"]] if buf["n_c"] else [])
-        for inf in infos:
-            v = inf.cpu().numpy()
+    def _check_info(self, buf, infos=None):
+        """Raise on a singular factor or a timed-out panel barrier; ``infos``
+        are host copies of the status words already read back, if any."""
+        if infos is None:
+            infos = [buf["info"]] + ([buf["info_c"]] if buf["n_c"] else [])
+            infos = [inf.cpu().numpy() for inf in infos]
+        for v in infos:
             if v[1] != 0:
                 raise RuntimeError(f"LU panel barrier timed out (device status {int(v[1])})")
             if v[0] > 0:
@@ -961,9 +1040,24 @@ class BSplineSolver:
         st = torch.cuda.current_stream(buf["Z"].device).cuda_stream
         X = self._device_solve(buf, st)
         n_p = buf["n_p"]
-        Xh = X.cpu().numpy().T.copy()
-        Yh = buf["Y"][:n_p, :n_p].cpu().numpy().T.copy() if n_p else np.zeros((0, 0), dtype=np.complex128)
-        self._check_info(buf)
+        # one stream-ordered read-back into page-locked host memory: the
+        # coefficients stay column-major (Xh is the transposed view), Y and
+        # the status words ride along, then a single stream synchronise
+        dev_stream = torch.cuda.current_stream(buf["Z"].device)
+        hx = torch.empty(X.shape, dtype=X.dtype, pin_memory=True)
+        hx.copy_(X, non_blocking=True)
+        hy = torch.empty((n_p, n_p), dtype=X.dtype, pin_memory=True)
+        if n_p:
+            hy.copy_(buf["Y"][:n_p, :n_p], non_blocking=True)
+        hinfo = [torch.empty(2, dtype=torch.int32, pin_memory=True)
+                 for _ in range(2 if buf["n_c"] else 1)]
+        hinfo[0].copy_(buf["info"][:2], non_blocking=True)
+        if buf["n_c"]:
+            hinfo[1].copy_(buf["info_c"][:2], non_blocking=True)
+        dev_stream.synchronize()
+        Xh = hx.numpy().T
+        Yh = hy.numpy().T
+        self._check_info(buf, [h.numpy() for h in hinfo])
         self.last_stats = {"h2d_bytes": buf["h2d_bytes"], "d2h_bytes": int(Xh.nbytes + Yh.nbytes + 16)}
         return PortSolution(
             y=Yh,
@@ -1045,6 +1139,7 @@ class BSplineSolver:
                   ob.data_ptr(), float(self.eps), float(self.mu), self.n_qp_pair, int(self.extended_kernel),
                   float(self.ground_z or 0.0), pec, table.data_ptr(), Z.data_ptr(), n, n * n, Z32.data_ptr(), n,
                   n * n, stream)
+        self._loading_device(Z, Z32, np.asarray(ks, dtype=np.float64) * self.c, stream)
         return Z, Z32
 
     def _batched_panel_width(self, ks):

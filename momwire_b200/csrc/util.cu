@@ -14,9 +14,61 @@ __global__ void scatter_add_c128_kernel(int64_t nnz, const int64_t* __restrict__
     }
 }
 
+// Z[b][rows[q] + cols[q] * ldz] += zw[b][wire[q]] * vals[q] for unique
+// (row, col) entries (no two threads touch one element), and the complex64
+// mirror, when given, takes the rounded new value.  Entries outside the
+// n x n matrix or naming a wire outside [0, n_wires) are skipped and counted.
+__global__ void add_loading_kernel(int64_t n, int batch, int64_t nnz, const int64_t* __restrict__ rows,
+                                   const int64_t* __restrict__ cols, const double* __restrict__ vals,
+                                   const int32_t* __restrict__ wire, const double2* __restrict__ zw, int n_wires,
+                                   double2* __restrict__ Z, int64_t ldz, int64_t sz, float2* __restrict__ Z32,
+                                   int64_t ld32, int64_t s32, int32_t* __restrict__ bad) {
+    const int64_t total = nnz * (int64_t)batch;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t b = t / nnz, q = t - b * nnz;
+        const int64_t r = rows[q], c = cols[q];
+        const int w = wire[q];
+        if (r < 0 || r >= n || c < 0 || c >= n || w < 0 || w >= n_wires) {
+            if (bad) atomicAdd(bad, 1);
+            continue;
+        }
+        const double2 z = zw[b * n_wires + w];
+        const double v = vals[q];
+        double2* p = Z + b * sz + r + c * ldz;
+        double2 cur = *p;
+        cur.x += z.x * v;
+        cur.y += z.y * v;
+        *p = cur;
+        if (Z32) Z32[b * s32 + r + c * ld32] = make_float2((float)cur.x, (float)cur.y);
+    }
+}
+
 }  // namespace mw
 
 using namespace mw;
+
+extern "C" mw_status mw_add_loading(int64_t n, int32_t batch, int64_t nnz, const int64_t* rows, const int64_t* cols,
+                                    const double* vals, const int32_t* wire, const double* zw, int32_t n_wires,
+                                    double* Z, int64_t ldz, int64_t z_stride, float* Z32, int64_t ld32,
+                                    int64_t z32_stride, int32_t* bad, void* stream) {
+    MW_REQUIRE(n >= 0 && nnz >= 0 && batch >= 0 && n_wires >= 0, "sizes must be >= 0");
+    MW_REQUIRE(ldz >= n && (Z32 == nullptr || ld32 >= n), "leading dimension smaller than n");
+    MW_REQUIRE(batch <= 1 || (z_stride >= ldz * n && (Z32 == nullptr || z32_stride >= ld32 * n)),
+               "batch stride smaller than one matrix");
+    if (nnz == 0 || batch == 0 || n == 0) return MW_OK;
+    MW_REQUIRE(rows && cols && vals && wire && zw && Z, "NULL argument");
+    MW_REQUIRE(n_wires > 0, "entries need at least one wire");
+    cudaStream_t st = as_stream(stream);
+    const int64_t total = nnz * (int64_t)batch;
+    const int64_t blocks = (total + 255) / 256;
+    add_loading_kernel<<<(unsigned)(blocks < 4096 ? blocks : 4096), 256, 0, st>>>(
+        n, batch, nnz, rows, cols, vals, wire, reinterpret_cast<const double2*>(zw), n_wires,
+        reinterpret_cast<double2*>(Z), ldz, z_stride, reinterpret_cast<float2*>(Z32), ld32, z32_stride, bad);
+    MW_CHECK_CUDA(cudaGetLastError());
+    count_launch();
+    return MW_OK;
+}
 
 extern "C" mw_status mw_scatter_c128(int64_t ld, int64_t ncols, int64_t nnz, const int64_t* rows,
                                      const int64_t* cols, const double* vals, double* out, void* stream) {

@@ -70,6 +70,9 @@ class Spec:
     ground_phi_mode: str = "normal"
     ground_model: str = "refl-coef"
     n_qp_sommerfeld: int = 3
+    wire_conductivity: np.ndarray | None = None  # per wire, NaN = off
+    insulation_radius: np.ndarray | None = None
+    insulation_eps_r: np.ndarray | None = None
 
     @property
     def k(self):
@@ -104,6 +107,9 @@ def make_spec(
     ground_phi_mode="normal",
     ground_model="refl-coef",
     n_qp_sommerfeld=3,
+    wire_conductivity=None,
+    insulation_radius=None,
+    insulation_eps_r=None,
 ):
     """Build a :class:`Spec` from BSplineSolver-style kwargs
     (``bspline.py:402-637``: per-edge counts, feeds, junction ports)."""
@@ -152,7 +158,17 @@ def make_spec(
         ground_phi_mode=ground_phi_mode,
         ground_model=ground_model,
         n_qp_sommerfeld=int(n_qp_sommerfeld),
+        wire_conductivity=_per_wire(wire_conductivity, n_w),
+        insulation_radius=_per_wire(insulation_radius, n_w),
+        insulation_eps_r=_per_wire(insulation_eps_r, n_w),
     )
+
+
+def _per_wire(v, n_w):
+    if v is None:
+        return None
+    a = np.asarray(v, dtype=float)
+    return np.full(n_w, float(a)) if a.ndim == 0 else a
 
 
 # ---------------------------------------------------------------------------
@@ -705,7 +721,74 @@ def compute_Z(spec, geom=None, basis=None, somm_master_values=None):
             img = img + so.remainder_Q(geom, basis.supp_seg, basis.polys, spec.degree, spec.n_qp_sommerfeld,
                                        spec.ground_z, k, grid)
         Z -= img
+    if loading_active(spec):
+        Z = Z + loading_matrix(spec, geom, basis, om)
     return Z
+
+
+# ---------------------------------------------------------------------------
+# Distributed series wire loading  (_wire_loading.py; bspline.py:2667-2760)
+# ---------------------------------------------------------------------------
+
+
+def loading_active(spec):
+    return spec.wire_conductivity is not None or spec.insulation_radius is not None
+
+
+def internal_impedance(omega, a, sigma):
+    """Round solid conductor, Z' = k_c / (2 pi a sigma) I0(k_c a) / I1(k_c a),
+    k_c = sqrt(j omega mu0 sigma) (``_wire_loading.py``
+    ``wire_internal_impedance``).  Unscaled Bessels: valid while |k_c a|
+    stays well below the overflow of I_n (a / skin depth < ~300)."""
+    from scipy.special import iv
+
+    kc = np.sqrt(1j * omega * MU0 * sigma)
+    return kc / (2 * math.pi * a * sigma) * iv(0, kc * a) / iv(1, kc * a)
+
+
+def z_per_wire(spec, omega):
+    """Z'_w(omega) per wire (``_wire_loading.py`` ``series_impedance_per_wire``)."""
+    n_w = len(spec.wires)
+    out = np.zeros(n_w, dtype=np.complex128)
+    for w in range(n_w):
+        a = spec.radius[w]
+        if spec.wire_conductivity is not None and np.isfinite(spec.wire_conductivity[w]):
+            out[w] += internal_impedance(omega, a, spec.wire_conductivity[w])
+        if spec.insulation_radius is not None and np.isfinite(spec.insulation_radius[w]):
+            b, er = spec.insulation_radius[w], spec.insulation_eps_r[w]
+            out[w] += 1j * omega * MU0 / (2 * math.pi) * (1 - 1 / er) * math.log(b / a)
+    return out
+
+
+def loading_gram(geom, basis):
+    """Dense S with S[m, n] = integral of Phi_m Phi_n over the segments both
+    bases cover, per wire: (n_wires, n_b, n_b).  Each shared segment is
+    integrated with (d+1)-point Gauss-Legendre, exact for the degree-2d
+    product (``bspline.py:2667-2731`` forms the same moment in closed form)."""
+    supp, polys = basis.supp_seg, basis.polys
+    n_b, n_wing, n_p = polys.shape
+    wire_of_seg = np.concatenate([np.full(w["n"], i) for i, w in enumerate(geom["wires"])])
+    x, wq = gl01(n_p)
+    by_seg = {}
+    for m in range(n_b):
+        for a in range(n_wing):
+            if np.any(polys[m, a] != 0.0):
+                by_seg.setdefault(int(supp[m, a]), []).append((m, a))
+    S = np.zeros((len(geom["wires"]), n_b, n_b))
+    for sgm, ents in by_seg.items():
+        h = geom["h"][sgm]
+        u = h * x
+        vals = [np.polyval(polys[m, a][::-1], u) for m, a in ents]
+        for i, (m, _a) in enumerate(ents):
+            for j, (n, _b) in enumerate(ents):
+                S[wire_of_seg[sgm], m, n] += h * np.sum(wq * vals[i] * vals[j])
+    return S
+
+
+def loading_matrix(spec, geom, basis, omega):
+    """sum_w Z'_w(omega) S_w (``bspline.py:2732-2753``)."""
+    S = loading_gram(geom, basis)
+    return np.einsum("w,wmn->mn", z_per_wire(spec, omega), S)
 
 
 # ---------------------------------------------------------------------------

@@ -141,6 +141,20 @@ CASES = {
 
 CASES["d2_somm_plate8"] = lambda: wire_grid_plate(n_cells=8, size=10.0, n_jports=3)
 
+# distributed series wire loading: skin-effect conductor loss and insulation
+SIGMA_CU = 5.8e7
+CASES["d2_loaded_dipole"] = lambda: dict(
+    wires=[np.array([[0.0, 0.0, -10.15 / 2], [0.0, 0.0, 10.15 / 2]])], nsegs=41, degree=2, wavelength=21.264,
+    wire_radius=0.16e-3, wire_conductivity=SIGMA_CU, insulation_radius=0.4e-3, insulation_eps_r=3.0)
+CASES["d1_loaded_yagi"] = lambda: dict(
+    CASES["d1_yagi"](), wire_conductivity=[SIGMA_CU, np.nan], insulation_radius=[1.5e-3, np.nan],
+    insulation_eps_r=[2.3, np.nan])
+CASES["d2_loaded_junction_pec"] = lambda: dict(
+    CASES["d2_junction"](), ground_z=-0.5, wire_conductivity=3.5e7)
+CASES["d2_loaded_mixed_radius"] = lambda: dict(
+    CASES["d2_mixed_radius_kink"](), wire_conductivity=[SIGMA_CU, 1.0e6])
+LOADED = {name for name in CASES if "_loaded_" in name}
+
 # Sommerfeld-ground cases whose fixtures also carry the grid master tables.
 SOMMERFELD = {name for name in CASES if "_somm_" in name}
 

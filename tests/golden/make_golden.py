@@ -90,6 +90,13 @@ def solve_case(momwire, kw, sample_seed=None, somm=False):
     out = {"y": sol.y, "t_fill": t_fill, "t_solve_total": t_all}
     if somm:
         out.update(somm_master(momwire, s, geom))
+    if getattr(s, "_loading_active", False):
+        from momwire import _wire_loading
+
+        r, c, v, w = s._loading_gram()
+        p_tot, p_wire = s.wire_loss_power(sol.coeffs[:, 0])
+        out.update(load_rows=r, load_cols=c, load_vals=v, load_wire=w,
+                   load_zw=_wire_loading.loading_for(s, s.omega).z_wire, loss_power=p_wire)
     if sample_seed is None:
         out["Z"] = Z
         out["coeffs"] = sol.coeffs
@@ -103,6 +110,21 @@ def solve_case(momwire, kw, sample_seed=None, somm=False):
     return out
 
 
+def wire_impedance_table(momwire):
+    """The reference's per-unit-length conductor and jacket impedances on a
+    grid from DC to extreme skin effect (a / skin depth ~ 1e-3 .. 5e4)."""
+    from momwire import _wire_loading
+
+    om = 2 * np.pi * np.array([10.0, 1e3, 1e5, 1e6, 14.1e6, 1e8, 1e10, 1e13])
+    rad = np.array([1e-4, 1e-3, 1e-2])
+    sig = np.array([1e6, 3.5e7, 5.8e7])
+    zi = np.array([[[_wire_loading.wire_internal_impedance(o, a, g) for g in sig] for a in rad] for o in om])
+    ins = np.array([[_wire_loading.insulation_inductance(1e-3, b, e) for e in (1.0, 2.3, 3.0, 10.0)]
+                    for b in (1.5e-3, 2.5e-3, 1e-2)])
+    return {"omega": om, "radius": rad, "sigma": sig, "z_int": zi, "ins_b": np.array([1.5e-3, 2.5e-3, 1e-2]),
+            "ins_eps": np.array([1.0, 2.3, 3.0, 10.0]), "ins_L": ins}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
@@ -110,6 +132,9 @@ def main():
     ap.add_argument("--only", default=None)
     args = ap.parse_args()
     momwire = import_reference(Path(args.ref))
+    if args.only in (None, "wire_impedance"):
+        np.savez_compressed(HERE / "wire_impedance.npz", **wire_impedance_table(momwire))
+        print("wire_impedance: table written", flush=True)
     todo = dict(CASES)
     if args.big:
         todo.update(BIG_CASES)

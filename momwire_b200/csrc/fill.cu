@@ -398,19 +398,19 @@ struct FillArgs {
     int nbatch;
 };
 
+// One (row tile, column tile) block of Z.  With allow_mirror the tile pair
+// is checked for symmetry (every staged segment of both tiles has the same
+// radius: the thin-wire kernel uses the observer radius, so only then is the
+// Galerkin block of (tc, tr) the transpose of that of (tr, tc)); a symmetric
+// pair also writes the transposed block.  Returns whether it did.
 template <int D, bool IMAGE, bool EK>
-__global__ void __launch_bounds__(256) fill_kernel(FillArgs A, GLParams gl) {
+__device__ __forceinline__ bool fill_tile(const FillArgs& A, const GLParams& gl, double* smem, const int tr,
+                                          const int tc, const bool allow_mirror) {
     constexpr int NM = D + 1, NMM = NM * NM;
-    extern __shared__ double smem[];
     const int nq = gl.nq;
     const int SD = SegStage<D>::stride(nq);
     const int SMAX = A.basis.max_tile_seg;
     const int TB = A.basis.max_tile_basis;
-    const int tr = blockIdx.y, tc = blockIdx.x;
-    if (IMAGE == false && tc > tr) {
-        // Galerkin symmetry is not exploited for writes: every tile is
-        // computed (Z is not assumed symmetric bit for bit).
-    }
     const int ns_r = A.basis.tile_ns[tr], ns_c = A.basis.tile_ns[tc];
     const int nb_r = A.basis.tile_nb[tr], nb_c = A.basis.tile_nb[tc];
     const int fb_r = A.basis.tile_first[tr], fb_c = A.basis.tile_first[tc];
@@ -428,7 +428,8 @@ __global__ void __launch_bounds__(256) fill_kernel(FillArgs A, GLParams gl) {
     double* s_W = s_J + (size_t)SMAX * SMAX * NMM * 2;  // image: SMAX*SMAX*4
     double* s_pr = s_W + (IMAGE ? (size_t)SMAX * SMAX * 4 : 0);  // TB*NMM
     double* s_pc = s_pr + TB * NMM;                     // TB*NMM
-    int* s_int = reinterpret_cast<int*>(s_pc + TB * NMM);
+    double* s_out = s_pc + TB * NMM;                    // TB*TB*2 (mirrored block)
+    int* s_int = reinterpret_cast<int*>(s_out + TB * TB * 2);
     int* s_seg_r = s_int;               // SMAX
     int* s_seg_c = s_seg_r + SMAX;      // SMAX
     int* s_edge_r = s_seg_c + SMAX;     // SMAX
@@ -444,8 +445,11 @@ __global__ void __launch_bounds__(256) fill_kernel(FillArgs A, GLParams gl) {
     const double gz = A.ground.ground_z;
 
     // ---- staging: segment lists, Gauss points, basis polynomials
+    const double r_ref = A.seg.radius[A.basis.tile_seg[(size_t)tr * SMAX]];
+    int odd_radius = 0;
     for (int i = tid; i < ns_r; i += blockDim.x) {
         int s = A.basis.tile_seg[(size_t)tr * SMAX + i];
+        odd_radius |= A.seg.radius[s] != r_ref;
         s_seg_r[i] = s;
         s_edge_r[i] = A.seg.edge[s];
         s_pos_r[i] = A.seg.pos_in_edge[s];
@@ -455,6 +459,7 @@ __global__ void __launch_bounds__(256) fill_kernel(FillArgs A, GLParams gl) {
     }
     for (int i = tid; i < ns_c; i += blockDim.x) {
         int s = A.basis.tile_seg[(size_t)tc * SMAX + i];
+        odd_radius |= A.seg.radius[s] != r_ref;
         s_seg_c[i] = s;
         s_edge_c[i] = A.seg.edge[s];
         s_pos_c[i] = A.seg.pos_in_edge[s];
@@ -468,7 +473,7 @@ __global__ void __launch_bounds__(256) fill_kernel(FillArgs A, GLParams gl) {
         s_pc[i] = A.basis.polys[(size_t)fb_c * NMM + i];
     for (int i = tid; i < nb_r * NM; i += blockDim.x) s_loc_r[i] = A.basis.loc[(size_t)fb_r * NM + i];
     for (int i = tid; i < nb_c * NM; i += blockDim.x) s_loc_c[i] = A.basis.loc[(size_t)fb_c * NM + i];
-    __syncthreads();
+    const bool mirror = __syncthreads_or(odd_radius) == 0 && allow_mirror;
 
     // ---- phase A: moments of every staged segment pair (4 lanes per pair)
     const int npair = ns_r * ns_c;
@@ -608,6 +613,10 @@ __global__ void __launch_bounds__(256) fill_kernel(FillArgs A, GLParams gl) {
         // j w mu zA + zP / (j w eps)
         double zre = -wmu * zA.im + inv_weps * zP.im;
         double zim = wmu * zA.re - inv_weps * zP.re;
+        if (mirror) {
+            s_out[(mi * TB + ni) * 2 + 0] = zre;
+            s_out[(mi * TB + ni) * 2 + 1] = zim;
+        }
         int64_t m = fb_r + mi, n = fb_c + ni;
         double* zp = Zb + m * 2 + n * A.ldz * 2;
         if (IMAGE) {
@@ -621,6 +630,56 @@ __global__ void __launch_bounds__(256) fill_kernel(FillArgs A, GLParams gl) {
             z32[0] = (float)zre;
             z32[1] = (float)zim;
         }
+    }
+    if (!mirror) return false;
+    __syncthreads();
+    // the transposed block Z[n, m], column tile index fastest (coalesced)
+    for (int pp = tid; pp < TB * TB; pp += blockDim.x) {
+        int ni = pp % TB, mi = pp / TB;
+        if (mi >= nb_r || ni >= nb_c) continue;
+        double zre = s_out[(mi * TB + ni) * 2 + 0];
+        double zim = s_out[(mi * TB + ni) * 2 + 1];
+        int64_t m = fb_r + mi, n = fb_c + ni;
+        double* zp = Zb + n * 2 + m * A.ldz * 2;
+        if (IMAGE) {
+            zre = zp[0] - zre;
+            zim = zp[1] - zim;
+        }
+        zp[0] = zre;
+        zp[1] = zim;
+        if (Z32b) {
+            float* z32 = Z32b + n * 2 + m * A.ldz32 * 2;
+            z32[0] = (float)zre;
+            z32[1] = (float)zim;
+        }
+    }
+    return true;
+}
+
+// Upper-triangle tile pair of block b: tc(tc+1)/2 <= b < (tc+1)(tc+2)/2,
+// tr = b - tc(tc+1)/2 <= tc.
+__device__ __forceinline__ void tri_pair(int64_t b, int& tr, int& tc) {
+    int64_t c = (int64_t)((sqrt(8.0 * (double)b + 1.0) - 1.0) * 0.5);
+    while ((c + 1) * (c + 2) / 2 <= b) ++c;
+    while (c * (c + 1) / 2 > b) --c;
+    tc = (int)c;
+    tr = (int)(b - c * (c + 1) / 2);
+}
+
+// One block per upper-triangle tile pair (tr <= tc).  A symmetric pair is
+// computed once and written to both blocks of Z; otherwise the block also
+// computes (tc, tr) itself.  The EK image fill labels direct and mirrored
+// segments separately, so it always computes both.
+template <int D, bool IMAGE, bool EK>
+__global__ void __launch_bounds__(256) fill_kernel(FillArgs A, GLParams gl) {
+    extern __shared__ double smem[];
+    int tr, tc;
+    tri_pair((int64_t)blockIdx.x, tr, tc);
+    const bool off_diag = tr != tc;
+    const bool mirrored = fill_tile<D, IMAGE, EK>(A, gl, smem, tr, tc, off_diag && !(IMAGE && EK));
+    if (off_diag && !mirrored) {
+        __syncthreads();
+        fill_tile<D, IMAGE, EK>(A, gl, smem, tc, tr, false);
     }
 }
 
@@ -687,7 +746,7 @@ static size_t fill_smem_bytes(int D, bool image, int nq, int smax, int tb) {
     int NM = D + 1, NMM = NM * NM;
     int SD = nq * 3 + nq * NM + 7;
     size_t dbl = (size_t)2 * smax * SD + (size_t)smax * smax * NMM * 2 + (image ? (size_t)smax * smax * 4 : 0) +
-                 (size_t)2 * tb * NMM;
+                 (size_t)2 * tb * NMM + (size_t)tb * tb * 2;
     size_t ints = (size_t)8 * smax + (size_t)2 * tb * NM;
     return dbl * 8 + ints * 4;
 }
@@ -708,9 +767,13 @@ static mw_status launch_fill(const FillArgs& A, const GLParams& gl, cudaStream_t
     auto kern = fill_kernel<D, IMAGE, EK>;
     MW_CHECK_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int nbz = A.nbatch > 0 ? A.nbatch : 1;
-    dim3 grid(A.basis.n_tile, A.basis.n_tile, nbz);
+    const int64_t nt = A.basis.n_tile;
+    dim3 grid((unsigned)(nt * (nt + 1) / 2), 1, nbz);
     double nb = A.basis.n_basis;
-    ProfileScope ps(IMAGE ? PC_FILL_IMAGE : PC_FILL, st, nbz * fill_flops(D, gl.nq, A.seg.n_seg, nb),
+    // flops of the upper-triangle tile pairs (the mirrored blocks are
+    // written, not recomputed, when every segment has one radius)
+    const double tri = (double)(nt + 1) / (2.0 * (double)nt);
+    ProfileScope ps(IMAGE ? PC_FILL_IMAGE : PC_FILL, st, tri * nbz * fill_flops(D, gl.nq, A.seg.n_seg, nb),
                     nbz * nb * nb * (16.0 + (A.Z32 ? 8.0 : 0.0)) * (IMAGE ? 2.0 : 1.0));
     kern<<<grid, 256, smem, st>>>(A, gl);
     MW_CHECK_CUDA(cudaGetLastError());

@@ -140,17 +140,25 @@ __device__ void static_half(double lo, double hi, double c, double h, double a,
     }
 }
 
+// Table modes: kTableFused writes static + smooth parts for one k per
+// blockIdx.y; a frequency batch instead runs kTableStatic once (the static
+// part is k-independent: it is written, as the real part, into all n_k
+// tables) and then kTableSmoothAdd per k, which adds the smooth part.
+enum { kTableFused = 0, kTableStatic = 1, kTableSmoothAdd = 2 };
+
 template <int D, bool EK>
 __global__ void same_edge_table_kernel(int n_edge, const int32_t* __restrict__ n_in_edge,
                                        const int64_t* __restrict__ table_off,
                                        const double* __restrict__ hs, const double* __restrict__ radii,
                                        int64_t rows, double k0, GLParams gl, double* __restrict__ out,
-                                       const double* __restrict__ kb, int64_t out_stride) {
+                                       const double* __restrict__ kb, int64_t out_stride, int mode = kTableFused,
+                                       int n_k = 1) {
     constexpr int NM = D + 1;
     int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (row >= rows) return;
     // frequency batch: blockIdx.y selects k and the output table
     const double k = kb ? kb[blockIdx.y] : k0;
+    double* const out0 = out;
     out += blockIdx.y * out_stride;
     // edge owning this row: last e with table_off[e] <= row
     int lo = 0, hi = n_edge - 1;
@@ -169,8 +177,23 @@ __global__ void same_edge_table_kernel(int n_edge, const int32_t* __restrict__ n
     for (int p = 0; p < NM; ++p)
 #pragma unroll
         for (int q = 0; q < NM; ++q) st[p][q] = 0.0;
-    static_half<D, EK>(-h, 0.0, c, h, a, gl, st);
-    static_half<D, EK>(0.0, h, c, h, a, gl, st);
+    if (mode != kTableSmoothAdd) {
+        static_half<D, EK>(-h, 0.0, c, h, a, gl, st);
+        static_half<D, EK>(0.0, h, c, h, a, gl, st);
+    }
+    if (mode == kTableStatic) {
+        for (int b = 0; b < n_k; ++b) {
+            double* o = out0 + b * out_stride + row * (NM * NM * 2);
+#pragma unroll
+            for (int p = 0; p < NM; ++p)
+#pragma unroll
+                for (int q = 0; q < NM; ++q) {
+                    o[(p * NM + q) * 2 + 0] = kInv4Pi * st[p][q];
+                    o[(p * NM + q) * 2 + 1] = 0.0;
+                }
+        }
+        return;
+    }
 
     // smooth part: (exp(-jkR) - 1)/(4 pi R) on nq x nq Gauss points
     cd rg[NM][NM];
@@ -215,8 +238,13 @@ __global__ void same_edge_table_kernel(int n_edge, const int32_t* __restrict__ n
     for (int p = 0; p < NM; ++p)
 #pragma unroll
         for (int q = 0; q < NM; ++q) {
-            o[(p * NM + q) * 2 + 0] = kInv4Pi * st[p][q] + rg[p][q].re;
-            o[(p * NM + q) * 2 + 1] = rg[p][q].im;
+            if (mode == kTableSmoothAdd) {
+                o[(p * NM + q) * 2 + 0] += rg[p][q].re;
+                o[(p * NM + q) * 2 + 1] += rg[p][q].im;
+            } else {
+                o[(p * NM + q) * 2 + 0] = kInv4Pi * st[p][q] + rg[p][q].re;
+                o[(p * NM + q) * 2 + 1] = rg[p][q].im;
+            }
         }
 }
 
@@ -920,17 +948,22 @@ extern "C" mw_status mw_fill_z_batch(const mw_segments* seg, const mw_basis* bas
     if (edges->table_rows > 0) {
         ProfileScope ps(PC_TABLE, st);
         const int threads = 128;
-        dim3 grid((unsigned)((edges->table_rows + threads - 1) / threads), (unsigned)n_k);
+        const unsigned bx = (unsigned)((edges->table_rows + threads - 1) / threads);
         const bool ek = extended_kernel != 0;
-        if (d == 1) {
-            if (ek) same_edge_table_kernel<1, true><<<grid, threads, 0, st>>>(edges->n_edge, edges->n_in_edge, edges->table_off, edges->h, edges->radius, edges->table_rows, 0.0, gl, table, k_dev, tstride);
-            else same_edge_table_kernel<1, false><<<grid, threads, 0, st>>>(edges->n_edge, edges->n_in_edge, edges->table_off, edges->h, edges->radius, edges->table_rows, 0.0, gl, table, k_dev, tstride);
-        } else {
-            if (ek) same_edge_table_kernel<2, true><<<grid, threads, 0, st>>>(edges->n_edge, edges->n_in_edge, edges->table_off, edges->h, edges->radius, edges->table_rows, 0.0, gl, table, k_dev, tstride);
-            else same_edge_table_kernel<2, false><<<grid, threads, 0, st>>>(edges->n_edge, edges->n_in_edge, edges->table_off, edges->h, edges->radius, edges->table_rows, 0.0, gl, table, k_dev, tstride);
+        // the k-independent static part once into every table, then the
+        // smooth part per k
+#define MW_TBL_B(DD, EE, GRID, MODE)                                                                            \
+    same_edge_table_kernel<DD, EE><<<GRID, threads, 0, st>>>(edges->n_edge, edges->n_in_edge, edges->table_off, \
+                                                             edges->h, edges->radius, edges->table_rows, 0.0, gl,   \
+                                                             table, k_dev, tstride, MODE, n_k)
+        for (int mode : {(int)kTableStatic, (int)kTableSmoothAdd}) {
+            dim3 grid(bx, mode == kTableStatic ? 1u : (unsigned)n_k);
+            if (d == 1) { if (ek) MW_TBL_B(1, true, grid, mode); else MW_TBL_B(1, false, grid, mode); }
+            else        { if (ek) MW_TBL_B(2, true, grid, mode); else MW_TBL_B(2, false, grid, mode); }
+            MW_CHECK_CUDA(cudaGetLastError());
+            count_launch();
         }
-        MW_CHECK_CUDA(cudaGetLastError());
-        count_launch();
+#undef MW_TBL_B
     }
     FillArgs A{};
     A.seg = *seg;

@@ -47,9 +47,12 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--fp64-steps", type=int, default=2, help="steps of the FP64 path timed beside a mixed run")
-    ap.add_argument("--sweep-structs", type=int, default=16,
+    ap.add_argument("--sweep-structs", type=int, default=512,
                     help="Yagis per rank in the sweep part of the line (0: none)")
     ap.add_argument("--sweep-workers", type=int, default=8, help="host threads (one CUDA stream each) per rank")
+    ap.add_argument("--sweep-mode", choices=("grouped", "workers"), default="grouped",
+                    help="grouped: padded groups of structures share one batched solve; workers: one batched "
+                         "solve per structure on --sweep-workers host threads")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--nx", type=int, default=16)
@@ -421,19 +424,25 @@ def run_sweep_part(args, rank, world, local, pg):
     # panel width outside the timed region)
     from momwire_b200 import autotune
 
-    seen = set()
-    for i in parts[rank]:
-        s0 = momwire_b200.BSplineSolver(**structs[i], precision="mixed", device=local)
-        key = autotune.key(s0._basis().n, s0.degree, "free")
-        if key not in seen:
-            seen.add(key)
-            fn(structs[i], ks[:8])
+    if args.sweep_mode == "grouped":
+        sweep.grouped_mixed_sweep(structs, ks[:8], device=local, indices=parts[rank])
+    else:
+        seen = set()
+        for i in parts[rank]:
+            s0 = momwire_b200.BSplineSolver(**structs[i], precision="mixed", device=local)
+            key = autotune.key(s0._basis().n, s0.degree, "free")
+            if key not in seen:
+                seen.add(key)
+                fn(structs[i], ks[:8])
     torch.cuda.synchronize()
     if pg:
         pg.barrier()
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     a.record(stream)
-    local_y = sweep.solve_shard(structs, ks, parts[rank], fn, workers=args.sweep_workers, device=local)
+    if args.sweep_mode == "grouped":
+        local_y = sweep.grouped_mixed_sweep(structs, ks, device=local, indices=parts[rank])
+    else:
+        local_y = sweep.solve_shard(structs, ks, parts[rank], fn, workers=args.sweep_workers, device=local)
     b.record(stream)
     torch.cuda.synchronize()
     ms = a.elapsed_time(b)
@@ -444,7 +453,9 @@ def run_sweep_part(args, rank, world, local, pg):
     ys = sweep.gather(local_y)
     out = {"workload": f"yagi_sweep_{len(structs)}x64", "solves": len(structs) * len(ks),
            "pts_per_s": len(structs) * len(ks) / (ms / 1e3), "ms": ms, "sharding": f"LPT x{world}",
-           "workers_per_rank": args.sweep_workers}
+           "mode": args.sweep_mode}
+    if args.sweep_mode == "workers":
+        out["workers_per_rank"] = args.sweep_workers
     if rank == 0:
         sub = ks[::8]
         f_ms, n64, err = 0.0, 0, 0.0

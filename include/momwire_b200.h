@@ -385,6 +385,17 @@ mw_status mw_add_loading(int64_t n, int32_t batch, int64_t nnz, const int64_t* r
                          void* stream);
 
 /*
+ * Pad `count` column-major matrices of order nb whose leading n x n block is
+ * filled to [[Z, 0], [0, I]] (complex128 Z with leading dimension ldz and
+ * z_stride complex elements between matrices; the complex64 mirror Z32 the
+ * same when given).  Structures of different orders then share one batched
+ * factorisation: partial pivoting never selects a padding row for a column
+ * < n, and the padding block of the solution is exactly zero.
+ */
+mw_status mw_pad_identity(int64_t n, int64_t nb, int32_t count, double* Z, int64_t ldz, int64_t z_stride,
+                          float* Z32, int64_t ld32, int64_t z32_stride, void* stream);
+
+/*
  * C = alpha * op(A) * op(B) + beta * C for complex128 column-major
  * matrices, op = 'N' or 'T' (transA/transB 0/1).  Used for the KCL Schur
  * step and Y = B^T X (bspline.py:2984-2989, 4179).

@@ -868,10 +868,10 @@ class BSplineSolver:
         np.add.at(per_wire, g.wire, contrib)
         return float(per_wire.sum()), per_wire
 
-    def _loading_device(self, Z, Z32, omegas, stream):
+    def _loading_device(self, Z, Z32, omegas, stream, ld=None):
         """Z_b += sum_w Z'_w(omega_b) S_w on the device for a stack of
-        column-major matrices (Z: (n_k, n, n) or (n, n) tensor; Z32 its
-        complex64 mirror or None)."""
+        column-major matrices (Z: (n_k, ld, ld) or (ld, ld) tensor, ld = n
+        by default; Z32 its complex64 mirror or None)."""
         if self._loading is None:
             return
         torch = _torch()
@@ -890,9 +890,10 @@ class BSplineSolver:
         zw = np.ascontiguousarray(self._loading.z_wire(omegas).T)  # (batch, n_wires)
         zt = torch.from_numpy(zw).to(dev)
         batch = omegas.size
+        ld = n if ld is None else int(ld)
         _lib.call("mw_add_loading", n, batch, rows.numel(), rows.data_ptr(), cols.data_ptr(), vals.data_ptr(),
-                  wire.data_ptr(), zt.data_ptr(), zw.shape[1], Z.data_ptr(), n, n * n,
-                  Z32.data_ptr() if Z32 is not None else None, n, n * n, None, stream)
+                  wire.data_ptr(), zt.data_ptr(), zw.shape[1], Z.data_ptr(), ld, ld * ld,
+                  Z32.data_ptr() if Z32 is not None else None, ld, ld * ld, None, stream)
 
     def _surrogate_check(self, stream):
         """(model, info) when the surrogate may serve this structure at this
@@ -1120,26 +1121,30 @@ class BSplineSolver:
         kcl, _pa, _pv = self._split_kcl_ports(self._basis().kcl_A)
         return kcl.shape[0] == 0 and self._basis().n <= 1600
 
-    def _fill_batched(self, ks, stream):
+    def _fill_batched(self, ks, stream, Z=None, Z32=None, ld=None):
         """(Z, Z32): device (n_k, n, n) complex128 / complex64 stacks, each
         matrix column-major (Z[b].T is the matrix at ks[b]), from one
-        batched fill launch."""
+        batched fill launch.  Given Z / Z32 of shape (n_k, ld, ld) with
+        ld >= n, the fill writes the leading n x n block of each."""
         torch = _torch()
         dev = self._torch_device()
         dt = self._dev_tables()
         n, d = self._basis().n, self.degree
         nk = len(ks)
+        ld = n if ld is None else int(ld)
         kb = torch.from_numpy(np.asarray(ks, dtype=np.float64)).to(dev)
         ob = torch.from_numpy(np.asarray(ks, dtype=np.float64) * self.c).to(dev)
         table = torch.empty((nk, max(dt.table_rows, 1), d + 1, d + 1), dtype=torch.complex128, device=dev)
-        Z = torch.empty((nk, n, n), dtype=torch.complex128, device=dev)
-        Z32 = torch.empty((nk, n, n), dtype=torch.complex64, device=dev)
+        if Z is None:
+            Z = torch.empty((nk, ld, ld), dtype=torch.complex128, device=dev)
+        if Z32 is None:
+            Z32 = torch.empty((nk, ld, ld), dtype=torch.complex64, device=dev)
         pec = 1 if self.ground_z is not None else 0
         _lib.call("mw_fill_z_batch", C.byref(dt.seg), C.byref(dt.basis), C.byref(dt.edges), nk, kb.data_ptr(),
                   ob.data_ptr(), float(self.eps), float(self.mu), self.n_qp_pair, int(self.extended_kernel),
-                  float(self.ground_z or 0.0), pec, table.data_ptr(), Z.data_ptr(), n, n * n, Z32.data_ptr(), n,
-                  n * n, stream)
-        self._loading_device(Z, Z32, np.asarray(ks, dtype=np.float64) * self.c, stream)
+                  float(self.ground_z or 0.0), pec, table.data_ptr(), Z.data_ptr(), ld, ld * ld, Z32.data_ptr(),
+                  ld, ld * ld, stream)
+        self._loading_device(Z, Z32, np.asarray(ks, dtype=np.float64) * self.c, stream, ld=ld)
         return Z, Z32
 
     def _batched_panel_width(self, ks):

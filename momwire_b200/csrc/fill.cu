@@ -94,50 +94,72 @@ __device__ __forceinline__ void conv_weights(double h, double t, double W[D + 1]
         }
 }
 
-template <int D, bool EK>
-__device__ void static_panel(double x0, double x1, double c, double h, double a,
-                             const GLParams& gl, double acc[D + 1][D + 1]) {
-    double half = 0.5 * (x1 - x0), mid = 0.5 * (x0 + x1);
-    for (int g = 0; g < 20; ++g) {
-        double t = mid + half * gl.x20[g];
-        double x = t - c;
-        double R2 = x * x + a * a;
-        double R = sqrt(R2);
-        double K = 1.0 / R;
-        if (EK) K += (a * a / (4.0 * R2 * R2 * R)) * (3.0 * a * a - 2.0 * R2);
-        double W[D + 1][D + 1];
-        conv_weights<D>(h, t, W);
-        double wk = half * gl.w20[g] * K;
-#pragma unroll
-        for (int p = 0; p <= D; ++p)
-#pragma unroll
-            for (int q = 0; q <= D; ++q) acc[p][q] += wk * W[p][q];
+// The static integral of one table row is a sum over Gauss points of
+// graded panels on the two half-intervals [-h, 0] and [0, h].  A half whose
+// kernel peak c is at least one interval length away is a single 20-point
+// panel; otherwise the panels grow geometrically from the end nearest the
+// peak: [0, s], [s, 2s], [2s, 4s], ... (s = the radius) until they cover the
+// interval.  The peak of every same-edge table entry sits on an end of the
+// half interval (c = delta*h with integer delta) or outside it.
+__device__ __forceinline__ int half_panels(double lo, double hi, double c, double a, bool& graded,
+                                           bool& near_left) {
+    const double L = hi - lo;
+    const double dist = (c < lo) ? lo - c : (c > hi ? c - hi : 0.0);
+    graded = dist < L;
+    near_left = fabs(lo - c) <= fabs(hi - c);
+    if (!graded) return 1;
+    int n = 1;
+    for (double s1 = fmax(a, 1e-300); s1 < L; s1 *= 2.0) ++n;
+    return n;
+}
+
+// Bounds of panel i of a half-interval (see half_panels).
+__device__ __forceinline__ void half_panel_bounds(double lo, double hi, double a, bool graded, bool near_left,
+                                                  int i, double& x0, double& x1) {
+    if (!graded) {
+        x0 = lo;
+        x1 = hi;
+        return;
+    }
+    const double L = hi - lo, s = fmax(a, 1e-300);
+    const double e0 = i == 0 ? 0.0 : fmin(ldexp(s, i - 1), L);
+    const double e1 = fmin(ldexp(s, i), L);
+    if (near_left) {
+        x0 = lo + e0;
+        x1 = lo + e1;
+    } else {
+        x0 = hi - e1;
+        x1 = hi - e0;
     }
 }
 
-// One half-interval [lo, hi] of the convolution integral, graded toward the
-// kernel peak c when it lies within one interval length.
+// One Gauss point g of panel [x0, x1] of the static integral:
+// acc += half_width w_g K(t - c) W(t), K = 1/R (+ the EK correction).
 template <int D, bool EK>
-__device__ void static_half(double lo, double hi, double c, double h, double a,
-                            const GLParams& gl, double acc[D + 1][D + 1]) {
-    double L = hi - lo;
-    double dist = (c < lo) ? lo - c : (c > hi ? c - hi : 0.0);
-    if (dist >= L) {
-        static_panel<D, EK>(lo, hi, c, h, a, gl, acc);
-        return;
-    }
-    // The peak of every same-edge table entry sits on an end of the half
-    // interval (c = delta*h with integer delta), or outside it.
-    bool near_left = fabs(lo - c) <= fabs(hi - c);
-    double s0 = 0.0, s1 = fmax(a, 1e-300);
-    while (true) {
-        double e = fmin(s1, L);
-        if (near_left) static_panel<D, EK>(lo + s0, lo + e, c, h, a, gl, acc);
-        else           static_panel<D, EK>(hi - e, hi - s0, c, h, a, gl, acc);
-        if (e >= L) break;
-        s0 = e;
-        s1 *= 2.0;
-    }
+__device__ __forceinline__ void static_point(double x0, double x1, int g, double c, double h, double a,
+                                             const GLParams& gl, double acc[D + 1][D + 1]) {
+    const double half = 0.5 * (x1 - x0), mid = 0.5 * (x0 + x1);
+    const double t = mid + half * gl.x20[g];
+    const double x = t - c;
+    const double R2 = x * x + a * a;
+    const double R = sqrt(R2);
+    double K = 1.0 / R;
+    if (EK) K += (a * a / (4.0 * R2 * R2 * R)) * (3.0 * a * a - 2.0 * R2);
+    double W[D + 1][D + 1];
+    conv_weights<D>(h, t, W);
+    const double wk = half * gl.w20[g] * K;
+#pragma unroll
+    for (int p = 0; p <= D; ++p)
+#pragma unroll
+        for (int q = 0; q <= D; ++q) acc[p][q] += wk * W[p][q];
+}
+
+template <int N>
+__device__ __forceinline__ void warp_sum(double (&v)[N]) {
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v[i] += __shfl_xor_sync(0xffffffffu, v[i], off);
 }
 
 // Table modes: kTableFused writes static + smooth parts for one k per
@@ -145,18 +167,20 @@ __device__ void static_half(double lo, double hi, double c, double h, double a,
 // part is k-independent: it is written, as the real part, into all n_k
 // tables) and then kTableSmoothAdd per k, which adds the smooth part.
 enum { kTableFused = 0, kTableStatic = 1, kTableSmoothAdd = 2 };
+constexpr int kTableThreads = 128;  // one warp per table row
 
+// One warp per same-edge table row: the lanes split the static quadrature
+// points and the nq x nq smooth-part samples, then reduce with shuffles.
 template <int D, bool EK>
-__global__ void same_edge_table_kernel(int n_edge, const int32_t* __restrict__ n_in_edge,
-                                       const int64_t* __restrict__ table_off,
-                                       const double* __restrict__ hs, const double* __restrict__ radii,
-                                       int64_t rows, double k0, GLParams gl, double* __restrict__ out,
-                                       const double* __restrict__ kb, int64_t out_stride, int mode = kTableFused,
-                                       int n_k = 1) {
-    constexpr int NM = D + 1;
-    int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (row >= rows) return;
-    // frequency batch: blockIdx.y selects k and the output table
+__global__ void __launch_bounds__(kTableThreads) same_edge_table_kernel(
+    int n_edge, const int32_t* __restrict__ n_in_edge, const int64_t* __restrict__ table_off,
+    const double* __restrict__ hs, const double* __restrict__ radii, int64_t rows, double k0, GLParams gl,
+    double* __restrict__ out, const double* __restrict__ kb, int64_t out_stride, int mode = kTableFused,
+    int n_k = 1) {
+    constexpr int NM = D + 1, NE = NM * NM * 2;
+    const int lane = threadIdx.x & 31;
+    const int64_t row = blockIdx.x * (int64_t)(kTableThreads / 32) + (threadIdx.x >> 5);
+    if (row >= rows) return;  // uniform per warp
     const double k = kb ? kb[blockIdx.y] : k0;
     double* const out0 = out;
     out += blockIdx.y * out_stride;
@@ -166,86 +190,90 @@ __global__ void same_edge_table_kernel(int n_edge, const int32_t* __restrict__ n
         int mid = (lo + hi + 1) >> 1;
         if (table_off[mid] <= row) lo = mid; else hi = mid - 1;
     }
-    int e = lo;
-    int n = n_in_edge[e];
-    int delta = (int)(row - table_off[e]) - (n - 1);
-    double h = hs[e], a = radii[e];
-    double c = delta * h;
+    const int e = lo;
+    const int n = n_in_edge[e];
+    const int delta = (int)(row - table_off[e]) - (n - 1);
+    const double h = hs[e], a = radii[e];
+    const double c = delta * h;
 
-    double st[NM][NM];
+    double st[NM * NM];
 #pragma unroll
-    for (int p = 0; p < NM; ++p)
-#pragma unroll
-        for (int q = 0; q < NM; ++q) st[p][q] = 0.0;
+    for (int i = 0; i < NM * NM; ++i) st[i] = 0.0;
     if (mode != kTableSmoothAdd) {
-        static_half<D, EK>(-h, 0.0, c, h, a, gl, st);
-        static_half<D, EK>(0.0, h, c, h, a, gl, st);
+        bool g0, l0, g1, l1;
+        const int n0 = half_panels(-h, 0.0, c, a, g0, l0);
+        const int n1 = half_panels(0.0, h, c, a, g1, l1);
+        double acc[NM][NM];
+#pragma unroll
+        for (int p = 0; p < NM; ++p)
+#pragma unroll
+            for (int q = 0; q < NM; ++q) acc[p][q] = 0.0;
+        for (int g = lane; g < 20 * (n0 + n1); g += 32) {
+            const int pi = g / 20, gi = g - pi * 20;
+            double x0, x1;
+            if (pi < n0) half_panel_bounds(-h, 0.0, a, g0, l0, pi, x0, x1);
+            else         half_panel_bounds(0.0, h, a, g1, l1, pi - n0, x0, x1);
+            static_point<D, EK>(x0, x1, gi, c, h, a, gl, acc);
+        }
+#pragma unroll
+        for (int p = 0; p < NM; ++p)
+#pragma unroll
+            for (int q = 0; q < NM; ++q) st[p * NM + q] = kInv4Pi * acc[p][q];
+        warp_sum(st);
     }
     if (mode == kTableStatic) {
-        for (int b = 0; b < n_k; ++b) {
-            double* o = out0 + b * out_stride + row * (NM * NM * 2);
-#pragma unroll
-            for (int p = 0; p < NM; ++p)
-#pragma unroll
-                for (int q = 0; q < NM; ++q) {
-                    o[(p * NM + q) * 2 + 0] = kInv4Pi * st[p][q];
-                    o[(p * NM + q) * 2 + 1] = 0.0;
-                }
+        for (int idx = lane; idx < n_k * NE; idx += 32) {
+            const int b = idx / NE, x = idx - b * NE;
+            out0[b * out_stride + row * NE + x] = (x & 1) ? 0.0 : st[x >> 1];
         }
         return;
     }
 
     // smooth part: (exp(-jkR) - 1)/(4 pi R) on nq x nq Gauss points
-    cd rg[NM][NM];
+    double rg[NE];
 #pragma unroll
-    for (int p = 0; p < NM; ++p)
-#pragma unroll
-        for (int q = 0; q < NM; ++q) rg[p][q] = cd{0.0, 0.0};
-    for (int qi = 0; qi < gl.nq; ++qi) {
-        double u = gl.t[qi] * h, wu = gl.w[qi] * h;
-        cd accP[NM];
-#pragma unroll
-        for (int P = 0; P < NM; ++P) accP[P] = cd{0.0, 0.0};
-        for (int ri = 0; ri < gl.nq; ++ri) {
-            double v = gl.t[ri] * h, wv = gl.w[ri] * h;
-            double x = u - v - c;
-            double R = sqrt(x * x + a * a);
-            double s, co, sh, ch;
-            sincos(k * R, &s, &co);
-            sincos(0.5 * k * R, &sh, &ch);
-            // exp(-jkR) - 1 = -2 sin^2(kR/2) - j sin(kR)
-            cd num = cd{-2.0 * sh * sh, -s};
-            if (EK) num = num * ek_factor(R, a, k) + ek_reg_extra(R, a, k);
-            double g = kInv4Pi / R;
-            cd G = cd{num.re * g, num.im * g};
-            double vp = wv;
-#pragma unroll
-            for (int P = 0; P < NM; ++P) {
-                accP[P] = accP[P] + vp * G;
-                vp *= v;
-            }
-        }
+    for (int i = 0; i < NE; ++i) rg[i] = 0.0;
+    for (int smp = lane; smp < gl.nq * gl.nq; smp += 32) {
+        const int qi = smp / gl.nq, ri = smp - qi * gl.nq;
+        const double u = gl.t[qi] * h, wu = gl.w[qi] * h;
+        const double v = gl.t[ri] * h, wv = gl.w[ri] * h;
+        const double x = u - v - c;
+        const double R = sqrt(x * x + a * a);
+        double s, co, sh, ch;
+        sincos(k * R, &s, &co);
+        sincos(0.5 * k * R, &sh, &ch);
+        // exp(-jkR) - 1 = -2 sin^2(kR/2) - j sin(kR)
+        cd num = cd{-2.0 * sh * sh, -s};
+        if (EK) num = num * ek_factor(R, a, k) + ek_reg_extra(R, a, k);
+        const double g = kInv4Pi / R;
+        const cd G = cd{num.re * g, num.im * g};
         double up = wu;
 #pragma unroll
         for (int p = 0; p < NM; ++p) {
+            double vp = wv;
 #pragma unroll
-            for (int P = 0; P < NM; ++P) rg[p][P] = rg[p][P] + up * accP[P];
+            for (int P = 0; P < NM; ++P) {
+                rg[(p * NM + P) * 2 + 0] += up * vp * G.re;
+                rg[(p * NM + P) * 2 + 1] += up * vp * G.im;
+                vp *= v;
+            }
             up *= u;
         }
     }
-    double* o = out + row * (NM * NM * 2);
+    warp_sum(rg);
+    if (lane < NE) {
+        double* o = out + row * NE + lane;
+        // rg[lane] with a lane-dependent index: pick it with a static loop
+        double mine = 0.0, stat = 0.0;
 #pragma unroll
-    for (int p = 0; p < NM; ++p)
+        for (int i = 0; i < NE; ++i)
+            if (i == lane) mine = rg[i];
 #pragma unroll
-        for (int q = 0; q < NM; ++q) {
-            if (mode == kTableSmoothAdd) {
-                o[(p * NM + q) * 2 + 0] += rg[p][q].re;
-                o[(p * NM + q) * 2 + 1] += rg[p][q].im;
-            } else {
-                o[(p * NM + q) * 2 + 0] = kInv4Pi * st[p][q] + rg[p][q].re;
-                o[(p * NM + q) * 2 + 1] = rg[p][q].im;
-            }
-        }
+        for (int i = 0; i < NM * NM; ++i)
+            if (2 * i == lane) stat = st[i];
+        if (mode == kTableSmoothAdd) *o += mine;
+        else *o = stat + mine;
+    }
 }
 
 // --------------------------------------------------------------------------
@@ -832,8 +860,8 @@ extern "C" mw_status mw_same_edge_table(const mw_edges* edges, int32_t degree, i
     MW_REQUIRE(n_qp >= 1 && n_qp <= 8, "n_qp_pair must be in [1, 8] (got %d)", n_qp);
     if (edges->table_rows == 0) return MW_OK;
     GLParams gl = make_gl(n_qp);
-    int threads = 128;
-    int64_t blocks = (edges->table_rows + threads - 1) / threads;
+    const int threads = kTableThreads, rows_per_block = kTableThreads / 32;
+    int64_t blocks = (edges->table_rows + rows_per_block - 1) / rows_per_block;
     cudaStream_t st = as_stream(stream);
     ProfileScope ps(PC_TABLE, st);
 #define MW_TBL(DD, EE)                                                                                 \
@@ -947,8 +975,8 @@ extern "C" mw_status mw_fill_z_batch(const mw_segments* seg, const mw_basis* bas
     cudaStream_t st = as_stream(stream);
     if (edges->table_rows > 0) {
         ProfileScope ps(PC_TABLE, st);
-        const int threads = 128;
-        const unsigned bx = (unsigned)((edges->table_rows + threads - 1) / threads);
+        const int threads = kTableThreads, rows_per_block = kTableThreads / 32;
+        const unsigned bx = (unsigned)((edges->table_rows + rows_per_block - 1) / rows_per_block);
         const bool ek = extended_kernel != 0;
         // the k-independent static part once into every table, then the
         // smooth part per k

@@ -120,7 +120,7 @@ extern "C" mw_status mw_zgesv_mixed(int64_t n, int64_t nrhs, const double* Z, in
     }
     // X = 0, R = B
     MW_CHECK_CUDA(cudaMemsetAsync(norms, 0, sizeof(double) * 2 * nrhs, st));
-    for (int64_t j = 0; j < nrhs; ++j) MW_CHECK_CUDA(cudaMemsetAsync(Xc + j * ldx, 0, sizeof(cd) * n, st));
+    MW_CHECK_CUDA(cudaMemset2DAsync(Xc, sizeof(cd) * ldx, 0, sizeof(cd) * n, nrhs, st));
     copy_c128_kernel<<<grid_for(tot), 256, 0, st>>>(Bc, ldb, R, n, n, nrhs);
     count_launch();
     double corr = INFINITY;

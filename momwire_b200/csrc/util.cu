@@ -44,9 +44,42 @@ __global__ void add_loading_kernel(int64_t n, int batch, int64_t nnz, const int6
     }
 }
 
+// Pad each of `count` matrices (column-major, order nb, the leading n x n
+// block already filled) to [[Z, 0], [0, I]]: rows n..nb-1 of the first n
+// columns and all of columns n..nb-1 are written, the diagonal with 1.
+__global__ void pad_identity_kernel(int64_t n, int64_t nb, double2* __restrict__ Z, int64_t ldz, int64_t sz,
+                                    float2* __restrict__ Z32, int64_t ld32, int64_t s32) {
+    const int64_t col = blockIdx.x, b = blockIdx.y;
+    const int64_t r0 = col < n ? n : 0;
+    double2* z = Z + b * sz + col * ldz;
+    float2* z32 = Z32 ? Z32 + b * s32 + col * ld32 : nullptr;
+    for (int64_t r = r0 + threadIdx.x; r < nb; r += blockDim.x) {
+        const double v = (r == col) ? 1.0 : 0.0;
+        z[r] = make_double2(v, 0.0);
+        if (z32) z32[r] = make_float2((float)v, 0.f);
+    }
+}
+
 }  // namespace mw
 
 using namespace mw;
+
+extern "C" mw_status mw_pad_identity(int64_t n, int64_t nb, int32_t count, double* Z, int64_t ldz, int64_t z_stride,
+                                     float* Z32, int64_t ld32, int64_t z32_stride, void* stream) {
+    MW_REQUIRE(n >= 0 && nb >= n && count >= 0 && count <= 65535, "bad sizes");
+    MW_REQUIRE(ldz >= nb && (Z32 == nullptr || ld32 >= nb), "leading dimension smaller than nb");
+    MW_REQUIRE(count <= 1 || (z_stride >= ldz * nb && (Z32 == nullptr || z32_stride >= ld32 * nb)),
+               "batch stride smaller than one matrix");
+    if (nb == n || count == 0) return MW_OK;
+    MW_REQUIRE(Z != nullptr, "NULL Z");
+    MW_REQUIRE(nb <= 0x7fffffff, "nb too large");
+    cudaStream_t st = as_stream(stream);
+    pad_identity_kernel<<<dim3((unsigned)nb, (unsigned)count), 128, 0, st>>>(
+        n, nb, reinterpret_cast<double2*>(Z), ldz, z_stride, reinterpret_cast<float2*>(Z32), ld32, z32_stride);
+    MW_CHECK_CUDA(cudaGetLastError());
+    count_launch();
+    return MW_OK;
+}
 
 extern "C" mw_status mw_add_loading(int64_t n, int32_t batch, int64_t nnz, const int64_t* rows, const int64_t* cols,
                                     const double* vals, const int32_t* wire, const double* zw, int32_t n_wires,

@@ -107,6 +107,174 @@ def gather(local, group=None):
     return merged
 
 
+def _ladder():
+    """Padded orders for grouping: multiples of 32 growing by about 20 %."""
+    out, v = [], 64
+    while v <= 8192:
+        out.append(v)
+        v = -(-int(v * 1.2) // 32) * 32
+    return out
+
+
+LADDER = _ladder()
+
+
+def padded_order(n):
+    """The smallest ladder order >= n (multiples of 64 beyond the ladder)."""
+    for v in LADDER:
+        if v >= n:
+            return v
+    return -(-int(n) // 64) * 64
+
+
+def group_plan(orders, n_k, budget_bytes, bytes_per_matrix):
+    """Groups of structure indices sharing one padded order: [(nb, [i, ...])].
+    Members are in index order; a group holds at most 65535 matrices and
+    ``budget_bytes`` of ``bytes_per_matrix(nb)`` each."""
+    buckets = {}
+    for i, n in enumerate(orders):
+        buckets.setdefault(padded_order(n), []).append(i)
+    plan = []
+    for nb in sorted(buckets):
+        per = max(1, int(n_k) * int(bytes_per_matrix(nb)))
+        cap = max(1, min(65535 // max(1, int(n_k)), int(budget_bytes // per)))
+        idx = buckets[nb]
+        for c in range(0, len(idx), cap):
+            plan.append((nb, idx[c : c + cap]))
+    return plan
+
+
+def _solve_group(solvers, nb, ks, stream, pw=None):
+    """Batched mixed solve of several structures at the frequencies ks in
+    one factorisation: each structure's n x n matrices are filled into the
+    leading block of order-nb matrices padded with the identity
+    (mw_pad_identity), so every (structure, frequency) system is one matrix
+    of one batch.  Returns ({position: Y stack (n_k, P, P)}, iterations)."""
+    import ctypes as C
+
+    import torch
+
+    from . import _lib
+
+    lib = _lib.load()
+    dev = solvers[0]._torch_device()
+    nk = len(ks)
+    G = len(solvers)
+    count = G * nk
+    Bs = [s._port_columns()[0] for s in solvers]
+    P = max(B.shape[1] for B in Bs)
+    Z = torch.empty((count, nb, nb), dtype=torch.complex128, device=dev)
+    Z32 = torch.empty((count, nb, nb), dtype=torch.complex64, device=dev)
+    Bd = torch.zeros((count, P, nb), dtype=torch.complex128, device=dev)
+    for g, (s, B) in enumerate(zip(solvers, Bs)):
+        n = s._basis().n
+        zb, z32b = Z[g * nk : (g + 1) * nk], Z32[g * nk : (g + 1) * nk]
+        s._fill_batched(ks, stream, Z=zb, Z32=z32b, ld=nb)
+        _lib.call("mw_pad_identity", n, nb, nk, zb.data_ptr(), nb, nb * nb, z32b.data_ptr(), nb, nb * nb, stream)
+        Bt = torch.from_numpy(np.ascontiguousarray(B.T)).to(dev)
+        Bd[g * nk : (g + 1) * nk, : B.shape[1], :n] = Bt
+    if pw is None:
+        pw = _group_width(solvers[0], nb, Z, Z32, Bd, P, stream)
+    X = torch.empty((count, P, nb), dtype=torch.complex128, device=dev)
+    ipiv = torch.empty((count, nb), dtype=torch.int32, device=dev)
+    info = torch.zeros(count, dtype=torch.int32, device=dev)
+    wsb = lib.mw_zgesv_mixed_batched_workspace_size(nb, P, count)
+    ws = torch.empty(wsb, dtype=torch.uint8, device=dev)
+    it, corr = C.c_int32(0), C.c_double(0.0)
+    s0 = solvers[0]
+    _lib.call("mw_zgesv_mixed_batched", nb, P, count, int(pw), Z.data_ptr(), nb, nb * nb, Z32.data_ptr(), nb,
+              nb * nb, ipiv.data_ptr(), info.data_ptr(), Bd.data_ptr(), nb, P * nb, X.data_ptr(),
+              float(s0.mixed_tol), int(s0.mixed_max_iter), ws.data_ptr(), wsb, C.byref(it), C.byref(corr), stream)
+    Xh = X.cpu().numpy()
+    out = {}
+    for g, (s, B) in enumerate(zip(solvers, Bs)):
+        n, p = B.shape
+        out[g] = np.einsum("kpn,nq->kqp", Xh[g * nk : (g + 1) * nk, :p, :n], B)
+    return out, int(it.value)
+
+
+def _group_width(s0, nb, Z, Z32, Bd, P, stream):
+    """Panel width for padded order nb: the autotuner's cached choice, else
+    timed on up to 64 matrices of this group (their complex64 copies are
+    factored in scratch buffers)."""
+    import ctypes as C
+
+    import torch
+
+    from . import _lib, autotune
+
+    lib = _lib.load()
+    m = min(Z.shape[0], 64)
+
+    def time_width(w):
+        z32 = Z32[:m].clone()
+        X = torch.empty((m, P, nb), dtype=torch.complex128, device=Z.device)
+        ipiv = torch.empty((m, nb), dtype=torch.int32, device=Z.device)
+        info = torch.zeros(m, dtype=torch.int32, device=Z.device)
+        wsb = lib.mw_zgesv_mixed_batched_workspace_size(nb, P, m)
+        ws = torch.empty(wsb, dtype=torch.uint8, device=Z.device)
+        st = torch.cuda.current_stream(Z.device)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ms = []
+        for _rep in range(2):  # the first run warms up
+            z32.copy_(Z32[:m])
+            it, corr = C.c_int32(0), C.c_double(0.0)
+            a.record(st)
+            _lib.call("mw_zgesv_mixed_batched", nb, P, m, int(w), Z.data_ptr(), nb, nb * nb, z32.data_ptr(), nb,
+                      nb * nb, ipiv.data_ptr(), info.data_ptr(), Bd.data_ptr(), nb, P * nb, X.data_ptr(),
+                      float(s0.mixed_tol), int(s0.mixed_max_iter), ws.data_ptr(), wsb, C.byref(it),
+                      C.byref(corr), stream)
+            b.record(st)
+            b.synchronize()
+            ms.append(a.elapsed_time(b))
+        return ms[-1]
+
+    return autotune.choose(nb, 0, "grouped", time_width)
+
+
+def grouped_mixed_sweep(structs, ks, device=None, budget_bytes=32 << 30, indices=None):
+    """{index: (n_k, P, P) Y stack} for the given structures, every one at
+    the frequencies ks, through grouped batched solves: structures are
+    bucketed by padded order (``padded_order``), and each group's
+    (structure, frequency) systems are filled into one padded stack and
+    factorised by one batched mixed-precision solve.  Structures the batched
+    route does not serve (finite grounds, KCL constraint rows, orders above
+    the batched panel's limit) take their own ``compute_y_matrix_swept``."""
+    import torch
+
+    import momwire_b200
+
+    from . import _lib
+
+    indices = list(range(len(structs))) if indices is None else list(indices)
+    solvers = {i: momwire_b200.BSplineSolver(**structs[i], precision="mixed", device=device) for i in indices}
+    out = {}
+    grouped = []
+    for i in indices:
+        s = solvers[i]
+        if s._swept_batched_available() and padded_order(s._basis().n) <= 1600:
+            grouped.append(i)
+        else:
+            out[i] = s.compute_y_matrix_swept(ks)
+    if not grouped:
+        return out
+    lib = _lib.load()
+    ks = np.asarray(ks, dtype=np.float64)
+
+    def per_matrix(nb):
+        return nb * nb * 24 + lib.mw_zgesv_mixed_batched_workspace_size(nb, 1, 1) + nb * 64
+
+    plan = group_plan([solvers[i]._basis().n for i in grouped], len(ks), budget_bytes, per_matrix)
+    dev = solvers[grouped[0]]._torch_device()
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    for nb, members in plan:
+        ids = [grouped[j] for j in members]
+        res, _it = _solve_group([solvers[i] for i in ids], nb, ks, stream)
+        for g, i in enumerate(ids):
+            out[i] = res[g]
+    return out
+
+
 def mixed_sweep_fn(device=None):
     """solve_fn for ``solve_shard``: the batched mixed-precision sweep of one
     structure on this rank's GPU."""

@@ -133,3 +133,54 @@ def test_batched_sweep_panel_widths(width, cuda_device):
     for i in range(len(ks)):
         z64, zmx = _zin(y64[i]), _zin(ymx[i])
         assert np.max(np.abs(zmx - z64) / np.abs(z64)) <= 1e-6
+
+
+def test_grouped_sweep_matches_per_structure(cuda_device):
+    """Structures of different orders, port counts, grounds and loading in
+    padded groups against each structure's own complex128 per-k solves."""
+    from momwire_b200 import sweep
+    from momwire_b200.workloads import yagi_sweep
+
+    structs, ks = yagi_sweep(n_structures=4, n_freq=6, seed=3)
+    structs = structs + [CASES["d1_multifeed"](), CASES["d2_pec"](), CASES["d2_loaded_dipole"](),
+                         CASES["d2_junction_port"]()]
+    kss = np.linspace(0.95, 1.05, 6)
+    out = {}
+    for i, kw in enumerate(structs):
+        k0 = momwire_b200.BSplineSolver(**kw).k if i >= 4 else None
+        out[i] = ks if k0 is None else kss * k0
+    # one frequency list per call: group the Yagis, then the rest one by one
+    got = sweep.grouped_mixed_sweep(structs, ks, indices=range(4))
+    for i in range(4):
+        y64 = momwire_b200.BSplineSolver(**structs[i]).compute_y_matrix_swept(ks)
+        z64, zg = 1.0 / y64[:, 0, 0], 1.0 / got[i][:, 0, 0]
+        assert np.max(np.abs(zg - z64) / np.abs(z64)) <= 1e-6
+    for i in range(4, len(structs)):
+        got = sweep.grouped_mixed_sweep(structs, out[i], indices=[i])
+        y64 = momwire_b200.BSplineSolver(**structs[i]).compute_y_matrix_swept(out[i])
+        for j in range(len(out[i])):
+            z64, zg = _zin(y64[j]), _zin(got[i][j])
+            assert np.max(np.abs(zg - z64) / np.abs(z64)) <= 1e-6
+
+
+def test_grouped_sweep_shares_one_factorisation(cuda_device):
+    """Two structures of different orders in one padded group give the same
+    Y as each one batched alone."""
+    from momwire_b200 import sweep
+    from momwire_b200.workloads import yagi_sweep
+
+    structs, ks = yagi_sweep(n_structures=12, n_freq=4, seed=5)
+    ns = [momwire_b200.BSplineSolver(**kw)._basis().n for kw in structs]
+    pairs = [(i, j) for i in range(12) for j in range(i + 1, 12)
+             if ns[i] != ns[j] and sweep.padded_order(ns[i]) == sweep.padded_order(ns[j])]
+    assert pairs, ns
+    i, j = pairs[0]
+    solvers = [momwire_b200.BSplineSolver(**structs[x], precision="mixed") for x in (i, j)]
+    import torch
+
+    st = torch.cuda.current_stream().cuda_stream
+    nb = sweep.padded_order(ns[i])
+    together, _ = sweep._solve_group(solvers, nb, ks, st, pw=16)
+    for g, x in enumerate((i, j)):
+        alone = momwire_b200.BSplineSolver(**structs[x], precision="mixed").compute_y_matrix_swept(ks)
+        assert np.max(np.abs(together[g] - alone) / np.abs(alone)) <= 1e-6

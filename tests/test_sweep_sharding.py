@@ -64,3 +64,27 @@ def test_two_rank_gather_matches_single_rank():
     structs, _ks = yagi_sweep(n_structures=9, n_freq=3, seed=1)
     want = {i: complex(sum(kw["n_per_edge_per_wire"]), len(kw["wires"])) for i, kw in enumerate(structs)}
     assert got == want
+
+
+def test_padded_order_ladder():
+    """Padded orders are multiples of 32, at most ~20 % above n, monotone."""
+    prev = 0
+    for n in range(1, 3000, 7):
+        nb = sweep.padded_order(n)
+        assert nb >= n and nb % 32 == 0 and nb >= prev
+        assert nb <= max(64, int(n * 1.2) + 64)
+        prev = nb
+
+
+def test_group_plan_caps_memory_and_batch():
+    orders = [40, 60, 500, 470, 481, 1000, 990, 65]
+    plan = sweep.group_plan(orders, 64, budget_bytes=3 * 64 * 480 * 480 * 24, bytes_per_matrix=lambda nb: nb * nb * 24)
+    seen = sorted(i for _nb, g in plan for i in g)
+    assert seen == list(range(len(orders)))
+    for nb, g in plan:
+        assert all(sweep.padded_order(orders[i]) == nb for i in g)
+        assert len(g) * 64 * nb * nb * 24 <= 3 * 64 * 480 * 480 * 24 or len(g) == 1
+    # 65535 matrices at most per group
+    plan = sweep.group_plan([100] * 2000, 64, budget_bytes=1 << 60, bytes_per_matrix=lambda nb: 1)
+    assert all(len(g) * 64 <= 65535 for _nb, g in plan)
+    assert sum(len(g) for _nb, g in plan) == 2000

@@ -1118,8 +1118,24 @@ class BSplineSolver:
         split, order within the batched panel's limit."""
         if self.precision != "mixed" or self.ground_eps is not None:
             return False
-        kcl, _pa, _pv = self._split_kcl_ports(self._basis().kcl_A)
-        return kcl.shape[0] == 0 and self._basis().n <= 1600
+        return self._kcl_rows_left() == 0 and self._basis_count() <= 1600
+
+    def _basis_count(self):
+        """Order of the system without building the basis: per wire its
+        segments + d - 2 interior bases plus the end bases a junction or the
+        ground holds (the rule of ``_tables.build_basis``)."""
+        if self._cached_basis is not None:
+            return self._basis().n
+        st, en = self._wire_endpoint_status()
+        d = self.degree
+        return int(sum(sum(npe) + d - 2 + (st[w] != "free") + (en[w] != "free")
+                       for w, npe in enumerate(self.n_per_edge_per_wire)))
+
+    def _kcl_rows_left(self):
+        """KCL constraint rows that stay after the junction-port split: one
+        per junction off the ground, less the junction ports."""
+        grounded = self._grounded_junctions()
+        return sum(1 for j in range(len(self.junctions)) if j not in grounded) - len(self.junction_ports)
 
     def _fill_batched(self, ks, stream, Z=None, Z32=None, ld=None):
         """(Z, Z32): device (n_k, n, n) complex128 / complex64 stacks, each

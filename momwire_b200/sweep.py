@@ -144,7 +144,7 @@ def group_plan(orders, n_k, budget_bytes, bytes_per_matrix):
     return plan
 
 
-def _solve_group(solvers, nb, ks, stream, pw=None):
+def _solve_group(solvers, nb, ks, stream, pw=None, Bs=None):
     """Batched mixed solve of several structures at the frequencies ks in
     one factorisation: each structure's n x n matrices are filled into the
     leading block of order-nb matrices padded with the identity
@@ -161,7 +161,8 @@ def _solve_group(solvers, nb, ks, stream, pw=None):
     nk = len(ks)
     G = len(solvers)
     count = G * nk
-    Bs = [s._port_columns()[0] for s in solvers]
+    if Bs is None:
+        Bs = [s._port_columns()[0] for s in solvers]
     P = max(B.shape[1] for B in Bs)
     Z = torch.empty((count, nb, nb), dtype=torch.complex128, device=dev)
     Z32 = torch.empty((count, nb, nb), dtype=torch.complex64, device=dev)
@@ -252,7 +253,7 @@ def grouped_mixed_sweep(structs, ks, device=None, budget_bytes=32 << 30, indices
     grouped = []
     for i in indices:
         s = solvers[i]
-        if s._swept_batched_available() and padded_order(s._basis().n) <= 1600:
+        if s._swept_batched_available() and padded_order(s._basis_count()) <= 1600:
             grouped.append(i)
         else:
             out[i] = s.compute_y_matrix_swept(ks)
@@ -264,14 +265,31 @@ def grouped_mixed_sweep(structs, ks, device=None, budget_bytes=32 << 30, indices
     def per_matrix(nb):
         return nb * nb * 24 + lib.mw_zgesv_mixed_batched_workspace_size(nb, 1, 1) + nb * 64
 
-    plan = group_plan([solvers[i]._basis().n for i in grouped], len(ks), budget_bytes, per_matrix)
+    plan = group_plan([solvers[i]._basis_count() for i in grouped], len(ks), budget_bytes, per_matrix)
     dev = solvers[grouped[0]]._torch_device()
     stream = torch.cuda.current_stream(dev).cuda_stream
-    for nb, members in plan:
-        ids = [grouped[j] for j in members]
-        res, _it = _solve_group([solvers[i] for i in ids], nb, ks, stream)
-        for g, i in enumerate(ids):
-            out[i] = res[g]
+    # one host thread prepares the next structures' tables (host build and
+    # upload on its own stream) while this thread fills and solves
+    import concurrent.futures as cf
+
+    prep_stream = torch.cuda.Stream(device=dev)
+    ports = {}
+
+    def prep(i):
+        with torch.cuda.device(dev), torch.cuda.stream(prep_stream):
+            solvers[i]._dev_tables()
+            ports[i] = solvers[i]._port_columns()[0]
+            prep_stream.synchronize()
+
+    with cf.ThreadPoolExecutor(max_workers=1) as ex:
+        futs = {grouped[j]: ex.submit(prep, grouped[j]) for _nb, members in plan for j in members}
+        for nb, members in plan:
+            ids = [grouped[j] for j in members]
+            for i in ids:
+                futs[i].result()
+            res, _it = _solve_group([solvers[i] for i in ids], nb, ks, stream, Bs=[ports[i] for i in ids])
+            for g, i in enumerate(ids):
+                out[i] = res[g]
     return out
 
 

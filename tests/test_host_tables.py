@@ -135,3 +135,13 @@ def test_constructor_validation_messages():
         momwire_b200.BSplineSolver(wires=w, junction_ports=[0])
     with pytest.raises(NotImplementedError, match="ground plane"):
         momwire_b200.BSplineSolver(wires=w, ground_z=0.0, ground_eps=(13, 0.005))
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_basis_count_and_kcl_rows_without_building(name):
+    s = momwire_b200.BSplineSolver(**CASES[name]())
+    n = s._basis_count()
+    left = s._kcl_rows_left()
+    assert n == s._basis().n
+    kcl, _pa, _pv = s._split_kcl_ports(s._basis().kcl_A)
+    assert left == kcl.shape[0]

@@ -868,6 +868,23 @@ class BSplineSolver:
         np.add.at(per_wire, g.wire, contrib)
         return float(per_wire.sum()), per_wire
 
+    def _loading_dev_tables(self):
+        """Device copies of the coalesced Gram entries (rows, cols, vals,
+        wire), uploaded once per solver; None without loading."""
+        if self._loading is None:
+            return None
+        if self._cached_loading_dev is None:
+            torch = _torch()
+            dev = self._torch_device()
+            g = self._loading_tables()
+            self._cached_loading_dev = (
+                torch.from_numpy(g.u_rows.astype(np.int64)).to(dev),
+                torch.from_numpy(g.u_cols.astype(np.int64)).to(dev),
+                torch.from_numpy(g.u_vals.astype(np.float64)).to(dev),
+                torch.from_numpy(g.u_wire.astype(np.int32)).to(dev),
+            )
+        return self._cached_loading_dev
+
     def _loading_device(self, Z, Z32, omegas, stream, ld=None):
         """Z_b += sum_w Z'_w(omega_b) S_w on the device for a stack of
         column-major matrices (Z: (n_k, ld, ld) or (ld, ld) tensor, ld = n
@@ -877,18 +894,12 @@ class BSplineSolver:
         torch = _torch()
         dev = self._torch_device()
         n = self._basis().n
-        if self._cached_loading_dev is None:
-            g = self._loading_tables()
-            self._cached_loading_dev = (
-                torch.from_numpy(g.u_rows.astype(np.int64)).to(dev),
-                torch.from_numpy(g.u_cols.astype(np.int64)).to(dev),
-                torch.from_numpy(g.u_vals.astype(np.float64)).to(dev),
-                torch.from_numpy(g.u_wire.astype(np.int32)).to(dev),
-            )
-        rows, cols, vals, wire = self._cached_loading_dev
+        rows, cols, vals, wire = self._loading_dev_tables()
         omegas = np.atleast_1d(np.asarray(omegas, dtype=np.float64))
         zw = np.ascontiguousarray(self._loading.z_wire(omegas).T)  # (batch, n_wires)
-        zt = torch.from_numpy(zw).to(dev)
+        zh = torch.empty(zw.shape, dtype=torch.complex128, pin_memory=True)
+        zh.copy_(torch.from_numpy(zw))
+        zt = zh.to(dev, non_blocking=True)
         batch = omegas.size
         ld = n if ld is None else int(ld)
         _lib.call("mw_add_loading", n, batch, rows.numel(), rows.data_ptr(), cols.data_ptr(), vals.data_ptr(),
@@ -1137,19 +1148,22 @@ class BSplineSolver:
         grounded = self._grounded_junctions()
         return sum(1 for j in range(len(self.junctions)) if j not in grounded) - len(self.junction_ports)
 
-    def _fill_batched(self, ks, stream, Z=None, Z32=None, ld=None):
+    def _fill_batched(self, ks, stream, Z=None, Z32=None, ld=None, k_dev=None):
         """(Z, Z32): device (n_k, n, n) complex128 / complex64 stacks, each
         matrix column-major (Z[b].T is the matrix at ks[b]), from one
         batched fill launch.  Given Z / Z32 of shape (n_k, ld, ld) with
-        ld >= n, the fill writes the leading n x n block of each."""
+        ld >= n, the fill writes the leading n x n block of each.  k_dev:
+        the (2, n_k) float64 device tensor [k; omega] when the caller has
+        uploaded it already (a pageable upload would wait for the stream)."""
         torch = _torch()
         dev = self._torch_device()
         dt = self._dev_tables()
         n, d = self._basis().n, self.degree
         nk = len(ks)
         ld = n if ld is None else int(ld)
-        kb = torch.from_numpy(np.asarray(ks, dtype=np.float64)).to(dev)
-        ob = torch.from_numpy(np.asarray(ks, dtype=np.float64) * self.c).to(dev)
+        if k_dev is None:
+            k_dev = self._upload_k(ks)
+        kb, ob = k_dev[0], k_dev[1]
         table = torch.empty((nk, max(dt.table_rows, 1), d + 1, d + 1), dtype=torch.complex128, device=dev)
         if Z is None:
             Z = torch.empty((nk, ld, ld), dtype=torch.complex128, device=dev)
@@ -1162,6 +1176,15 @@ class BSplineSolver:
                   ld, ld * ld, stream)
         self._loading_device(Z, Z32, np.asarray(ks, dtype=np.float64) * self.c, stream, ld=ld)
         return Z, Z32
+
+    def _upload_k(self, ks):
+        """[k; omega] (2, n_k) float64 on the device, through page-locked
+        memory with a stream-ordered copy (no host wait on queued work)."""
+        torch = _torch()
+        h = torch.empty((2, len(ks)), dtype=torch.float64, pin_memory=True)
+        h[0] = torch.from_numpy(np.asarray(ks, dtype=np.float64))
+        h[1] = torch.from_numpy(np.asarray(ks, dtype=np.float64) * self.c)
+        return h.to(self._torch_device(), non_blocking=True)
 
     def _batched_panel_width(self, ks):
         """Columns per batched panel step for this order: the autotuner's
@@ -1207,7 +1230,9 @@ class BSplineSolver:
         chunk = int(max(1, min(len(k_array), 65535, mem_budget_bytes // max(per_k, 1))))
         st = torch.cuda.current_stream(dev).cuda_stream
         lib = _lib.load()
-        Bd = torch.from_numpy(np.ascontiguousarray(B.T)).to(dev)  # column-major n x n_p
+        Bh = torch.empty((n_p, n), dtype=torch.complex128, pin_memory=True)
+        Bh.copy_(torch.from_numpy(np.ascontiguousarray(B.T)))
+        Bd = Bh.to(dev, non_blocking=True)  # column-major n x n_p
         out = np.zeros((len(k_array), n_p, n_p), dtype=np.complex128)
         iters = []
         for c0 in range(0, len(k_array), chunk):

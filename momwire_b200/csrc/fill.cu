@@ -726,8 +726,12 @@ __device__ __forceinline__ void tri_pair(int64_t b, int& tr, int& tc) {
 // computed once and written to both blocks of Z; otherwise the block also
 // computes (tc, tr) itself.  The EK image fill labels direct and mirrored
 // segments separately, so it always computes both.
+#ifndef MW_FILL_MIN_BLOCKS
+#define MW_FILL_MIN_BLOCKS 3  // resident CTAs per SM the register allocation must allow
+#endif
+
 template <int D, bool IMAGE, bool EK>
-__global__ void __launch_bounds__(256) fill_kernel(FillArgs A, GLParams gl) {
+__global__ void __launch_bounds__(256, MW_FILL_MIN_BLOCKS) fill_kernel(FillArgs A, GLParams gl) {
     extern __shared__ double smem[];
     int tr, tc;
     tri_pair((int64_t)blockIdx.x, tr, tc);

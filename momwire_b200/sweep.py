@@ -166,14 +166,20 @@ def _solve_group(solvers, nb, ks, stream, pw=None, Bs=None):
     P = max(B.shape[1] for B in Bs)
     Z = torch.empty((count, nb, nb), dtype=torch.complex128, device=dev)
     Z32 = torch.empty((count, nb, nb), dtype=torch.complex64, device=dev)
-    Bd = torch.zeros((count, P, nb), dtype=torch.complex128, device=dev)
-    for g, (s, B) in enumerate(zip(solvers, Bs)):
+    # the right-hand sides of every structure, staged in page-locked memory
+    # and uploaded with one stream-ordered copy (pageable uploads would make
+    # the host wait for the fills queued before them)
+    Bh = torch.zeros((G, P, nb), dtype=torch.complex128, pin_memory=True)
+    for g, B in enumerate(Bs):
+        Bh[g, : B.shape[1], : B.shape[0]] = torch.from_numpy(np.ascontiguousarray(B.T))
+    Bg = Bh.to(dev, non_blocking=True)
+    Bd = Bg.repeat_interleave(nk, dim=0)
+    k_dev = solvers[0]._upload_k(ks)
+    for g, s in enumerate(solvers):
         n = s._basis().n
         zb, z32b = Z[g * nk : (g + 1) * nk], Z32[g * nk : (g + 1) * nk]
-        s._fill_batched(ks, stream, Z=zb, Z32=z32b, ld=nb)
+        s._fill_batched(ks, stream, Z=zb, Z32=z32b, ld=nb, k_dev=k_dev)
         _lib.call("mw_pad_identity", n, nb, nk, zb.data_ptr(), nb, nb * nb, z32b.data_ptr(), nb, nb * nb, stream)
-        Bt = torch.from_numpy(np.ascontiguousarray(B.T)).to(dev)
-        Bd[g * nk : (g + 1) * nk, : B.shape[1], :n] = Bt
     if pw is None:
         pw = _group_width(solvers[0], nb, Z, Z32, Bd, P, stream)
     X = torch.empty((count, P, nb), dtype=torch.complex128, device=dev)
@@ -278,6 +284,7 @@ def grouped_mixed_sweep(structs, ks, device=None, budget_bytes=32 << 30, indices
     def prep(i):
         with torch.cuda.device(dev), torch.cuda.stream(prep_stream):
             solvers[i]._dev_tables()
+            solvers[i]._loading_dev_tables()
             ports[i] = solvers[i]._port_columns()[0]
             prep_stream.synchronize()
 

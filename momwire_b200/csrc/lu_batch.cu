@@ -290,17 +290,24 @@ static mw_status cgetrf_batched(int n, int batch, cf* A, int64_t lda, int64_t st
         }
         const int right = n - j0 - jb;
         if (j0 > 0) {
+            ProfileScope ps(PC_LASWP, st);
             laswp_batched_kernel<cf><<<dim3((j0 + 127) / 128, batch), 128, 0, st>>>(A, lda, stride, 0, j0, ipiv, n,
                                                                                     j0, j0 + jb);
             count_launch();
         }
         if (right > 0) {
-            laswp_batched_kernel<cf><<<dim3((right + 127) / 128, batch), 128, 0, st>>>(A, lda, stride, j0 + jb, right,
-                                                                                       ipiv, n, j0, j0 + jb);
+            {
+                ProfileScope ps(PC_LASWP, st);
+                laswp_batched_kernel<cf><<<dim3((right + 127) / 128, batch), 128, 0, st>>>(
+                    A, lda, stride, j0 + jb, right, ipiv, n, j0, j0 + jb);
+            }
             cf* A11 = A + j0 + (int64_t)j0 * lda;
             cf* A12 = A + j0 + (int64_t)(j0 + jb) * lda;
-            trsm_batched_kernel<false><<<dim3((right + 7) / 8, batch), 256, 0, st>>>(A11, lda, stride, A12, lda, stride,
-                                                                                     jb, right);
+            {
+                ProfileScope ps(PC_TRSM, st, 4.0 * (double)jb * jb * right * batch);
+                trsm_batched_kernel<false><<<dim3((right + 7) / 8, batch), 256, 0, st>>>(A11, lda, stride, A12, lda,
+                                                                                         stride, jb, right);
+            }
             count_launch(2);
             mw_status s = cgemm_tc_update_batched(right, right, jb, batch, A + (j0 + jb) + (int64_t)j0 * lda, lda,
                                                   stride, A12, lda, stride, A + (j0 + jb) + (int64_t)(j0 + jb) * lda,
@@ -316,6 +323,7 @@ static mw_status cgetrf_batched(int n, int batch, cf* A, int64_t lda, int64_t st
 static mw_status cgetrs_batched(int n, int nr, int batch, const cf* LU, int64_t lda, int64_t stride,
                                 const int32_t* ipiv, cf* B, cudaStream_t st) {
     const int64_t bs = (int64_t)n * nr;
+    ProfileScope ps(PC_ZGEMM, st, 8.0 * (double)n * n * nr * batch);  // the whole batched getrs
     laswp_batched_kernel<cf><<<dim3((nr + 127) / 128, batch), 128, 0, st>>>(B, n, bs, 0, nr, ipiv, n, 0, n);
     count_launch();
     for (int j0 = 0; j0 < n; j0 += kBSB) {

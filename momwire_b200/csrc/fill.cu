@@ -325,10 +325,13 @@ __device__ __forceinline__ void stage_segment(double* dst, int nq, const GLParam
 
 // Lane `qi` of a pair computes its observer quadrature row and returns its
 // share of all (D+1)^2 moments; the caller reduces the shares over lanes.
-template <int D, bool EK>
-__device__ __forceinline__ void pair_row(const double* si, const double* sj, int nq, int qi,
+// NQ > 0: the quadrature order is known at compile time (nq == NQ), so the
+// source-point loop unrolls and its independent samples interleave.
+template <int D, bool EK, int NQ = 0>
+__device__ __forceinline__ void pair_row(const double* si, const double* sj, int nq_rt, int qi,
                                          double k, bool ek_on, cd Jp[D + 1][D + 1]) {
     constexpr int NM = D + 1;
+    const int nq = NQ > 0 ? NQ : nq_rt;
 #pragma unroll
     for (int p = 0; p < NM; ++p)
 #pragma unroll
@@ -341,7 +344,9 @@ __device__ __forceinline__ void pair_row(const double* si, const double* sj, int
 #pragma unroll
     for (int P = 0; P < NM; ++P) accP[P] = cd{0.0, 0.0};
     const double* wv = sj + nq * 3;
-    for (int r = 0; r < nq; ++r) {
+#pragma unroll
+    for (int r = 0; r < (NQ > 0 ? NQ : 8); ++r) {
+        if (NQ == 0 && r >= nq) break;
         double dx = xi - sj[r * 3 + 0];
         double dy = yi - sj[r * 3 + 1];
         double dz = zi - sj[r * 3 + 2];
@@ -547,16 +552,19 @@ __device__ __forceinline__ bool fill_tile(const FillArgs& A, const GLParams& gl,
         // groups contribute zeros
         if (valid && !same_edge) {
             bool ek_on = EK && (s_grp_r[li] == s_grp_c[lj]);
-            double acc_re = 0;  // silence unused warnings
-            (void)acc_re;
-            cd Jt[NM][NM];
-            pair_row<D, EK>(s_row + li * SD, s_col + lj * SD, nq, lane4, kz, ek_on, Jt);
-            cd Jt2[NM][NM];
-            pair_row<D, EK>(s_row + li * SD, s_col + lj * SD, nq, lane4 + 4, kz, ek_on, Jt2);
+            if (nq == 4) {
+                // the default rule: one observer point per lane
+                pair_row<D, EK, 4>(s_row + li * SD, s_col + lj * SD, 4, lane4, kz, ek_on, Jp);
+            } else {
+                cd Jt[NM][NM];
+                pair_row<D, EK>(s_row + li * SD, s_col + lj * SD, nq, lane4, kz, ek_on, Jt);
+                cd Jt2[NM][NM];
+                pair_row<D, EK>(s_row + li * SD, s_col + lj * SD, nq, lane4 + 4, kz, ek_on, Jt2);
 #pragma unroll
-            for (int p = 0; p < NM; ++p)
+                for (int p = 0; p < NM; ++p)
 #pragma unroll
-                for (int P = 0; P < NM; ++P) Jp[p][P] = Jt[p][P] + Jt2[p][P];
+                    for (int P = 0; P < NM; ++P) Jp[p][P] = Jt[p][P] + Jt2[p][P];
+            }
         } else {
 #pragma unroll
             for (int p = 0; p < NM; ++p)

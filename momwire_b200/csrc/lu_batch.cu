@@ -129,7 +129,8 @@ __device__ __forceinline__ cf shfl_cf(cf v, int src) {
 }
 
 // X <- L^-1 X (unit lower) or U^-1 X (upper) for the jb x jb diagonal block
-// at T (jb <= 64); one warp per column, batch on blockIdx.y.
+// at T (jb <= 64); a warp per column at a time, batch on blockIdx.y.
+constexpr int kTrsmColsPerWarp = 8;
 template <bool UPPER>
 __global__ void __launch_bounds__(256) trsm_batched_kernel(const cf* Tm, int64_t ldt, int64_t ts, cf* X, int64_t ldx,
                                                            int64_t xs, int jb, int ncols) {
@@ -142,31 +143,39 @@ __global__ void __launch_bounds__(256) trsm_batched_kernel(const cf* Tm, int64_t
         sT[r][c] = Tm[r + (int64_t)c * ldt];
     }
     __syncthreads();
-    const int col = blockIdx.x * 8 + warp;
-    if (col >= ncols) return;
-    cf* x = X + (int64_t)col * ldx;
-    cf x0 = lane < jb ? x[lane] : cf{0.f, 0.f};
-    cf x1 = lane + 32 < jb ? x[lane + 32] : cf{0.f, 0.f};
-    if (!UPPER) {
-        for (int k = 0; k < jb; ++k) {
-            const cf xk = shfl_cf(k < 32 ? x0 : x1, k & 31);
-            if (lane > k && lane < jb) x0 = x0 - sT[lane][k] * xk;
-            if (lane + 32 > k && lane + 32 < jb) x1 = x1 - sT[lane + 32][k] * xk;
-        }
-    } else {
-        for (int k = jb - 1; k >= 0; --k) {
-            if (k < 32) {
-                if (lane == k) x0 = cdiv(x0, sT[k][k]);
-            } else if (lane == k - 32) {
-                x1 = cdiv(x1, sT[k][k]);
+    // each warp solves kTrsmColsPerWarp columns in turn (the staged triangle
+    // serves 8 x kTrsmColsPerWarp consecutive columns)
+    for (int cc = 0; cc < kTrsmColsPerWarp; ++cc) {
+        const int col = (blockIdx.x * kTrsmColsPerWarp + cc) * 8 + warp;
+        if (col >= ncols) return;  // whole warp leaves together
+        cf* x = X + (int64_t)col * ldx;
+        cf x0 = lane < jb ? x[lane] : cf{0.f, 0.f};
+        cf x1 = lane + 32 < jb ? x[lane + 32] : cf{0.f, 0.f};
+        if (!UPPER) {
+            for (int k = 0; k < jb; ++k) {
+                const cf xk = shfl_cf(k < 32 ? x0 : x1, k & 31);
+                if (lane > k && lane < jb) x0 = x0 - sT[lane][k] * xk;
+                if (lane + 32 > k && lane + 32 < jb) x1 = x1 - sT[lane + 32][k] * xk;
             }
-            const cf xk = shfl_cf(k < 32 ? x0 : x1, k & 31);
-            if (lane < k) x0 = x0 - sT[lane][k] * xk;
-            if (lane + 32 < k) x1 = x1 - sT[lane + 32][k] * xk;
+        } else {
+            for (int k = jb - 1; k >= 0; --k) {
+                if (k < 32) {
+                    if (lane == k) x0 = cdiv(x0, sT[k][k]);
+                } else if (lane == k - 32) {
+                    x1 = cdiv(x1, sT[k][k]);
+                }
+                const cf xk = shfl_cf(k < 32 ? x0 : x1, k & 31);
+                if (lane < k) x0 = x0 - sT[lane][k] * xk;
+                if (lane + 32 < k) x1 = x1 - sT[lane + 32][k] * xk;
+            }
         }
+        if (lane < jb) x[lane] = x0;
+        if (lane + 32 < jb) x[lane + 32] = x1;
     }
-    if (lane < jb) x[lane] = x0;
-    if (lane + 32 < jb) x[lane + 32] = x1;
+}
+
+static dim3 trsm_batched_grid(int ncols, int batch) {
+    return dim3((unsigned)((ncols + 8 * kTrsmColsPerWarp - 1) / (8 * kTrsmColsPerWarp)), (unsigned)batch);
 }
 
 // Y (m x nr) -= A (m x k) X (k x nr), complex64, batch on blockIdx.y;
@@ -305,7 +314,7 @@ static mw_status cgetrf_batched(int n, int batch, cf* A, int64_t lda, int64_t st
             cf* A12 = A + j0 + (int64_t)(j0 + jb) * lda;
             {
                 ProfileScope ps(PC_TRSM, st, 4.0 * (double)jb * jb * right * batch);
-                trsm_batched_kernel<false><<<dim3((right + 7) / 8, batch), 256, 0, st>>>(A11, lda, stride, A12, lda,
+                trsm_batched_kernel<false><<<trsm_batched_grid(right, batch), 256, 0, st>>>(A11, lda, stride, A12, lda,
                                                                                          stride, jb, right);
             }
             count_launch(2);
@@ -328,7 +337,7 @@ static mw_status cgetrs_batched(int n, int nr, int batch, const cf* LU, int64_t 
     count_launch();
     for (int j0 = 0; j0 < n; j0 += kBSB) {
         const int jb = (n - j0) < kBSB ? (n - j0) : kBSB;
-        trsm_batched_kernel<false><<<dim3((nr + 7) / 8, batch), 256, 0, st>>>(LU + j0 + (int64_t)j0 * lda, lda, stride,
+        trsm_batched_kernel<false><<<trsm_batched_grid(nr, batch), 256, 0, st>>>(LU + j0 + (int64_t)j0 * lda, lda, stride,
                                                                              B + j0, n, bs, jb, nr);
         count_launch();
         const int rest = n - j0 - jb;
@@ -340,7 +349,7 @@ static mw_status cgetrs_batched(int n, int nr, int batch, const cf* LU, int64_t 
     }
     for (int j0 = ((n - 1) / kBSB) * kBSB; j0 >= 0; j0 -= kBSB) {
         const int jb = (n - j0) < kBSB ? (n - j0) : kBSB;
-        trsm_batched_kernel<true><<<dim3((nr + 7) / 8, batch), 256, 0, st>>>(LU + j0 + (int64_t)j0 * lda, lda, stride,
+        trsm_batched_kernel<true><<<trsm_batched_grid(nr, batch), 256, 0, st>>>(LU + j0 + (int64_t)j0 * lda, lda, stride,
                                                                             B + j0, n, bs, jb, nr);
         count_launch();
         if (j0 > 0) {

@@ -26,7 +26,7 @@ mw_status cgemm_tc_update(int64_t m, int64_t n, int64_t k, const cf* A, int64_t 
                           int64_t ldc, void* ws, size_t ws_bytes, int* err, cudaStream_t st, int max_ctas);
 size_t cgemm_tc_workspace(int64_t m, int64_t n, int64_t k);
 
-constexpr int kNB = 64;         // triangular-solve block (and getrs block)
+constexpr int kNB = 64;         // panel half width (rank-1 work per cooperative panel)
 constexpr int kOuterNB = 128;   // getrf block: panel width and trailing-update k
 constexpr int kPanelMaxJb = 128;
 constexpr int kPanelThreads = 256;
@@ -427,74 +427,124 @@ __device__ __forceinline__ cf shfl_c(cf v, int src) {
     return cf{__shfl_sync(0xffffffffu, v.re, src), __shfl_sync(0xffffffffu, v.im, src)};
 }
 
+// Rows of a triangular-solve leaf in the multi-right-hand-side solve:
+// 128 for complex64 (its staged triangle, 132 KB, fits shared memory; half
+// the sequential steps of 64-row leaves), 64 for complex128.  The
+// factorisation's own block-row solves (thousands of columns) keep 64-row
+// leaves, whose 33 KB lets several CTAs share an SM.
+template <class T>
+struct GetrsLeaf {
+    static constexpr int value = 64;
+};
+template <>
+struct GetrsLeaf<cf> {
+    static constexpr int value = 128;
+};
+
 // X (jb x ncols, leading dim ldx) <- L^-1 X with L unit lower (jb x jb),
-// or U^-1 X with U upper non-unit (jb <= 64).  The CTA stages the triangle
+// or U^-1 X with U upper non-unit (jb <= leaf).  The CTA stages the triangle
 // in shared memory; each warp then owns one column of X in registers (lane
-// l holds rows l and l+32) and substitutes with warp shuffles only.
+// l holds rows l, l+32, ...) and substitutes with warp shuffles only.
 constexpr int kTrsmWarps = 8;
-template <class T, bool UPPER>
+template <class T, bool UPPER, int L>
 __global__ void __launch_bounds__(32 * kTrsmWarps) trsm_kernel(const T* Tm, int64_t ldt, T* X, int64_t ldx, int jb,
                                                                int64_t ncols) {
+    constexpr int R = L / 32;
     extern __shared__ __align__(16) unsigned char trsm_smem[];
-    T(*sT)[kNB + 1] = reinterpret_cast<T(*)[kNB + 1]>(trsm_smem);
+    T(*sT)[L + 1] = reinterpret_cast<T(*)[L + 1]>(trsm_smem);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int i = tid; i < jb * jb; i += blockDim.x) {
-        int r = i % jb, cc = i / jb;
-        sT[r][cc] = Tm[r + cc * ldt];
+    // stage the triangle the solve reads (strictly lower for L, upper with
+    // the diagonal for U), eight loads in flight per thread before the
+    // shared-memory stores
+    constexpr int kU = 8;
+    const int tot = jb * jb;
+    for (int base = 0; base < tot; base += kU * (int)blockDim.x) {
+        T v[kU];
+        bool need[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const int i = base + u * (int)blockDim.x + tid;
+            const int r = i % jb, cc = i / jb;
+            need[u] = i < tot && (UPPER ? r <= cc : r > cc);
+            if (need[u]) v[u] = Tm[r + (int64_t)cc * ldt];
+        }
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const int i = base + u * (int)blockDim.x + tid;
+            if (need[u]) sT[i % jb][i / jb] = v[u];
+        }
     }
     __syncthreads();
     const int64_t col = (int64_t)blockIdx.x * kTrsmWarps + warp;
     if (col >= ncols) return;  // whole warp leaves together
     T* x = X + col * ldx;
     const T zero{};
-    T x0 = lane < jb ? x[lane] : zero;
-    T x1 = lane + 32 < jb ? x[lane + 32] : zero;
+    T v[R];
+#pragma unroll
+    for (int i = 0; i < R; ++i) v[i] = lane + 32 * i < jb ? x[lane + 32 * i] : zero;
     if (!UPPER) {
         for (int k = 0; k < jb; ++k) {
-            const T xk = shfl_c(k < 32 ? x0 : x1, k & 31);
-            if (lane > k && lane < jb) x0 = x0 - sT[lane][k] * xk;
-            if (lane + 32 > k && lane + 32 < jb) x1 = x1 - sT[lane + 32][k] * xk;
+            T src = v[0];
+#pragma unroll
+            for (int i = 1; i < R; ++i)
+                if ((k >> 5) == i) src = v[i];
+            const T xk = shfl_c(src, k & 31);
+#pragma unroll
+            for (int i = 0; i < R; ++i) {
+                const int row = lane + 32 * i;
+                if (row > k && row < jb) v[i] = v[i] - sT[row][k] * xk;
+            }
         }
     } else {
         for (int k = jb - 1; k >= 0; --k) {
-            if (k < 32) {
-                if (lane == k) x0 = cdiv(x0, sT[k][k]);
-            } else if (lane == k - 32) {
-                x1 = cdiv(x1, sT[k][k]);
+#pragma unroll
+            for (int i = 0; i < R; ++i)
+                if ((k >> 5) == i && lane == (k & 31)) v[i] = cdiv(v[i], sT[k][k]);
+            T src = v[0];
+#pragma unroll
+            for (int i = 1; i < R; ++i)
+                if ((k >> 5) == i) src = v[i];
+            const T xk = shfl_c(src, k & 31);
+#pragma unroll
+            for (int i = 0; i < R; ++i) {
+                const int row = lane + 32 * i;
+                if (row < k) v[i] = v[i] - sT[row][k] * xk;
             }
-            const T xk = shfl_c(k < 32 ? x0 : x1, k & 31);
-            if (lane < k) x0 = x0 - sT[lane][k] * xk;
-            if (lane + 32 < k) x1 = x1 - sT[lane + 32][k] * xk;
         }
     }
-    if (lane < jb) x[lane] = x0;
-    if (lane + 32 < jb) x[lane + 32] = x1;
+#pragma unroll
+    for (int i = 0; i < R; ++i)
+        if (lane + 32 * i < jb) x[lane + 32 * i] = v[i];
 }
 
-template <class T>
+template <class T, int L>
 constexpr size_t trsm_smem_bytes() {
-    return sizeof(T) * (kNB * (kNB + 1));
+    return sizeof(T) * (L * (L + 1));
 }
 
 template <class T>
 static mw_status trsm_setup() {
     static bool done = false;
     if (!done) {
-        MW_CHECK_CUDA(cudaFuncSetAttribute(trsm_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)trsm_smem_bytes<T>()));
-        MW_CHECK_CUDA(cudaFuncSetAttribute(trsm_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)trsm_smem_bytes<T>()));
+        constexpr int GL = GetrsLeaf<T>::value;
+        MW_CHECK_CUDA(cudaFuncSetAttribute(trsm_kernel<T, false, kNB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)trsm_smem_bytes<T, kNB>()));
+        MW_CHECK_CUDA(cudaFuncSetAttribute(trsm_kernel<T, true, kNB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)trsm_smem_bytes<T, kNB>()));
+        MW_CHECK_CUDA(cudaFuncSetAttribute(trsm_kernel<T, false, GL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)trsm_smem_bytes<T, GL>()));
+        MW_CHECK_CUDA(cudaFuncSetAttribute(trsm_kernel<T, true, GL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)trsm_smem_bytes<T, GL>()));
         done = true;
     }
     return MW_OK;
 }
 
-template <class T, bool UPPER>
+template <class T, bool UPPER, int L = kNB>
 static void trsm_launch(const T* Tm, int64_t ldt, T* X, int64_t ldx, int jb, int64_t ncols, cudaStream_t st) {
     ProfileScope ps(PC_TRSM, st, 4.0 * (double)jb * jb * ncols, 2.0 * sizeof(T) * (double)jb * ncols);
-    trsm_kernel<T, UPPER><<<(unsigned)((ncols + kTrsmWarps - 1) / kTrsmWarps), 32 * kTrsmWarps, trsm_smem_bytes<T>(),
-                            st>>>(Tm, ldt, X, ldx, jb,
-                                                                                            ncols);
+    trsm_kernel<T, UPPER, L><<<(unsigned)((ncols + kTrsmWarps - 1) / kTrsmWarps), 32 * kTrsmWarps,
+                               trsm_smem_bytes<T, L>(), st>>>(Tm, ldt, X, ldx, jb, ncols);
     count_launch();
 }
 
@@ -1131,9 +1181,10 @@ static mw_status getrs(int64_t n, int64_t nrhs, const T* LU, int64_t lda, const 
         if (s0 != MW_OK) return s0;
     }
     laswp_launch<T>(B, ldb, 0, nrhs, ipiv, 0, n, st);
-    for (int64_t j0 = 0; j0 < n; j0 += kNB) {
-        const int jb = (int)((n - j0) < kNB ? (n - j0) : kNB);
-        trsm_launch<T, false>(LU + j0 + j0 * lda, lda, B + j0, ldb, jb, nrhs, st);
+    constexpr int LF = GetrsLeaf<T>::value;
+    for (int64_t j0 = 0; j0 < n; j0 += LF) {
+        const int jb = (int)((n - j0) < LF ? (n - j0) : LF);
+        trsm_launch<T, false, LF>(LU + j0 + j0 * lda, lda, B + j0, ldb, jb, nrhs, st);
         const int64_t rest = n - j0 - jb;
         if (rest > 0) {
             mw_status s = block_update(LU + (j0 + jb) + j0 * lda, lda, B + j0, ldb, B + j0 + jb, ldb, rest, nrhs, jb,
@@ -1141,10 +1192,10 @@ static mw_status getrs(int64_t n, int64_t nrhs, const T* LU, int64_t lda, const 
             if (s != MW_OK) return s;
         }
     }
-    const int64_t last = ((n - 1) / kNB) * kNB;
-    for (int64_t j0 = last; j0 >= 0; j0 -= kNB) {
-        const int jb = (int)((n - j0) < kNB ? (n - j0) : kNB);
-        trsm_launch<T, true>(LU + j0 + j0 * lda, lda, B + j0, ldb, jb, nrhs, st);
+    const int64_t last = ((n - 1) / LF) * LF;
+    for (int64_t j0 = last; j0 >= 0; j0 -= LF) {
+        const int jb = (int)((n - j0) < LF ? (n - j0) : LF);
+        trsm_launch<T, true, LF>(LU + j0 + j0 * lda, lda, B + j0, ldb, jb, nrhs, st);
         if (j0 > 0) {
             mw_status s = block_update(LU + j0 * lda, lda, B + j0, ldb, B, ldb, j0, nrhs, jb, up, st);
             if (s != MW_OK) return s;

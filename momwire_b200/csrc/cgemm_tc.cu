@@ -8,14 +8,16 @@
 // as x = hi + lo with hi = tf32(x), and the MMA sums hi*hi + hi*lo + lo*hi
 // ("3xTF32"), which keeps fp32-level accuracy at tensor-core rate.
 //
-// Kernel structure (one persistent CTA per SM, 192 threads):
+// Kernel structure (one persistent CTA per SM, 64 + 32 x TC_EPI_WARPS threads):
 //   warp 0      producer: cp.async.bulk copies of pre-tiled operand stages
-//               into a 2-deep shared-memory ring (mbarrier complete_tx);
+//               into a TC_STAGES-deep shared-memory ring (mbarrier complete_tx);
 //   warp 1      allocates 512 TMEM columns; one lane issues tcgen05.mma
 //               (M=128, N=256, K=8, kind::tf32) into one of two TMEM
 //               accumulators and commits to mbarriers;
-//   warps 2..5  epilogue: tcgen05.ld the accumulator, C -= D with coalesced
-//               loads/stores, then hand the accumulator back.
+//   warps 2..   epilogue: tcgen05.ld the accumulator, C -= D with coalesced
+//               loads/stores (two warps per TMEM lane quadrant, each half
+//               of the columns, so twice the loads are in flight), then
+//               hand the accumulator back.
 // Operands are packed by the two pack kernels below into the shared-memory
 // image of a K-major, no-swizzle UMMA tile: [block][stage][chunk][row][4],
 // so each stage block is one contiguous bulk copy.
@@ -28,14 +30,28 @@
 
 namespace mw {
 
+#ifndef MW_TC_KS
+#define MW_TC_KS 16
+#endif
+#ifndef MW_TC_STAGES
+#define MW_TC_STAGES 4
+#endif
+#ifndef MW_TC_EPI_WARPS
+#define MW_TC_EPI_WARPS 8
+#endif
 constexpr int TC_M = 128;                           // real rows per tile
 constexpr int TC_N = 256;                           // columns per tile
-constexpr int TC_KS = 32;                           // real K per stage
-constexpr int TC_STAGES = 2;
-constexpr int TC_A_BYTES = TC_M * TC_KS * 4;        // 16 KB per plane
-constexpr int TC_B_BYTES = TC_N * TC_KS * 4;        // 32 KB per plane
+constexpr int TC_KS = MW_TC_KS;                     // real K per stage (a multiple of 8)
+constexpr int TC_CHUNKS = TC_KS / 4;                // 16-byte K chunks per stage
+constexpr int TC_STAGES = MW_TC_STAGES;             // depth of the shared-memory ring
+constexpr int TC_A_BYTES = TC_M * TC_KS * 4;        // per plane and stage
+constexpr int TC_B_BYTES = TC_N * TC_KS * 4;
 constexpr int TC_STAGE_BYTES = 2 * TC_A_BYTES + 2 * TC_B_BYTES;
-constexpr int TC_THREADS = 192;
+constexpr int TC_EPI_WARPS = MW_TC_EPI_WARPS;       // 4 or 8: each TMEM lane quadrant by 1 or 2 warps
+constexpr int TC_THREADS = 64 + 32 * TC_EPI_WARPS;
+static_assert(TC_KS % 8 == 0, "a stage holds whole K=8 MMA steps");
+static_assert(TC_EPI_WARPS == 4 || TC_EPI_WARPS == 8, "epilogue warps cover the four TMEM lane quadrants");
+static_assert(TC_STAGES * TC_STAGE_BYTES <= 200 * 1024, "operand ring exceeds shared memory");
 constexpr uint32_t TC_TMEM_COLS = 512;              // two 256-column accumulators
 
 struct TcArgs {
@@ -76,7 +92,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) cgemm_tc_kernel(TcArgs P) {
         }
         for (int a = 0; a < 2; ++a) {
             mbar_init(&bar_accf[a], 1);
-            mbar_init(&bar_acce[a], 4);
+            mbar_init(&bar_acce[a], TC_EPI_WARPS);
         }
         mbar_init(&bar_done, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -96,16 +112,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1) cgemm_tc_kernel(TcArgs P) {
         // ------------------------------------------------ producer
         if (lane == 0) {
             int slot = 0;
-            uint32_t ph_empty[TC_STAGES];
-            uint32_t issued[TC_STAGES] = {};
-            for (int s = 0; s < TC_STAGES; ++s) ph_empty[s] = 1;
+            // phase bit of each slot's empty barrier (bit s), all 1 at start;
+            // slots fill round-robin from 0, so `issued` counts every slot
+            uint32_t ph_empty = (1u << TC_STAGES) - 1u;
+            long long issued = 0;
             bool dead = false;
             for (int t = blockIdx.x; t < n_tiles && !dead; t += gridDim.x) {
                 const int bt = t / per_mat, tr = t - bt * per_mat;
                 const int mb = tr % P.n_mb, nb = tr / P.n_mb;
                 for (int ks = 0; ks < P.n_ks; ++ks) {
-                    if (!mbar_wait(&bar_empty[slot], ph_empty[slot], err)) { dead = true; break; }
-                    ph_empty[slot] ^= 1;
+                    if (!mbar_wait(&bar_empty[slot], (ph_empty >> slot) & 1u, err)) { dead = true; break; }
+                    ph_empty ^= 1u << slot;
                     uint8_t* st = tc_smem + (size_t)slot * TC_STAGE_BYTES;
                     const size_t ao = (size_t)bt * P.a_pstride + ((size_t)mb * P.n_ks + ks) * (TC_A_BYTES / 4);
                     const size_t bo = (size_t)bt * P.b_pstride + ((size_t)nb * P.n_ks + ks) * (TC_B_BYTES / 4);
@@ -114,7 +131,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) cgemm_tc_kernel(TcArgs P) {
                     bulk_g2s(st + TC_A_BYTES, P.a_lo + ao, TC_A_BYTES, &bar_full[slot]);
                     bulk_g2s(st + 2 * TC_A_BYTES, P.b_hi + bo, TC_B_BYTES, &bar_full[slot]);
                     bulk_g2s(st + 2 * TC_A_BYTES + TC_B_BYTES, P.b_lo + bo, TC_B_BYTES, &bar_full[slot]);
-                    issued[slot] += 1;
+                    issued += 1;
                     slot = (slot + 1) % TC_STAGES;
                 }
             }
@@ -123,9 +140,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) cgemm_tc_kernel(TcArgs P) {
             // k-1 of its full barrier); bounded, and independent of the MMA
             // side so that it also ends when another role gave up
             for (int s = 0; s < TC_STAGES; ++s) {
-                if (issued[s] == 0) continue;
+                const long long fills = issued / TC_STAGES + (s < issued % TC_STAGES ? 1 : 0);
+                if (fills == 0) continue;
                 for (long long it = 0; it < TC_SPIN_LIMIT; ++it)
-                    if (mbar_try_wait(&bar_full[s], (issued[s] - 1) & 1)) break;
+                    if (mbar_try_wait(&bar_full[s], (uint32_t)((fills - 1) & 1))) break;
             }
         }
         __syncwarp();
@@ -134,7 +152,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) cgemm_tc_kernel(TcArgs P) {
         if (lane == 0) {
             const uint32_t idesc = idesc_tf32(TC_M, TC_N);
             int slot = 0;
-            uint32_t ph_full[TC_STAGES] = {};
+            uint32_t ph_full = 0;  // phase bit of each slot's full barrier (bit s)
             uint32_t ph_acce[2] = {1, 1};
             bool dead = false;
             int lt = 0;
@@ -145,8 +163,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) cgemm_tc_kernel(TcArgs P) {
                 tc_fence_after();
                 const uint32_t tmem_d = tmem_base + acc * TC_N;
                 for (int ks = 0; ks < P.n_ks; ++ks) {
-                    if (!mbar_wait(&bar_full[slot], ph_full[slot], err)) { dead = true; break; }
-                    ph_full[slot] ^= 1;
+                    if (!mbar_wait(&bar_full[slot], (ph_full >> slot) & 1u, err)) { dead = true; break; }
+                    ph_full ^= 1u << slot;
                     tc_fence_after();
                     const uint32_t st = smem_u32(tc_smem + (size_t)slot * TC_STAGE_BYTES);
                     const uint32_t a_hi = st, a_lo = st + TC_A_BYTES;
@@ -177,8 +195,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) cgemm_tc_kernel(TcArgs P) {
         }
         __syncwarp();
     } else {
-        // ------------------------------------------------ epilogue (warps 2..5)
+        // ------------------------------------------------ epilogue (warps 2..)
         const int quad = warp & 3;  // TMEM lane quadrant this warp may access
+        // with eight epilogue warps, two share a quadrant and split its columns
+        constexpr int kCols = TC_N * 4 / TC_EPI_WARPS;
+        const int cbeg = ((warp - 2) / 4) * kCols;
         uint32_t ph_accf[2] = {0, 0};
         bool dead = false;
         int lt = 0;
@@ -196,7 +217,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) cgemm_tc_kernel(TcArgs P) {
             const uint32_t taddr = tmem_base + ((uint32_t)(quad * 32) << 16) + acc * TC_N;
             // 32 columns per round: all loads of C issue before any store so
             // that they overlap (a store may alias the next load otherwise)
-            for (int c0 = 0; c0 < TC_N; c0 += 32) {
+            for (int c0 = cbeg; c0 < cbeg + kCols; c0 += 32) {
                 float v[32], old[32];
                 tmem_ld16(taddr + c0, v);
                 tmem_ld16(taddr + c0 + 16, v + 16);
@@ -232,18 +253,18 @@ __device__ __forceinline__ float tf32_hi(float x) {
 }
 
 // Ahat (2m x 2k, from complex A at A + (i + l*lda)) packed as
-// [mb][ks][chunk 8][row 128][4]; zero beyond (2m, 2k).
+// [mb][ks][chunk TC_CHUNKS][row 128][4]; zero beyond (2m, 2k).
 __global__ void pack_a_kernel(const cf* __restrict__ A, int64_t lda, int64_t m, int64_t k, int n_mb, int n_ks,
                               float* __restrict__ hi, float* __restrict__ lo, int64_t a_stride, int64_t p_stride) {
-    const int64_t total = (int64_t)n_mb * n_ks * 8 * TC_M;  // float4 slots
+    const int64_t total = (int64_t)n_mb * n_ks * TC_CHUNKS * TC_M;  // float4 slots
     A += blockIdx.y * a_stride;  // batch entry
     hi += blockIdx.y * p_stride;
     lo += blockIdx.y * p_stride;
     for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
         const int row = (int)(q % TC_M);
         int64_t rest = q / TC_M;
-        const int ch = (int)(rest % 8);
-        rest /= 8;
+        const int ch = (int)(rest % TC_CHUNKS);
+        rest /= TC_CHUNKS;
         const int ks = (int)(rest % n_ks);
         const int mb = (int)(rest / n_ks);
         const int64_t rho = (int64_t)mb * TC_M + row;  // real row
@@ -270,18 +291,18 @@ __global__ void pack_a_kernel(const cf* __restrict__ A, int64_t lda, int64_t m, 
 }
 
 // Breal^T (n x 2k, from complex B at B + (l + j*ldb)) packed as
-// [nb][ks][chunk 8][row 256][4]; zero beyond (n, 2k).
+// [nb][ks][chunk TC_CHUNKS][row 256][4]; zero beyond (n, 2k).
 __global__ void pack_b_kernel(const cf* __restrict__ B, int64_t ldb, int64_t k, int64_t n, int n_nb, int n_ks,
                               float* __restrict__ hi, float* __restrict__ lo, int64_t b_stride, int64_t p_stride) {
-    const int64_t total = (int64_t)n_nb * n_ks * 8 * TC_N;
+    const int64_t total = (int64_t)n_nb * n_ks * TC_CHUNKS * TC_N;
     B += blockIdx.y * b_stride;  // batch entry
     hi += blockIdx.y * p_stride;
     lo += blockIdx.y * p_stride;
     for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
         const int row = (int)(q % TC_N);
         int64_t rest = q / TC_N;
-        const int ch = (int)(rest % 8);
-        rest /= 8;
+        const int ch = (int)(rest % TC_CHUNKS);
+        rest /= TC_CHUNKS;
         const int ks = (int)(rest % n_ks);
         const int nb = (int)(rest / n_ks);
         const int64_t j = (int64_t)nb * TC_N + row;
@@ -336,7 +357,7 @@ mw_status cgemm_tc_update_batched(int64_t m, int64_t n, int64_t k, int batch, co
     float* b_lo = reinterpret_cast<float*>(w + 2 * al(ab * batch) + al(bb * batch));
     {
         ProfileScope ps(PC_MISC, st);
-        int64_t qa = (int64_t)n_mb * n_ks * 8 * TC_M, qb = (int64_t)n_nb * n_ks * 8 * TC_N;
+        int64_t qa = (int64_t)n_mb * n_ks * TC_CHUNKS * TC_M, qb = (int64_t)n_nb * n_ks * TC_CHUNKS * TC_N;
         dim3 ga((unsigned)((qa + 255) / 256), (unsigned)batch), gb((unsigned)((qb + 255) / 256), (unsigned)batch);
         pack_a_kernel<<<ga, 256, 0, st>>>(A, lda, m, k, n_mb, n_ks, a_hi, a_lo, sa, (int64_t)(ab / 4));
         pack_b_kernel<<<gb, 256, 0, st>>>(B, ldb, k, n, n_nb, n_ks, b_hi, b_lo, sb, (int64_t)(bb / 4));

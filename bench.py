@@ -347,8 +347,11 @@ def run_b200(args, kw):
         "vs_baseline": None,
         "dtype": "complex128" if args.precision == "fp64" else "complex64+fp64-refine",
         "data": "synthetic (seeded dipole array)",
-        "config": {"workload": WORKLOAD, "n_unknowns": buf["n"], "ports": buf["n_p"], "precision": args.precision,
-                   "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (Z = 1.76 GB per step)"},
+        "config": {"workload": WORKLOAD if args.nx == 16 else WORKLOAD.replace("16x16", f"{args.nx}x{args.nx}").replace(
+                       "256port", f"{buf['n_p']}port"),
+                   "n_unknowns": buf["n"], "ports": buf["n_p"], "precision": args.precision,
+                   "parallelism": f"replicas x{world}",
+                   "l2": f"inputs larger than L2 (Z = {buf['n'] ** 2 * 16 / 1e9:.2f} GB per step)"},
         "e2e": {"value": world * 1e3 / e2e_step, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": e2e_step},
         "gpu_launches": int(launches),

@@ -276,6 +276,11 @@ __device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned l
     asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
+// The exchange of column jj+1 overlaps the bulk of column jj's update: once
+// column jj's pivot is known, every CTA updates column jj+1 of its rows,
+// finds its candidate for jj+1, finishes that candidate row (and, on the
+// owner, row c+1) over the remaining columns, publishes them, and only then
+// updates the rest of its rows while the other CTAs' words arrive.
 __global__ void __launch_bounds__(kPanelThreads) panel_kernel_c64(PanelArgs P) {
     extern __shared__ __align__(16) unsigned char panel_smem[];
     cf* slab = reinterpret_cast<cf*>(panel_smem);
@@ -308,11 +313,13 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel_c64(PanelArgs P) {
     }
     __syncthreads();
 
-    for (int jj = 0; jj < jb; ++jj) {
+    // Candidate of column jj: block argmax of |re|+|im| over rows >= c (LAPACK
+    // rule at float resolution), its row and (owner) row c copied to the
+    // slots, then one release store of [seq 8 | float key 32 | 2^24-1-(row-j0)
+    // 24].  Every row written here is final in every panel column.
+    auto publish = [&](int jj) {
         const int64_t c = P.j0 + jj;
         const int buf = jj & 1;
-        // 1..255, never the 0 the slots are cleared to; a stale word in a
-        // slot is at most jb + 2 columns old, so it never matches
         const unsigned long long seq = (unsigned long long)((c + 1) % 255 + 1);
         const int i0 = (int)max((int64_t)0, c - r0);
         double best = -1.0;
@@ -333,6 +340,16 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel_c64(PanelArgs P) {
             }
             st_release_u64(words + (size_t)buf * G + g, (seq << 56) | key);
         }
+        return bidx;
+    };
+
+    publish(0);
+    for (int jj = 0; jj < jb; ++jj) {
+        const int64_t c = P.j0 + jj;
+        const int buf = jj & 1;
+        // 1..255, never the 0 the slots are cleared to; a stale word in a
+        // slot is at most jb + 2 columns old, so it never matches
+        const unsigned long long seq = (unsigned long long)((c + 1) % 255 + 1);
         if (tid < 32) {
             unsigned long long bk = 0;
             int bg = 0, ok = 1;
@@ -380,8 +397,12 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel_c64(PanelArgs P) {
         if (!s_ok) return;  // a wait gave up: the error word is set
         const int64_t p = s_p;
         if (s_zero && g == 0 && tid == 0 && P.info[0] == 0) P.info[0] = (int32_t)(c + 1);
+        // LAPACK: an exact zero pivot is neither divided by nor applied
         const bool apply = !s_zero;
         const cf inv = apply ? cdiv(cone<cf>(), s_piv[jj]) : cone<cf>();
+        const int i0 = (int)max((int64_t)0, c - r0);
+        const bool last = jj + 1 >= jb;
+        // 1. swap rows c and p, scale column jj below c, update column jj+1
         for (int i = i0 + tid; i < R; i += blockDim.x) {
             const int64_t gr = r0 + i;
             if (gr == c) {
@@ -394,8 +415,55 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel_c64(PanelArgs P) {
             if (!apply) continue;
             const cf l = slab[jj * rcap + i] * inv;
             slab[jj * rcap + i] = l;
-            for (int x = jj + 1; x < jb; ++x) slab[x * rcap + i] = slab[x * rcap + i] - l * s_piv[x];
+            if (!last) slab[(jj + 1) * rcap + i] = slab[(jj + 1) * rcap + i] - l * s_piv[jj + 1];
         }
+        __syncthreads();
+        if (last) break;
+        // 2. the candidate row for column jj+1 and row c+1, finished over the
+        // remaining columns, then published
+        const int64_t cn = c + 1;
+        double best = -1.0;
+        int64_t bidx = INT64_MAX;
+        {
+            const int j1 = (int)max((int64_t)0, cn - r0);
+            for (int i = j1 + tid; i < R; i += blockDim.x)
+                argmax_merge(best, bidx, cabs1(slab[(jj + 1) * rcap + i]), r0 + i);
+            block_argmax(best, bidx, s_v, s_i);
+        }
+        const int lb = bidx != INT64_MAX ? (int)(bidx - r0) : -1;
+        const int lc = (cn >= r0 && cn < r1) ? (int)(cn - r0) : -1;
+        if (apply)
+            for (int x = jj + 2 + tid; x < jb; x += blockDim.x) {
+                if (lb >= 0) slab[x * rcap + lb] = slab[x * rcap + lb] - slab[jj * rcap + lb] * s_piv[x];
+                if (lc >= 0 && lc != lb) slab[x * rcap + lc] = slab[x * rcap + lc] - slab[jj * rcap + lc] * s_piv[x];
+            }
+        __syncthreads();
+        {
+            const int nbuf = (jj + 1) & 1;
+            const unsigned long long nseq = (unsigned long long)((cn + 1) % 255 + 1);
+            if (lb >= 0)
+                for (int x = tid; x < jb; x += blockDim.x)
+                    slot_row[((size_t)nbuf * G + g) * kPanelMaxJb + x] = slab[x * rcap + lb];
+            if (lc >= 0)
+                for (int x = tid; x < jb; x += blockDim.x) cur_row[nbuf * kPanelMaxJb + x] = slab[x * rcap + lc];
+            __syncthreads();
+            if (tid == 0) {
+                unsigned long long key = 0;
+                if (bidx != INT64_MAX) {
+                    const unsigned int fb = __float_as_uint((float)best);
+                    key = ((unsigned long long)fb << 24) | (unsigned long long)(0xFFFFFFll - (bidx - P.j0));
+                }
+                st_release_u64(words + (size_t)nbuf * G + g, (nseq << 56) | key);
+            }
+        }
+        // 3. the rest of column jj's update while the other CTAs publish
+        if (apply)
+            for (int i = i0 + tid; i < R; i += blockDim.x) {
+                const int64_t gr = r0 + i;
+                if (gr <= c || i == lb || i == lc) continue;
+                const cf l = slab[jj * rcap + i];
+                for (int x = jj + 2; x < jb; ++x) slab[x * rcap + i] = slab[x * rcap + i] - l * s_piv[x];
+            }
         __syncthreads();
     }
     for (int idx = tid; idx < R * jb; idx += blockDim.x) {

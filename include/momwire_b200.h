@@ -396,6 +396,18 @@ mw_status mw_pad_identity(int64_t n, int64_t nb, int32_t count, double* Z, int64
                           float* Z32, int64_t ld32, int64_t z32_stride, void* stream);
 
 /*
+ * Y (n_out x ncols, complex128 column-major, ld ldy) = S X with S sparse in
+ * CSR form (row_ptr[n_out + 1], col_idx, vals interleaved re/im; a row's
+ * entries are summed in stored order, so results are deterministic) and X
+ * column-major with ld ldx.  The port and KCL matrices of the solve are a
+ * few nonzeros per row: Y = B^T X (bspline.py:4179) and the Schur products
+ * A Xc, A W (bspline.py:2984-2987) as sparse gathers instead of dense GEMMs
+ * whose inner dimension is the number of unknowns.
+ */
+mw_status mw_csr_mm_c128(int64_t n_out, int64_t ncols, const int64_t* row_ptr, const int64_t* col_idx,
+                         const double* vals, const double* X, int64_t ldx, double* Y, int64_t ldy, void* stream);
+
+/*
  * C = alpha * op(A) * op(B) + beta * C for complex128 column-major
  * matrices, op = 'N' or 'T' (transA/transB 0/1).  Used for the KCL Schur
  * step and Y = B^T X (bspline.py:2984-2989, 4179).

@@ -77,6 +77,17 @@ class _SplineBasis:
     n_poly: int
 
 
+def _csr(rows, cols, vals, n_rows):
+    """(row_ptr, col_idx, vals) int64 / int64 / complex128 of a coordinate
+    list; entries of a row keep their given order."""
+    rows = np.asarray(rows, dtype=np.int64)
+    order = np.argsort(rows, kind="stable")
+    ptr = np.zeros(n_rows + 1, dtype=np.int64)
+    np.cumsum(np.bincount(rows, minlength=n_rows)[:n_rows], out=ptr[1:])
+    return ptr, np.ascontiguousarray(np.asarray(cols, dtype=np.int64)[order]), np.ascontiguousarray(
+        np.asarray(vals, dtype=np.complex128)[order])
+
+
 def _torch():
     import torch
 
@@ -729,7 +740,8 @@ class BSplineSolver:
     def _alloc(self):
         """Device buffers of one solve at this geometry (reused across calls
         by the benchmark): Z, the same-edge table, the port right-hand sides
-        [B | kcl_con^T], LU workspace, pivots, status and Y."""
+        [B | kcl_con^T], the sparse B^T and kcl_con (CSR), LU workspace,
+        pivots, status and Y."""
         torch = _torch()
         dev = self._torch_device()
         dt = self._dev_tables()
@@ -744,16 +756,18 @@ class BSplineSolver:
         kr, kc = kcl_con.row.astype(np.int64), kcl_con.col.astype(np.int64)
         kv = kcl_con.data.astype(np.complex128)
         rr, rc, rv = np.concatenate([pr, kc]), np.concatenate([pc, kr + n_p]), np.concatenate([pv, kv])
+        # CSR of B^T (one row per port) and of kcl_con for the sparse
+        # products Y = B^T X, A Xc and A W
+        bt_ptr, bt_col, bt_val = _csr(pc, pr, pv, n_p)
+        a_ptr, a_col, a_val = _csr(kr, kc, kv, n_c)
         host = [pr, pc, np.ascontiguousarray(pv).view(np.float64), kr, kc, np.ascontiguousarray(kv).view(np.float64),
-                rr, rc, np.ascontiguousarray(rv).view(np.float64)]
+                rr, rc, np.ascontiguousarray(rv).view(np.float64), bt_ptr, bt_col, bt_val.view(np.float64), a_ptr,
+                a_col, a_val.view(np.float64)]
         ent = [torch.from_numpy(np.ascontiguousarray(a)).to(dev) for a in host]
         lib = _lib.load()
         st = torch.cuda.current_stream(dev).cuda_stream
         m = n_p + n_c
         rhs0 = torch.empty((max(m, 1), n), dtype=torch.complex128, device=dev)
-        Bd = torch.empty((max(n_p, 1), n), dtype=torch.complex128, device=dev)
-        _lib.call("mw_scatter_c128", n, n_p, pr.size, ent[0].data_ptr(), ent[1].data_ptr(), ent[2].data_ptr(),
-                  Bd.data_ptr(), st)
         _lib.call("mw_scatter_c128", n, m, rr.size, ent[6].data_ptr(), ent[7].data_ptr(), ent[8].data_ptr(),
                   rhs0.data_ptr(), st)
         buf = {
@@ -764,7 +778,6 @@ class BSplineSolver:
             "table": torch.empty((max(dt.table_rows, 1), nm, nm), dtype=torch.complex128, device=dev),
             # column-major (n x m) right-hand sides live in an (m, n) tensor
             "RHS0": rhs0,
-            "B": Bd,
             "entries": ent,
             "ws": torch.empty(lib.mw_getrf_workspace_size(n), dtype=torch.uint8, device=dev),
             "ipiv": torch.empty(max(n, 1), dtype=torch.int32, device=dev),
@@ -778,10 +791,6 @@ class BSplineSolver:
             buf["Z32"] = torch.empty((n, n), dtype=torch.complex64, device=dev)
             buf["ws_mix"] = torch.empty(lib.mw_zgesv_mixed_workspace_size(n, m), dtype=torch.uint8, device=dev)
         if n_c:
-            # kcl_con (n_c x n, column-major, ld n_c)
-            buf["A"] = torch.empty((n, n_c), dtype=torch.complex128, device=dev)
-            _lib.call("mw_scatter_c128", n_c, n, kr.size, ent[3].data_ptr(), ent[4].data_ptr(), ent[5].data_ptr(),
-                      buf["A"].data_ptr(), st)
             buf["S"] = torch.empty((n_c, n_c), dtype=torch.complex128, device=dev)
             buf["AW"] = torch.empty((max(n_p, 1), n_c), dtype=torch.complex128, device=dev)
             buf["ws_c"] = torch.empty(lib.mw_getrf_workspace_size(n_c), dtype=torch.uint8, device=dev)
@@ -1000,15 +1009,17 @@ class BSplineSolver:
             buf["RHS"].copy_(buf["RHS0"], non_blocking=True)
             self._lu_solve(buf["Z"], n, buf["ws"], buf["ipiv"], buf["info"], buf["RHS"], n_p + n_c, stream)
         X = buf["RHS"]
+        ent = buf["entries"]
         if n_c:
-            # Lam = (A Xc)^-1 (A W); X <- W - Xc Lam   (bspline.py:2980-2989)
-            A, S, AW = buf["A"], buf["S"], buf["AW"]
+            # Lam = (A Xc)^-1 (A W); X <- W - Xc Lam   (bspline.py:2980-2989);
+            # A (the KCL rows, a few +-1 each) applied as a sparse gather
+            S, AW = buf["S"], buf["AW"]
             Wd, Xc = X[:n_p], X[n_p:]
-            _lib.call("mw_zgemm", 0, 0, n_c, n_c, n, 1.0, 0.0, A.data_ptr(), n_c, Xc.data_ptr(), n, 0.0, 0.0,
-                      S.data_ptr(), n_c, stream)
+            _lib.call("mw_csr_mm_c128", n_c, n_c, ent[12].data_ptr(), ent[13].data_ptr(), ent[14].data_ptr(),
+                      Xc.data_ptr(), n, S.data_ptr(), n_c, stream)
             if n_p:
-                _lib.call("mw_zgemm", 0, 0, n_c, n_p, n, 1.0, 0.0, A.data_ptr(), n_c, Wd.data_ptr(), n, 0.0, 0.0,
-                          AW.data_ptr(), n_c, stream)
+                _lib.call("mw_csr_mm_c128", n_c, n_p, ent[12].data_ptr(), ent[13].data_ptr(), ent[14].data_ptr(),
+                          Wd.data_ptr(), n, AW.data_ptr(), n_c, stream)
             self._lu_solve(S, n_c, buf["ws_c"], buf["ipiv_c"], buf["info_c"], AW, n_p, stream)
             W = buf["W"][:n_p]
             W.copy_(Wd, non_blocking=True)
@@ -1017,8 +1028,9 @@ class BSplineSolver:
                           0.0, W.data_ptr(), n, stream)
             X = W
         if n_p:
-            _lib.call("mw_zgemm", 1, 0, n_p, n_p, n, 1.0, 0.0, buf["B"].data_ptr(), n, X.data_ptr(), n, 0.0, 0.0,
-                      buf["Y"].data_ptr(), n_p, stream)
+            # Y = B^T X with B's few nonzeros per port column
+            _lib.call("mw_csr_mm_c128", n_p, n_p, ent[9].data_ptr(), ent[10].data_ptr(), ent[11].data_ptr(),
+                      X.data_ptr(), n, buf["Y"].data_ptr(), n_p, stream)
         return X
 
     def _check_info(self, buf, infos=None):

@@ -520,7 +520,9 @@ __global__ void __launch_bounds__(32 * kTrsmWarps) trsm_kernel(const T* Tm, int6
     constexpr int R = L / 32;
     extern __shared__ __align__(16) unsigned char trsm_smem[];
     T(*sT)[L + 1] = reinterpret_cast<T(*)[L + 1]>(trsm_smem);
+    T* sD = reinterpret_cast<T*>(trsm_smem) + L * (L + 1);  // U: reciprocals of the diagonal
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (UPPER && tid < jb) sD[tid] = cdiv(cone<T>(), Tm[tid + (int64_t)tid * ldt]);
     // stage the triangle the solve reads (strictly lower for L, upper with
     // the diagonal for U), eight loads in flight per thread before the
     // shared-memory stores
@@ -567,7 +569,7 @@ __global__ void __launch_bounds__(32 * kTrsmWarps) trsm_kernel(const T* Tm, int6
         for (int k = jb - 1; k >= 0; --k) {
 #pragma unroll
             for (int i = 0; i < R; ++i)
-                if ((k >> 5) == i && lane == (k & 31)) v[i] = cdiv(v[i], sT[k][k]);
+                if ((k >> 5) == i && lane == (k & 31)) v[i] = v[i] * sD[k];
             T src = v[0];
 #pragma unroll
             for (int i = 1; i < R; ++i)
@@ -587,7 +589,7 @@ __global__ void __launch_bounds__(32 * kTrsmWarps) trsm_kernel(const T* Tm, int6
 
 template <class T, int L>
 constexpr size_t trsm_smem_bytes() {
-    return sizeof(T) * (L * (L + 1));
+    return sizeof(T) * (L * (L + 1) + L);
 }
 
 template <class T>

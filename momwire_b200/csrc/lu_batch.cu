@@ -135,9 +135,11 @@ template <bool UPPER>
 __global__ void __launch_bounds__(256) trsm_batched_kernel(const cf* Tm, int64_t ldt, int64_t ts, cf* X, int64_t ldx,
                                                            int64_t xs, int jb, int ncols) {
     __shared__ cf sT[64][65];
+    __shared__ cf sD[64];  // U: reciprocals of the diagonal
     Tm += (int64_t)blockIdx.y * ts;
     X += (int64_t)blockIdx.y * xs;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (UPPER && tid < jb) sD[tid] = cdiv(cf{1.f, 0.f}, Tm[tid + (int64_t)tid * ldt]);
     for (int i = tid; i < jb * jb; i += blockDim.x) {
         const int r = i % jb, c = i / jb;
         sT[r][c] = Tm[r + (int64_t)c * ldt];
@@ -160,9 +162,9 @@ __global__ void __launch_bounds__(256) trsm_batched_kernel(const cf* Tm, int64_t
         } else {
             for (int k = jb - 1; k >= 0; --k) {
                 if (k < 32) {
-                    if (lane == k) x0 = cdiv(x0, sT[k][k]);
+                    if (lane == k) x0 = x0 * sD[k];
                 } else if (lane == k - 32) {
-                    x1 = cdiv(x1, sT[k][k]);
+                    x1 = x1 * sD[k];
                 }
                 const cf xk = shfl_cf(k < 32 ? x0 : x1, k & 31);
                 if (lane < k) x0 = x0 - sT[lane][k] * xk;

@@ -396,6 +396,19 @@ mw_status mw_pad_identity(int64_t n, int64_t nb, int32_t count, double* Z, int64
                           float* Z32, int64_t ld32, int64_t z32_stride, void* stream);
 
 /*
+ * Host function (no device work): the fill's basis tiles.  Greedy split of
+ * the n_b bases (supp: n_b x wings int32, -1 = no segment) into runs of at
+ * most max_basis consecutive bases whose wings touch at most max_seg
+ * distinct segments.  Outputs (caller-allocated host arrays, n_b entries
+ * each at most): first, nb, ns per tile; seg (tile-major, max_seg columns,
+ * sorted, -1 padded); loc (n_b x wings: a wing's slot in its tile's list,
+ * -1 for no segment); *n_tile.  The tiling itself has no counterpart in the
+ * reference (its fill is organised by observer chunks, bspline.py:2386).
+ */
+mw_status mw_build_tiles(const int32_t* supp, int64_t n_b, int32_t wings, int32_t max_basis, int32_t max_seg,
+                         int32_t* first, int32_t* nb, int32_t* ns, int32_t* seg, int32_t* loc, int64_t* n_tile);
+
+/*
  * Y (n_out x ncols, complex128 column-major, ld ldy) = S X with S sparse in
  * CSR form (row_ptr[n_out + 1], col_idx, vals interleaved re/im; a row's
  * entries are summed in stored order, so results are deterministic) and X

@@ -329,53 +329,33 @@ class Tiles:
 
 def build_tiles(supp: np.ndarray, max_basis=MAX_TILE_BASIS, max_seg=MAX_TILE_SEG) -> Tiles:
     """Greedy split of the basis list into runs of consecutive bases whose
-    wings touch at most ``max_seg`` distinct segments."""
-    n_b = supp.shape[0]
-    rows = [[x for x in r if x >= 0] for r in supp.tolist()]
-    firsts, nbs, segs = [], [], []
-    m = 0
-    while m < n_b:
-        cur = set()
-        cnt = 0
-        while m + cnt < n_b and cnt < max_basis:
-            row = rows[m + cnt]
-            new = {x for x in row if x not in cur}
-            if len(cur) + len(new) > max_seg:
-                break
-            cur |= new
-            cnt += 1
-        if cnt == 0:
-            raise ValueError("a single basis touches more segments than a tile holds")
-        firsts.append(m)
-        nbs.append(cnt)
-        segs.append(sorted(cur))
-        m += cnt
-    T = len(firsts)
-    ns = np.asarray([len(s) for s in segs], dtype=np.int64)
-    used = int(ns.max()) if T else 1
-    seg_arr = np.full((T, used), -1, dtype=np.int32)
-    loc = np.full(supp.shape, -1, dtype=np.int32)
-    if T:
-        # every tile's sorted segment list, keyed by (tile, segment), is one
-        # sorted array; a basis' local slot is its key's rank within its tile
-        flat = np.fromiter((x for s in segs for x in s), dtype=np.int64, count=int(ns.sum()))
-        tile_of_flat = np.repeat(np.arange(T), ns)
-        start = np.concatenate(([0], np.cumsum(ns)[:-1]))
-        seg_arr[tile_of_flat, np.arange(flat.size) - start[tile_of_flat]] = flat
-        stride = int(max(flat.max(), supp.max())) + 1
-        keys = tile_of_flat * stride + flat
-        tile_of_basis = np.repeat(np.arange(T), np.asarray(nbs))
-        want = tile_of_basis[:, None] * stride + supp.astype(np.int64)
-        pos = np.searchsorted(keys, want) - start[tile_of_basis][:, None]
-        loc[:] = np.where(supp >= 0, pos, -1)
+    wings touch at most ``max_seg`` distinct segments (native host routine
+    ``mw_build_tiles``)."""
+    import ctypes as C
+
+    from . import _lib
+
+    supp = np.ascontiguousarray(supp, dtype=np.int32)
+    n_b, wings = supp.shape
+    cap = max(n_b, 1)
+    first = np.zeros(cap, dtype=np.int32)
+    nb = np.zeros(cap, dtype=np.int32)
+    ns = np.zeros(cap, dtype=np.int32)
+    seg = np.full((cap, max_seg), -1, dtype=np.int32)
+    loc = np.full((cap, wings), -1, dtype=np.int32)
+    nt = C.c_int64(0)
+    _lib.call("mw_build_tiles", supp.ctypes.data, n_b, wings, int(max_basis), int(max_seg), first.ctypes.data,
+              nb.ctypes.data, ns.ctypes.data, seg.ctypes.data, loc.ctypes.data, C.byref(nt))
+    T = int(nt.value)
+    used = int(ns[:T].max()) if T else 1
     return Tiles(
-        first=np.asarray(firsts, dtype=np.int32),
-        nb=np.asarray(nbs, dtype=np.int32),
-        ns=ns.astype(np.int32),
-        seg=seg_arr,
-        loc=loc,
-        max_basis=int(max(nbs)) if nbs else 1,
-        max_seg=int(used),
+        first=first[:T].copy(),
+        nb=nb[:T].copy(),
+        ns=ns[:T].copy(),
+        seg=np.ascontiguousarray(seg[:T, :used]),
+        loc=loc[:n_b].copy(),
+        max_basis=int(nb[:T].max()) if T else 1,
+        max_seg=used,
     )
 
 

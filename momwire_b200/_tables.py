@@ -257,7 +257,7 @@ def build_basis(geom: Geometry, degree, start_status, end_status, n_junctions, g
     # Vandermonde V[s] = U diag(h_s^p) with U[sample, p] = unit^p, so
     # V[s]^-1 vals[s] = diag(h_s^-p) U^-1 vals[s]
     Uinv = np.linalg.inv(unit[:, None] ** np.arange(d + 1)[None, :])
-    coef = np.einsum("pq,sqc->scp", Uinv, vals) * hs[:, None, None] ** -np.arange(d + 1)[None, None, :]
+    coef = np.matmul(Uinv, vals).transpose(0, 2, 1) * hs[:, None, None] ** -np.arange(d + 1)[None, None, :]
     # ---- kept bases: interior bases, plus end bases a junction / ground holds
     def end_kind(status):
         if status == "ground":

@@ -1167,7 +1167,7 @@ static mw_status aux_streams(AuxStreams** out) {
 template <class T>
 static mw_status getrf_lookahead(int64_t n, T* A, int64_t lda, int32_t* ipiv, int32_t* info, char* ws,
                                  const volatile int32_t* cancel, const Updater& up_main, const Updater& up_trail,
-                                 cudaStream_t st) {
+                                 cudaStream_t st, T* Baug = nullptr, int64_t ldb = 0, int64_t nrhs = 0) {
     MW_CHECK_CUDA(cudaMemsetAsync(info, 0, 2 * sizeof(int32_t), st));
     MW_CHECK_CUDA(cudaMemsetAsync(ws, 0, sizeof(PanelWs), st));
     {
@@ -1228,6 +1228,20 @@ static mw_status getrf_lookahead(int64_t n, T* A, int64_t lda, int32_t* ipiv, in
                              jb, up_trail, tr);
             if (s != MW_OK) return s;
         }
+        if (Baug != nullptr && nrhs > 0) {
+            // right-hand sides carried as extra columns right of the matrix:
+            // this panel's interchanges, L11^-1 on its rows, L21 update below
+            // (L21 stays as it is until the deferred left interchanges at the
+            // end, which the later rows of Baug then mirror in its own swaps)
+            laswp_launch<T>(Baug, ldb, 0, nrhs, ipiv, j0, j0 + jb, tr);
+            s = trsm_lower_blocked<T>(A + j0 + j0 * lda, lda, Baug + j0, ldb, jb, nrhs, up_trail, tr);
+            if (s != MW_OK) return s;
+            if (n - c1 > 0) {
+                s = block_update(A + c1 + j0 * lda, lda, Baug + j0, ldb, Baug + c1, ldb, n - c1, nrhs, jb, up_trail,
+                                 tr);
+                if (s != MW_OK) return s;
+            }
+        }
         MW_CHECK_CUDA(cudaEventRecord(ax->ev_trail[j & 3], tr));
         MW_CHECK_CUDA(cudaGetLastError());
     }
@@ -1239,6 +1253,24 @@ static mw_status getrf_lookahead(int64_t n, T* A, int64_t lda, int32_t* ipiv, in
         laswp_launch<T>(A, lda, 0, j0, ipiv, j0, j0 + jb, st);
     }
     MW_CHECK_CUDA(cudaMemcpyAsync(info + 1, &pws->err, sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
+    return MW_OK;
+}
+
+// X <- U^-1 X (the back substitution of a solve).
+template <class T>
+static mw_status getrs_upper(int64_t n, int64_t nrhs, const T* LU, int64_t lda, T* B, int64_t ldb, const Updater& up,
+                             cudaStream_t st) {
+    constexpr int LF = GetrsLeaf<T>::value;
+    const int64_t last = ((n - 1) / LF) * LF;
+    for (int64_t j0 = last; j0 >= 0; j0 -= LF) {
+        const int jb = (int)((n - j0) < LF ? (n - j0) : LF);
+        trsm_launch<T, true, LF>(LU + j0 + j0 * lda, lda, B + j0, ldb, jb, nrhs, st);
+        if (j0 > 0) {
+            mw_status s = block_update(LU + j0 * lda, lda, B + j0, ldb, B, ldb, j0, nrhs, jb, up, st);
+            if (s != MW_OK) return s;
+        }
+    }
+    MW_CHECK_CUDA(cudaGetLastError());
     return MW_OK;
 }
 
@@ -1365,6 +1397,44 @@ extern "C" mw_status mw_cgetrf(int64_t n, float* Ad, int64_t lda, int32_t* ipiv,
     MW_CHECK_CUDA(cudaMemcpyAsync(info + 1, up.tc_err, sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
     return MW_OK;
 }
+
+namespace mw {
+// Complex64 factorisation that also carries nrhs right-hand sides (B, ld
+// ldb, permuted and overwritten with L^-1 P B) through the trail stream;
+// the forward substitution of the first solve then costs no extra pass.
+mw_status cgetrf_forward(int64_t n, float* Ad, int64_t lda, int32_t* ipiv, int32_t* info, void* workspace,
+                         size_t workspace_bytes, float* Bd, int64_t ldb, int64_t nrhs, const volatile int32_t* cancel,
+                         void* stream) {
+    MW_REQUIRE(n >= 0 && lda >= (n > 0 ? n : 1) && nrhs >= 0 && ldb >= (n > 0 ? n : 1), "bad sizes");
+    MW_REQUIRE(Ad && ipiv && info && workspace && (nrhs == 0 || Bd), "NULL argument");
+    MW_REQUIRE(workspace_bytes >= cgetrf_ws_bytes(n, nrhs), "workspace too small");
+    char* ws = static_cast<char*>(workspace);
+    Updater up = tc_updater(ws, workspace_bytes, n, nrhs);
+    Updater up_main = tc_updater_main(ws, n, nrhs);
+    up.max_ctas = panel_sms<cf>() - kLaPanelCtas;
+    cudaStream_t st = as_stream(stream);
+    MW_CHECK_CUDA(cudaMemsetAsync(up.tc_err, 0, sizeof(int), st));
+    mw_status s = getrf_lookahead<cf>(n, reinterpret_cast<cf*>(Ad), lda, ipiv, info, ws, cancel, up_main, up, st,
+                                      reinterpret_cast<cf*>(Bd), ldb, nrhs);
+    if (s != MW_OK) return s;
+    MW_CHECK_CUDA(cudaMemcpyAsync(info + 1, up.tc_err, sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
+    return MW_OK;
+}
+
+// B <- U^-1 B with the factors of cgetrf_forward.
+mw_status cgetrs_upper(int64_t n, int64_t nrhs, const float* LUd, int64_t lda, float* Bd, int64_t ldb, void* workspace,
+                       size_t workspace_bytes, void* stream) {
+    MW_REQUIRE(workspace_bytes >= cgetrf_ws_bytes(n, nrhs), "workspace too small");
+    if (n == 0 || nrhs == 0) return MW_OK;
+    {
+        mw_status s0 = trsm_setup<cf>();
+        if (s0 != MW_OK) return s0;
+    }
+    Updater up = tc_updater(static_cast<char*>(workspace), workspace_bytes, n, nrhs);
+    return getrs_upper<cf>(n, nrhs, reinterpret_cast<const cf*>(LUd), lda, reinterpret_cast<cf*>(Bd), ldb, up,
+                           as_stream(stream));
+}
+}  // namespace mw
 
 extern "C" mw_status mw_cgetrs(int64_t n, int64_t nrhs, const float* LUd, int64_t lda, const int32_t* ipiv, float* Bd,
                                int64_t ldb, void* workspace, size_t workspace_bytes, void* stream) {

@@ -76,6 +76,14 @@ extern "C" mw_status mw_cgetrf(int64_t n, float* A, int64_t lda, int32_t* ipiv, 
 extern "C" mw_status mw_cgetrs(int64_t n, int64_t nrhs, const float* LU, int64_t lda, const int32_t* ipiv, float* B,
                                int64_t ldb, void* workspace, size_t workspace_bytes, void* stream);
 
+namespace mw {
+mw_status cgetrf_forward(int64_t n, float* Ad, int64_t lda, int32_t* ipiv, int32_t* info, void* workspace,
+                         size_t workspace_bytes, float* Bd, int64_t ldb, int64_t nrhs, const volatile int32_t* cancel,
+                         void* stream);
+mw_status cgetrs_upper(int64_t n, int64_t nrhs, const float* LUd, int64_t lda, float* Bd, int64_t ldb, void* workspace,
+                       size_t workspace_bytes, void* stream);
+}  // namespace mw
+
 static size_t al256(size_t x) { return (x + 255) & ~size_t(255); }
 
 extern "C" size_t mw_zgesv_mixed_workspace_size(int64_t n, int64_t nrhs) {
@@ -105,7 +113,12 @@ extern "C" mw_status mw_zgesv_mixed(int64_t n, int64_t nrhs, const double* Z, in
     cd* Xc = reinterpret_cast<cd*>(X);
     const int64_t tot = n * nrhs;
 
-    mw_status s = mw_cgetrf(n, Z32, ldz32, ipiv, info, ws_lu, lu_ws, nrhs, cancel, stream);
+    // the first solve's right-hand sides ride through the factorisation
+    // (complex64 B, forward-substituted as the trailing columns are updated)
+    to_c64_kernel<<<grid_for(tot), 256, 0, st>>>(Bc, ldb, R32, n, n, nrhs);
+    count_launch();
+    mw_status s = cgetrf_forward(n, Z32, ldz32, ipiv, info, ws_lu, lu_ws, reinterpret_cast<float*>(R32), n, nrhs,
+                                 cancel, stream);
     if (s != MW_OK) return s;
     int32_t hinfo[2] = {0, 0};
     MW_CHECK_CUDA(cudaMemcpyAsync(hinfo, info, sizeof(hinfo), cudaMemcpyDeviceToHost, st));
@@ -131,12 +144,17 @@ extern "C" mw_status mw_zgesv_mixed(int64_t n, int64_t nrhs, const double* Z, in
             set_error("solve cancelled");
             return MW_ERR_CANCELLED;
         }
-        {
-            ProfileScope ps(PC_REFINE, st, 0.0, 24.0 * (double)tot);
-            to_c64_kernel<<<grid_for(tot), 256, 0, st>>>(R, n, R32, n, n, nrhs);
-            count_launch();
+        if (it == 0) {
+            // R32 holds L^-1 P B from the factorisation
+            s = cgetrs_upper(n, nrhs, Z32, ldz32, reinterpret_cast<float*>(R32), n, ws_lu, lu_ws, stream);
+        } else {
+            {
+                ProfileScope ps(PC_REFINE, st, 0.0, 24.0 * (double)tot);
+                to_c64_kernel<<<grid_for(tot), 256, 0, st>>>(R, n, R32, n, n, nrhs);
+                count_launch();
+            }
+            s = mw_cgetrs(n, nrhs, Z32, ldz32, ipiv, reinterpret_cast<float*>(R32), n, ws_lu, lu_ws, stream);
         }
-        s = mw_cgetrs(n, nrhs, Z32, ldz32, ipiv, reinterpret_cast<float*>(R32), n, ws_lu, lu_ws, stream);
         if (s != MW_OK) return s;
         MW_CHECK_CUDA(cudaMemsetAsync(norms, 0, sizeof(double) * 2 * nrhs, st));
         {

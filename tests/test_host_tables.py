@@ -145,3 +145,18 @@ def test_basis_count_and_kcl_rows_without_building(name):
     assert n == s._basis().n
     kcl, _pa, _pv = s._split_kcl_ports(s._basis().kcl_A)
     assert left == kcl.shape[0]
+
+
+def test_native_tiles_edge_cases():
+    """mw_build_tiles: empty input, one basis per tile, and a basis wider
+    than a tile is rejected with a clear error."""
+    from momwire_b200 import _lib
+
+    t = T.build_tiles(np.zeros((0, 3), dtype=np.int32))
+    assert t.first.size == 0 and t.loc.shape == (0, 3)
+    supp = np.array([[0, 1, 2], [1, 2, 3], [5, -1, -1]], dtype=np.int32)
+    t = T.build_tiles(supp, max_basis=1, max_seg=3)
+    assert list(t.first) == [0, 1, 2] and list(t.nb) == [1, 1, 1] and list(t.ns) == [3, 3, 1]
+    assert list(t.loc[2]) == [0, -1, -1] and list(t.seg[2, :1]) == [5]
+    with pytest.raises(_lib.NativeError, match="touches more segments than a tile holds"):
+        T.build_tiles(supp, max_basis=4, max_seg=2)

@@ -144,7 +144,17 @@ def group_plan(orders, n_k, budget_bytes, bytes_per_matrix):
     return plan
 
 
-def _solve_group(solvers, nb, ks, stream, pw=None, Bs=None):
+def _group_bytes(count, nb, P):
+    """Device bytes of one group's Z, Z32 and solver workspace (each part
+    256-byte aligned), the arena ``_solve_group`` carves them from."""
+    from . import _lib
+
+    al = lambda x: (int(x) + 255) & ~255  # noqa: E731
+    wsb = _lib.load().mw_zgesv_mixed_batched_workspace_size(nb, P, count)
+    return al(count * nb * nb * 16) + al(count * nb * nb * 8) + al(wsb)
+
+
+def _solve_group(solvers, nb, ks, stream, pw=None, Bs=None, arena=None):
     """Batched mixed solve of several structures at the frequencies ks in
     one factorisation: each structure's n x n matrices are filled into the
     leading block of order-nb matrices padded with the identity
@@ -164,8 +174,20 @@ def _solve_group(solvers, nb, ks, stream, pw=None, Bs=None):
     if Bs is None:
         Bs = [s._port_columns()[0] for s in solvers]
     P = max(B.shape[1] for B in Bs)
-    Z = torch.empty((count, nb, nb), dtype=torch.complex128, device=dev)
-    Z32 = torch.empty((count, nb, nb), dtype=torch.complex64, device=dev)
+    wsb = lib.mw_zgesv_mixed_batched_workspace_size(nb, P, count)
+    if arena is not None and arena.numel() >= _group_bytes(count, nb, P):
+        # views of one allocation made for the whole sweep (no allocation
+        # per group)
+        al = lambda x: (int(x) + 255) & ~255  # noqa: E731
+        o1 = al(count * nb * nb * 16)
+        o2 = o1 + al(count * nb * nb * 8)
+        Z = arena[: count * nb * nb * 16].view(torch.complex128).view(count, nb, nb)
+        Z32 = arena[o1 : o1 + count * nb * nb * 8].view(torch.complex64).view(count, nb, nb)
+        ws = arena[o2 : o2 + wsb]
+    else:
+        Z = torch.empty((count, nb, nb), dtype=torch.complex128, device=dev)
+        Z32 = torch.empty((count, nb, nb), dtype=torch.complex64, device=dev)
+        ws = torch.empty(wsb, dtype=torch.uint8, device=dev)
     # the right-hand sides of every structure, staged in page-locked memory
     # and uploaded with one stream-ordered copy (pageable uploads would make
     # the host wait for the fills queued before them)
@@ -185,8 +207,6 @@ def _solve_group(solvers, nb, ks, stream, pw=None, Bs=None):
     X = torch.empty((count, P, nb), dtype=torch.complex128, device=dev)
     ipiv = torch.empty((count, nb), dtype=torch.int32, device=dev)
     info = torch.zeros(count, dtype=torch.int32, device=dev)
-    wsb = lib.mw_zgesv_mixed_batched_workspace_size(nb, P, count)
-    ws = torch.empty(wsb, dtype=torch.uint8, device=dev)
     it, corr = C.c_int32(0), C.c_double(0.0)
     s0 = solvers[0]
     _lib.call("mw_zgesv_mixed_batched", nb, P, count, int(pw), Z.data_ptr(), nb, nb * nb, Z32.data_ptr(), nb,
@@ -272,8 +292,14 @@ def grouped_mixed_sweep(structs, ks, device=None, budget_bytes=32 << 30, indices
         return nb * nb * 24 + lib.mw_zgesv_mixed_batched_workspace_size(nb, 1, 1) + nb * 64
 
     plan = group_plan([solvers[i]._basis_count() for i in grouped], len(ks), budget_bytes, per_matrix)
+    # the heaviest groups first: the first group waits for its host tables,
+    # after which the helper thread prepares the rest while the GPU works
+    plan.sort(key=lambda g: -len(g[1]) * g[0] ** 3)
     dev = solvers[grouped[0]]._torch_device()
     stream = torch.cuda.current_stream(dev).cuda_stream
+    P_max = max(solvers[i]._port_count() for i in grouped)
+    arena = torch.empty(max(_group_bytes(len(g) * len(ks), nb, P_max) for nb, g in plan), dtype=torch.uint8,
+                        device=dev)
     # one host thread prepares the next structures' tables (host build and
     # upload on its own stream) while this thread fills and solves
     import concurrent.futures as cf
@@ -294,7 +320,8 @@ def grouped_mixed_sweep(structs, ks, device=None, budget_bytes=32 << 30, indices
             ids = [grouped[j] for j in members]
             for i in ids:
                 futs[i].result()
-            res, _it = _solve_group([solvers[i] for i in ids], nb, ks, stream, Bs=[ports[i] for i in ids])
+            res, _it = _solve_group([solvers[i] for i in ids], nb, ks, stream, Bs=[ports[i] for i in ids],
+                                    arena=arena)
             for g, i in enumerate(ids):
                 out[i] = res[g]
     return out

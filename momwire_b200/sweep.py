@@ -144,6 +144,17 @@ def group_plan(orders, n_k, budget_bytes, bytes_per_matrix):
     return plan
 
 
+class _Ports:
+    """The port columns of a group's members, read once every member's
+    preparation has finished (after its fills were issued)."""
+
+    def __init__(self, ports, ids):
+        self._ports, self._ids = ports, ids
+
+    def __iter__(self):
+        return (self._ports[i] for i in self._ids)
+
+
 def _group_bytes(count, nb, P):
     """Device bytes of one group's Z, Z32 and solver workspace (each part
     256-byte aligned), the arena ``_solve_group`` carves them from."""
@@ -154,7 +165,7 @@ def _group_bytes(count, nb, P):
     return al(count * nb * nb * 16) + al(count * nb * nb * 8) + al(wsb)
 
 
-def _solve_group(solvers, nb, ks, stream, pw=None, Bs=None, arena=None):
+def _solve_group(solvers, nb, ks, stream, pw=None, Bs=None, arena=None, wait=None):
     """Batched mixed solve of several structures at the frequencies ks in
     one factorisation: each structure's n x n matrices are filled into the
     leading block of order-nb matrices padded with the identity
@@ -171,9 +182,7 @@ def _solve_group(solvers, nb, ks, stream, pw=None, Bs=None, arena=None):
     nk = len(ks)
     G = len(solvers)
     count = G * nk
-    if Bs is None:
-        Bs = [s._port_columns()[0] for s in solvers]
-    P = max(B.shape[1] for B in Bs)
+    P = max(s._port_count() for s in solvers)
     wsb = lib.mw_zgesv_mixed_batched_workspace_size(nb, P, count)
     if arena is not None and arena.numel() >= _group_bytes(count, nb, P):
         # views of one allocation made for the whole sweep (no allocation
@@ -188,6 +197,16 @@ def _solve_group(solvers, nb, ks, stream, pw=None, Bs=None, arena=None):
         Z = torch.empty((count, nb, nb), dtype=torch.complex128, device=dev)
         Z32 = torch.empty((count, nb, nb), dtype=torch.complex64, device=dev)
         ws = torch.empty(wsb, dtype=torch.uint8, device=dev)
+    k_dev = solvers[0]._upload_k(ks)
+    for g, s in enumerate(solvers):
+        if wait is not None:
+            wait(g)  # this structure's host tables (later ones may still be in preparation)
+        n = s._basis().n
+        zb, z32b = Z[g * nk : (g + 1) * nk], Z32[g * nk : (g + 1) * nk]
+        s._fill_batched(ks, stream, Z=zb, Z32=z32b, ld=nb, k_dev=k_dev)
+        _lib.call("mw_pad_identity", n, nb, nk, zb.data_ptr(), nb, nb * nb, z32b.data_ptr(), nb, nb * nb, stream)
+    if Bs is None:
+        Bs = [s._port_columns()[0] for s in solvers]
     # the right-hand sides of every structure, staged in page-locked memory
     # and uploaded with one stream-ordered copy (pageable uploads would make
     # the host wait for the fills queued before them)
@@ -196,12 +215,6 @@ def _solve_group(solvers, nb, ks, stream, pw=None, Bs=None, arena=None):
         Bh[g, : B.shape[1], : B.shape[0]] = torch.from_numpy(np.ascontiguousarray(B.T))
     Bg = Bh.to(dev, non_blocking=True)
     Bd = Bg.repeat_interleave(nk, dim=0)
-    k_dev = solvers[0]._upload_k(ks)
-    for g, s in enumerate(solvers):
-        n = s._basis().n
-        zb, z32b = Z[g * nk : (g + 1) * nk], Z32[g * nk : (g + 1) * nk]
-        s._fill_batched(ks, stream, Z=zb, Z32=z32b, ld=nb, k_dev=k_dev)
-        _lib.call("mw_pad_identity", n, nb, nk, zb.data_ptr(), nb, nb * nb, z32b.data_ptr(), nb, nb * nb, stream)
     if pw is None:
         pw = _group_width(solvers[0], nb, Z, Z32, Bd, P, stream)
     X = torch.empty((count, P, nb), dtype=torch.complex128, device=dev)
@@ -318,10 +331,12 @@ def grouped_mixed_sweep(structs, ks, device=None, budget_bytes=32 << 30, indices
         futs = {grouped[j]: ex.submit(prep, grouped[j]) for _nb, members in plan for j in members}
         for nb, members in plan:
             ids = [grouped[j] for j in members]
-            for i in ids:
-                futs[i].result()
-            res, _it = _solve_group([solvers[i] for i in ids], nb, ks, stream, Bs=[ports[i] for i in ids],
-                                    arena=arena)
+
+            def wait(g, ids=ids):
+                futs[ids[g]].result()
+
+            res, _it = _solve_group([solvers[i] for i in ids], nb, ks, stream, arena=arena, wait=wait,
+                                    Bs=_Ports(ports, ids))
             for g, i in enumerate(ids):
                 out[i] = res[g]
     return out

@@ -409,6 +409,19 @@ mw_status mw_build_tiles(const int32_t* supp, int64_t n_b, int32_t wings, int32_
                          int32_t* first, int32_t* nb, int32_t* ns, int32_t* seg, int32_t* loc, int64_t* n_tile);
 
 /*
+ * Host function (no device work): the basis polynomials of
+ * _build_basis_polynomials (bspline.py:1318-1414) for m kept bases, basis b
+ * being local basis js[b] of wire bw[b].  garc: every wire's knot arc
+ * positions back to back (wire w at arc_off[w], wire_n[w] + 1 values);
+ * wire_first[w]: global index of its first segment.  Outputs supp (m x
+ * (d+1) int32, -1 where a wing has no segment) and poly (m x (d+1) x (d+1):
+ * wing a's monomial coefficients in the local arc length).
+ */
+mw_status mw_basis_polys(const double* garc, const int64_t* arc_off, const int64_t* wire_n, const int64_t* wire_first,
+                         int64_t n_wires, int32_t degree, const int64_t* js, const int64_t* bw, int64_t m,
+                         int32_t* supp, double* poly);
+
+/*
  * Y (n_out x ncols, complex128 column-major, ld ldy) = S X with S sparse in
  * CSR form (row_ptr[n_out + 1], col_idx, vals interleaved re/im; a row's
  * entries are summed in stored order, so results are deterministic) and X

@@ -142,6 +142,7 @@ _SIGS = {
     "mw_pad_identity": (i32, [i64, i64, i32, vp, i64, i64, vp, i64, i64, vp]),
     "mw_csr_mm_c128": (i32, [i64, i64, vp, vp, vp, vp, i64, vp, i64, vp]),
     "mw_build_tiles": (i32, [vp, i64, i32, i32, i32, vp, vp, vp, vp, vp, C.POINTER(i64)]),
+    "mw_basis_polys": (i32, [vp, vp, vp, vp, i64, i32, vp, vp, i64, vp, vp]),
     "mw_zgemm": (i32, [i32, i32, i64, i64, i64, f64, f64, vp, i64, vp, i64, f64, f64, vp, i64, vp]),
     "mw_somm_surfaces_workspace_size": (sz, []),
     "mw_somm_surfaces": (i32, [i64, vp, vp, vp, vp, f64, f64, f64, f64, f64, f64, vp, vp, vp]),

@@ -227,37 +227,16 @@ def build_basis(geom: Geometry, degree, start_status, end_status, n_junctions, g
     """Clamped knot vector per wire; keep interior bases plus the value-1
     end basis at junction / ground ends; per-wing monomial coefficients in
     local arc length from values at d+1 uniform points (the reference's
-    design-matrix + Vandermonde step, ``bspline.py:1318-1414``).
-
-    The per-segment coefficients of all wires come from one batched
-    evaluation: segment s of a wire reads the knots at spans s+1-d .. s+d,
-    which in the clamped vector are the wire's arc positions at indices
-    clip(s+t, 0, n_w) for t in 1-d .. d."""
+    design-matrix + Vandermonde step, ``bspline.py:1318-1414``), computed by
+    the native host routine ``mw_basis_polys``: segment s of a wire reads the
+    knots at spans s+1-d .. s+d, which in the clamped vector are the wire's
+    arc positions at indices clip(s+t, 0, n_w) for t in 1-d .. d."""
     d = int(degree)
     n_wires = len(geom.wire_first)
     wire_n = np.asarray(geom.wire_n, dtype=np.int64)
     firsts = np.asarray(geom.wire_first, dtype=np.int64)
     arcs = geom.wire_arc
     knots_all = [np.concatenate([np.zeros(d), arc, np.full(d, arc[-1])]) for arc in arcs]
-    # ---- per-segment coefficients [segment, active basis c (= j - s), power p]
-    n_seg = int(wire_n.sum())
-    garc = np.concatenate(arcs)
-    arc_off = np.concatenate(([0], np.cumsum(wire_n + 1)[:-1]))
-    seg_wire = np.repeat(np.arange(n_wires), wire_n)
-    s_loc = np.arange(n_seg) - np.repeat(firsts - firsts[0], wire_n)
-    t = np.arange(1 - d, d + 1)
-    win = np.clip(s_loc[:, None] + t[None, :], 0, wire_n[seg_wire][:, None]) + arc_off[seg_wire][:, None]
-    K = garc[win]  # (n_seg, 2d) knots of spans s+1-d .. s+d
-    a0 = garc[arc_off[seg_wire] + s_loc]
-    hs = garc[arc_off[seg_wire] + s_loc + 1] - a0
-    unit = np.linspace(0.0, 1.0, d + 1)
-    us = hs[:, None] * unit[None, :]  # (n_seg, d+1) local sample points
-    span = np.repeat(np.arange(n_seg) * (2 * d) + (d - 1), d + 1)
-    vals = _span_values(K.ravel(), d, span, (a0[:, None] + us).ravel()).reshape(n_seg, d + 1, d + 1)
-    # Vandermonde V[s] = U diag(h_s^p) with U[sample, p] = unit^p, so
-    # V[s]^-1 vals[s] = diag(h_s^-p) U^-1 vals[s]
-    Uinv = np.linalg.inv(unit[:, None] ** np.arange(d + 1)[None, :])
-    coef = np.matmul(Uinv, vals).transpose(0, 2, 1) * hs[:, None, None] ** -np.arange(d + 1)[None, None, :]
     # ---- kept bases: interior bases, plus end bases a junction / ground holds
     def end_kind(status):
         if status == "ground":
@@ -281,16 +260,20 @@ def build_basis(geom: Geometry, degree, start_status, end_status, n_junctions, g
     bw = np.repeat(np.arange(n_wires), n_kept)
     # local basis index: 1 - has_start at a wire's first kept basis, +1 after
     js = np.arange(m) - np.repeat(m_first, n_kept) + np.repeat(1 - has_s, n_kept)
-    supp = np.full((m, d + 1), -1, dtype=np.int32)
-    poly = np.zeros((m, d + 1, d + 1))
-    lo = np.maximum(0, js - d)  # first wing of basis j
-    hi = np.minimum(wire_n[bw], js + 1)  # one past its last wing
-    for a in range(d + 1):
-        sl = lo + a
-        ok = sl < hi
-        gs = firsts[bw[ok]] + sl[ok]
-        supp[ok, a] = gs
-        poly[ok, a, :] = coef[gs - firsts[0], (js - sl)[ok], :]
+    # supports and per-wing monomial coefficients: native host routine
+    import ctypes as C
+
+    from . import _lib
+
+    garc = np.ascontiguousarray(np.concatenate(arcs), dtype=np.float64)
+    arc_off = np.ascontiguousarray(np.concatenate(([0], np.cumsum(wire_n + 1)[:-1])), dtype=np.int64)
+    js = np.ascontiguousarray(js, dtype=np.int64)
+    bw = np.ascontiguousarray(bw, dtype=np.int64)
+    supp = np.empty((m, d + 1), dtype=np.int32)
+    poly = np.empty((m, d + 1, d + 1))
+    _lib.call("mw_basis_polys", garc.ctypes.data, arc_off.ctypes.data, np.ascontiguousarray(wire_n).ctypes.data,
+              np.ascontiguousarray(firsts).ctypes.data, n_wires, d, js.ctypes.data, bw.ctypes.data, m,
+              supp.ctypes.data, poly.ctypes.data)
     rows = [j for j in range(n_junctions) if j not in grounded]
     ri, ci, vi = [], [], []
     for r, j in enumerate(rows):

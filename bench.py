@@ -37,6 +37,10 @@ sys.path.insert(0, str(ROOT))
 METRIC = "sweep pts/s & fill+LU time, mixed+batched vs FP64 GPU at |ΔZin|/|Zin|≤1e-6"
 UNIT = "pts/s"
 WORKLOAD = "dipole_array_16x16_300MHz_41seg_d2_256port"
+# ncu dram__bytes_read.sum + dram__bytes_write.sum averaged over the 810
+# tensor-core launches of one 16x16 mixed step (43.32 GB read + 19.53 GB
+# written)
+TC_TRAFFIC_PER_LAUNCH = 77.6e6
 
 
 def parse():
@@ -317,8 +321,13 @@ def run_b200(args, kw):
             # rate; the 3xTF32 split issues three MMAs per algorithmic one
             bf16 = float(peaks.get("bf16_tflops", 1590.0))
             peak = bf16 / 2.0
+            # DRAM bytes per launch of this kernel on this workload, from an
+            # ncu capture of every tensor-core launch of one step (ncu cannot
+            # run inside the timed bench)
+            traffic = TC_TRAFFIC_PER_LAUNCH if (args.nx == 16 and args.precision == "mixed") else None
             roof = {"kernel": name, "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                    "frac": achieved / peak, "tensor_pipe_frac": 3.0 * achieved / peak, "traffic": None,
+                    "frac": achieved / peak, "tensor_pipe_frac": 3.0 * achieved / peak, "traffic": traffic,
+                    "traffic_unit": "bytes per launch (dram read + write, ncu)",
                     "launches_per_step": cnt / args.steps, "avg_launch_ms": tms / cnt,
                     "peak_source": "MEASURED_PEAKS bf16_tflops / 2 (TF32 rate); achieved counts 8mnk complex "
                                    "flops, the tensor pipe executes 3x that (3xTF32)"}

@@ -26,7 +26,8 @@ mw_status cgemm_tc_update_batched(int64_t m, int64_t n, int64_t k, int batch, co
 size_t cgemm_tc_workspace_batched(int64_t m, int64_t n, int64_t k, int batch);
 
 constexpr int kBNB = 16;       // default panel width of the batched factorisation
-constexpr int kBNBMax = 32;    // widest panel the workspace is sized for
+constexpr int kBNBMax = 32;    // widest panel of the batched factorisation (<= kBOuter)
+constexpr int kBOuter = 64;    // block of the batched factorisation: the trailing update's k
 constexpr int kBSB = 64;       // block size of the batched triangular solves
 constexpr int kBThreads = 256;
 
@@ -262,7 +263,7 @@ struct BatchWs {
 };
 
 static size_t batch_ws_bytes(int n, int nrhs, int batch) {
-    return al256(cgemm_tc_workspace_batched(n, n, kBNBMax, batch)) + 256 + al256((size_t)batch * n * nrhs * 16) +
+    return al256(cgemm_tc_workspace_batched(n, n, kBOuter, batch)) + 256 + al256((size_t)batch * n * nrhs * 16) +
            al256((size_t)batch * n * nrhs * 8) + al256((size_t)batch * 16);
 }
 
@@ -270,7 +271,7 @@ static BatchWs batch_ws(void* ws, int n, int nrhs, int batch) {
     char* w = static_cast<char*>(ws);
     BatchWs b;
     b.tc = w;
-    b.tc_bytes = cgemm_tc_workspace_batched(n, n, kBNBMax, batch);
+    b.tc_bytes = cgemm_tc_workspace_batched(n, n, kBOuter, batch);
     w += al256(b.tc_bytes);
     b.tc_err = reinterpret_cast<int*>(w);
     w += 256;
@@ -291,37 +292,66 @@ static mw_status cgetrf_batched(int n, int batch, cf* A, int64_t lda, int64_t st
         MW_CHECK_CUDA(cudaFuncSetAttribute(panel1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
         attr = true;
     }
-    for (int j0 = 0; j0 < n; j0 += pw) {
-        const int jb = (n - j0) < pw ? (n - j0) : pw;
-        {
-            ProfileScope ps(PC_PANEL, st, 4.0 * (double)(n - j0) * jb * jb * batch);
-            panel1_kernel<<<batch, kBThreads, (size_t)(n - j0) * jb * sizeof(cf), st>>>(A, lda, stride, n, j0, jb,
-                                                                                        ipiv, info);
-            count_launch();
+    // Blocked right-looking factorisation: kBOuter-column blocks, each
+    // factored as pw-column panels (one CTA per matrix) whose updates stay
+    // inside the block; the rest of the matrix then takes the block's row
+    // interchanges, one triangular solve and ONE tensor-core update with
+    // k = kBOuter (a pw-wide k would underuse the tensor pipe).
+    for (int J0 = 0; J0 < n; J0 += kBOuter) {
+        const int bw = (n - J0) < kBOuter ? (n - J0) : kBOuter;
+        for (int j0 = J0; j0 < J0 + bw; j0 += pw) {
+            const int jb = (J0 + bw - j0) < pw ? (J0 + bw - j0) : pw;
+            {
+                ProfileScope ps(PC_PANEL, st, 4.0 * (double)(n - j0) * jb * jb * batch);
+                panel1_kernel<<<batch, kBThreads, (size_t)(n - j0) * jb * sizeof(cf), st>>>(A, lda, stride, n, j0, jb,
+                                                                                            ipiv, info);
+                count_launch();
+            }
+            if (j0 > 0) {
+                ProfileScope ps(PC_LASWP, st);
+                laswp_batched_kernel<cf><<<dim3((j0 + 127) / 128, batch), 128, 0, st>>>(A, lda, stride, 0, j0, ipiv,
+                                                                                        n, j0, j0 + jb);
+                count_launch();
+            }
+            const int inner = J0 + bw - j0 - jb;  // block columns right of this panel
+            if (inner > 0) {
+                {
+                    ProfileScope ps(PC_LASWP, st);
+                    laswp_batched_kernel<cf><<<dim3((inner + 127) / 128, batch), 128, 0, st>>>(
+                        A, lda, stride, j0 + jb, inner, ipiv, n, j0, j0 + jb);
+                }
+                cf* A11 = A + j0 + (int64_t)j0 * lda;
+                cf* A12 = A + j0 + (int64_t)(j0 + jb) * lda;
+                {
+                    ProfileScope ps(PC_TRSM, st, 4.0 * (double)jb * jb * inner * batch);
+                    trsm_batched_kernel<false><<<trsm_batched_grid(inner, batch), 256, 0, st>>>(A11, lda, stride, A12,
+                                                                                             lda, stride, jb, inner);
+                }
+                count_launch(2);
+                mw_status s = cgemm_tc_update_batched(n - j0 - jb, inner, jb, batch, A + (j0 + jb) + (int64_t)j0 * lda,
+                                                      lda, stride, A12, lda, stride,
+                                                      A + (j0 + jb) + (int64_t)(j0 + jb) * lda, lda, stride, w.tc,
+                                                      w.tc_bytes, w.tc_err, st, 0);
+                if (s != MW_OK) return s;
+            }
         }
-        const int right = n - j0 - jb;
-        if (j0 > 0) {
-            ProfileScope ps(PC_LASWP, st);
-            laswp_batched_kernel<cf><<<dim3((j0 + 127) / 128, batch), 128, 0, st>>>(A, lda, stride, 0, j0, ipiv, n,
-                                                                                    j0, j0 + jb);
-            count_launch();
-        }
+        const int right = n - J0 - bw;
         if (right > 0) {
             {
                 ProfileScope ps(PC_LASWP, st);
                 laswp_batched_kernel<cf><<<dim3((right + 127) / 128, batch), 128, 0, st>>>(
-                    A, lda, stride, j0 + jb, right, ipiv, n, j0, j0 + jb);
+                    A, lda, stride, J0 + bw, right, ipiv, n, J0, J0 + bw);
             }
-            cf* A11 = A + j0 + (int64_t)j0 * lda;
-            cf* A12 = A + j0 + (int64_t)(j0 + jb) * lda;
+            cf* A11 = A + J0 + (int64_t)J0 * lda;
+            cf* A12 = A + J0 + (int64_t)(J0 + bw) * lda;
             {
-                ProfileScope ps(PC_TRSM, st, 4.0 * (double)jb * jb * right * batch);
+                ProfileScope ps(PC_TRSM, st, 4.0 * (double)bw * bw * right * batch);
                 trsm_batched_kernel<false><<<trsm_batched_grid(right, batch), 256, 0, st>>>(A11, lda, stride, A12, lda,
-                                                                                         stride, jb, right);
+                                                                                         stride, bw, right);
             }
             count_launch(2);
-            mw_status s = cgemm_tc_update_batched(right, right, jb, batch, A + (j0 + jb) + (int64_t)j0 * lda, lda,
-                                                  stride, A12, lda, stride, A + (j0 + jb) + (int64_t)(j0 + jb) * lda,
+            mw_status s = cgemm_tc_update_batched(right, right, bw, batch, A + (J0 + bw) + (int64_t)J0 * lda, lda,
+                                                  stride, A12, lda, stride, A + (J0 + bw) + (int64_t)(J0 + bw) * lda,
                                                   lda, stride, w.tc, w.tc_bytes, w.tc_err, st, 0);
             if (s != MW_OK) return s;
         }
@@ -389,7 +419,7 @@ extern "C" mw_status mw_zgesv_mixed_batched(int32_t n, int32_t nrhs, int32_t bat
     MW_CHECK_CUDA(cudaMemsetAsync(w.tc_err, 0, sizeof(int), st));
     cf* Z32c = reinterpret_cast<cf*>(Z32);
     const int pw = panel_width > 0 ? panel_width : kBNB;
-    MW_REQUIRE(pw == 8 || pw == 16 || pw == 32, "panel_width must be 8, 16 or 32 (got %d)", pw);
+    MW_REQUIRE((pw == 8 || pw == 16 || pw == 32) && pw <= kBNBMax, "panel_width must be 8, 16 or 32 (got %d)", pw);
     mw_status s = cgetrf_batched(n, batch, Z32c, ldz32, z32_stride, ipiv, info, w, pw, st);
     if (s != MW_OK) return s;
     const int64_t per = (int64_t)n * nrhs;

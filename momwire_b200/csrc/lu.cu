@@ -1256,55 +1256,94 @@ static mw_status getrf_lookahead(int64_t n, T* A, int64_t lda, int32_t* ipiv, in
     return MW_OK;
 }
 
-// X <- U^-1 X (the back substitution of a solve).
+// One triangular sweep over the right-hand sides B with look-ahead: the
+// leaf solve of block i, then on the caller's stream only the update of the
+// next block's rows (the next leaf's input), while a second stream applies
+// block i's update to all rows beyond it, overlapping block i's small update
+// and leaf i+1 (the two streams never write the same rows at once: st's
+// small update of step i waits for the second stream's update of step i-1).
+// upper = false: X <- L^-1 X (unit lower, blocks in order); upper = true:
+// X <- U^-1 X (blocks in reverse).
 template <class T>
-static mw_status getrs_upper(int64_t n, int64_t nrhs, const T* LU, int64_t lda, T* B, int64_t ldb, const Updater& up,
-                             cudaStream_t st) {
+static mw_status trsm_sweep(bool upper, int64_t n, int64_t nrhs, const T* LU, int64_t lda, T* B, int64_t ldb,
+                            const Updater& up_main, const Updater& up_rest, cudaStream_t st) {
     constexpr int LF = GetrsLeaf<T>::value;
-    const int64_t last = ((n - 1) / LF) * LF;
-    for (int64_t j0 = last; j0 >= 0; j0 -= LF) {
-        const int jb = (int)((n - j0) < LF ? (n - j0) : LF);
-        trsm_launch<T, true, LF>(LU + j0 + j0 * lda, lda, B + j0, ldb, jb, nrhs, st);
-        if (j0 > 0) {
-            mw_status s = block_update(LU + j0 * lda, lda, B + j0, ldb, B, ldb, j0, nrhs, jb, up, st);
-            if (s != MW_OK) return s;
-        }
+    if (n <= 0 || nrhs <= 0) return MW_OK;
+    AuxStreams* ax = nullptr;
+    {
+        mw_status s0 = aux_streams(&ax);
+        if (s0 != MW_OK) return s0;
     }
+    cudaStream_t tr = ax->trail;
+    const int64_t nblk = (n + LF - 1) / LF;
+    auto blk0 = [&](int64_t b) { return b * LF; };
+    auto blk1 = [&](int64_t b) { return (b + 1) * LF < n ? (b + 1) * LF : n; };
+    // the second stream starts after everything queued on st
+    MW_CHECK_CUDA(cudaEventRecord(ax->ev_main, st));
+    MW_CHECK_CUDA(cudaStreamWaitEvent(tr, ax->ev_main, 0));
+    for (int64_t i = 0; i < nblk; ++i) {
+        const int64_t b = upper ? nblk - 1 - i : i;
+        const int64_t r0 = blk0(b), r1 = blk1(b);
+        const int jb = (int)(r1 - r0);
+        // (this leaf's rows are final: the update of block i-1 came on st,
+        // the others on the second stream before step i-1's small update)
+        if (upper) trsm_launch<T, true, LF>(LU + r0 + r0 * lda, lda, B + r0, ldb, jb, nrhs, st);
+        else trsm_launch<T, false, LF>(LU + r0 + r0 * lda, lda, B + r0, ldb, jb, nrhs, st);
+        MW_CHECK_CUDA(cudaEventRecord(ax->ev_main, st));
+        // the next block's rows are also written by block i-1's update on
+        // the second stream: it must be done before st touches them
+        if (i >= 1) MW_CHECK_CUDA(cudaStreamWaitEvent(st, ax->ev_trail[(i - 1) & 3], 0));
+        mw_status s;
+        if (!upper) {
+            if (r1 < n) {  // next block's rows, on st
+                const int64_t n1 = blk1(b + 1);
+                s = block_update(LU + r1 + r0 * lda, lda, B + r0, ldb, B + r1, ldb, n1 - r1, nrhs, jb, up_main, st);
+                if (s != MW_OK) return s;
+                if (n1 < n) {  // the rest, on the second stream
+                    MW_CHECK_CUDA(cudaStreamWaitEvent(tr, ax->ev_main, 0));
+                    s = block_update(LU + n1 + r0 * lda, lda, B + r0, ldb, B + n1, ldb, n - n1, nrhs, jb, up_rest, tr);
+                    if (s != MW_OK) return s;
+                }
+            }
+        } else {
+            if (r0 > 0) {
+                const int64_t p0 = blk0(b - 1);
+                s = block_update(LU + p0 + r0 * lda, lda, B + r0, ldb, B + p0, ldb, r0 - p0, nrhs, jb, up_main, st);
+                if (s != MW_OK) return s;
+                if (p0 > 0) {
+                    MW_CHECK_CUDA(cudaStreamWaitEvent(tr, ax->ev_main, 0));
+                    s = block_update(LU + r0 * lda, lda, B + r0, ldb, B, ldb, p0, nrhs, jb, up_rest, tr);
+                    if (s != MW_OK) return s;
+                }
+            }
+        }
+        MW_CHECK_CUDA(cudaEventRecord(ax->ev_trail[i & 3], tr));
+    }
+    MW_CHECK_CUDA(cudaEventRecord(ax->ev_main, tr));
+    MW_CHECK_CUDA(cudaStreamWaitEvent(st, ax->ev_main, 0));
     MW_CHECK_CUDA(cudaGetLastError());
     return MW_OK;
+}
+
+// X <- U^-1 X (the back substitution of a solve).
+template <class T>
+static mw_status getrs_upper(int64_t n, int64_t nrhs, const T* LU, int64_t lda, T* B, int64_t ldb,
+                             const Updater& up_main, const Updater& up, cudaStream_t st) {
+    return trsm_sweep<T>(true, n, nrhs, LU, lda, B, ldb, up_main, up, st);
 }
 
 // Solve A X = B from the factors (forward with unit L, back with U).
 template <class T>
 static mw_status getrs(int64_t n, int64_t nrhs, const T* LU, int64_t lda, const int32_t* ipiv, T* B, int64_t ldb,
-                       const Updater& up, cudaStream_t st) {
+                       const Updater& up_main, const Updater& up, cudaStream_t st) {
     {
         mw_status s0 = trsm_setup<T>();
         if (s0 != MW_OK) return s0;
     }
     laswp_launch<T>(B, ldb, 0, nrhs, ipiv, 0, n, st);
-    constexpr int LF = GetrsLeaf<T>::value;
-    for (int64_t j0 = 0; j0 < n; j0 += LF) {
-        const int jb = (int)((n - j0) < LF ? (n - j0) : LF);
-        trsm_launch<T, false, LF>(LU + j0 + j0 * lda, lda, B + j0, ldb, jb, nrhs, st);
-        const int64_t rest = n - j0 - jb;
-        if (rest > 0) {
-            mw_status s = block_update(LU + (j0 + jb) + j0 * lda, lda, B + j0, ldb, B + j0 + jb, ldb, rest, nrhs, jb,
-                                       up, st);
-            if (s != MW_OK) return s;
-        }
-    }
-    const int64_t last = ((n - 1) / LF) * LF;
-    for (int64_t j0 = last; j0 >= 0; j0 -= LF) {
-        const int jb = (int)((n - j0) < LF ? (n - j0) : LF);
-        trsm_launch<T, true, LF>(LU + j0 + j0 * lda, lda, B + j0, ldb, jb, nrhs, st);
-        if (j0 > 0) {
-            mw_status s = block_update(LU + j0 * lda, lda, B + j0, ldb, B, ldb, j0, nrhs, jb, up, st);
-            if (s != MW_OK) return s;
-        }
-    }
-    MW_CHECK_CUDA(cudaGetLastError());
-    return MW_OK;
+    mw_status s = trsm_sweep<T>(false, n, nrhs, LU, lda, B, ldb, up_main, up, st);
+    if (s != MW_OK) return s;
+    return trsm_sweep<T>(true, n, nrhs, LU, lda, B, ldb, up_main, up, st);
 }
 
 static size_t panel_ws_bytes() {
@@ -1318,9 +1357,11 @@ static size_t panel_ws_bytes() {
 static size_t cgetrf_ws_bytes(int64_t n, int64_t nrhs_max) {
     int64_t w = n > nrhs_max ? n : nrhs_max;
     // panel slots | trail-stream operand planes | status word | main-stream
-    // operand planes (updates at most kOuterNB columns wide)
+    // operand planes (k at most kOuterNB; at most kOuterNB columns wide in
+    // the factorisation, nrhs_max wide in the solves)
+    const int64_t wm = nrhs_max > kOuterNB ? nrhs_max : kOuterNB;
     return panel_ws_bytes() + 1024 + ((cgemm_tc_workspace(n, w, kOuterNB) + 255) & ~size_t(255)) + 256 +
-           cgemm_tc_workspace(n, kOuterNB, kOuterNB) + 1024;
+           cgemm_tc_workspace(n, wm, kOuterNB) + 1024;
 }
 
 static Updater tc_updater(char* ws, size_t ws_bytes, int64_t n, int64_t nrhs_max) {
@@ -1342,7 +1383,7 @@ static Updater tc_updater_main(char* ws, int64_t n, int64_t nrhs_max) {
     Updater u;
     char* base = static_cast<char*>(t.tc_ws) + ((t.tc_ws_bytes + 255) & ~size_t(255)) + 256;
     u.tc_ws = reinterpret_cast<void*>((reinterpret_cast<uintptr_t>(base) + 1023) & ~uintptr_t(1023));
-    u.tc_ws_bytes = cgemm_tc_workspace(n, kOuterNB, kOuterNB);
+    u.tc_ws_bytes = cgemm_tc_workspace(n, nrhs_max > kOuterNB ? nrhs_max : kOuterNB, kOuterNB);
     u.tc_err = t.tc_err;
     u.max_ctas = kLaPanelCtas;
     return u;
@@ -1374,8 +1415,11 @@ extern "C" mw_status mw_zgetrs(int64_t n, int64_t nrhs, const double* LUd, int64
     MW_REQUIRE(n >= 0 && nrhs >= 0 && lda >= (n > 0 ? n : 1) && ldb >= (n > 0 ? n : 1), "bad sizes");
     MW_REQUIRE(LUd && ipiv && Bd, "NULL argument");
     if (n == 0 || nrhs == 0) return MW_OK;
-    return getrs<cd>(n, nrhs, reinterpret_cast<const cd*>(LUd), lda, ipiv, reinterpret_cast<cd*>(Bd), ldb, Updater{},
-                     as_stream(stream));
+    Updater up_main, up_rest;
+    up_main.max_ctas = kLaPanelCtas;                  // leaves and next-block updates
+    up_rest.max_ctas = panel_sms<cd>() - kLaPanelCtas;  // the rest, beside them
+    return getrs<cd>(n, nrhs, reinterpret_cast<const cd*>(LUd), lda, ipiv, reinterpret_cast<cd*>(Bd), ldb, up_main,
+                     up_rest, as_stream(stream));
 }
 
 extern "C" size_t mw_cgetrf_workspace_size(int64_t n, int64_t nrhs_max) { return cgetrf_ws_bytes(n, nrhs_max); }
@@ -1430,9 +1474,12 @@ mw_status cgetrs_upper(int64_t n, int64_t nrhs, const float* LUd, int64_t lda, f
         mw_status s0 = trsm_setup<cf>();
         if (s0 != MW_OK) return s0;
     }
-    Updater up = tc_updater(static_cast<char*>(workspace), workspace_bytes, n, nrhs);
-    return getrs_upper<cf>(n, nrhs, reinterpret_cast<const cf*>(LUd), lda, reinterpret_cast<cf*>(Bd), ldb, up,
-                           as_stream(stream));
+    char* ws = static_cast<char*>(workspace);
+    Updater up = tc_updater(ws, workspace_bytes, n, nrhs);
+    Updater up_main = tc_updater_main(ws, n, nrhs);
+    up.max_ctas = panel_sms<cf>() - kLaPanelCtas;
+    return getrs_upper<cf>(n, nrhs, reinterpret_cast<const cf*>(LUd), lda, reinterpret_cast<cf*>(Bd), ldb, up_main,
+                           up, as_stream(stream));
 }
 }  // namespace mw
 
@@ -1444,7 +1491,9 @@ extern "C" mw_status mw_cgetrs(int64_t n, int64_t nrhs, const float* LUd, int64_
     if (n == 0 || nrhs == 0) return MW_OK;
     char* ws = static_cast<char*>(workspace);
     Updater up = tc_updater(ws, workspace_bytes, n, nrhs);
-    return getrs<cf>(n, nrhs, reinterpret_cast<const cf*>(LUd), lda, ipiv, reinterpret_cast<cf*>(Bd), ldb, up,
+    Updater up_main = tc_updater_main(ws, n, nrhs);
+    up.max_ctas = panel_sms<cf>() - kLaPanelCtas;  // the rest updates leave the leaves their SMs
+    return getrs<cf>(n, nrhs, reinterpret_cast<const cf*>(LUd), lda, ipiv, reinterpret_cast<cf*>(Bd), ldb, up_main, up,
                      as_stream(stream));
 }
 

@@ -1297,6 +1297,36 @@ class BSplineSolver:
             out.append(T.basis_values(knots, d, s) @ c if s.size else np.zeros(0, dtype=np.complex128))
         return out
 
+    def current_slopes(self, coeffs, s_array=None):
+        """Per-wire dI/ds, the solved current's exact arc-length derivative
+        (``bspline.py:4523-4584``), at the mesh knots or at the given arc
+        positions per wire, clipped into each wire's knot range like
+        ``currents_at_knots``.  The derivative of a degree-d B-spline sum is
+        the degree-(d-1) sum on the inner knots with coefficients
+        d (c_{j+1} - c_j) / (t_{j+d+1} - t_{j+1}); at degree 1 it is
+        piecewise constant and a knot takes its right-hand span."""
+        coeffs = np.asarray(coeffs)
+        geom, basis = self._geometry(), self._basis()
+        d = self.degree
+        out = []
+        for w in range(len(self.wires_polylines)):
+            knots = basis.knots[w]
+            if s_array is None:
+                s = np.clip(geom.wire_arc[w], knots[0], knots[-1])
+            else:
+                s = np.clip(np.asarray(s_array[w], dtype=np.float64), knots[0], knots[-1])
+            c = np.zeros(len(knots) - d - 1, dtype=np.complex128)
+            for j, _k, _jn, _e, mg in basis.kept[w]:
+                c[j] = coeffs[mg]
+            if s.size == 0:
+                out.append(np.zeros(0, dtype=np.complex128))
+                continue
+            nb = c.size
+            dt = knots[d + 1 : nb + d] - knots[1:nb]
+            cd = np.where(dt > 0, d * (c[1:] - c[:-1]) / np.where(dt > 0, dt, 1.0), 0.0)
+            out.append(T.basis_values(knots[1:-1], d - 1, s) @ cd)
+        return out
+
     def element_currents(self, coeffs, subdiv: int = 1):
         """(mid, moment, nodes, delta) per mesh element
         (reference ``_element_currents.py:33-120``)."""

@@ -102,6 +102,7 @@ def solve_case(momwire, kw, sample_seed=None, somm=False):
         out["coeffs"] = sol.coeffs
         cur = s.currents_at_knots(sol.coeffs[:, 0])
         out["currents0"] = np.concatenate(cur)
+        out["slopes0"] = np.concatenate(s.current_slopes(sol.coeffs[:, 0]))
     else:
         out["z_i"], out["z_j"], out["z_v"] = samples
         out["coeff_colsum"] = sol.coeffs.sum(axis=0)

@@ -32,6 +32,8 @@ def test_port_solution_matches_reference(name, cuda_device):
     assert rel_err(sol.coeffs, g["coeffs"]) < 1e-9
     cur = np.concatenate(s.currents_at_knots(sol.coeffs[:, 0]))
     assert rel_err(cur, g["currents0"]) < 1e-9
+    slopes = np.concatenate(s.current_slopes(sol.coeffs[:, 0]))
+    assert rel_err(slopes, g["slopes0"]) < 1e-8
 
 
 def _sampled_check(name, s):

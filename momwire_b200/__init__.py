@@ -9,6 +9,23 @@ library ``libmomwire_b200.so`` (see ``include/momwire_b200.h``).
 
 from ._port_solution import PortSolution
 from .bspline import BSplineSolver, CancelToken, SolveAborted
+from .loading import insulation_inductance, wire_internal_impedance
 
-__all__ = ["BSplineSolver", "PortSolution", "CancelToken", "SolveAborted"]
+
+def _native_loaded() -> bool:
+    """The reference's ``momwire.accelerated``: whether the native library
+    (here the sm_100a one) loads in this process."""
+    try:
+        from . import _lib
+
+        _lib.load()
+        return True
+    except (OSError, RuntimeError):
+        return False
+
+
+accelerated = _native_loaded()
+
+__all__ = ["BSplineSolver", "PortSolution", "CancelToken", "SolveAborted", "wire_internal_impedance",
+           "insulation_inductance", "accelerated"]
 __version__ = "0.1.0"

@@ -1054,9 +1054,12 @@ class BSplineSolver:
         self._fill_device(buf, st)
         return buf["Z"].cpu().numpy().T.copy()
 
-    def compute_port_solution(self) -> PortSolution:
+    def compute_port_solution(self, same_edge_prep=None) -> PortSolution:
         """Solve every port from ONE fill and ONE factorisation
-        (``bspline.py:4053-4179``)."""
+        (``bspline.py:4053-4179``).  ``same_edge_prep`` (the reference's
+        precomputed same-edge moments for sweeps) is accepted for signature
+        compatibility and unused: the device builds its same-edge table at
+        each call for a fraction of a millisecond."""
         torch = _torch()
         self._checkpoint()
         geom, basis = self._geometry(), self._basis()
@@ -1094,7 +1097,7 @@ class BSplineSolver:
         """Short-circuit admittance matrix (``bspline.py:4019``)."""
         return self.compute_port_solution().y
 
-    def compute_impedance(self):
+    def compute_impedance(self, same_edge_prep=None):
         """Drive-point impedance(s) for the configured voltages and the
         solved coefficients (``bspline.py:3919-4017``)."""
         sol = self.compute_port_solution()

@@ -236,19 +236,30 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel(PanelArgs P) {
         // applied)
         const bool apply = s_pv != 0.0;
         const T inv = apply ? cdiv(cone<T>(), s_piv[jj]) : cone<T>();
-        for (int i = i0 + tid; i < R; i += blockDim.x) {
-            const int64_t gr = r0 + i;
-            if (gr == c) {
-                if (p != c)
-                    for (int x = 0; x < jb; ++x) slab[x * rcap + i] = s_piv[x];
-                continue;
+        // the swap, one column per thread, then the scale and rank-1 update
+        // with two threads per row (the two halves of the block, alternate
+        // columns); each half reads the multiplier from the pivot column
+        if (p != c) {
+            const int lc0 = (c >= r0 && c < r1) ? (int)(c - r0) : -1;
+            const int lp0 = (p >= r0 && p < r1) ? (int)(p - r0) : -1;
+            for (int x = tid; x < jb; x += blockDim.x) {
+                if (lc0 >= 0) slab[x * rcap + lc0] = s_piv[x];
+                if (lp0 >= 0) slab[x * rcap + lp0] = s_cur[x];
             }
-            if (gr == p && p != c)
-                for (int x = 0; x < jb; ++x) slab[x * rcap + i] = s_cur[x];
-            if (!apply) continue;
-            const T l = slab[jj * rcap + i] * inv;
-            slab[jj * rcap + i] = l;
-            for (int x = jj + 1; x < jb; ++x) slab[x * rcap + i] = slab[x * rcap + i] - l * s_piv[x];
+            __syncthreads();
+        }
+        if (apply) {
+            constexpr int kHalf = kPanelThreads / 2;
+            const int par = tid / kHalf;
+            for (int i = i0 + (tid % kHalf); i < R; i += kHalf) {
+                if (r0 + i == c) continue;
+                const T l = slab[jj * rcap + i] * inv;
+                for (int x = jj + 1 + par; x < jb; x += 2) slab[x * rcap + i] = slab[x * rcap + i] - l * s_piv[x];
+            }
+            __syncthreads();
+            // the multipliers last: both halves read column jj above
+            for (int i = i0 + tid; i < R; i += blockDim.x)
+                if (r0 + i != c) slab[jj * rcap + i] = slab[jj * rcap + i] * inv;
         }
         __syncthreads();
     }
@@ -258,38 +269,71 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel(PanelArgs P) {
     }
 }
 
-// Complex64 panel with one exchange word per CTA and column.  Each CTA
-// publishes its candidate as a single 64-bit word
-//     [seq 8 | float(|re|+|im|) bits 32 | 2^24-1 - (row - j0) 24]
-// with a release store after its candidate row; every CTA's warp 0 polls
-// the G words (acquire), keeps the largest key -- largest value, then
-// smallest row, LAPACK's rule at float resolution -- and fetches that row.
-// Two dependent L2 round trips per column, no atomics.  The key's float
-// rounding can only change the choice between candidates within one float
-// ulp of each other, which the FP64 refinement of the mixed path absorbs.
-__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+// Complex64 panel with self-validating exchange records.  Every word a CTA
+// publishes carries the column it belongs to, so no fence orders the
+// publication and a reader needs no second round trip:
+//   key  : one 64-bit word per CTA [seq 8 | float(|re|+|im|) bits 32 |
+//          2^24-1 - (row - j0) 24]; largest key wins (largest value, then
+//          smallest row: LAPACK's izamax rule at float resolution);
+//   rows : the CTA's candidate row (zeros when it has none) and, from the
+//          owner of row c, row c itself, each element as two 64-bit words
+//          [tag 32 | float bits 32] with tag = c + 1.
+// Each CTA reads all G keys and all G + 1 rows in one batch of relaxed
+// loads (G <= kC64MaxGrid, so at most 33 rows of 64 elements), re-reading a
+// word until its tag matches (bounded), and takes the winner's row from
+// shared memory.  The key's float rounding can only change the choice
+// between candidates within one float ulp of each other, which the FP64
+// refinement of the mixed path absorbs.  The record area is cleared at the
+// start of a factorisation, so a word from an earlier one never matches.
+constexpr int kC64MaxGrid = 32;
+constexpr int kC64RecStride = kC64MaxGrid * kPanelMaxJb;  // 16-byte elements per buffer
+constexpr int kC64Items = ((kC64MaxGrid + 1) * kNB + kPanelThreads - 1) / kPanelThreads;
+
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p) {
     unsigned long long v;
-    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
     return v;
 }
-__device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v) {
-    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+__device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ void ld_tagged(const unsigned long long* p, unsigned long long& a, unsigned long long& b) {
+    asm volatile("ld.relaxed.gpu.global.v2.u64 {%0, %1}, [%2];" : "=l"(a), "=l"(b) : "l"(p) : "memory");
+}
+__device__ __forceinline__ void st_tagged(unsigned long long* p, cf v, unsigned int tag) {
+    const unsigned long long a = ((unsigned long long)tag << 32) | __float_as_uint(v.re);
+    const unsigned long long b = ((unsigned long long)tag << 32) | __float_as_uint(v.im);
+    asm volatile("st.relaxed.gpu.global.v2.u64 [%0], {%1, %2};" ::"l"(p), "l"(a), "l"(b) : "memory");
+}
+
+// 1 / z for the complex64 panel: z scaled by the reciprocal of its larger
+// component (so |z|^2 neither overflows nor underflows; tiny z take Smith's
+// form), then two correctly
+// rounded reciprocals instead of Smith's three divisions -- a few ulp, which
+// the FP64 refinement of the mixed path absorbs.
+__device__ __forceinline__ cf crcp_scaled(cf z) {
+    const float s = fmaxf(fabsf(z.re), fabsf(z.im));
+    if (s < 1e-30f) return cdiv(cone<cf>(), z);  // 1/s would overflow: Smith's form
+    const float rs = __frcp_rn(s);
+    const float a = z.re * rs, b = z.im * rs;
+    const float t = rs * __frcp_rn(a * a + b * b);
+    return cf{a * t, -b * t};
 }
 
 // The exchange of column jj+1 overlaps the bulk of column jj's update: once
 // column jj's pivot is known, every CTA updates column jj+1 of its rows,
 // finds its candidate for jj+1, finishes that candidate row (and, on the
 // owner, row c+1) over the remaining columns, publishes them, and only then
-// updates the rest of its rows while the other CTAs' words arrive.
+// updates the rest of its rows while the other CTAs' records arrive.
 __global__ void __launch_bounds__(kPanelThreads) panel_kernel_c64(PanelArgs P) {
     extern __shared__ __align__(16) unsigned char panel_smem[];
     cf* slab = reinterpret_cast<cf*>(panel_smem);
     __shared__ double s_v[kPanelThreads / 32];
     __shared__ int64_t s_i[kPanelThreads / 32];
-    __shared__ cf s_piv[kPanelMaxJb];
-    __shared__ cf s_cur[kPanelMaxJb];
-    __shared__ int64_t s_p;
-    __shared__ int s_zero, s_ok;
+    __shared__ cf s_rows[(kC64MaxGrid + 1) * kNB];  // G candidate rows, then row c
+    __shared__ unsigned long long s_bk;
+    __shared__ int s_bg;
+    __shared__ unsigned int s_wfb[kPanelThreads / 32], s_wrow[kPanelThreads / 32];
 
     const int G = gridDim.x;
     const int g = blockIdx.x;
@@ -302,10 +346,10 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel_c64(PanelArgs P) {
     const int rcap = P.rcap;
     const int jb = P.jb;
     cf* A = static_cast<cf*>(P.A);
-    cf* slot_row = static_cast<cf*>(P.slot_row);
-    cf* cur_row = static_cast<cf*>(P.cur_row);
+    unsigned long long* rec = static_cast<unsigned long long*>(P.slot_row);  // [2][kC64RecStride] x 2 words
     unsigned long long* words = reinterpret_cast<unsigned long long*>(P.slot_idx);  // [2][G]
     const int64_t lda = P.lda;
+    const int n_items = (G + 1) * jb;
 
     for (int idx = tid; idx < R * jb; idx += blockDim.x) {
         int i = idx % R, x = idx / R;
@@ -313,157 +357,220 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel_c64(PanelArgs P) {
     }
     __syncthreads();
 
-    // Candidate of column jj: block argmax of |re|+|im| over rows >= c (LAPACK
-    // rule at float resolution), its row and (owner) row c copied to the
-    // slots, then one release store of [seq 8 | float key 32 | 2^24-1-(row-j0)
-    // 24].  Every row written here is final in every panel column.
-    auto publish = [&](int jj) {
-        const int64_t c = P.j0 + jj;
-        const int buf = jj & 1;
-        const unsigned long long seq = (unsigned long long)((c + 1) % 255 + 1);
-        const int i0 = (int)max((int64_t)0, c - r0);
-        double best = -1.0;
-        int64_t bidx = INT64_MAX;
-        for (int i = i0 + tid; i < R; i += blockDim.x) argmax_merge(best, bidx, cabs1(slab[jj * rcap + i]), r0 + i);
-        block_argmax(best, bidx, s_v, s_i);
-        if (bidx != INT64_MAX)
-            for (int x = tid; x < jb; x += blockDim.x)
-                slot_row[((size_t)buf * G + g) * kPanelMaxJb + x] = slab[x * rcap + (int)(bidx - r0)];
-        if (c >= r0 && c < r1)
-            for (int x = tid; x < jb; x += blockDim.x) cur_row[buf * kPanelMaxJb + x] = slab[x * rcap + (int)(c - r0)];
-        __syncthreads();
-        if (tid == 0) {
-            unsigned long long key = 0;  // no candidate: loses to every row
-            if (bidx != INT64_MAX) {
-                const unsigned int fb = __float_as_uint((float)best);
-                key = ((unsigned long long)fb << 24) | (unsigned long long)(0xFFFFFFll - (bidx - P.j0));
-            }
-            st_release_u64(words + (size_t)buf * G + g, (seq << 56) | key);
+    // Publish the records of column cc (candidate local row lb or -1 with
+    // value best, local row lc of cc or -1).  Thread x writes element x of
+    // the candidate row, thread jb + x element x of row cc, the last thread
+    // the key; a caller that finishes rows lb / lc first keeps the same
+    // thread-to-column mapping, so no barrier is needed in between.
+    auto publish = [&](int64_t cc, int lb, int lc, double best) {
+        const int nbuf = (int)((cc - P.j0) & 1);
+        const unsigned int tag = (unsigned int)(cc + 1);
+        unsigned long long* rb = rec + (size_t)nbuf * kC64RecStride * 2;
+        if (tid < jb) {
+            const cf v = lb >= 0 ? slab[tid * rcap + lb] : cf{0.0f, 0.0f};
+            st_tagged(rb + (size_t)(g * jb + tid) * 2, v, tag);
+        } else if (tid < 2 * jb) {
+            if (lc >= 0) st_tagged(rb + (size_t)(G * jb + (tid - jb)) * 2, slab[(tid - jb) * rcap + lc], tag);
         }
-        return bidx;
+        if (tid == kPanelThreads - 1) {
+            const unsigned long long seq = (unsigned long long)((cc + 1) % 255 + 1);
+            unsigned long long key = 0;  // no candidate: loses to every row
+            if (lb >= 0) {
+                const unsigned int fb = __float_as_uint((float)best);
+                key = ((unsigned long long)fb << 24) | (unsigned long long)(0xFFFFFFll - (r0 + lb - P.j0));
+            }
+            st_relaxed_u64(words + (size_t)nbuf * G + g, (seq << 56) | key);
+        }
     };
 
-    publish(0);
+    {
+        double best = -1.0;
+        int64_t bidx = INT64_MAX;
+        for (int i = tid; i < R; i += blockDim.x) argmax_merge(best, bidx, cabs1(slab[i]), r0 + i);
+        block_argmax(best, bidx, s_v, s_i);
+        publish(P.j0, bidx != INT64_MAX ? (int)(bidx - r0) : -1, (P.j0 >= r0 && P.j0 < r1) ? (int)(P.j0 - r0) : -1,
+                best);
+    }
     for (int jj = 0; jj < jb; ++jj) {
         const int64_t c = P.j0 + jj;
         const int buf = jj & 1;
+        const unsigned int tag = (unsigned int)(c + 1);
         // 1..255, never the 0 the slots are cleared to; a stale word in a
-        // slot is at most jb + 2 columns old, so it never matches
+        // slot is at most 2 * kNB + 2 columns old, so it never matches
         const unsigned long long seq = (unsigned long long)((c + 1) % 255 + 1);
-        if (tid < 32) {
-            unsigned long long bk = 0;
-            int bg = 0, ok = 1;
-            for (int x = tid; x < G; x += 32) {
-                unsigned long long w;
-                long long spins = 0;
-                while (((w = ld_acquire_u64(words + (size_t)buf * G + x)) >> 56) != seq) {
-                    if ((++spins & 1023) == 0 && (spins > (1ll << 26) || *(volatile int*)&P.ws->err)) {
-                        atomicExch(&P.ws->err, MW_ERR_TIMEOUT);
-                        ok = 0;
-                        break;
-                    }
-                }
-                if (!ok) break;
-                const unsigned long long key = w & 0x00FFFFFFFFFFFFFFull;
-                if (key > bk) {
-                    bk = key;
-                    bg = x;
-                }
-            }
-            ok = __all_sync(0xffffffffu, ok);
+        const unsigned long long* rb = rec + (size_t)buf * kC64RecStride * 2;
+        // every load of the column in flight at once, then the re-reads
+        unsigned long long wa[kC64Items], wb[kC64Items];
 #pragma unroll
-            for (int off = 16; off > 0; off >>= 1) {
-                const unsigned long long k2 = __shfl_xor_sync(0xffffffffu, bk, off);
-                const int g2 = __shfl_xor_sync(0xffffffffu, bg, off);
-                if (k2 > bk || (k2 == bk && g2 < bg)) {
-                    bk = k2;
-                    bg = g2;
-                }
-            }
-            const int64_t p = P.j0 + (0xFFFFFFll - (int64_t)(bk & 0xFFFFFFull));
-            if (tid == 0) {
-                s_ok = ok;
-                s_p = p;
-                s_zero = ((bk >> 24) & 0xFFFFFFFFull) == 0ull;  // |pivot| == 0
-                if (g == 0 && ok) P.ipiv[c] = (int32_t)(p + 1);
-            }
-            if (ok)
-                for (int x = tid; x < jb; x += 32) {
-                    s_piv[x] = ldcg_c(slot_row + ((size_t)buf * G + bg) * kPanelMaxJb + x);
-                    s_cur[x] = ldcg_c(cur_row + buf * kPanelMaxJb + x);
-                }
+        for (int k = 0; k < kC64Items; ++k) {
+            const int idx = tid + k * kPanelThreads;
+            if (idx < n_items) ld_tagged(rb + (size_t)idx * 2, wa[k], wb[k]);
         }
-        __syncthreads();
-        if (!s_ok) return;  // a wait gave up: the error word is set
-        const int64_t p = s_p;
-        if (s_zero && g == 0 && tid == 0 && P.info[0] == 0) P.info[0] = (int32_t)(c + 1);
+        unsigned long long kw = 0;
+        if (tid < G) kw = ld_relaxed_u64(words + (size_t)buf * G + tid);
+        int ok = 1;
+        long long spins = 0;
+        auto give_up = [&]() {
+            if ((++spins & 1023) == 0 && (spins > (1ll << 24) || *(volatile int*)&P.ws->err)) {
+                atomicExch(&P.ws->err, MW_ERR_TIMEOUT);
+                ok = 0;
+            }
+            return !ok;
+        };
+#pragma unroll
+        for (int k = 0; k < kC64Items; ++k) {
+            const int idx = tid + k * kPanelThreads;
+            if (idx < n_items && ok) {
+                while ((unsigned int)(wa[k] >> 32) != tag || (unsigned int)(wb[k] >> 32) != tag) {
+                    if (give_up()) break;
+                    ld_tagged(rb + (size_t)idx * 2, wa[k], wb[k]);
+                }
+                s_rows[idx] = cf{__uint_as_float((unsigned int)wa[k]), __uint_as_float((unsigned int)wb[k])};
+            }
+        }
+        if (tid < G && ok)
+            while ((kw >> 56) != seq) {
+                if (give_up()) break;
+                kw = ld_relaxed_u64(words + (size_t)buf * G + tid);
+            }
+        if (tid < 32) {
+            // largest key: largest value bits, then largest inverted row;
+            // the lowest lane on (impossible) full ties
+            const unsigned long long key = tid < G ? (kw & 0x00FFFFFFFFFFFFFFull) : 0ull;
+            const unsigned int fb = (unsigned int)(key >> 24), lo = (unsigned int)(key & 0xFFFFFFull);
+            const unsigned int mfb = __reduce_max_sync(0xffffffffu, fb);
+            const unsigned int mlo = __reduce_max_sync(0xffffffffu, fb == mfb ? lo : 0u);
+            const unsigned int win = __ballot_sync(0xffffffffu, fb == mfb && lo == mlo);
+            if (tid == 0) {
+                s_bk = ((unsigned long long)mfb << 24) | mlo;
+                s_bg = __ffs(win) - 1;
+            }
+        }
+        if (!__syncthreads_and(ok)) return;  // a wait gave up: the error word is set
+        const unsigned long long bk = s_bk;
+        const cf* s_piv = s_rows + s_bg * jb;
+        const cf* s_cur = s_rows + G * jb;
+        const int64_t p = P.j0 + (0xFFFFFFll - (int64_t)(bk & 0xFFFFFFull));
+        const bool zero = ((bk >> 24) & 0xFFFFFFFFull) == 0ull;  // |pivot| == 0
         // LAPACK: an exact zero pivot is neither divided by nor applied
-        const bool apply = !s_zero;
-        const cf inv = apply ? cdiv(cone<cf>(), s_piv[jj]) : cone<cf>();
+        const bool apply = !zero;
+        const cf inv = apply ? crcp_scaled(s_piv[jj]) : cone<cf>();
         const int i0 = (int)max((int64_t)0, c - r0);
         const bool last = jj + 1 >= jb;
-        // 1. swap rows c and p, scale column jj below c, update column jj+1
+        // 1. swap rows c and p (one column per thread; row p's columns jj
+        // and jj+1 belong to its row thread below), scale column jj below c,
+        // update column jj+1
+        if (p != c) {
+            const int lc0 = (c >= r0 && c < r1) ? (int)(c - r0) : -1;
+            const int lp0 = (p >= r0 && p < r1) ? (int)(p - r0) : -1;
+            for (int x = tid; x < jb; x += blockDim.x) {
+                if (lc0 >= 0) slab[x * rcap + lc0] = s_piv[x];
+                if (lp0 >= 0 && x != jj && x != jj + 1) slab[x * rcap + lp0] = s_cur[x];
+            }
+        }
+        // the candidate of column jj+1 among this thread's rows (all > c):
+        // largest float |re|+|im| (LAPACK's scabs1), then smallest row
+        unsigned int bfb = 0u, brow = 0xFFFFFFFFu;
         for (int i = i0 + tid; i < R; i += blockDim.x) {
             const int64_t gr = r0 + i;
-            if (gr == c) {
-                if (p != c)
-                    for (int x = 0; x < jb; ++x) slab[x * rcap + i] = s_piv[x];
-                continue;
+            if (gr == c) continue;
+            const bool swapped = gr == p && p != c;
+            // both loads ahead of the stores
+            const cf a0 = swapped ? s_cur[jj] : slab[jj * rcap + i];
+            const cf a1 = last ? cf{0.0f, 0.0f} : (swapped ? s_cur[jj + 1] : slab[(jj + 1) * rcap + i]);
+            cf n1 = a1;
+            if (!apply) {
+                if (swapped) {
+                    slab[jj * rcap + i] = a0;
+                    if (!last) slab[(jj + 1) * rcap + i] = a1;
+                }
+            } else {
+                const cf l = a0 * inv;
+                slab[jj * rcap + i] = l;
+                if (!last) {
+                    n1 = a1 - l * s_piv[jj + 1];
+                    slab[(jj + 1) * rcap + i] = n1;
+                }
             }
-            if (gr == p && p != c)
-                for (int x = 0; x < jb; ++x) slab[x * rcap + i] = s_cur[x];
-            if (!apply) continue;
-            const cf l = slab[jj * rcap + i] * inv;
-            slab[jj * rcap + i] = l;
-            if (!last) slab[(jj + 1) * rcap + i] = slab[(jj + 1) * rcap + i] - l * s_piv[jj + 1];
+            const unsigned int fb = __float_as_uint(fabsf(n1.re) + fabsf(n1.im));
+            if (fb > bfb || brow == 0xFFFFFFFFu) {  // rows ascend: ties keep the first
+                bfb = fb;
+                brow = (unsigned int)i;
+            }
+        }
+        {
+            const unsigned int mfb = __reduce_max_sync(0xffffffffu, brow == 0xFFFFFFFFu ? 0u : bfb);
+            const unsigned int mrow =
+                __reduce_min_sync(0xffffffffu, (brow != 0xFFFFFFFFu && bfb == mfb) ? brow : 0xFFFFFFFFu);
+            if ((tid & 31) == 0) {
+                s_wfb[tid >> 5] = mfb;
+                s_wrow[tid >> 5] = mrow;
+            }
         }
         __syncthreads();
-        if (last) break;
-        // 2. the candidate row for column jj+1 and row c+1, finished over the
-        // remaining columns, then published
-        const int64_t cn = c + 1;
-        double best = -1.0;
-        int64_t bidx = INT64_MAX;
-        {
-            const int j1 = (int)max((int64_t)0, cn - r0);
-            for (int i = j1 + tid; i < R; i += blockDim.x)
-                argmax_merge(best, bidx, cabs1(slab[(jj + 1) * rcap + i]), r0 + i);
-            block_argmax(best, bidx, s_v, s_i);
+        if (last) {
+            if (g == 0 && tid == 0) {
+                P.ipiv[c] = (int32_t)(p + 1);
+                if (zero && P.info[0] == 0) P.info[0] = (int32_t)(c + 1);
+            }
+            break;
         }
+        // 2. the candidate row for column jj+1 and row c+1, finished over the
+        // remaining columns by the threads that publish them
+        const int64_t cn = c + 1;
+        unsigned int cfb, crow;
+        {
+            // every warp combines the eight warp results itself
+            const int ln = tid & 31;
+            const unsigned int f = ln < kPanelThreads / 32 ? s_wfb[ln] : 0u;
+            const unsigned int r = ln < kPanelThreads / 32 ? s_wrow[ln] : 0xFFFFFFFFu;
+            cfb = __reduce_max_sync(0xffffffffu, r != 0xFFFFFFFFu ? f : 0u);
+            crow = __reduce_min_sync(0xffffffffu, (r != 0xFFFFFFFFu && f == cfb) ? r : 0xFFFFFFFFu);
+        }
+        const double best = (double)__uint_as_float(cfb);
+        const int64_t bidx = crow != 0xFFFFFFFFu ? r0 + crow : INT64_MAX;
         const int lb = bidx != INT64_MAX ? (int)(bidx - r0) : -1;
         const int lc = (cn >= r0 && cn < r1) ? (int)(cn - r0) : -1;
-        if (apply)
-            for (int x = jj + 2 + tid; x < jb; x += blockDim.x) {
-                if (lb >= 0) slab[x * rcap + lb] = slab[x * rcap + lb] - slab[jj * rcap + lb] * s_piv[x];
-                if (lc >= 0 && lc != lb) slab[x * rcap + lc] = slab[x * rcap + lc] - slab[jj * rcap + lc] * s_piv[x];
-            }
-        __syncthreads();
-        {
-            const int nbuf = (jj + 1) & 1;
-            const unsigned long long nseq = (unsigned long long)((cn + 1) % 255 + 1);
-            if (lb >= 0)
-                for (int x = tid; x < jb; x += blockDim.x)
-                    slot_row[((size_t)nbuf * G + g) * kPanelMaxJb + x] = slab[x * rcap + lb];
-            if (lc >= 0)
-                for (int x = tid; x < jb; x += blockDim.x) cur_row[nbuf * kPanelMaxJb + x] = slab[x * rcap + lc];
-            __syncthreads();
-            if (tid == 0) {
-                unsigned long long key = 0;
-                if (bidx != INT64_MAX) {
-                    const unsigned int fb = __float_as_uint((float)best);
-                    key = ((unsigned long long)fb << 24) | (unsigned long long)(0xFFFFFFll - (bidx - P.j0));
-                }
-                st_release_u64(words + (size_t)nbuf * G + g, (nseq << 56) | key);
+        if (apply) {
+            if (tid < jb) {
+                if (lb >= 0 && tid >= jj + 2) slab[tid * rcap + lb] = slab[tid * rcap + lb] - slab[jj * rcap + lb] * s_piv[tid];
+            } else if (tid < 2 * jb) {
+                const int x = tid - jb;
+                if (lc >= 0 && lc != lb && x >= jj + 2)
+                    slab[x * rcap + lc] = slab[x * rcap + lc] - slab[jj * rcap + lc] * s_piv[x];
             }
         }
-        // 3. the rest of column jj's update while the other CTAs publish
-        if (apply)
-            for (int i = i0 + tid; i < R; i += blockDim.x) {
+        // (row lc == lb: the candidate's thread finished it; its row-c
+        // element is read by thread jb + x after the barrier in phase 3)
+        if (lc >= 0 && lc == lb) __syncthreads();
+        publish(cn, lb, lc, best);
+        if (g == 0 && tid == 0) {
+            P.ipiv[c] = (int32_t)(p + 1);
+            if (zero && P.info[0] == 0) P.info[0] = (int32_t)(c + 1);
+        }
+        // 3. the rest of column jj's update while the other CTAs publish:
+        // two threads per row (the two halves of the block), alternate columns
+        if (apply) {
+            constexpr int kHalf = kPanelThreads / 2;
+            const int par = tid / kHalf;
+            for (int i = i0 + (tid % kHalf); i < R; i += kHalf) {
                 const int64_t gr = r0 + i;
                 if (gr <= c || i == lb || i == lc) continue;
                 const cf l = slab[jj * rcap + i];
-                for (int x = jj + 2; x < jb; ++x) slab[x * rcap + i] = slab[x * rcap + i] - l * s_piv[x];
+                int x = jj + 2 + par;
+                // four columns' loads ahead of their stores
+                for (; x + 6 < jb; x += 8) {
+                    const cf a0 = slab[x * rcap + i], a1 = slab[(x + 2) * rcap + i];
+                    const cf a2 = slab[(x + 4) * rcap + i], a3 = slab[(x + 6) * rcap + i];
+                    const cf p0 = s_piv[x], p1 = s_piv[x + 2], p2 = s_piv[x + 4], p3 = s_piv[x + 6];
+                    slab[x * rcap + i] = a0 - l * p0;
+                    slab[(x + 2) * rcap + i] = a1 - l * p1;
+                    slab[(x + 4) * rcap + i] = a2 - l * p2;
+                    slab[(x + 6) * rcap + i] = a3 - l * p3;
+                }
+                for (; x < jb; x += 2) slab[x * rcap + i] = slab[x * rcap + i] - l * s_piv[x];
             }
+        }
         __syncthreads();
     }
     for (int idx = tid; idx < R * jb; idx += blockDim.x) {
@@ -1032,6 +1139,8 @@ static mw_status panel_factor(T* A, int64_t lda, int64_t n, int64_t j0, int jb, 
     int G = (int)(want < sms ? want : sms);
     if (grid_cap > 0 && G > grid_cap) G = grid_cap;
     if (G > kMaxPanelGrid) G = kMaxPanelGrid;
+    // the complex64 kernel reads every CTA's candidate row each column
+    if (std::is_same<T, cf>::value && G > kC64MaxGrid) G = kC64MaxGrid;
     if (G < 1) G = 1;
     const int64_t per = (m + G - 1) / G;
     const size_t smem = (size_t)per * jb * sizeof(T);
@@ -1094,6 +1203,9 @@ static mw_status getrf(int64_t n, T* A, int64_t lda, int32_t* ipiv, int32_t* inf
         size_t ov, oi, orow, ocur;
         ws_layout(kMaxPanelGrid, &ov, &oi, &orow, &ocur);
         MW_CHECK_CUDA(cudaMemsetAsync(ws + oi, 0, sizeof(int64_t) * 2 * kMaxPanelGrid, st));
+        // and the complex64 panel's tagged records (no tag from an earlier
+        // factorisation may match)
+        MW_CHECK_CUDA(cudaMemsetAsync(ws + orow, 0, sizeof(unsigned long long) * 2 * 2 * kC64RecStride, st));
     }
     {
         mw_status s0 = trsm_setup<T>();
@@ -1175,6 +1287,9 @@ static mw_status getrf_lookahead(int64_t n, T* A, int64_t lda, int32_t* ipiv, in
         size_t ov, oi, orow, ocur;
         ws_layout(kMaxPanelGrid, &ov, &oi, &orow, &ocur);
         MW_CHECK_CUDA(cudaMemsetAsync(ws + oi, 0, sizeof(int64_t) * 2 * kMaxPanelGrid, st));
+        // and the complex64 panel's tagged records (no tag from an earlier
+        // factorisation may match)
+        MW_CHECK_CUDA(cudaMemsetAsync(ws + orow, 0, sizeof(unsigned long long) * 2 * 2 * kC64RecStride, st));
     }
     {
         mw_status s0 = trsm_setup<T>();

@@ -330,7 +330,9 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel_c64(PanelArgs P) {
     cf* slab = reinterpret_cast<cf*>(panel_smem);
     __shared__ double s_v[kPanelThreads / 32];
     __shared__ int64_t s_i[kPanelThreads / 32];
-    __shared__ cf s_rows[(kC64MaxGrid + 1) * kNB];  // G candidate rows, then row c
+    // per column parity: G candidate rows, then row c (two buffers, so the
+    // next column's records land while the bulk update still reads these)
+    __shared__ cf s_rows[2][(kC64MaxGrid + 1) * kNB];
     __shared__ unsigned long long s_bk;
     __shared__ int s_bg;
     __shared__ unsigned int s_wfb[kPanelThreads / 32], s_wrow[kPanelThreads / 32];
@@ -425,7 +427,7 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel_c64(PanelArgs P) {
                     if (give_up()) break;
                     ld_tagged(rb + (size_t)idx * 2, wa[k], wb[k]);
                 }
-                s_rows[idx] = cf{__uint_as_float((unsigned int)wa[k]), __uint_as_float((unsigned int)wb[k])};
+                s_rows[buf][idx] = cf{__uint_as_float((unsigned int)wa[k]), __uint_as_float((unsigned int)wb[k])};
             }
         }
         if (tid < G && ok)
@@ -446,10 +448,11 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel_c64(PanelArgs P) {
                 s_bg = __ffs(win) - 1;
             }
         }
+        // (this barrier also ends the previous column's bulk update)
         if (!__syncthreads_and(ok)) return;  // a wait gave up: the error word is set
         const unsigned long long bk = s_bk;
-        const cf* s_piv = s_rows + s_bg * jb;
-        const cf* s_cur = s_rows + G * jb;
+        const cf* s_piv = s_rows[buf] + s_bg * jb;
+        const cf* s_cur = s_rows[buf] + G * jb;
         const int64_t p = P.j0 + (0xFFFFFFll - (int64_t)(bk & 0xFFFFFFull));
         const bool zero = ((bk >> 24) & 0xFFFFFFFFull) == 0ull;  // |pivot| == 0
         // LAPACK: an exact zero pivot is neither divided by nor applied
@@ -571,7 +574,6 @@ __global__ void __launch_bounds__(kPanelThreads) panel_kernel_c64(PanelArgs P) {
                 for (; x < jb; x += 2) slab[x * rcap + i] = slab[x * rcap + i] - l * s_piv[x];
             }
         }
-        __syncthreads();
     }
     for (int idx = tid; idx < R * jb; idx += blockDim.x) {
         int i = idx % R, x = idx / R;
@@ -624,74 +626,105 @@ constexpr int kTrsmWarps = 8;
 template <class T, bool UPPER, int L>
 __global__ void __launch_bounds__(32 * kTrsmWarps) trsm_kernel(const T* Tm, int64_t ldt, T* X, int64_t ldx, int jb,
                                                                int64_t ncols) {
-    constexpr int R = L / 32;
+    // Lane l owns rows RP*l .. RP*l+RP-1 of the block, so a RP x RP diagonal
+    // block is solved inside one lane; its RP results reach the other lanes
+    // in RP independent shuffles and every lane applies the RP x RP update:
+    // 32 short dependent chains instead of L long ones.  The triangle is
+    // staged as S[block kb][a*RP + b][lane] = T(RP*lane + a, RP*kb + b), so
+    // a lane's loads are consecutive across the warp (no bank conflicts).
+    // Accumulation order per row is the substitution order (columns
+    // ascending for L, descending for U).
+    constexpr int RP = L / 32;
+    static_assert(RP * 32 == L, "leaf order must be a multiple of 32");
     extern __shared__ __align__(16) unsigned char trsm_smem[];
-    T(*sT)[L + 1] = reinterpret_cast<T(*)[L + 1]>(trsm_smem);
-    T* sD = reinterpret_cast<T*>(trsm_smem) + L * (L + 1);  // U: reciprocals of the diagonal
+    T* S = reinterpret_cast<T*>(trsm_smem);
+    T* sD = S + L * L;  // U: reciprocals of the diagonal (zero beyond jb)
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (UPPER && tid < jb) sD[tid] = cdiv(cone<T>(), Tm[tid + (int64_t)tid * ldt]);
-    // stage the triangle the solve reads (strictly lower for L, upper with
-    // the diagonal for U), eight loads in flight per thread before the
-    // shared-memory stores
+    const T zero{};
+    if (UPPER && tid < L) sD[tid] = tid < jb ? cdiv(cone<T>(), Tm[tid + (int64_t)tid * ldt]) : zero;
+    // the strict triangle the solve reads, zero elsewhere; eight loads in
+    // flight per thread before the shared-memory stores
     constexpr int kU = 8;
-    const int tot = jb * jb;
-    for (int base = 0; base < tot; base += kU * (int)blockDim.x) {
+    for (int base = 0; base < L * L; base += kU * (int)blockDim.x) {
         T v[kU];
-        bool need[kU];
 #pragma unroll
         for (int u = 0; u < kU; ++u) {
             const int i = base + u * (int)blockDim.x + tid;
-            const int r = i % jb, cc = i / jb;
-            need[u] = i < tot && (UPPER ? r <= cc : r > cc);
-            if (need[u]) v[u] = Tm[r + (int64_t)cc * ldt];
+            const int r = i % L, c = i / L;
+            const bool need = i < L * L && r < jb && c < jb && (UPPER ? r < c : r > c);
+            v[u] = need ? Tm[r + (int64_t)c * ldt] : zero;
         }
 #pragma unroll
         for (int u = 0; u < kU; ++u) {
             const int i = base + u * (int)blockDim.x + tid;
-            if (need[u]) sT[i % jb][i / jb] = v[u];
+            if (i < L * L) {
+                const int r = i % L, c = i / L;
+                S[((c / RP) * RP * RP + (r % RP) * RP + (c % RP)) * 32 + r / RP] = v[u];
+            }
         }
     }
     __syncthreads();
     const int64_t col = (int64_t)blockIdx.x * kTrsmWarps + warp;
     if (col >= ncols) return;  // whole warp leaves together
     T* x = X + col * ldx;
-    const T zero{};
-    T v[R];
+    T v[RP];
 #pragma unroll
-    for (int i = 0; i < R; ++i) v[i] = lane + 32 * i < jb ? x[lane + 32 * i] : zero;
+    for (int a = 0; a < RP; ++a) v[a] = RP * lane + a < jb ? x[RP * lane + a] : zero;
+    const int nkb = (jb + RP - 1) / RP;
     if (!UPPER) {
-        for (int k = 0; k < jb; ++k) {
-            T src = v[0];
+        for (int kb = 0; kb < nkb; ++kb) {
+            const T* Sk = S + kb * RP * RP * 32 + lane;
+            T xb[RP];
 #pragma unroll
-            for (int i = 1; i < R; ++i)
-                if ((k >> 5) == i) src = v[i];
-            const T xk = shfl_c(src, k & 31);
+            for (int b = 0; b < RP; ++b) xb[b] = zero;
+            if (lane == kb) {
 #pragma unroll
-            for (int i = 0; i < R; ++i) {
-                const int row = lane + 32 * i;
-                if (row > k && row < jb) v[i] = v[i] - sT[row][k] * xk;
+                for (int a = 0; a < RP; ++a) {
+                    T t = v[a];
+#pragma unroll
+                    for (int b = 0; b < a; ++b) t = t - Sk[(a * RP + b) * 32] * xb[b];
+                    xb[a] = t;
+                    v[a] = t;
+                }
+            }
+#pragma unroll
+            for (int b = 0; b < RP; ++b) xb[b] = shfl_c(xb[b], kb);
+            if (lane > kb) {
+#pragma unroll
+                for (int a = 0; a < RP; ++a)
+#pragma unroll
+                    for (int b = 0; b < RP; ++b) v[a] = v[a] - Sk[(a * RP + b) * 32] * xb[b];
             }
         }
     } else {
-        for (int k = jb - 1; k >= 0; --k) {
+        for (int kb = nkb - 1; kb >= 0; --kb) {
+            const T* Sk = S + kb * RP * RP * 32 + lane;
+            T xb[RP];
 #pragma unroll
-            for (int i = 0; i < R; ++i)
-                if ((k >> 5) == i && lane == (k & 31)) v[i] = v[i] * sD[k];
-            T src = v[0];
+            for (int b = 0; b < RP; ++b) xb[b] = zero;
+            if (lane == kb) {
 #pragma unroll
-            for (int i = 1; i < R; ++i)
-                if ((k >> 5) == i) src = v[i];
-            const T xk = shfl_c(src, k & 31);
+                for (int a = RP - 1; a >= 0; --a) {
+                    T t = v[a];
 #pragma unroll
-            for (int i = 0; i < R; ++i) {
-                const int row = lane + 32 * i;
-                if (row < k) v[i] = v[i] - sT[row][k] * xk;
+                    for (int b = RP - 1; b > a; --b) t = t - Sk[(a * RP + b) * 32] * xb[b];
+                    xb[a] = t * sD[RP * lane + a];
+                    v[a] = xb[a];
+                }
+            }
+#pragma unroll
+            for (int b = 0; b < RP; ++b) xb[b] = shfl_c(xb[b], kb);
+            if (lane < kb) {
+#pragma unroll
+                for (int a = 0; a < RP; ++a)
+#pragma unroll
+                    for (int b = RP - 1; b >= 0; --b) v[a] = v[a] - Sk[(a * RP + b) * 32] * xb[b];
             }
         }
     }
 #pragma unroll
-    for (int i = 0; i < R; ++i)
-        if (lane + 32 * i < jb) x[lane + 32 * i] = v[i];
+    for (int a = 0; a < RP; ++a)
+        if (RP * lane + a < jb) x[RP * lane + a] = v[a];
 }
 
 template <class T, int L>
@@ -1053,7 +1086,7 @@ mw_status zgemm_launch_simt(bool ta, bool tb, int64_t m, int64_t n, int64_t k, c
 }
 
 // --------------------------------------------------------------- driver
-constexpr size_t kPanelSmemMax = 200 * 1024;  // slab bytes per CTA
+constexpr size_t kPanelSmemMax = 192 * 1024;  // slab bytes per CTA (beside 34 KB of static buffers)
 
 template <class T>
 static int panel_sms() {

@@ -625,7 +625,8 @@ struct GetrsLeaf<cf> {
 constexpr int kTrsmWarps = 8;
 template <class T, bool UPPER, int L>
 __global__ void __launch_bounds__(32 * kTrsmWarps) trsm_kernel(const T* Tm, int64_t ldt, T* X, int64_t ldx, int jb,
-                                                               int64_t ncols) {
+                                                               int64_t ncols, const T* Aoff, int64_t ldo, const T* Xp,
+                                                               int K) {
     // Lane l owns rows RP*l .. RP*l+RP-1 of the block, so a RP x RP diagonal
     // block is solved inside one lane; its RP results reach the other lanes
     // in RP independent shuffles and every lane applies the RP x RP update:
@@ -634,6 +635,10 @@ __global__ void __launch_bounds__(32 * kTrsmWarps) trsm_kernel(const T* Tm, int6
     // a lane's loads are consecutive across the warp (no bank conflicts).
     // Accumulation order per row is the substitution order (columns
     // ascending for L, descending for U).
+    // With K > 0 the leaf first applies the block solved before it,
+    // X -= Aoff (jb x K) * Xp (K rows of the same columns), staged in the
+    // same lane-major form -- the next-block update of a blocked sweep, done
+    // where its result is consumed.
     constexpr int RP = L / 32;
     static_assert(RP * 32 == L, "leaf order must be a multiple of 32");
     extern __shared__ __align__(16) unsigned char trsm_smem[];
@@ -642,34 +647,63 @@ __global__ void __launch_bounds__(32 * kTrsmWarps) trsm_kernel(const T* Tm, int6
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const T zero{};
     if (UPPER && tid < L) sD[tid] = tid < jb ? cdiv(cone<T>(), Tm[tid + (int64_t)tid * ldt]) : zero;
-    // the strict triangle the solve reads, zero elsewhere; eight loads in
-    // flight per thread before the shared-memory stores
-    constexpr int kU = 8;
-    for (int base = 0; base < L * L; base += kU * (int)blockDim.x) {
-        T v[kU];
+    // Stage rows < nr, columns < nc of M (leading dimension ld) into S
+    // lane-major -- all of it (part 0), the strict upper (1) or strict lower
+    // (-1) triangle -- zero elsewhere; sixteen loads in flight per thread
+    // before the shared-memory stores.
+    auto stage = [&](const T* M, int64_t ld, int nr, int nc, int part) {
+        constexpr int kU = 16;
+        for (int base = 0; base < L * L; base += kU * (int)blockDim.x) {
+            T t[kU];
 #pragma unroll
-        for (int u = 0; u < kU; ++u) {
-            const int i = base + u * (int)blockDim.x + tid;
-            const int r = i % L, c = i / L;
-            const bool need = i < L * L && r < jb && c < jb && (UPPER ? r < c : r > c);
-            v[u] = need ? Tm[r + (int64_t)c * ldt] : zero;
-        }
-#pragma unroll
-        for (int u = 0; u < kU; ++u) {
-            const int i = base + u * (int)blockDim.x + tid;
-            if (i < L * L) {
+            for (int u = 0; u < kU; ++u) {
+                const int i = base + u * (int)blockDim.x + tid;
                 const int r = i % L, c = i / L;
-                S[((c / RP) * RP * RP + (r % RP) * RP + (c % RP)) * 32 + r / RP] = v[u];
+                const bool need = i < L * L && r < nr && c < nc && (part == 0 || (part > 0 ? r < c : r > c));
+                t[u] = need ? M[r + (int64_t)c * ld] : zero;
+            }
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const int i = base + u * (int)blockDim.x + tid;
+                if (i < L * L) {
+                    const int r = i % L, c = i / L;
+                    S[((c / RP) * RP * RP + (r % RP) * RP + (c % RP)) * 32 + r / RP] = t[u];
+                }
             }
         }
-    }
-    __syncthreads();
+    };
     const int64_t col = (int64_t)blockIdx.x * kTrsmWarps + warp;
-    if (col >= ncols) return;  // whole warp leaves together
-    T* x = X + col * ldx;
+    const bool active = col < ncols;  // (a whole warp; it stays for the barriers)
+    T* x = X + (active ? col : 0) * ldx;
     T v[RP];
 #pragma unroll
-    for (int a = 0; a < RP; ++a) v[a] = RP * lane + a < jb ? x[RP * lane + a] : zero;
+    for (int a = 0; a < RP; ++a) v[a] = active && RP * lane + a < jb ? x[RP * lane + a] : zero;
+    if (K > 0) {
+        stage(Aoff, ldo, jb, K, 0);
+        __syncthreads();
+        if (active) {
+            const T* xq = Xp + col * ldx;
+            T xp[RP];
+#pragma unroll
+            for (int a = 0; a < RP; ++a) xp[a] = RP * lane + a < K ? xq[RP * lane + a] : zero;
+            const int nkq = (K + RP - 1) / RP;
+            for (int kb = 0; kb < nkq; ++kb) {
+                const T* Sk = S + kb * RP * RP * 32 + lane;
+                T xb[RP];
+#pragma unroll
+                for (int b = 0; b < RP; ++b) xb[b] = shfl_c(xp[b], kb);
+#pragma unroll
+                for (int a = 0; a < RP; ++a)
+#pragma unroll
+                    for (int b = 0; b < RP; ++b) v[a] = v[a] - Sk[(a * RP + b) * 32] * xb[b];
+            }
+        }
+        __syncthreads();  // S is the triangle's from here
+    }
+    // the strict triangle the solve reads
+    stage(Tm, ldt, jb, jb, UPPER ? 1 : -1);
+    __syncthreads();
+    if (!active) return;  // whole warp leaves together
     const int nkb = (jb + RP - 1) / RP;
     if (!UPPER) {
         for (int kb = 0; kb < nkb; ++kb) {
@@ -751,10 +785,12 @@ static mw_status trsm_setup() {
 }
 
 template <class T, bool UPPER, int L = kNB>
-static void trsm_launch(const T* Tm, int64_t ldt, T* X, int64_t ldx, int jb, int64_t ncols, cudaStream_t st) {
-    ProfileScope ps(PC_TRSM, st, 4.0 * (double)jb * jb * ncols, 2.0 * sizeof(T) * (double)jb * ncols);
+static void trsm_launch(const T* Tm, int64_t ldt, T* X, int64_t ldx, int jb, int64_t ncols, cudaStream_t st,
+                        const T* Aoff = nullptr, int64_t ldo = 0, const T* Xp = nullptr, int K = 0) {
+    ProfileScope ps(PC_TRSM, st, 4.0 * (double)jb * jb * ncols + 8.0 * (double)jb * K * ncols,
+                    2.0 * sizeof(T) * (double)jb * ncols);
     trsm_kernel<T, UPPER, L><<<(unsigned)((ncols + kTrsmWarps - 1) / kTrsmWarps), 32 * kTrsmWarps,
-                               trsm_smem_bytes<T, L>(), st>>>(Tm, ldt, X, ldx, jb, ncols);
+                               trsm_smem_bytes<T, L>(), st>>>(Tm, ldt, X, ldx, jb, ncols, Aoff, ldo, Xp, K);
     count_launch();
 }
 
@@ -1404,18 +1440,20 @@ static mw_status getrf_lookahead(int64_t n, T* A, int64_t lda, int32_t* ipiv, in
     return MW_OK;
 }
 
-// One triangular sweep over the right-hand sides B with look-ahead: the
-// leaf solve of block i, then on the caller's stream only the update of the
-// next block's rows (the next leaf's input), while a second stream applies
-// block i's update to all rows beyond it, overlapping block i's small update
-// and leaf i+1 (the two streams never write the same rows at once: st's
-// small update of step i waits for the second stream's update of step i-1).
-// upper = false: X <- L^-1 X (unit lower, blocks in order); upper = true:
-// X <- U^-1 X (blocks in reverse).
+// One triangular sweep over the right-hand sides B with look-ahead.  Step i
+// runs leaf block i on the caller's stream, which first applies the block
+// solved at step i-1 (the leaf kernel's fused update), then a second stream
+// applies block i's solution to the blocks from i+2 on.  Block j thus gets
+// block j-1 inside its leaf and every earlier block from the second stream;
+// the second stream's update of step k writes blocks >= k+2, so leaf i
+// waits only for step i-2's, and the streams never write the same rows at
+// once.  upper = false: X <- L^-1 X (unit lower, blocks in order);
+// upper = true: X <- U^-1 X (blocks in reverse).
 template <class T>
 static mw_status trsm_sweep(bool upper, int64_t n, int64_t nrhs, const T* LU, int64_t lda, T* B, int64_t ldb,
                             const Updater& up_main, const Updater& up_rest, cudaStream_t st) {
     constexpr int LF = GetrsLeaf<T>::value;
+    (void)up_main;
     if (n <= 0 || nrhs <= 0) return MW_OK;
     AuxStreams* ax = nullptr;
     {
@@ -1424,7 +1462,7 @@ static mw_status trsm_sweep(bool upper, int64_t n, int64_t nrhs, const T* LU, in
     }
     cudaStream_t tr = ax->trail;
     const int64_t nblk = (n + LF - 1) / LF;
-    auto blk0 = [&](int64_t b) { return b * LF; };
+    auto blk0 = [&](int64_t b) { return b * LF < n ? b * LF : n; };
     auto blk1 = [&](int64_t b) { return (b + 1) * LF < n ? (b + 1) * LF : n; };
     // the second stream starts after everything queued on st
     MW_CHECK_CUDA(cudaEventRecord(ax->ev_main, st));
@@ -1433,37 +1471,34 @@ static mw_status trsm_sweep(bool upper, int64_t n, int64_t nrhs, const T* LU, in
         const int64_t b = upper ? nblk - 1 - i : i;
         const int64_t r0 = blk0(b), r1 = blk1(b);
         const int jb = (int)(r1 - r0);
-        // (this leaf's rows are final: the update of block i-1 came on st,
-        // the others on the second stream before step i-1's small update)
-        if (upper) trsm_launch<T, true, LF>(LU + r0 + r0 * lda, lda, B + r0, ldb, jb, nrhs, st);
-        else trsm_launch<T, false, LF>(LU + r0 + r0 * lda, lda, B + r0, ldb, jb, nrhs, st);
+        // the blocks before i-1 reach this leaf's rows on the second stream
+        if (i >= 2) MW_CHECK_CUDA(cudaStreamWaitEvent(st, ax->ev_trail[(i - 2) & 3], 0));
+        const T* Aoff = nullptr;
+        const T* Xp = nullptr;
+        int K = 0;
+        if (i >= 1) {  // the block solved at step i-1
+            const int64_t q = upper ? b + 1 : b - 1;
+            const int64_t q0 = blk0(q), q1 = blk1(q);
+            Aoff = LU + r0 + q0 * lda;
+            Xp = B + q0;
+            K = (int)(q1 - q0);
+        }
+        if (upper) trsm_launch<T, true, LF>(LU + r0 + r0 * lda, lda, B + r0, ldb, jb, nrhs, st, Aoff, lda, Xp, K);
+        else trsm_launch<T, false, LF>(LU + r0 + r0 * lda, lda, B + r0, ldb, jb, nrhs, st, Aoff, lda, Xp, K);
         MW_CHECK_CUDA(cudaEventRecord(ax->ev_main, st));
-        // the next block's rows are also written by block i-1's update on
-        // the second stream: it must be done before st touches them
-        if (i >= 1) MW_CHECK_CUDA(cudaStreamWaitEvent(st, ax->ev_trail[(i - 1) & 3], 0));
         mw_status s;
         if (!upper) {
-            if (r1 < n) {  // next block's rows, on st
-                const int64_t n1 = blk1(b + 1);
-                s = block_update(LU + r1 + r0 * lda, lda, B + r0, ldb, B + r1, ldb, n1 - r1, nrhs, jb, up_main, st);
+            const int64_t f0 = blk0(b + 2);
+            if (f0 < n) {  // blocks i+2.., on the second stream
+                MW_CHECK_CUDA(cudaStreamWaitEvent(tr, ax->ev_main, 0));
+                s = block_update(LU + f0 + r0 * lda, lda, B + r0, ldb, B + f0, ldb, n - f0, nrhs, jb, up_rest, tr);
                 if (s != MW_OK) return s;
-                if (n1 < n) {  // the rest, on the second stream
-                    MW_CHECK_CUDA(cudaStreamWaitEvent(tr, ax->ev_main, 0));
-                    s = block_update(LU + n1 + r0 * lda, lda, B + r0, ldb, B + n1, ldb, n - n1, nrhs, jb, up_rest, tr);
-                    if (s != MW_OK) return s;
-                }
             }
-        } else {
-            if (r0 > 0) {
-                const int64_t p0 = blk0(b - 1);
-                s = block_update(LU + p0 + r0 * lda, lda, B + r0, ldb, B + p0, ldb, r0 - p0, nrhs, jb, up_main, st);
-                if (s != MW_OK) return s;
-                if (p0 > 0) {
-                    MW_CHECK_CUDA(cudaStreamWaitEvent(tr, ax->ev_main, 0));
-                    s = block_update(LU + r0 * lda, lda, B + r0, ldb, B, ldb, p0, nrhs, jb, up_rest, tr);
-                    if (s != MW_OK) return s;
-                }
-            }
+        } else if (b >= 2) {  // the blocks above block b-1, on the second stream
+            const int64_t f1 = blk0(b - 1);
+            MW_CHECK_CUDA(cudaStreamWaitEvent(tr, ax->ev_main, 0));
+            s = block_update(LU + r0 * lda, lda, B + r0, ldb, B, ldb, f1, nrhs, jb, up_rest, tr);
+            if (s != MW_OK) return s;
         }
         MW_CHECK_CUDA(cudaEventRecord(ax->ev_trail[i & 3], tr));
     }

@@ -319,6 +319,7 @@ def run_b200(args, kw):
         if name == "cgemm_tc":
             # tcgen05 kind::tf32: B200's TF32 tensor rate is half its BF16
             # rate; the 3xTF32 split issues three MMAs per algorithmic one
+            measured = "bf16_tflops" in peaks
             bf16 = float(peaks.get("bf16_tflops", 1590.0))
             peak = bf16 / 2.0
             # DRAM bytes per launch of this kernel on this workload, from an
@@ -329,8 +330,10 @@ def run_b200(args, kw):
                     "frac": achieved / peak, "tensor_pipe_frac": 3.0 * achieved / peak, "traffic": traffic,
                     "traffic_unit": "bytes per launch (dram read + write, ncu)",
                     "launches_per_step": cnt / args.steps, "avg_launch_ms": tms / cnt,
-                    "peak_source": "MEASURED_PEAKS bf16_tflops / 2 (TF32 rate); achieved counts 8mnk complex "
-                                   "flops, the tensor pipe executes 3x that (3xTF32)"}
+                    "peak_source": ("of measured: MEASURED_PEAKS bf16_tflops / 2" if measured else
+                                    "of fallback: 1590 TFLOP/s bf16 / 2 (MEASURED_PEAKS.json absent)")
+                                   + " (TF32 rate); achieved counts 8mnk complex flops, the tensor pipe executes "
+                                   "3x that (3xTF32)"}
         else:
             # FP64 work has no measured peak in MEASURED_PEAKS.json: the
             # nominal B200 FP64 rate is the denominator there.

@@ -1175,19 +1175,26 @@ static mw_status block_update(const cf* A, int64_t lda, const cf* B, int64_t ldb
     return cgemm_tc_update(m, n, k, A, lda, B, ldb, C, ldc, u.tc_ws, u.tc_ws_bytes, u.tc_err, st, u.max_ctas);
 }
 
-// X <- L^-1 X for a unit lower triangle of any order: kNB-row diagonal
-// blocks by the warp-per-column kernel, the rest of X updated in between.
+// X <- L^-1 X for a unit lower triangle of any order, in kNB-row diagonal
+// blocks: each leaf applies the block just before it itself (the leaf
+// kernel's fused update), blocks further back -- orders above 2 kNB only --
+// reach it through one block update.
 template <class T>
 static mw_status trsm_lower_blocked(const T* L, int64_t ldl, T* X, int64_t ldx, int jb, int64_t ncols,
                                     const Updater& up, cudaStream_t st) {
     for (int b0 = 0; b0 < jb; b0 += kNB) {
         const int bb = (jb - b0) < kNB ? (jb - b0) : kNB;
-        trsm_launch<T, false>(L + b0 + (int64_t)b0 * ldl, ldl, X + b0, ldx, bb, ncols, st);
-        const int rest = jb - b0 - bb;
-        if (rest > 0) {
-            mw_status s = block_update(L + (b0 + bb) + (int64_t)b0 * ldl, ldl, X + b0, ldx, X + b0 + bb, ldx, rest,
-                                       ncols, bb, up, st);
+        if (b0 >= 2 * kNB) {
+            const int k = b0 - kNB;  // blocks 0 .. b0-kNB-1
+            mw_status s = block_update(L + b0, ldl, X, ldx, X + b0, ldx, bb, ncols, k, up, st);
             if (s != MW_OK) return s;
+        }
+        if (b0 == 0) {
+            trsm_launch<T, false>(L, ldl, X, ldx, bb, ncols, st);
+        } else {
+            const int p0 = b0 - kNB;
+            trsm_launch<T, false>(L + b0 + (int64_t)b0 * ldl, ldl, X + b0, ldx, bb, ncols, st,
+                                  L + b0 + (int64_t)p0 * ldl, ldl, X + p0, kNB);
         }
     }
     return MW_OK;

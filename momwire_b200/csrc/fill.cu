@@ -323,6 +323,33 @@ __device__ __forceinline__ void stage_segment(double* dst, int nq, const GLParam
     dst[o + 6] = a;
 }
 
+// sin x and cos x for |x| <= kPhaseStepMax from their Taylor series through
+// x^17 and x^16 (Horner in x^2; coefficients 1/n!).  At |x| = 0.75 the first
+// omitted terms, x^19/19! and x^18/18!, are below 1e-18: full double
+// precision.
+constexpr double kPhaseStepMax = 0.75;
+__device__ __forceinline__ void phase_step(double x, double* sx, double* cx) {
+    const double t = x * x;
+    double c = 1.0 / 20922789888000.0;  // 1/16!
+    c = fma(c, t, -1.0 / 87178291200.0);
+    c = fma(c, t, 1.0 / 479001600.0);
+    c = fma(c, t, -1.0 / 3628800.0);
+    c = fma(c, t, 1.0 / 40320.0);
+    c = fma(c, t, -1.0 / 720.0);
+    c = fma(c, t, 1.0 / 24.0);
+    c = fma(c, t, -0.5);
+    *cx = fma(c, t, 1.0);
+    double s = 1.0 / 355687428096000.0;  // 1/17!
+    s = fma(s, t, -1.0 / 1307674368000.0);
+    s = fma(s, t, 1.0 / 6227020800.0);
+    s = fma(s, t, -1.0 / 39916800.0);
+    s = fma(s, t, 1.0 / 362880.0);
+    s = fma(s, t, -1.0 / 5040.0);
+    s = fma(s, t, 1.0 / 120.0);
+    s = fma(s, t, -1.0 / 6.0);
+    *sx = fma(s * t, x, x);
+}
+
 // Lane `qi` of a pair computes its observer quadrature row and returns its
 // share of all (D+1)^2 moments; the caller reduces the shares over lanes.
 // NQ > 0: the quadrature order is known at compile time (nq == NQ), so the
@@ -344,6 +371,7 @@ __device__ __forceinline__ void pair_row(const double* si, const double* sj, int
 #pragma unroll
     for (int P = 0; P < NM; ++P) accP[P] = cd{0.0, 0.0};
     const double* wv = sj + nq * 3;
+    double R0 = 0.0, s0 = 0.0, c0 = 1.0;
 #pragma unroll
     for (int r = 0; r < (NQ > 0 ? NQ : 8); ++r) {
         if (NQ == 0 && r >= nq) break;
@@ -355,7 +383,23 @@ __device__ __forceinline__ void pair_row(const double* si, const double* sj, int
         double iR = rsqrt(R2);
         double R = R2 * iR;
         double s, c;
-        sincos(k * R, &s, &c);
+        // the first source point's phase in full; the others rotate it by
+        // k (R - R0), at most k times a segment length, through that angle's
+        // Taylor series (phase_step) -- a full sincos where it is wider
+        const double x = k * (R - R0);
+        if (r == 0 || fabs(x) > kPhaseStepMax) {
+            sincos(k * R, &s, &c);
+            if (r == 0) {
+                R0 = R;
+                s0 = s;
+                c0 = c;
+            }
+        } else {
+            double sx, cx;
+            phase_step(x, &sx, &cx);
+            s = s0 * cx + c0 * sx;
+            c = c0 * cx - s0 * sx;
+        }
         double g = kInv4Pi * iR;
         cd G = cd{c * g, -s * g};
         if (EK && ek_on) G = G * ek_factor(R, a, k);

@@ -39,6 +39,18 @@ def test_lu_solve_random(n, cuda_device):
     assert rel_err(X, np.linalg.solve(A, B)) < 1e-9
 
 
+@pytest.mark.parametrize("n,nrhs", [(300, 37), (650, 129)])
+def test_lu_solve_many_right_hand_sides(n, nrhs, cuda_device):
+    """Complex128 sweeps over several leaf CTAs with a partial last block and
+    the fused next-block update."""
+    rng = np.random.default_rng(n + nrhs)
+    A = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    B = rng.standard_normal((n, nrhs)) + 1j * rng.standard_normal((n, nrhs))
+    _LU, _ipiv, info, X = _factor_solve(A, B, cuda_device)
+    assert info[0] == 0 and info[1] == 0
+    assert rel_err(X, np.linalg.solve(A, B)) < 1e-9
+
+
 def test_lu_pivoting_needed(cuda_device):
     """A matrix that fails without row interchanges."""
     A = np.array([[0, 1, 2], [1, 0, 3], [4, 5, 0]], dtype=np.complex128)

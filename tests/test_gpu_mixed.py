@@ -42,6 +42,53 @@ def test_cgetrf_cgetrs_random(n, cuda_device):
     assert rel_err(X, want) < 50 * cond * 6e-8
 
 
+def _cgetrf(A, nrhs_max, device):
+    import torch
+
+    n = A.shape[0]
+    Ad = torch.from_numpy(np.ascontiguousarray(A.T)).to(device)
+    lib = _lib.load()
+    wsb = lib.mw_cgetrf_workspace_size(n, nrhs_max)
+    ws = torch.empty(wsb, dtype=torch.uint8, device=device)
+    ipiv = torch.empty(n, dtype=torch.int32, device=device)
+    info = torch.zeros(2, dtype=torch.int32, device=device)
+    _lib.call("mw_cgetrf", n, Ad.data_ptr(), n, ipiv.data_ptr(), info.data_ptr(), ws.data_ptr(), wsb, nrhs_max, None,
+              None)
+    return Ad, ipiv, info, ws, wsb
+
+
+@pytest.mark.parametrize("n,nrhs", [(390, 37), (1000, 300)])
+def test_cgetrs_many_right_hand_sides(n, nrhs, cuda_device):
+    """Triangular sweeps over several leaf CTAs, a partial last block and
+    the fused next-block update (every leaf after the first)."""
+    import torch
+
+    rng = np.random.default_rng(7 * n + nrhs)
+    A = (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))).astype(np.complex64)
+    A += np.eye(n, dtype=np.complex64) * 2
+    B = (rng.standard_normal((n, nrhs)) + 1j * rng.standard_normal((n, nrhs))).astype(np.complex64)
+    Ad, ipiv, info, ws, wsb = _cgetrf(A, nrhs, cuda_device)
+    Bd = torch.from_numpy(np.ascontiguousarray(B.T)).to(cuda_device)
+    _lib.call("mw_cgetrs", n, nrhs, Ad.data_ptr(), n, ipiv.data_ptr(), Bd.data_ptr(), n, ws.data_ptr(), wsb, None)
+    inf = info.cpu().numpy()
+    assert inf[0] == 0 and inf[1] == 0
+    X = Bd.cpu().numpy().T.astype(np.complex128)
+    want = scipy.linalg.solve(A.astype(np.complex128), B.astype(np.complex128))
+    cond = np.linalg.cond(A.astype(np.complex128))
+    assert rel_err(X, want) < 50 * cond * 6e-8
+
+
+def test_cgetrf_exact_zero_pivot_reports_info(cuda_device):
+    """LAPACK's convention on the complex64 panel: the 1-based column of
+    the first exact zero pivot, no interchange and no scaling there."""
+    n = 200
+    A = np.eye(n, dtype=np.complex64)
+    A[165, 165] = 0.0
+    _Ad, ipiv, info, _ws, _wsb = _cgetrf(A, 1, cuda_device)
+    assert info.cpu().numpy()[0] == 166
+    assert np.array_equal(ipiv.cpu().numpy(), np.arange(1, n + 1))
+
+
 def _zin(y):
     return 1.0 / np.diag(y)
 

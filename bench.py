@@ -37,10 +37,10 @@ sys.path.insert(0, str(ROOT))
 METRIC = "sweep pts/s & fill+LU time, mixed+batched vs FP64 GPU at |ΔZin|/|Zin|≤1e-6"
 UNIT = "pts/s"
 WORKLOAD = "dipole_array_16x16_300MHz_41seg_d2_256port"
-# ncu dram__bytes_read.sum + dram__bytes_write.sum averaged over the 810
-# tensor-core launches of one 16x16 mixed step (43.32 GB read + 19.53 GB
+# ncu dram__bytes_read.sum + dram__bytes_write.sum averaged over the 564
+# tensor-core launches of one 16x16 mixed step (42.25 GB read + 19.50 GB
 # written)
-TC_TRAFFIC_PER_LAUNCH = 77.6e6
+TC_TRAFFIC_PER_LAUNCH = 109.5e6
 
 
 def parse():

@@ -650,7 +650,10 @@ __global__ void __launch_bounds__(32 * kTrsmWarps) trsm_kernel(const T* Tm, int6
     // Stage rows < nr, columns < nc of M (leading dimension ld) into S
     // lane-major -- all of it (part 0), the strict upper (1) or strict lower
     // (-1) triangle -- zero elsewhere; sixteen loads in flight per thread
-    // before the shared-memory stores.
+    // before the shared-memory stores.  Lane slots are swizzled by the row
+    // phase a (slot = lane ^ a*32/RP): the RP phases of a warp's consecutive
+    // rows land in different banks, and a lane's reads stay a permutation of
+    // the 32 slots.
     auto stage = [&](const T* M, int64_t ld, int nr, int nc, int part) {
         constexpr int kU = 16;
         for (int base = 0; base < L * L; base += kU * (int)blockDim.x) {
@@ -667,7 +670,7 @@ __global__ void __launch_bounds__(32 * kTrsmWarps) trsm_kernel(const T* Tm, int6
                 const int i = base + u * (int)blockDim.x + tid;
                 if (i < L * L) {
                     const int r = i % L, c = i / L;
-                    S[((c / RP) * RP * RP + (r % RP) * RP + (c % RP)) * 32 + r / RP] = t[u];
+                    S[((c / RP) * RP * RP + (r % RP) * RP + (c % RP)) * 32 + ((r / RP) ^ ((r % RP) * (32 / RP)))] = t[u];
                 }
             }
         }
@@ -688,14 +691,14 @@ __global__ void __launch_bounds__(32 * kTrsmWarps) trsm_kernel(const T* Tm, int6
             for (int a = 0; a < RP; ++a) xp[a] = RP * lane + a < K ? xq[RP * lane + a] : zero;
             const int nkq = (K + RP - 1) / RP;
             for (int kb = 0; kb < nkq; ++kb) {
-                const T* Sk = S + kb * RP * RP * 32 + lane;
+                const T* Sk = S + kb * RP * RP * 32;
                 T xb[RP];
 #pragma unroll
                 for (int b = 0; b < RP; ++b) xb[b] = shfl_c(xp[b], kb);
 #pragma unroll
                 for (int a = 0; a < RP; ++a)
 #pragma unroll
-                    for (int b = 0; b < RP; ++b) v[a] = v[a] - Sk[(a * RP + b) * 32] * xb[b];
+                    for (int b = 0; b < RP; ++b) v[a] = v[a] - Sk[(a * RP + b) * 32 + (lane ^ (a * (32 / RP)))] * xb[b];
             }
         }
         __syncthreads();  // S is the triangle's from here
@@ -707,7 +710,7 @@ __global__ void __launch_bounds__(32 * kTrsmWarps) trsm_kernel(const T* Tm, int6
     const int nkb = (jb + RP - 1) / RP;
     if (!UPPER) {
         for (int kb = 0; kb < nkb; ++kb) {
-            const T* Sk = S + kb * RP * RP * 32 + lane;
+            const T* Sk = S + kb * RP * RP * 32;
             T xb[RP];
 #pragma unroll
             for (int b = 0; b < RP; ++b) xb[b] = zero;
@@ -716,7 +719,7 @@ __global__ void __launch_bounds__(32 * kTrsmWarps) trsm_kernel(const T* Tm, int6
                 for (int a = 0; a < RP; ++a) {
                     T t = v[a];
 #pragma unroll
-                    for (int b = 0; b < a; ++b) t = t - Sk[(a * RP + b) * 32] * xb[b];
+                    for (int b = 0; b < a; ++b) t = t - Sk[(a * RP + b) * 32 + (lane ^ (a * (32 / RP)))] * xb[b];
                     xb[a] = t;
                     v[a] = t;
                 }
@@ -727,12 +730,12 @@ __global__ void __launch_bounds__(32 * kTrsmWarps) trsm_kernel(const T* Tm, int6
 #pragma unroll
                 for (int a = 0; a < RP; ++a)
 #pragma unroll
-                    for (int b = 0; b < RP; ++b) v[a] = v[a] - Sk[(a * RP + b) * 32] * xb[b];
+                    for (int b = 0; b < RP; ++b) v[a] = v[a] - Sk[(a * RP + b) * 32 + (lane ^ (a * (32 / RP)))] * xb[b];
             }
         }
     } else {
         for (int kb = nkb - 1; kb >= 0; --kb) {
-            const T* Sk = S + kb * RP * RP * 32 + lane;
+            const T* Sk = S + kb * RP * RP * 32;
             T xb[RP];
 #pragma unroll
             for (int b = 0; b < RP; ++b) xb[b] = zero;
@@ -741,7 +744,7 @@ __global__ void __launch_bounds__(32 * kTrsmWarps) trsm_kernel(const T* Tm, int6
                 for (int a = RP - 1; a >= 0; --a) {
                     T t = v[a];
 #pragma unroll
-                    for (int b = RP - 1; b > a; --b) t = t - Sk[(a * RP + b) * 32] * xb[b];
+                    for (int b = RP - 1; b > a; --b) t = t - Sk[(a * RP + b) * 32 + (lane ^ (a * (32 / RP)))] * xb[b];
                     xb[a] = t * sD[RP * lane + a];
                     v[a] = xb[a];
                 }
@@ -752,7 +755,7 @@ __global__ void __launch_bounds__(32 * kTrsmWarps) trsm_kernel(const T* Tm, int6
 #pragma unroll
                 for (int a = 0; a < RP; ++a)
 #pragma unroll
-                    for (int b = RP - 1; b >= 0; --b) v[a] = v[a] - Sk[(a * RP + b) * 32] * xb[b];
+                    for (int b = RP - 1; b >= 0; --b) v[a] = v[a] - Sk[(a * RP + b) * 32 + (lane ^ (a * (32 / RP)))] * xb[b];
             }
         }
     }

@@ -4,16 +4,21 @@
 // momwire (bspline.py:2971-2989).  Right-looking blocked algorithm, generic
 // in the element type (complex128 for the plain path, complex64 for the
 // mixed-precision path):
-//   panel   : one cooperative kernel per panel; rows split over all SMs,
+//   panel   : one cooperative kernel per panel; rows split over the CTAs,
 //             each CTA's row slab kept in shared memory for the whole panel,
-//             one bounded grid barrier per column; pivot candidates and their
-//             rows travel through double-buffered slots; panels whose slabs
-//             would not fit are split in two and recursed;
+//             one all-to-all pivot exchange per column -- complex128: a
+//             bounded grid barrier and double-buffered slots; complex64:
+//             self-validating tagged records read in one batch (no fence);
+//             panels whose slabs would not fit are split in two and
+//             recursed;
 //   laswp   : row interchanges outside the panel;
-//   trsm    : U12 = L11^-1 A12 with L11 staged in shared memory;
+//   trsm    : triangular leaves with the triangle staged lane-major in
+//             shared memory, each optionally applying the block solved
+//             before it (the next-block update of a blocked sweep);
 //   update  : A22 -= L21 U12 -- complex128: register-tiled FP64 GEMM;
 //             complex64: tcgen05 tensor cores, 3xTF32 (cgemm_tc.cu).
-// Pivot choice follows LAPACK's izamax: max |re| + |im|, first index wins.
+// Pivot choice follows LAPACK's izamax: max |re| + |im|, first index wins
+// (complex64: the float sum, as LAPACK's icamax).
 #include <cstdio>
 #include <type_traits>
 
@@ -90,8 +95,9 @@ struct PanelArgs {
     int32_t* ipiv;
     int32_t* info;
     PanelWs* ws;
-    // double-buffered slots: [2][G] values, [2][G] indices,
-    // [2][G][kPanelMaxJb] candidate rows, [2][kPanelMaxJb] current row
+    // double-buffered slots: [2][G] values, [2][G] indices (complex64: the
+    // key words), [2][G][kPanelMaxJb] candidate rows (complex64: the tagged
+    // records, candidate rows then row c), [2][kPanelMaxJb] current row
     double* slot_val;
     int64_t* slot_idx;
     void* slot_row;

@@ -50,10 +50,15 @@ def build_geometry(wires, npe, radius_per_wire) -> Geometry:
     """Uniform segments on every polyline edge: knots by linspace between
     the edge's anchors, h = |edge| / n (``bspline.py:1027-1050``).  All
     edges of all wires are laid out in one pass."""
-    p0 = np.concatenate([np.asarray(pl, dtype=np.float64)[:-1] for pl in wires], axis=0)
-    p1 = np.concatenate([np.asarray(pl, dtype=np.float64)[1:] for pl in wires], axis=0)
+    n_pts = np.fromiter((len(pl) for pl in wires), dtype=np.int64, count=len(wires))
+    pts = np.concatenate([np.asarray(pl, dtype=np.float64) for pl in wires], axis=0)
+    # an edge starts at every point but a wire's last
+    is_start = np.ones(pts.shape[0], dtype=bool)
+    is_start[np.cumsum(n_pts) - 1] = False
+    p0 = pts[is_start]
+    p1 = pts[np.flatnonzero(is_start) + 1]
     e_n = np.concatenate([np.asarray(c, dtype=np.int64).reshape(-1) for c in npe])
-    e_wire = np.concatenate([np.full(len(pl) - 1, w, dtype=np.int64) for w, pl in enumerate(wires)])
+    e_wire = np.repeat(np.arange(len(wires), dtype=np.int64), n_pts - 1)
     if e_n.shape[0] != p0.shape[0]:
         raise ValueError("one segment count per polyline edge is needed")
     vec = p1 - p0
@@ -78,7 +83,13 @@ def build_geometry(wires, npe, radius_per_wire) -> Geometry:
     h = e_h[edge]
     w_n = np.bincount(e_wire, weights=e_n, minlength=len(wires)).astype(np.int64)
     w_first = np.concatenate(([0], np.cumsum(w_n)[:-1])).astype(np.int64)
-    w_arc = [np.concatenate([[0.0], np.cumsum(h[f : f + n])]) for f, n in zip(w_first.tolist(), w_n.tolist())]
+    # arc length at knots per wire: one row-wise running sum over a padded
+    # table (the same left-to-right additions as a per-wire cumsum)
+    pad = np.zeros((len(wires), int(w_n.max(initial=0)) + 1))
+    col = np.arange(h.shape[0]) - np.repeat(w_first, w_n)
+    pad[np.repeat(np.arange(len(wires)), w_n), col + 1] = h
+    np.cumsum(pad[:, 1:], axis=1, out=pad[:, 1:])
+    w_arc = [pad[w, : n + 1] for w, n in enumerate(w_n.tolist())]
     return Geometry(
         seg_l=np.ascontiguousarray(seg_l),
         seg_r=np.ascontiguousarray(seg_r),

@@ -140,16 +140,30 @@ def point_values(knots_list, d, wires, xs):
     Same span rule as ``basis_values``; one batched Cox-de Boor evaluation
     over 2d-knot windows."""
     n = len(xs)
-    K = np.empty((n, 2 * d))
-    first = np.empty(n, dtype=np.int64)
-    for i, (w, x) in enumerate(zip(wires, xs)):
-        kn = knots_list[w]
-        n_b = len(kn) - d - 1
-        sp = min(max(int(np.searchsorted(kn, x, side="right")) - 1, d), n_b - 1)
-        K[i] = kn[sp + 1 - d : sp + d + 1]
-        first[i] = sp - d
+    xs = np.asarray(xs, dtype=np.float64).reshape(-1)
+    w = np.asarray(wires, dtype=np.int64).reshape(-1)
+    lens = np.fromiter((len(k) for k in knots_list), dtype=np.int64, count=len(knots_list))
+    offs = np.concatenate(([0], np.cumsum(lens)[:-1])).astype(np.int64)
+    cat = np.concatenate(knots_list) if len(knots_list) else np.zeros(0)
+    # bisect-right of x in its own wire's knot vector, all points at once
+    # (the index np.searchsorted(kn, x, side="right") returns)
+    lo = offs[w].copy()
+    hi = lo + lens[w]
+    while True:
+        act = lo < hi
+        if not act.any():
+            break
+        mid = (lo + hi) // 2
+        right = act & (cat[np.minimum(mid, cat.size - 1)] <= xs)
+        left = act & ~right
+        lo = np.where(right, mid + 1, lo)
+        hi = np.where(left, mid, hi)
+    n_b = lens[w] - d - 1
+    sp = np.minimum(np.maximum(lo - offs[w] - 1, d), n_b - 1)
+    K = cat[(offs[w] + sp + 1 - d)[:, None] + np.arange(2 * d)[None, :]].reshape(n, 2 * d)
+    first = (sp - d).astype(np.int64)
     span = np.arange(n) * (2 * d) + (d - 1)
-    vals = _span_values(K.ravel(), d, span, np.asarray(xs, dtype=np.float64))
+    vals = _span_values(K.ravel(), d, span, xs)
     return vals.reshape(n, d + 1), first
 
 

@@ -91,6 +91,10 @@ XQ
 EN
 """,
 }
+DECKS["dipole_free_d1"] = DECKS["dipole_free"]
+
+# the reference's basis name per deck (its BASES table): degree 2 unless named
+BASIS_OF = {"dipole_free_d1": "bspline-d1"}
 
 
 def _jsonable(v):
@@ -126,12 +130,17 @@ def main():
             super().__init__(**kw)
 
     stock = deck_solver.BASES
-    deck_solver.BASES = MappingProxyType({**stock, "bspline": (Recording, MappingProxyType({}))})
+    deck_solver.BASES = MappingProxyType({
+        **stock,
+        "bspline": (Recording, stock["bspline"][1]),
+        "bspline-d1": (Recording, stock["bspline-d1"][1]),
+    })
     out = {}
     try:
         for name, text in DECKS.items():
             model = deck.parse(text)
-            built = deck.build_solver(model, basis="bspline")
+            basis = BASIS_OF.get(name, "bspline")
+            built = deck.build_solver(model, basis=basis)
             kw = {k: v for k, v in recorded.items() if k != "cancel"}
             sol = built.solver.compute_port_solution()
             y = np.asarray(sol.y)
@@ -139,6 +148,7 @@ def main():
             np.savez(HERE / f"deck_{name}.npz", y=y, zin=zin)
             out[name] = {
                 "deck": text,
+                "basis": basis,
                 "kwargs": _jsonable(kw),
                 "frequency_mhz": built.frequency_mhz,
                 "n_ports": int(y.shape[0]),

@@ -2,7 +2,8 @@
 ``deck.build_solver`` passes to ``BSplineSolver`` for NEC-2 decks (recorded
 by ``tests/golden/make_decks.py``: a dipole, a Yagi bare and with copper
 conductors, an inverted V over a perfect ground, a monopole with radials
-over a Sommerfeld ground) construct ``momwire_b200.BSplineSolver`` as they
+over a Sommerfeld ground, and the dipole again through the degree-1 basis
+entry) construct ``momwire_b200.BSplineSolver`` as they
 are, with the reference's port count and host tables equal to the oracle's."""
 
 import numpy as np
@@ -39,3 +40,4 @@ def test_deck_fixtures_cover_the_front_end_paths():
     assert "wire_conductivity" in kinds["yagi3_copper"]
     assert kinds["inverted_v_pec"]["ground_z"] == 0.0 and "ground_eps" not in kinds["inverted_v_pec"]
     assert kinds["dipole_free"]["ground_z"] is None
+    assert DECKS["dipole_free_d1"]["basis"] == "bspline-d1" and kinds["dipole_free_d1"]["degree"] == 1

@@ -109,6 +109,21 @@ def test_kept_index_and_point_values(name):
         assert np.count_nonzero(np.delete(full, np.arange(first[i], first[i] + d + 1))) == 0
 
 
+@pytest.mark.parametrize("name", ["d1_dipole20", "d2_junction", "d2_mixed_radius_kink", "d2_somm_plate8"])
+def test_point_values_at_every_knot(name):
+    """The batched point evaluation at every knot of every wire -- the
+    right-open span rule's ties -- against the full design matrix."""
+    s = momwire_b200.BSplineSolver(**CASES[name]())
+    g, b = s._geometry(), s._basis()
+    d = b.degree
+    ws = np.concatenate([np.full(len(a), w) for w, a in enumerate(g.wire_arc)])
+    xs = np.concatenate(g.wire_arc)
+    vals, first = T.point_values(b.knots, d, ws, xs)
+    for i, (w, x) in enumerate(zip(ws, xs)):
+        full = T.basis_values(b.knots[w], d, [x])[0]
+        assert np.array_equal(full[first[i] : first[i] + d + 1], vals[i])
+
+
 def test_ek_labels_match_oracle():
     kw = CASES["d2_ek_monopole_pec"]()
     s = momwire_b200.BSplineSolver(**kw)

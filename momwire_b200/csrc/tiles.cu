@@ -2,6 +2,10 @@
 // consecutive bases whose wings touch at most max_seg distinct segments
 // (the tiles the fill kernel stages in shared memory).  Plain C++ on the
 // host; no device work.
+#include <algorithm>
+#include <thread>
+#include <vector>
+
 #include "common.cuh"
 
 extern "C" mw_status mw_build_tiles(const int32_t* supp, int64_t n_b, int32_t wings, int32_t max_basis,
@@ -87,9 +91,12 @@ extern "C" mw_status mw_basis_polys(const double* garc, const int64_t* arc_off, 
     // inverse of U[i][p] = (i/d)^p
     static const double kUinv1[2][2] = {{1.0, 0.0}, {-1.0, 1.0}};
     static const double kUinv2[3][3] = {{1.0, 0.0, 0.0}, {-3.0, 4.0, -1.0}, {2.0, -4.0, 2.0}};
-    for (int64_t b = 0; b < m; ++b) {
+    for (int64_t b = 0; b < m; ++b)
+        MW_REQUIRE(bw[b] >= 0 && bw[b] < n_wires, "basis %lld: wire out of range", (long long)b);
+    // every basis is independent: contiguous chunks on host threads for
+    // large structures (the same arithmetic per basis, so the same bits)
+    auto one = [&](int64_t b) {
         const int64_t w = bw[b], j = js[b];
-        MW_REQUIRE(w >= 0 && w < n_wires, "basis %lld: wire out of range", (long long)b);
         const int64_t nw = wire_n[w], off = arc_off[w];
         const double* arc = garc + off;
         const int64_t lo = j - d > 0 ? j - d : 0, hi = nw < j + 1 ? nw : j + 1;
@@ -137,6 +144,20 @@ extern "C" mw_status mw_basis_polys(const double* garc, const int64_t* arc_off, 
                 hp *= h;
             }
         }
+    };
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int64_t nt = std::min<int64_t>(std::min<int64_t>(hw ? hw : 1, 8), m / 1024);
+    if (nt <= 1) {
+        for (int64_t b = 0; b < m; ++b) one(b);
+    } else {
+        std::vector<std::thread> pool;
+        const int64_t chunk = (m + nt - 1) / nt;
+        for (int64_t t = 0; t < nt; ++t)
+            pool.emplace_back([&, t] {
+                const int64_t b1 = std::min(m, (t + 1) * chunk);
+                for (int64_t b = t * chunk; b < b1; ++b) one(b);
+            });
+        for (auto& th : pool) th.join();
     }
     return MW_OK;
 }

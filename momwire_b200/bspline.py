@@ -352,9 +352,9 @@ class BSplineSolver:
             self.feeds = norm
         self.feed_wire_index = self.feeds[0][0] if self.feeds else None
         self.feed_arclength = self.feeds[0][1] if self.feeds else None
+        # checked where the reference's quadrature first uses it: at the
+        # solve (``_dev_tables``), with the reference's exception and text
         self.n_qp_pair = int(n_qp_pair)
-        if not (1 <= self.n_qp_pair <= 8):
-            raise ValueError(f"n_qp_pair must be in [1, 8], got {n_qp_pair}")
 
         self.junctions = []
         if junctions is not None:
@@ -571,6 +571,14 @@ class BSplineSolver:
 
     def _dev_tables(self) -> _DeviceTables:
         if self._cached_dev is None:
+            # the reference refuses these at the solve: numpy's Gauss-Legendre
+            # rule for a non-positive order, its native pair quadrature above
+            # eight points (``_accelerators.cpp`` scratch buffers); so do the
+            # device kernels here
+            if self.n_qp_pair < 1:
+                np.polynomial.legendre.leggauss(self.n_qp_pair)
+            if self.n_qp_pair > 8:
+                raise RuntimeError("n_qp > 8 not supported (scratch buffer size)")
             geom, basis = self._geometry(), self._basis()
             if self._cached_tiles is None:
                 self._cached_tiles = T.build_tiles(basis.supp)

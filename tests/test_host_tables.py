@@ -152,6 +152,17 @@ def test_constructor_validation_messages():
         momwire_b200.BSplineSolver(wires=w, ground_z=0.0, ground_eps=(13, 0.005))
 
 
+@pytest.mark.parametrize("q,exc,msg", [(0, ValueError, "deg must be a positive integer"),
+                                       (9, RuntimeError, "n_qp > 8 not supported")])
+def test_pair_quadrature_order_refused_at_the_solve(q, exc, msg):
+    """As the reference: any order is taken by the constructor; a solve with
+    none, or with more than eight points per segment, is refused."""
+    s = momwire_b200.BSplineSolver(wires=[np.array([[0, 0, -5.0], [0, 0, 5.0]])], nsegs=21, wavelength=21.0,
+                                   n_qp_pair=q)
+    with pytest.raises(exc, match=msg):
+        s._dev_tables()
+
+
 @pytest.mark.parametrize("name", sorted(CASES))
 def test_basis_count_and_kcl_rows_without_building(name):
     s = momwire_b200.BSplineSolver(**CASES[name]())

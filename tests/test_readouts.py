@@ -1,7 +1,11 @@
 """Host readouts from a solve's coefficients: the current's arc-length
 derivative (current_slopes) against the reference's own values for the
 golden cases, and at arbitrary arc positions against scipy's B-spline
-derivative (the routine the reference evaluates it with)."""
+derivative (the routine the reference evaluates it with); the currents at
+knots and the field evaluator's element terms (element_currents) against
+the reference's, all from the reference's own coefficients."""
+
+from pathlib import Path
 
 import numpy as np
 import pytest
@@ -46,3 +50,31 @@ def test_current_slopes_at_arc_positions(name):
         np.testing.assert_allclose(got[w], want, rtol=1e-12, atol=1e-12 * np.abs(want).max())
     empty = s.current_slopes(c, [np.zeros(0)] * len(b.knots))
     assert all(e.size == 0 for e in empty)
+
+
+_READOUT_CASES = sorted(n for n in CASES if (Path(__file__).resolve().parent / "golden" / f"readouts_{n}.npz").exists())
+
+
+@pytest.mark.parametrize("name", _READOUT_CASES)
+def test_currents_at_knots_match_reference(name):
+    """Host readout of the reference's own first port column."""
+    g = golden(name)
+    s = momwire_b200.BSplineSolver(**CASES[name]())
+    cur = np.concatenate(s.currents_at_knots(g["coeffs"][:, 0]))
+    assert rel_err(cur, g["currents0"]) < 1e-12
+
+
+@pytest.mark.parametrize("name", _READOUT_CASES)
+@pytest.mark.parametrize("subdiv", [1, 3])
+def test_element_currents_match_reference(name, subdiv):
+    """(mid, moment, nodes, delta) of the reference's own first port column
+    against its ``element_currents`` (``_element_currents.py:33-120``)."""
+    g = golden(name)
+    want = golden(f"readouts_{name}")
+    s = momwire_b200.BSplineSolver(**CASES[name]())
+    mid, mom, nodes, delta = s.element_currents(g["coeffs"][:, 0], subdiv=subdiv)
+    np.testing.assert_allclose(mid, want[f"mid{subdiv}"], rtol=0, atol=1e-12 * np.abs(want[f"mid{subdiv}"]).max())
+    np.testing.assert_allclose(nodes, want[f"nodes{subdiv}"], rtol=0,
+                               atol=1e-12 * np.abs(want[f"nodes{subdiv}"]).max())
+    assert rel_err(mom, want[f"mom{subdiv}"]) < 1e-12
+    assert rel_err(delta, want[f"delta{subdiv}"]) < 1e-11

@@ -1,0 +1,34 @@
+"""Invalid constructor inputs, shared by the generator of the reference's
+refusals (``make_refusals.py``) and the test that replays them."""
+
+import numpy as np
+
+_D = [np.array([[0, 0, -5.0], [0, 0, 5.0]])]
+_Y = [np.array([[0, 0, -5.0], [0, 0, 5.0]]), np.array([[1, 0, -5.0], [1, 0, 5.0]])]
+_V = [np.array([[0, 0, 0.0], [1, 0, 1.0]]), np.array([[0, 0, 0.0], [-1, 0, 1.0]])]
+
+REFUSALS = {
+    "feed_wire_out_of_range": lambda: dict(wires=_D, feeds=[(2, None, 1.0)]),
+    "feed_arclength_beyond_wire": lambda: dict(wires=_D, feeds=[(0, 50.0, 1.0)]),
+    "feed_negative_arclength": lambda: dict(wires=_D, feeds=[(0, -1.0, 1.0)]),
+    "degree_0": lambda: dict(wires=_D, degree=0),
+    "degree_3": lambda: dict(wires=_D, degree=3),
+    "nsegs_0": lambda: dict(wires=_D, nsegs=0),
+    "radius_negative": lambda: dict(wires=_D, wire_radius=-1e-3),
+    "radius_list_length": lambda: dict(wires=_Y, wire_radius=[1e-3]),
+    "ground_eps_without_ground_z": lambda: dict(wires=_D, ground_eps=(13, 0.005)),
+    "ground_model_unknown": lambda: dict(wires=_D, ground_z=-6.0, ground_eps=(13, 0.005), ground_model="bogus"),
+    "ground_phi_mode_unknown": lambda: dict(wires=_D, ground_z=-6.0, ground_eps=(13, 0.005), ground_phi_mode="bogus"),
+    "junction_port_out_of_range": lambda: dict(wires=_D, junction_ports=[0]),
+    "junction_wire_out_of_range": lambda: dict(wires=_V, junctions=[[(0, "start"), (5, "start")]]),
+    "junction_end_unknown": lambda: dict(wires=_V, junctions=[[(0, "start"), (1, "middle")]]),
+    "node_gap_wire_out_of_range": lambda: dict(wires=_D, node_gaps=[(3, "start", 1.0)]),
+    "edge_counts_per_wire": lambda: dict(wires=_D, n_per_edge_per_wire=[[5, 5]]),
+    "feed_model_unknown": lambda: dict(wires=_D, feed_model="bogus"),
+    "zero_length_wire": lambda: dict(wires=[np.array([[0, 0, 0.0], [0, 0, 0.0]])]),
+    "conductivity_negative": lambda: dict(wires=_D, wire_conductivity=-1.0),
+    # refused at the solve, not by the constructor
+    "pair_quadrature_0": lambda: dict(wires=_D, nsegs=21, wavelength=21.0, n_qp_pair=0),
+    "pair_quadrature_9": lambda: dict(wires=_D, nsegs=21, wavelength=21.0, n_qp_pair=9),
+}
+AT_SOLVE = {"pair_quadrature_0", "pair_quadrature_9"}

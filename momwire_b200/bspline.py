@@ -1280,13 +1280,20 @@ class BSplineSolver:
         return out
 
     def compute_impedance_swept(self, k_array):
-        """Per-k drive-point impedance (``bspline.py:4479``)."""
-        out = []
+        """Drive-point impedances over a batch of wavenumbers
+        (``bspline.py:4479-4513``): complex, (n_k,) for one port and
+        (n_k, n_feeds + n_junction_ports) otherwise -- the layout the
+        reference allocates before its per-k loop, empty sweeps included."""
+        k_array = np.asarray(k_array, dtype=float)
+        n_total = len(self.feeds) + len(self.junction_ports)
+        shape = (k_array.shape[0],) if n_total == 1 else (k_array.shape[0], n_total)
+        z_out = np.zeros(shape, dtype=np.complex128)
         with self._k_restored():
-            for kk in np.asarray(k_array, dtype=float):
+            for i, kk in enumerate(k_array):
+                self._checkpoint()
                 self._set_k(kk)
-                out.append(self.compute_impedance()[0])
-        return np.asarray(out)
+                z_out[i] = self.compute_impedance()[0]
+        return z_out
 
     # -------------------------------------------------------------- readout
     def currents_at_knots(self, coeffs, s_array=None):

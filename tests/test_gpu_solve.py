@@ -128,3 +128,17 @@ def test_plate64_sommerfeld_mixed(cuda_device):
     y = s.compute_port_solution().y
     zin, zref = 1.0 / np.diag(y), 1.0 / np.diag(g["y"])
     assert np.max(np.abs(zin - zref) / np.abs(zref)) <= 1e-6
+
+
+def test_impedance_swept_all_ports(cuda_device):
+    """Multi-port sweeps return every port's impedance per k, (n_k, n_ports),
+    each row the per-k compute_impedance (``bspline.py:4496-4513``)."""
+    kw = CASES["d2_junction_port"]()
+    s = momwire_b200.BSplineSolver(**kw)
+    ks = s.k * np.array([0.97, 1.03])
+    zs = s.compute_impedance_swept(ks)
+    assert zs.shape == (2, 2)
+    for i, kk in enumerate(ks):
+        t = momwire_b200.BSplineSolver(**dict(kw, wavelength=2 * np.pi / kk))
+        z, _ = t.compute_impedance()
+        np.testing.assert_allclose(zs[i], z, rtol=1e-12)

@@ -34,6 +34,7 @@ from . import autotune
 from . import loading as wl
 from . import sommerfeld as somm
 from . import surrogate as sur
+from ._capabilities import Capabilities
 from ._port_solution import PortSolution
 
 
@@ -167,6 +168,10 @@ class _DeviceTables:
         )
 
 
+_ENRICHMENT_REFUSAL = "use_singular_enrichment is outside the B200 dense path"
+_CONTACT_REFUSAL = "ground contact is refused under ground_model='refl-coef' (use ground_model='sommerfeld')"
+
+
 class BSplineSolver:
     """Degree-d B-spline Galerkin MoM on multi-wire polylines with
     junctions, filled and factorised on a B200.
@@ -179,6 +184,19 @@ class BSplineSolver:
     precision : "fp64" (default) or "mixed".
     device : CUDA device index or torch.device (default: current device).
     """
+
+    # what the class serves, read by consumers before they build one
+    # (``bspline.py:495-509``; singular enrichment is not served here)
+    capabilities = Capabilities(
+        grounds=frozenset({"pec", "refl-coef", "sommerfeld"}),
+        wire_loading=True,
+        extended_kernel=True,
+        junction_ports=True,
+        node_gaps=True,
+        per_wire_radius=True,
+        singular_enrichment=False,
+        refusals={"singular_enrichment": _ENRICHMENT_REFUSAL, "contact+refl-coef": _CONTACT_REFUSAL},
+    )
 
     eps = 8.8541878188e-12
     mu = 1.25663706127e-6
@@ -213,6 +231,11 @@ class BSplineSolver:
         ground_model="refl-coef",
         n_qp_sommerfeld=3,
         use_singular_enrichment=False,
+        n_qp_sing=32,
+        enrichment_min_k=3,
+        enrichment_variant="raw",
+        tikhonov_lambda=1e-3,
+        auto_tap_ratio_threshold=0.3,
         swept_mem_mb=256,
         cancel=None,
         precision="fp64",
@@ -230,7 +253,20 @@ class BSplineSolver:
         if not wires:
             raise ValueError("wires must be non-empty")
         if use_singular_enrichment:
-            raise NotImplementedError("use_singular_enrichment is outside the B200 dense path")
+            raise NotImplementedError(_ENRICHMENT_REFUSAL)
+        # the enrichment settings are taken and kept (their consumers read
+        # them) with the reference's validation (``bspline.py:793-838``)
+        self.use_singular_enrichment = False
+        self.n_qp_sing = int(n_qp_sing)
+        self.enrichment_min_k = int(enrichment_min_k)
+        if enrichment_variant not in ("raw", "stable", "tikhonov", "auto"):
+            raise ValueError(
+                f"enrichment_variant must be one of 'raw', 'stable', "
+                f"'tikhonov', 'auto', got {enrichment_variant!r}"
+            )
+        self.enrichment_variant = enrichment_variant
+        self.tikhonov_lambda = float(tikhonov_lambda)
+        self.auto_tap_ratio_threshold = float(auto_tap_ratio_threshold)
         if precision not in ("fp64", "mixed"):
             raise ValueError(f"precision must be 'fp64' or 'mixed', got {precision!r}")
         self.precision = precision
@@ -294,10 +330,7 @@ class BSplineSolver:
             touching = self._contact_ends()
             if touching:
                 where = ", ".join(f"wire {w} {kind}" for w, kind in touching)
-                raise NotImplementedError(
-                    f"{where} lies in the ground plane: ground contact is refused "
-                    "under ground_model='refl-coef' (use ground_model='sommerfeld')"
-                )
+                raise NotImplementedError(f"{where} lies in the ground plane: {_CONTACT_REFUSAL}")
         r = np.asarray(wire_radius, dtype=float)
         if r.ndim == 0:
             r = np.full(n_w, float(r))

@@ -27,6 +27,10 @@ REFUSALS = {
     "feed_model_unknown": lambda: dict(wires=_D, feed_model="bogus"),
     "zero_length_wire": lambda: dict(wires=[np.array([[0, 0, 0.0], [0, 0, 0.0]])]),
     "conductivity_negative": lambda: dict(wires=_D, wire_conductivity=-1.0),
+    "enrichment_variant_unknown": lambda: dict(wires=_D, enrichment_variant="bogus"),
+    "enrichment_settings_with_enrichment_off": lambda: dict(wires=_D, n_qp_sing=16, enrichment_min_k=4,
+                                                            enrichment_variant="stable", tikhonov_lambda=1e-2,
+                                                            auto_tap_ratio_threshold=0.5),
     # refused at the solve, not by the constructor
     "pair_quadrature_0": lambda: dict(wires=_D, nsegs=21, wavelength=21.0, n_qp_pair=0),
     "pair_quadrature_9": lambda: dict(wires=_D, nsegs=21, wavelength=21.0, n_qp_pair=9),

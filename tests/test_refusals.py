@@ -44,3 +44,26 @@ def test_empty_sweeps_have_the_reference_layout(name, shape):
     y = s.compute_y_matrix_swept(np.array([]))
     assert y.shape == (0, n_p, n_p) and y.dtype == np.complex128
     assert s.compute_port_solution_swept(np.array([])) == []
+
+
+def test_capabilities_declaration():
+    """The class-level declaration consumers read (the reference's
+    ``capabilities`` interface) with this package's values."""
+    cap = momwire_b200.BSplineSolver.capabilities
+    assert cap.grounds == frozenset({"pec", "refl-coef", "sommerfeld"})
+    assert cap.wire_loading and cap.extended_kernel and cap.junction_ports and cap.node_gaps
+    assert cap.per_wire_radius and not cap.singular_enrichment
+    assert cap.refusal("sommerfeld", "junction_ports") is None
+    assert cap.refusal("wire_loading") is None
+    assert "outside the B200 dense path" in cap.refusal("singular_enrichment")
+    assert "ground contact is refused" in cap.refusal("refl-coef", "contact")
+    assert cap.refusal("bogus_axis") is None  # a condition token alone is served
+
+
+def test_enrichment_settings_are_kept():
+    from refusal_cases import REFUSALS
+
+    s = momwire_b200.BSplineSolver(**REFUSALS["enrichment_settings_with_enrichment_off"]())
+    assert (s.use_singular_enrichment, s.n_qp_sing, s.enrichment_min_k, s.enrichment_variant) == (False, 16, 4,
+                                                                                                  "stable")
+    assert (s.tikhonov_lambda, s.auto_tap_ratio_threshold) == (1e-2, 0.5)

@@ -57,7 +57,8 @@ def parse():
     ap.add_argument("--sweep-mode", choices=("grouped", "workers"), default="grouped",
                     help="grouped: padded groups of structures share one batched solve; workers: one batched "
                          "solve per structure on --sweep-workers host threads")
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=None,
+                    help="public-API calls timed for e2e (default: --steps)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--nx", type=int, default=16)
     ap.add_argument("--micro", default=None, choices=["cgemm_tc"], help="kernel microbenchmark instead")
@@ -128,42 +129,78 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------ reference
-def cpu_baseline_sample(kw):
-    """The reference's own CPU kernels (oracle/_ref) + LAPACK on a bounded
-    sample: a quarter of the observer rows, and the LU of their leading
-    block, extrapolated to the full workload."""
+def load_workloads():
+    """The seeded workload generators, loaded from their file so that the
+    package itself (and its native library) is not imported by the
+    reference arm."""
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("_mw_workloads", ROOT / "momwire_b200" / "workloads.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def workload_config(n_unknowns, ports, nx=16):
+    """The ``config`` object of both arms (identical keys and values)."""
+    name = WORKLOAD if nx == 16 else WORKLOAD.replace("16x16", f"{nx}x{nx}").replace("256port", f"{ports}port")
+    zb = n_unknowns ** 2 * 16
+    l2 = (f"inputs larger than L2 (Z = {zb / 1e9:.2f} GB per step, no flush)" if zb > 126e6 else
+          f"inputs smaller than L2 (Z = {zb / 1e6:.1f} MB; not a headline size)")
+    return {"workload": name, "n_unknowns": int(n_unknowns), "ports": int(ports), "l2": l2}
+
+
+def cpu_baseline_full(kw):
+    """The reference's own ``compute_port_solution()`` (its C++ fill kernels
+    with OpenMP and LAPACK zgesv) on the full workload, once, on every host
+    core; with the reference's Y for the parity check of the GPU arm."""
     from oracle import ref_baseline
 
-    r = ref_baseline.time_sample(kw, row_fraction=0.25)
-    t = r["fill_s"] + r["solve_s"]
+    cores = ref_baseline.pin_threads()
+    mw = ref_baseline.import_reference()
+    sol, ph = ref_baseline.time_solve(mw, kw)
     return {
-        "value": 1.0 / t,
+        "value": 1.0 / ph["total_s"],
         "unit": UNIT,
-        "cores": r["threads"],
+        "cores": cores,
         "kind": "reference",
-        "sample": (f"reference C++ fill kernels on {r['rows']}/{r['n_seg']} observer rows "
-                   f"(x{r['n_seg'] / r['rows']:.1f}) + LAPACK zgetrf/zgetrs on the leading "
-                   f"{r['lu_block']} block with {r['n_ports']} rhs (x(n/{r['lu_block']})^3 / ^2); "
-                   f"est. fill {r['fill_s']:.2f} s + solve {r['solve_s']:.2f} s"),
-        "fill_s": r["fill_s"],
-        "solve_s": r["solve_s"],
-    }
+        "sample": (f"one full reference compute_port_solution() of the workload (no extrapolation): fill "
+                   f"{ph['fill_s']:.2f} s + LU/solve {ph['solve_s']:.2f} s of {ph['total_s']:.2f} s, "
+                   f"OMP_NUM_THREADS=OPENBLAS_NUM_THREADS={cores}"),
+        "fill_s": ph["fill_s"],
+        "solve_s": ph["solve_s"],
+        "total_s": ph["total_s"],
+    }, sol
 
 
-def run_reference(args, kw):
+def run_reference(args):
+    """The reference arm: the reference's own public call on the same
+    workload, one full solve per step, on rank 0 (other ranks exit)."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
+    from oracle import ref_baseline
+
+    cores = ref_baseline.pin_threads()  # before numpy is imported
+    kw = load_workloads().dipole_array(args.nx, args.nx)
+    try:
+        mw = ref_baseline.import_reference()
+    except ImportError as e:
+        print(json.dumps({"impl": "reference", "unavailable": f"reference package not staged: {e}"}), flush=True)
+        return
     for _ in range(args.warmup):
-        cpu_baseline_sample(kw)
-    vals = []
+        ref_baseline.time_solve(mw, kw)
+    per = []
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        vals.append(cpu_baseline_sample(kw))
+        sol, ph = ref_baseline.time_solve(mw, kw)
+        per.append(ph)
     wall = time.perf_counter() - t0
-    per_step = sum(1.0 / v["value"] for v in vals) / len(vals)
+    per_step = sum(p["total_s"] for p in per) / len(per)
     value = 1.0 / per_step
-    base = vals[-1]
+    n_b = int(sol.coeffs.shape[0])
+    ports = int(sol.y.shape[0])
+    mapped = [p for p in ref_baseline.loaded_native_objects() if str(ROOT) in p]
     line = {
         "impl": "reference",
         "metric": METRIC,
@@ -178,12 +215,17 @@ def run_reference(args, kw):
         "vs_baseline": None,
         "dtype": "complex128",
         "data": "synthetic (seeded dipole array)",
-        "config": {"workload": WORKLOAD, "n_unknowns": base.get("n_basis", 10496), "ports": 256,
-                   "parallelism": "host threads"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": base["cores"], "kind": "reference",
-                         "sample": base["sample"]},
+        "config": workload_config(n_b, ports, args.nx),
+        "parallelism": f"host threads x{cores}",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                         "sample": (f"the full workload each step: reference BSplineSolver(...)."
+                                    f"compute_port_solution() with its C++ kernels (OpenMP) and LAPACK zgesv, "
+                                    f"OMP_NUM_THREADS=OPENBLAS_NUM_THREADS={cores}")},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "wall_s": wall,
+        "phases_s": {"fill": sum(p["fill_s"] for p in per) / len(per),
+                     "lu_solve": sum(p["solve_s"] for p in per) / len(per)},
+        "timed_wall_s": wall,
+        "native_objects_in_repo": mapped,
     }
     print(json.dumps(line), flush=True)
 
@@ -259,7 +301,8 @@ def run_b200(args, kw):
     # e2e through the public API: host tables in, coefficients + Y out
     e2e_ms = []
     h2d = d2h = 0
-    for i in range(args.e2e_steps + 1 if args.e2e_steps > 0 else 0):
+    e2e_steps = args.steps if args.e2e_steps is None else args.e2e_steps
+    for i in range(e2e_steps + 1 if e2e_steps > 0 else 0):
         s = momwire_b200.BSplineSolver(**kw, precision=args.precision, device=local)
         torch.cuda.synchronize()
         a = torch.cuda.Event(enable_timing=True)
@@ -359,11 +402,9 @@ def run_b200(args, kw):
         "vs_baseline": None,
         "dtype": "complex128" if args.precision == "fp64" else "complex64+fp64-refine",
         "data": "synthetic (seeded dipole array)",
-        "config": {"workload": WORKLOAD if args.nx == 16 else WORKLOAD.replace("16x16", f"{args.nx}x{args.nx}").replace(
-                       "256port", f"{buf['n_p']}port"),
-                   "n_unknowns": buf["n"], "ports": buf["n_p"], "precision": args.precision,
-                   "parallelism": f"replicas x{world}",
-                   "l2": f"inputs larger than L2 (Z = {buf['n'] ** 2 * 16 / 1e9:.2f} GB per step)"},
+        "config": workload_config(buf["n"], buf["n_p"], args.nx),
+        "precision": args.precision,
+        "parallelism": f"replicas x{world}",
         "e2e": {"value": world * 1e3 / e2e_step, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": e2e_step},
         "gpu_launches": int(launches),
@@ -377,7 +418,10 @@ def run_b200(args, kw):
         "sweep": sweep_part,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline_sample(kw)
+        cpu, ref_sol = cpu_baseline_full(kw)
+        line["cpu_baseline"] = cpu
+        # the timed GPU result against the reference's, run on this host
+        line["y_rel_err_vs_reference_run"] = float(np.max(np.abs(y_dev - ref_sol.y)) / np.max(np.abs(ref_sol.y)))
     if rank == 0:
         print(json.dumps(line), flush=True)
     if pg:
@@ -634,13 +678,12 @@ def main():
     if args.workload == "plate":
         run_plate(args)
         return
+    if args.impl == "reference":
+        run_reference(args)
+        return
     from momwire_b200.workloads import dipole_array
 
-    kw = dipole_array(args.nx, args.nx)
-    if args.impl == "reference":
-        run_reference(args, kw)
-    else:
-        run_b200(args, kw)
+    run_b200(args, dipole_array(args.nx, args.nx))
 
 
 if __name__ == "__main__":

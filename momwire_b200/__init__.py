@@ -4,7 +4,9 @@ B-spline Galerkin thin-wire solver.
 The public surface mirrors the reference package for this path:
 ``BSplineSolver`` (same constructor keywords), ``PortSolution``,
 ``CancelToken`` and ``SolveAborted``.  The heavy lifting runs in the native
-library ``libmomwire_b200.so`` (see ``include/momwire_b200.h``).
+library ``libmomwire_b200.so`` (see ``include/momwire_b200.h``).  Importing
+the package does not load that library; the first solve (or reading
+``accelerated``) does.
 """
 
 from ._port_solution import PortSolution
@@ -20,11 +22,19 @@ def _native_loaded() -> bool:
 
         _lib.load()
         return True
-    except (OSError, RuntimeError):
+    except (OSError, RuntimeError, ImportError):
         return False
 
 
-accelerated = _native_loaded()
+def __getattr__(name):
+    # ``accelerated`` is evaluated on first access, so that importing the
+    # package (for its workloads or tables) maps no native code.
+    if name == "accelerated":
+        value = _native_loaded()
+        globals()["accelerated"] = value
+        return value
+    raise AttributeError(f"module {__name__!r} has no attribute {name!r}")
+
 
 __all__ = ["BSplineSolver", "PortSolution", "CancelToken", "SolveAborted", "wire_internal_impedance",
            "insulation_inductance", "accelerated"]

@@ -4,10 +4,11 @@ suite, parsed and mapped onto a solver by the reference's OWN deck front end
 constructor keywords that front end passes to ``BSplineSolver`` recorded and
 the reference's multi-port solve of each deck stored beside them.
 
-Run in a container that has the reference source tree (default
-/root/reference) and its native kernels built by ``make -C oracle``:
+Run where the reference source tree is checked out (its root given by
+``--ref`` or ``$MOMWIRE_REF``) and its native kernels are built by
+``make -C oracle REF=<root>/src/momwire``:
 
-    python tests/golden/make_decks.py [--ref /root/reference]
+    python tests/golden/make_decks.py --ref <reference checkout>
 
 Writes ``decks.json`` (deck text, recorded keywords, port plan) and
 ``deck_<name>.npz`` (the reference's Y and port impedances) next to this
@@ -19,6 +20,7 @@ replay the recorded keywords into it.
 from __future__ import annotations
 
 import argparse
+import os
 import json
 import sys
 from pathlib import Path
@@ -115,8 +117,11 @@ def _jsonable(v):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("MOMWIRE_REF"),
+                    help="root of the reference checkout (default: $MOMWIRE_REF)")
     args = ap.parse_args()
+    if not args.ref:
+        ap.error("--ref (or $MOMWIRE_REF) is required")
     momwire = import_reference(Path(args.ref))
     from momwire import deck
     from momwire.deck import _solver as deck_solver

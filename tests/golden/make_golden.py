@@ -1,9 +1,10 @@
 """Generate golden vectors by running the reference momwire itself.
 
-Run in a container that has the reference source tree (default
-/root/reference) and its native kernels built by ``make -C oracle``:
+Run where the reference source tree is checked out (its root given by
+``--ref`` or ``$MOMWIRE_REF``) and its native kernels are built by
+``make -C oracle REF=<root>/src/momwire``:
 
-    python tests/golden/make_golden.py [--ref /root/reference] [--big]
+    python tests/golden/make_golden.py --ref <reference checkout> [--big]
 
 The reference package is copied to a temporary directory together with the
 compiled ``_accelerators`` module, imported from there, and every case in
@@ -128,10 +129,13 @@ def wire_impedance_table(momwire):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("MOMWIRE_REF"),
+                    help="root of the reference checkout (default: $MOMWIRE_REF)")
     ap.add_argument("--big", action="store_true")
     ap.add_argument("--only", default=None)
     args = ap.parse_args()
+    if not args.ref:
+        ap.error("--ref (or $MOMWIRE_REF) is required")
     momwire = import_reference(Path(args.ref))
     if args.only in (None, "wire_impedance"):
         np.savez_compressed(HERE / "wire_impedance.npz", **wire_impedance_table(momwire))

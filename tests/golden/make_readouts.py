@@ -1,11 +1,12 @@
 """Golden readouts: the reference's ``element_currents`` of its own first
 port column, for every full golden case.
 
-Run in a container that has the reference source tree (default
-/root/reference) and its native kernels built by ``make -C oracle``, after
+Run where the reference source tree is checked out (its root given by
+``--ref`` or ``$MOMWIRE_REF``) and its native kernels are built by
+``make -C oracle REF=<root>/src/momwire``, after
 ``make_golden.py`` (it reads the ``coeffs`` stored there):
 
-    python tests/golden/make_readouts.py [--ref /root/reference]
+    python tests/golden/make_readouts.py --ref <reference checkout>
 
 The readout is host-side arithmetic on a coefficient vector (no solve), so
 each case only constructs the reference's ``BSplineSolver``.  Writes
@@ -16,6 +17,7 @@ subdiv 1 and 3.
 from __future__ import annotations
 
 import argparse
+import os
 import sys
 from pathlib import Path
 
@@ -29,8 +31,11 @@ from make_golden import import_reference  # noqa: E402
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("MOMWIRE_REF"),
+                    help="root of the reference checkout (default: $MOMWIRE_REF)")
     args = ap.parse_args()
+    if not args.ref:
+        ap.error("--ref (or $MOMWIRE_REF) is required")
     momwire = import_reference(Path(args.ref))
     n = 0
     for name in sorted(CASES):

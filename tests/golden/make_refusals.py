@@ -2,9 +2,9 @@
 ``refusal_cases.py``, the exception type and text the reference's
 ``BSplineSolver`` raises (at construction, or at the solve for the cases it
 only refuses there).  Run where the reference and its native kernels (``make
--C oracle``) are available:
+-C oracle REF=...``) are available:
 
-    python tests/golden/make_refusals.py [--ref /root/reference]
+    python tests/golden/make_refusals.py --ref <reference checkout>
 
 Writes ``refusals.json`` next to this script.
 """
@@ -12,6 +12,7 @@ Writes ``refusals.json`` next to this script.
 from __future__ import annotations
 
 import argparse
+import os
 import json
 import sys
 from pathlib import Path
@@ -24,8 +25,11 @@ from refusal_cases import AT_SOLVE, REFUSALS  # noqa: E402
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("MOMWIRE_REF"),
+                    help="root of the reference checkout (default: $MOMWIRE_REF)")
     args = ap.parse_args()
+    if not args.ref:
+        ap.error("--ref (or $MOMWIRE_REF) is required")
     momwire = import_reference(Path(args.ref))
     out = {}
     for name, make in REFUSALS.items():

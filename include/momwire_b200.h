@@ -58,6 +58,15 @@ void mw_profile_enable(int32_t on);
 int32_t mw_profile_read(int32_t cls, int64_t* launches, double* total_ms,
                         double* flops, double* bytes);
 
+/* Failure-handling self-test (no counterpart in the reference, whose
+ * kernels have no device waits): runs one of this library's bounded device
+ * waits with a short limit and an event that never comes -- which = 0 the
+ * complex128 panel's grid barrier, 1 the tensor-core kernels' mbarrier
+ * wait -- and returns the status the wait recorded: MW_ERR_TIMEOUT when it
+ * gave up as designed (the context stays usable).  spin_limit in
+ * [256, 2^24]; workspace: 16 bytes of device memory; synchronises stream. */
+mw_status mw_selftest_wait_timeout(int32_t which, int64_t spin_limit, void* workspace, void* stream);
+
 /* Ground models served by the fill (bspline.py:182-287 ground kwargs). */
 #define MW_GROUND_NONE        0  /* free space                              */
 #define MW_GROUND_PEC         1  /* perfect image, ground_eps=None          */
@@ -219,18 +228,21 @@ mw_status mw_fill_z_image(const mw_segments* seg, const mw_basis* basis,
  * the library holds from load until exit.  This call allocates nothing.
  * Writes the same Z as mw_same_edge_table + mw_fill_z (Z32 not written).
  * Limits: at most mw_fill_z_noalloc_capacity(degree) table rows (32768 at
- * degree 2, 81920 at degree 1; a structure needs the sum over its straight
+ * degree 2, 73728 at degree 1; a structure needs the sum over its straight
  * edges of 2*n_segments - 1), otherwise MW_ERR_WORKSPACE.  All calls share
- * the array, so calls that overlap on the GPU race: serialise them.  The
- * first call on a device looks up the array's device address; make it
- * before any stream capture.
+ * the array, so calls that overlap on the GPU race: serialise them.  Each
+ * call outside stream capture looks up the array's device address on the
+ * current device (so a device reset or a non-primary context is picked
+ * up); a call during capture reuses the last address seen on that device,
+ * so make one call on each device before any stream capture.
  */
 mw_status mw_fill_z_noalloc(const mw_segments* seg, const mw_basis* basis,
                             const mw_edges* edges, const mw_freq* freq,
                             int32_t n_qp, int32_t extended_kernel,
                             double* Z, int64_t ldz, void* stream);
 
-/* Table rows mw_fill_z_noalloc can hold at this degree (0 if invalid). */
+/* Table rows mw_fill_z_noalloc can hold at this degree (0 unless the
+ * degree is 1 or 2). */
 size_t mw_fill_z_noalloc_capacity(int32_t degree);
 
 /*

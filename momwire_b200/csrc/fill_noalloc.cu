@@ -13,7 +13,7 @@
 //
 // Limits and sharing rules:
 //   * capacity: kNoallocTableDoubles doubles (4.5 MiB), i.e. 32768 table
-//     rows at degree 2 (81920 at degree 1); the number of rows a structure
+//     rows at degree 2 (73728 at degree 1); the number of rows a structure
 //     needs is the sum over its straight edges of 2*n_segments - 1, and a
 //     larger structure is rejected with MW_ERR_WORKSPACE;
 //   * every GPU that loads the library holds this array until the process
@@ -21,9 +21,12 @@
 //   * all calls share the one array: two calls whose work overlaps on the
 //     GPU (different streams, or different host threads on one device) race
 //     on it, so serialise them;
-//   * the first call on each device resolves the array's device address
-//     (cudaGetSymbolAddress) and remembers it; make that first call before
-//     any stream capture;
+//   * every call resolves the array's device address on the current device
+//     (cudaGetSymbolAddress) unless the stream is being captured, when the
+//     address remembered from the last uncaptured call on that device is
+//     used; make one call on each device before any stream capture.  A
+//     cudaDeviceReset, or a context other than the device's primary one,
+//     gets a fresh address on the next uncaptured call;
 //   * nothing needs to start at zero: every call overwrites the rows it
 //     reads.
 #include <mutex>
@@ -40,19 +43,28 @@ constexpr int kMaxDevices = 64;
 std::mutex g_noalloc_mu;
 double* g_noalloc_ptr[kMaxDevices] = {};
 
-// Device address of the array on the current device (resolved once per
-// device; host code cannot use the symbol's name as a device pointer).
-mw_status noalloc_table_ptr(double** out) {
+// Device address of the array on the current device.  Host code cannot use
+// the symbol's name as a device pointer, so the runtime is asked for it on
+// every call (cheap) -- a cached address could outlive its context after a
+// device reset.  While `stream` is capturing, the runtime may not be queried
+// in ways that break the capture, so the address remembered from the last
+// uncaptured call on this device is used.
+mw_status noalloc_table_ptr(void* stream, double** out) {
     int dev = 0;
     MW_CHECK_CUDA(cudaGetDevice(&dev));
     MW_REQUIRE(dev >= 0 && dev < kMaxDevices, "device ordinal %d out of range", dev);
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    MW_CHECK_CUDA(cudaStreamIsCapturing(static_cast<cudaStream_t>(stream), &cap));
     std::lock_guard<std::mutex> g(g_noalloc_mu);
-    if (g_noalloc_ptr[dev] == nullptr) {
+    if (cap == cudaStreamCaptureStatusNone) {
         void* p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_table);
         if (e != cudaSuccess) return mw::cuda_status(e, "cudaGetSymbolAddress(g_noalloc_table)");
         g_noalloc_ptr[dev] = static_cast<double*>(p);
     }
+    MW_REQUIRE(g_noalloc_ptr[dev] != nullptr,
+               "mw_fill_z_noalloc: the first call on device %d was made during stream capture; make one call "
+               "before capturing", dev);
     *out = g_noalloc_ptr[dev];
     return MW_OK;
 }
@@ -60,8 +72,9 @@ mw_status noalloc_table_ptr(double** out) {
 }  // namespace
 
 extern "C" size_t mw_fill_z_noalloc_capacity(int32_t degree) {
+    if (degree != 1 && degree != 2) return 0;
     size_t per_row = (size_t)(degree + 1) * (degree + 1) * 2;
-    return degree >= 1 ? kNoallocTableDoubles / per_row : 0;
+    return kNoallocTableDoubles / per_row;
 }
 
 extern "C" mw_status mw_fill_z_noalloc(const mw_segments* seg, const mw_basis* basis, const mw_edges* edges,
@@ -77,7 +90,7 @@ extern "C" mw_status mw_fill_z_noalloc(const mw_segments* seg, const mw_basis* b
         return MW_ERR_WORKSPACE;
     }
     double* table = nullptr;
-    mw_status s = noalloc_table_ptr(&table);
+    mw_status s = noalloc_table_ptr(stream, &table);
     if (s != MW_OK) return s;
     s = mw_same_edge_table(edges, basis->degree, n_qp, extended_kernel, freq->k, table, stream);
     if (s != MW_OK) return s;

@@ -64,6 +64,10 @@ def test_noalloc_rejects_oversized_table(cuda_device):
     dt = s._dev_tables()
     cap = lib.mw_fill_z_noalloc_capacity(s.degree)
     assert cap == 32768
+    # 4.5 MiB of doubles: 8 per row at degree 1, 18 at degree 2; no other
+    # degree is served
+    assert lib.mw_fill_z_noalloc_capacity(1) == 73728
+    assert [lib.mw_fill_z_noalloc_capacity(d) for d in (-1, 0, 3, 4)] == [0, 0, 0, 0]
     edges = _lib.Edges.from_buffer_copy(dt.edges)
     edges.table_rows = cap + 1  # rejected on the host, before any launch
     fr = _lib.Freq(float(s.k), float(s.omega), float(s.eps), float(s.mu))

@@ -115,6 +115,7 @@ _SIGS = {
     "mw_launch_count": (i64, []),
     "mw_profile_enable": (None, [i32]),
     "mw_profile_read": (i32, [i32, C.POINTER(i64), C.POINTER(f64), C.POINTER(f64), C.POINTER(f64)]),
+    "mw_selftest_wait_timeout": (i32, [i32, i64, vp, vp]),
     "mw_same_edge_table": (i32, [C.POINTER(Edges), i32, i32, i32, f64, vp, vp]),
     "mw_offedge_moments": (i32, [C.POINTER(Segments), C.POINTER(Segments), i32, i32, f64, i32, f64, vp, vp, vp, vp]),
     "mw_fill_z": (i32, [C.POINTER(Segments), C.POINTER(BasisT), vp, C.POINTER(Edges), C.POINTER(Freq), i32, vp, i64, vp, i64, vp]),

@@ -23,6 +23,7 @@
 #include <type_traits>
 
 #include "common.cuh"
+#include "waits.cuh"
 
 namespace mw {
 
@@ -35,46 +36,6 @@ constexpr int kNB = 64;         // panel half width (rank-1 work per cooperative
 constexpr int kOuterNB = 128;   // getrf block: panel width and trailing-update k
 constexpr int kPanelMaxJb = 128;
 constexpr int kPanelThreads = 256;
-
-struct PanelWs {
-    unsigned int counter;  // grid barrier arrivals
-    int err;               // device status (MW_ERR_TIMEOUT)
-    int pad[2];
-};
-
-__device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
-    unsigned int v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-
-// Bounded grid barrier; returns false (for every thread of the CTA) when
-// the wait gave up, after recording MW_ERR_TIMEOUT.
-__device__ bool grid_sync_bounded(PanelWs* ws, unsigned int target) {
-    __shared__ int s_ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        // the release add publishes every write the CTA made before the
-        // __syncthreads above (cumulativity); the acquire loads order the
-        // reads that follow the barrier
-        asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(&ws->counter) : "memory");
-        int ok = 1;
-        long long spins = 0;
-        while (ld_acquire(&ws->counter) < target) {
-            if ((++spins & 255) == 0) {
-                if (*(volatile int*)&ws->err) { ok = 0; break; }
-                if (spins > (1ll << 26)) {
-                    atomicExch(&ws->err, MW_ERR_TIMEOUT);
-                    ok = 0;
-                    break;
-                }
-            }
-        }
-        s_ok = ok;
-    }
-    __syncthreads();
-    return s_ok != 0;
-}
 
 __device__ __forceinline__ cd ldcg_c(const cd* p) {
     double2 v = __ldcg(reinterpret_cast<const double2*>(p));

@@ -32,10 +32,11 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     return ok != 0;
 }
 
-// Bounded wait; returns false (and raises the error word) on a timeout or
-// when another role has already given up.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
-    for (long long it = 0; it < TC_SPIN_LIMIT; ++it) {
+// Bounded wait; returns false (and raises the error word) on a timeout --
+// `limit` polls -- or when another role has already given up.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err,
+                                          long long limit = TC_SPIN_LIMIT) {
+    for (long long it = 0; it < limit; ++it) {
         if (mbar_try_wait(bar, parity)) return true;
         if ((it & 1023) == 1023 && *(volatile int*)err) return false;
     }

@@ -240,6 +240,7 @@ class Basis:
     supp: np.ndarray  # (n_b, d+1) int32, -1 = padded wing
     polys: np.ndarray  # (n_b, d+1, d+1)
     kcl_A: "scipy.sparse.csr_matrix"  # (n_c, n_b) KCL rows, entries +-1
+    kcl_junction: np.ndarray  # (n_c,) int64: the junction of each KCL row (ascending)
     knots: list  # per wire
     kept: KeptBases  # per wire: list of (j_local, kind, junction, end, m_global)
 
@@ -248,9 +249,12 @@ class Basis:
         return int(self.supp.shape[0])
 
 
-def build_basis(geom: Geometry, degree, start_status, end_status, n_junctions, grounded) -> Basis:
+def build_basis(geom: Geometry, degree, ends, n_junctions, grounded) -> Basis:
     """Clamped knot vector per wire; keep interior bases plus the value-1
-    end basis at junction / ground ends; per-wing monomial coefficients in
+    end basis at junction / ground ends (``ends``: the (n_wires, 2) table of
+    end holders of ``_topology.end_table`` -- junction index, FREE or
+    GROUND); one KCL row per junction off the ground, in junction order;
+    per-wing monomial coefficients in
     local arc length from values at d+1 uniform points (the reference's
     design-matrix + Vandermonde step, ``bspline.py:1318-1414``), computed by
     the native host routine ``mw_basis_polys``: segment s of a wire reads the
@@ -263,14 +267,16 @@ def build_basis(geom: Geometry, degree, start_status, end_status, n_junctions, g
     arcs = geom.wire_arc
     knots_all = [np.concatenate([np.zeros(d), arc, np.full(d, arc[-1])]) for arc in arcs]
     # ---- kept bases: interior bases, plus end bases a junction / ground holds
-    def end_kind(status):
-        if status == "ground":
-            return ("gnd", None)
-        if status != "free":
-            return ("dir", status)
-        return None
+    from ._topology import FREE, GROUND
 
-    ends = [(end_kind(start_status[w]), end_kind(end_status[w])) for w in range(n_wires)]
+    def end_kind(code):
+        if code == GROUND:
+            return ("gnd", None)
+        if code == FREE:
+            return None
+        return ("dir", int(code))
+
+    ends = [(end_kind(ends[w, 0]), end_kind(ends[w, 1])) for w in range(n_wires)]
     has_s = np.fromiter((e[0] is not None for e in ends), dtype=np.int64, count=n_wires)
     has_e = np.fromiter((e[1] is not None for e in ends), dtype=np.int64, count=n_wires)
     n_kept = (wire_n + d - 2) + has_s + has_e
@@ -314,6 +320,7 @@ def build_basis(geom: Geometry, degree, start_status, end_status, n_junctions, g
         supp=supp,
         polys=poly,
         kcl_A=kcl,
+        kcl_junction=np.asarray(rows, dtype=np.int64),
         knots=knots_all,
         kept=KeptBases(ends, wire_n + d, m_first),
     )

@@ -30,6 +30,8 @@ import scipy.sparse
 
 from . import _lib
 from . import _tables as T
+from . import _topology as topo
+from . import _validate as V
 from . import autotune
 from . import loading as wl
 from . import sommerfeld as somm
@@ -243,35 +245,21 @@ class BSplineSolver:
         sommerfeld_method="grid",
     ):
         self._cancel = cancel
-        if degree < 1:
-            raise ValueError(f"degree must be >= 1, got {degree}")
-        if degree > 2:
-            raise NotImplementedError(
-                "degree > 2 needs scripts/derive_bspline_static_moments.py "
-                "to be re-run with a larger MAX_D"
-            )
-        if not wires:
-            raise ValueError("wires must be non-empty")
-        if use_singular_enrichment:
-            raise NotImplementedError(_ENRICHMENT_REFUSAL)
-        # the enrichment settings are taken and kept (their consumers read
-        # them) with the reference's validation (``bspline.py:793-838``)
+        V.settings(dict(degree=degree, wires=wires, use_singular_enrichment=use_singular_enrichment,
+                        enrichment_refusal=_ENRICHMENT_REFUSAL, enrichment_variant=enrichment_variant,
+                        precision=precision, sommerfeld_method=sommerfeld_method, ground_eps=ground_eps,
+                        ground_z=ground_z, ground_phi_mode=ground_phi_mode, phi_modes=_lib.PHI_MODES,
+                        ground_model=ground_model, swept_mem_mb=swept_mem_mb, feed_model=feed_model,
+                        feed_smoothing_factor=feed_smoothing_factor))
+        # the enrichment settings are kept (their consumers read them);
+        # enrichment itself is not served
         self.use_singular_enrichment = False
         self.n_qp_sing = int(n_qp_sing)
         self.enrichment_min_k = int(enrichment_min_k)
-        if enrichment_variant not in ("raw", "stable", "tikhonov", "auto"):
-            raise ValueError(
-                f"enrichment_variant must be one of 'raw', 'stable', "
-                f"'tikhonov', 'auto', got {enrichment_variant!r}"
-            )
         self.enrichment_variant = enrichment_variant
         self.tikhonov_lambda = float(tikhonov_lambda)
         self.auto_tap_ratio_threshold = float(auto_tap_ratio_threshold)
-        if precision not in ("fp64", "mixed"):
-            raise ValueError(f"precision must be 'fp64' or 'mixed', got {precision!r}")
         self.precision = precision
-        if sommerfeld_method not in ("grid", "surrogate"):
-            raise ValueError(f"sommerfeld_method must be 'grid' or 'surrogate', got {sommerfeld_method!r}")
         self.sommerfeld_method = sommerfeld_method
         self.last_sommerfeld = None
         # mixed: stop refining once the largest relative correction of any
@@ -286,182 +274,53 @@ class BSplineSolver:
         self.wire_radius = wire_radius
         self.nsegs = nsegs
         self.ground_z = ground_z
-        if ground_eps is not None and ground_z is None:
-            raise ValueError("ground_eps requires ground_z to be set")
-        if ground_phi_mode not in _lib.PHI_MODES:
-            raise ValueError(
-                f"ground_phi_mode must be one of {tuple(_lib.PHI_MODES)}, got {ground_phi_mode!r}"
-            )
         self.ground_eps = ground_eps
         self.ground_phi_mode = ground_phi_mode
-        if ground_model not in ("refl-coef", "sommerfeld"):
-            raise ValueError(f"ground_model must be 'refl-coef' or 'sommerfeld', got {ground_model!r}")
-        if ground_model == "sommerfeld" and ground_eps is None:
-            raise ValueError("ground_model='sommerfeld' requires ground_eps")
         self.ground_model = ground_model
         self.n_qp_sommerfeld = int(n_qp_sommerfeld)
         self.extended_kernel = bool(extended_kernel)
         self.swept_mem_mb = int(swept_mem_mb)
-        if self.swept_mem_mb < 1:
-            raise ValueError(f"swept_mem_mb must be >= 1, got {swept_mem_mb}")
-        if feed_model not in ("point", "segment"):
-            raise ValueError(f"feed_model must be 'point' or 'segment', got {feed_model!r}")
-        if feed_model == "segment" and feed_smoothing_factor is not None:
-            raise ValueError(
-                "feed_model='segment' and feed_smoothing_factor are mutually "
-                "exclusive — both replace the point drive with a spread one"
-            )
         self.feed_model = feed_model
         self.feed_smoothing_factor = feed_smoothing_factor
         self.n_qp_source = int(n_qp_source)
 
+        # wavenumber from the solver's own c = 1 / sqrt(eps mu)
         self.c = 1 / np.sqrt(self.eps * self.mu)
         self.freq = self.c / self.wavelength
         self.omega = 2 * np.pi * self.freq
         self.k = self.omega / self.c
         self.halfdriver = self.halfdriver_factor * self.wavelength / 4
 
-        self.wires_polylines = [np.asarray(w, dtype=float) for w in wires]
-        for i, pl in enumerate(self.wires_polylines):
-            if pl.ndim != 2 or pl.shape[0] < 2 or pl.shape[1] != 3:
-                raise ValueError(f"wire {i}: polyline must be (M, 3) with M >= 2")
+        self.wires_polylines = V.polylines(wires)
         n_w = len(self.wires_polylines)
         if self.ground_eps is not None and self.ground_model == "refl-coef":
             touching = self._contact_ends()
             if touching:
                 where = ", ".join(f"wire {w} {kind}" for w, kind in touching)
                 raise NotImplementedError(f"{where} lies in the ground plane: {_CONTACT_REFUSAL}")
-        r = np.asarray(wire_radius, dtype=float)
-        if r.ndim == 0:
-            r = np.full(n_w, float(r))
-        elif r.shape != (n_w,):
-            raise ValueError(
-                f"wire_radius: expected a scalar or a length-{n_w} sequence "
-                f"(one entry per wire), got shape {r.shape}"
-            )
-        if not np.all(np.isfinite(r)) or np.any(r <= 0.0):
-            raise ValueError(f"wire_radius entries must be positive and finite, got {r}")
-        self._radius_per_wire = r
+        self._radius_per_wire = V.radii(wire_radius, n_w)
         # distributed series loading (bspline.py:715-728): None when off
-        self._loading = wl.configure(n_w, r, wire_conductivity, insulation_radius, insulation_eps_r)
+        self._loading = wl.configure(n_w, self._radius_per_wire, wire_conductivity, insulation_radius,
+                                     insulation_eps_r)
         self.wire_conductivity = None if self._loading is None else self._loading.conductivity
         self.insulation_radius = None if self._loading is None else self._loading.insulation_radius
         self.insulation_eps_r = None if self._loading is None else self._loading.insulation_eps_r
         self._cached_loading = None
         self._cached_loading_dev = None
+        self.n_per_edge_per_wire = V.edge_counts(self.wires_polylines, n_per_edge_per_wire, self.nsegs)
 
-        if n_per_edge_per_wire is None:
-            n_per_edge_per_wire = [None] * n_w
-        if len(n_per_edge_per_wire) != n_w:
-            raise ValueError(f"n_per_edge_per_wire length {len(n_per_edge_per_wire)} != n_wires {n_w}")
-        self.n_per_edge_per_wire = []
-        for i, (pl, npe) in enumerate(zip(self.wires_polylines, n_per_edge_per_wire)):
-            n_edges_w = pl.shape[0] - 1
-            if npe is None:
-                npe = self.nsegs
-            if np.isscalar(npe):
-                npe = [int(npe)] * n_edges_w
-            npe = list(npe)
-            if len(npe) != n_edges_w:
-                raise ValueError(f"wire {i}: n_per_edge length {len(npe)} != n_edges {n_edges_w}")
-            self.n_per_edge_per_wire.append(npe)
-
-        if feeds is None:
-            if not (0 <= feed_wire_index < n_w):
-                raise ValueError(f"feed_wire_index {feed_wire_index} out of range")
-            self.feeds = [(int(feed_wire_index), feed_arclength, 1.0 + 0.0j)]
-        else:
-            if len(feeds) == 0 and not junction_ports and not node_gaps:
-                raise ValueError("feeds must contain at least one entry")
-            norm = []
-            for i, f in enumerate(feeds):
-                if len(f) != 3:
-                    raise ValueError(f"feeds[{i}]: expected (wire_index, arclength, voltage), got {f!r}")
-                w_i, arc_i, v_i = f
-                if not (0 <= w_i < n_w):
-                    raise ValueError(f"feeds[{i}]: wire_index {w_i} out of range [0, {n_w})")
-                arc_i = None if arc_i is None else float(arc_i)
-                norm.append((int(w_i), arc_i, complex(v_i)))
-            self.feeds = norm
+        # the port and connection keywords: entry by entry against ordered
+        # rule tables (the reference's refusal texts and order)
+        self.feeds = V.feeds(feeds, n_w, feed_wire_index, feed_arclength, bool(junction_ports) or bool(node_gaps))
         self.feed_wire_index = self.feeds[0][0] if self.feeds else None
         self.feed_arclength = self.feeds[0][1] if self.feeds else None
         # checked where the reference's quadrature first uses it: at the
         # solve (``_dev_tables``), with the reference's exception and text
         self.n_qp_pair = int(n_qp_pair)
-
-        self.junctions = []
-        if junctions is not None:
-            for j, jw in enumerate(junctions):
-                if len(jw) < 1:
-                    raise ValueError(f"junction {j}: need >= 1 wire-end")
-                normalized = []
-                for w, end in jw:
-                    if not (0 <= w < n_w):
-                        raise ValueError(f"junction {j}: wire_idx {w} out of range [0, {n_w})")
-                    if end not in ("start", "end"):
-                        raise ValueError(f"junction {j}: end must be 'start' or 'end', got {end!r}")
-                    normalized.append((int(w), end))
-                self.junctions.append(normalized)
-            self._check_junction_coincidence()
-
-        self.junction_ports = []
-        if junction_ports is not None:
-            seen = set()
-            for p in junction_ports:
-                if isinstance(p, (int, np.integer)):
-                    j_idx, volt = int(p), 0j
-                else:
-                    j_idx, volt = int(p[0]), complex(p[1])
-                if not (0 <= j_idx < len(self.junctions)):
-                    raise ValueError(
-                        f"junction_ports: junction index {j_idx} out of range [0, {len(self.junctions)})"
-                    )
-                if j_idx in seen:
-                    raise ValueError(f"junction_ports: junction {j_idx} listed twice")
-                seen.add(j_idx)
-                self.junction_ports.append((j_idx, volt))
-
-        self.node_gaps = []
-        if node_gaps is not None:
-            end_to_junction = {m: j for j, jw in enumerate(self.junctions) for m in jw}
-            seen_m, seen_j = set(), set()
-            ported = {j for j, _v in self.junction_ports}
-            for i, g in enumerate(node_gaps):
-                if len(g) != 3:
-                    raise ValueError(
-                        f"node_gaps[{i}]: expected (wire_index, 'start'|'end', voltage), got {g!r}"
-                    )
-                w_i, end_i, v_i = g
-                if not (0 <= w_i < n_w):
-                    raise ValueError(f"node_gaps[{i}]: wire_index {w_i} out of range [0, {n_w})")
-                if end_i not in ("start", "end"):
-                    raise ValueError(f"node_gaps[{i}]: end must be 'start' or 'end', got {end_i!r}")
-                member = (int(w_i), end_i)
-                j_idx = end_to_junction.get(member)
-                if j_idx is None:
-                    raise ValueError(
-                        f"node_gaps[{i}]: wire {w_i} {end_i!r} is not a member of any junction group — a "
-                        "series node gap lives at a junction; for a feed inside a wire use feeds="
-                    )
-                if len(self.junctions[j_idx]) < 2:
-                    raise ValueError(
-                        f"node_gaps[{i}]: junction {j_idx} has a single member — there is no "
-                        "through-current path to be in series with (a lone-end attachment is junction_ports=)"
-                    )
-                if member in seen_m:
-                    raise ValueError(f"node_gaps[{i}]: wire {w_i} {end_i!r} listed twice")
-                if j_idx in seen_j:
-                    raise ValueError(
-                        f"node_gaps[{i}]: junction {j_idx} already carries a node gap — one series gap per junction"
-                    )
-                if j_idx in ported:
-                    raise ValueError(
-                        f"node_gaps[{i}]: junction {j_idx} is also a junction port — the shunt and series "
-                        "ports of one node cannot be driven together yet"
-                    )
-                seen_m.add(member)
-                seen_j.add(j_idx)
-                self.node_gaps.append((int(w_i), end_i, complex(v_i)))
+        self.junctions = V.junctions(junctions, n_w)
+        V.junction_anchor_check(self.junctions, self.wires_polylines, self.n_per_edge_per_wire)
+        self.junction_ports = V.junction_ports(junction_ports, len(self.junctions))
+        self.node_gaps = V.node_gaps(node_gaps, n_w, self.junctions, self.junction_ports)
 
         self._device = device
         self._cached_geometry = None
@@ -489,29 +348,6 @@ class BSplineSolver:
                 out.append((i, "end"))
         return tuple(sorted(out))
 
-    def _check_junction_coincidence(self):
-        """``_wire_spec.check_junction_coincidence`` (reference ``_wire_spec.py:62``)."""
-        for j, group in enumerate(self.junctions):
-            anchors, lens = [], []
-            for w, end in group:
-                pl = self.wires_polylines[w]
-                npe = self.n_per_edge_per_wire[w]
-                if end == "start":
-                    anchor, edge, count = pl[0], pl[1] - pl[0], npe[0]
-                else:
-                    anchor, edge, count = pl[-1], pl[-1] - pl[-2], npe[-1]
-                anchors.append(anchor)
-                lens.append(float(np.linalg.norm(edge)) / max(int(count), 1))
-            tol = max(1e-5, 1e-3 * min(lens))
-            w0, e0 = group[0]
-            for (w, e), a in zip(group[1:], anchors[1:]):
-                dist = float(np.linalg.norm(a - anchors[0]))
-                if dist > tol:
-                    raise ValueError(
-                        f"junction {j}: wire {w} {e!r} is {dist:.6g} from wire {w0} {e0!r} "
-                        f"(tolerance {tol:.3g}) — junction members must coincide"
-                    )
-
     def _set_k(self, kk):
         self.k = float(kk)
         self.omega = self.k * self.c
@@ -526,51 +362,19 @@ class BSplineSolver:
             self.k, self.wavelength, self.omega = saved
 
     # ------------------------------------------------------------ topology
+    def _end_table(self):
+        """(n_wires, 2) end holders: junction index, FREE or GROUND
+        (``_topology.end_table``; ``bspline.py:1108-1150``)."""
+        return topo.end_table(self.wires_polylines, self.junctions, self.ground_z)
+
     def _wire_endpoint_status(self):
-        """``bspline.py:1108-1150``."""
-        n_w = len(self.wires_polylines)
-        st = ["free"] * n_w
-        en = ["free"] * n_w
-        for j, jw in enumerate(self.junctions):
-            for w, end in jw:
-                if end == "start":
-                    st[w] = j
-                else:
-                    en[w] = j
-        gz = self.ground_z
-        if gz is not None:
-            for w, pl in enumerate(self.wires_polylines):
-                tol = T.touch_tol(pl)
-                if float(pl[:, 2].min()) < gz - tol:
-                    raise ValueError(
-                        f"wire {w} dips below the ground plane "
-                        f"(min z = {pl[:, 2].min():.6g} < ground_z = {gz:g})"
-                    )
-                at = np.abs(pl[:, 2] - gz) <= tol
-                if np.any(at[:-1] & at[1:]):
-                    raise ValueError(
-                        f"wire {w} has an edge lying in the ground plane "
-                        "(both endpoints at ground_z) — degenerate over a conducting ground"
-                    )
-                if st[w] == "free" and at[0]:
-                    st[w] = "ground"
-                if en[w] == "free" and at[-1]:
-                    en[w] = "ground"
-        return st, en
+        """Per-wire start and end labels (junction index, "free" or
+        "ground"), the reference's ``_wire_endpoint_status`` view."""
+        return topo.end_status(self._end_table())
 
     def _grounded_junctions(self):
         """``bspline.py:1152-1169``."""
-        gz = self.ground_z
-        if gz is None or not self.junctions:
-            return frozenset()
-        out = set()
-        for j, jw in enumerate(self.junctions):
-            w, end = jw[0]
-            pl = self.wires_polylines[w]
-            pt = pl[0] if end == "start" else pl[-1]
-            if abs(pt[2] - gz) <= T.touch_tol(pl):
-                out.add(j)
-        return frozenset(out)
+        return topo.grounded_junctions(self.wires_polylines, self.junctions, self.ground_z)
 
     def _geometry(self) -> T.Geometry:
         if self._cached_geometry is None:
@@ -581,9 +385,8 @@ class BSplineSolver:
 
     def _basis(self) -> T.Basis:
         if self._cached_basis is None:
-            st, en = self._wire_endpoint_status()
             self._cached_basis = T.build_basis(
-                self._geometry(), self.degree, st, en, len(self.junctions), self._grounded_junctions()
+                self._geometry(), self.degree, self._end_table(), len(self.junctions), self._grounded_junctions()
             )
         return self._cached_basis
 
@@ -620,27 +423,10 @@ class BSplineSolver:
 
     # --------------------------------------------------------------- ports
     def _split_kcl_ports(self, kcl_A):
-        """``bspline.py:1171-1214``."""
-        if not self.junction_ports:
-            return kcl_A, scipy.sparse.csr_matrix((0, kcl_A.shape[1])), np.zeros(0, dtype=np.complex128)
-        grounded = self._grounded_junctions()
-        row_of, row = {}, 0
-        for j in range(len(self.junctions)):
-            if j not in grounded:
-                row_of[j] = row
-                row += 1
-        port_rows = []
-        for j_idx, _v in self.junction_ports:
-            if j_idx in grounded:
-                raise ValueError(
-                    f"junction {j_idx} is both grounded and a junction port — a grounded node's "
-                    "voltage is pinned by the ground image, so it cannot also be a driven port"
-                )
-            port_rows.append(row_of[j_idx])
-        port_set = set(port_rows)
-        keep = [r for r in range(kcl_A.shape[0]) if r not in port_set]
-        port_V = np.array([v for _j, v in self.junction_ports], dtype=np.complex128)
-        return kcl_A[keep, :], kcl_A[port_rows, :], port_V
+        """(constraint rows, port rows, port voltages) of this solver's KCL
+        rows ``kcl_A`` (``bspline.py:1171-1214``)."""
+        return topo.split_kcl_ports(kcl_A, self._basis().kcl_junction, self.junction_ports,
+                                    self._grounded_junctions())
 
     def _source_entries(self, w, s_f):
         """Nonzeros (basis indices, values) of the Galerkin drive column of
@@ -1101,8 +887,8 @@ class BSplineSolver:
         precomputed same-edge moments for sweeps) is accepted for signature
         compatibility and unused: the device builds its same-edge table at
         each call for a fraction of a millisecond."""
-        torch = _torch()
         self._checkpoint()
+        torch = _torch()
         geom, basis = self._geometry(), self._basis()
         buf = self._alloc()
         st = torch.cuda.current_stream(buf["Z"].device).cuda_stream
@@ -1171,6 +957,7 @@ class BSplineSolver:
         launch and factorised together (``_swept_batched``); otherwise each
         k takes the single-solve path."""
         k_array = np.asarray(k_array, dtype=float)
+        self._checkpoint()
         if self._swept_batched_available():
             return self._swept_batched(k_array)
         n_p = self._port_count()
@@ -1193,10 +980,9 @@ class BSplineSolver:
         ground holds (the rule of ``_tables.build_basis``)."""
         if self._cached_basis is not None:
             return self._basis().n
-        st, en = self._wire_endpoint_status()
-        d = self.degree
-        return int(sum(sum(npe) + d - 2 + (st[w] != "free") + (en[w] != "free")
-                       for w, npe in enumerate(self.n_per_edge_per_wire)))
+        held = int(np.count_nonzero(self._end_table() != topo.FREE))
+        segs = sum(sum(npe) for npe in self.n_per_edge_per_wire)
+        return int(segs + (self.degree - 2) * len(self.n_per_edge_per_wire) + held)
 
     def _kcl_rows_left(self):
         """KCL constraint rows that stay after the junction-port split: one
@@ -1292,6 +1078,7 @@ class BSplineSolver:
         out = np.zeros((len(k_array), n_p, n_p), dtype=np.complex128)
         iters = []
         for c0 in range(0, len(k_array), chunk):
+            self._checkpoint()
             ks = np.asarray(k_array[c0 : c0 + chunk], dtype=np.float64)
             nk = len(ks)
             Z, Z32 = self._fill_batched(ks, st)

@@ -31,8 +31,43 @@ REFUSALS = {
     "enrichment_settings_with_enrichment_off": lambda: dict(wires=_D, n_qp_sing=16, enrichment_min_k=4,
                                                             enrichment_variant="stable", tikhonov_lambda=1e-2,
                                                             auto_tap_ratio_threshold=0.5),
+    # the port and connection keywords, entry by entry
+    "feeds_empty": lambda: dict(wires=_D, feeds=[]),
+    "feeds_empty_with_junction_port": lambda: dict(wires=_V, junctions=[[(0, "start"), (1, "start")]], feeds=[],
+                                                   junction_ports=[0]),
+    "feed_arity": lambda: dict(wires=_D, feeds=[(0, None)]),
+    "feed_second_entry_bad": lambda: dict(wires=_Y, feeds=[(0, None, 1.0), (1, None, 1.0, 0.0)]),
+    "feed_wire_index_out_of_range": lambda: dict(wires=_D, feed_wire_index=3),
+    "junction_group_empty": lambda: dict(wires=_V, junctions=[[(0, "start"), (1, "start")], []]),
+    "junction_members_apart": lambda: dict(wires=_V, junctions=[[(0, "start"), (1, "end")]]),
+    "junction_members_apart_third": lambda: dict(wires=_V + [np.array([[0, 0, 0.0], [0, 1, 1.0]])],
+                                                 junctions=[[(0, "start"), (2, "start"), (1, "end")]]),
+    "junction_port_listed_twice": lambda: dict(wires=_V, junctions=[[(0, "start"), (1, "start")]],
+                                               junction_ports=[0, (0, 1.0)]),
+    "node_gap_arity": lambda: dict(wires=_V, junctions=[[(0, "start"), (1, "start")]], node_gaps=[(0, "start")]),
+    "node_gap_end_unknown": lambda: dict(wires=_V, junctions=[[(0, "start"), (1, "start")]],
+                                         node_gaps=[(0, "middle", 1.0)]),
+    "node_gap_not_at_junction": lambda: dict(wires=_V, junctions=[[(0, "start"), (1, "start")]],
+                                             node_gaps=[(0, "end", 1.0)]),
+    "node_gap_single_member": lambda: dict(wires=_V, junctions=[[(0, "start")]], node_gaps=[(0, "start", 1.0)]),
+    "node_gap_member_twice": lambda: dict(wires=_V, junctions=[[(0, "start"), (1, "start")]],
+                                          node_gaps=[(0, "start", 1.0), (0, "start", 1.0)]),
+    "node_gap_junction_twice": lambda: dict(wires=_V, junctions=[[(0, "start"), (1, "start")]],
+                                            node_gaps=[(0, "start", 1.0), (1, "start", 1.0)]),
+    "node_gap_at_junction_port": lambda: dict(wires=_V, junctions=[[(0, "start"), (1, "start")]],
+                                              junction_ports=[0], node_gaps=[(1, "start", 1.0)]),
     # refused at the solve, not by the constructor
     "pair_quadrature_0": lambda: dict(wires=_D, nsegs=21, wavelength=21.0, n_qp_pair=0),
     "pair_quadrature_9": lambda: dict(wires=_D, nsegs=21, wavelength=21.0, n_qp_pair=9),
+    "wire_below_ground": lambda: dict(wires=_Y, nsegs=21, wavelength=21.0, ground_z=0.0),
+    "edge_in_ground_plane": lambda: dict(wires=[np.array([[0, 0, 0.0], [1, 0, 0.0], [1, 0, 2.0]])], nsegs=11,
+                                         wavelength=21.0, ground_z=0.0),
+    "grounded_junction_port": lambda: dict(wires=_V, nsegs=11, wavelength=21.0, ground_z=0.0,
+                                           junctions=[[(0, "start"), (1, "start")]], junction_ports=[0]),
+    "second_junction_port_grounded": lambda: dict(
+        wires=_V + [np.array([[0, 0, 2.0], [0, 0, 1.0]]), np.array([[0, 0, 2.0], [0, 1, 3.0]])], nsegs=11,
+        wavelength=21.0, ground_z=0.0, junctions=[[(2, "start"), (3, "start")], [(0, "start"), (1, "start")]],
+        junction_ports=[0, 1]),
 }
-AT_SOLVE = {"pair_quadrature_0", "pair_quadrature_9"}
+AT_SOLVE = {"pair_quadrature_0", "pair_quadrature_9", "wire_below_ground", "edge_in_ground_plane",
+            "grounded_junction_port", "second_junction_port_grounded"}

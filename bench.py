@@ -353,6 +353,7 @@ def run_b200(args, kw):
     # update on the mixed path (the LU panel, often as long, is latency-
     # bound -- one cross-CTA pivot exchange per column -- and reported
     # beside it), the dominant kernel class otherwise
+    walls = {k: prof.pop(k) for k in ("factor_wall", "solve_wall") if k in prof}
     by_time = max(prof.items(), key=lambda kv: kv[1][1]) if prof else None
     dom = ("cgemm_tc", prof["cgemm_tc"]) if "cgemm_tc" in prof else by_time
     roof = None
@@ -388,6 +389,37 @@ def run_b200(args, kw):
     breakdown = {k: {"launches": v[0] / args.steps, "ms_per_step": v[1] / args.steps,
                      "tflops": (v[2] / (v[1] / 1e3) / 1e12) if v[1] > 0 and v[2] > 0 else None}
                  for k, v in prof.items()}
+    # the kernel class that takes the most device time, against its own
+    # bound (latency-bound classes against the nominal FP32 rate, which
+    # they are far from by design)
+    roof_time = None
+    if by_time and (dom is None or by_time[0] != dom[0]):
+        name, (cnt, tms, fl, by) = by_time
+        fp32_nominal = 75.0
+        roof_time = {"kernel": name, "bound": "latency" if name in ("lu_panel", "trsm", "laswp") else "fp64",
+                     "achieved": fl / (tms / 1e3) / 1e12 if fl > 0 else None, "unit": "TFLOP/s",
+                     "peak": fp32_nominal if name in ("lu_panel", "trsm") else 37.0,
+                     "ms_per_step": tms / args.steps, "launches_per_step": cnt / args.steps,
+                     "peak_source": "nominal B200 FP32 (75) / FP64 (37) rates; no measured entry"}
+        if roof_time["achieved"] is not None:
+            roof_time["frac"] = roof_time["achieved"] / roof_time["peak"]
+    # whole-phase rates: fill pairs/s (N_s^2 segment pairs per fill) and the
+    # factorisation's (8/3) n^3 over its wall time
+    n_seg = int(solver._geometry().n)
+    phases = {}
+    if "fill" in prof:
+        f_ms = prof["fill"][1] / prof["fill"][0]
+        phases["fill_ms"] = f_ms
+        phases["fill_pairs_per_s"] = n_seg ** 2 / (f_ms / 1e3)
+        phases["fill_segments"] = n_seg
+    if "factor_wall" in walls:
+        cnt, tms, fl, _by = walls["factor_wall"]
+        phases["lu_ms"] = tms / cnt
+        phases["lu_tflops"] = (8.0 / 3.0) * buf["n"] ** 3 / (tms / cnt / 1e3) / 1e12
+        phases["lu_tflops_note"] = "(8/3) n^3 complex-LU flops over the factorisation's wall time"
+    if "solve_wall" in walls:
+        cnt, tms, _fl, _by = walls["solve_wall"]
+        phases["triangular_solves_ms_per_step"] = tms / args.steps
 
     line = {
         "metric": METRIC,
@@ -411,6 +443,10 @@ def run_b200(args, kw):
         "roofline": roof,
         "kernels": breakdown,
         "dominant_by_time": by_time[0] if by_time else None,
+        "roofline_by_time": roof_time,
+        "phases": phases,
+        "pivoting": {0: "static (diagonal block)", 1: "partial", 2: "static rejected, then partial"}.get(
+            int(lib.mw_last_mixed_pivoting()), None) if args.precision == "mixed" else "partial",
         "clocks": clocks.summary(),
         "y_rel_err_vs_reference": y_err,
         "fp64_ms_per_step": fp64_ms,
@@ -465,8 +501,10 @@ def run_sweep_part(args, rank, world, local, pg):
     """Sweep part of the headline line: world x --sweep-structs seeded Yagis
     at 64 frequencies, sharded over the ranks (LPT on n^3), each rank's
     shard device-timed; pts/s = all solves / the slowest rank.  Rank 0 also
-    times the plain FP64 GPU path on a sample (2 structures, every 8th
-    frequency) and compares drive-point impedances."""
+    times the plain FP64 GPU path on a stratified sample (the median
+    structure of each of 16 size strata, every 8th frequency), compares
+    drive-point impedances, and at one GPU times the reference's CPU sweep
+    on the same sample."""
     import numpy as np
     import torch
 
@@ -475,7 +513,7 @@ def run_sweep_part(args, rank, world, local, pg):
     from momwire_b200.workloads import yagi_sweep
 
     structs, ks = yagi_sweep(n_structures=args.sweep_structs * world, n_freq=64, seed=0)
-    parts = sweep.partition([sweep.structure_cost(k) for k in structs], world)
+    parts = [sweep.shard_indices(structs, r, world) for r in range(world)]
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream(dev)
     fn = sweep.mixed_sweep_fn(local)
@@ -516,21 +554,79 @@ def run_sweep_part(args, rank, world, local, pg):
     if args.sweep_mode == "workers":
         out["workers_per_rank"] = args.sweep_workers
     if rank == 0:
-        sub = ks[::8]
-        f_ms, n64, err = 0.0, 0, 0.0
-        for i in range(min(2, len(structs))):
-            s = momwire_b200.BSplineSolver(**structs[i], device=local)
-            a.record(stream)
-            y = s.compute_y_matrix_swept(sub)
-            b.record(stream)
-            torch.cuda.synchronize()
-            f_ms += a.elapsed_time(b)
-            n64 += len(sub)
-            z64, zmx = 1.0 / y[:, 0, 0], 1.0 / ys[i][::8, 0, 0]
-            err = max(err, float(np.max(np.abs(zmx - z64) / np.abs(z64))))
-        out.update(fp64_pts_per_s=n64 / (f_ms / 1e3), max_rel_dZin_vs_fp64=err)
+        out.update(fp64_sweep_sample(structs, ks, ys, local, stream))
         out["speedup_vs_fp64"] = out["pts_per_s"] / out["fp64_pts_per_s"]
+        if world == 1 and not args.no_cpu_baseline:
+            out["cpu_baseline"] = cpu_sweep_sample(structs, ks)
     return out
+
+
+def sweep_strata(structs, n_strata=16):
+    """Stratified sample of a structure population: sorted by unknown count
+    and cut into n_strata equal strata; returns (the structure nearest each
+    stratum's median, the stratum sizes)."""
+    import numpy as np
+
+    from momwire_b200 import sweep
+
+    order = sorted(range(len(structs)), key=lambda i: (sweep.structure_cost(structs[i]), i))
+    strata = [list(x) for x in np.array_split(order, min(n_strata, len(order))) if len(x)]
+    return [st[len(st) // 2] for st in strata], [len(st) for st in strata]
+
+
+def fp64_sweep_sample(structs, ks, ys, local, stream, kstep=8):
+    """The plain FP64 GPU path (per-frequency complex128 solves) on a
+    stratified sample -- the median structure of each of 16 size strata at
+    every kstep-th frequency -- extrapolated to the whole sweep by stratum
+    size; and the sample's drive-point impedances against the mixed sweep's."""
+    import numpy as np
+    import torch
+
+    import momwire_b200
+
+    picks, weights = sweep_strata(structs)
+    sub = ks[::kstep]
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    momwire_b200.BSplineSolver(**structs[picks[0]], device=local).compute_y_matrix_swept(sub[:1])  # warm
+    total_ms, err, sample_ms = 0.0, 0.0, 0.0
+    for i, w in zip(picks, weights):
+        s = momwire_b200.BSplineSolver(**structs[i], device=local)
+        a.record(stream)
+        y = s.compute_y_matrix_swept(sub)
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b)
+        sample_ms += ms
+        total_ms += w * ms / len(sub) * len(ks)
+        z64, zmx = 1.0 / y[:, 0, 0], 1.0 / ys[i][::kstep, 0, 0]
+        err = max(err, float(np.max(np.abs(zmx - z64) / np.abs(z64))))
+    return {"fp64_pts_per_s": len(structs) * len(ks) / (total_ms / 1e3), "max_rel_dZin_vs_fp64": err,
+            "fp64_sample": (f"{len(picks)} structures (median of each of {len(picks)} size strata) x {len(sub)} "
+                            f"frequencies (every {kstep}th), {sample_ms:.0f} ms device time, extrapolated by "
+                            "stratum size to every structure and frequency")}
+
+
+def cpu_sweep_sample(structs, ks, kstep=8):
+    """The reference's own compute_y_matrix_swept (its C++ swept fill and
+    LAPACK per frequency) on the same stratified sample, on every host
+    core, extrapolated to the whole sweep by stratum size."""
+    from oracle import ref_baseline
+
+    cores = ref_baseline.pin_threads()
+    mw = ref_baseline.import_reference()
+    picks, weights = sweep_strata(structs)
+    sub = ks[::kstep]
+    total_s, sample_s = 0.0, 0.0
+    for i, w in zip(picks, weights):
+        t0 = time.perf_counter()
+        mw.BSplineSolver(**structs[i]).compute_y_matrix_swept(sub)
+        dt = time.perf_counter() - t0
+        sample_s += dt
+        total_s += w * dt / len(sub) * len(ks)
+    return {"value": len(structs) * len(ks) / total_s, "unit": UNIT, "cores": cores, "kind": "reference",
+            "sample": (f"reference compute_y_matrix_swept on {len(picks)} structures (median of each size "
+                       f"stratum) x {len(sub)} frequencies: {sample_s:.1f} s, extrapolated by stratum size to "
+                       f"{len(structs)} x {len(ks)} solves")}
 
 
 def run_somm(args):

@@ -51,7 +51,10 @@ int64_t mw_launch_count(void);
  * launch on its own stream (for roofline figures).  Classes: 0 same-edge
  * table, 1 fill, 2 image fill, 3 LU panel, 4 row swaps, 5 triangular solve
  * block, 6 complex128 GEMM, 7 tensor-core complex GEMM, 8 refinement,
- * 9 other.  mw_profile_enable(1) clears the counters and starts recording;
+ * 9 other, 10 Sommerfeld grid, 11 Sommerfeld remainder; 12 and 13 enclose
+ * whole factorisations and whole many-right-hand-side triangular solves
+ * (their wall time on the calling stream, overlapping classes 3-9).
+ * mw_profile_enable(1) clears the counters and starts recording;
  * mw_profile_read synchronises the recorded events and returns the launch
  * count, summed device time and the algorithmic flops / bytes of a class. */
 void mw_profile_enable(int32_t on);
@@ -326,6 +329,22 @@ mw_status mw_zgesv_mixed(int64_t n, int64_t nrhs, const double* Z, int64_t ldz,
                          size_t workspace_bytes, int32_t* info,
                          int32_t* iterations, double* last_correction,
                          const volatile int32_t* cancel, void* stream);
+
+/* Pivoting of mw_zgesv_mixed's complex64 factorisation (no counterpart in
+ * the reference, whose LAPACK zgesv always pivots over whole columns).
+ * mode 0 (default): pivots are chosen within each 128-row diagonal block
+ * (static pivoting -- no column-wide search, so no grid-wide exchange per
+ * column); the factorisation is rejected when any |L21| (|re| + |im|)
+ * exceeds 64 or a block is singular, and when the FP64 refinement does not
+ * reach its tolerance, and the solve is then repeated with partial
+ * pivoting.  mode 1: partial pivoting over whole columns (LAPACK's rows).
+ * Process-wide; returns the previous mode (MW_ERR_INVALID for another
+ * value). */
+int32_t mw_set_mixed_pivoting(int32_t mode);
+
+/* Pivoting the last mw_zgesv_mixed on this host thread used: 0 static,
+ * 1 partial, 2 static rejected then partial; -1 before the first call. */
+int32_t mw_last_mixed_pivoting(void);
 
 /*
  * Frequency-batched fill: Z_b (and Z32_b when Z32 != NULL) for n_k

@@ -110,7 +110,9 @@ enum ProfileClass {
     PC_MISC = 9,
     PC_SOMM_GRID = 10,
     PC_SOMM_Q = 11,
-    PC_COUNT = 12
+    PC_FACTOR = 12,  // whole factorisations (wall, enclosing the classes above)
+    PC_SOLVE = 13,   // whole triangular solves with many right-hand sides (wall)
+    PC_COUNT = 14
 };
 
 struct ProfileScope {

@@ -32,6 +32,10 @@ mw_status cgemm_tc_update(int64_t m, int64_t n, int64_t k, const cf* A, int64_t 
                           int64_t ldc, void* ws, size_t ws_bytes, int* err, cudaStream_t st, int max_ctas);
 size_t cgemm_tc_workspace(int64_t m, int64_t n, int64_t k);
 
+// static-pivot panel of the complex64 path (lu_static.cu)
+mw_status static_panel_c64(cf* A, int64_t lda, int64_t n, int64_t j0, int jb, int32_t* ipiv, int32_t* info,
+                           PanelWs* ws, cf* inv_diag, cudaStream_t st);
+
 constexpr int kNB = 64;         // panel half width (rank-1 work per cooperative panel)
 constexpr int kOuterNB = 128;   // getrf block: panel width and trailing-update k
 constexpr int kPanelMaxJb = 128;
@@ -1325,7 +1329,8 @@ static mw_status aux_streams(AuxStreams** out) {
 template <class T>
 static mw_status getrf_lookahead(int64_t n, T* A, int64_t lda, int32_t* ipiv, int32_t* info, char* ws,
                                  const volatile int32_t* cancel, const Updater& up_main, const Updater& up_trail,
-                                 cudaStream_t st, T* Baug = nullptr, int64_t ldb = 0, int64_t nrhs = 0) {
+                                 cudaStream_t st, T* Baug = nullptr, int64_t ldb = 0, int64_t nrhs = 0,
+                                 bool static_pivot = false) {
     MW_CHECK_CUDA(cudaMemsetAsync(info, 0, 2 * sizeof(int32_t), st));
     MW_CHECK_CUDA(cudaMemsetAsync(ws, 0, sizeof(PanelWs), st));
     {
@@ -1362,7 +1367,18 @@ static mw_status getrf_lookahead(int64_t n, T* A, int64_t lda, int32_t* ipiv, in
         const int64_t j0 = j * kOuterNB;
         const int jb = (int)((n - j0) < kOuterNB ? (n - j0) : kOuterNB);
         if (j >= 2) MW_CHECK_CUDA(cudaStreamWaitEvent(st, ax->ev_trail[(j - 2) & 3], 0));
-        mw_status s = panel_factor<T>(A, lda, n, j0, jb, ipiv, info, ws, up_main, st, kLaPanelCtas);
+        mw_status s;
+        if constexpr (std::is_same<T, cf>::value) {
+            if (static_pivot) {
+                size_t ov, oi, orow, ocur;
+                ws_layout(kMaxPanelGrid, &ov, &oi, &orow, &ocur);
+                s = static_panel_c64(A, lda, n, j0, jb, ipiv, info, pws, reinterpret_cast<cf*>(ws + ocur), st);
+            } else {
+                s = panel_factor<T>(A, lda, n, j0, jb, ipiv, info, ws, up_main, st, kLaPanelCtas);
+            }
+        } else {
+            s = panel_factor<T>(A, lda, n, j0, jb, ipiv, info, ws, up_main, st, kLaPanelCtas);
+        }
         if (s != MW_OK) return s;
         MW_CHECK_CUDA(cudaEventRecord(ax->ev_main, st));
         // (the swaps of panel j on the columns left of it wait until the
@@ -1538,6 +1554,12 @@ static Updater tc_updater(char* ws, size_t ws_bytes, int64_t n, int64_t nrhs_max
 // The main-stream updater of the look-ahead factorisation: its own operand
 // planes (after the trail region and the status word), the shared status
 // word, and the panel's CTA budget.
+// info[1] = the panel's wait status, else the tensor-core kernels'
+__global__ void merge_status_kernel(int32_t* out, const int* panel_err, const int* tc_err) {
+    const int a = *panel_err;
+    *out = a != 0 ? a : *tc_err;
+}
+
 static Updater tc_updater_main(char* ws, int64_t n, int64_t nrhs_max) {
     Updater t = tc_updater(ws, 0, n, nrhs_max);
     Updater u;
@@ -1566,6 +1588,7 @@ extern "C" mw_status mw_zgetrf(int64_t n, double* Ad, int64_t lda, int32_t* ipiv
     Updater up_main, up_trail;
     up_main.max_ctas = kLaPanelCtas;
     up_trail.max_ctas = panel_sms<cd>() - kLaPanelCtas;
+    ProfileScope ps(PC_FACTOR, as_stream(stream), 8.0 / 3.0 * (double)n * n * n, 0.0);
     return getrf_lookahead<cd>(n, reinterpret_cast<cd*>(Ad), lda, ipiv, info, static_cast<char*>(workspace), cancel,
                                up_main, up_trail, as_stream(stream));
 }
@@ -1578,6 +1601,7 @@ extern "C" mw_status mw_zgetrs(int64_t n, int64_t nrhs, const double* LUd, int64
     Updater up_main, up_rest;
     up_main.max_ctas = kLaPanelCtas;                  // leaves and next-block updates
     up_rest.max_ctas = panel_sms<cd>() - kLaPanelCtas;  // the rest, beside them
+    ProfileScope ps(PC_SOLVE, as_stream(stream), 8.0 * (double)n * n * nrhs, 0.0);
     return getrs<cd>(n, nrhs, reinterpret_cast<const cd*>(LUd), lda, ipiv, reinterpret_cast<cd*>(Bd), ldb, up_main,
                      up_rest, as_stream(stream));
 }
@@ -1597,8 +1621,10 @@ extern "C" mw_status mw_cgetrf(int64_t n, float* Ad, int64_t lda, int32_t* ipiv,
     MW_CHECK_CUDA(cudaMemsetAsync(up.tc_err, 0, sizeof(int), st));
     mw_status s = getrf_lookahead<cf>(n, reinterpret_cast<cf*>(Ad), lda, ipiv, info, ws, cancel, up_main, up, st);
     if (s != MW_OK) return s;
-    // fold a tensor-core timeout into info[1] (barrier timeouts already there)
-    MW_CHECK_CUDA(cudaMemcpyAsync(info + 1, up.tc_err, sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
+    // info[1]: a panel wait's timeout, else a tensor-core one
+    merge_status_kernel<<<1, 1, 0, st>>>(info + 1, &reinterpret_cast<PanelWs*>(ws)->err, up.tc_err);
+    count_launch();
+    MW_CHECK_CUDA(cudaGetLastError());
     return MW_OK;
 }
 
@@ -1608,7 +1634,7 @@ namespace mw {
 // the forward substitution of the first solve then costs no extra pass.
 mw_status cgetrf_forward(int64_t n, float* Ad, int64_t lda, int32_t* ipiv, int32_t* info, void* workspace,
                          size_t workspace_bytes, float* Bd, int64_t ldb, int64_t nrhs, const volatile int32_t* cancel,
-                         void* stream) {
+                         void* stream, bool static_pivot) {
     MW_REQUIRE(n >= 0 && lda >= (n > 0 ? n : 1) && nrhs >= 0 && ldb >= (n > 0 ? n : 1), "bad sizes");
     MW_REQUIRE(Ad && ipiv && info && workspace && (nrhs == 0 || Bd), "NULL argument");
     MW_REQUIRE(workspace_bytes >= cgetrf_ws_bytes(n, nrhs), "workspace too small");
@@ -1619,9 +1645,11 @@ mw_status cgetrf_forward(int64_t n, float* Ad, int64_t lda, int32_t* ipiv, int32
     cudaStream_t st = as_stream(stream);
     MW_CHECK_CUDA(cudaMemsetAsync(up.tc_err, 0, sizeof(int), st));
     mw_status s = getrf_lookahead<cf>(n, reinterpret_cast<cf*>(Ad), lda, ipiv, info, ws, cancel, up_main, up, st,
-                                      reinterpret_cast<cf*>(Bd), ldb, nrhs);
+                                      reinterpret_cast<cf*>(Bd), ldb, nrhs, static_pivot);
     if (s != MW_OK) return s;
-    MW_CHECK_CUDA(cudaMemcpyAsync(info + 1, up.tc_err, sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
+    merge_status_kernel<<<1, 1, 0, st>>>(info + 1, &reinterpret_cast<PanelWs*>(ws)->err, up.tc_err);
+    count_launch();
+    MW_CHECK_CUDA(cudaGetLastError());
     return MW_OK;
 }
 

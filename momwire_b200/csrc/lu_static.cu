@@ -1,0 +1,264 @@
+// Static-pivot panel of the complex64 LU (sm_100a).
+//
+// The mixed-precision path factors Z in complex64 and refines the solution
+// against the FP64 Z, so its factors need only be a good preconditioner,
+// not LAPACK's partial-pivoting factors.  Pivoting is therefore restricted
+// to the rows of each 128 x 128 diagonal block ("static pivoting", Li and
+// Demmel 1998: factor with pivots chosen locally, recover accuracy by
+// iterative refinement): the panel no longer needs a pivot search over all
+// the rows below it, so it has no grid-wide exchange per column.  A panel is
+//   sp_diag_kernel  one CTA factors the diagonal block in registers with
+//                   partial pivoting among its own rows (row interchanges
+//                   kept as a row arrangement, written back once), and
+//   sp_l21_kernel   every row below is solved against the block's upper
+//                   factor, L21 = A21 U11^-1, one warp per eight rows.
+// The growth the restriction allows is measured: sp_l21_kernel raises the
+// largest |L21| (|re| + |im|) into PanelWs::lmax_bits, and an exact zero
+// pivot sets it to +inf.  The caller refactors with full partial pivoting
+// when it exceeds its bound, and the FP64 refinement checks the result.
+// Galerkin thin-wire impedance matrices are strongly diagonal: partial
+// pivoting rarely leaves the diagonal block on them (no interchange at all
+// on the planar dipole arrays, a few per cent of columns on Yagis, where
+// the local pivot's |L| stays below 3).
+#include "common.cuh"
+#include "waits.cuh"
+
+namespace mw {
+
+constexpr int kSpB = 128;          // diagonal block order
+constexpr int kSpDiagThreads = 512;  // 128 rows x 4 groups of 32 columns
+constexpr int kSpRowsPerWarp = 8;
+constexpr int kSpL21Warps = 12;
+constexpr int kSpUStride = kSpB + 2;  // complex elements per shared-memory row of U (16-byte aligned)
+
+namespace {
+
+__device__ __forceinline__ cf crcp_sp(cf z) {
+    // 1 / z with z scaled by its larger component (|z|^2 neither overflows
+    // nor underflows); two reciprocals instead of Smith's three divisions
+    const float s = fmaxf(fabsf(z.re), fabsf(z.im));
+    if (s < 1e-30f) return cdiv(cone<cf>(), z);
+    const float rs = __frcp_rn(s);
+    const float a = z.re * rs, b = z.im * rs;
+    const float t = rs * __frcp_rn(a * a + b * b);
+    return cf{a * t, -b * t};
+}
+
+__device__ __forceinline__ float cabs1f(cf z) { return fabsf(z.re) + fabsf(z.im); }
+
+// Factor A[j0 .. j0+jb) x [j0 .. j0+jb) in place with partial pivoting among
+// these rows.  Thread (r, g) holds row r's columns 32g .. 32g+31 in
+// registers; a chosen pivot row stops updating (its remaining columns are
+// its U row), so no data moves until the block is written back in pivot
+// order.  Two barriers per column.
+__global__ void __launch_bounds__(kSpDiagThreads, 1)
+    sp_diag_kernel(cf* __restrict__ A, int64_t lda, int64_t j0, int jb, int32_t* __restrict__ ipiv,
+                   int32_t* __restrict__ info, cf* __restrict__ inv_diag, PanelWs* ws) {
+    __shared__ cf s_col[kSpB];
+    __shared__ cf s_u[kSpB];
+    __shared__ unsigned long long s_wkey[4];
+    const int tid = threadIdx.x;
+    const int r = tid & (kSpB - 1);
+    const int g = tid >> 7;
+    const int lane = tid & 31;
+    const int wig = (tid >> 5) & 3;  // warp within its column group
+    cf a[32];
+#pragma unroll
+    for (int i = 0; i < 32; ++i) {
+        const int col = 32 * g + i;
+        a[i] = (r < jb && col < jb) ? A[(j0 + r) + (j0 + col) * lda] : cf{0.0f, 0.0f};
+    }
+    bool active = r < jb;
+    // this row's position in the arranged block (LAPACK's row order after
+    // the interchanges so far); every thread of the row tracks it
+    int mypos = r;
+    for (int c = 0; c < jb; ++c) {
+        const int gc = c >> 5, ic = c & 31;
+        if (g == gc) {
+            cf v = a[0];
+#pragma unroll
+            for (int i = 1; i < 32; ++i)
+                if (i == ic) v = a[i];
+            s_col[r] = v;
+            // largest |re| + |im| among the rows not yet chosen, then the
+            // smallest position (LAPACK's icamax on the arranged rows); the
+            // low bits carry the physical row
+            unsigned long long key = 0;
+            if (active)
+                key = ((unsigned long long)__float_as_uint(cabs1f(v)) << 32) |
+                      ((unsigned long long)(0xFFFFu - (unsigned int)mypos) << 16) | (unsigned long long)r;
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                const unsigned long long o = __shfl_xor_sync(0xffffffffu, key, off);
+                key = o > key ? o : key;
+            }
+            if (lane == 0) s_wkey[wig] = key;
+        }
+        __syncthreads();
+        unsigned long long best = s_wkey[0];
+#pragma unroll
+        for (int w = 1; w < 4; ++w) best = s_wkey[w] > best ? s_wkey[w] : best;
+        const int p = (int)(best & 0xFFFFull);
+        const int pos_best = (int)(0xFFFFu - (unsigned int)((best >> 16) & 0xFFFFull));
+        const bool zero = (best >> 32) == 0ull;
+        const cf inv = zero ? cone<cf>() : crcp_sp(s_col[p]);
+        if (r == p) {
+#pragma unroll
+            for (int i = 0; i < 32; ++i) s_u[32 * g + i] = a[i];
+            active = false;
+        }
+        const cf l = (active && !zero) ? s_col[r] * inv : cf{0.0f, 0.0f};
+        // the interchange LAPACK makes: positions c and pos_best
+        if (r == p)
+            mypos = c;
+        else if (mypos == c)
+            mypos = pos_best;
+        __syncthreads();  // s_u complete; s_col and s_wkey read
+        if (tid == 0) {
+            ipiv[j0 + c] = (int32_t)(j0 + pos_best + 1);
+            if (zero) {
+                if (info[0] == 0) info[0] = (int32_t)(j0 + c + 1);
+                atomicExch(&ws->lmax_bits, 0x7f800000u);  // +inf: the block is singular
+            }
+            inv_diag[c] = inv;
+        }
+        if (active) {
+            if (g == gc) {
+#pragma unroll
+                for (int i = 0; i < 32; ++i)
+                    if (i == ic && !zero) a[i] = l;
+            }
+            if (!zero) {
+#pragma unroll
+                for (int i = 0; i < 32; ++i) {
+                    const int col = 32 * g + i;
+                    if (col > c) a[i] = a[i] - l * s_u[col];
+                }
+            }
+        }
+    }
+    if (r < jb) {
+        const int64_t row = j0 + mypos;
+#pragma unroll
+        for (int i = 0; i < 32; ++i) {
+            const int col = 32 * g + i;
+            if (col < jb) A[row + (j0 + col) * lda] = a[i];
+        }
+    }
+}
+
+// L21 = A21 U11^-1 for the rows below the diagonal block: one warp per eight
+// rows, lane l holding columns 4l .. 4l+3 of each; step j finishes column j
+// on its owner lane, broadcasts it and removes it from the later columns.
+// U11 (upper triangle of the factored block) is staged row-major in shared
+// memory.  The largest |L21| goes to ws->lmax_bits.
+__global__ void __launch_bounds__(32 * kSpL21Warps, 1)
+    sp_l21_kernel(cf* __restrict__ A, int64_t lda, int64_t j0, int jb, int64_t row_end,
+                  const cf* __restrict__ inv_diag, PanelWs* ws) {
+    extern __shared__ __align__(16) unsigned char sp_smem[];
+    cf* sU = reinterpret_cast<cf*>(sp_smem);              // [kSpB][kSpUStride]
+    cf* sInv = sU + (size_t)kSpB * kSpUStride;            // [kSpB]
+    const int tid = threadIdx.x;
+    for (int idx = tid; idx < kSpB * kSpB; idx += blockDim.x) {
+        const int j = idx % kSpB, col = idx / kSpB;  // coalesced down each column
+        sU[j * kSpUStride + col] = (j <= col && col < jb) ? A[(j0 + j) + (j0 + col) * lda] : cf{0.0f, 0.0f};
+    }
+    for (int j = tid; j < kSpB; j += blockDim.x) sInv[j] = j < jb ? inv_diag[j] : cf{0.0f, 0.0f};
+    __syncthreads();
+    const int lane = tid & 31, warp = tid >> 5;
+    const int64_t rbase = j0 + jb + ((int64_t)blockIdx.x * kSpL21Warps + warp) * kSpRowsPerWarp;
+    if (rbase >= row_end) return;
+    cf a[kSpRowsPerWarp][4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int col = 4 * lane + q;
+#pragma unroll
+        for (int rr = 0; rr < kSpRowsPerWarp; ++rr) {
+            const int64_t row = rbase + rr;
+            a[rr][q] = (col < jb && row < row_end) ? A[row + (j0 + col) * lda] : cf{0.0f, 0.0f};
+        }
+    }
+    float lmax = 0.0f;
+    for (int j = 0; j < jb; ++j) {
+        const int owner = j >> 2, slot = j & 3;
+        cf x[kSpRowsPerWarp];
+        if (lane == owner) {
+            const cf d = sInv[j];
+#pragma unroll
+            for (int rr = 0; rr < kSpRowsPerWarp; ++rr) {
+                cf v = a[rr][0];
+#pragma unroll
+                for (int q = 1; q < 4; ++q)
+                    if (q == slot) v = a[rr][q];
+                v = v * d;
+                lmax = fmaxf(lmax, cabs1f(v));
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    if (q == slot) a[rr][q] = v;
+                x[rr] = v;
+            }
+        }
+#pragma unroll
+        for (int rr = 0; rr < kSpRowsPerWarp; ++rr) {
+            x[rr].re = __shfl_sync(0xffffffffu, x[rr].re, owner);
+            x[rr].im = __shfl_sync(0xffffffffu, x[rr].im, owner);
+        }
+        const cf* urow = sU + (size_t)j * kSpUStride + 4 * lane;
+        const float4 u01 = *reinterpret_cast<const float4*>(urow);
+        const float4 u23 = *reinterpret_cast<const float4*>(urow + 2);
+        const cf u[4] = {cf{u01.x, u01.y}, cf{u01.z, u01.w}, cf{u23.x, u23.y}, cf{u23.z, u23.w}};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            if (4 * lane + q > j) {
+#pragma unroll
+                for (int rr = 0; rr < kSpRowsPerWarp; ++rr) a[rr][q] = a[rr][q] - x[rr] * u[q];
+            }
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int col = 4 * lane + q;
+#pragma unroll
+        for (int rr = 0; rr < kSpRowsPerWarp; ++rr) {
+            const int64_t row = rbase + rr;
+            if (col < jb && row < row_end) A[row + (j0 + col) * lda] = a[rr][q];
+        }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) lmax = fmaxf(lmax, __shfl_xor_sync(0xffffffffu, lmax, off));
+    // NaN-safe: a NaN compares false and leaves the bound raised by atomicMax
+    // of +inf below
+    if (lane == 0) atomicMax(&ws->lmax_bits, (lmax == lmax) ? __float_as_uint(lmax) : 0x7f800000u);
+}
+
+}  // namespace
+
+// The panel of columns [j0, j0+jb) (jb <= 128) over rows [j0, n): the
+// diagonal block factored with pivots among its own rows, then L21.
+// `inv_diag`: 128 complex64 of device scratch for the reciprocal pivots.
+mw_status static_panel_c64(cf* A, int64_t lda, int64_t n, int64_t j0, int jb, int32_t* ipiv, int32_t* info,
+                           PanelWs* ws, cf* inv_diag, cudaStream_t st) {
+    MW_REQUIRE(jb >= 1 && jb <= kSpB, "static panel width %d outside 1..%d", jb, kSpB);
+    static bool configured = false;
+    const size_t smem = sizeof(cf) * ((size_t)kSpB * kSpUStride + kSpB);
+    if (!configured) {
+        MW_CHECK_CUDA(cudaFuncSetAttribute(sp_l21_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        configured = true;
+    }
+    {
+        ProfileScope ps(PC_PANEL, st, 8.0 * (double)jb * jb * jb / 3.0, 16.0 * (double)jb * jb);
+        sp_diag_kernel<<<1, kSpDiagThreads, 0, st>>>(A, lda, j0, jb, ipiv, info, inv_diag, ws);
+        count_launch();
+        const int64_t rows = n - j0 - jb;
+        if (rows > 0) {
+            const int64_t per_cta = (int64_t)kSpL21Warps * kSpRowsPerWarp;
+            const unsigned grid = (unsigned)((rows + per_cta - 1) / per_cta);
+            sp_l21_kernel<<<grid, 32 * kSpL21Warps, smem, st>>>(A, lda, j0, jb, n, inv_diag, ws);
+            count_launch();
+        }
+    }
+    MW_CHECK_CUDA(cudaGetLastError());
+    return MW_OK;
+}
+
+}  // namespace mw

@@ -8,7 +8,10 @@
 // from mw_cgetrf (tensor-core trailing updates, 3xTF32); the residual uses
 // the FP64 Z.  The reference solves in complex128 LAPACK
 // (bspline.py:2971-2989); this path adds nothing to its algebra.
+#include <algorithm>
+#include <atomic>
 #include <cmath>
+#include <cstring>
 #include <vector>
 
 #include "common.cuh"
@@ -79,12 +82,36 @@ extern "C" mw_status mw_cgetrs(int64_t n, int64_t nrhs, const float* LU, int64_t
 namespace mw {
 mw_status cgetrf_forward(int64_t n, float* Ad, int64_t lda, int32_t* ipiv, int32_t* info, void* workspace,
                          size_t workspace_bytes, float* Bd, int64_t ldb, int64_t nrhs, const volatile int32_t* cancel,
-                         void* stream);
+                         void* stream, bool static_pivot);
 mw_status cgetrs_upper(int64_t n, int64_t nrhs, const float* LUd, int64_t lda, float* Bd, int64_t ldb, void* workspace,
                        size_t workspace_bytes, void* stream);
 }  // namespace mw
 
 static size_t al256(size_t x) { return (x + 255) & ~size_t(255); }
+
+namespace {
+// Pivoting of the complex64 factorisation: 0 pivots within each diagonal
+// block (static pivoting) and falls back to partial pivoting, 1 partial
+// pivoting only.
+std::atomic<int> g_pivot_mode{0};
+// What the last mw_zgesv_mixed on this host thread used: 0 static pivots,
+// 1 partial pivoting, 2 static pivots rejected then partial pivoting.
+thread_local int g_last_pivoting = -1;
+// A static-pivot factorisation is kept while every |L21| (|re| + |im|) stays
+// within this bound (partial pivoting keeps |L| <= 1); the FP64 refinement
+// then has to converge as well.
+constexpr float kStaticLmaxBound = 64.0f;
+}  // namespace
+
+extern "C" int32_t mw_set_mixed_pivoting(int32_t mode) {
+    if (mode != 0 && mode != 1) {
+        set_error("pivoting mode must be 0 (static with fallback) or 1 (partial), got %d", mode);
+        return MW_ERR_INVALID;
+    }
+    return g_pivot_mode.exchange(mode);
+}
+
+extern "C" int32_t mw_last_mixed_pivoting(void) { return g_last_pivoting; }
 
 extern "C" size_t mw_zgesv_mixed_workspace_size(int64_t n, int64_t nrhs) {
     return al256(mw_cgetrf_workspace_size(n, nrhs)) + al256((size_t)n * nrhs * 16) + al256((size_t)n * nrhs * 8) +
@@ -113,81 +140,111 @@ extern "C" mw_status mw_zgesv_mixed(int64_t n, int64_t nrhs, const double* Z, in
     cd* Xc = reinterpret_cast<cd*>(X);
     const int64_t tot = n * nrhs;
 
-    // the first solve's right-hand sides ride through the factorisation
-    // (complex64 B, forward-substituted as the trailing columns are updated)
-    to_c64_kernel<<<grid_for(tot), 256, 0, st>>>(Bc, ldb, R32, n, n, nrhs);
-    count_launch();
-    mw_status s = cgetrf_forward(n, Z32, ldz32, ipiv, info, ws_lu, lu_ws, reinterpret_cast<float*>(R32), n, nrhs,
-                                 cancel, stream);
-    if (s != MW_OK) return s;
-    int32_t hinfo[2] = {0, 0};
-    MW_CHECK_CUDA(cudaMemcpyAsync(hinfo, info, sizeof(hinfo), cudaMemcpyDeviceToHost, st));
-    MW_CHECK_CUDA(cudaStreamSynchronize(st));
-    if (hinfo[1] != 0) {
-        set_error("factorisation: a bounded device wait timed out");
-        return MW_ERR_TIMEOUT;
-    }
-    if (hinfo[0] > 0) {
-        set_error("exact zero pivot at column %d", hinfo[0]);
-        return MW_ERR_SINGULAR;
-    }
-    // X = 0, R = B
-    MW_CHECK_CUDA(cudaMemsetAsync(norms, 0, sizeof(double) * 2 * nrhs, st));
-    MW_CHECK_CUDA(cudaMemset2DAsync(Xc, sizeof(cd) * ldx, 0, sizeof(cd) * n, nrhs, st));
-    copy_c128_kernel<<<grid_for(tot), 256, 0, st>>>(Bc, ldb, R, n, n, nrhs);
-    count_launch();
+    bool static_pivot = g_pivot_mode.load() == 0;
+    bool fell_back = false;
     double corr = INFINITY;
     int it = 0;
     std::vector<double> hn(2 * nrhs), prev(nrhs, 0.0);
-    for (;; ++it) {
-        if (cancel && *cancel) {
-            set_error("solve cancelled");
-            return MW_ERR_CANCELLED;
-        }
-        if (it == 0) {
-            // R32 holds L^-1 P B from the factorisation
-            s = cgetrs_upper(n, nrhs, Z32, ldz32, reinterpret_cast<float*>(R32), n, ws_lu, lu_ws, stream);
-        } else {
-            {
-                ProfileScope ps(PC_REFINE, st, 0.0, 24.0 * (double)tot);
-                to_c64_kernel<<<grid_for(tot), 256, 0, st>>>(R, n, R32, n, n, nrhs);
-                count_launch();
-            }
-            s = mw_cgetrs(n, nrhs, Z32, ldz32, ipiv, reinterpret_cast<float*>(R32), n, ws_lu, lu_ws, stream);
-        }
-        if (s != MW_OK) return s;
-        MW_CHECK_CUDA(cudaMemsetAsync(norms, 0, sizeof(double) * 2 * nrhs, st));
-        {
-            ProfileScope ps(PC_REFINE, st, 2.0 * (double)tot, 40.0 * (double)tot);
-            dim3 g((unsigned)((n + 255) / 256 < 64 ? (n + 255) / 256 : 64), (unsigned)nrhs);
-            accumulate_kernel<<<g, 256, 0, st>>>(R32, n, Xc, ldx, n, norms, norms + nrhs);
+    for (int attempt = 0;; ++attempt) {
+        if (attempt > 0) {
+            // partial pivoting after a rejected static-pivot factorisation:
+            // Z32 again from the FP64 Z (the same rounding as the fill's)
+            static_pivot = false;
+            fell_back = true;
+            to_c64_kernel<<<grid_for(n * n), 256, 0, st>>>(Zc, ldz, reinterpret_cast<cf*>(Z32), ldz32, n, n);
             count_launch();
         }
-        MW_CHECK_CUDA(cudaMemcpyAsync(hn.data(), norms, sizeof(double) * 2 * nrhs, cudaMemcpyDeviceToHost, st));
-        MW_CHECK_CUDA(cudaStreamSynchronize(st));
-        // per column: the relative correction r, and once corrections
-        // contract (q = r / r_prev <= 1/2), the error left after this one,
-        // about r q.  The initial solve counts as the first correction: it
-        // starts from X = 0, so its error was the whole solution (r = 1) and
-        // the first refinement correction r_1 measures the contraction
-        // itself.  The controlling value is the smaller of r and r q,
-        // maximised over the columns.
-        corr = 0.0;
-        for (int64_t j = 0; j < nrhs; ++j) {
-            double xm = hn[nrhs + j];
-            double r = xm > 0.0 ? hn[j] / xm : (hn[j] > 0.0 ? INFINITY : 0.0);
-            double v = r;
-            if (it > 0 && prev[j] > 0.0 && r <= 0.5 * prev[j]) v = fmin(r, r * (r / prev[j]));
-            prev[j] = r;
-            if (!(v <= corr)) corr = v;  // NaN-propagating max
+        // the first solve's right-hand sides ride through the factorisation
+        // (complex64 B, forward-substituted as the trailing columns are updated)
+        to_c64_kernel<<<grid_for(tot), 256, 0, st>>>(Bc, ldb, R32, n, n, nrhs);
+        count_launch();
+        mw_status s;
+        {
+            ProfileScope ps(PC_FACTOR, st, 8.0 / 3.0 * (double)n * n * n + 4.0 * (double)n * n * nrhs, 0.0);
+            s = cgetrf_forward(n, Z32, ldz32, ipiv, info, ws_lu, lu_ws, reinterpret_cast<float*>(R32), n, nrhs,
+                               cancel, stream, static_pivot);
         }
-        if (corr <= tol || it >= max_iter) break;
-        // R = B - Z X   (FP64)
+        if (s != MW_OK) return s;
+        int32_t hinfo[2] = {0, 0};
+        unsigned int hws[4] = {0, 0, 0, 0};  // the panel status block at the start of the workspace
+        MW_CHECK_CUDA(cudaMemcpyAsync(hinfo, info, sizeof(hinfo), cudaMemcpyDeviceToHost, st));
+        MW_CHECK_CUDA(cudaMemcpyAsync(hws, ws_lu, sizeof(hws), cudaMemcpyDeviceToHost, st));
+        MW_CHECK_CUDA(cudaStreamSynchronize(st));
+        if (hinfo[1] != 0) {
+            set_error("factorisation: a bounded device wait timed out");
+            return MW_ERR_TIMEOUT;
+        }
+        if (static_pivot) {
+            float lmax;
+            std::memcpy(&lmax, &hws[2], sizeof(float));
+            if (!(lmax <= kStaticLmaxBound) || hinfo[0] > 0) continue;  // growth too large or singular block
+        }
+        if (hinfo[0] > 0) {
+            set_error("exact zero pivot at column %d", hinfo[0]);
+            return MW_ERR_SINGULAR;
+        }
+        // X = 0, R = B
+        MW_CHECK_CUDA(cudaMemsetAsync(norms, 0, sizeof(double) * 2 * nrhs, st));
+        MW_CHECK_CUDA(cudaMemset2DAsync(Xc, sizeof(cd) * ldx, 0, sizeof(cd) * n, nrhs, st));
         copy_c128_kernel<<<grid_for(tot), 256, 0, st>>>(Bc, ldb, R, n, n, nrhs);
         count_launch();
-        s = zgemm_launch(false, false, n, nrhs, n, cd{-1.0, 0.0}, Zc, ldz, Xc, ldx, cd{1.0, 0.0}, R, n, st, 0);
-        if (s != MW_OK) return s;
+        corr = INFINITY;
+        std::fill(prev.begin(), prev.end(), 0.0);
+        for (it = 0;; ++it) {
+            if (cancel && *cancel) {
+                set_error("solve cancelled");
+                return MW_ERR_CANCELLED;
+            }
+            if (it == 0) {
+                // R32 holds L^-1 P B from the factorisation
+                ProfileScope ps(PC_SOLVE, st, 4.0 * (double)n * n * nrhs, 0.0);
+                s = cgetrs_upper(n, nrhs, Z32, ldz32, reinterpret_cast<float*>(R32), n, ws_lu, lu_ws, stream);
+            } else {
+                {
+                    ProfileScope ps(PC_REFINE, st, 0.0, 24.0 * (double)tot);
+                    to_c64_kernel<<<grid_for(tot), 256, 0, st>>>(R, n, R32, n, n, nrhs);
+                    count_launch();
+                }
+                ProfileScope ps(PC_SOLVE, st, 8.0 * (double)n * n * nrhs, 0.0);
+                s = mw_cgetrs(n, nrhs, Z32, ldz32, ipiv, reinterpret_cast<float*>(R32), n, ws_lu, lu_ws, stream);
+            }
+            if (s != MW_OK) return s;
+            MW_CHECK_CUDA(cudaMemsetAsync(norms, 0, sizeof(double) * 2 * nrhs, st));
+            {
+                ProfileScope ps(PC_REFINE, st, 2.0 * (double)tot, 40.0 * (double)tot);
+                dim3 g((unsigned)((n + 255) / 256 < 64 ? (n + 255) / 256 : 64), (unsigned)nrhs);
+                accumulate_kernel<<<g, 256, 0, st>>>(R32, n, Xc, ldx, n, norms, norms + nrhs);
+                count_launch();
+            }
+            MW_CHECK_CUDA(cudaMemcpyAsync(hn.data(), norms, sizeof(double) * 2 * nrhs, cudaMemcpyDeviceToHost, st));
+            MW_CHECK_CUDA(cudaStreamSynchronize(st));
+            // per column: the relative correction r, and once corrections
+            // contract (q = r / r_prev <= 1/2), the error left after this one,
+            // about r q.  The initial solve counts as the first correction: it
+            // starts from X = 0, so its error was the whole solution (r = 1) and
+            // the first refinement correction r_1 measures the contraction
+            // itself.  The controlling value is the smaller of r and r q,
+            // maximised over the columns.
+            corr = 0.0;
+            for (int64_t j = 0; j < nrhs; ++j) {
+                double xm = hn[nrhs + j];
+                double r = xm > 0.0 ? hn[j] / xm : (hn[j] > 0.0 ? INFINITY : 0.0);
+                double v = r;
+                if (it > 0 && prev[j] > 0.0 && r <= 0.5 * prev[j]) v = fmin(r, r * (r / prev[j]));
+                prev[j] = r;
+                if (!(v <= corr)) corr = v;  // NaN-propagating max
+            }
+            if (corr <= tol || it >= max_iter) break;
+            // R = B - Z X   (FP64)
+            copy_c128_kernel<<<grid_for(tot), 256, 0, st>>>(Bc, ldb, R, n, n, nrhs);
+            count_launch();
+            s = zgemm_launch(false, false, n, nrhs, n, cd{-1.0, 0.0}, Zc, ldz, Xc, ldx, cd{1.0, 0.0}, R, n, st, 0);
+            if (s != MW_OK) return s;
+        }
+        if (corr <= tol || !static_pivot) break;
+        // the static-pivot factors did not refine to tol: partial pivoting
     }
+    g_last_pivoting = static_pivot ? 0 : (fell_back ? 2 : 1);
     if (iterations) *iterations = it;
     if (last_correction) *last_correction = corr;
     if (!(corr <= tol)) {

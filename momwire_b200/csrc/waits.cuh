@@ -12,9 +12,10 @@ namespace mw {
 constexpr long long kGridSpinLimit = 1ll << 26;
 
 struct PanelWs {
-    unsigned int counter;  // grid barrier arrivals
-    int err;               // device status (MW_ERR_TIMEOUT)
-    int pad[2];
+    unsigned int counter;    // grid barrier arrivals
+    int err;                 // device status (MW_ERR_TIMEOUT)
+    unsigned int lmax_bits;  // static-pivot panels: largest |L21| (float bits; +inf when singular)
+    int spare;
 };
 
 __device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {

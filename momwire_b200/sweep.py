@@ -272,74 +272,113 @@ def _group_width(s0, nb, Z, Z32, Bd, P, stream):
     return autotune.choose(nb, 0, "grouped", time_width)
 
 
-def grouped_mixed_sweep(structs, ks, device=None, budget_bytes=32 << 30, indices=None):
+def shard_indices(structs, rank, world):
+    """This rank's structures: the LPT partition of ``structure_cost``."""
+    return partition([structure_cost(kw) for kw in structs], world)[rank]
+
+
+class _DeviceGroups:
+    """Solves the groups of a sweep on the GPU: one device arena for every
+    group, the heaviest groups first, and a helper thread that builds and
+    uploads the next structures' host tables on its own stream while the
+    current group is filled and factorised."""
+
+    def __init__(self, solvers, ks, plan_ids, P_max):
+        import concurrent.futures as cf
+
+        import torch
+
+        self.solvers, self.ks = solvers, ks
+        first = solvers[plan_ids[0][1][0]]
+        self.dev = first._torch_device()
+        self.stream = torch.cuda.current_stream(self.dev).cuda_stream
+        self.arena = torch.empty(max(_group_bytes(len(ids) * len(ks), nb, P_max) for nb, ids in plan_ids),
+                                 dtype=torch.uint8, device=self.dev)
+        self.prep_stream = torch.cuda.Stream(device=self.dev)
+        self.ports = {}
+        self.ex = cf.ThreadPoolExecutor(max_workers=1)
+        self.futs = {i: self.ex.submit(self._prep, i) for _nb, ids in plan_ids for i in ids}
+
+    def _prep(self, i):
+        import torch
+
+        with torch.cuda.device(self.dev), torch.cuda.stream(self.prep_stream):
+            s = self.solvers[i]
+            s._dev_tables()
+            s._loading_dev_tables()
+            self.ports[i] = s._port_columns()[0]
+            self.prep_stream.synchronize()
+
+    def solve(self, nb, ids):
+        def wait(g):
+            self.futs[ids[g]].result()
+
+        res, _it = _solve_group([self.solvers[i] for i in ids], nb, self.ks, self.stream, arena=self.arena,
+                                wait=wait, Bs=_Ports(self.ports, ids))
+        return res
+
+    def single(self, solver):
+        return solver.compute_y_matrix_swept(self.ks)
+
+    def close(self):
+        self.ex.shutdown(wait=True)
+
+
+def grouped_mixed_sweep(structs, ks, device=None, budget_bytes=32 << 30, indices=None, groups=None):
     """{index: (n_k, P, P) Y stack} for the given structures, every one at
     the frequencies ks, through grouped batched solves: structures are
     bucketed by padded order (``padded_order``), and each group's
     (structure, frequency) systems are filled into one padded stack and
     factorised by one batched mixed-precision solve.  Structures the batched
     route does not serve (finite grounds, KCL constraint rows, orders above
-    the batched panel's limit) take their own ``compute_y_matrix_swept``."""
-    import torch
+    the batched panel's limit) take their own ``compute_y_matrix_swept``.
 
+    ``groups(solvers, ks, plan, P_max)`` makes the group solver (``solve(nb,
+    ids)`` -> {position: Y stack}, ``single(solver)``, ``close()``); the
+    default solves on the GPU."""
     import momwire_b200
 
     from . import _lib
 
     indices = list(range(len(structs))) if indices is None else list(indices)
     solvers = {i: momwire_b200.BSplineSolver(**structs[i], precision="mixed", device=device) for i in indices}
-    out = {}
-    grouped = []
+    ks = np.asarray(ks, dtype=np.float64)
+    grouped, single = [], []
     for i in indices:
         s = solvers[i]
-        if s._swept_batched_available() and padded_order(s._basis_count()) <= 1600:
-            grouped.append(i)
-        else:
-            out[i] = s.compute_y_matrix_swept(ks)
-    if not grouped:
-        return out
-    lib = _lib.load()
-    ks = np.asarray(ks, dtype=np.float64)
+        (grouped if s._swept_batched_available() and padded_order(s._basis_count()) <= 1600 else single).append(i)
+    if groups is None:
+        lib = _lib.load()
 
-    def per_matrix(nb):
-        return nb * nb * 24 + lib.mw_zgesv_mixed_batched_workspace_size(nb, 1, 1) + nb * 64
+        def per_matrix(nb):
+            return nb * nb * 24 + lib.mw_zgesv_mixed_batched_workspace_size(nb, 1, 1) + nb * 64
+
+        groups = _DeviceGroups
+    else:
+        def per_matrix(nb):
+            return nb * nb * 24
 
     plan = group_plan([solvers[i]._basis_count() for i in grouped], len(ks), budget_bytes, per_matrix)
     # the heaviest groups first: the first group waits for its host tables,
-    # after which the helper thread prepares the rest while the GPU works
+    # after which the helper prepares the rest while the GPU works
     plan.sort(key=lambda g: -len(g[1]) * g[0] ** 3)
-    dev = solvers[grouped[0]]._torch_device()
-    stream = torch.cuda.current_stream(dev).cuda_stream
-    P_max = max(solvers[i]._port_count() for i in grouped)
-    arena = torch.empty(max(_group_bytes(len(g) * len(ks), nb, P_max) for nb, g in plan), dtype=torch.uint8,
-                        device=dev)
-    # one host thread prepares the next structures' tables (host build and
-    # upload on its own stream) while this thread fills and solves
-    import concurrent.futures as cf
-
-    prep_stream = torch.cuda.Stream(device=dev)
-    ports = {}
-
-    def prep(i):
-        with torch.cuda.device(dev), torch.cuda.stream(prep_stream):
-            solvers[i]._dev_tables()
-            solvers[i]._loading_dev_tables()
-            ports[i] = solvers[i]._port_columns()[0]
-            prep_stream.synchronize()
-
-    with cf.ThreadPoolExecutor(max_workers=1) as ex:
-        futs = {grouped[j]: ex.submit(prep, grouped[j]) for _nb, members in plan for j in members}
-        for nb, members in plan:
-            ids = [grouped[j] for j in members]
-
-            def wait(g, ids=ids):
-                futs[ids[g]].result()
-
-            res, _it = _solve_group([solvers[i] for i in ids], nb, ks, stream, arena=arena, wait=wait,
-                                    Bs=_Ports(ports, ids))
+    plan_ids = [(nb, [grouped[j] for j in members]) for nb, members in plan]
+    out = {}
+    if not plan_ids and not single:
+        return out
+    P_max = max([solvers[i]._port_count() for i in grouped] or [1])
+    runner = groups(solvers, ks, plan_ids, P_max) if plan_ids else None
+    try:
+        for i in single:
+            out[i] = runner.single(solvers[i]) if runner is not None else solvers[i].compute_y_matrix_swept(ks)
+        for nb, ids in plan_ids:
+            res = runner.solve(nb, ids)
             for g, i in enumerate(ids):
                 out[i] = res[g]
-    return out
+    finally:
+        if runner is not None:
+            runner.close()
+    return {i: out[i] for i in indices}
 
 
 def mixed_sweep_fn(device=None):

@@ -66,6 +66,79 @@ def test_two_rank_gather_matches_single_rank():
     assert got == want
 
 
+class _FakeGroups:
+    """Stand-in group solver (no GPU): each structure's Y stack is filled
+    with (segments + 1j * wires), tagged with the padded order it was
+    grouped at, so that the test can check both the routing and the merge."""
+
+    log = []
+
+    def __init__(self, solvers, ks, plan, P_max):
+        self.solvers, self.ks = solvers, ks
+
+    def _y(self, s, tag):
+        kw_segs = sum(sum(npe) for npe in s.n_per_edge_per_wire)
+        return np.full((len(self.ks), 1, 1), kw_segs + 1j * len(s.wires_polylines) + 1000 * tag)
+
+    def solve(self, nb, ids):
+        _FakeGroups.log.append((nb, list(ids)))
+        return {g: self._y(self.solvers[i], sweep.padded_order(self.solvers[i]._basis_count()) == nb)
+                for g, i in enumerate(ids)}
+
+    def single(self, solver):
+        return self._y(solver, 0)
+
+    def close(self):
+        pass
+
+
+def _grouped_rank(rank, world, port, out):
+    """The bench's shard path on one gloo rank: this rank's LPT share,
+    ``grouped_mixed_sweep(indices=...)`` with a stand-in group solver, and
+    the rank-0 merge."""
+    import torch.distributed as dist
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    structs, ks = yagi_sweep(n_structures=11, n_freq=3, seed=2)
+    idx = sweep.shard_indices(structs, rank, world)
+    local = sweep.grouped_mixed_sweep(structs, ks, indices=idx, groups=_FakeGroups)
+    assert sorted(local) == sorted(idx)
+    merged = sweep.gather(local)
+    if rank == 0:
+        out.put({i: complex(v[0, 0, 0]) for i, v in merged.items()})
+    dist.destroy_process_group()
+
+
+def test_two_rank_grouped_sweep_shards_and_merges():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_grouped_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = q.get(timeout=180)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    structs, _ks = yagi_sweep(n_structures=11, n_freq=3, seed=2)
+    # every structure once, grouped at its own padded order (tag 1000)
+    want = {i: complex(sum(kw["n_per_edge_per_wire"]) + 1000, len(kw["wires"])) for i, kw in enumerate(structs)}
+    assert got == want
+
+
+def test_grouped_sweep_groups_by_padded_order_single_rank():
+    structs, ks = yagi_sweep(n_structures=7, n_freq=2, seed=3)
+    _FakeGroups.log = []
+    out = sweep.grouped_mixed_sweep(structs, ks, groups=_FakeGroups)
+    assert sorted(out) == list(range(7))
+    seen = sorted(i for _nb, ids in _FakeGroups.log for i in ids)
+    assert seen == list(range(7))
+    # groups in decreasing work order, one padded order each
+    work = [len(ids) * nb ** 3 for nb, ids in _FakeGroups.log]
+    assert work == sorted(work, reverse=True)
+
+
 def test_padded_order_ladder():
     """Padded orders are multiples of 32, at most ~20 % above n, monotone."""
     prev = 0

@@ -16,7 +16,9 @@ For ``ground_model="sommerfeld"`` the remainder surfaces come from the
 reference's quadrature grid (``sommerfeld_method="grid"``, the default and
 the drop-in) or from the learned surrogate (``"surrogate"``), which falls
 back to the grid outside its domain or when a quadrature spot check of the
-structure misses ``SURROGATE_BOUND``.
+structure misses ``surrogate_tol`` (relative surface error; default 1e-6,
+which the shipped network does not reach, so the grid serves -- the
+surrogate is an approximation at ``surrogate_tol=surrogate.APPROX_TOL``).
 """
 
 from __future__ import annotations
@@ -243,6 +245,7 @@ class BSplineSolver:
         precision="fp64",
         device=None,
         sommerfeld_method="grid",
+        surrogate_tol=sur.DEFAULT_TOL,
     ):
         self._cancel = cancel
         V.settings(dict(degree=degree, wires=wires, use_singular_enrichment=use_singular_enrichment,
@@ -261,6 +264,9 @@ class BSplineSolver:
         self.auto_tap_ratio_threshold = float(auto_tap_ratio_threshold)
         self.precision = precision
         self.sommerfeld_method = sommerfeld_method
+        if not float(surrogate_tol) > 0.0:
+            raise ValueError(f"surrogate_tol must be > 0, got {surrogate_tol!r}")
+        self.surrogate_tol = float(surrogate_tol)
         self.last_sommerfeld = None
         # mixed: stop refining once the largest relative correction of any
         # port column is below this (the remaining error is then ~ kappa *
@@ -746,8 +752,9 @@ class BSplineSolver:
         """(model, info) when the surrogate may serve this structure at this
         k, else (None, info with the reason): the weights must exist, eps~
         and f and every Gauss-node pair must lie in the training domain, and
-        the largest error of a quadrature spot check on sampled node pairs
-        must be within SURROGATE_BOUND (of the surfaces' scale)."""
+        the largest error of a quadrature spot check on sampled node pairs,
+        relative to the largest quadrature surface value, must be within
+        ``surrogate_tol``."""
         model = sur.get_model(self._torch_device())
         if model is None:
             return None, {"reason": "no surrogate weights"}
@@ -772,11 +779,11 @@ class BSplineSolver:
         d = nodes[a] - nodes[b]
         rho = np.hypot(d[:, 0], d[:, 1]) / lam
         h = ((nodes[a, 2] - self.ground_z) + (nodes[b, 2] - self.ground_z)) / lam
-        err = float(sur.spot_check(model, rho, h, et, f))
-        info = {"spot_max_err": err, "struct_features": sur.features(0.0, 1.0, et, f)[2:5]}
-        if not err <= sur.SURROGATE_BOUND:
+        err, rel = sur.spot_check(model, rho, h, et, f)
+        info = {"spot_max_err": err, "spot_rel_err": rel, "struct_features": sur.features(0.0, 1.0, et, f)[2:5]}
+        if not rel <= self.surrogate_tol:
             info.pop("struct_features")
-            info["reason"] = "spot check over the bound"
+            info["reason"] = f"spot check {rel:.2e} over surrogate_tol {self.surrogate_tol:.1e}"
             return None, info
         return model, info
 

@@ -17,8 +17,18 @@ same frequency factor a scaled grid carries.  The forward, backward and Adam
 steps are hand-written CUDA (``mlp.cu``); inference runs on tcgen05 tensor
 cores, standalone (``mw_mlp_infer``) or fused into the remainder fill
 (``mw_somm_remainder_q_mlp``).  Queries outside ``DOMAIN`` and structures
-whose spot check against quadrature misses the error bound take the grid
-path instead.
+whose spot check against quadrature misses the error tolerance take the
+grid path instead.
+
+Accuracy.  The shipped network reproduces the surfaces to about 1e-3 of
+their size (held-out rms 2.5e-3 of SCALE), which moves drive-point
+impedances by 1e-4 to 3e-3 -- far outside the 1e-6 that the mixed-precision
+path holds to.  A structure is therefore served only when the spot check's
+relative surface error is within the solver's ``surrogate_tol``: at the
+default, ``DEFAULT_TOL`` = 1e-6, the shipped network serves no structure of
+the seeded Sommerfeld workload and every solve takes the quadrature grid;
+with ``surrogate_tol=APPROX_TOL`` it serves them as an approximation, which
+is not counted toward the 1e-6 gate.
 """
 
 from __future__ import annotations
@@ -46,12 +56,14 @@ F_HZ = (2.5e6, 35e6)
 
 WEIGHTS_PATH = Path(__file__).resolve().parent / "data" / "somm_mlp.npz"
 
-# spot check: node pairs sampled per structure and the largest accepted
-# |surrogate - quadrature| / SCALE over them
+# spot check: node pairs sampled per structure; the surrogate serves a
+# structure when max |surrogate - quadrature| / max |quadrature| over them
+# is within the solver's surrogate_tol
 SPOT_PAIRS = 64
-SURROGATE_BOUND = 2e-2
-# drive-point impedance agreement with the quadrature-grid path that the
-# shipped weights are tested to (|dZin| / |Zin| on seeded structures)
+DEFAULT_TOL = 1e-6
+# the approximation setting: the shipped network serves the seeded
+# structures at drive-point impedances within ZIN_TOL of the grid path
+APPROX_TOL = 2e-2
 ZIN_TOL = 1e-2
 
 
@@ -285,7 +297,9 @@ def get_model(device):
 
 
 def spot_check(model, rho_wl, h_wl, eps, f_hz):
-    """Largest |surrogate - quadrature| / SCALE over the given queries."""
+    """(largest |surrogate - quadrature| / SCALE, the same relative to the
+    largest |quadrature|) over the given queries."""
     q = quadrature_surfaces(rho_wl, h_wl, np.full(np.shape(rho_wl), eps), model.device)
     p = model.surfaces(rho_wl, h_wl, eps, f_hz)
-    return float((p - q).abs().max()) / SCALE
+    d = float((p - q).abs().max())
+    return d / SCALE, d / max(float(q.abs().max()), 1e-300)

@@ -81,16 +81,31 @@ def test_static_pivots_within_the_block(cuda_device):
     assert rel_err(x, np.linalg.solve(Z, B)) < 1e-9
 
 
+def _swapped_blocks(n, rng):
+    """100 I + 1e-3 noise with the two 128-row halves exchanged: every
+    diagonal block holds only the noise, the large entries sit below it."""
+    Z = 100.0 * np.eye(n) + 1e-3 * (rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n)))
+    return Z[np.concatenate([np.arange(128, 256), np.arange(0, 128)])]
+
+
 def test_nearly_singular_blocks_fall_back(cuda_device):
-    """Rows of neighbouring blocks exchanged: each diagonal block holds only
-    small entries, |L21| grows past the bound, and the solve is repeated
-    with partial pivoting."""
+    """|L21| grows far past the bound (~1e5): the static factorisation is
+    rejected and the solve repeated with partial pivoting."""
     rng = np.random.default_rng(11)
-    n = 256
-    Z = _diag_heavy(n, rng)
-    perm = np.concatenate([np.arange(128, 256), np.arange(0, 128)])
-    Z = Z[perm]
-    B = rng.standard_normal((n, 4)) + 1j * rng.standard_normal((n, 4))
+    Z = _swapped_blocks(256, rng)
+    B = rng.standard_normal((256, 4)) + 1j * rng.standard_normal((256, 4))
+    x, _it, used = _zgesv_mixed(Z, B, cuda_device, 0)
+    assert used == 2
+    assert rel_err(x, np.linalg.solve(Z, B)) < 1e-9
+
+
+def test_exact_zero_block_pivot_falls_back(cuda_device):
+    """A diagonal block with an exactly zero column: the block is singular,
+    so the static factorisation is rejected (the matrix itself is not)."""
+    rng = np.random.default_rng(12)
+    Z = _swapped_blocks(256, rng)
+    Z[:128, 5] = 0.0
+    B = rng.standard_normal((256, 2)) + 1j * rng.standard_normal((256, 2))
     x, _it, used = _zgesv_mixed(Z, B, cuda_device, 0)
     assert used == 2
     assert rel_err(x, np.linalg.solve(Z, B)) < 1e-9

@@ -447,6 +447,8 @@ def run_b200(args, kw):
         "phases": phases,
         "pivoting": {0: "static (diagonal block)", 1: "partial", 2: "static rejected, then partial"}.get(
             int(lib.mw_last_mixed_pivoting()), None) if args.precision == "mixed" else "partial",
+        "static_pivot_max_abs_l21": float(lib.mw_last_mixed_growth()) if args.precision == "mixed" else None,
+        "refinement": solver.last_refinement,
         "clocks": clocks.summary(),
         "y_rel_err_vs_reference": y_err,
         "fp64_ms_per_step": fp64_ms,

@@ -51,7 +51,8 @@ int64_t mw_launch_count(void);
  * launch on its own stream (for roofline figures).  Classes: 0 same-edge
  * table, 1 fill, 2 image fill, 3 LU panel, 4 row swaps, 5 triangular solve
  * block, 6 complex128 GEMM, 7 tensor-core complex GEMM, 8 refinement,
- * 9 other, 10 Sommerfeld grid, 11 Sommerfeld remainder; 12 and 13 enclose
+ * 9 other, 10 Sommerfeld grid, 11 Sommerfeld remainder, 14 the rows
+ * below a static-pivot panel's diagonal block; 12 and 13 enclose
  * whole factorisations and whole many-right-hand-side triangular solves
  * (their wall time on the calling stream, overlapping classes 3-9).
  * mw_profile_enable(1) clears the counters and starts recording;
@@ -345,6 +346,10 @@ int32_t mw_set_mixed_pivoting(int32_t mode);
 /* Pivoting the last mw_zgesv_mixed on this host thread used: 0 static,
  * 1 partial, 2 static rejected then partial; -1 before the first call. */
 int32_t mw_last_mixed_pivoting(void);
+
+/* Largest |L21| (|re| + |im|) of the last static-pivot factorisation made
+ * by mw_zgesv_mixed on this host thread (partial pivoting keeps it <= 1). */
+double mw_last_mixed_growth(void);
 
 /*
  * Frequency-batched fill: Z_b (and Z32_b when Z32 != NULL) for n_k

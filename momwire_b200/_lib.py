@@ -118,6 +118,7 @@ _SIGS = {
     "mw_selftest_wait_timeout": (i32, [i32, i64, vp, vp]),
     "mw_set_mixed_pivoting": (i32, [i32]),
     "mw_last_mixed_pivoting": (i32, []),
+    "mw_last_mixed_growth": (f64, []),
     "mw_same_edge_table": (i32, [C.POINTER(Edges), i32, i32, i32, f64, vp, vp]),
     "mw_offedge_moments": (i32, [C.POINTER(Segments), C.POINTER(Segments), i32, i32, f64, i32, f64, vp, vp, vp, vp]),
     "mw_fill_z": (i32, [C.POINTER(Segments), C.POINTER(BasisT), vp, C.POINTER(Edges), C.POINTER(Freq), i32, vp, i64, vp, i64, vp]),
@@ -169,7 +170,7 @@ _SIGS = {
 EXPORTED = tuple(_SIGS)
 
 PROFILE_CLASSES = ("same_edge_table", "fill", "fill_image", "lu_panel", "laswp", "trsm", "zgemm",
-                   "cgemm_tc", "refine", "misc", "somm_grid", "somm_q", "factor_wall", "solve_wall")
+                   "cgemm_tc", "refine", "misc", "somm_grid", "somm_q", "factor_wall", "solve_wall", "lu_l21")
 
 
 def profile_enable(on=True):

@@ -101,6 +101,22 @@ def _torch():
     return torch
 
 
+def _swept_y(Xt, B, A):
+    """Y stack (n_k, P, P) from the swept solutions Xt (n_k, P + n_c, n),
+    each X_k^T of Z_k [W | Xc] = [B | A^T]: with KCL rows the Schur step
+    Lambda = (A Xc)^-1 (A W), X = W - Xc Lambda (``bspline.py:2980-2989``),
+    then Y = B^T X."""
+    P = B.shape[1]
+    Wt = Xt[:, :P, :]
+    if A.shape[0]:
+        Xct = Xt[:, P:, :]
+        S = np.einsum("cn,kdn->kcd", A, Xct)  # A Xc   (n_k, n_c, n_c)
+        AW = np.einsum("cn,kpn->kcp", A, Wt)  # A W    (n_k, n_c, P)
+        Lam = np.linalg.solve(S, AW)  # (n_k, n_c, P)
+        Wt = Wt - np.einsum("kcp,kcn->kpn", Lam, Xct)
+    return np.einsum("kpn,nq->kqp", Wt, B)
+
+
 class _DeviceTables:
     """Device copies of the k-independent tables plus their C structs."""
 
@@ -959,27 +975,54 @@ class BSplineSolver:
     def compute_y_matrix_swept(self, k_array) -> np.ndarray:
         """(n_k, n_ports, n_ports) Y matrices (``_port_solution.py:142``).
 
-        With ``precision="mixed"`` on free space or a PEC ground and no KCL
-        constraint rows, every frequency of a chunk is filled in one batched
-        launch and factorised together (``_swept_batched``); otherwise each
-        k takes the single-solve path."""
+        On free space or a PEC ground every frequency of a chunk is filled in
+        one batched launch; with ``precision="mixed"`` the chunk is then
+        factorised together (``_swept_batched``), with ``"fp64"`` each
+        matrix of the stack takes the complex128 LU (``_swept_fp64_batched``,
+        the reference's k-batched fill with stacked LAPACK solves).  KCL
+        constraint rows (junctions) ride along as extra right-hand sides and
+        the Schur step closes each frequency (``bspline.py:3017-3038``).
+        Other grounds take the single-solve path per k."""
         k_array = np.asarray(k_array, dtype=float)
         self._checkpoint()
+        if k_array.shape[0] == 0:
+            n_p = self._port_count()
+            return np.zeros((0, n_p, n_p), dtype=np.complex128)
         if self._swept_batched_available():
             return self._swept_batched(k_array)
+        if self._swept_fp64_batched_available():
+            return self._swept_fp64_batched(k_array)
         n_p = self._port_count()
         out = np.zeros((k_array.shape[0], n_p, n_p), dtype=np.complex128)
         for i, sol in enumerate(self.compute_port_solution_swept(k_array)):
             out[i] = sol.y
         return out
 
+    # KCL rows a batched sweep carries as extra right-hand sides
+    SWEPT_MAX_KCL = 64
+
     def _swept_batched_available(self):
-        """Batched route: mixed precision, free space or PEC image (finite
-        grounds carry per-k weight tables), no KCL rows left after the port
-        split, order within the batched panel's limit."""
+        """Batched mixed route: mixed precision, free space or PEC image
+        (finite grounds carry per-k weight tables), at most SWEPT_MAX_KCL
+        KCL rows left after the port split, order within the batched
+        panel's limit."""
         if self.precision != "mixed" or self.ground_eps is not None:
             return False
-        return self._kcl_rows_left() == 0 and self._basis_count() <= 1600
+        return self._kcl_rows_left() <= self.SWEPT_MAX_KCL and self._basis_count() <= 1600
+
+    def _swept_fp64_batched_available(self):
+        """Batched-fill FP64 route: complex128, free space or PEC image, at
+        most SWEPT_MAX_KCL KCL rows."""
+        return (self.precision == "fp64" and self.ground_eps is None
+                and self._kcl_rows_left() <= self.SWEPT_MAX_KCL)
+
+    def _sweep_rhs(self):
+        """(R, B, A): the right-hand sides of a swept solve, R = [B | A^T]
+        (n x (P + n_c), complex128) with B the port columns and A the dense
+        KCL constraint rows (n_c x n)."""
+        B, kcl = self._port_columns()
+        A = kcl.toarray().astype(np.complex128) if kcl.shape[0] else np.zeros((0, B.shape[0]), np.complex128)
+        return np.hstack([B, A.T]), B, A
 
     def _basis_count(self):
         """Order of the system without building the basis: per wire its
@@ -997,7 +1040,7 @@ class BSplineSolver:
         grounded = self._grounded_junctions()
         return sum(1 for j in range(len(self.junctions)) if j not in grounded) - len(self.junction_ports)
 
-    def _fill_batched(self, ks, stream, Z=None, Z32=None, ld=None, k_dev=None):
+    def _fill_batched(self, ks, stream, Z=None, Z32=None, ld=None, k_dev=None, want32=True):
         """(Z, Z32): device (n_k, n, n) complex128 / complex64 stacks, each
         matrix column-major (Z[b].T is the matrix at ks[b]), from one
         batched fill launch.  Given Z / Z32 of shape (n_k, ld, ld) with
@@ -1016,13 +1059,13 @@ class BSplineSolver:
         table = torch.empty((nk, max(dt.table_rows, 1), d + 1, d + 1), dtype=torch.complex128, device=dev)
         if Z is None:
             Z = torch.empty((nk, ld, ld), dtype=torch.complex128, device=dev)
-        if Z32 is None:
+        if Z32 is None and want32:
             Z32 = torch.empty((nk, ld, ld), dtype=torch.complex64, device=dev)
         pec = 1 if self.ground_z is not None else 0
         _lib.call("mw_fill_z_batch", C.byref(dt.seg), C.byref(dt.basis), C.byref(dt.edges), nk, kb.data_ptr(),
                   ob.data_ptr(), float(self.eps), float(self.mu), self.n_qp_pair, int(self.extended_kernel),
-                  float(self.ground_z or 0.0), pec, table.data_ptr(), Z.data_ptr(), ld, ld * ld, Z32.data_ptr(),
-                  ld, ld * ld, stream)
+                  float(self.ground_z or 0.0), pec, table.data_ptr(), Z.data_ptr(), ld, ld * ld,
+                  Z32.data_ptr() if Z32 is not None else None, ld, ld * ld, stream)
         self._loading_device(Z, Z32, np.asarray(ks, dtype=np.float64) * self.c, stream, ld=ld)
         return Z, Z32
 
@@ -1073,16 +1116,16 @@ class BSplineSolver:
         dt = self._dev_tables()
         basis = self._basis()
         n, d = basis.n, self.degree
-        B, _kcl = self._port_columns()
-        n_p = B.shape[1]
+        R, B, A = self._sweep_rhs()
+        n_p = R.shape[1]
         per_k = n * n * (16 + 8) + dt.table_rows * (d + 1) ** 2 * 16 + n * n_p * 48 + n * 4
         chunk = int(max(1, min(len(k_array), 65535, mem_budget_bytes // max(per_k, 1))))
         st = torch.cuda.current_stream(dev).cuda_stream
         lib = _lib.load()
         Bh = torch.empty((n_p, n), dtype=torch.complex128, pin_memory=True)
-        Bh.copy_(torch.from_numpy(np.ascontiguousarray(B.T)))
-        Bd = Bh.to(dev, non_blocking=True)  # column-major n x n_p
-        out = np.zeros((len(k_array), n_p, n_p), dtype=np.complex128)
+        Bh.copy_(torch.from_numpy(np.ascontiguousarray(R.T)))
+        Bd = Bh.to(dev, non_blocking=True)  # column-major n x (P + n_c)
+        out = np.zeros((len(k_array), B.shape[1], B.shape[1]), dtype=np.complex128)
         iters = []
         for c0 in range(0, len(k_array), chunk):
             self._checkpoint()
@@ -1100,10 +1143,58 @@ class BSplineSolver:
                       ipiv.data_ptr(), info.data_ptr(), Bd.data_ptr(), n, 0, X.data_ptr(), float(self.mixed_tol),
                       int(self.mixed_max_iter), ws.data_ptr(), wsb, C.byref(it), C.byref(corr), st)
             iters.append(int(it.value))
-            Xh = X.cpu().numpy()  # (nk, n_p, n): X_k^T
-            out[c0 : c0 + nk] = np.einsum("kpn,nq->kqp", Xh, B)
+            out[c0 : c0 + nk] = _swept_y(X.cpu().numpy(), B, A)  # X: (nk, P + n_c, n), X_k^T
             del Z, Z32, X, ws
         self.last_refinement = {"iterations": max(iters) if iters else 0, "chunks": len(iters)}
+        return out
+
+    def _swept_fp64_batched(self, k_array, mem_budget_bytes=16 << 30):
+        """FP64 sweep: per chunk of frequencies one batched complex128 fill,
+        then each matrix of the stack factorised and solved in complex128
+        (``mw_zgetrf`` / ``mw_zgetrs``) on the device, the right-hand sides
+        [B | A^T] uploaded once; Y_k from the Schur step on the host."""
+        torch = _torch()
+        dev = self._torch_device()
+        dt = self._dev_tables()
+        n, d = self._basis().n, self.degree
+        R, B, A = self._sweep_rhs()
+        m = R.shape[1]
+        per_k = n * n * 16 + dt.table_rows * (d + 1) ** 2 * 16 + n * m * 16 + n * 4
+        chunk = int(max(1, min(len(k_array), 65535, mem_budget_bytes // max(per_k, 1))))
+        st = torch.cuda.current_stream(dev).cuda_stream
+        lib = _lib.load()
+        Rh = torch.empty((m, n), dtype=torch.complex128, pin_memory=True)
+        Rh.copy_(torch.from_numpy(np.ascontiguousarray(R.T)))
+        Rd = Rh.to(dev, non_blocking=True)  # column-major n x (P + n_c)
+        wsb = lib.mw_getrf_workspace_size(n)
+        ws = torch.empty(wsb, dtype=torch.uint8, device=dev)
+        cancel = C.c_void_p(self._cancel.ptr) if self._cancel is not None else None
+        out = np.zeros((len(k_array), B.shape[1], B.shape[1]), dtype=np.complex128)
+        for c0 in range(0, len(k_array), chunk):
+            self._checkpoint()
+            ks = np.asarray(k_array[c0 : c0 + chunk], dtype=np.float64)
+            nk = len(ks)
+            Z, _ = self._fill_batched(ks, st, want32=False)
+            X = Rd.unsqueeze(0).repeat(nk, 1, 1)  # (nk, m, n): X_k^T, overwritten by the solves
+            ipiv = torch.empty((nk, n), dtype=torch.int32, device=dev)
+            info = torch.zeros((nk, 2), dtype=torch.int32, device=dev)
+            for b in range(nk):
+                try:
+                    _lib.call("mw_zgetrf", n, Z[b].data_ptr(), n, ipiv[b].data_ptr(), info[b].data_ptr(),
+                              ws.data_ptr(), wsb, cancel, st)
+                except _lib.NativeError as e:
+                    if e.status == _lib.MW_ERR_CANCELLED:
+                        raise SolveAborted() from e
+                    raise
+                _lib.call("mw_zgetrs", n, m, Z[b].data_ptr(), n, ipiv[b].data_ptr(), X[b].data_ptr(), n, st)
+            hinfo = info.cpu().numpy()
+            if np.any(hinfo[:, 1] != 0):
+                raise RuntimeError("factorisation: a bounded device wait timed out")
+            if np.any(hinfo[:, 0] > 0):
+                raise np.linalg.LinAlgError("Singular matrix")
+            out[c0 : c0 + nk] = _swept_y(X.cpu().numpy(), B, A)
+            del Z, X
+        self.last_refinement = None
         return out
 
     def compute_impedance_swept(self, k_array):

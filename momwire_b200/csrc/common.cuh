@@ -112,7 +112,8 @@ enum ProfileClass {
     PC_SOMM_Q = 11,
     PC_FACTOR = 12,  // whole factorisations (wall, enclosing the classes above)
     PC_SOLVE = 13,   // whole triangular solves with many right-hand sides (wall)
-    PC_COUNT = 14
+    PC_L21 = 14,     // static-pivot panels: the rows below the diagonal block
+    PC_COUNT = 15
 };
 
 struct ProfileScope {

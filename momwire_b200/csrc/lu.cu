@@ -34,7 +34,9 @@ size_t cgemm_tc_workspace(int64_t m, int64_t n, int64_t k);
 
 // static-pivot panel of the complex64 path (lu_static.cu)
 mw_status static_panel_c64(cf* A, int64_t lda, int64_t n, int64_t j0, int jb, int32_t* ipiv, int32_t* info,
-                           PanelWs* ws, cf* inv_diag, cudaStream_t st);
+                           PanelWs* ws, cf* inv_diag, int32_t* perm, cudaStream_t st);
+void static_permute_c64(cf* A, int64_t lda, int64_t row0, int jb, int64_t col0, int64_t ncols, const int32_t* perm,
+                        cudaStream_t st);
 
 constexpr int kNB = 64;         // panel half width (rank-1 work per cooperative panel)
 constexpr int kOuterNB = 128;   // getrf block: panel width and trailing-update k
@@ -591,9 +593,11 @@ struct GetrsLeaf<cf> {
 
 // X (jb x ncols, leading dim ldx) <- L^-1 X with L unit lower (jb x jb),
 // or U^-1 X with U upper non-unit (jb <= leaf).  The CTA stages the triangle
-// in shared memory; each warp then owns one column of X in registers (lane
-// l holds rows l, l+32, ...) and substitutes with warp shuffles only.
+// in shared memory; each warp then owns kTrsmCols columns of X in registers
+// (lane l holds rows RP*l .. RP*l+RP-1 of each) and substitutes with warp
+// shuffles only, every staged triangle element read once for all of them.
 constexpr int kTrsmWarps = 8;
+constexpr int kTrsmCols = 4;  // columns per warp
 template <class T, bool UPPER, int L>
 __global__ void __launch_bounds__(32 * kTrsmWarps) trsm_kernel(const T* Tm, int64_t ldt, T* X, int64_t ldx, int jb,
                                                                int64_t ncols, const T* Aoff, int64_t ldo, const T* Xp,
@@ -611,6 +615,7 @@ __global__ void __launch_bounds__(32 * kTrsmWarps) trsm_kernel(const T* Tm, int6
     // same lane-major form -- the next-block update of a blocked sweep, done
     // where its result is consumed.
     constexpr int RP = L / 32;
+    constexpr int NC = kTrsmCols;
     static_assert(RP * 32 == L, "leaf order must be a multiple of 32");
     extern __shared__ __align__(16) unsigned char trsm_smem[];
     T* S = reinterpret_cast<T*>(trsm_smem);
@@ -646,30 +651,43 @@ __global__ void __launch_bounds__(32 * kTrsmWarps) trsm_kernel(const T* Tm, int6
             }
         }
     };
-    const int64_t col = (int64_t)blockIdx.x * kTrsmWarps + warp;
-    const bool active = col < ncols;  // (a whole warp; it stays for the barriers)
-    T* x = X + (active ? col : 0) * ldx;
-    T v[RP];
+    const int64_t col0 = ((int64_t)blockIdx.x * kTrsmWarps + warp) * NC;
+    const bool active = col0 < ncols;  // (a whole warp; it stays for the barriers)
+    bool cok[NC];
 #pragma unroll
-    for (int a = 0; a < RP; ++a) v[a] = active && RP * lane + a < jb ? x[RP * lane + a] : zero;
+    for (int q = 0; q < NC; ++q) cok[q] = col0 + q < ncols;
+    T v[NC][RP];
+#pragma unroll
+    for (int q = 0; q < NC; ++q)
+#pragma unroll
+        for (int a = 0; a < RP; ++a)
+            v[q][a] = cok[q] && RP * lane + a < jb ? X[(col0 + q) * ldx + RP * lane + a] : zero;
     if (K > 0) {
         stage(Aoff, ldo, jb, K, 0);
         __syncthreads();
         if (active) {
-            const T* xq = Xp + col * ldx;
-            T xp[RP];
+            T xp[NC][RP];
 #pragma unroll
-            for (int a = 0; a < RP; ++a) xp[a] = RP * lane + a < K ? xq[RP * lane + a] : zero;
+            for (int q = 0; q < NC; ++q)
+#pragma unroll
+                for (int a = 0; a < RP; ++a)
+                    xp[q][a] = cok[q] && RP * lane + a < K ? Xp[(col0 + q) * ldx + RP * lane + a] : zero;
             const int nkq = (K + RP - 1) / RP;
             for (int kb = 0; kb < nkq; ++kb) {
                 const T* Sk = S + kb * RP * RP * 32;
-                T xb[RP];
+                T xb[NC][RP];
 #pragma unroll
-                for (int b = 0; b < RP; ++b) xb[b] = shfl_c(xp[b], kb);
+                for (int q = 0; q < NC; ++q)
+#pragma unroll
+                    for (int b = 0; b < RP; ++b) xb[q][b] = shfl_c(xp[q][b], kb);
 #pragma unroll
                 for (int a = 0; a < RP; ++a)
 #pragma unroll
-                    for (int b = 0; b < RP; ++b) v[a] = v[a] - Sk[(a * RP + b) * 32 + (lane ^ (a * (32 / RP)))] * xb[b];
+                    for (int b = 0; b < RP; ++b) {
+                        const T sab = Sk[(a * RP + b) * 32 + (lane ^ (a * (32 / RP)))];
+#pragma unroll
+                        for (int q = 0; q < NC; ++q) v[q][a] = v[q][a] - sab * xb[q][b];
+                    }
             }
         }
         __syncthreads();  // S is the triangle's from here
@@ -682,57 +700,85 @@ __global__ void __launch_bounds__(32 * kTrsmWarps) trsm_kernel(const T* Tm, int6
     if (!UPPER) {
         for (int kb = 0; kb < nkb; ++kb) {
             const T* Sk = S + kb * RP * RP * 32;
-            T xb[RP];
+            T xb[NC][RP];
 #pragma unroll
-            for (int b = 0; b < RP; ++b) xb[b] = zero;
+            for (int q = 0; q < NC; ++q)
+#pragma unroll
+                for (int b = 0; b < RP; ++b) xb[q][b] = zero;
             if (lane == kb) {
 #pragma unroll
                 for (int a = 0; a < RP; ++a) {
-                    T t = v[a];
 #pragma unroll
-                    for (int b = 0; b < a; ++b) t = t - Sk[(a * RP + b) * 32 + (lane ^ (a * (32 / RP)))] * xb[b];
-                    xb[a] = t;
-                    v[a] = t;
+                    for (int q = 0; q < NC; ++q) {
+                        T t = v[q][a];
+#pragma unroll
+                        for (int b = 0; b < a; ++b)
+                            t = t - Sk[(a * RP + b) * 32 + (lane ^ (a * (32 / RP)))] * xb[q][b];
+                        xb[q][a] = t;
+                        v[q][a] = t;
+                    }
                 }
             }
 #pragma unroll
-            for (int b = 0; b < RP; ++b) xb[b] = shfl_c(xb[b], kb);
+            for (int q = 0; q < NC; ++q)
+#pragma unroll
+                for (int b = 0; b < RP; ++b) xb[q][b] = shfl_c(xb[q][b], kb);
             if (lane > kb) {
 #pragma unroll
                 for (int a = 0; a < RP; ++a)
 #pragma unroll
-                    for (int b = 0; b < RP; ++b) v[a] = v[a] - Sk[(a * RP + b) * 32 + (lane ^ (a * (32 / RP)))] * xb[b];
+                    for (int b = 0; b < RP; ++b) {
+                        const T sab = Sk[(a * RP + b) * 32 + (lane ^ (a * (32 / RP)))];
+#pragma unroll
+                        for (int q = 0; q < NC; ++q) v[q][a] = v[q][a] - sab * xb[q][b];
+                    }
             }
         }
     } else {
         for (int kb = nkb - 1; kb >= 0; --kb) {
             const T* Sk = S + kb * RP * RP * 32;
-            T xb[RP];
+            T xb[NC][RP];
 #pragma unroll
-            for (int b = 0; b < RP; ++b) xb[b] = zero;
+            for (int q = 0; q < NC; ++q)
+#pragma unroll
+                for (int b = 0; b < RP; ++b) xb[q][b] = zero;
             if (lane == kb) {
 #pragma unroll
                 for (int a = RP - 1; a >= 0; --a) {
-                    T t = v[a];
 #pragma unroll
-                    for (int b = RP - 1; b > a; --b) t = t - Sk[(a * RP + b) * 32 + (lane ^ (a * (32 / RP)))] * xb[b];
-                    xb[a] = t * sD[RP * lane + a];
-                    v[a] = xb[a];
+                    for (int q = 0; q < NC; ++q) {
+                        T t = v[q][a];
+#pragma unroll
+                        for (int b = RP - 1; b > a; --b)
+                            t = t - Sk[(a * RP + b) * 32 + (lane ^ (a * (32 / RP)))] * xb[q][b];
+                        xb[q][a] = t * sD[RP * lane + a];
+                        v[q][a] = xb[q][a];
+                    }
                 }
             }
 #pragma unroll
-            for (int b = 0; b < RP; ++b) xb[b] = shfl_c(xb[b], kb);
+            for (int q = 0; q < NC; ++q)
+#pragma unroll
+                for (int b = 0; b < RP; ++b) xb[q][b] = shfl_c(xb[q][b], kb);
             if (lane < kb) {
 #pragma unroll
                 for (int a = 0; a < RP; ++a)
 #pragma unroll
-                    for (int b = RP - 1; b >= 0; --b) v[a] = v[a] - Sk[(a * RP + b) * 32 + (lane ^ (a * (32 / RP)))] * xb[b];
+                    for (int b = RP - 1; b >= 0; --b) {
+                        const T sab = Sk[(a * RP + b) * 32 + (lane ^ (a * (32 / RP)))];
+#pragma unroll
+                        for (int q = 0; q < NC; ++q) v[q][a] = v[q][a] - sab * xb[q][b];
+                    }
             }
         }
     }
 #pragma unroll
-    for (int a = 0; a < RP; ++a)
-        if (RP * lane + a < jb) x[RP * lane + a] = v[a];
+    for (int q = 0; q < NC; ++q)
+        if (cok[q]) {
+#pragma unroll
+            for (int a = 0; a < RP; ++a)
+                if (RP * lane + a < jb) X[(col0 + q) * ldx + RP * lane + a] = v[q][a];
+        }
 }
 
 template <class T, int L>
@@ -763,8 +809,9 @@ static void trsm_launch(const T* Tm, int64_t ldt, T* X, int64_t ldx, int jb, int
                         const T* Aoff = nullptr, int64_t ldo = 0, const T* Xp = nullptr, int K = 0) {
     ProfileScope ps(PC_TRSM, st, 4.0 * (double)jb * jb * ncols + 8.0 * (double)jb * K * ncols,
                     2.0 * sizeof(T) * (double)jb * ncols);
-    trsm_kernel<T, UPPER, L><<<(unsigned)((ncols + kTrsmWarps - 1) / kTrsmWarps), 32 * kTrsmWarps,
-                               trsm_smem_bytes<T, L>(), st>>>(Tm, ldt, X, ldx, jb, ncols, Aoff, ldo, Xp, K);
+    const int64_t per_cta = (int64_t)kTrsmWarps * kTrsmCols;
+    trsm_kernel<T, UPPER, L><<<(unsigned)((ncols + per_cta - 1) / per_cta), 32 * kTrsmWarps, trsm_smem_bytes<T, L>(),
+                               st>>>(Tm, ldt, X, ldx, jb, ncols, Aoff, ldo, Xp, K);
     count_launch();
 }
 
@@ -1368,11 +1415,17 @@ static mw_status getrf_lookahead(int64_t n, T* A, int64_t lda, int32_t* ipiv, in
         const int jb = (int)((n - j0) < kOuterNB ? (n - j0) : kOuterNB);
         if (j >= 2) MW_CHECK_CUDA(cudaStreamWaitEvent(st, ax->ev_trail[(j - 2) & 3], 0));
         mw_status s;
+        // static pivots: the block's interchanges never leave it, so they
+        // reach the columns beside it as one parallel row permutation
+        // (double-buffered per block: the trail stream still reads block
+        // j's while the main stream factors block j+1)
+        int32_t* perm = nullptr;
         if constexpr (std::is_same<T, cf>::value) {
             if (static_pivot) {
                 size_t ov, oi, orow, ocur;
                 ws_layout(kMaxPanelGrid, &ov, &oi, &orow, &ocur);
-                s = static_panel_c64(A, lda, n, j0, jb, ipiv, info, pws, reinterpret_cast<cf*>(ws + ocur), st);
+                perm = reinterpret_cast<int32_t*>(ws + ocur + 2048 + (j & 1) * 512);
+                s = static_panel_c64(A, lda, n, j0, jb, ipiv, info, pws, reinterpret_cast<cf*>(ws + ocur), perm, st);
             } else {
                 s = panel_factor<T>(A, lda, n, j0, jb, ipiv, info, ws, up_main, st, kLaPanelCtas);
             }
@@ -1380,6 +1433,15 @@ static mw_status getrf_lookahead(int64_t n, T* A, int64_t lda, int32_t* ipiv, in
             s = panel_factor<T>(A, lda, n, j0, jb, ipiv, info, ws, up_main, st, kLaPanelCtas);
         }
         if (s != MW_OK) return s;
+        auto swap_rows = [&](T* M, int64_t ldm, int64_t col0, int64_t ncols, cudaStream_t sx) {
+            if constexpr (std::is_same<T, cf>::value) {
+                if (perm != nullptr) {
+                    static_permute_c64(M, ldm, j0, jb, col0, ncols, perm, sx);
+                    return;
+                }
+            }
+            laswp_launch<T>(M, ldm, col0, ncols, ipiv, j0, j0 + jb, sx);
+        };
         MW_CHECK_CUDA(cudaEventRecord(ax->ev_main, st));
         // (the swaps of panel j on the columns left of it wait until the
         // end: trail j-1 may still be reading those rows of panel j-1)
@@ -1388,7 +1450,7 @@ static mw_status getrf_lookahead(int64_t n, T* A, int64_t lda, int32_t* ipiv, in
         const int64_t c2 = c1 + jbn;                                      // rest
         if (jbn > 0) {
             if (j >= 1) MW_CHECK_CUDA(cudaStreamWaitEvent(st, ax->ev_trail[(j - 1) & 3], 0));
-            laswp_launch<T>(A, lda, c1, jbn, ipiv, j0, j0 + jb, st);
+            swap_rows(A, lda, c1, jbn, st);
             s = trsm_lower_blocked<T>(A + j0 + j0 * lda, lda, A + j0 + c1 * lda, lda, jb, jbn, up_main, st);
             if (s != MW_OK) return s;
             s = block_update(A + c1 + j0 * lda, lda, A + j0 + c1 * lda, lda, A + c1 + c1 * lda, lda, n - c1, jbn, jb,
@@ -1398,7 +1460,7 @@ static mw_status getrf_lookahead(int64_t n, T* A, int64_t lda, int32_t* ipiv, in
         // trail: everything right of the next block, after panel j
         MW_CHECK_CUDA(cudaStreamWaitEvent(tr, ax->ev_main, 0));
         if (n - c2 > 0) {
-            laswp_launch<T>(A, lda, c2, n - c2, ipiv, j0, j0 + jb, tr);
+            swap_rows(A, lda, c2, n - c2, tr);
             s = trsm_lower_blocked<T>(A + j0 + j0 * lda, lda, A + j0 + c2 * lda, lda, jb, n - c2, up_trail, tr);
             if (s != MW_OK) return s;
             s = block_update(A + c1 + j0 * lda, lda, A + j0 + c2 * lda, lda, A + c1 + c2 * lda, lda, n - c1, n - c2,
@@ -1410,7 +1472,7 @@ static mw_status getrf_lookahead(int64_t n, T* A, int64_t lda, int32_t* ipiv, in
             // this panel's interchanges, L11^-1 on its rows, L21 update below
             // (L21 stays as it is until the deferred left interchanges at the
             // end, which the later rows of Baug then mirror in its own swaps)
-            laswp_launch<T>(Baug, ldb, 0, nrhs, ipiv, j0, j0 + jb, tr);
+            swap_rows(Baug, ldb, 0, nrhs, tr);
             s = trsm_lower_blocked<T>(A + j0 + j0 * lda, lda, Baug + j0, ldb, jb, nrhs, up_trail, tr);
             if (s != MW_OK) return s;
             if (n - c1 > 0) {

@@ -11,7 +11,7 @@
 //                   partial pivoting among its own rows (row interchanges
 //                   kept as a row arrangement, written back once), and
 //   sp_l21_kernel   every row below is solved against the block's upper
-//                   factor, L21 = A21 U11^-1, one warp per eight rows.
+//                   factor, L21 = A21 U11^-1, four warps per 32 rows.
 // The growth the restriction allows is measured: sp_l21_kernel raises the
 // largest |L21| (|re| + |im|) into PanelWs::lmax_bits, and an exact zero
 // pivot sets it to +inf.  The caller refactors with full partial pivoting
@@ -27,8 +27,6 @@ namespace mw {
 
 constexpr int kSpB = 128;          // diagonal block order
 constexpr int kSpDiagThreads = 512;  // 128 rows x 4 groups of 32 columns
-constexpr int kSpRowsPerWarp = 8;
-constexpr int kSpL21Warps = 12;
 constexpr int kSpUStride = kSpB + 2;  // complex elements per shared-memory row of U (16-byte aligned)
 
 namespace {
@@ -53,7 +51,7 @@ __device__ __forceinline__ float cabs1f(cf z) { return fabsf(z.re) + fabsf(z.im)
 // order.  Two barriers per column.
 __global__ void __launch_bounds__(kSpDiagThreads, 1)
     sp_diag_kernel(cf* __restrict__ A, int64_t lda, int64_t j0, int jb, int32_t* __restrict__ ipiv,
-                   int32_t* __restrict__ info, cf* __restrict__ inv_diag, PanelWs* ws) {
+                   int32_t* __restrict__ info, cf* __restrict__ inv_diag, int32_t* __restrict__ perm, PanelWs* ws) {
     __shared__ cf s_col[kSpB];
     __shared__ cf s_u[kSpB];
     __shared__ unsigned long long s_wkey[4];
@@ -122,13 +120,15 @@ __global__ void __launch_bounds__(kSpDiagThreads, 1)
             }
             inv_diag[c] = inv;
         }
-        if (active) {
-            if (g == gc) {
+        if (active && g == gc && !zero) {
 #pragma unroll
-                for (int i = 0; i < 32; ++i)
-                    if (i == ic && !zero) a[i] = l;
-            }
-            if (!zero) {
+            for (int i = 0; i < 32; ++i)
+                if (i == ic) a[i] = l;
+        }
+        // the rank-1 update, skipped by whole warps: column groups left of c
+        // and warps whose rows are all chosen already
+        if (!zero && 32 * g + 31 > c && __any_sync(0xffffffffu, active)) {
+            if (active) {
 #pragma unroll
                 for (int i = 0; i < 32; ++i) {
                     const int col = 32 * g + i;
@@ -144,90 +144,128 @@ __global__ void __launch_bounds__(kSpDiagThreads, 1)
             const int col = 32 * g + i;
             if (col < jb) A[row + (j0 + col) * lda] = a[i];
         }
+        // the block's rows in pivot order: position mypos holds row r
+        if (g == 0) perm[mypos] = r;
     }
 }
 
-// L21 = A21 U11^-1 for the rows below the diagonal block: one warp per eight
-// rows, lane l holding columns 4l .. 4l+3 of each; step j finishes column j
-// on its owner lane, broadcasts it and removes it from the later columns.
-// U11 (upper triangle of the factored block) is staged row-major in shared
-// memory.  The largest |L21| goes to ws->lmax_bits.
-__global__ void __launch_bounds__(32 * kSpL21Warps, 1)
+// Rows [row0, row0 + jb) of columns [col0, col0 + ncols) rearranged in
+// place, row row0 + i taking the old row row0 + perm[i]: one warp per
+// column, all of the column's rows read before any is written.  Applies a
+// diagonal block's interchanges to the columns beside it in one parallel
+// pass (the interchanges never leave the block).
+__global__ void __launch_bounds__(256) sp_permute_kernel(cf* __restrict__ A, int64_t lda, int64_t row0, int jb,
+                                                         int64_t col0, int64_t ncols,
+                                                         const int32_t* __restrict__ perm) {
+    const int lane = threadIdx.x & 31;
+    const int64_t col = col0 + (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (col >= col0 + ncols) return;
+    cf* a = A + col * lda + row0;
+    cf v[kSpB / 32];
+#pragma unroll
+    for (int u = 0; u < kSpB / 32; ++u) {
+        const int i = lane + 32 * u;
+        v[u] = i < jb ? a[perm[i]] : cf{0.0f, 0.0f};
+    }
+    __syncwarp();
+#pragma unroll
+    for (int u = 0; u < kSpB / 32; ++u) {
+        const int i = lane + 32 * u;
+        if (i < jb) a[i] = v[u];
+    }
+}
+
+// L21 = A21 U11^-1 for the rows below the diagonal block.  Four warps share
+// 32 rows: lane i holds row i, warp w its columns 32w .. 32w+31 in
+// registers.  The solve proceeds by column chunks: in phase k warp k
+// finishes chunk k lane-locally (x_j = a_j / U_jj, then a_l -= x_j U_jl for
+// the later columns of the chunk) and publishes it in shared memory; after
+// one barrier the warps of later chunks remove it from theirs (a 32 x 32
+// block product per lane).  No shuffles, no divergence; U11 (upper
+// triangle of the factored block) is staged row-major in shared memory and
+// read as broadcasts.  The largest |L21| goes to ws->lmax_bits.
+constexpr int kSpGroups = 2;                     // 32-row groups per CTA
+constexpr int kSpL21Threads = 32 * 4 * kSpGroups;
+constexpr int kSpXStride = 33;                   // complex elements per row of the exchange buffer
+
+__device__ __forceinline__ void load_u2(const cf* __restrict__ src, cf& u0, cf& u1) {
+    const float4 v = *reinterpret_cast<const float4*>(src);
+    u0 = cf{v.x, v.y};
+    u1 = cf{v.z, v.w};
+}
+
+__global__ void __launch_bounds__(kSpL21Threads, 1)
     sp_l21_kernel(cf* __restrict__ A, int64_t lda, int64_t j0, int jb, int64_t row_end,
                   const cf* __restrict__ inv_diag, PanelWs* ws) {
     extern __shared__ __align__(16) unsigned char sp_smem[];
-    cf* sU = reinterpret_cast<cf*>(sp_smem);              // [kSpB][kSpUStride]
-    cf* sInv = sU + (size_t)kSpB * kSpUStride;            // [kSpB]
+    cf* sU = reinterpret_cast<cf*>(sp_smem);                 // [kSpB][kSpUStride]
+    cf* sInv = sU + (size_t)kSpB * kSpUStride;               // [kSpB]
+    cf* sX = sInv + kSpB;                                    // [2][kSpGroups][32][kSpXStride]
     const int tid = threadIdx.x;
     for (int idx = tid; idx < kSpB * kSpB; idx += blockDim.x) {
         const int j = idx % kSpB, col = idx / kSpB;  // coalesced down each column
         sU[j * kSpUStride + col] = (j <= col && col < jb) ? A[(j0 + j) + (j0 + col) * lda] : cf{0.0f, 0.0f};
     }
     for (int j = tid; j < kSpB; j += blockDim.x) sInv[j] = j < jb ? inv_diag[j] : cf{0.0f, 0.0f};
-    __syncthreads();
     const int lane = tid & 31, warp = tid >> 5;
-    const int64_t rbase = j0 + jb + ((int64_t)blockIdx.x * kSpL21Warps + warp) * kSpRowsPerWarp;
-    if (rbase >= row_end) return;
-    cf a[kSpRowsPerWarp][4];
+    const int w = warp & 3;          // column chunk of this warp
+    const int grp = warp >> 2;       // 32-row group
+    const int64_t row = j0 + jb + ((int64_t)blockIdx.x * kSpGroups + grp) * 32 + lane;
+    const bool row_ok = row < row_end;
+    cf a[32];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        const int col = 4 * lane + q;
-#pragma unroll
-        for (int rr = 0; rr < kSpRowsPerWarp; ++rr) {
-            const int64_t row = rbase + rr;
-            a[rr][q] = (col < jb && row < row_end) ? A[row + (j0 + col) * lda] : cf{0.0f, 0.0f};
-        }
+    for (int l = 0; l < 32; ++l) {
+        const int col = 32 * w + l;
+        a[l] = (row_ok && col < jb) ? A[row + (j0 + col) * lda] : cf{0.0f, 0.0f};
     }
+    __syncthreads();
     float lmax = 0.0f;
-    for (int j = 0; j < jb; ++j) {
-        const int owner = j >> 2, slot = j & 3;
-        cf x[kSpRowsPerWarp];
-        if (lane == owner) {
-            const cf d = sInv[j];
+    const int nchunks = (jb + 31) / 32;
+    for (int k = 0; k < nchunks; ++k) {
+        cf* xb = sX + ((size_t)((k & 1) * kSpGroups + grp) * 32 + lane) * kSpXStride;
+        if (w == k) {
 #pragma unroll
-            for (int rr = 0; rr < kSpRowsPerWarp; ++rr) {
-                cf v = a[rr][0];
+            for (int j = 0; j < 32; ++j) {
+                const cf* urow = sU + (size_t)(32 * k + j) * kSpUStride + 32 * k;
+                const cf x = a[j] * sInv[32 * k + j];
+                a[j] = x;
+                lmax = fmaxf(lmax, cabs1f(x));
 #pragma unroll
-                for (int q = 1; q < 4; ++q)
-                    if (q == slot) v = a[rr][q];
-                v = v * d;
-                lmax = fmaxf(lmax, cabs1f(v));
-#pragma unroll
-                for (int q = 0; q < 4; ++q)
-                    if (q == slot) a[rr][q] = v;
-                x[rr] = v;
+                for (int l0 = (j + 1) & ~1; l0 < 32; l0 += 2) {
+                    cf u0, u1;
+                    load_u2(urow + l0, u0, u1);
+                    if (l0 > j) a[l0] = a[l0] - x * u0;
+                    a[l0 + 1] = a[l0 + 1] - x * u1;
+                }
             }
+#pragma unroll
+            for (int j = 0; j < 32; ++j) xb[j] = a[j];
         }
+        __syncthreads();
+        if (w > k) {
+            for (int j = 0; j < 32; ++j) {
+                const cf* urow = sU + (size_t)(32 * k + j) * kSpUStride + 32 * w;
+                const cf x = xb[j];
 #pragma unroll
-        for (int rr = 0; rr < kSpRowsPerWarp; ++rr) {
-            x[rr].re = __shfl_sync(0xffffffffu, x[rr].re, owner);
-            x[rr].im = __shfl_sync(0xffffffffu, x[rr].im, owner);
-        }
-        const cf* urow = sU + (size_t)j * kSpUStride + 4 * lane;
-        const float4 u01 = *reinterpret_cast<const float4*>(urow);
-        const float4 u23 = *reinterpret_cast<const float4*>(urow + 2);
-        const cf u[4] = {cf{u01.x, u01.y}, cf{u01.z, u01.w}, cf{u23.x, u23.y}, cf{u23.z, u23.w}};
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            if (4 * lane + q > j) {
-#pragma unroll
-                for (int rr = 0; rr < kSpRowsPerWarp; ++rr) a[rr][q] = a[rr][q] - x[rr] * u[q];
+                for (int l0 = 0; l0 < 32; l0 += 2) {
+                    cf u0, u1;
+                    load_u2(urow + l0, u0, u1);
+                    a[l0] = a[l0] - x * u0;
+                    a[l0 + 1] = a[l0 + 1] - x * u1;
+                }
             }
         }
     }
+    if (row_ok) {
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        const int col = 4 * lane + q;
-#pragma unroll
-        for (int rr = 0; rr < kSpRowsPerWarp; ++rr) {
-            const int64_t row = rbase + rr;
-            if (col < jb && row < row_end) A[row + (j0 + col) * lda] = a[rr][q];
+        for (int l = 0; l < 32; ++l) {
+            const int col = 32 * w + l;
+            if (col < jb) A[row + (j0 + col) * lda] = a[l];
         }
     }
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) lmax = fmaxf(lmax, __shfl_xor_sync(0xffffffffu, lmax, off));
-    // NaN-safe: a NaN compares false and leaves the bound raised by atomicMax
-    // of +inf below
+    // NaN-safe: a NaN compares false and raises the bound to +inf
     if (lane == 0) atomicMax(&ws->lmax_bits, (lmax == lmax) ? __float_as_uint(lmax) : 0x7f800000u);
 }
 
@@ -235,30 +273,43 @@ __global__ void __launch_bounds__(32 * kSpL21Warps, 1)
 
 // The panel of columns [j0, j0+jb) (jb <= 128) over rows [j0, n): the
 // diagonal block factored with pivots among its own rows, then L21.
-// `inv_diag`: 128 complex64 of device scratch for the reciprocal pivots.
+// `inv_diag`: 128 complex64 of device scratch for the reciprocal pivots;
+// `perm` (128 int32) receives the block's rows in pivot order.
 mw_status static_panel_c64(cf* A, int64_t lda, int64_t n, int64_t j0, int jb, int32_t* ipiv, int32_t* info,
-                           PanelWs* ws, cf* inv_diag, cudaStream_t st) {
+                           PanelWs* ws, cf* inv_diag, int32_t* perm, cudaStream_t st) {
     MW_REQUIRE(jb >= 1 && jb <= kSpB, "static panel width %d outside 1..%d", jb, kSpB);
     static bool configured = false;
-    const size_t smem = sizeof(cf) * ((size_t)kSpB * kSpUStride + kSpB);
+    const size_t smem = sizeof(cf) * ((size_t)kSpB * kSpUStride + kSpB + (size_t)2 * kSpGroups * 32 * kSpXStride);
     if (!configured) {
         MW_CHECK_CUDA(cudaFuncSetAttribute(sp_l21_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         configured = true;
     }
     {
         ProfileScope ps(PC_PANEL, st, 8.0 * (double)jb * jb * jb / 3.0, 16.0 * (double)jb * jb);
-        sp_diag_kernel<<<1, kSpDiagThreads, 0, st>>>(A, lda, j0, jb, ipiv, info, inv_diag, ws);
+        sp_diag_kernel<<<1, kSpDiagThreads, 0, st>>>(A, lda, j0, jb, ipiv, info, inv_diag, perm, ws);
         count_launch();
+    }
+    {
         const int64_t rows = n - j0 - jb;
+        ProfileScope ps(PC_L21, st, 4.0 * (double)rows * jb * jb, 16.0 * (double)rows * jb);
         if (rows > 0) {
-            const int64_t per_cta = (int64_t)kSpL21Warps * kSpRowsPerWarp;
+            const int64_t per_cta = (int64_t)kSpGroups * 32;
             const unsigned grid = (unsigned)((rows + per_cta - 1) / per_cta);
-            sp_l21_kernel<<<grid, 32 * kSpL21Warps, smem, st>>>(A, lda, j0, jb, n, inv_diag, ws);
+            sp_l21_kernel<<<grid, kSpL21Threads, smem, st>>>(A, lda, j0, jb, n, inv_diag, ws);
             count_launch();
         }
     }
     MW_CHECK_CUDA(cudaGetLastError());
     return MW_OK;
+}
+
+// The block's interchanges applied to columns [col0, col0 + ncols).
+void static_permute_c64(cf* A, int64_t lda, int64_t row0, int jb, int64_t col0, int64_t ncols, const int32_t* perm,
+                        cudaStream_t st) {
+    if (ncols <= 0) return;
+    ProfileScope ps(PC_LASWP, st, 0.0, 2.0 * sizeof(cf) * (double)jb * ncols);
+    sp_permute_kernel<<<(unsigned)((ncols + 7) / 8), 256, 0, st>>>(A, lda, row0, jb, col0, ncols, perm);
+    count_launch();
 }
 
 }  // namespace mw

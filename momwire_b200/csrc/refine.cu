@@ -97,6 +97,8 @@ std::atomic<int> g_pivot_mode{0};
 // What the last mw_zgesv_mixed on this host thread used: 0 static pivots,
 // 1 partial pivoting, 2 static pivots rejected then partial pivoting.
 thread_local int g_last_pivoting = -1;
+// the largest |L21| of the last static-pivot factorisation (0 when none)
+thread_local double g_last_growth = 0.0;
 // A static-pivot factorisation is kept while every |L21| (|re| + |im|) stays
 // within this bound (partial pivoting keeps |L| <= 1); the FP64 refinement
 // then has to converge as well.
@@ -112,6 +114,8 @@ extern "C" int32_t mw_set_mixed_pivoting(int32_t mode) {
 }
 
 extern "C" int32_t mw_last_mixed_pivoting(void) { return g_last_pivoting; }
+
+extern "C" double mw_last_mixed_growth(void) { return g_last_growth; }
 
 extern "C" size_t mw_zgesv_mixed_workspace_size(int64_t n, int64_t nrhs) {
     return al256(mw_cgetrf_workspace_size(n, nrhs)) + al256((size_t)n * nrhs * 16) + al256((size_t)n * nrhs * 8) +
@@ -177,6 +181,7 @@ extern "C" mw_status mw_zgesv_mixed(int64_t n, int64_t nrhs, const double* Z, in
         if (static_pivot) {
             float lmax;
             std::memcpy(&lmax, &hws[2], sizeof(float));
+            g_last_growth = lmax;
             if (!(lmax <= kStaticLmaxBound) || hinfo[0] > 0) continue;  // growth too large or singular block
         }
         if (hinfo[0] > 0) {

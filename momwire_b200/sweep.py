@@ -145,8 +145,9 @@ def group_plan(orders, n_k, budget_bytes, bytes_per_matrix):
 
 
 class _Ports:
-    """The port columns of a group's members, read once every member's
-    preparation has finished (after its fills were issued)."""
+    """The right-hand sides ([B | A^T], B, A) of a group's members, read
+    once every member's preparation has finished (after its fills were
+    issued)."""
 
     def __init__(self, ports, ids):
         self._ports, self._ids = ports, ids
@@ -182,7 +183,8 @@ def _solve_group(solvers, nb, ks, stream, pw=None, Bs=None, arena=None, wait=Non
     nk = len(ks)
     G = len(solvers)
     count = G * nk
-    P = max(s._port_count() for s in solvers)
+    # right-hand sides per structure: ports plus its KCL rows (Schur step after)
+    P = max(s._port_count() + s._kcl_rows_left() for s in solvers)
     wsb = lib.mw_zgesv_mixed_batched_workspace_size(nb, P, count)
     if arena is not None and arena.numel() >= _group_bytes(count, nb, P):
         # views of one allocation made for the whole sweep (no allocation
@@ -206,13 +208,14 @@ def _solve_group(solvers, nb, ks, stream, pw=None, Bs=None, arena=None, wait=Non
         s._fill_batched(ks, stream, Z=zb, Z32=z32b, ld=nb, k_dev=k_dev)
         _lib.call("mw_pad_identity", n, nb, nk, zb.data_ptr(), nb, nb * nb, z32b.data_ptr(), nb, nb * nb, stream)
     if Bs is None:
-        Bs = [s._port_columns()[0] for s in solvers]
+        Bs = [s._sweep_rhs() for s in solvers]
+    Bs = list(Bs)  # (R = [B | A^T], B, A) per structure
     # the right-hand sides of every structure, staged in page-locked memory
     # and uploaded with one stream-ordered copy (pageable uploads would make
     # the host wait for the fills queued before them)
     Bh = torch.zeros((G, P, nb), dtype=torch.complex128, pin_memory=True)
-    for g, B in enumerate(Bs):
-        Bh[g, : B.shape[1], : B.shape[0]] = torch.from_numpy(np.ascontiguousarray(B.T))
+    for g, (R, _B, _A) in enumerate(Bs):
+        Bh[g, : R.shape[1], : R.shape[0]] = torch.from_numpy(np.ascontiguousarray(R.T))
     Bg = Bh.to(dev, non_blocking=True)
     Bd = Bg.repeat_interleave(nk, dim=0)
     if pw is None:
@@ -227,9 +230,11 @@ def _solve_group(solvers, nb, ks, stream, pw=None, Bs=None, arena=None, wait=Non
               float(s0.mixed_tol), int(s0.mixed_max_iter), ws.data_ptr(), wsb, C.byref(it), C.byref(corr), stream)
     Xh = X.cpu().numpy()
     out = {}
-    for g, (s, B) in enumerate(zip(solvers, Bs)):
-        n, p = B.shape
-        out[g] = np.einsum("kpn,nq->kqp", Xh[g * nk : (g + 1) * nk, :p, :n], B)
+    from .bspline import _swept_y
+
+    for g, (R, B, A) in enumerate(Bs):
+        n, m = R.shape
+        out[g] = _swept_y(Xh[g * nk : (g + 1) * nk, :m, :n], B, A)
     return out, int(it.value)
 
 
@@ -306,7 +311,7 @@ class _DeviceGroups:
             s = self.solvers[i]
             s._dev_tables()
             s._loading_dev_tables()
-            self.ports[i] = s._port_columns()[0]
+            self.ports[i] = s._sweep_rhs()
             self.prep_stream.synchronize()
 
     def solve(self, nb, ids):
@@ -366,7 +371,7 @@ def grouped_mixed_sweep(structs, ks, device=None, budget_bytes=32 << 30, indices
     out = {}
     if not plan_ids and not single:
         return out
-    P_max = max([solvers[i]._port_count() for i in grouped] or [1])
+    P_max = max([solvers[i]._port_count() + solvers[i]._kcl_rows_left() for i in grouped] or [1])
     runner = groups(solvers, ks, plan_ids, P_max) if plan_ids else None
     try:
         for i in single:

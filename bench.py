@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
+    ap.add_argument("--pivoting", default="static", choices=["static", "partial"],
+                    help="mixed path: pivots within each diagonal block (with fallback) or partial pivoting")
     ap.add_argument("--fp64-steps", type=int, default=2, help="steps of the FP64 path timed beside a mixed run")
     ap.add_argument("--sweep-structs", type=int, default=512,
                     help="Yagis per rank in the sweep part of the line (0: none)")
@@ -250,6 +252,7 @@ def run_b200(args, kw):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
         pg = dist
     lib = _lib.load()
+    lib.mw_set_mixed_pivoting(0 if args.pivoting == "static" else 1)
 
     solver = momwire_b200.BSplineSolver(**kw, precision=args.precision, device=local)
     buf = solver._alloc()
@@ -448,7 +451,7 @@ def run_b200(args, kw):
         "pivoting": {0: "static (diagonal block)", 1: "partial", 2: "static rejected, then partial"}.get(
             int(lib.mw_last_mixed_pivoting()), None) if args.precision == "mixed" else "partial",
         "static_pivot_max_abs_l21": float(lib.mw_last_mixed_growth()) if args.precision == "mixed" else None,
-        "refinement": solver.last_refinement,
+        "refinement": dict(solver.last_refinement or {}, history=refine_history(lib)),
         "clocks": clocks.summary(),
         "y_rel_err_vs_reference": y_err,
         "fp64_ms_per_step": fp64_ms,
@@ -464,6 +467,16 @@ def run_b200(args, kw):
         print(json.dumps(line), flush=True)
     if pg:
         pg.destroy_process_group()
+
+
+def refine_history(lib):
+    """The controlling relative correction of each refinement step of the
+    last mixed solve on this thread."""
+    import ctypes
+
+    buf = (ctypes.c_double * 16)()
+    n = lib.mw_last_mixed_history(buf, 16)
+    return [float(buf[i]) for i in range(min(n, 16))]
 
 
 def run_micro(args):

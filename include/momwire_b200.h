@@ -351,6 +351,11 @@ int32_t mw_last_mixed_pivoting(void);
  * by mw_zgesv_mixed on this host thread (partial pivoting keeps it <= 1). */
 double mw_last_mixed_growth(void);
 
+/* The controlling relative correction of each refinement step of the last
+ * mw_zgesv_mixed on this host thread (the initial solve first): writes at
+ * most max_n values to out and returns how many steps there were. */
+int32_t mw_last_mixed_history(double* out, int32_t max_n);
+
 /*
  * Frequency-batched fill: Z_b (and Z32_b when Z32 != NULL) for n_k
  * wavenumbers k_dev[b] / omega_dev[b] (device arrays), free space or a PEC

@@ -119,6 +119,7 @@ _SIGS = {
     "mw_set_mixed_pivoting": (i32, [i32]),
     "mw_last_mixed_pivoting": (i32, []),
     "mw_last_mixed_growth": (f64, []),
+    "mw_last_mixed_history": (i32, [C.POINTER(f64), i32]),
     "mw_same_edge_table": (i32, [C.POINTER(Edges), i32, i32, i32, f64, vp, vp]),
     "mw_offedge_moments": (i32, [C.POINTER(Segments), C.POINTER(Segments), i32, i32, f64, i32, f64, vp, vp, vp, vp]),
     "mw_fill_z": (i32, [C.POINTER(Segments), C.POINTER(BasisT), vp, C.POINTER(Edges), C.POINTER(Freq), i32, vp, i64, vp, i64, vp]),

@@ -284,10 +284,11 @@ class BSplineSolver:
             raise ValueError(f"surrogate_tol must be > 0, got {surrogate_tol!r}")
         self.surrogate_tol = float(surrogate_tol)
         self.last_sommerfeld = None
-        # mixed: stop refining once the largest relative correction of any
-        # port column is below this (the remaining error is then ~ kappa *
-        # 6e-8 times smaller still)
-        self.mixed_tol = 1e-7
+        # mixed: stop refining once the relative error estimated to remain in
+        # every port column (the last correction, times the contraction the
+        # corrections show) is below this -- a third of the 1e-6 the mixed
+        # path holds drive-point impedances to
+        self.mixed_tol = 3e-7
         self.mixed_max_iter = 10
         self.last_refinement = None
         self.degree = int(degree)

@@ -37,6 +37,7 @@ mw_status static_panel_c64(cf* A, int64_t lda, int64_t n, int64_t j0, int jb, in
                            PanelWs* ws, cf* inv_diag, int32_t* perm, cudaStream_t st);
 void static_permute_c64(cf* A, int64_t lda, int64_t row0, int jb, int64_t col0, int64_t ncols, const int32_t* perm,
                         cudaStream_t st);
+void static_left_permute_c64(cf* A, int64_t lda, int64_t n, const int32_t* perm_all, cudaStream_t st);
 
 constexpr int kNB = 64;         // panel half width (rank-1 work per cooperative panel)
 constexpr int kOuterNB = 128;   // getrf block: panel width and trailing-update k
@@ -593,12 +594,13 @@ struct GetrsLeaf<cf> {
 
 // X (jb x ncols, leading dim ldx) <- L^-1 X with L unit lower (jb x jb),
 // or U^-1 X with U upper non-unit (jb <= leaf).  The CTA stages the triangle
-// in shared memory; each warp then owns kTrsmCols columns of X in registers
-// (lane l holds rows RP*l .. RP*l+RP-1 of each) and substitutes with warp
-// shuffles only, every staged triangle element read once for all of them.
+// in shared memory; each warp then owns NC columns of X in registers (lane l
+// holds rows RP*l .. RP*l+RP-1 of each) and substitutes with warp shuffles
+// only, every staged triangle element read once for all of them.  Wide
+// solves take NC = 4 (a quarter of the CTAs stage the triangle); narrow
+// ones, whose latency sits on the critical path, NC = 1 (more CTAs).
 constexpr int kTrsmWarps = 8;
-constexpr int kTrsmCols = 4;  // columns per warp
-template <class T, bool UPPER, int L>
+template <class T, bool UPPER, int L, int NC>
 __global__ void __launch_bounds__(32 * kTrsmWarps) trsm_kernel(const T* Tm, int64_t ldt, T* X, int64_t ldx, int jb,
                                                                int64_t ncols, const T* Aoff, int64_t ldo, const T* Xp,
                                                                int K) {
@@ -615,7 +617,6 @@ __global__ void __launch_bounds__(32 * kTrsmWarps) trsm_kernel(const T* Tm, int6
     // same lane-major form -- the next-block update of a blocked sweep, done
     // where its result is consumed.
     constexpr int RP = L / 32;
-    constexpr int NC = kTrsmCols;
     static_assert(RP * 32 == L, "leaf order must be a multiple of 32");
     extern __shared__ __align__(16) unsigned char trsm_smem[];
     T* S = reinterpret_cast<T*>(trsm_smem);
@@ -786,19 +787,29 @@ constexpr size_t trsm_smem_bytes() {
     return sizeof(T) * (L * (L + 1) + L);
 }
 
+// columns at which a solve switches to four columns per warp: enough CTAs
+// remain to cover the SMs twice
+constexpr int64_t kTrsmWide = 4 * 8 * 2 * 148;
+
+template <class T, int L, int NC>
+static mw_status trsm_attr() {
+    MW_CHECK_CUDA(cudaFuncSetAttribute(trsm_kernel<T, false, L, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)trsm_smem_bytes<T, L>()));
+    MW_CHECK_CUDA(cudaFuncSetAttribute(trsm_kernel<T, true, L, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)trsm_smem_bytes<T, L>()));
+    return MW_OK;
+}
+
 template <class T>
 static mw_status trsm_setup() {
     static bool done = false;
     if (!done) {
         constexpr int GL = GetrsLeaf<T>::value;
-        MW_CHECK_CUDA(cudaFuncSetAttribute(trsm_kernel<T, false, kNB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)trsm_smem_bytes<T, kNB>()));
-        MW_CHECK_CUDA(cudaFuncSetAttribute(trsm_kernel<T, true, kNB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)trsm_smem_bytes<T, kNB>()));
-        MW_CHECK_CUDA(cudaFuncSetAttribute(trsm_kernel<T, false, GL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)trsm_smem_bytes<T, GL>()));
-        MW_CHECK_CUDA(cudaFuncSetAttribute(trsm_kernel<T, true, GL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)trsm_smem_bytes<T, GL>()));
+        mw_status s = trsm_attr<T, kNB, 1>();
+        if (s == MW_OK) s = trsm_attr<T, kNB, 4>();
+        if (s == MW_OK) s = trsm_attr<T, GL, 1>();
+        if (s == MW_OK) s = trsm_attr<T, GL, 4>();
+        if (s != MW_OK) return s;
         done = true;
     }
     return MW_OK;
@@ -809,9 +820,14 @@ static void trsm_launch(const T* Tm, int64_t ldt, T* X, int64_t ldx, int jb, int
                         const T* Aoff = nullptr, int64_t ldo = 0, const T* Xp = nullptr, int K = 0) {
     ProfileScope ps(PC_TRSM, st, 4.0 * (double)jb * jb * ncols + 8.0 * (double)jb * K * ncols,
                     2.0 * sizeof(T) * (double)jb * ncols);
-    const int64_t per_cta = (int64_t)kTrsmWarps * kTrsmCols;
-    trsm_kernel<T, UPPER, L><<<(unsigned)((ncols + per_cta - 1) / per_cta), 32 * kTrsmWarps, trsm_smem_bytes<T, L>(),
-                               st>>>(Tm, ldt, X, ldx, jb, ncols, Aoff, ldo, Xp, K);
+    if (ncols >= kTrsmWide) {
+        const int64_t per_cta = (int64_t)kTrsmWarps * 4;
+        trsm_kernel<T, UPPER, L, 4><<<(unsigned)((ncols + per_cta - 1) / per_cta), 32 * kTrsmWarps,
+                                      trsm_smem_bytes<T, L>(), st>>>(Tm, ldt, X, ldx, jb, ncols, Aoff, ldo, Xp, K);
+    } else {
+        trsm_kernel<T, UPPER, L, 1><<<(unsigned)((ncols + kTrsmWarps - 1) / kTrsmWarps), 32 * kTrsmWarps,
+                                      trsm_smem_bytes<T, L>(), st>>>(Tm, ldt, X, ldx, jb, ncols, Aoff, ldo, Xp, K);
+    }
     count_launch();
 }
 
@@ -1377,7 +1393,9 @@ template <class T>
 static mw_status getrf_lookahead(int64_t n, T* A, int64_t lda, int32_t* ipiv, int32_t* info, char* ws,
                                  const volatile int32_t* cancel, const Updater& up_main, const Updater& up_trail,
                                  cudaStream_t st, T* Baug = nullptr, int64_t ldb = 0, int64_t nrhs = 0,
-                                 bool static_pivot = false) {
+                                 int32_t* perm_all = nullptr) {
+    // static pivots when the caller passes room for every block's row order
+    const bool static_pivot = perm_all != nullptr;
     MW_CHECK_CUDA(cudaMemsetAsync(info, 0, 2 * sizeof(int32_t), st));
     MW_CHECK_CUDA(cudaMemsetAsync(ws, 0, sizeof(PanelWs), st));
     {
@@ -1416,15 +1434,14 @@ static mw_status getrf_lookahead(int64_t n, T* A, int64_t lda, int32_t* ipiv, in
         if (j >= 2) MW_CHECK_CUDA(cudaStreamWaitEvent(st, ax->ev_trail[(j - 2) & 3], 0));
         mw_status s;
         // static pivots: the block's interchanges never leave it, so they
-        // reach the columns beside it as one parallel row permutation
-        // (double-buffered per block: the trail stream still reads block
-        // j's while the main stream factors block j+1)
+        // reach the columns beside it as one parallel row permutation (each
+        // block's row order kept, for the columns left of it at the end)
         int32_t* perm = nullptr;
         if constexpr (std::is_same<T, cf>::value) {
             if (static_pivot) {
                 size_t ov, oi, orow, ocur;
                 ws_layout(kMaxPanelGrid, &ov, &oi, &orow, &ocur);
-                perm = reinterpret_cast<int32_t*>(ws + ocur + 2048 + (j & 1) * 512);
+                perm = perm_all + j0;
                 s = static_panel_c64(A, lda, n, j0, jb, ipiv, info, pws, reinterpret_cast<cf*>(ws + ocur), perm, st);
             } else {
                 s = panel_factor<T>(A, lda, n, j0, jb, ipiv, info, ws, up_main, st, kLaPanelCtas);
@@ -1485,8 +1502,16 @@ static mw_status getrf_lookahead(int64_t n, T* A, int64_t lda, int32_t* ipiv, in
         MW_CHECK_CUDA(cudaGetLastError());
     }
     if (nb > 0) MW_CHECK_CUDA(cudaStreamWaitEvent(st, ax->ev_trail[(nb - 1) & 3], 0));
-    // every panel's row swaps on the columns left of it, in panel order
-    for (int64_t j = 1; j < nb; ++j) {
+    // every panel's row swaps on the columns left of it, in panel order (the
+    // static path's stay inside their blocks: one launch for all of them)
+    bool left_done = false;
+    if constexpr (std::is_same<T, cf>::value) {
+        if (static_pivot) {
+            static_left_permute_c64(A, lda, n, perm_all, st);
+            left_done = true;
+        }
+    }
+    for (int64_t j = 1; j < nb && !left_done; ++j) {
         const int64_t j0 = j * kOuterNB;
         const int jb = (int)((n - j0) < kOuterNB ? (n - j0) : kOuterNB);
         laswp_launch<T>(A, lda, 0, j0, ipiv, j0, j0 + jb, st);
@@ -1592,14 +1617,19 @@ static size_t panel_ws_bytes() {
 // Workspace of the complex64 path: panel slots, then the tensor-core
 // operand planes for the largest update (m = n, n = n, k = kOuterNB), then the
 // device status word.
-static size_t cgetrf_ws_bytes(int64_t n, int64_t nrhs_max) {
+static size_t cgetrf_perm_offset(int64_t n, int64_t nrhs_max) {
     int64_t w = n > nrhs_max ? n : nrhs_max;
     // panel slots | trail-stream operand planes | status word | main-stream
     // operand planes (k at most kOuterNB; at most kOuterNB columns wide in
-    // the factorisation, nrhs_max wide in the solves)
+    // the factorisation, nrhs_max wide in the solves) | static pivot orders
     const int64_t wm = nrhs_max > kOuterNB ? nrhs_max : kOuterNB;
-    return panel_ws_bytes() + 1024 + ((cgemm_tc_workspace(n, w, kOuterNB) + 255) & ~size_t(255)) + 256 +
-           cgemm_tc_workspace(n, wm, kOuterNB) + 1024;
+    const size_t o = panel_ws_bytes() + 1024 + ((cgemm_tc_workspace(n, w, kOuterNB) + 255) & ~size_t(255)) + 256 +
+                     cgemm_tc_workspace(n, wm, kOuterNB) + 1024;
+    return (o + 255) & ~size_t(255);
+}
+
+static size_t cgetrf_ws_bytes(int64_t n, int64_t nrhs_max) {
+    return cgetrf_perm_offset(n, nrhs_max) + sizeof(int32_t) * (size_t)(n > 0 ? n : 1) + 256;
 }
 
 static Updater tc_updater(char* ws, size_t ws_bytes, int64_t n, int64_t nrhs_max) {
@@ -1706,8 +1736,9 @@ mw_status cgetrf_forward(int64_t n, float* Ad, int64_t lda, int32_t* ipiv, int32
     up.max_ctas = panel_sms<cf>() - kLaPanelCtas;
     cudaStream_t st = as_stream(stream);
     MW_CHECK_CUDA(cudaMemsetAsync(up.tc_err, 0, sizeof(int), st));
+    int32_t* perm_all = static_pivot ? reinterpret_cast<int32_t*>(ws + cgetrf_perm_offset(n, nrhs)) : nullptr;
     mw_status s = getrf_lookahead<cf>(n, reinterpret_cast<cf*>(Ad), lda, ipiv, info, ws, cancel, up_main, up, st,
-                                      reinterpret_cast<cf*>(Bd), ldb, nrhs, static_pivot);
+                                      reinterpret_cast<cf*>(Bd), ldb, nrhs, perm_all);
     if (s != MW_OK) return s;
     merge_status_kernel<<<1, 1, 0, st>>>(info + 1, &reinterpret_cast<PanelWs*>(ws)->err, up.tc_err);
     count_launch();

@@ -44,17 +44,37 @@ __device__ __forceinline__ cf crcp_sp(cf z) {
 
 __device__ __forceinline__ float cabs1f(cf z) { return fabsf(z.re) + fabsf(z.im); }
 
+constexpr size_t kSpDiagSmem = sizeof(cf) * (kSpB * 33 + 3 * 32 * 33);
+
+__device__ __forceinline__ void group_sync(int id) {
+    // the 128 threads (four warps) of one column group
+    asm volatile("bar.sync %0, 128;" ::"r"(id) : "memory");
+}
+
 // Factor A[j0 .. j0+jb) x [j0 .. j0+jb) in place with partial pivoting among
-// these rows.  Thread (r, g) holds row r's columns 32g .. 32g+31 in
-// registers; a chosen pivot row stops updating (its remaining columns are
-// its U row), so no data moves until the block is written back in pivot
-// order.  Two barriers per column.
+// these rows, blocked by 32-column chunks.  Thread (r, g) holds row r's
+// columns 32g .. 32g+31 (chunk g) in registers.  Chunk k is factored by its
+// own four warps alone (rank-1 updates inside the chunk, two group
+// barriers per column); then every later chunk g takes the chunk's U rows
+// (the pivot rows' chunk-g values, solved with the chunk's unit lower
+// triangle by one warp) and removes the chunk from its unpivoted rows with
+// one 32 x 32 block product per row.  A chosen pivot row keeps its place in
+// registers (its later columns become its U row); rows move once, when the
+// block is written back in pivot order.
 __global__ void __launch_bounds__(kSpDiagThreads, 1)
     sp_diag_kernel(cf* __restrict__ A, int64_t lda, int64_t j0, int jb, int32_t* __restrict__ ipiv,
                    int32_t* __restrict__ info, cf* __restrict__ inv_diag, int32_t* __restrict__ perm, PanelWs* ws) {
-    __shared__ cf s_col[kSpB];
-    __shared__ cf s_u[kSpB];
+    __shared__ cf s_col[kSpB];                 // column c of every row
+    __shared__ cf s_u[32];                     // the pivot row's chunk values
+    // dynamic: chunk k of every row (L values of the unpivoted rows), then
+    // the U rows of chunk k's pivots in each later chunk
+    extern __shared__ __align__(16) unsigned char sp_diag_smem[];
+    auto s_L = reinterpret_cast<cf(*)[33]>(sp_diag_smem);                          // [kSpB][33]
+    auto s_Ug = reinterpret_cast<cf(*)[32][33]>(sp_diag_smem + sizeof(cf) * kSpB * 33);  // [3][32][33]
     __shared__ unsigned long long s_wkey[4];
+    __shared__ int s_piv[32];                  // physical rows chosen in chunk k
+    __shared__ int s_pos_of[kSpB];             // current position of each physical row
+    __shared__ int s_row_at[kSpB];             // physical row at each position
     const int tid = threadIdx.x;
     const int r = tid & (kSpB - 1);
     const int g = tid >> 7;
@@ -67,85 +87,130 @@ __global__ void __launch_bounds__(kSpDiagThreads, 1)
         a[i] = (r < jb && col < jb) ? A[(j0 + r) + (j0 + col) * lda] : cf{0.0f, 0.0f};
     }
     bool active = r < jb;
-    // this row's position in the arranged block (LAPACK's row order after
-    // the interchanges so far); every thread of the row tracks it
-    int mypos = r;
-    for (int c = 0; c < jb; ++c) {
-        const int gc = c >> 5, ic = c & 31;
-        if (g == gc) {
-            cf v = a[0];
+    if (tid < kSpB) {
+        s_pos_of[tid] = tid;
+        s_row_at[tid] = tid;
+    }
+    __syncthreads();
+    const int nchunk = (jb + 31) / 32;
+    for (int k = 0; k < nchunk; ++k) {
+        const int nck = (jb - 32 * k) < 32 ? (jb - 32 * k) : 32;  // columns in chunk k
+        if (g == k) {
+            // ---- (a) chunk k, by its own four warps
 #pragma unroll
-            for (int i = 1; i < 32; ++i)
-                if (i == ic) v = a[i];
-            s_col[r] = v;
-            // largest |re| + |im| among the rows not yet chosen, then the
-            // smallest position (LAPACK's icamax on the arranged rows); the
-            // low bits carry the physical row
-            unsigned long long key = 0;
-            if (active)
-                key = ((unsigned long long)__float_as_uint(cabs1f(v)) << 32) |
-                      ((unsigned long long)(0xFFFFu - (unsigned int)mypos) << 16) | (unsigned long long)r;
+            for (int cc = 0; cc < 32; ++cc) {
+                if (cc < nck) {
+                    const int c = 32 * k + cc;
+                    const cf v = a[cc];
+                    s_col[r] = v;
+                    // largest |re| + |im| among the rows not yet chosen, then
+                    // the smallest position (LAPACK's icamax on the arranged
+                    // rows); the low bits carry the physical row
+                    unsigned long long key = 0;
+                    if (active)
+                        key = ((unsigned long long)__float_as_uint(cabs1f(v)) << 32) |
+                              ((unsigned long long)(0xFFFFu - (unsigned int)s_pos_of[r]) << 16) |
+                              (unsigned long long)r;
 #pragma unroll
-            for (int off = 16; off > 0; off >>= 1) {
-                const unsigned long long o = __shfl_xor_sync(0xffffffffu, key, off);
-                key = o > key ? o : key;
-            }
-            if (lane == 0) s_wkey[wig] = key;
-        }
-        __syncthreads();
-        unsigned long long best = s_wkey[0];
+                    for (int off = 16; off > 0; off >>= 1) {
+                        const unsigned long long o = __shfl_xor_sync(0xffffffffu, key, off);
+                        key = o > key ? o : key;
+                    }
+                    if (lane == 0) s_wkey[wig] = key;
+                    group_sync(1 + k);
+                    unsigned long long best = s_wkey[0];
 #pragma unroll
-        for (int w = 1; w < 4; ++w) best = s_wkey[w] > best ? s_wkey[w] : best;
-        const int p = (int)(best & 0xFFFFull);
-        const int pos_best = (int)(0xFFFFu - (unsigned int)((best >> 16) & 0xFFFFull));
-        const bool zero = (best >> 32) == 0ull;
-        const cf inv = zero ? cone<cf>() : crcp_sp(s_col[p]);
-        if (r == p) {
+                    for (int w = 1; w < 4; ++w) best = s_wkey[w] > best ? s_wkey[w] : best;
+                    const int p = (int)(best & 0xFFFFull);
+                    const int pos_best = (int)(0xFFFFu - (unsigned int)((best >> 16) & 0xFFFFull));
+                    const bool zero = (best >> 32) == 0ull;
+                    const cf inv = zero ? cone<cf>() : crcp_sp(s_col[p]);
+                    if (r == p) {
 #pragma unroll
-            for (int i = 0; i < 32; ++i) s_u[32 * g + i] = a[i];
-            active = false;
-        }
-        const cf l = (active && !zero) ? s_col[r] * inv : cf{0.0f, 0.0f};
-        // the interchange LAPACK makes: positions c and pos_best
-        if (r == p)
-            mypos = c;
-        else if (mypos == c)
-            mypos = pos_best;
-        __syncthreads();  // s_u complete; s_col and s_wkey read
-        if (tid == 0) {
-            ipiv[j0 + c] = (int32_t)(j0 + pos_best + 1);
-            if (zero) {
-                if (info[0] == 0) info[0] = (int32_t)(j0 + c + 1);
-                atomicExch(&ws->lmax_bits, 0x7f800000u);  // +inf: the block is singular
-            }
-            inv_diag[c] = inv;
-        }
-        if (active && g == gc && !zero) {
+                        for (int l = cc; l < 32; ++l) s_u[l] = a[l];
+                        active = false;
+                        s_piv[cc] = p;
+                    }
+                    const cf lr = (active && !zero) ? s_col[r] * inv : cf{0.0f, 0.0f};
+                    if (tid == 128 * k) {
+                        // the interchange LAPACK makes: positions c and pos_best
+                        ipiv[j0 + c] = (int32_t)(j0 + pos_best + 1);
+                        if (zero) {
+                            if (info[0] == 0) info[0] = (int32_t)(j0 + c + 1);
+                            atomicExch(&ws->lmax_bits, 0x7f800000u);  // +inf: the block is singular
+                        }
+                        inv_diag[c] = inv;
+                        const int pc = s_row_at[c];
+                        s_row_at[c] = p;
+                        s_row_at[pos_best] = pc;
+                        s_pos_of[p] = c;
+                        s_pos_of[pc] = pos_best;
+                    }
+                    group_sync(1 + k);  // s_u, s_pos_of complete; s_col and s_wkey read
+                    if (active && !zero) {
+                        a[cc] = lr;
 #pragma unroll
-            for (int i = 0; i < 32; ++i)
-                if (i == ic) a[i] = l;
-        }
-        // the rank-1 update, skipped by whole warps: column groups left of c
-        // and warps whose rows are all chosen already
-        if (!zero && 32 * g + 31 > c && __any_sync(0xffffffffu, active)) {
-            if (active) {
-#pragma unroll
-                for (int i = 0; i < 32; ++i) {
-                    const int col = 32 * g + i;
-                    if (col > c) a[i] = a[i] - l * s_u[col];
+                        for (int l = cc + 1; l < 32; ++l) a[l] = a[l] - lr * s_u[l];
+                    }
                 }
             }
+#pragma unroll
+            for (int l = 0; l < 32; ++l) s_L[r][l] = a[l];
         }
+        __syncthreads();  // chunk k factored: s_L and s_piv published
+        if (g > k) {
+            // rows chosen in chunk k stop updating; the chunk's pivot rows
+            // publish their chunk-g values (row i of the U block)
+            int my_i = -1;
+            for (int i = 0; i < nck; ++i)
+                if (s_piv[i] == r) my_i = i;
+            if (my_i >= 0) {
+                active = false;
+#pragma unroll
+                for (int l = 0; l < 32; ++l) s_Ug[g - k - 1][my_i][l] = a[l];
+            }
+            group_sync(1 + g);
+            if (wig == 0) {
+                // U = L_kk^-1 (pivot rows): lane l solves column l, the rows
+                // already solved read back from shared memory
+                for (int i = 1; i < nck; ++i) {
+                    const int pi = s_piv[i];
+                    cf t = s_Ug[g - k - 1][i][lane];
+                    for (int jj = 0; jj < i; ++jj) t = t - s_L[pi][jj] * s_Ug[g - k - 1][jj][lane];
+                    s_Ug[g - k - 1][i][lane] = t;
+                }
+            }
+            group_sync(1 + g);
+            if (my_i >= 0) {
+#pragma unroll
+                for (int l = 0; l < 32; ++l) a[l] = s_Ug[g - k - 1][my_i][l];
+            }
+            // the block product, by whole warps that still hold unpivoted rows
+            if (__any_sync(0xffffffffu, active) && active) {
+                for (int jj = 0; jj < nck; ++jj) {
+                    const cf x = s_L[r][jj];
+                    const cf* urow = &s_Ug[g - k - 1][jj][0];
+#pragma unroll
+                    for (int l = 0; l < 32; ++l) a[l] = a[l] - x * urow[l];
+                }
+            }
+        } else if (g < k) {
+            // earlier chunks: only the chosen rows change state
+            for (int i = 0; i < nck; ++i)
+                if (s_piv[i] == r) active = false;
+        }
+        __syncthreads();  // s_L, s_Ug and s_piv free for the next chunk
     }
     if (r < jb) {
-        const int64_t row = j0 + mypos;
+        const int pos = s_pos_of[r];
+        const int64_t row = j0 + pos;
 #pragma unroll
         for (int i = 0; i < 32; ++i) {
             const int col = 32 * g + i;
             if (col < jb) A[row + (j0 + col) * lda] = a[i];
         }
-        // the block's rows in pivot order: position mypos holds row r
-        if (g == 0) perm[mypos] = r;
+        // the block's rows in pivot order: position pos holds row r
+        if (g == 0) perm[pos] = r;
     }
 }
 
@@ -202,9 +267,21 @@ __global__ void __launch_bounds__(kSpL21Threads, 1)
     cf* sInv = sU + (size_t)kSpB * kSpUStride;               // [kSpB]
     cf* sX = sInv + kSpB;                                    // [2][kSpGroups][32][kSpXStride]
     const int tid = threadIdx.x;
-    for (int idx = tid; idx < kSpB * kSpB; idx += blockDim.x) {
-        const int j = idx % kSpB, col = idx / kSpB;  // coalesced down each column
-        sU[j * kSpUStride + col] = (j <= col && col < jb) ? A[(j0 + j) + (j0 + col) * lda] : cf{0.0f, 0.0f};
+    // staged with sixteen loads in flight per thread before the stores
+    constexpr int kU = 16;
+    for (int base = 0; base < kSpB * kSpB; base += kU * kSpL21Threads) {
+        cf t[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const int idx = base + u * kSpL21Threads + tid;
+            const int j = idx % kSpB, col = idx / kSpB;  // coalesced down each column
+            t[u] = (idx < kSpB * kSpB && j <= col && col < jb) ? A[(j0 + j) + (j0 + col) * lda] : cf{0.0f, 0.0f};
+        }
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            const int idx = base + u * kSpL21Threads + tid;
+            if (idx < kSpB * kSpB) sU[(idx % kSpB) * kSpUStride + idx / kSpB] = t[u];
+        }
     }
     for (int j = tid; j < kSpB; j += blockDim.x) sInv[j] = j < jb ? inv_diag[j] : cf{0.0f, 0.0f};
     const int lane = tid & 31, warp = tid >> 5;
@@ -282,11 +359,13 @@ mw_status static_panel_c64(cf* A, int64_t lda, int64_t n, int64_t j0, int jb, in
     const size_t smem = sizeof(cf) * ((size_t)kSpB * kSpUStride + kSpB + (size_t)2 * kSpGroups * 32 * kSpXStride);
     if (!configured) {
         MW_CHECK_CUDA(cudaFuncSetAttribute(sp_l21_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        MW_CHECK_CUDA(cudaFuncSetAttribute(sp_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)kSpDiagSmem));
         configured = true;
     }
     {
         ProfileScope ps(PC_PANEL, st, 8.0 * (double)jb * jb * jb / 3.0, 16.0 * (double)jb * jb);
-        sp_diag_kernel<<<1, kSpDiagThreads, 0, st>>>(A, lda, j0, jb, ipiv, info, inv_diag, perm, ws);
+        sp_diag_kernel<<<1, kSpDiagThreads, kSpDiagSmem, st>>>(A, lda, j0, jb, ipiv, info, inv_diag, perm, ws);
         count_launch();
     }
     {
@@ -301,6 +380,43 @@ mw_status static_panel_c64(cf* A, int64_t lda, int64_t n, int64_t j0, int jb, in
     }
     MW_CHECK_CUDA(cudaGetLastError());
     return MW_OK;
+}
+
+// Every block's interchanges applied to the columns left of it (the L
+// factors of the earlier blocks), all blocks in one launch: blockIdx.y + 1
+// is the block, blockIdx.x a chunk of eight columns.  `perm_all` holds the
+// n rows in pivot order, block by block.
+__global__ void __launch_bounds__(256) sp_left_permute_kernel(cf* __restrict__ A, int64_t lda, int64_t n,
+                                                              const int32_t* __restrict__ perm_all) {
+    const int64_t j0 = ((int64_t)blockIdx.y + 1) * kSpB;
+    const int jb = (int)((n - j0) < kSpB ? (n - j0) : kSpB);
+    const int lane = threadIdx.x & 31;
+    const int64_t col = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (col >= j0) return;
+    const int32_t* perm = perm_all + j0;
+    cf* a = A + col * lda + j0;
+    cf v[kSpB / 32];
+#pragma unroll
+    for (int u = 0; u < kSpB / 32; ++u) {
+        const int i = lane + 32 * u;
+        v[u] = i < jb ? a[perm[i]] : cf{0.0f, 0.0f};
+    }
+    __syncwarp();
+#pragma unroll
+    for (int u = 0; u < kSpB / 32; ++u) {
+        const int i = lane + 32 * u;
+        if (i < jb) a[i] = v[u];
+    }
+}
+
+void static_left_permute_c64(cf* A, int64_t lda, int64_t n, const int32_t* perm_all, cudaStream_t st) {
+    const int64_t nb = (n + kSpB - 1) / kSpB;
+    if (nb < 2) return;
+    const int64_t last0 = (nb - 1) * kSpB;  // widest left part
+    ProfileScope ps(PC_LASWP, st, 0.0, sizeof(cf) * (double)n * n);
+    dim3 grid((unsigned)((last0 + 7) / 8), (unsigned)(nb - 1));
+    sp_left_permute_kernel<<<grid, 256, 0, st>>>(A, lda, n, perm_all);
+    count_launch();
 }
 
 // The block's interchanges applied to columns [col0, col0 + ncols).

@@ -99,6 +99,9 @@ std::atomic<int> g_pivot_mode{0};
 thread_local int g_last_pivoting = -1;
 // the largest |L21| of the last static-pivot factorisation (0 when none)
 thread_local double g_last_growth = 0.0;
+// the controlling relative correction of every refinement step of the last
+// call (the initial solve first)
+thread_local std::vector<double> g_last_history;
 // A static-pivot factorisation is kept while every |L21| (|re| + |im|) stays
 // within this bound (partial pivoting keeps |L| <= 1); the FP64 refinement
 // then has to converge as well.
@@ -116,6 +119,12 @@ extern "C" int32_t mw_set_mixed_pivoting(int32_t mode) {
 extern "C" int32_t mw_last_mixed_pivoting(void) { return g_last_pivoting; }
 
 extern "C" double mw_last_mixed_growth(void) { return g_last_growth; }
+
+extern "C" int32_t mw_last_mixed_history(double* out, int32_t max_n) {
+    const int32_t n = (int32_t)g_last_history.size();
+    for (int32_t i = 0; i < n && i < max_n; ++i) out[i] = g_last_history[i];
+    return n;
+}
 
 extern "C" size_t mw_zgesv_mixed_workspace_size(int64_t n, int64_t nrhs) {
     return al256(mw_cgetrf_workspace_size(n, nrhs)) + al256((size_t)n * nrhs * 16) + al256((size_t)n * nrhs * 8) +
@@ -195,6 +204,7 @@ extern "C" mw_status mw_zgesv_mixed(int64_t n, int64_t nrhs, const double* Z, in
         count_launch();
         corr = INFINITY;
         std::fill(prev.begin(), prev.end(), 0.0);
+        g_last_history.clear();
         for (it = 0;; ++it) {
             if (cancel && *cancel) {
                 set_error("solve cancelled");
@@ -239,6 +249,7 @@ extern "C" mw_status mw_zgesv_mixed(int64_t n, int64_t nrhs, const double* Z, in
                 prev[j] = r;
                 if (!(v <= corr)) corr = v;  // NaN-propagating max
             }
+            g_last_history.push_back(corr);
             if (corr <= tol || it >= max_iter) break;
             // R = B - Z X   (FP64)
             copy_c128_kernel<<<grid_for(tot), 256, 0, st>>>(Bc, ldb, R, n, n, nrhs);

@@ -101,7 +101,7 @@ def test_mixed_matches_reference(name, cuda_device):
     sol = s.compute_port_solution()
     assert rel_err(sol.y, g["y"]) < 1e-6
     assert np.max(np.abs(_zin(sol.y) - _zin(g["y"])) / np.abs(_zin(g["y"]))) <= 1e-6
-    assert s.last_refinement["last_correction"] <= 1e-7
+    assert s.last_refinement["last_correction"] <= s.mixed_tol
 
 
 @pytest.mark.parametrize("name", ["d1_dipole20", "d2_pec", "d2_ek_monopole_pec"])

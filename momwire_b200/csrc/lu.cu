@@ -1368,8 +1368,10 @@ constexpr int kLaPanelCtas = 32;
 
 struct AuxStreams {
     cudaStream_t trail = nullptr;
+    cudaStream_t critical = nullptr;  // highest priority: the chain the other stream feeds
     cudaEvent_t ev_main = nullptr;  // main -> trail
     cudaEvent_t ev_trail[4] = {};   // trail j -> main (ring)
+    cudaEvent_t ev_handover = nullptr, ev_back = nullptr;  // caller <-> critical
 };
 
 // one set per host thread and device: concurrent factorisations from
@@ -1381,11 +1383,34 @@ static mw_status aux_streams(AuxStreams** out) {
     MW_REQUIRE(dev >= 0 && dev < 64, "device index out of range");
     AuxStreams& a = per_dev[dev];
     if (!a.trail) {
+        int least = 0, greatest = 0;
+        MW_CHECK_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
         MW_CHECK_CUDA(cudaStreamCreateWithFlags(&a.trail, cudaStreamNonBlocking));
+        MW_CHECK_CUDA(cudaStreamCreateWithPriority(&a.critical, cudaStreamNonBlocking, greatest));
         MW_CHECK_CUDA(cudaEventCreateWithFlags(&a.ev_main, cudaEventDisableTiming));
         for (auto& e : a.ev_trail) MW_CHECK_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        MW_CHECK_CUDA(cudaEventCreateWithFlags(&a.ev_handover, cudaEventDisableTiming));
+        MW_CHECK_CUDA(cudaEventCreateWithFlags(&a.ev_back, cudaEventDisableTiming));
     }
     *out = &a;
+    return MW_OK;
+}
+
+// The critical chain of a two-stream routine (panels, leaves) runs on the
+// highest-priority stream, so that the CTA scheduler hands it the first SMs
+// that free up while the bulk updates fill the rest: the caller's stream
+// hands over (everything queued on it first) ...
+static mw_status critical_begin(AuxStreams* ax, cudaStream_t caller, cudaStream_t* out) {
+    MW_CHECK_CUDA(cudaEventRecord(ax->ev_handover, caller));
+    MW_CHECK_CUDA(cudaStreamWaitEvent(ax->critical, ax->ev_handover, 0));
+    *out = ax->critical;
+    return MW_OK;
+}
+
+// ... and waits for it at the end.
+static mw_status critical_end(AuxStreams* ax, cudaStream_t caller) {
+    MW_CHECK_CUDA(cudaEventRecord(ax->ev_back, ax->critical));
+    MW_CHECK_CUDA(cudaStreamWaitEvent(caller, ax->ev_back, 0));
     return MW_OK;
 }
 
@@ -1419,13 +1444,19 @@ static mw_status getrf_lookahead(int64_t n, T* A, int64_t lda, int32_t* ipiv, in
     cudaStream_t tr = ax->trail;
     PanelWs* pws = reinterpret_cast<PanelWs*>(ws);
     const int64_t nb = (n + kOuterNB - 1) / kOuterNB;
+    const cudaStream_t caller = st;
+    {
+        mw_status s0 = critical_begin(ax, caller, &st);
+        if (s0 != MW_OK) return s0;
+    }
     // the trail stream starts after everything already queued on st
     MW_CHECK_CUDA(cudaEventRecord(ax->ev_main, st));
     MW_CHECK_CUDA(cudaStreamWaitEvent(tr, ax->ev_main, 0));
     for (int64_t j = 0; j < nb; ++j) {
         if (cancel && *cancel) {
-            // let the trail stream finish what it was given before returning
+            // let both streams finish what they were given before returning
             MW_CHECK_CUDA(cudaStreamSynchronize(tr));
+            MW_CHECK_CUDA(cudaStreamSynchronize(st));
             set_error("factorisation cancelled");
             return MW_ERR_CANCELLED;
         }
@@ -1517,7 +1548,7 @@ static mw_status getrf_lookahead(int64_t n, T* A, int64_t lda, int32_t* ipiv, in
         laswp_launch<T>(A, lda, 0, j0, ipiv, j0, j0 + jb, st);
     }
     MW_CHECK_CUDA(cudaMemcpyAsync(info + 1, &pws->err, sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
-    return MW_OK;
+    return critical_end(ax, caller);
 }
 
 // One triangular sweep over the right-hand sides B with look-ahead.  Step i
@@ -1542,6 +1573,11 @@ static mw_status trsm_sweep(bool upper, int64_t n, int64_t nrhs, const T* LU, in
     }
     cudaStream_t tr = ax->trail;
     const int64_t nblk = (n + LF - 1) / LF;
+    const cudaStream_t caller = st;
+    {
+        mw_status s0 = critical_begin(ax, caller, &st);
+        if (s0 != MW_OK) return s0;
+    }
     auto blk0 = [&](int64_t b) { return b * LF < n ? b * LF : n; };
     auto blk1 = [&](int64_t b) { return (b + 1) * LF < n ? (b + 1) * LF : n; };
     // the second stream starts after everything queued on st
@@ -1585,7 +1621,7 @@ static mw_status trsm_sweep(bool upper, int64_t n, int64_t nrhs, const T* LU, in
     MW_CHECK_CUDA(cudaEventRecord(ax->ev_main, tr));
     MW_CHECK_CUDA(cudaStreamWaitEvent(st, ax->ev_main, 0));
     MW_CHECK_CUDA(cudaGetLastError());
-    return MW_OK;
+    return critical_end(ax, caller);
 }
 
 // X <- U^-1 X (the back substitution of a solve).

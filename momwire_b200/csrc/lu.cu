@@ -20,6 +20,7 @@
 // Pivot choice follows LAPACK's izamax: max |re| + |im|, first index wins
 // (complex64: the float sum, as LAPACK's icamax).
 #include <cstdio>
+#include <cstdlib>
 #include <type_traits>
 
 #include "common.cuh"
@@ -1366,6 +1367,20 @@ static mw_status getrf(int64_t n, T* A, int64_t lda, int32_t* ipiv, int32_t* inf
 // two streams use separate packed-operand workspaces; events order them.
 constexpr int kLaPanelCtas = 32;
 
+// SMs the complex64 factorisation's critical chain keeps free of the bulk
+// updates: kLaPanelCtas, or $MOMWIRE_B200_MAIN_SMS (8 .. 120) for tuning.
+static int main_sms() {
+    static int v = -1;
+    if (v < 0) {
+        v = kLaPanelCtas;
+        if (const char* e = getenv("MOMWIRE_B200_MAIN_SMS")) {
+            const int x = atoi(e);
+            if (x >= 8 && x <= 120) v = x;
+        }
+    }
+    return v;
+}
+
 struct AuxStreams {
     cudaStream_t trail = nullptr;
     cudaStream_t critical = nullptr;  // highest priority: the chain the other stream feeds
@@ -1695,7 +1710,7 @@ static Updater tc_updater_main(char* ws, int64_t n, int64_t nrhs_max) {
     u.tc_ws = reinterpret_cast<void*>((reinterpret_cast<uintptr_t>(base) + 1023) & ~uintptr_t(1023));
     u.tc_ws_bytes = cgemm_tc_workspace(n, nrhs_max > kOuterNB ? nrhs_max : kOuterNB, kOuterNB);
     u.tc_err = t.tc_err;
-    u.max_ctas = kLaPanelCtas;
+    u.max_ctas = main_sms();
     return u;
 }
 
@@ -1744,7 +1759,7 @@ extern "C" mw_status mw_cgetrf(int64_t n, float* Ad, int64_t lda, int32_t* ipiv,
     char* ws = static_cast<char*>(workspace);
     Updater up = tc_updater(ws, workspace_bytes, n, nrhs_max);
     Updater up_main = tc_updater_main(ws, n, nrhs_max);
-    up.max_ctas = panel_sms<cf>() - kLaPanelCtas;  // the trail stream leaves the panel its SMs
+    up.max_ctas = panel_sms<cf>() - main_sms();  // the trail stream leaves the panel its SMs
     cudaStream_t st = as_stream(stream);
     MW_CHECK_CUDA(cudaMemsetAsync(up.tc_err, 0, sizeof(int), st));
     mw_status s = getrf_lookahead<cf>(n, reinterpret_cast<cf*>(Ad), lda, ipiv, info, ws, cancel, up_main, up, st);
@@ -1769,7 +1784,7 @@ mw_status cgetrf_forward(int64_t n, float* Ad, int64_t lda, int32_t* ipiv, int32
     char* ws = static_cast<char*>(workspace);
     Updater up = tc_updater(ws, workspace_bytes, n, nrhs);
     Updater up_main = tc_updater_main(ws, n, nrhs);
-    up.max_ctas = panel_sms<cf>() - kLaPanelCtas;
+    up.max_ctas = panel_sms<cf>() - main_sms();
     cudaStream_t st = as_stream(stream);
     MW_CHECK_CUDA(cudaMemsetAsync(up.tc_err, 0, sizeof(int), st));
     int32_t* perm_all = static_pivot ? reinterpret_cast<int32_t*>(ws + cgetrf_perm_offset(n, nrhs)) : nullptr;
@@ -1794,7 +1809,7 @@ mw_status cgetrs_upper(int64_t n, int64_t nrhs, const float* LUd, int64_t lda, f
     char* ws = static_cast<char*>(workspace);
     Updater up = tc_updater(ws, workspace_bytes, n, nrhs);
     Updater up_main = tc_updater_main(ws, n, nrhs);
-    up.max_ctas = panel_sms<cf>() - kLaPanelCtas;
+    up.max_ctas = panel_sms<cf>() - main_sms();
     return getrs_upper<cf>(n, nrhs, reinterpret_cast<const cf*>(LUd), lda, reinterpret_cast<cf*>(Bd), ldb, up_main,
                            up, as_stream(stream));
 }
@@ -1809,7 +1824,7 @@ extern "C" mw_status mw_cgetrs(int64_t n, int64_t nrhs, const float* LUd, int64_
     char* ws = static_cast<char*>(workspace);
     Updater up = tc_updater(ws, workspace_bytes, n, nrhs);
     Updater up_main = tc_updater_main(ws, n, nrhs);
-    up.max_ctas = panel_sms<cf>() - kLaPanelCtas;  // the rest updates leave the leaves their SMs
+    up.max_ctas = panel_sms<cf>() - main_sms();  // the rest updates leave the leaves their SMs
     return getrs<cf>(n, nrhs, reinterpret_cast<const cf*>(LUd), lda, ipiv, reinterpret_cast<cf*>(Bd), ldb, up_main, up,
                      as_stream(stream));
 }

@@ -44,174 +44,190 @@ __device__ __forceinline__ cf crcp_sp(cf z) {
 
 __device__ __forceinline__ float cabs1f(cf z) { return fabsf(z.re) + fabsf(z.im); }
 
-constexpr size_t kSpDiagSmem = sizeof(cf) * (kSpB * 33 + 3 * 32 * 33);
-
-__device__ __forceinline__ void group_sync(int id) {
-    // the 128 threads (four warps) of one column group
-    asm volatile("bar.sync %0, 128;" ::"r"(id) : "memory");
-}
+constexpr int kSpLD = kSpB + 2;  // column stride of the staged block (complex; 16-byte aligned columns)
+constexpr int kSpPW = 32;        // panel width inside the block
+constexpr size_t kSpDiagSmem = sizeof(cf) * (size_t)kSpB * kSpLD;
 
 // Factor A[j0 .. j0+jb) x [j0 .. j0+jb) in place with partial pivoting among
-// these rows, blocked by 32-column chunks.  Thread (r, g) holds row r's
-// columns 32g .. 32g+31 (chunk g) in registers.  Chunk k is factored by its
-// own four warps alone (rank-1 updates inside the chunk, two group
-// barriers per column); then every later chunk g takes the chunk's U rows
-// (the pivot rows' chunk-g values, solved with the chunk's unit lower
-// triangle by one warp) and removes the chunk from its unpivoted rows with
-// one 32 x 32 block product per row.  A chosen pivot row keeps its place in
-// registers (its later columns become its U row); rows move once, when the
-// block is written back in pivot order.
+// these rows: a blocked LU of the block staged in shared memory (column
+// major).  Each 32-column panel is factored in registers -- thread (r, s)
+// holds row r's panel columns 8s .. 8s+7, every thread takes part in every
+// column -- with rows interchanged physically (registers for the panel,
+// shared memory for the other columns); then the panel's U rows of the
+// later columns (U12 = L11^-1 A12, one thread per column) and the update of
+// the trailing block (A22 -= L21 U12, 4 x 2 register tiles) follow.  Two
+// barriers per column, a few per panel.
 __global__ void __launch_bounds__(kSpDiagThreads, 1)
     sp_diag_kernel(cf* __restrict__ A, int64_t lda, int64_t j0, int jb, int32_t* __restrict__ ipiv,
                    int32_t* __restrict__ info, cf* __restrict__ inv_diag, int32_t* __restrict__ perm, PanelWs* ws) {
-    __shared__ cf s_col[kSpB];                 // column c of every row
-    __shared__ cf s_u[32];                     // the pivot row's chunk values
-    // dynamic: chunk k of every row (L values of the unpivoted rows), then
-    // the U rows of chunk k's pivots in each later chunk
     extern __shared__ __align__(16) unsigned char sp_diag_smem[];
-    auto s_L = reinterpret_cast<cf(*)[33]>(sp_diag_smem);                          // [kSpB][33]
-    auto s_Ug = reinterpret_cast<cf(*)[32][33]>(sp_diag_smem + sizeof(cf) * kSpB * 33);  // [3][32][33]
-    __shared__ unsigned long long s_wkey[4];
-    __shared__ int s_piv[32];                  // physical rows chosen in chunk k
-    __shared__ int s_pos_of[kSpB];             // current position of each physical row
-    __shared__ int s_row_at[kSpB];             // physical row at each position
+    cf* S = reinterpret_cast<cf*>(sp_diag_smem);  // S[col * kSpLD + row]
+    __shared__ cf s_col[2][kSpB];                 // column c of every row (by column parity)
+    __shared__ unsigned long long s_key[2][4];
+    __shared__ cf s_u[2][kSpPW];                  // the pivot row's panel values
+    __shared__ cf s_rc[2][kSpPW];                 // row c's panel values before the interchange
+    __shared__ int s_row_at[kSpB];                // original row at each position
     const int tid = threadIdx.x;
-    const int r = tid & (kSpB - 1);
-    const int g = tid >> 7;
     const int lane = tid & 31;
-    const int wig = (tid >> 5) & 3;  // warp within its column group
-    cf a[32];
+    for (int base = 0; base < kSpB * kSpB; base += 8 * kSpDiagThreads) {
+        cf t[8];
 #pragma unroll
-    for (int i = 0; i < 32; ++i) {
-        const int col = 32 * g + i;
-        a[i] = (r < jb && col < jb) ? A[(j0 + r) + (j0 + col) * lda] : cf{0.0f, 0.0f};
+        for (int u = 0; u < 8; ++u) {
+            const int idx = base + u * kSpDiagThreads + tid;
+            const int rr = idx % kSpB, col = idx / kSpB;
+            t[u] = (rr < jb && col < jb) ? A[(j0 + rr) + (j0 + col) * lda] : cf{0.0f, 0.0f};
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int idx = base + u * kSpDiagThreads + tid;
+            S[(idx / kSpB) * kSpLD + idx % kSpB] = t[u];
+        }
     }
-    bool active = r < jb;
-    if (tid < kSpB) {
-        s_pos_of[tid] = tid;
-        s_row_at[tid] = tid;
-    }
+    if (tid < kSpB) s_row_at[tid] = tid;
     __syncthreads();
-    const int nchunk = (jb + 31) / 32;
-    for (int k = 0; k < nchunk; ++k) {
-        const int nck = (jb - 32 * k) < 32 ? (jb - 32 * k) : 32;  // columns in chunk k
-        if (g == k) {
-            // ---- (a) chunk k, by its own four warps
+    const int r = tid & (kSpB - 1);
+    const int sg = tid >> 7;  // panel column group: columns 8 sg .. 8 sg + 7 of the panel
+    const int wig = (tid >> 5) & 3;
+    for (int c0 = 0; c0 < jb; c0 += kSpPW) {
+        const int nck = (jb - c0) < kSpPW ? (jb - c0) : kSpPW;
+        cf pr[8];
 #pragma unroll
-            for (int cc = 0; cc < 32; ++cc) {
-                if (cc < nck) {
-                    const int c = 32 * k + cc;
-                    const cf v = a[cc];
-                    s_col[r] = v;
-                    // largest |re| + |im| among the rows not yet chosen, then
-                    // the smallest position (LAPACK's icamax on the arranged
-                    // rows); the low bits carry the physical row
-                    unsigned long long key = 0;
-                    if (active)
-                        key = ((unsigned long long)__float_as_uint(cabs1f(v)) << 32) |
-                              ((unsigned long long)(0xFFFFu - (unsigned int)s_pos_of[r]) << 16) |
-                              (unsigned long long)r;
+        for (int q = 0; q < 8; ++q) pr[q] = S[(c0 + 8 * sg + q) * kSpLD + r];
+#pragma unroll 1
+        for (int cc = 0; cc < nck; ++cc) {
+            const int c = c0 + cc, scol = cc >> 3, qc = cc & 7, par = cc & 1;
+            if (sg == scol) {
+                cf v = pr[0];
 #pragma unroll
-                    for (int off = 16; off > 0; off >>= 1) {
-                        const unsigned long long o = __shfl_xor_sync(0xffffffffu, key, off);
-                        key = o > key ? o : key;
-                    }
-                    if (lane == 0) s_wkey[wig] = key;
-                    group_sync(1 + k);
-                    unsigned long long best = s_wkey[0];
+                for (int q = 1; q < 8; ++q)
+                    if (q == qc) v = pr[q];
+                s_col[par][r] = v;
+                // largest |re| + |im| among rows c .. jb-1, then the smallest
+                // row (LAPACK's icamax); the low bits carry the row
+                unsigned long long key = 0;
+                if (r >= c && r < jb)
+                    key = ((unsigned long long)__float_as_uint(cabs1f(v)) << 32) |
+                          ((unsigned long long)(0xFFFFu - (unsigned int)r) << 16) | (unsigned long long)r;
 #pragma unroll
-                    for (int w = 1; w < 4; ++w) best = s_wkey[w] > best ? s_wkey[w] : best;
-                    const int p = (int)(best & 0xFFFFull);
-                    const int pos_best = (int)(0xFFFFu - (unsigned int)((best >> 16) & 0xFFFFull));
-                    const bool zero = (best >> 32) == 0ull;
-                    const cf inv = zero ? cone<cf>() : crcp_sp(s_col[p]);
-                    if (r == p) {
+                for (int off = 16; off > 0; off >>= 1) {
+                    const unsigned long long o = __shfl_xor_sync(0xffffffffu, key, off);
+                    key = o > key ? o : key;
+                }
+                if (lane == 0) s_key[par][wig] = key;
+            }
+            __syncthreads();
+            unsigned long long best = s_key[par][0];
 #pragma unroll
-                        for (int l = cc; l < 32; ++l) s_u[l] = a[l];
-                        active = false;
-                        s_piv[cc] = p;
-                    }
-                    const cf lr = (active && !zero) ? s_col[r] * inv : cf{0.0f, 0.0f};
-                    if (tid == 128 * k) {
-                        // the interchange LAPACK makes: positions c and pos_best
-                        ipiv[j0 + c] = (int32_t)(j0 + pos_best + 1);
-                        if (zero) {
-                            if (info[0] == 0) info[0] = (int32_t)(j0 + c + 1);
-                            atomicExch(&ws->lmax_bits, 0x7f800000u);  // +inf: the block is singular
-                        }
-                        inv_diag[c] = inv;
-                        const int pc = s_row_at[c];
-                        s_row_at[c] = p;
-                        s_row_at[pos_best] = pc;
-                        s_pos_of[p] = c;
-                        s_pos_of[pc] = pos_best;
-                    }
-                    group_sync(1 + k);  // s_u, s_pos_of complete; s_col and s_wkey read
-                    if (active && !zero) {
-                        a[cc] = lr;
+            for (int w = 1; w < 4; ++w) best = s_key[par][w] > best ? s_key[par][w] : best;
+            const int p = (int)(best & 0xFFFFull);
+            const bool zero = (best >> 32) == 0ull;
+            const cf inv = zero ? cone<cf>() : crcp_sp(s_col[par][p]);
+            if (r == p) {
 #pragma unroll
-                        for (int l = cc + 1; l < 32; ++l) a[l] = a[l] - lr * s_u[l];
-                    }
+                for (int q = 0; q < 8; ++q) s_u[par][8 * sg + q] = pr[q];
+            }
+            if (r == c) {
+#pragma unroll
+                for (int q = 0; q < 8; ++q) s_rc[par][8 * sg + q] = pr[q];
+            }
+            // the interchange in the columns outside the panel, one column
+            // per thread
+            if (p != c && tid < kSpB && (tid < c0 || tid >= c0 + kSpPW)) {
+                cf* col = S + tid * kSpLD;
+                const cf t0 = col[c];
+                col[c] = col[p];
+                col[p] = t0;
+            }
+            if (tid == 0) {
+                ipiv[j0 + c] = (int32_t)(j0 + p + 1);
+                if (zero) {
+                    if (info[0] == 0) info[0] = (int32_t)(j0 + c + 1);
+                    atomicExch(&ws->lmax_bits, 0x7f800000u);  // +inf: the block is singular
+                }
+                inv_diag[c] = inv;
+                const int t0 = s_row_at[c];
+                s_row_at[c] = s_row_at[p];
+                s_row_at[p] = t0;
+            }
+            __syncthreads();  // s_u, s_rc complete
+            if (r == c) {
+#pragma unroll
+                for (int q = 0; q < 8; ++q) pr[q] = s_u[par][8 * sg + q];
+            } else if (r == p) {
+#pragma unroll
+                for (int q = 0; q < 8; ++q) pr[q] = s_rc[par][8 * sg + q];
+            }
+            if (r > c && r < jb && !zero) {
+                // row p now holds row c's old values
+                const cf l = (r == p ? s_col[par][c] : s_col[par][r]) * inv;
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    const int pc = 8 * sg + q;
+                    if (pc == cc) pr[q] = l;
+                    else if (pc > cc) pr[q] = pr[q] - l * s_u[par][pc];
                 }
             }
-#pragma unroll
-            for (int l = 0; l < 32; ++l) s_L[r][l] = a[l];
         }
-        __syncthreads();  // chunk k factored: s_L and s_piv published
-        if (g > k) {
-            // rows chosen in chunk k stop updating; the chunk's pivot rows
-            // publish their chunk-g values (row i of the U block)
-            int my_i = -1;
-            for (int i = 0; i < nck; ++i)
-                if (s_piv[i] == r) my_i = i;
-            if (my_i >= 0) {
-                active = false;
 #pragma unroll
-                for (int l = 0; l < 32; ++l) s_Ug[g - k - 1][my_i][l] = a[l];
-            }
-            group_sync(1 + g);
-            if (wig == 0) {
-                // U = L_kk^-1 (pivot rows): lane l solves column l, the rows
-                // already solved read back from shared memory
-                for (int i = 1; i < nck; ++i) {
-                    const int pi = s_piv[i];
-                    cf t = s_Ug[g - k - 1][i][lane];
-                    for (int jj = 0; jj < i; ++jj) t = t - s_L[pi][jj] * s_Ug[g - k - 1][jj][lane];
-                    s_Ug[g - k - 1][i][lane] = t;
+        for (int q = 0; q < 8; ++q) S[(c0 + 8 * sg + q) * kSpLD + r] = pr[q];
+        __syncthreads();
+        const int t0 = c0 + kSpPW;  // first trailing column (and row)
+        const int nt = jb - t0;
+        if (nt > 0) {
+            // U12 = L11^-1 A12 on the panel's rows, one thread per column
+            if (tid < nt) {
+                cf* col = S + (t0 + tid) * kSpLD + c0;
+                cf x[kSpPW];
+#pragma unroll
+                for (int i = 0; i < kSpPW; ++i) x[i] = col[i];
+#pragma unroll
+                for (int i = 1; i < kSpPW; ++i) {
+                    cf t = x[i];
+#pragma unroll
+                    for (int jj = 0; jj < i; ++jj) t = t - S[(c0 + jj) * kSpLD + c0 + i] * x[jj];
+                    x[i] = t;
                 }
-            }
-            group_sync(1 + g);
-            if (my_i >= 0) {
 #pragma unroll
-                for (int l = 0; l < 32; ++l) a[l] = s_Ug[g - k - 1][my_i][l];
+                for (int i = 0; i < kSpPW; ++i) col[i] = x[i];
             }
-            // the block product, by whole warps that still hold unpivoted rows
-            if (__any_sync(0xffffffffu, active) && active) {
-                for (int jj = 0; jj < nck; ++jj) {
-                    const cf x = s_L[r][jj];
-                    const cf* urow = &s_Ug[g - k - 1][jj][0];
+            __syncthreads();
+            // A22 -= L21 U12 over rows and columns t0 .. jb-1, 4 x 2 tiles
+            const int ntr = (nt + 3) / 4, ntc = (nt + 1) / 2;
+            for (int tile = tid; tile < ntr * ntc; tile += kSpDiagThreads) {
+                const int i0 = t0 + 4 * (tile % ntr), jc = t0 + 2 * (tile / ntr);
+                cf acc[4][2];
 #pragma unroll
-                    for (int l = 0; l < 32; ++l) a[l] = a[l] - x * urow[l];
+                for (int b2 = 0; b2 < 2; ++b2)
+#pragma unroll
+                    for (int a4 = 0; a4 < 4; ++a4) acc[a4][b2] = S[(jc + b2) * kSpLD + i0 + a4];
+#pragma unroll 4
+                for (int jj = 0; jj < kSpPW; ++jj) {
+                    const cf* lcol = S + (c0 + jj) * kSpLD + i0;
+                    const float4 l01 = *reinterpret_cast<const float4*>(lcol);
+                    const float4 l23 = *reinterpret_cast<const float4*>(lcol + 2);
+                    const cf l[4] = {cf{l01.x, l01.y}, cf{l01.z, l01.w}, cf{l23.x, l23.y}, cf{l23.z, l23.w}};
+                    const cf u0 = S[jc * kSpLD + c0 + jj], u1 = S[(jc + 1) * kSpLD + c0 + jj];
+#pragma unroll
+                    for (int a4 = 0; a4 < 4; ++a4) {
+                        acc[a4][0] = acc[a4][0] - l[a4] * u0;
+                        acc[a4][1] = acc[a4][1] - l[a4] * u1;
+                    }
                 }
+#pragma unroll
+                for (int b2 = 0; b2 < 2; ++b2)
+#pragma unroll
+                    for (int a4 = 0; a4 < 4; ++a4) S[(jc + b2) * kSpLD + i0 + a4] = acc[a4][b2];
             }
-        } else if (g < k) {
-            // earlier chunks: only the chosen rows change state
-            for (int i = 0; i < nck; ++i)
-                if (s_piv[i] == r) active = false;
+            __syncthreads();
         }
-        __syncthreads();  // s_L, s_Ug and s_piv free for the next chunk
     }
-    if (r < jb) {
-        const int pos = s_pos_of[r];
-        const int64_t row = j0 + pos;
-#pragma unroll
-        for (int i = 0; i < 32; ++i) {
-            const int col = 32 * g + i;
-            if (col < jb) A[row + (j0 + col) * lda] = a[i];
-        }
-        // the block's rows in pivot order: position pos holds row r
-        if (g == 0) perm[pos] = r;
+    for (int base = 0; base < kSpB * kSpB; base += kSpDiagThreads) {
+        const int idx = base + tid;
+        const int rr = idx % kSpB, col = idx / kSpB;
+        if (rr < jb && col < jb) A[(j0 + rr) + (j0 + col) * lda] = S[col * kSpLD + rr];
     }
+    // the block's rows in pivot order: position i holds original row s_row_at[i]
+    if (tid < jb) perm[tid] = s_row_at[tid];
 }
 
 // Rows [row0, row0 + jb) of columns [col0, col0 + ncols) rearranged in

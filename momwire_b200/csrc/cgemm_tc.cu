@@ -27,25 +27,17 @@
 
 #include "common.cuh"
 #include "tc_common.cuh"
+#include "tc_layout.cuh"
 
 namespace mw {
 
-#ifndef MW_TC_KS
-#define MW_TC_KS 16
-#endif
 #ifndef MW_TC_STAGES
 #define MW_TC_STAGES 4
 #endif
 #ifndef MW_TC_EPI_WARPS
 #define MW_TC_EPI_WARPS 8
 #endif
-constexpr int TC_M = 128;                           // real rows per tile
-constexpr int TC_N = 256;                           // columns per tile
-constexpr int TC_KS = MW_TC_KS;                     // real K per stage (a multiple of 8)
-constexpr int TC_CHUNKS = TC_KS / 4;                // 16-byte K chunks per stage
 constexpr int TC_STAGES = MW_TC_STAGES;             // depth of the shared-memory ring
-constexpr int TC_A_BYTES = TC_M * TC_KS * 4;        // per plane and stage
-constexpr int TC_B_BYTES = TC_N * TC_KS * 4;
 constexpr int TC_STAGE_BYTES = 2 * TC_A_BYTES + 2 * TC_B_BYTES;
 constexpr int TC_EPI_WARPS = MW_TC_EPI_WARPS;       // 4 or 8: each TMEM lane quadrant by 1 or 2 warps
 constexpr int TC_THREADS = 64 + 32 * TC_EPI_WARPS;
@@ -246,11 +238,6 @@ __global__ void __launch_bounds__(TC_THREADS, 1) cgemm_tc_kernel(TcArgs P) {
 }
 
 // -------------------------------------------------------------- packing
-__device__ __forceinline__ float tf32_hi(float x) {
-    uint32_t r;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-    return __uint_as_float(r);
-}
 
 // Ahat (2m x 2k, from complex A at A + (i + l*lda)) packed as
 // [mb][ks][chunk TC_CHUNKS][row 128][4]; zero beyond (2m, 2k).
@@ -379,6 +366,48 @@ mw_status cgemm_tc_update_batched(int64_t m, int64_t n, int64_t k, int batch, co
     const int grid = tiles < cap ? (int)tiles : cap;
     {
         ProfileScope ps(PC_CGEMM_TC, st, 8.0 * (double)m * n * k * batch, 8.0 * 2.0 * (double)m * n * batch);
+        cgemm_tc_kernel<<<grid, TC_THREADS, TC_STAGES * TC_STAGE_BYTES, st>>>(P);
+    }
+    MW_CHECK_CUDA(cudaGetLastError());
+    count_launch();
+    return MW_OK;
+}
+
+// The four planes inside a workspace laid out as cgemm_tc_workspace(m_max,
+// n_max, k) lays it out; updates of any m <= m_max, n <= n_max, k may use
+// them (the blocks of a plane keep their offsets).
+TcPlanes tc_planes(void* ws, int64_t m_max, int64_t n_max, int64_t k) {
+    auto al = [](size_t x) { return (x + 1023) & ~size_t(1023); };
+    const size_t ab = tc_pack_a_bytes(m_max, k), bb = tc_pack_b_bytes(k, n_max);
+    char* w = static_cast<char*>(ws);
+    return TcPlanes{reinterpret_cast<float*>(w), reinterpret_cast<float*>(w + al(ab)),
+                    reinterpret_cast<float*>(w + 2 * al(ab)), reinterpret_cast<float*>(w + 2 * al(ab) + al(bb))};
+}
+
+// C (m x n complex64, column-major) -= A B from operands already packed in
+// the planes (for an inner dimension k): no packing pass.
+mw_status cgemm_tc_prepacked(int64_t m, int64_t n, int64_t k, const TcPlanes& pl, cf* C, int64_t ldc, int* err,
+                             cudaStream_t st, int max_ctas) {
+    if (m <= 0 || n <= 0 || k <= 0) return MW_OK;
+    const int n_mb = (int)((2 * m + TC_M - 1) / TC_M);
+    const int n_nb = (int)((n + TC_N - 1) / TC_N);
+    const int n_ks = tc_n_ks(k);
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        MW_CHECK_CUDA(cudaFuncSetAttribute(cgemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           TC_STAGES * TC_STAGE_BYTES));
+    }
+    TcArgs P{pl.a_hi, pl.a_lo, pl.b_hi, pl.b_lo, reinterpret_cast<float*>(C), ldc, 2 * m, n, n_mb, n_nb, n_ks, err,
+             1, 0, 0, 0};
+    const int64_t tiles = (int64_t)n_mb * n_nb;
+    MW_REQUIRE(tiles < (1ll << 31), "too many tiles");
+    const int cap = (max_ctas > 0 && max_ctas < sms) ? max_ctas : sms;
+    const int grid = tiles < cap ? (int)tiles : cap;
+    {
+        ProfileScope ps(PC_CGEMM_TC, st, 8.0 * (double)m * n * k, 8.0 * 2.0 * (double)m * n);
         cgemm_tc_kernel<<<grid, TC_THREADS, TC_STAGES * TC_STAGE_BYTES, st>>>(P);
     }
     MW_CHECK_CUDA(cudaGetLastError());

@@ -24,6 +24,7 @@
 #include <type_traits>
 
 #include "common.cuh"
+#include "tc_layout.cuh"
 #include "waits.cuh"
 
 namespace mw {
@@ -32,10 +33,13 @@ namespace mw {
 mw_status cgemm_tc_update(int64_t m, int64_t n, int64_t k, const cf* A, int64_t lda, const cf* B, int64_t ldb, cf* C,
                           int64_t ldc, void* ws, size_t ws_bytes, int* err, cudaStream_t st, int max_ctas);
 size_t cgemm_tc_workspace(int64_t m, int64_t n, int64_t k);
+TcPlanes tc_planes(void* ws, int64_t m_max, int64_t n_max, int64_t k);
+mw_status cgemm_tc_prepacked(int64_t m, int64_t n, int64_t k, const TcPlanes& pl, cf* C, int64_t ldc, int* err,
+                             cudaStream_t st, int max_ctas);
 
 // static-pivot panel of the complex64 path (lu_static.cu)
 mw_status static_panel_c64(cf* A, int64_t lda, int64_t n, int64_t j0, int jb, int32_t* ipiv, int32_t* info,
-                           PanelWs* ws, cf* inv_diag, int32_t* perm, cudaStream_t st);
+                           PanelWs* ws, cf* inv_diag, int32_t* perm, const TcPlanes* pack_a, cudaStream_t st);
 void static_permute_c64(cf* A, int64_t lda, int64_t row0, int jb, int64_t col0, int64_t ncols, const int32_t* perm,
                         cudaStream_t st);
 void static_left_permute_c64(cf* A, int64_t lda, int64_t n, const int32_t* perm_all, cudaStream_t st);
@@ -601,10 +605,20 @@ struct GetrsLeaf<cf> {
 // solves take NC = 4 (a quarter of the CTAs stage the triangle); narrow
 // ones, whose latency sits on the critical path, NC = 1 (more CTAs).
 constexpr int kTrsmWarps = 8;
+// Packed-B output of a leaf (complex64 only): the solved rows also written
+// as the B operand of a tensor-core update, rows at K offset kap0 / 2 of an
+// inner dimension of b_nks stages.
+struct LeafPack {
+    float* b_hi = nullptr;
+    float* b_lo = nullptr;
+    int b_nks = 0;
+    int kap0 = 0;
+};
+
 template <class T, bool UPPER, int L, int NC>
 __global__ void __launch_bounds__(32 * kTrsmWarps) trsm_kernel(const T* Tm, int64_t ldt, T* X, int64_t ldx, int jb,
                                                                int64_t ncols, const T* Aoff, int64_t ldo, const T* Xp,
-                                                               int K) {
+                                                               int K, LeafPack pk) {
     // Lane l owns rows RP*l .. RP*l+RP-1 of the block, so a RP x RP diagonal
     // block is solved inside one lane; its RP results reach the other lanes
     // in RP independent shuffles and every lane applies the RP x RP update:
@@ -781,6 +795,23 @@ __global__ void __launch_bounds__(32 * kTrsmWarps) trsm_kernel(const T* Tm, int6
             for (int a = 0; a < RP; ++a)
                 if (RP * lane + a < jb) X[(col0 + q) * ldx + RP * lane + a] = v[q][a];
         }
+    if constexpr (std::is_same<T, cf>::value && RP % 2 == 0) {
+        if (pk.b_hi != nullptr) {
+            // rows RP*lane .. +RP-1 are real K rows kap0 + 2 RP lane .. (re, im
+            // interleaved), whole 16-byte chunks; rows past jb carry zeros
+#pragma unroll
+            for (int q = 0; q < NC; ++q)
+                if (cok[q]) {
+#pragma unroll
+                    for (int a = 0; a < RP; a += 2) {
+                        const int64_t kap4 = pk.kap0 + 2 * (RP * lane + a);
+                        if (kap4 < (int64_t)pk.b_nks * TC_KS)
+                            tc_store_b4(pk.b_hi, pk.b_lo, pk.b_nks, col0 + q, kap4,
+                                        make_float4(v[q][a].re, v[q][a].im, v[q][a + 1].re, v[q][a + 1].im));
+                    }
+                }
+        }
+    }
 }
 
 template <class T, int L>
@@ -818,16 +849,19 @@ static mw_status trsm_setup() {
 
 template <class T, bool UPPER, int L = kNB>
 static void trsm_launch(const T* Tm, int64_t ldt, T* X, int64_t ldx, int jb, int64_t ncols, cudaStream_t st,
-                        const T* Aoff = nullptr, int64_t ldo = 0, const T* Xp = nullptr, int K = 0) {
+                        const T* Aoff = nullptr, int64_t ldo = 0, const T* Xp = nullptr, int K = 0,
+                        LeafPack pk = LeafPack{}) {
     ProfileScope ps(PC_TRSM, st, 4.0 * (double)jb * jb * ncols + 8.0 * (double)jb * K * ncols,
                     2.0 * sizeof(T) * (double)jb * ncols);
     if (ncols >= kTrsmWide) {
         const int64_t per_cta = (int64_t)kTrsmWarps * 4;
         trsm_kernel<T, UPPER, L, 4><<<(unsigned)((ncols + per_cta - 1) / per_cta), 32 * kTrsmWarps,
-                                      trsm_smem_bytes<T, L>(), st>>>(Tm, ldt, X, ldx, jb, ncols, Aoff, ldo, Xp, K);
+                                      trsm_smem_bytes<T, L>(), st>>>(Tm, ldt, X, ldx, jb, ncols, Aoff, ldo, Xp, K,
+                                                                     pk);
     } else {
         trsm_kernel<T, UPPER, L, 1><<<(unsigned)((ncols + kTrsmWarps - 1) / kTrsmWarps), 32 * kTrsmWarps,
-                                      trsm_smem_bytes<T, L>(), st>>>(Tm, ldt, X, ldx, jb, ncols, Aoff, ldo, Xp, K);
+                                      trsm_smem_bytes<T, L>(), st>>>(Tm, ldt, X, ldx, jb, ncols, Aoff, ldo, Xp, K,
+                                                                     pk);
     }
     count_launch();
 }
@@ -1201,11 +1235,26 @@ struct Updater {
     size_t tc_ws_bytes = 0;
     int* tc_err = nullptr;
     int max_ctas = 0;
+    int64_t ws_m = 0, ws_n = 0;  // the largest update the workspace was laid out for (k = kOuterNB)
 };
 
 static mw_status block_update(const cd* A, int64_t lda, const cd* B, int64_t ldb, cd* C, int64_t ldc, int64_t m,
                               int64_t n, int64_t k, const Updater& u, cudaStream_t st) {
     return zgemm_launch(false, false, m, n, k, cd{-1.0, 0.0}, A, lda, B, ldb, cd{1.0, 0.0}, C, ldc, st, u.max_ctas);
+}
+
+// C -= A B from operands already in the updater's planes (complex64).
+template <class T>
+static mw_status update_prepacked(int64_t m, int64_t n, int64_t k, const TcPlanes& pl, T* C, int64_t ldc,
+                                  const Updater& u, cudaStream_t st) {
+    if constexpr (std::is_same<T, cf>::value) {
+        MW_REQUIRE(m <= u.ws_m && n <= u.ws_n && k <= kOuterNB, "prepacked update larger than its planes");
+        return cgemm_tc_prepacked(m, n, k, pl, C, ldc, u.tc_err, st, u.max_ctas);
+    } else {
+        (void)m, (void)n, (void)k, (void)pl, (void)C, (void)ldc, (void)u, (void)st;
+        set_error("prepacked update is complex64 only");
+        return MW_ERR_INVALID;
+    }
 }
 
 static mw_status block_update(const cf* A, int64_t lda, const cf* B, int64_t ldb, cf* C, int64_t ldc, int64_t m,
@@ -1219,20 +1268,29 @@ static mw_status block_update(const cf* A, int64_t lda, const cf* B, int64_t ldb
 // reach it through one block update.
 template <class T>
 static mw_status trsm_lower_blocked(const T* L, int64_t ldl, T* X, int64_t ldx, int jb, int64_t ncols,
-                                    const Updater& up, cudaStream_t st) {
+                                    const Updater& up, cudaStream_t st, const TcPlanes* pack = nullptr) {
+    // with `pack` (complex64, jb <= 2 kNB) the solved rows are also written
+    // as the packed B operand of the update with inner dimension jb
     for (int b0 = 0; b0 < jb; b0 += kNB) {
         const int bb = (jb - b0) < kNB ? (jb - b0) : kNB;
+        LeafPack pk;
+        if (pack != nullptr) {
+            pk.b_hi = pack->b_hi;
+            pk.b_lo = pack->b_lo;
+            pk.b_nks = tc_n_ks(jb);
+            pk.kap0 = 2 * b0;
+        }
         if (b0 >= 2 * kNB) {
             const int k = b0 - kNB;  // blocks 0 .. b0-kNB-1
             mw_status s = block_update(L + b0, ldl, X, ldx, X + b0, ldx, bb, ncols, k, up, st);
             if (s != MW_OK) return s;
         }
         if (b0 == 0) {
-            trsm_launch<T, false>(L, ldl, X, ldx, bb, ncols, st);
+            trsm_launch<T, false>(L, ldl, X, ldx, bb, ncols, st, nullptr, 0, nullptr, 0, pk);
         } else {
             const int p0 = b0 - kNB;
             trsm_launch<T, false>(L + b0 + (int64_t)b0 * ldl, ldl, X + b0, ldx, bb, ncols, st,
-                                  L + b0 + (int64_t)p0 * ldl, ldl, X + p0, kNB);
+                                  L + b0 + (int64_t)p0 * ldl, ldl, X + p0, kNB, pk);
         }
     }
     return MW_OK;
@@ -1483,12 +1541,29 @@ static mw_status getrf_lookahead(int64_t n, T* A, int64_t lda, int32_t* ipiv, in
         // reach the columns beside it as one parallel row permutation (each
         // block's row order kept, for the columns left of it at the end)
         int32_t* perm = nullptr;
+        // static pivots, complex64: the panel's L21 and each solved block
+        // row are written straight into the tensor-core operand planes, so
+        // the updates run without a packing pass.  L21 of even panels lives
+        // in the trail updater's A planes, of odd ones in the main
+        // updater's: panel j + 2 overwrites them only after trail j, the
+        // last reader, has finished (the wait on ev_trail above).
+        bool prepacked = false;
+        TcPlanes pl_main{}, pl_trail{};
         if constexpr (std::is_same<T, cf>::value) {
             if (static_pivot) {
                 size_t ov, oi, orow, ocur;
                 ws_layout(kMaxPanelGrid, &ov, &oi, &orow, &ocur);
                 perm = perm_all + j0;
-                s = static_panel_c64(A, lda, n, j0, jb, ipiv, info, pws, reinterpret_cast<cf*>(ws + ocur), perm, st);
+                prepacked = up_main.tc_ws != nullptr && up_trail.tc_ws != nullptr && jb == kOuterNB;
+                if (prepacked) {
+                    pl_main = tc_planes(up_main.tc_ws, up_main.ws_m, up_main.ws_n, kOuterNB);
+                    pl_trail = tc_planes(up_trail.tc_ws, up_trail.ws_m, up_trail.ws_n, kOuterNB);
+                    const TcPlanes& own = (j & 1) ? pl_main : pl_trail;
+                    pl_main.a_hi = pl_trail.a_hi = own.a_hi;
+                    pl_main.a_lo = pl_trail.a_lo = own.a_lo;
+                }
+                s = static_panel_c64(A, lda, n, j0, jb, ipiv, info, pws, reinterpret_cast<cf*>(ws + ocur), perm,
+                                     prepacked ? &pl_main : nullptr, st);
             } else {
                 s = panel_factor<T>(A, lda, n, j0, jb, ipiv, info, ws, up_main, st, kLaPanelCtas);
             }
@@ -1514,20 +1589,24 @@ static mw_status getrf_lookahead(int64_t n, T* A, int64_t lda, int32_t* ipiv, in
         if (jbn > 0) {
             if (j >= 1) MW_CHECK_CUDA(cudaStreamWaitEvent(st, ax->ev_trail[(j - 1) & 3], 0));
             swap_rows(A, lda, c1, jbn, st);
-            s = trsm_lower_blocked<T>(A + j0 + j0 * lda, lda, A + j0 + c1 * lda, lda, jb, jbn, up_main, st);
+            s = trsm_lower_blocked<T>(A + j0 + j0 * lda, lda, A + j0 + c1 * lda, lda, jb, jbn, up_main, st,
+                                      prepacked ? &pl_main : nullptr);
             if (s != MW_OK) return s;
-            s = block_update(A + c1 + j0 * lda, lda, A + j0 + c1 * lda, lda, A + c1 + c1 * lda, lda, n - c1, jbn, jb,
-                             up_main, st);
+            s = prepacked ? update_prepacked(n - c1, jbn, jb, pl_main, A + c1 + c1 * lda, lda, up_main, st)
+                          : block_update(A + c1 + j0 * lda, lda, A + j0 + c1 * lda, lda, A + c1 + c1 * lda, lda,
+                                         n - c1, jbn, jb, up_main, st);
             if (s != MW_OK) return s;
         }
         // trail: everything right of the next block, after panel j
         MW_CHECK_CUDA(cudaStreamWaitEvent(tr, ax->ev_main, 0));
         if (n - c2 > 0) {
             swap_rows(A, lda, c2, n - c2, tr);
-            s = trsm_lower_blocked<T>(A + j0 + j0 * lda, lda, A + j0 + c2 * lda, lda, jb, n - c2, up_trail, tr);
+            s = trsm_lower_blocked<T>(A + j0 + j0 * lda, lda, A + j0 + c2 * lda, lda, jb, n - c2, up_trail, tr,
+                                      prepacked ? &pl_trail : nullptr);
             if (s != MW_OK) return s;
-            s = block_update(A + c1 + j0 * lda, lda, A + j0 + c2 * lda, lda, A + c1 + c2 * lda, lda, n - c1, n - c2,
-                             jb, up_trail, tr);
+            s = prepacked ? update_prepacked(n - c1, n - c2, jb, pl_trail, A + c1 + c2 * lda, lda, up_trail, tr)
+                          : block_update(A + c1 + j0 * lda, lda, A + j0 + c2 * lda, lda, A + c1 + c2 * lda, lda,
+                                         n - c1, n - c2, jb, up_trail, tr);
             if (s != MW_OK) return s;
         }
         if (Baug != nullptr && nrhs > 0) {
@@ -1536,11 +1615,14 @@ static mw_status getrf_lookahead(int64_t n, T* A, int64_t lda, int32_t* ipiv, in
             // (L21 stays as it is until the deferred left interchanges at the
             // end, which the later rows of Baug then mirror in its own swaps)
             swap_rows(Baug, ldb, 0, nrhs, tr);
-            s = trsm_lower_blocked<T>(A + j0 + j0 * lda, lda, Baug + j0, ldb, jb, nrhs, up_trail, tr);
+            const bool pk_rhs = prepacked && n - c1 > 0;
+            s = trsm_lower_blocked<T>(A + j0 + j0 * lda, lda, Baug + j0, ldb, jb, nrhs, up_trail, tr,
+                                      pk_rhs ? &pl_trail : nullptr);
             if (s != MW_OK) return s;
             if (n - c1 > 0) {
-                s = block_update(A + c1 + j0 * lda, lda, Baug + j0, ldb, Baug + c1, ldb, n - c1, nrhs, jb, up_trail,
-                                 tr);
+                s = pk_rhs ? update_prepacked(n - c1, nrhs, jb, pl_trail, Baug + c1, ldb, up_trail, tr)
+                           : block_update(A + c1 + j0 * lda, lda, Baug + j0, ldb, Baug + c1, ldb, n - c1, nrhs, jb,
+                                          up_trail, tr);
                 if (s != MW_OK) return s;
             }
         }
@@ -1689,6 +1771,8 @@ static Updater tc_updater(char* ws, size_t ws_bytes, int64_t n, int64_t nrhs_max
     int64_t w = n > nrhs_max ? n : nrhs_max;
     u.tc_ws = ws + p;
     u.tc_ws_bytes = cgemm_tc_workspace(n, w, kOuterNB);
+    u.ws_m = n;
+    u.ws_n = w;
     u.tc_err = reinterpret_cast<int*>(ws + p + ((u.tc_ws_bytes + 255) & ~size_t(255)));
     (void)ws_bytes;
     return u;
@@ -1708,7 +1792,9 @@ static Updater tc_updater_main(char* ws, int64_t n, int64_t nrhs_max) {
     Updater u;
     char* base = static_cast<char*>(t.tc_ws) + ((t.tc_ws_bytes + 255) & ~size_t(255)) + 256;
     u.tc_ws = reinterpret_cast<void*>((reinterpret_cast<uintptr_t>(base) + 1023) & ~uintptr_t(1023));
-    u.tc_ws_bytes = cgemm_tc_workspace(n, nrhs_max > kOuterNB ? nrhs_max : kOuterNB, kOuterNB);
+    u.ws_m = n;
+    u.ws_n = nrhs_max > kOuterNB ? nrhs_max : kOuterNB;
+    u.tc_ws_bytes = cgemm_tc_workspace(u.ws_m, u.ws_n, kOuterNB);
     u.tc_err = t.tc_err;
     u.max_ctas = main_sms();
     return u;

@@ -21,6 +21,7 @@
 // on the planar dipole arrays, a few per cent of columns on Yagis, where
 // the local pivot's |L| stays below 3).
 #include "common.cuh"
+#include "tc_layout.cuh"
 #include "waits.cuh"
 
 namespace mw {
@@ -277,7 +278,7 @@ __device__ __forceinline__ void load_u2(const cf* __restrict__ src, cf& u0, cf& 
 
 __global__ void __launch_bounds__(kSpL21Threads, 1)
     sp_l21_kernel(cf* __restrict__ A, int64_t lda, int64_t j0, int jb, int64_t row_end,
-                  const cf* __restrict__ inv_diag, PanelWs* ws) {
+                  const cf* __restrict__ inv_diag, PanelWs* ws, float* __restrict__ a_hi, float* __restrict__ a_lo) {
     extern __shared__ __align__(16) unsigned char sp_smem[];
     cf* sU = reinterpret_cast<cf*>(sp_smem);                 // [kSpB][kSpUStride]
     cf* sInv = sU + (size_t)kSpB * kSpUStride;               // [kSpB]
@@ -356,6 +357,23 @@ __global__ void __launch_bounds__(kSpL21Threads, 1)
             if (col < jb) A[row + (j0 + col) * lda] = a[l];
         }
     }
+    if (a_hi != nullptr) {
+        // L21 also as the packed operand of the trailing updates (rows from
+        // j0 + jb, inner dimension jb): each complex l is the 2 x 2 block
+        // [[re, -im], [im, re]]; rows past the matrix and columns past jb
+        // hold zeros, so that the tiles they pad contribute nothing
+        const int n_ks = tc_n_ks(jb);
+        const int64_t rho = 2 * (row - (j0 + jb));
+#pragma unroll
+        for (int l = 0; l < 32; l += 2) {
+            const int64_t kap4 = 2 * (32 * w + l);
+            if (kap4 < (int64_t)n_ks * TC_KS) {
+                const cf v0 = a[l], v1 = a[l + 1];
+                tc_store_a4(a_hi, a_lo, n_ks, rho, kap4, make_float4(v0.re, -v0.im, v1.re, -v1.im));
+                tc_store_a4(a_hi, a_lo, n_ks, rho + 1, kap4, make_float4(v0.im, v0.re, v1.im, v1.re));
+            }
+        }
+    }
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) lmax = fmaxf(lmax, __shfl_xor_sync(0xffffffffu, lmax, off));
     // NaN-safe: a NaN compares false and raises the bound to +inf
@@ -367,9 +385,11 @@ __global__ void __launch_bounds__(kSpL21Threads, 1)
 // The panel of columns [j0, j0+jb) (jb <= 128) over rows [j0, n): the
 // diagonal block factored with pivots among its own rows, then L21.
 // `inv_diag`: 128 complex64 of device scratch for the reciprocal pivots;
-// `perm` (128 int32) receives the block's rows in pivot order.
+// `perm` (128 int32) receives the block's rows in pivot order; with
+// `pack_a` set, L21 is also written as the packed A operand (hi / lo
+// planes) of the updates that follow.
 mw_status static_panel_c64(cf* A, int64_t lda, int64_t n, int64_t j0, int jb, int32_t* ipiv, int32_t* info,
-                           PanelWs* ws, cf* inv_diag, int32_t* perm, cudaStream_t st) {
+                           PanelWs* ws, cf* inv_diag, int32_t* perm, const TcPlanes* pack_a, cudaStream_t st) {
     MW_REQUIRE(jb >= 1 && jb <= kSpB, "static panel width %d outside 1..%d", jb, kSpB);
     static bool configured = false;
     const size_t smem = sizeof(cf) * ((size_t)kSpB * kSpUStride + kSpB + (size_t)2 * kSpGroups * 32 * kSpXStride);
@@ -390,7 +410,9 @@ mw_status static_panel_c64(cf* A, int64_t lda, int64_t n, int64_t j0, int jb, in
         if (rows > 0) {
             const int64_t per_cta = (int64_t)kSpGroups * 32;
             const unsigned grid = (unsigned)((rows + per_cta - 1) / per_cta);
-            sp_l21_kernel<<<grid, kSpL21Threads, smem, st>>>(A, lda, j0, jb, n, inv_diag, ws);
+            sp_l21_kernel<<<grid, kSpL21Threads, smem, st>>>(A, lda, j0, jb, n, inv_diag, ws,
+                                                             pack_a ? pack_a->a_hi : nullptr,
+                                                             pack_a ? pack_a->a_lo : nullptr);
             count_launch();
         }
     }

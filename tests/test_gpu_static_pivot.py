@@ -67,13 +67,14 @@ def test_static_pivots_solve_like_partial_pivoting(n, nrhs, cuda_device):
     assert rel_err(xp, want) < 1e-9
 
 
-def test_static_pivots_within_the_block(cuda_device):
+@pytest.mark.parametrize("n", [384, 300, 100, 38])
+def test_static_pivots_within_the_block(n, cuda_device):
     """Interchanges that stay inside the diagonal blocks are made: each
-    block's rows reversed, so that partial pivoting must swap within it."""
+    block's rows reversed, so that partial pivoting must swap within it
+    (in the 32-column panels of a full block and of a partial last one)."""
     rng = np.random.default_rng(7)
-    n = 384
     Z = _diag_heavy(n, rng)
-    perm = np.concatenate([np.arange(b + 127, b - 1, -1) for b in range(0, n, 128)])
+    perm = np.concatenate([np.arange(min(b + 128, n) - 1, b - 1, -1) for b in range(0, n, 128)])
     Z = Z[perm]
     B = rng.standard_normal((n, 3)) + 1j * rng.standard_normal((n, 3))
     x, _it, used = _zgesv_mixed(Z, B, cuda_device, 0)

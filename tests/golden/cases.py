@@ -201,3 +201,64 @@ BIG_CASES = {
     "array16x16": lambda: dipole_array(16, 16),
     "plate64_somm": lambda: wire_grid_plate(),
 }
+
+
+# Singular basis enrichment (t log t bases beside K >= enrichment_min_k
+# junctions; bspline.py use_singular_enrichment)
+def _fan():
+    """Fan dipole: two arms of different length leave each feed-side end,
+    a dominant-pair K=3 junction at each side of the feed gap."""
+    return [
+        np.array([[0.0, 0.0, 0.0], [0.0, 0.0, 0.4]]),
+        np.array([[0.0, 0.0, 0.4], [0.0, 5.1, 0.4]]),
+        np.array([[0.0, 0.0, 0.4], [0.0, 3.6, 1.2]]),
+        np.array([[0.0, 0.0, 0.0], [0.0, -5.1, 0.0]]),
+        np.array([[0.0, 0.0, 0.0], [0.0, -3.6, -0.8]]),
+    ]
+
+
+def _radials(z0=1.0):
+    base = np.array([0.0, 0.0, z0])
+    wires = [np.array([base, base + [0, 0, 5.0]])]
+    for ang in (0.0, 0.5 * np.pi, np.pi, 1.5 * np.pi):
+        wires.append(np.array([base, base + 4.8 * np.array([np.cos(ang), np.sin(ang), -0.15])]))
+    return wires
+
+
+_RADIAL_JUNCTION = [[(0, "start"), (1, "start"), (2, "start"), (3, "start"), (4, "start")]]
+_STAR_JUNCTION = [[(0, "end"), (1, "start"), (2, "start")]]
+
+ENRICH_CASES = {
+    "enr_star_raw": lambda: dict(wires=_star(), nsegs=6, degree=2, junctions=_STAR_JUNCTION, feeds=[(0, 2.5, 1.0)],
+                                 use_singular_enrichment=True),
+    "enr_star_stable": lambda: dict(wires=_star(), nsegs=6, degree=2, junctions=_STAR_JUNCTION,
+                                    feeds=[(0, 2.5, 1.0)], use_singular_enrichment=True,
+                                    enrichment_variant="stable"),
+    "enr_star_tikhonov": lambda: dict(wires=_star(), nsegs=6, degree=2, junctions=_STAR_JUNCTION,
+                                      feeds=[(0, 2.5, 1.0)], use_singular_enrichment=True,
+                                      enrichment_variant="tikhonov", tikhonov_lambda=0.05),
+    "enr_star_auto": lambda: dict(wires=_star(), nsegs=6, degree=2, junctions=_STAR_JUNCTION,
+                                  feeds=[(0, 2.5, 1.0)], use_singular_enrichment=True, enrichment_variant="auto"),
+    "enr_star_port": lambda: dict(wires=_star(), nsegs=6, degree=2, junctions=_STAR_JUNCTION,
+                                  feeds=[(0, 2.5, 1.0)], junction_ports=[0], use_singular_enrichment=True),
+    "enr_star_d1": lambda: dict(wires=_star(), nsegs=8, degree=1, junctions=_STAR_JUNCTION, feeds=[(0, 2.5, 1.0)],
+                                use_singular_enrichment=True),
+    "enr_fan_auto": lambda: dict(wires=_fan(), nsegs=9, degree=2,
+                                 junctions=[[(0, "end"), (1, "start"), (2, "start")],
+                                            [(0, "start"), (3, "start"), (4, "start")]],
+                                 feeds=[(0, 0.2, 1.0)], use_singular_enrichment=True, enrichment_variant="auto"),
+    "enr_fan_raw": lambda: dict(wires=_fan(), nsegs=9, degree=2,
+                                junctions=[[(0, "end"), (1, "start"), (2, "start")],
+                                           [(0, "start"), (3, "start"), (4, "start")]],
+                                feeds=[(0, 0.2, 1.0)], use_singular_enrichment=True),
+    "enr_node_gap_mink2": lambda: dict(
+        wires=[np.array([[0, 0, -5.0], [0, 0, 0.0]]), np.array([[0, 0, 0.0], [0, 0, 5.0]])], nsegs=10, degree=2,
+        junctions=[[(0, "end"), (1, "start")]], feeds=[], node_gaps=[(1, "start", 1.0)],
+        use_singular_enrichment=True, enrichment_min_k=2),
+    "enr_radials_pec": lambda: dict(wires=_radials(), nsegs=7, degree=2, junctions=_RADIAL_JUNCTION,
+                                    feeds=[(0, 0.4, 1.0)], ground_z=0.0, use_singular_enrichment=True),
+    "enr_radials_refl": lambda: dict(wires=_radials(), nsegs=7, degree=2, junctions=_RADIAL_JUNCTION,
+                                     feeds=[(0, 0.4, 1.0)], ground_z=0.0, ground_eps=(13.0, 0.005),
+                                     use_singular_enrichment=True, enrichment_variant="stable"),
+    "enr_radials_somm": lambda: dict(somm_ground_plane(), use_singular_enrichment=True),
+}

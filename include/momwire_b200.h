@@ -223,6 +223,41 @@ mw_status mw_fill_z_image(const mw_segments* seg, const mw_basis* basis,
                           float* Z32, int64_t ldz32, void* stream);
 
 /*
+ * Singular basis enrichment (bspline.py:3048-3076 specs): one basis per
+ * wire end at a junction of at least enrichment_min_k ends, on the segment
+ * beside the junction, shaped u log u - P(u) with u the normalised distance
+ * from the junction and P the polynomial proj[0..d] (zeros: the "raw"
+ * shape; the "stable" shape subtracts its bubble projection).
+ */
+typedef struct mw_enrich {
+    int32_t        n_enrich;
+    const int32_t* seg;      /* (n_enrich) segment of each basis (device)      */
+    const int32_t* origin;   /* (n_enrich) 0: junction at the segment's start,
+                                1: at its end (device)                         */
+    int32_t        n_qp;     /* Gauss nodes per axis (n_qp_sing)               */
+    const double*  t01;      /* (n_qp) nodes on [0, 1] (device)                */
+    const double*  w01;      /* (n_qp) weights on [0, 1] (device)              */
+    double         proj[4];  /* P's monomial coefficients, degree <= 3         */
+    double         radius;   /* the structure's (uniform) wire radius          */
+} mw_enrich;
+
+/*
+ * The enrichment blocks of the augmented system [[Z, Z_pe], [Z_ep, Z_ee]]:
+ * Z_pe into rows 0..n_basis-1 / columns n_basis.., Z_ep and Z_ee into rows
+ * n_basis.. of the column-major Z (ldz >= n_basis + n_enrich; the
+ * polynomial block is mw_fill_z's, written separately), and their complex64
+ * copy into Z32 when it is not NULL.  ground (NULL = free space): PEC,
+ * reflection-coefficient and Sommerfeld C2 image reactions are subtracted;
+ * the Sommerfeld remainder is the caller's (mw_somm_field_proj).  Replaces
+ * assemble_Z_enrich (_accelerators.cpp:2997) and
+ * _assemble_Z_enrich_image_numpy (bspline.py:3308-3521) as called by
+ * _enrichment_Z_assemble (bspline.py:3523-3693).
+ */
+mw_status mw_enrich_blocks(const mw_segments* seg, const mw_basis* basis, const mw_enrich* en,
+                           const mw_freq* freq, const mw_ground* ground, double* Z, int64_t ldz,
+                           float* Z32, int64_t ldz32, void* stream);
+
+/*
  * mw_fill_z for callers that cannot allocate device memory -- no
  * counterpart in the reference (its fills run on the host).  Some hosts
  * own every device allocation (a plugin given only its input and output

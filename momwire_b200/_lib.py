@@ -89,6 +89,19 @@ class Ground(C.Structure):
     ]
 
 
+class Enrich(C.Structure):
+    _fields_ = [
+        ("n_enrich", i32),
+        ("seg", vp),
+        ("origin", vp),
+        ("n_qp", i32),
+        ("t01", vp),
+        ("w01", vp),
+        ("proj", f64 * 4),
+        ("radius", f64),
+    ]
+
+
 class SommGrid(C.Structure):
     _fields_ = [
         ("n_region", i32),
@@ -124,6 +137,8 @@ _SIGS = {
     "mw_offedge_moments": (i32, [C.POINTER(Segments), C.POINTER(Segments), i32, i32, f64, i32, f64, vp, vp, vp, vp]),
     "mw_fill_z": (i32, [C.POINTER(Segments), C.POINTER(BasisT), vp, C.POINTER(Edges), C.POINTER(Freq), i32, vp, i64, vp, i64, vp]),
     "mw_fill_z_image": (i32, [C.POINTER(Segments), C.POINTER(BasisT), C.POINTER(Ground), C.POINTER(Freq), i32, vp, i64, vp, i64, vp]),
+    "mw_enrich_blocks": (i32, [C.POINTER(Segments), C.POINTER(BasisT), C.POINTER(Enrich), C.POINTER(Freq),
+                               C.POINTER(Ground), vp, i64, vp, i64, vp]),
     "mw_fill_z_noalloc": (i32, [C.POINTER(Segments), C.POINTER(BasisT), C.POINTER(Edges), C.POINTER(Freq), i32, i32, vp, i64, vp]),
     "mw_fill_z_noalloc_capacity": (sz, [i32]),
     "mw_cgemm_tc_workspace_size": (sz, [i64, i64, i64]),

@@ -234,7 +234,8 @@ SETTING_RULES = (
     (lambda k: k["degree"] > 2, NotImplementedError,
      lambda k: "degree > 2 needs scripts/derive_bspline_static_moments.py to be re-run with a larger MAX_D"),
     (lambda k: not k["wires"], ValueError, lambda k: "wires must be non-empty"),
-    (lambda k: k["use_singular_enrichment"], NotImplementedError, lambda k: k["enrichment_refusal"]),
+    (lambda k: k["use_singular_enrichment"] and k["enrichment_loading"], NotImplementedError,
+     lambda k: k["enrichment_loading_refusal"]),
     (lambda k: k["enrichment_variant"] not in _VARIANTS, ValueError,
      lambda k: f"enrichment_variant must be one of 'raw', 'stable', 'tikhonov', 'auto', got "
                f"{k['enrichment_variant']!r}"),
@@ -257,6 +258,8 @@ SETTING_RULES = (
     (lambda k: k["feed_model"] == "segment" and k["feed_smoothing_factor"] is not None, ValueError,
      lambda k: "feed_model='segment' and feed_smoothing_factor are mutually exclusive — both replace the point "
                "drive with a spread one"),
+    (lambda k: bool(k["extended_kernel"]) and k["use_singular_enrichment"], NotImplementedError,
+     lambda k: k["enrichment_ek_refusal"]),
 )
 
 

@@ -35,6 +35,7 @@ from . import _tables as T
 from . import _topology as topo
 from . import _validate as V
 from . import autotune
+from . import enrichment as EN
 from . import loading as wl
 from . import sommerfeld as somm
 from . import surrogate as sur
@@ -188,7 +189,19 @@ class _DeviceTables:
         )
 
 
-_ENRICHMENT_REFUSAL = "use_singular_enrichment is outside the B200 dense path"
+# the reference's refusals of enrichment combinations (bspline.py:308-330):
+# their texts are part of the interface consumers read
+_ENRICHMENT_WIRE_LOADING_REFUSAL = (
+    "use_singular_enrichment + distributed wire loading together not supported yet — the enrichment bases don't "
+    "carry the loading overlap term")
+_ENRICHMENT_EXTENDED_KERNEL_REFUSAL = (
+    "extended_kernel=True + use_singular_enrichment=True not supported yet — the enrichment DOFs bypass the moment "
+    "kernels entirely (they carry their own Φ_sing quadrature), they exist only at K >= 3 junctions where NEC's own "
+    "gating turns EK off, and the O(a²) tube expansion was never derived for the s^(-1/2) shapes "
+    "(stevenmburns/momwire#249 follow-up C)")
+_ENRICHMENT_PER_WIRE_RADIUS_REFUSAL = (
+    "use_singular_enrichment + mixed per-wire radii together not supported yet — the enrichment kernels take a "
+    "single radius (stevenmburns/momwire#147)")
 _CONTACT_REFUSAL = "ground contact is refused under ground_model='refl-coef' (use ground_model='sommerfeld')"
 
 
@@ -198,15 +211,17 @@ class BSplineSolver:
 
     Keyword arguments follow the reference constructor (``bspline.py:511-548``).
     Served: degree 1-2, reduced or extended thin-wire kernel, free space,
-    PEC image and reflection-coefficient ground, point/segment feeds,
-    junctions, junction ports and node gaps, per-wire radii.  Additional:
+    PEC image, reflection-coefficient and Sommerfeld grounds, point/segment
+    feeds, junctions, junction ports and node gaps, per-wire radii,
+    distributed wire loading, singular basis enrichment at junctions.
+    Additional:
 
     precision : "fp64" (default) or "mixed".
     device : CUDA device index or torch.device (default: current device).
     """
 
     # what the class serves, read by consumers before they build one
-    # (``bspline.py:495-509``; singular enrichment is not served here)
+    # (``bspline.py:495-509``)
     capabilities = Capabilities(
         grounds=frozenset({"pec", "refl-coef", "sommerfeld"}),
         wire_loading=True,
@@ -214,8 +229,13 @@ class BSplineSolver:
         junction_ports=True,
         node_gaps=True,
         per_wire_radius=True,
-        singular_enrichment=False,
-        refusals={"singular_enrichment": _ENRICHMENT_REFUSAL, "contact+refl-coef": _CONTACT_REFUSAL},
+        singular_enrichment=True,
+        refusals={
+            "wire_loading+singular_enrichment": _ENRICHMENT_WIRE_LOADING_REFUSAL,
+            "extended_kernel+singular_enrichment": _ENRICHMENT_EXTENDED_KERNEL_REFUSAL,
+            "per_wire_radius+singular_enrichment": _ENRICHMENT_PER_WIRE_RADIUS_REFUSAL,
+            "contact+refl-coef": _CONTACT_REFUSAL,
+        },
     )
 
     eps = 8.8541878188e-12
@@ -265,14 +285,19 @@ class BSplineSolver:
     ):
         self._cancel = cancel
         V.settings(dict(degree=degree, wires=wires, use_singular_enrichment=use_singular_enrichment,
-                        enrichment_refusal=_ENRICHMENT_REFUSAL, enrichment_variant=enrichment_variant,
+                        enrichment_loading=wire_conductivity is not None or insulation_radius is not None,
+                        enrichment_loading_refusal=_ENRICHMENT_WIRE_LOADING_REFUSAL,
+                        extended_kernel=extended_kernel, enrichment_ek_refusal=_ENRICHMENT_EXTENDED_KERNEL_REFUSAL,
+                        enrichment_variant=enrichment_variant,
                         precision=precision, sommerfeld_method=sommerfeld_method, ground_eps=ground_eps,
                         ground_z=ground_z, ground_phi_mode=ground_phi_mode, phi_modes=_lib.PHI_MODES,
                         ground_model=ground_model, swept_mem_mb=swept_mem_mb, feed_model=feed_model,
                         feed_smoothing_factor=feed_smoothing_factor))
-        # the enrichment settings are kept (their consumers read them);
-        # enrichment itself is not served
-        self.use_singular_enrichment = False
+        # singular basis enrichment at junctions of >= enrichment_min_k ends
+        self.use_singular_enrichment = bool(use_singular_enrichment)
+        # the junctions the "auto" variant enriched in the last solve (None:
+        # every qualifying junction), read back by currents_at_knots
+        self._auto_active_junctions = None
         self.n_qp_sing = int(n_qp_sing)
         self.enrichment_min_k = int(enrichment_min_k)
         self.enrichment_variant = enrichment_variant
@@ -322,6 +347,8 @@ class BSplineSolver:
                 where = ", ".join(f"wire {w} {kind}" for w, kind in touching)
                 raise NotImplementedError(f"{where} lies in the ground plane: {_CONTACT_REFUSAL}")
         self._radius_per_wire = V.radii(wire_radius, n_w)
+        if self.use_singular_enrichment and np.any(self._radius_per_wire != self._radius_per_wire[0]):
+            raise NotImplementedError(_ENRICHMENT_PER_WIRE_RADIUS_REFUSAL)
         # distributed series loading (bspline.py:715-728): None when off
         self._loading = wl.configure(n_w, self._radius_per_wire, wire_conductivity, insulation_radius,
                                      insulation_eps_r)
@@ -587,15 +614,18 @@ class BSplineSolver:
         g.phi_mode = _lib.PHI_MODES[self.ground_phi_mode]
         return g
 
-    def _alloc(self):
+    def _alloc(self, enrich=None):
         """Device buffers of one solve at this geometry (reused across calls
         by the benchmark): Z, the same-edge table, the port right-hand sides
         [B | kcl_con^T], the sparse B^T and kcl_con (CSR), LU workspace,
-        pivots, status and Y."""
+        pivots, status and Y.  With ``enrich`` (enrichment specs) the system
+        is the augmented one: the enrichment bases follow the polynomial
+        ones, with zero port and KCL entries (``bspline.py:4150-4175``)."""
         torch = _torch()
         dev = self._torch_device()
         dt = self._dev_tables()
-        n = self._basis().n
+        n_poly = self._basis().n
+        n = n_poly + (len(enrich) if enrich else 0)
         nm = self.degree + 1
         # port columns and KCL rows are a few nonzeros each: upload them in
         # coordinate form and scatter [B | kcl_con^T], B and kcl_con on the
@@ -622,6 +652,8 @@ class BSplineSolver:
                   rhs0.data_ptr(), st)
         buf = {
             "n": n,
+            "n_poly": n_poly,
+            "enrich": enrich or [],
             "n_p": n_p,
             "n_c": n_c,
             "Z": torch.empty((n, n), dtype=torch.complex128, device=dev),
@@ -684,6 +716,101 @@ class BSplineSolver:
                 self.last_sommerfeld = dict(info, method="grid")
         # distributed series wire loading, added once to the final Z
         self._loading_device(Z, buf.get("Z32"), [self.omega], stream)
+        if buf["enrich"]:
+            self._enrich_device(buf, stream)
+
+    # ----------------------------------------------------------- enrichment
+    def _enrich_device(self, buf, stream):
+        """The enrichment blocks of the augmented Z (and Z32): quadrature on
+        the device (``mw_enrich_blocks``), the Sommerfeld remainder reaction
+        from device field projections, and the "tikhonov" variant's
+        lambda * mean|diag Z_ee| on the enrichment diagonal
+        (``bspline.py:3523-3693``, ``4162-4164``)."""
+        torch = _torch()
+        dev = buf["Z"].device
+        sp = buf["enrich"]
+        n, n_poly, E = buf["n"], buf["n_poly"], len(sp)
+        dt = self._dev_tables()
+        t, w = EN.gauss01(self.n_qp_sing)
+        poly = EN.shape_polynomial(self.enrichment_variant, self.degree)
+        seg = torch.tensor([s.seg for s in sp], dtype=torch.int32, device=dev)
+        org = torch.tensor([s.origin for s in sp], dtype=torch.int32, device=dev)
+        t_d = torch.from_numpy(t).to(dev)
+        w_d = torch.from_numpy(w).to(dev)
+        en = _lib.Enrich()
+        en.n_enrich, en.seg, en.origin, en.n_qp = E, seg.data_ptr(), org.data_ptr(), int(self.n_qp_sing)
+        en.t01, en.w01 = t_d.data_ptr(), w_d.data_ptr()
+        for i in range(4):
+            en.proj[i] = float(poly[i]) if i < poly.size else 0.0
+        en.radius = float(self._radius_per_wire[0])
+        fr = _lib.Freq(float(self.k), float(self.omega), float(self.eps), float(self.mu))
+        g = self._ground_struct()
+        Z = buf["Z"]
+        Z32 = buf.get("Z32")
+        _lib.call("mw_enrich_blocks", C.byref(dt.seg), C.byref(dt.basis), C.byref(en), C.byref(fr),
+                  C.byref(g) if g is not None else None, Z.data_ptr(), n,
+                  Z32.data_ptr() if Z32 is not None else None, n, stream)
+        # column-major Z in a row-major (n, n) tensor: Z[row, col] is zt[col, row]
+        zt = Z.view(n, n)
+        if self._is_sommerfeld():
+            q_pe, q_ee = self._enrich_somm_remainder(sp, t, w, poly, stream)
+            zt[n_poly:, :n_poly] -= q_pe.T  # Z_pe (rows m, columns e)
+            zt[:n_poly, n_poly:] -= q_pe  # Z_ep = Z_pe^T by reciprocity
+            zt[n_poly:, n_poly:] -= q_ee.T
+        if self.enrichment_variant == "tikhonov":
+            d = torch.diagonal(zt[n_poly:, n_poly:])
+            scale = float(self.tikhonov_lambda) * float(d.abs().mean())
+            d += scale
+        if Z32 is not None and (self._is_sommerfeld() or self.enrichment_variant == "tikhonov"):
+            z32t = Z32.view(n, n)
+            z32t[n_poly:, :] = zt[n_poly:, :].to(torch.complex64)
+            z32t[:n_poly, n_poly:] = zt[:n_poly, n_poly:].to(torch.complex64)
+
+    def _enrich_somm_remainder(self, sp, t, w, poly, stream):
+        """(Q_pe (n_poly, E), Q_ee (E, E)): the Sommerfeld remainder field
+        between the enrichment bases' nodes (weight times shape) and the
+        polynomial bases' n_qp_sommerfeld nodes per segment (u^p moments
+        contracted with the basis polynomials), ``bspline.py:1919-2033``.
+        Field projections on the device (mw_somm_field_proj), contractions
+        as device GEMMs."""
+        torch = _torch()
+        dev = self._torch_device()
+        geom, basis = self._geometry(), self._basis()
+        grid = self._somm_grid(stream)
+        E, q_e = len(sp), t.size
+        pts_e, val_e = EN.shape_values(sp, geom, t, poly)
+        h_e = np.array([geom.h[s.seg] for s in sp])
+        wphi = torch.from_numpy((w[None, :] * h_e[:, None]) * val_e).to(dev).to(torch.complex128)  # (E, q_e)
+        obs_e = torch.from_numpy(np.ascontiguousarray(pts_e.reshape(-1, 3))).to(dev)
+        tan_e = torch.from_numpy(np.ascontiguousarray(np.repeat(geom.tangents[[s.seg for s in sp]], q_e, 0))).to(dev)
+        q = int(self.n_qp_sommerfeld)
+        tq, wq = EN.gauss01(q)
+        nodes = geom.seg_l[:, None, :] + tq[None, :, None] * (geom.seg_r - geom.seg_l)[:, None, :]
+        obs_p = torch.from_numpy(np.ascontiguousarray(nodes.reshape(-1, 3))).to(dev)
+        tan_p = torch.from_numpy(np.ascontiguousarray(np.repeat(geom.tangents, q, axis=0))).to(dev)
+        n_seg, d1 = geom.n, self.degree + 1
+
+        def proj(o, to, s_, ts):
+            out = torch.empty((o.shape[0], s_.shape[0]), dtype=torch.complex128, device=dev)
+            _lib.call("mw_somm_field_proj", o.shape[0], o.data_ptr(), to.data_ptr(), s_.shape[0], s_.data_ptr(),
+                      ts.data_ptr(), float(self.ground_z), float(self.k), C.byref(grid), out.data_ptr(), stream)
+            return out
+
+        f_ee = proj(obs_e, tan_e, obs_e, tan_e).view(E, q_e, E, q_e)
+        q_ee = torch.einsum("eq,eqfr,fr->ef", wphi, f_ee, wphi)
+        f_pe = proj(obs_p, tan_p, obs_e, tan_e).view(n_seg, q, E, q_e)
+        field = torch.einsum("iqer,er->iqe", f_pe, wphi)  # (n_seg, q, E)
+        u = geom.h[:, None] * tq[None, :]
+        wm = (wq[None, :] * geom.h[:, None])[None] * u[None] ** np.arange(d1)[:, None, None]
+        jf = torch.einsum("piq,iqe->pie", torch.from_numpy(wm).to(dev).to(torch.complex128), field)  # (d1, n_seg, E)
+        supp = torch.from_numpy(basis.supp.astype(np.int64)).to(dev)
+        polys = torch.from_numpy(basis.polys).to(dev).to(torch.complex128)
+        q_pe = torch.zeros((basis.n, E), dtype=torch.complex128, device=dev)
+        for a in range(d1):
+            sm = supp[:, a].clamp(min=0)
+            live = (supp[:, a] >= 0).to(torch.complex128)[:, None]
+            q_pe += live * torch.einsum("mp,pme->me", polys[:, a, :], jf[:, sm, :])
+        return q_pe, q_ee
 
     # ------------------------------------------------------------ loading
     def _loading_tables(self) -> wl.LoadingGram:
@@ -910,11 +1037,42 @@ class BSplineSolver:
         (``bspline.py:4053-4179``).  ``same_edge_prep`` (the reference's
         precomputed same-edge moments for sweeps) is accepted for signature
         compatibility and unused: the device builds its same-edge table at
-        each call for a fraction of a millisecond."""
+        each call for a fraction of a millisecond.
+
+        With ``use_singular_enrichment`` the system is augmented by the
+        enrichment bases (coefficients after the polynomial ones); the
+        "auto" variant first solves without them and enriches only the
+        junctions whose tap ratio exceeds ``auto_tap_ratio_threshold`` under
+        any port's drive (``bspline.py:4121-4175``)."""
         self._checkpoint()
+        self._auto_active_junctions = None
+        enrich = None
+        if self.use_singular_enrichment:
+            active = None
+            if self.enrichment_variant == "auto":
+                first = self._solve_once(None)
+                act = set()
+                for j in range(first.coeffs.shape[1]):
+                    cur = self.currents_at_knots(first.coeffs[:, j])
+                    act |= {i for i, r in enumerate(EN.tap_ratios(self.junctions, cur, self.enrichment_min_k))
+                            if r is not None and r > self.auto_tap_ratio_threshold}
+                active = sorted(act)
+                self._auto_active_junctions = active
+                if not active:
+                    return first
+            enrich = EN.specs(self.junctions, self._geometry(), self.enrichment_min_k, active) or None
+        return self._solve_once(enrich)
+
+    def _enrichment_specs_now(self):
+        """The enrichment bases of the last solve's system (empty when off)."""
+        if not self.use_singular_enrichment:
+            return []
+        return EN.specs(self.junctions, self._geometry(), self.enrichment_min_k, self._auto_active_junctions)
+
+    def _solve_once(self, enrich) -> PortSolution:
         torch = _torch()
         geom, basis = self._geometry(), self._basis()
-        buf = self._alloc()
+        buf = self._alloc(enrich)
         st = torch.cuda.current_stream(buf["Z"].device).cuda_stream
         X = self._device_solve(buf, st)
         n_p = buf["n_p"]
@@ -957,8 +1115,9 @@ class BSplineSolver:
         volts = np.concatenate([np.array([v for _w, _a, v in self.feeds], dtype=np.complex128), port_V, gap_V])
         coeffs = sol.coeffs @ volts
         pr, pc, pv, n_p = self._port_entries()
-        Bs = scipy.sparse.csr_matrix((pv, (pr, pc)), shape=(self._basis().n, n_p))
-        currents = Bs.T @ coeffs
+        nb = self._basis().n
+        Bs = scipy.sparse.csr_matrix((pv, (pr, pc)), shape=(nb, n_p))
+        currents = Bs.T @ coeffs[:nb]  # port entries sit on the polynomial bases
         z = volts / currents
         return (z[0] if len(volts) == 1 else z), coeffs
 
@@ -1007,14 +1166,14 @@ class BSplineSolver:
         (finite grounds carry per-k weight tables), at most SWEPT_MAX_KCL
         KCL rows left after the port split, order within the batched
         panel's limit."""
-        if self.precision != "mixed" or self.ground_eps is not None:
+        if self.precision != "mixed" or self.ground_eps is not None or self.use_singular_enrichment:
             return False
         return self._kcl_rows_left() <= self.SWEPT_MAX_KCL and self._basis_count() <= 1600
 
     def _swept_fp64_batched_available(self):
         """Batched-fill FP64 route: complex128, free space or PEC image, at
         most SWEPT_MAX_KCL KCL rows."""
-        return (self.precision == "fp64" and self.ground_eps is None
+        return (self.precision == "fp64" and self.ground_eps is None and not self.use_singular_enrichment
                 and self._kcl_rows_left() <= self.SWEPT_MAX_KCL)
 
     def _sweep_rhs(self):
@@ -1232,6 +1391,14 @@ class BSplineSolver:
             for j, _k, _jn, _e, mg in basis.kept[w]:
                 c[j] = coeffs[mg]
             out.append(T.basis_values(knots, d, s) @ c if s.size else np.zeros(0, dtype=np.complex128))
+        sp = self._enrichment_specs_now()
+        if sp and s_array is not None:
+            # the enrichment shapes vanish at the knots, so only arcs between
+            # knots carry them (bspline.py:4649-4683)
+            s_eval = [np.clip(np.asarray(s_array[w], dtype=np.float64), basis.knots[w][0], basis.knots[w][-1])
+                      for w in range(len(self.wires_polylines))]
+            out = EN.add_between_knots(out, coeffs, sp, geom, s_eval,
+                                       EN.shape_polynomial(self.enrichment_variant, d), basis.n)
         return out
 
     def current_slopes(self, coeffs, s_array=None):
@@ -1241,7 +1408,14 @@ class BSplineSolver:
         ``currents_at_knots``.  The derivative of a degree-d B-spline sum is
         the degree-(d-1) sum on the inner knots with coefficients
         d (c_{j+1} - c_j) / (t_{j+d+1} - t_{j+1}); at degree 1 it is
-        piecewise constant and a knot takes its right-hand span."""
+        piecewise constant and a knot takes its right-hand span.  Refused
+        under singular enrichment, whose shapes' slope diverges at the
+        junction knot (the reference's refusal and text)."""
+        if self.use_singular_enrichment:
+            raise NotImplementedError(
+                "current_slopes does not serve use_singular_enrichment=True: the enrichment shape's slope is "
+                "singular at the junction knot, so dropping it would be a silent error rather than an "
+                "approximation")
         coeffs = np.asarray(coeffs)
         geom, basis = self._geometry(), self._basis()
         d = self.degree

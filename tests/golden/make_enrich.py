@@ -8,7 +8,8 @@ added to Z (``_enrichment_Z_assemble``, bspline.py:3523-3693, ground
 reaction included), the polynomial Z, the port solution (Y, all
 coefficients, the enrichment block among them), the junctions the "auto"
 variant activated, the drive-point impedance of ``compute_impedance`` and
-the knot currents of the first port column (and, over a Sommerfeld
+the first port column's currents at the knots and at the segment
+midpoints (and, over a Sommerfeld
 ground, the grid master the solve interpolated).
 
 Run where the reference source tree is checked out (its root given by
@@ -64,6 +65,9 @@ def record(momwire, kw):
         for key in ("Z_pe", "Z_ep", "Z_ee"):
             out[key] = np.asarray(blocks[key]) if blocks is not None else np.zeros((0, 0), np.complex128)
     out["currents0"] = np.concatenate(s.currents_at_knots(np.asarray(sol.coeffs)[:, 0]))
+    # between the knots the enrichment shapes add to the current
+    mids = [0.5 * (pw["arc_at_knot"][1:] + pw["arc_at_knot"][:-1]) for pw in geom["per_wire"]]
+    out["currents_mid"] = np.concatenate(s.currents_at_knots(np.asarray(sol.coeffs)[:, 0], mids))
     if kw.get("ground_model") == "sommerfeld":
         out.update(somm_master(momwire, s, geom))
     zin = s.compute_impedance()

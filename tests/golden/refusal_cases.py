@@ -31,6 +31,17 @@ REFUSALS = {
     "enrichment_settings_with_enrichment_off": lambda: dict(wires=_D, n_qp_sing=16, enrichment_min_k=4,
                                                             enrichment_variant="stable", tikhonov_lambda=1e-2,
                                                             auto_tap_ratio_threshold=0.5),
+    # singular enrichment: served alone, refused in three combinations
+    "enrichment_on": lambda: dict(wires=_V, junctions=[[(0, "start"), (1, "start")]], use_singular_enrichment=True,
+                                  enrichment_min_k=2),
+    "enrichment_with_loading": lambda: dict(wires=_D, use_singular_enrichment=True, wire_conductivity=5.8e7),
+    "enrichment_with_insulation": lambda: dict(wires=_D, use_singular_enrichment=True, insulation_radius=1e-3,
+                                               insulation_eps_r=2.0),
+    "enrichment_with_extended_kernel": lambda: dict(wires=_D, use_singular_enrichment=True, extended_kernel=True),
+    "enrichment_with_per_wire_radius": lambda: dict(wires=_Y, use_singular_enrichment=True,
+                                                    wire_radius=[1e-3, 2e-3]),
+    "enrichment_with_equal_per_wire_radius": lambda: dict(wires=_Y, use_singular_enrichment=True,
+                                                          wire_radius=[1e-3, 1e-3]),
     # the port and connection keywords, entry by entry
     "feeds_empty": lambda: dict(wires=_D, feeds=[]),
     "feeds_empty_with_junction_port": lambda: dict(wires=_V, junctions=[[(0, "start"), (1, "start")]], feeds=[],

@@ -56,10 +56,13 @@ def test_capabilities_declaration():
     cap = momwire_b200.BSplineSolver.capabilities
     assert cap.grounds == frozenset({"pec", "refl-coef", "sommerfeld"})
     assert cap.wire_loading and cap.extended_kernel and cap.junction_ports and cap.node_gaps
-    assert cap.per_wire_radius and not cap.singular_enrichment
+    assert cap.per_wire_radius and cap.singular_enrichment
     assert cap.refusal("sommerfeld", "junction_ports") is None
     assert cap.refusal("wire_loading") is None
-    assert "outside the B200 dense path" in cap.refusal("singular_enrichment")
+    assert cap.refusal("singular_enrichment") is None
+    assert "distributed wire loading" in cap.refusal("wire_loading", "singular_enrichment")
+    assert "extended_kernel=True" in cap.refusal("extended_kernel", "singular_enrichment")
+    assert "per-wire radii" in cap.refusal("per_wire_radius", "singular_enrichment")
     assert "ground contact is refused" in cap.refusal("refl-coef", "contact")
     assert cap.refusal("bogus_axis") is None  # a condition token alone is served
 

@@ -37,10 +37,13 @@ sys.path.insert(0, str(ROOT))
 METRIC = "sweep pts/s & fill+LU time, mixed+batched vs FP64 GPU at |ΔZin|/|Zin|≤1e-6"
 UNIT = "pts/s"
 WORKLOAD = "dipole_array_16x16_300MHz_41seg_d2_256port"
-# ncu dram__bytes_read.sum + dram__bytes_write.sum averaged over the 564
-# tensor-core launches of one 16x16 mixed step (42.25 GB read + 19.50 GB
-# written)
-TC_TRAFFIC_PER_LAUNCH = 109.5e6
+# DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) per
+# algorithmic byte of the tensor-core update (C read and written plus the
+# hi / lo operand planes), measured on three consecutive launches of the
+# 12x12 array's factorisation (a next-block, a trailing and a right-hand-side
+# update of one panel: 158.8 MB against 219.3 MB); the bench line scales it
+# by the step's algorithmic bytes per launch
+TC_TRAFFIC_PER_ALG_BYTE = 158.8 / 219.3
 
 
 def parse():
@@ -369,13 +372,15 @@ def run_b200(args, kw):
             measured = "bf16_tflops" in peaks
             bf16 = float(peaks.get("bf16_tflops", 1590.0))
             peak = bf16 / 2.0
-            # DRAM bytes per launch of this kernel on this workload, from an
-            # ncu capture of every tensor-core launch of one step (ncu cannot
-            # run inside the timed bench)
-            traffic = TC_TRAFFIC_PER_LAUNCH if (args.nx == 16 and args.precision == "mixed") else None
+            # DRAM bytes per launch: the measured DRAM-to-algorithmic ratio
+            # (ncu cannot run inside the timed bench) times this step's
+            # algorithmic bytes per launch
+            traffic = TC_TRAFFIC_PER_ALG_BYTE * by / cnt if cnt else None
             roof = {"kernel": name, "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                     "frac": achieved / peak, "tensor_pipe_frac": 3.0 * achieved / peak, "traffic": traffic,
-                    "traffic_unit": "bytes per launch (dram read + write, ncu)",
+                    "traffic_unit": "bytes per launch (dram read + write: ncu ratio to algorithmic bytes on "
+                                    "three 12x12 launches, times this step's algorithmic bytes per launch)",
+                    "algorithmic_bytes_per_launch": by / cnt if cnt else None,
                     "launches_per_step": cnt / args.steps, "avg_launch_ms": tms / cnt,
                     "peak_source": ("of measured: MEASURED_PEAKS bf16_tflops / 2" if measured else
                                     "of fallback: 1590 TFLOP/s bf16 / 2 (MEASURED_PEAKS.json absent)")

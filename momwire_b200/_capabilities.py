@@ -3,7 +3,7 @@ read from a solver class (``_capabilities.py`` of the reference,
 ``bspline.py:495-509``): one named tuple of axes plus the refusal text for
 each unserved cell or "a+b" combination.  The field names and the
 ``refusal`` lookup are the reference's interface; the values are this
-package's own (singular enrichment is not served here)."""
+package's own."""
 
 from __future__ import annotations
 

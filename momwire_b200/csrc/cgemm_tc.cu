@@ -365,7 +365,10 @@ mw_status cgemm_tc_update_batched(int64_t m, int64_t n, int64_t k, int batch, co
     const int cap = (max_ctas > 0 && max_ctas < sms) ? max_ctas : sms;  // CTAs (= SMs) this update may hold
     const int grid = tiles < cap ? (int)tiles : cap;
     {
-        ProfileScope ps(PC_CGEMM_TC, st, 8.0 * (double)m * n * k * batch, 8.0 * 2.0 * (double)m * n * batch);
+        // bytes: C read and written (complex64) plus the hi / lo operand
+        // planes (Ahat 2m x 2k, Breal 2k x n, fp32 each)
+        ProfileScope ps(PC_CGEMM_TC, st, 8.0 * (double)m * n * k * batch,
+                        (16.0 * (double)m * n + 32.0 * (double)m * k + 16.0 * (double)k * n) * batch);
         cgemm_tc_kernel<<<grid, TC_THREADS, TC_STAGES * TC_STAGE_BYTES, st>>>(P);
     }
     MW_CHECK_CUDA(cudaGetLastError());
@@ -407,7 +410,8 @@ mw_status cgemm_tc_prepacked(int64_t m, int64_t n, int64_t k, const TcPlanes& pl
     const int cap = (max_ctas > 0 && max_ctas < sms) ? max_ctas : sms;
     const int grid = tiles < cap ? (int)tiles : cap;
     {
-        ProfileScope ps(PC_CGEMM_TC, st, 8.0 * (double)m * n * k, 8.0 * 2.0 * (double)m * n);
+        ProfileScope ps(PC_CGEMM_TC, st, 8.0 * (double)m * n * k,
+                        16.0 * (double)m * n + 32.0 * (double)m * k + 16.0 * (double)k * n);
         cgemm_tc_kernel<<<grid, TC_THREADS, TC_STAGES * TC_STAGE_BYTES, st>>>(P);
     }
     MW_CHECK_CUDA(cudaGetLastError());

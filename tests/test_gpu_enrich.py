@@ -59,7 +59,8 @@ def test_enriched_solve_matches_reference(name, cuda_device):
     mids = [0.5 * (a[1:] + a[:-1]) for a in s._geometry().wire_arc]
     assert rel_err(np.concatenate(s.currents_at_knots(sol.coeffs[:, 0], mids)), g["currents_mid"]) < 1e-9
     z, _c = s.compute_impedance()
-    assert np.max(np.abs(np.atleast_1d(z) - g["zin"]) / np.abs(g["zin"])) < 1e-9
+    # (an undriven junction port reads 0 / its current: zero in both)
+    assert rel_err(np.atleast_1d(z), g["zin"]) < 1e-9
 
 
 @pytest.mark.parametrize("name", ["enr_star_raw", "enr_fan_raw", "enr_radials_pec", "enr_radials_somm"])

@@ -49,15 +49,83 @@ constexpr int kSpLD = kSpB + 2;  // column stride of the staged block (complex; 
 constexpr int kSpPW = 32;        // panel width inside the block
 constexpr size_t kSpDiagSmem = sizeof(cf) * (size_t)kSpB * kSpLD;
 
-// Factor A[j0 .. j0+jb) x [j0 .. j0+jb) in place with partial pivoting among
-// these rows: a blocked LU of the block staged in shared memory (column
-// major).  Each 32-column panel is factored in registers -- thread (r, s)
-// holds row r's panel columns 8s .. 8s+7, every thread takes part in every
-// column -- with rows interchanged physically (registers for the panel,
-// shared memory for the other columns); then the panel's U rows of the
-// later columns (U12 = L11^-1 A12, one thread per column) and the update of
-// the trailing block (A22 -= L21 U12, 4 x 2 register tiles) follow.  Two
-// barriers per column, a few per panel.
+// The later columns of a factored 32-column panel (columns c0 .. c0+31 of
+// the staged block): U12 = L11^-1 A12 on the panel's rows, one thread per
+// column, then A22 -= L21 U12 over rows and columns c0+32 .. jb-1 in 4 x 2
+// register tiles.  All threads of the block take part.
+__device__ __forceinline__ void sp_trailing(cf* S, int c0, int jb, int tid) {
+    const int t0 = c0 + kSpPW;  // first trailing column (and row)
+    const int nt = jb - t0;
+    if (nt > 0) {
+        // U12 = L11^-1 A12 on the panel's rows, one thread per column
+        if (tid < nt) {
+            cf* col = S + (t0 + tid) * kSpLD + c0;
+            cf x[kSpPW];
+#pragma unroll
+            for (int i = 0; i < kSpPW; ++i) x[i] = col[i];
+#pragma unroll
+            for (int i = 1; i < kSpPW; ++i) {
+                cf t = x[i];
+#pragma unroll
+                for (int jj = 0; jj < i; ++jj) t = t - S[(c0 + jj) * kSpLD + c0 + i] * x[jj];
+                x[i] = t;
+            }
+#pragma unroll
+            for (int i = 0; i < kSpPW; ++i) col[i] = x[i];
+        }
+        __syncthreads();
+        // A22 -= L21 U12 over rows and columns t0 .. jb-1, 4 x 2 tiles
+        const int ntr = (nt + 3) / 4, ntc = (nt + 1) / 2;
+        for (int tile = tid; tile < ntr * ntc; tile += kSpDiagThreads) {
+            const int i0 = t0 + 4 * (tile % ntr), jc = t0 + 2 * (tile / ntr);
+            cf acc[4][2];
+#pragma unroll
+            for (int b2 = 0; b2 < 2; ++b2)
+#pragma unroll
+                for (int a4 = 0; a4 < 4; ++a4) acc[a4][b2] = S[(jc + b2) * kSpLD + i0 + a4];
+#pragma unroll 4
+            for (int jj = 0; jj < kSpPW; ++jj) {
+                const cf* lcol = S + (c0 + jj) * kSpLD + i0;
+                const float4 l01 = *reinterpret_cast<const float4*>(lcol);
+                const float4 l23 = *reinterpret_cast<const float4*>(lcol + 2);
+                const cf l[4] = {cf{l01.x, l01.y}, cf{l01.z, l01.w}, cf{l23.x, l23.y}, cf{l23.z, l23.w}};
+                const cf u0 = S[jc * kSpLD + c0 + jj], u1 = S[(jc + 1) * kSpLD + c0 + jj];
+#pragma unroll
+                for (int a4 = 0; a4 < 4; ++a4) {
+                    acc[a4][0] = acc[a4][0] - l[a4] * u0;
+                    acc[a4][1] = acc[a4][1] - l[a4] * u1;
+                }
+            }
+#pragma unroll
+            for (int b2 = 0; b2 < 2; ++b2)
+#pragma unroll
+                for (int a4 = 0; a4 < 4; ++a4) S[(jc + b2) * kSpLD + i0 + a4] = acc[a4][b2];
+        }
+        __syncthreads();
+    }
+}
+
+// Factor A[j0 .. j0+jb) x [j0 .. j0+jb) in place, pivots among these rows
+// only: a blocked LU of the block staged in shared memory (column major),
+// 32 columns at a time.
+//   first   without interchanges: warps 0-3 hold the panel's rows in
+//           registers (thread r = row r); per column the pivot row, whose
+//           values are final, is published in shared memory, one 128-thread
+//           named barrier, then every row below takes its multiplier and
+//           updates its panel columns.  Kept when every pivot is nonzero and
+//           every |l| (|re| + |im|) stays within kSpNoPivotBound -- on the
+//           strongly diagonal Galerkin blocks partial pivoting would keep
+//           the diagonal anyway, and the factors are then the same.
+//   else    the block is staged again and factored with partial pivoting
+//           among its rows: thread (r, s) holds row r's panel columns
+//           8s .. 8s+7, every thread takes part in every column, rows are
+//           interchanged physically (registers for the panel, shared memory
+//           for the other columns); two block barriers per column.
+// Each panel is followed by its U12 and A22 updates (sp_trailing).
+constexpr float kSpNoPivotBound = 2.0f;
+
+__device__ __forceinline__ void sp_bar_panel() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+
 __global__ void __launch_bounds__(kSpDiagThreads, 1)
     sp_diag_kernel(cf* __restrict__ A, int64_t lda, int64_t j0, int jb, int32_t* __restrict__ ipiv,
                    int32_t* __restrict__ info, cf* __restrict__ inv_diag, int32_t* __restrict__ perm, PanelWs* ws) {
@@ -65,9 +133,11 @@ __global__ void __launch_bounds__(kSpDiagThreads, 1)
     cf* S = reinterpret_cast<cf*>(sp_diag_smem);  // S[col * kSpLD + row]
     __shared__ cf s_col[2][kSpB];                 // column c of every row (by column parity)
     __shared__ unsigned long long s_key[2][4];
-    __shared__ cf s_u[2][kSpPW];                  // the pivot row's panel values
+    __shared__ __align__(16) cf s_u[2][kSpPW];    // the pivot row's panel values
     __shared__ cf s_rc[2][kSpPW];                 // row c's panel values before the interchange
     __shared__ int s_row_at[kSpB];                // original row at each position
+    __shared__ cf s_inv[kSpB];
+    __shared__ int s_bad;
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     for (int base = 0; base < kSpB * kSpB; base += 8 * kSpDiagThreads) {
@@ -84,151 +154,178 @@ __global__ void __launch_bounds__(kSpDiagThreads, 1)
             S[(idx / kSpB) * kSpLD + idx % kSpB] = t[u];
         }
     }
-    if (tid < kSpB) s_row_at[tid] = tid;
+    if (tid == 0) s_bad = 0;
     __syncthreads();
-    const int r = tid & (kSpB - 1);
-    const int sg = tid >> 7;  // panel column group: columns 8 sg .. 8 sg + 7 of the panel
-    const int wig = (tid >> 5) & 3;
+    // ---- without interchanges
     for (int c0 = 0; c0 < jb; c0 += kSpPW) {
         const int nck = (jb - c0) < kSpPW ? (jb - c0) : kSpPW;
-        cf pr[8];
+        if (tid < kSpB) {
+            const int r = tid;
+            cf a[kSpPW];
 #pragma unroll
-        for (int q = 0; q < 8; ++q) pr[q] = S[(c0 + 8 * sg + q) * kSpLD + r];
-#pragma unroll 1
-        for (int cc = 0; cc < nck; ++cc) {
-            const int c = c0 + cc, scol = cc >> 3, qc = cc & 7, par = cc & 1;
-            if (sg == scol) {
-                cf v = pr[0];
+            for (int q = 0; q < kSpPW; ++q) a[q] = S[(c0 + q) * kSpLD + r];
+            float lmax = 0.0f;
+            bool bad = false;
 #pragma unroll
-                for (int q = 1; q < 8; ++q)
-                    if (q == qc) v = pr[q];
-                s_col[par][r] = v;
-                // largest |re| + |im| among rows c .. jb-1, then the smallest
-                // row (LAPACK's icamax); the low bits carry the row
-                unsigned long long key = 0;
-                if (r >= c && r < jb)
-                    key = ((unsigned long long)__float_as_uint(cabs1f(v)) << 32) |
-                          ((unsigned long long)(0xFFFFu - (unsigned int)r) << 16) | (unsigned long long)r;
+            for (int cc = 0; cc < kSpPW; ++cc) {
+                if (cc < nck) {
+                    const int c = c0 + cc, par = cc & 1;
+                    if (r == c) {
+                        // row c is final: its values from column cc on
 #pragma unroll
-                for (int off = 16; off > 0; off >>= 1) {
-                    const unsigned long long o = __shfl_xor_sync(0xffffffffu, key, off);
-                    key = o > key ? o : key;
-                }
-                if (lane == 0) s_key[par][wig] = key;
-            }
-            __syncthreads();
-            unsigned long long best = s_key[par][0];
+                        for (int q = cc & ~1; q < kSpPW; q += 2)
+                            *reinterpret_cast<float4*>(&s_u[par][q]) =
+                                make_float4(a[q].re, a[q].im, a[q + 1].re, a[q + 1].im);
+                    }
+                    sp_bar_panel();
+                    const cf piv = s_u[par][cc];
+                    const float pa = cabs1f(piv);
+                    bad = bad || !(pa > 0.0f);
+                    const cf inv = pa > 0.0f ? crcp_sp(piv) : cone<cf>();
+                    if (r == c) s_inv[c] = inv;
+                    if (r > c && r < jb) {
+                        const cf l = a[cc] * inv;
+                        a[cc] = l;
+                        lmax = fmaxf(lmax, cabs1f(l));
 #pragma unroll
-            for (int w = 1; w < 4; ++w) best = s_key[par][w] > best ? s_key[par][w] : best;
-            const int p = (int)(best & 0xFFFFull);
-            const bool zero = (best >> 32) == 0ull;
-            const cf inv = zero ? cone<cf>() : crcp_sp(s_col[par][p]);
-            if (r == p) {
-#pragma unroll
-                for (int q = 0; q < 8; ++q) s_u[par][8 * sg + q] = pr[q];
-            }
-            if (r == c) {
-#pragma unroll
-                for (int q = 0; q < 8; ++q) s_rc[par][8 * sg + q] = pr[q];
-            }
-            // the interchange in the columns outside the panel, one column
-            // per thread
-            if (p != c && tid < kSpB && (tid < c0 || tid >= c0 + kSpPW)) {
-                cf* col = S + tid * kSpLD;
-                const cf t0 = col[c];
-                col[c] = col[p];
-                col[p] = t0;
-            }
-            if (tid == 0) {
-                ipiv[j0 + c] = (int32_t)(j0 + p + 1);
-                if (zero) {
-                    if (info[0] == 0) info[0] = (int32_t)(j0 + c + 1);
-                    atomicExch(&ws->lmax_bits, 0x7f800000u);  // +inf: the block is singular
-                }
-                inv_diag[c] = inv;
-                const int t0 = s_row_at[c];
-                s_row_at[c] = s_row_at[p];
-                s_row_at[p] = t0;
-            }
-            __syncthreads();  // s_u, s_rc complete
-            if (r == c) {
-#pragma unroll
-                for (int q = 0; q < 8; ++q) pr[q] = s_u[par][8 * sg + q];
-            } else if (r == p) {
-#pragma unroll
-                for (int q = 0; q < 8; ++q) pr[q] = s_rc[par][8 * sg + q];
-            }
-            if (r > c && r < jb && !zero) {
-                // row p now holds row c's old values
-                const cf l = (r == p ? s_col[par][c] : s_col[par][r]) * inv;
-#pragma unroll
-                for (int q = 0; q < 8; ++q) {
-                    const int pc = 8 * sg + q;
-                    if (pc == cc) pr[q] = l;
-                    else if (pc > cc) pr[q] = pr[q] - l * s_u[par][pc];
-                }
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < 8; ++q) S[(c0 + 8 * sg + q) * kSpLD + r] = pr[q];
-        __syncthreads();
-        const int t0 = c0 + kSpPW;  // first trailing column (and row)
-        const int nt = jb - t0;
-        if (nt > 0) {
-            // U12 = L11^-1 A12 on the panel's rows, one thread per column
-            if (tid < nt) {
-                cf* col = S + (t0 + tid) * kSpLD + c0;
-                cf x[kSpPW];
-#pragma unroll
-                for (int i = 0; i < kSpPW; ++i) x[i] = col[i];
-#pragma unroll
-                for (int i = 1; i < kSpPW; ++i) {
-                    cf t = x[i];
-#pragma unroll
-                    for (int jj = 0; jj < i; ++jj) t = t - S[(c0 + jj) * kSpLD + c0 + i] * x[jj];
-                    x[i] = t;
-                }
-#pragma unroll
-                for (int i = 0; i < kSpPW; ++i) col[i] = x[i];
-            }
-            __syncthreads();
-            // A22 -= L21 U12 over rows and columns t0 .. jb-1, 4 x 2 tiles
-            const int ntr = (nt + 3) / 4, ntc = (nt + 1) / 2;
-            for (int tile = tid; tile < ntr * ntc; tile += kSpDiagThreads) {
-                const int i0 = t0 + 4 * (tile % ntr), jc = t0 + 2 * (tile / ntr);
-                cf acc[4][2];
-#pragma unroll
-                for (int b2 = 0; b2 < 2; ++b2)
-#pragma unroll
-                    for (int a4 = 0; a4 < 4; ++a4) acc[a4][b2] = S[(jc + b2) * kSpLD + i0 + a4];
-#pragma unroll 4
-                for (int jj = 0; jj < kSpPW; ++jj) {
-                    const cf* lcol = S + (c0 + jj) * kSpLD + i0;
-                    const float4 l01 = *reinterpret_cast<const float4*>(lcol);
-                    const float4 l23 = *reinterpret_cast<const float4*>(lcol + 2);
-                    const cf l[4] = {cf{l01.x, l01.y}, cf{l01.z, l01.w}, cf{l23.x, l23.y}, cf{l23.z, l23.w}};
-                    const cf u0 = S[jc * kSpLD + c0 + jj], u1 = S[(jc + 1) * kSpLD + c0 + jj];
-#pragma unroll
-                    for (int a4 = 0; a4 < 4; ++a4) {
-                        acc[a4][0] = acc[a4][0] - l[a4] * u0;
-                        acc[a4][1] = acc[a4][1] - l[a4] * u1;
+                        for (int q = cc + 1; q < kSpPW; ++q) a[q] = a[q] - l * s_u[par][q];
                     }
                 }
-#pragma unroll
-                for (int b2 = 0; b2 < 2; ++b2)
-#pragma unroll
-                    for (int a4 = 0; a4 < 4; ++a4) S[(jc + b2) * kSpLD + i0 + a4] = acc[a4][b2];
             }
-            __syncthreads();
+#pragma unroll
+            for (int q = 0; q < kSpPW; ++q) S[(c0 + q) * kSpLD + r] = a[q];
+            // NaN-safe: a NaN multiplier fails the comparison
+            if (bad || !(lmax <= kSpNoPivotBound)) atomicOr(&s_bad, 1);
         }
+        __syncthreads();
+        if (s_bad) break;
+        sp_trailing(S, c0, jb, tid);
+        __syncthreads();
     }
+    if (!s_bad) {
+        for (int c = tid; c < jb; c += kSpDiagThreads) {
+            ipiv[j0 + c] = (int32_t)(j0 + c + 1);
+            inv_diag[c] = s_inv[c];
+            perm[c] = c;
+        }
+    } else {
+        // ---- partial pivoting among the block's rows, from the block as
+        // it came
+        __syncthreads();
+        for (int base = 0; base < kSpB * kSpB; base += 8 * kSpDiagThreads) {
+            cf t[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int idx = base + u * kSpDiagThreads + tid;
+                const int rr = idx % kSpB, col = idx / kSpB;
+                t[u] = (rr < jb && col < jb) ? A[(j0 + rr) + (j0 + col) * lda] : cf{0.0f, 0.0f};
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int idx = base + u * kSpDiagThreads + tid;
+                S[(idx / kSpB) * kSpLD + idx % kSpB] = t[u];
+            }
+        }
+        if (tid < kSpB) s_row_at[tid] = tid;
+        __syncthreads();
+        const int r = tid & (kSpB - 1);
+        const int sg = tid >> 7;  // panel column group: columns 8 sg .. 8 sg + 7 of the panel
+        const int wig = (tid >> 5) & 3;
+        for (int c0 = 0; c0 < jb; c0 += kSpPW) {
+            const int nck = (jb - c0) < kSpPW ? (jb - c0) : kSpPW;
+            cf pr[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) pr[q] = S[(c0 + 8 * sg + q) * kSpLD + r];
+#pragma unroll 1
+            for (int cc = 0; cc < nck; ++cc) {
+                const int c = c0 + cc, scol = cc >> 3, qc = cc & 7, par = cc & 1;
+                if (sg == scol) {
+                    cf v = pr[0];
+#pragma unroll
+                    for (int q = 1; q < 8; ++q)
+                        if (q == qc) v = pr[q];
+                    s_col[par][r] = v;
+                    // largest |re| + |im| among rows c .. jb-1, then the smallest
+                    // row (LAPACK's icamax); the low bits carry the row
+                    unsigned long long key = 0;
+                    if (r >= c && r < jb)
+                        key = ((unsigned long long)__float_as_uint(cabs1f(v)) << 32) |
+                              ((unsigned long long)(0xFFFFu - (unsigned int)r) << 16) | (unsigned long long)r;
+#pragma unroll
+                    for (int off = 16; off > 0; off >>= 1) {
+                        const unsigned long long o = __shfl_xor_sync(0xffffffffu, key, off);
+                        key = o > key ? o : key;
+                    }
+                    if (lane == 0) s_key[par][wig] = key;
+                }
+                __syncthreads();
+                unsigned long long best = s_key[par][0];
+#pragma unroll
+                for (int w = 1; w < 4; ++w) best = s_key[par][w] > best ? s_key[par][w] : best;
+                const int p = (int)(best & 0xFFFFull);
+                const bool zero = (best >> 32) == 0ull;
+                const cf inv = zero ? cone<cf>() : crcp_sp(s_col[par][p]);
+                if (r == p) {
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) s_u[par][8 * sg + q] = pr[q];
+                }
+                if (r == c) {
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) s_rc[par][8 * sg + q] = pr[q];
+                }
+                // the interchange in the columns outside the panel, one column
+                // per thread
+                if (p != c && tid < kSpB && (tid < c0 || tid >= c0 + kSpPW)) {
+                    cf* col = S + tid * kSpLD;
+                    const cf t0 = col[c];
+                    col[c] = col[p];
+                    col[p] = t0;
+                }
+                if (tid == 0) {
+                    ipiv[j0 + c] = (int32_t)(j0 + p + 1);
+                    if (zero) {
+                        if (info[0] == 0) info[0] = (int32_t)(j0 + c + 1);
+                        atomicExch(&ws->lmax_bits, 0x7f800000u);  // +inf: the block is singular
+                    }
+                    inv_diag[c] = inv;
+                    const int t0 = s_row_at[c];
+                    s_row_at[c] = s_row_at[p];
+                    s_row_at[p] = t0;
+                }
+                __syncthreads();  // s_u, s_rc complete
+                if (r == c) {
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) pr[q] = s_u[par][8 * sg + q];
+                } else if (r == p) {
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) pr[q] = s_rc[par][8 * sg + q];
+                }
+                if (r > c && r < jb && !zero) {
+                    // row p now holds row c's old values
+                    const cf l = (r == p ? s_col[par][c] : s_col[par][r]) * inv;
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        const int pc = 8 * sg + q;
+                        if (pc == cc) pr[q] = l;
+                        else if (pc > cc) pr[q] = pr[q] - l * s_u[par][pc];
+                    }
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < 8; ++q) S[(c0 + 8 * sg + q) * kSpLD + r] = pr[q];
+            __syncthreads();
+            sp_trailing(S, c0, jb, tid);
+        }
+
+        // the block's rows in pivot order: position i holds original row s_row_at[i]
+        if (tid < jb) perm[tid] = s_row_at[tid];
+    }
+    __syncthreads();
     for (int base = 0; base < kSpB * kSpB; base += kSpDiagThreads) {
         const int idx = base + tid;
         const int rr = idx % kSpB, col = idx / kSpB;
         if (rr < jb && col < jb) A[(j0 + rr) + (j0 + col) * lda] = S[col * kSpLD + rr];
     }
-    // the block's rows in pivot order: position i holds original row s_row_at[i]
-    if (tid < jb) perm[tid] = s_row_at[tid];
 }
 
 // Rows [row0, row0 + jb) of columns [col0, col0 + ncols) rearranged in

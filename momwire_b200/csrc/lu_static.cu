@@ -49,60 +49,69 @@ constexpr int kSpLD = kSpB + 2;  // column stride of the staged block (complex; 
 constexpr int kSpPW = 32;        // panel width inside the block
 constexpr size_t kSpDiagSmem = sizeof(cf) * (size_t)kSpB * kSpLD;
 
-// The later columns of a factored 32-column panel (columns c0 .. c0+31 of
-// the staged block): U12 = L11^-1 A12 on the panel's rows, one thread per
-// column, then A22 -= L21 U12 over rows and columns c0+32 .. jb-1 in 4 x 2
-// register tiles.  All threads of the block take part.
-__device__ __forceinline__ void sp_trailing(cf* S, int c0, int jb, int tid) {
-    const int t0 = c0 + kSpPW;  // first trailing column (and row)
+// U12 = L11^-1 A12 on the rows of the panel at c0 (unit lower L11), one
+// thread per later column; `t` is the caller's index among the threads
+// that take part (the others pass t < 0).
+__device__ __forceinline__ void sp_u12(cf* S, int c0, int jb, int t) {
+    const int t0 = c0 + kSpPW;
     const int nt = jb - t0;
-    if (nt > 0) {
-        // U12 = L11^-1 A12 on the panel's rows, one thread per column
-        if (tid < nt) {
-            cf* col = S + (t0 + tid) * kSpLD + c0;
-            cf x[kSpPW];
+    if (t < 0 || t >= nt) return;
+    cf* col = S + (t0 + t) * kSpLD + c0;
+    cf x[kSpPW];
 #pragma unroll
-            for (int i = 0; i < kSpPW; ++i) x[i] = col[i];
+    for (int i = 0; i < kSpPW; ++i) x[i] = col[i];
 #pragma unroll
-            for (int i = 1; i < kSpPW; ++i) {
-                cf t = x[i];
+    for (int i = 1; i < kSpPW; ++i) {
+        cf v = x[i];
 #pragma unroll
-                for (int jj = 0; jj < i; ++jj) t = t - S[(c0 + jj) * kSpLD + c0 + i] * x[jj];
-                x[i] = t;
-            }
-#pragma unroll
-            for (int i = 0; i < kSpPW; ++i) col[i] = x[i];
-        }
-        __syncthreads();
-        // A22 -= L21 U12 over rows and columns t0 .. jb-1, 4 x 2 tiles
-        const int ntr = (nt + 3) / 4, ntc = (nt + 1) / 2;
-        for (int tile = tid; tile < ntr * ntc; tile += kSpDiagThreads) {
-            const int i0 = t0 + 4 * (tile % ntr), jc = t0 + 2 * (tile / ntr);
-            cf acc[4][2];
-#pragma unroll
-            for (int b2 = 0; b2 < 2; ++b2)
-#pragma unroll
-                for (int a4 = 0; a4 < 4; ++a4) acc[a4][b2] = S[(jc + b2) * kSpLD + i0 + a4];
-#pragma unroll 4
-            for (int jj = 0; jj < kSpPW; ++jj) {
-                const cf* lcol = S + (c0 + jj) * kSpLD + i0;
-                const float4 l01 = *reinterpret_cast<const float4*>(lcol);
-                const float4 l23 = *reinterpret_cast<const float4*>(lcol + 2);
-                const cf l[4] = {cf{l01.x, l01.y}, cf{l01.z, l01.w}, cf{l23.x, l23.y}, cf{l23.z, l23.w}};
-                const cf u0 = S[jc * kSpLD + c0 + jj], u1 = S[(jc + 1) * kSpLD + c0 + jj];
-#pragma unroll
-                for (int a4 = 0; a4 < 4; ++a4) {
-                    acc[a4][0] = acc[a4][0] - l[a4] * u0;
-                    acc[a4][1] = acc[a4][1] - l[a4] * u1;
-                }
-            }
-#pragma unroll
-            for (int b2 = 0; b2 < 2; ++b2)
-#pragma unroll
-                for (int a4 = 0; a4 < 4; ++a4) S[(jc + b2) * kSpLD + i0 + a4] = acc[a4][b2];
-        }
-        __syncthreads();
+        for (int jj = 0; jj < i; ++jj) v = v - S[(c0 + jj) * kSpLD + c0 + i] * x[jj];
+        x[i] = v;
     }
+#pragma unroll
+    for (int i = 0; i < kSpPW; ++i) col[i] = x[i];
+}
+
+// A22 -= L21 U12 over rows and columns c0+32 .. jb-1 in 4 x 2 register
+// tiles (all threads of the block).
+__device__ __forceinline__ void sp_a22(cf* S, int c0, int jb, int tid) {
+    const int t0 = c0 + kSpPW;
+    const int nt = jb - t0;
+    if (nt <= 0) return;
+    const int ntr = (nt + 3) / 4, ntc = (nt + 1) / 2;
+    for (int tile = tid; tile < ntr * ntc; tile += kSpDiagThreads) {
+        const int i0 = t0 + 4 * (tile % ntr), jc = t0 + 2 * (tile / ntr);
+        cf acc[4][2];
+#pragma unroll
+        for (int b2 = 0; b2 < 2; ++b2)
+#pragma unroll
+            for (int a4 = 0; a4 < 4; ++a4) acc[a4][b2] = S[(jc + b2) * kSpLD + i0 + a4];
+#pragma unroll 4
+        for (int jj = 0; jj < kSpPW; ++jj) {
+            const cf* lcol = S + (c0 + jj) * kSpLD + i0;
+            const float4 l01 = *reinterpret_cast<const float4*>(lcol);
+            const float4 l23 = *reinterpret_cast<const float4*>(lcol + 2);
+            const cf l[4] = {cf{l01.x, l01.y}, cf{l01.z, l01.w}, cf{l23.x, l23.y}, cf{l23.z, l23.w}};
+            const cf u0 = S[jc * kSpLD + c0 + jj], u1 = S[(jc + 1) * kSpLD + c0 + jj];
+#pragma unroll
+            for (int a4 = 0; a4 < 4; ++a4) {
+                acc[a4][0] = acc[a4][0] - l[a4] * u0;
+                acc[a4][1] = acc[a4][1] - l[a4] * u1;
+            }
+        }
+#pragma unroll
+        for (int b2 = 0; b2 < 2; ++b2)
+#pragma unroll
+            for (int a4 = 0; a4 < 4; ++a4) S[(jc + b2) * kSpLD + i0 + a4] = acc[a4][b2];
+    }
+}
+
+// The later columns of a factored 32-column panel: U12, then A22 (all
+// threads; the caller synchronises after it).
+__device__ __forceinline__ void sp_trailing(cf* S, int c0, int jb, int tid) {
+    if (jb - (c0 + kSpPW) <= 0) return;
+    sp_u12(S, c0, jb, tid);
+    __syncthreads();
+    sp_a22(S, c0, jb, tid);
 }
 
 // Factor A[j0 .. j0+jb) x [j0 .. j0+jb) in place, pivots among these rows
@@ -123,8 +132,6 @@ __device__ __forceinline__ void sp_trailing(cf* S, int c0, int jb, int tid) {
 //           for the other columns); two block barriers per column.
 // Each panel is followed by its U12 and A22 updates (sp_trailing).
 constexpr float kSpNoPivotBound = 2.0f;
-
-__device__ __forceinline__ void sp_bar_panel() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
 
 __global__ void __launch_bounds__(kSpDiagThreads, 1)
     sp_diag_kernel(cf* __restrict__ A, int64_t lda, int64_t j0, int jb, int32_t* __restrict__ ipiv,
@@ -159,47 +166,59 @@ __global__ void __launch_bounds__(kSpDiagThreads, 1)
     // ---- without interchanges
     for (int c0 = 0; c0 < jb; c0 += kSpPW) {
         const int nck = (jb - c0) < kSpPW ? (jb - c0) : kSpPW;
-        if (tid < kSpB) {
-            const int r = tid;
-            cf a[kSpPW];
-#pragma unroll
-            for (int q = 0; q < kSpPW; ++q) a[q] = S[(c0 + q) * kSpLD + r];
-            float lmax = 0.0f;
-            bool bad = false;
-#pragma unroll
-            for (int cc = 0; cc < kSpPW; ++cc) {
-                if (cc < nck) {
-                    const int c = c0 + cc, par = cc & 1;
-                    if (r == c) {
-                        // row c is final: its values from column cc on
-#pragma unroll
-                        for (int q = cc & ~1; q < kSpPW; q += 2)
-                            *reinterpret_cast<float4*>(&s_u[par][q]) =
-                                make_float4(a[q].re, a[q].im, a[q + 1].re, a[q + 1].im);
-                    }
-                    sp_bar_panel();
-                    const cf piv = s_u[par][cc];
-                    const float pa = cabs1f(piv);
-                    bad = bad || !(pa > 0.0f);
-                    const cf inv = pa > 0.0f ? crcp_sp(piv) : cone<cf>();
-                    if (r == c) s_inv[c] = inv;
-                    if (r > c && r < jb) {
-                        const cf l = a[cc] * inv;
-                        a[cc] = l;
-                        lmax = fmaxf(lmax, cabs1f(l));
-#pragma unroll
-                        for (int q = cc + 1; q < kSpPW; ++q) a[q] = a[q] - l * s_u[par][q];
-                    }
+        const int warp = tid >> 5;
+        float lmax = 0.0f;
+        bool bad = false;
+        // (1) the panel's 32 x 32 diagonal sub-block by warp 0, lane = row
+        // c0 + lane: the pivot row is read in place (broadcast), one warp
+        // synchronisation per column
+        if (warp == 0) {
+            cf* row = S + c0 + lane;
+            for (int cc = 0; cc < nck; ++cc) {
+                __syncwarp();
+                const int c = c0 + cc;
+                const cf piv = S[c * kSpLD + c];
+                const float pa = cabs1f(piv);
+                bad = bad || !(pa > 0.0f);
+                const cf inv = pa > 0.0f ? crcp_sp(piv) : cone<cf>();
+                if (lane == cc) s_inv[c] = inv;
+                if (lane > cc && lane < nck) {
+                    const cf l = row[c * kSpLD] * inv;
+                    row[c * kSpLD] = l;
+                    lmax = fmaxf(lmax, cabs1f(l));
+#pragma unroll 4
+                    for (int q = cc + 1; q < nck; ++q)
+                        row[(c0 + q) * kSpLD] = row[(c0 + q) * kSpLD] - l * S[(c0 + q) * kSpLD + c];
                 }
             }
-#pragma unroll
-            for (int q = 0; q < kSpPW; ++q) S[(c0 + q) * kSpLD + r] = a[q];
-            // NaN-safe: a NaN multiplier fails the comparison
-            if (bad || !(lmax <= kSpNoPivotBound)) atomicOr(&s_bad, 1);
         }
         __syncthreads();
+        // (2) in parallel: the rows below the sub-block, L = A U11^-1 (warps
+        // 0-3, a row each, right-looking along the row), and the columns
+        // right of it, U12 = L11^-1 A12 (warps 4-7, a column each)
+        const int t0 = c0 + kSpPW;
+        if (tid < kSpB) {
+            const int R = t0 + tid;
+            if (R < jb) {
+                cf* row = S + R;
+                for (int jj = 0; jj < nck; ++jj) {
+                    const cf l = row[(c0 + jj) * kSpLD] * s_inv[c0 + jj];
+                    row[(c0 + jj) * kSpLD] = l;
+                    lmax = fmaxf(lmax, cabs1f(l));
+#pragma unroll 4
+                    for (int q = jj + 1; q < nck; ++q)
+                        row[(c0 + q) * kSpLD] = row[(c0 + q) * kSpLD] - l * S[(c0 + q) * kSpLD + c0 + jj];
+                }
+            }
+        } else if (tid < 2 * kSpB) {
+            sp_u12(S, c0, jb, tid - kSpB);
+        }
+        // NaN-safe: a NaN multiplier fails the comparison
+        if (bad || !(lmax <= kSpNoPivotBound)) atomicOr(&s_bad, 1);
+        __syncthreads();
         if (s_bad) break;
-        sp_trailing(S, c0, jb, tid);
+        // (3) the trailing block
+        sp_a22(S, c0, jb, tid);
         __syncthreads();
     }
     if (!s_bad) {
@@ -315,6 +334,7 @@ __global__ void __launch_bounds__(kSpDiagThreads, 1)
             for (int q = 0; q < 8; ++q) S[(c0 + 8 * sg + q) * kSpLD + r] = pr[q];
             __syncthreads();
             sp_trailing(S, c0, jb, tid);
+            __syncthreads();
         }
 
         // the block's rows in pivot order: position i holds original row s_row_at[i]

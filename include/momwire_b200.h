@@ -223,6 +223,50 @@ mw_status mw_fill_z_image(const mw_segments* seg, const mw_basis* basis,
                           float* Z32, int64_t ldz32, void* stream);
 
 /*
+ * One side of an off-edge block: n_basis bases whose d+1 wings index this
+ * side's own segment arrays (supp (n_basis, d+1), -1 = no wing; polys
+ * (n_basis, d+1, d+1) monomial coefficients in local arc length), the
+ * segments' end points and unit tangents (n_seg, 3), and for the extended
+ * kernel their coaxial group labels (n_seg; -1 = none) or NULL.  All device
+ * pointers.
+ */
+typedef struct mw_block_side {
+    int32_t        n_basis;
+    const int32_t* supp;
+    const double*  polys;
+    int32_t        n_seg;
+    const double*  seg_l;
+    const double*  seg_r;
+    const double*  tangent;
+    const int32_t* ek_group;
+} mw_block_side;
+
+/* Reflection-coefficient image weights of the block sampler: eps~ and the
+ * charge weight w_Phi = c0 + c1 rho_v (_ground_refl.py phi_mode_coeffs). */
+typedef struct mw_block_refl {
+    double eps_re, eps_im;
+    double phi_c0_re, phi_c0_im;
+    double phi_c1_re, phi_c1_im;
+} mw_block_refl;
+
+/*
+ * The off-edge Galerkin block Z[I, J] (row-major, Z[m * ldz + n],
+ * complex128) between two basis sets by plain n_qp x n_qp Gauss quadrature
+ * of every wing pair, fused with the EFIE combine: the H-matrix / array-
+ * block ACA row, column and block sampler.  refl == NULL: free space (or a
+ * PEC image with the J side passed mirrored); refl != NULL: the Fresnel
+ * image, J side mirrored.  a_ek > 0 applies the extended kernel's coaxial
+ * factor (radius a_ek) on pairs with equal non-negative group labels.
+ * gl_t / gl_w: n_qp <= 8 host-side nodes and weights on [0, 1].  Replaces
+ * bspline_assemble_offedge_block, _refl, _ek and _refl_ek
+ * (_accelerators.cpp:1977-2680, bound at :6440-6500) as called by
+ * hmatrix.py _offedge_block_evaluators_uniform (hmatrix.py:1157-1290).
+ */
+mw_status mw_offedge_block(int32_t degree, const mw_block_side* I, const mw_block_side* J, double a_squared,
+                           const mw_freq* freq, int32_t n_qp, const double* gl_t, const double* gl_w,
+                           const mw_block_refl* refl, double a_ek, double* Z, int64_t ldz, void* stream);
+
+/*
  * Singular basis enrichment (bspline.py:3048-3076 specs): one basis per
  * wire end at a junction of at least enrichment_min_k ends, on the segment
  * beside the junction, shaped u log u - P(u) with u the normalised distance

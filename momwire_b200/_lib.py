@@ -89,6 +89,23 @@ class Ground(C.Structure):
     ]
 
 
+class BlockSide(C.Structure):
+    _fields_ = [
+        ("n_basis", i32),
+        ("supp", vp),
+        ("polys", vp),
+        ("n_seg", i32),
+        ("seg_l", vp),
+        ("seg_r", vp),
+        ("tangent", vp),
+        ("ek_group", vp),
+    ]
+
+
+class BlockRefl(C.Structure):
+    _fields_ = [(n, f64) for n in ("eps_re", "eps_im", "phi_c0_re", "phi_c0_im", "phi_c1_re", "phi_c1_im")]
+
+
 class Enrich(C.Structure):
     _fields_ = [
         ("n_enrich", i32),
@@ -137,6 +154,8 @@ _SIGS = {
     "mw_offedge_moments": (i32, [C.POINTER(Segments), C.POINTER(Segments), i32, i32, f64, i32, f64, vp, vp, vp, vp]),
     "mw_fill_z": (i32, [C.POINTER(Segments), C.POINTER(BasisT), vp, C.POINTER(Edges), C.POINTER(Freq), i32, vp, i64, vp, i64, vp]),
     "mw_fill_z_image": (i32, [C.POINTER(Segments), C.POINTER(BasisT), C.POINTER(Ground), C.POINTER(Freq), i32, vp, i64, vp, i64, vp]),
+    "mw_offedge_block": (i32, [i32, C.POINTER(BlockSide), C.POINTER(BlockSide), f64, C.POINTER(Freq), i32, vp, vp,
+                               C.POINTER(BlockRefl), f64, vp, i64, vp]),
     "mw_enrich_blocks": (i32, [C.POINTER(Segments), C.POINTER(BasisT), C.POINTER(Enrich), C.POINTER(Freq),
                                C.POINTER(Ground), vp, i64, vp, i64, vp]),
     "mw_fill_z_noalloc": (i32, [C.POINTER(Segments), C.POINTER(BasisT), C.POINTER(Edges), C.POINTER(Freq), i32, i32, vp, i64, vp]),

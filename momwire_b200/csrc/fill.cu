@@ -40,17 +40,6 @@ static GLParams make_gl(int nq) {
     return g;
 }
 
-// NEC Eq 89 coaxial factor 1 + T1*C2 - T2*C1 (_bspline_kernels.py:198).
-__device__ __forceinline__ cd ek_factor(double R, double a, double k) {
-    double kr = k * R;
-    double ar = a / R;
-    double ar2 = ar * ar;
-    double t1 = 0.25 * ar2 * ar2;
-    double t2 = 0.5 * ar2;
-    // c1 = 1 + j kr ; c2 = 3 c1 - kr^2
-    double c2re = 3.0 - kr * kr, c2im = 3.0 * kr;
-    return cd{1.0 + t1 * c2re - t2, t1 * c2im - t2 * kr};
-}
 // fac - fac_static = T1 (3 j kr - kr^2) - T2 (j kr)   (_bspline_kernels.py:225)
 __device__ __forceinline__ cd ek_reg_extra(double R, double a, double k) {
     double kr = k * R;

@@ -118,75 +118,77 @@ def _swept_y(Xt, B, A):
     return np.einsum("kpn,nq->kqp", Wt, B)
 
 
-class _DeviceTables:
-    """Device copies of the k-independent tables plus their C structs."""
+class _PackedTables:
+    """The k-independent tables of one structure laid out in one page-locked
+    host buffer (256-byte aligned pieces), ready for ONE stream-ordered
+    upload.  Built on the host only (no CUDA call but the pinned
+    allocation), so a helper thread can prepare the next structures while
+    the GPU works: a copy per table (seventeen per structure) from pageable
+    memory made each solver's set-up wait for the device, and that wait
+    bounded sweeps over many structures."""
 
-    def __init__(self, solver, geom: T.Geometry, basis: T.Basis, tiles: T.Tiles, ek, dev):
+    def __init__(self, geom: T.Geometry, basis: T.Basis, tiles: T.Tiles, ek):
         torch = _torch()
-        self.keep = []
-        self.h2d_bytes = 0
+        arrays, idx = [], {}
 
-        def up(a, dtype):
-            t = torch.from_numpy(np.ascontiguousarray(a, dtype=dtype)).to(dev)
-            self.keep.append(t)
-            self.h2d_bytes += t.numel() * t.element_size()
-            return t
+        def put(key, a, dtype):
+            idx[key] = len(arrays)
+            arrays.append(np.ascontiguousarray(a, dtype=dtype))
 
-        self.seg_l = up(geom.seg_l, np.float64)
-        self.seg_r = up(geom.seg_r, np.float64)
-        self.tan = up(geom.tangents, np.float64)
-        self.rad = up(geom.radius, np.float64)
-        self.edge = up(geom.edge, np.int32)
-        self.pos = up(geom.pos_in_edge, np.int32)
-        self.grp = up(ek[0], np.int32) if ek is not None else None
-        self.grp_img = up(ek[1], np.int32) if (ek is not None and ek[1] is not None) else None
-        self.seg = _lib.Segments(
-            geom.n,
-            self.seg_l.data_ptr(),
-            self.seg_r.data_ptr(),
-            self.tan.data_ptr(),
-            self.rad.data_ptr(),
-            self.edge.data_ptr(),
-            self.pos.data_ptr(),
-            self.grp.data_ptr() if self.grp is not None else None,
-            self.grp_img.data_ptr() if self.grp_img is not None else None,
-        )
+        put("seg_l", geom.seg_l, np.float64)
+        put("seg_r", geom.seg_r, np.float64)
+        put("tan", geom.tangents, np.float64)
+        put("rad", geom.radius, np.float64)
+        put("edge", geom.edge, np.int32)
+        put("pos", geom.pos_in_edge, np.int32)
+        if ek is not None:
+            put("grp", ek[0], np.int32)
+            if ek[1] is not None:
+                put("grp_img", ek[1], np.int32)
         off, rows = T.edge_table_offsets(geom.edge_n)
-        self.e_n = up(geom.edge_n, np.int32)
-        self.e_off = up(off, np.int64)
-        self.e_h = up(geom.edge_h, np.float64)
-        self.e_r = up(geom.edge_radius, np.float64)
-        self.table_rows = rows
-        self.edges = _lib.Edges(
-            len(geom.edge_n),
-            self.e_n.data_ptr(),
-            self.e_off.data_ptr(),
-            self.e_h.data_ptr(),
-            self.e_r.data_ptr(),
-            rows,
-            int(geom.edge_n.max()),
-        )
-        self.supp = up(basis.supp, np.int32)
-        self.polys = up(basis.polys, np.float64)
-        self.t_first = up(tiles.first, np.int32)
-        self.t_nb = up(tiles.nb, np.int32)
-        self.t_ns = up(tiles.ns, np.int32)
-        self.t_seg = up(tiles.seg, np.int32)
-        self.loc = up(tiles.loc, np.int32)
-        self.basis = _lib.BasisT(
-            basis.degree,
-            basis.n,
-            self.supp.data_ptr(),
-            self.polys.data_ptr(),
-            len(tiles.first),
-            tiles.max_basis,
-            tiles.max_seg,
-            self.t_first.data_ptr(),
-            self.t_nb.data_ptr(),
-            self.t_ns.data_ptr(),
-            self.t_seg.data_ptr(),
-            self.loc.data_ptr(),
-        )
+        put("e_n", geom.edge_n, np.int32)
+        put("e_off", off, np.int64)
+        put("e_h", geom.edge_h, np.float64)
+        put("e_r", geom.edge_radius, np.float64)
+        put("supp", basis.supp, np.int32)
+        put("polys", basis.polys, np.float64)
+        put("t_first", tiles.first, np.int32)
+        put("t_nb", tiles.nb, np.int32)
+        put("t_ns", tiles.ns, np.int32)
+        put("t_seg", tiles.seg, np.int32)
+        put("loc", tiles.loc, np.int32)
+        offs, total = [], 0
+        for x in arrays:
+            offs.append(total)
+            total += (x.nbytes + 255) & ~255
+        self.host = torch.empty(max(total, 256), dtype=torch.uint8, pin_memory=True)
+        hv = self.host.numpy()
+        for x, o in zip(arrays, offs):
+            hv[o : o + x.nbytes] = x.view(np.uint8).reshape(-1)
+        self.offset = {k: offs[i] for k, i in idx.items()}
+        self.nbytes = int(sum(x.nbytes for x in arrays))
+        self.rows = rows
+        self.meta = (geom.n, len(geom.edge_n), int(geom.edge_n.max()), basis.degree, basis.n, len(tiles.first),
+                     tiles.max_basis, tiles.max_seg)
+
+
+class _DeviceTables:
+    """Device copies of the k-independent tables plus their C structs: one
+    stream-ordered copy of a _PackedTables buffer on the caller's current
+    stream (the host buffer stays referenced until the object goes)."""
+
+    def __init__(self, packed: _PackedTables, dev):
+        devbuf = packed.host.to(dev, non_blocking=True)
+        self.keep = [packed.host, devbuf]
+        self.h2d_bytes = packed.nbytes
+        ptr = {k: devbuf.data_ptr() + o for k, o in packed.offset.items()}
+        n_seg, n_edge, max_n, degree, n_basis, n_tile, max_basis, max_seg = packed.meta
+        self.seg = _lib.Segments(n_seg, ptr["seg_l"], ptr["seg_r"], ptr["tan"], ptr["rad"], ptr["edge"],
+                                 ptr["pos"], ptr.get("grp"), ptr.get("grp_img"))
+        self.table_rows = packed.rows
+        self.edges = _lib.Edges(n_edge, ptr["e_n"], ptr["e_off"], ptr["e_h"], ptr["e_r"], packed.rows, max_n)
+        self.basis = _lib.BasisT(degree, n_basis, ptr["supp"], ptr["polys"], n_tile, max_basis, max_seg,
+                                 ptr["t_first"], ptr["t_nb"], ptr["t_ns"], ptr["t_seg"], ptr["loc"])
 
 
 # the reference's refusals of enrichment combinations (bspline.py:308-330):
@@ -377,6 +379,7 @@ class BSplineSolver:
         self._cached_basis = None
         self._cached_tiles = None
         self._cached_dev = None
+        self._cached_packed = None
         self._cached_ek = None
         self.last_stats = {}
 
@@ -465,11 +468,18 @@ class BSplineSolver:
                 np.polynomial.legendre.leggauss(self.n_qp_pair)
             if self.n_qp_pair > 8:
                 raise RuntimeError("n_qp > 8 not supported (scratch buffer size)")
+            self._cached_dev = _DeviceTables(self._packed_tables(), self._torch_device())
+        return self._cached_dev
+
+    def _packed_tables(self) -> _PackedTables:
+        """The host side of _dev_tables (geometry, basis, fill tiles, packed
+        for one upload): no device work, so it can be prepared ahead."""
+        if self._cached_packed is None:
             geom, basis = self._geometry(), self._basis()
             if self._cached_tiles is None:
                 self._cached_tiles = T.build_tiles(basis.supp)
-            self._cached_dev = _DeviceTables(self, geom, basis, self._cached_tiles, self._ek(), self._torch_device())
-        return self._cached_dev
+            self._cached_packed = _PackedTables(geom, basis, self._cached_tiles, self._ek())
+        return self._cached_packed
 
     # --------------------------------------------------------------- ports
     def _split_kcl_ports(self, kcl_A):

@@ -284,8 +284,8 @@ def shard_indices(structs, rank, world):
 
 class _DeviceGroups:
     """Solves the groups of a sweep on the GPU: one device arena for every
-    group, the heaviest groups first, and a helper thread that builds and
-    uploads the next structures' host tables on its own stream while the
+    group, the heaviest groups first, and a helper thread that builds the
+    next structures' host tables (packed for one upload each) while the
     current group is filled and factorised."""
 
     def __init__(self, solvers, ks, plan_ids, P_max):
@@ -299,20 +299,19 @@ class _DeviceGroups:
         self.stream = torch.cuda.current_stream(self.dev).cuda_stream
         self.arena = torch.empty(max(_group_bytes(len(ids) * len(ks), nb, P_max) for nb, ids in plan_ids),
                                  dtype=torch.uint8, device=self.dev)
-        self.prep_stream = torch.cuda.Stream(device=self.dev)
         self.ports = {}
         self.ex = cf.ThreadPoolExecutor(max_workers=1)
         self.futs = {i: self.ex.submit(self._prep, i) for _nb, ids in plan_ids for i in ids}
 
     def _prep(self, i):
-        import torch
-
-        with torch.cuda.device(self.dev), torch.cuda.stream(self.prep_stream):
-            s = self.solvers[i]
-            s._dev_tables()
-            s._loading_dev_tables()
-            self.ports[i] = s._sweep_rhs()
-            self.prep_stream.synchronize()
+        # host work only (tables packed for one upload, port columns); the
+        # uploads themselves are stream-ordered on the main thread, so the
+        # helper never waits for the device
+        s = self.solvers[i]
+        s._packed_tables()
+        if s._loading is not None:
+            s._loading_tables()
+        self.ports[i] = s._sweep_rhs()
 
     def solve(self, nb, ids):
         def wait(g):

@@ -57,8 +57,8 @@ def test_offedge_moments_match_oracle(name, mirror, cuda_device):
     groups = None
     if s.extended_kernel:
         lab, lab_img = s._ek()
-        gi = dt.grp.data_ptr()
-        gj = (dt.grp_img if mirror else dt.grp).data_ptr()
+        gi = dt.seg.ek_group
+        gj = dt.seg.ek_group_img if mirror else dt.seg.ek_group
         groups = (lab, lab_img if mirror else lab)
     gz = float(s.ground_z or 0.0)
     _lib.call("mw_offedge_moments", C.byref(dt.seg), C.byref(dt.seg), d, s.n_qp_pair, float(s.k), mirror, gz,

@@ -1002,12 +1002,30 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
                  : "d"(a), "d"(b));
 }
 
+// The last, partial wave of output tiles may be split along K (chosen by
+// zgemm_launch): tiles [0, full) are computed whole; every tile from `full`
+// on is cut into `splits` K chunks of whole DM_K steps, one work unit each.
+// A chunk's partial sum goes to `part` in the threads' fragment order; the
+// unit that brings its tile's count to `splits` adds the chunks in chunk
+// order (the same sum whichever unit finishes last), applies alpha and beta,
+// writes C and resets the count to zero for the next launch.  No unit waits
+// on another.
+struct DmSplit {
+    unsigned int* count;  // one per split tile, zero between launches
+    cd* part;             // [split tiles * splits][DM_M * DM_N]
+    int64_t full;
+    int splits;
+};
+constexpr int kDmSplitMaxUnits = 256;
+constexpr size_t kDmSplitCountBytes = sizeof(unsigned int) * kDmSplitMaxUnits;
+
 template <bool TA, bool TB>
 __global__ void __launch_bounds__(256, 1) zgemm_dmma_kernel(int64_t m, int64_t n, int64_t k, cd alpha,
                                                             const cd* __restrict__ A, int64_t lda,
                                                             const cd* __restrict__ B, int64_t ldb, cd beta,
-                                                            cd* __restrict__ C, int64_t ldc) {
+                                                            cd* __restrict__ C, int64_t ldc, DmSplit split) {
     extern __shared__ __align__(16) unsigned char dm_smem[];
+    __shared__ int s_last;
     cd* sA0 = reinterpret_cast<cd*>(dm_smem);  // [2][DM_K][DM_PA]
     cd* sB0 = sA0 + 2 * DM_K * DM_PA;          // [2][DM_N][DM_PB]
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -1018,7 +1036,18 @@ __global__ void __launch_bounds__(256, 1) zgemm_dmma_kernel(int64_t m, int64_t n
     // to a concurrent kernel)
     const int64_t n_mt = (m + DM_M - 1) / DM_M;
     const int64_t n_tiles = n_mt * ((n + DM_N - 1) / DM_N);
-    for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+    const int64_t n_units = split.full + (n_tiles - split.full) * split.splits;
+    const int64_t kchunk = ((k + DM_K - 1) / DM_K + split.splits - 1) / split.splits * DM_K;
+    for (int64_t unit = blockIdx.x; unit < n_units; unit += gridDim.x) {
+    int64_t tile = unit, kb = 0, ke = k;
+    int chunk = -1;
+    if (unit >= split.full) {
+        const int64_t v = unit - split.full;
+        tile = split.full + v / split.splits;
+        chunk = (int)(v % split.splits);
+        kb = chunk * kchunk;
+        ke = kb + kchunk < k ? kb + kchunk : k;
+    }
     const int64_t m0 = (tile % n_mt) * DM_M, n0 = (tile / n_mt) * DM_N;
     double cr[4][4][2], ci[4][4][2];
 #pragma unroll
@@ -1034,7 +1063,7 @@ __global__ void __launch_bounds__(256, 1) zgemm_dmma_kernel(int64_t m, int64_t n
             const int r = TA ? i / DM_K : i % DM_M;
             const int kk = TA ? i % DM_K : i / DM_M;
             const int64_t gr = m0 + r, gk = k0 + kk;
-            ra[u] = (gr < m && gk < k) ? (TA ? A[gk + gr * lda] : A[gr + gk * lda]) : cd{0.0, 0.0};
+            ra[u] = (gr < m && gk < ke) ? (TA ? A[gk + gr * lda] : A[gr + gk * lda]) : cd{0.0, 0.0};
         }
 #pragma unroll
         for (int u = 0; u < LB; ++u) {
@@ -1042,7 +1071,7 @@ __global__ void __launch_bounds__(256, 1) zgemm_dmma_kernel(int64_t m, int64_t n
             const int kk = TB ? i / DM_N : i % DM_K;
             const int cc = TB ? i % DM_N : i / DM_K;
             const int64_t gk = k0 + kk, gc = n0 + cc;
-            rb[u] = (gk < k && gc < n) ? (TB ? B[gc + gk * ldb] : B[gk + gc * ldb]) : cd{0.0, 0.0};
+            rb[u] = (gk < ke && gc < n) ? (TB ? B[gc + gk * ldb] : B[gk + gc * ldb]) : cd{0.0, 0.0};
         }
     };
     auto stash = [&](int slot) {
@@ -1064,12 +1093,12 @@ __global__ void __launch_bounds__(256, 1) zgemm_dmma_kernel(int64_t m, int64_t n
         }
     };
 
-    fetch(0);
+    fetch(kb);
     stash(0);
     __syncthreads();
     int slot = 0;
-    for (int64_t k0 = 0; k0 < k; k0 += DM_K) {
-        const bool more = k0 + DM_K < k;
+    for (int64_t k0 = kb; k0 < ke; k0 += DM_K) {
+        const bool more = k0 + DM_K < ke;
         if (more) fetch(k0 + DM_K);
         const cd* sA = sA0 + slot * DM_K * DM_PA;
         const cd* sB = sB0 + slot * DM_N * DM_PB;
@@ -1104,6 +1133,41 @@ __global__ void __launch_bounds__(256, 1) zgemm_dmma_kernel(int64_t m, int64_t n
         slot ^= 1;
     }
     const bool beta_zero = (beta.re == 0.0 && beta.im == 0.0);
+    if (chunk >= 0) {
+        // partial sum of a split tile: element e of this thread at e * 256 + tid
+        const int64_t st = tile - split.full;
+        cd* P = split.part + (st * split.splits + chunk) * (DM_M * DM_N);
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+#pragma unroll
+                for (int h = 0; h < 2; ++h) P[((i * 4 + j) * 2 + h) * 256 + tid] = cd{cr[i][j][h], ci[i][j][h]};
+        __threadfence();
+        __syncthreads();
+        if (tid == 0) s_last = atomicAdd(split.count + st, 1u) == (unsigned)split.splits - 1;
+        __syncthreads();
+        if (!s_last) continue;
+        __threadfence();
+        const cd* P0 = split.part + st * split.splits * (DM_M * DM_N);
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    double sr = 0.0, si = 0.0;
+                    for (int c = 0; c < split.splits; ++c) {
+                        const double2 v = __ldcg(reinterpret_cast<const double2*>(
+                            P0 + (int64_t)c * (DM_M * DM_N) + ((i * 4 + j) * 2 + h) * 256 + tid));
+                        sr += v.x;
+                        si += v.y;
+                    }
+                    cr[i][j][h] = sr;
+                    ci[i][j][h] = si;
+                }
+        if (tid == 0) split.count[st] = 0u;
+    }
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
         const int64_t gr = m0 + wm * 32 + i * 8 + gid;
@@ -1120,18 +1184,47 @@ __global__ void __launch_bounds__(256, 1) zgemm_dmma_kernel(int64_t m, int64_t n
                 *cp = v;
             }
     }
-    }  // tiles
+    }  // units
 }
 
 mw_status zgemm_launch_simt(bool ta, bool tb, int64_t m, int64_t n, int64_t k, cd alpha, const cd* A, int64_t lda,
                             const cd* B, int64_t ldb, cd beta, cd* C, int64_t ldc, cudaStream_t st);
 
+// Workspace for splitting the DMMA kernel's last wave of an m x n product
+// along K: the tile counts, then one partial tile per work unit.
+size_t zgemm_split_ws_bytes(int64_t m, int64_t n) {
+    const int64_t tiles = ((m + DM_M - 1) / DM_M) * ((n + DM_N - 1) / DM_N);
+    const int64_t units = 16 * tiles < kDmSplitMaxUnits ? 16 * tiles : kDmSplitMaxUnits;
+    return kDmSplitCountBytes + (size_t)units * DM_M * DM_N * sizeof(cd);
+}
+
+mw_status zgemm_split_ws_init(void* split_ws, cudaStream_t st) {
+    MW_CHECK_CUDA(cudaMemsetAsync(split_ws, 0, kDmSplitCountBytes, st));
+    return MW_OK;
+}
+
+static int dmma_sms() {
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms < 1) sms = 1;
+    }
+    return sms;
+}
+
 // Shape dispatch (measured on B200, 16x16 dipole array): the register-tiled
 // DFMA kernel wins on the LU's rank-64 updates (16.4 vs 13.8 TFLOP/s: short
 // K, epilogue-bound), the DMMA kernel on long-K products such as the
-// refinement residual Z X (14.4 vs 9.6 TFLOP/s).
+// refinement residual Z X (14.4 vs 9.6 TFLOP/s).  The DMMA kernel runs one
+// CTA per SM over its tiles; given a workspace (zgemm_split_ws_bytes, counts
+// zeroed once), a last wave that would leave SMs idle is split along K so
+// that it fills them: the residual of the 16x16 array has 328 tiles on 148
+// SMs, 2 whole waves and 32 tiles cut into 4 chunks each.
 mw_status zgemm_launch(bool ta, bool tb, int64_t m, int64_t n, int64_t k, cd alpha, const cd* A, int64_t lda,
-                       const cd* B, int64_t ldb, cd beta, cd* C, int64_t ldc, cudaStream_t st, int max_ctas) {
+                       const cd* B, int64_t ldb, cd beta, cd* C, int64_t ldc, cudaStream_t st, int max_ctas,
+                       void* split_ws, size_t split_ws_bytes) {
     if (m <= 0 || n <= 0) return MW_OK;
     if (k < 128) return zgemm_launch_simt(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, st);
     {
@@ -1148,18 +1241,41 @@ mw_status zgemm_launch(bool ta, bool tb, int64_t m, int64_t n, int64_t k, cd alp
             attr = true;
         }
         // one CTA per SM (register-bound); a cap leaves SMs to other work
-        int64_t tiles = ((m + DM_M - 1) / DM_M) * ((n + DM_N - 1) / DM_N);
-        if (max_ctas > 0 && tiles > max_ctas) tiles = max_ctas;
-        dim3 grid((unsigned)tiles);
+        const int64_t tiles = ((m + DM_M - 1) / DM_M) * ((n + DM_N - 1) / DM_N);
+        int64_t ctas = dmma_sms();
+        if (max_ctas > 0 && ctas > max_ctas) ctas = max_ctas;
+        DmSplit split{nullptr, nullptr, tiles, 1};
+        const int64_t tail = tiles % ctas;
+        if (split_ws && tail > 0 && split_ws_bytes > kDmSplitCountBytes) {
+            const int64_t room = (int64_t)((split_ws_bytes - kDmSplitCountBytes) / (DM_M * DM_N * sizeof(cd)));
+            int64_t s = ctas / tail;
+            const int64_t ksteps = (k + DM_K - 1) / DM_K;
+            if (s > ksteps) s = ksteps;
+            if (tail * s > room) s = room / tail;
+            if (tail * s > kDmSplitMaxUnits) s = kDmSplitMaxUnits / tail;
+            if (s >= 2) s = (ksteps + (ksteps + s - 1) / s - 1) / ((ksteps + s - 1) / s);  // no empty chunk
+            if (s >= 2) {
+                split.count = static_cast<unsigned int*>(split_ws);
+                split.part = reinterpret_cast<cd*>(static_cast<char*>(split_ws) + kDmSplitCountBytes);
+                split.full = tiles - tail;
+                split.splits = (int)s;
+            }
+        }
+        const int64_t units = split.full + (tiles - split.full) * split.splits;
+        dim3 grid((unsigned)(units < ctas ? units : ctas));
         ProfileScope ps(PC_ZGEMM, st, 8.0 * (double)m * n * k, 16.0 * ((double)m * k + (double)k * n + 2.0 * m * n));
         if (!ta && !tb)
-            zgemm_dmma_kernel<false, false><<<grid, 256, kDmmaSmem, st>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+            zgemm_dmma_kernel<false, false><<<grid, 256, kDmmaSmem, st>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc,
+                                                                             split);
         else if (ta && !tb)
-            zgemm_dmma_kernel<true, false><<<grid, 256, kDmmaSmem, st>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+            zgemm_dmma_kernel<true, false><<<grid, 256, kDmmaSmem, st>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc,
+                                                                             split);
         else if (!ta && tb)
-            zgemm_dmma_kernel<false, true><<<grid, 256, kDmmaSmem, st>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+            zgemm_dmma_kernel<false, true><<<grid, 256, kDmmaSmem, st>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc,
+                                                                             split);
         else
-            zgemm_dmma_kernel<true, true><<<grid, 256, kDmmaSmem, st>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+            zgemm_dmma_kernel<true, true><<<grid, 256, kDmmaSmem, st>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc,
+                                                                             split);
         MW_CHECK_CUDA(cudaGetLastError());
         count_launch();
         return MW_OK;
@@ -1240,7 +1356,8 @@ struct Updater {
 
 static mw_status block_update(const cd* A, int64_t lda, const cd* B, int64_t ldb, cd* C, int64_t ldc, int64_t m,
                               int64_t n, int64_t k, const Updater& u, cudaStream_t st) {
-    return zgemm_launch(false, false, m, n, k, cd{-1.0, 0.0}, A, lda, B, ldb, cd{1.0, 0.0}, C, ldc, st, u.max_ctas);
+    return zgemm_launch(false, false, m, n, k, cd{-1.0, 0.0}, A, lda, B, ldb, cd{1.0, 0.0}, C, ldc, st, u.max_ctas,
+                        nullptr, 0);
 }
 
 // C -= A B from operands already in the updater's planes (complex64).
@@ -1922,5 +2039,5 @@ extern "C" mw_status mw_zgemm(int32_t transA, int32_t transB, int64_t m, int64_t
     MW_REQUIRE(A && B && C, "NULL argument");
     return zgemm_launch(transA != 0, transB != 0, m, n, k, cd{alpha_re, alpha_im}, reinterpret_cast<const cd*>(A),
                         lda, reinterpret_cast<const cd*>(B), ldb, cd{beta_re, beta_im}, reinterpret_cast<cd*>(C), ldc,
-                        as_stream(stream), 0);
+                        as_stream(stream), 0, nullptr, 0);
 }

@@ -18,7 +18,10 @@
 
 namespace mw {
 mw_status zgemm_launch(bool ta, bool tb, int64_t m, int64_t n, int64_t k, cd alpha, const cd* A, int64_t lda,
-                       const cd* B, int64_t ldb, cd beta, cd* C, int64_t ldc, cudaStream_t st, int max_ctas);
+                       const cd* B, int64_t ldb, cd beta, cd* C, int64_t ldc, cudaStream_t st, int max_ctas,
+                       void* split_ws, size_t split_ws_bytes);
+size_t zgemm_split_ws_bytes(int64_t m, int64_t n);
+mw_status zgemm_split_ws_init(void* split_ws, cudaStream_t st);
 
 __global__ void to_c64_kernel(const cd* __restrict__ src, int64_t lds, cf* __restrict__ dst, int64_t ldd, int64_t n,
                               int64_t ncol) {
@@ -128,7 +131,7 @@ extern "C" int32_t mw_last_mixed_history(double* out, int32_t max_n) {
 
 extern "C" size_t mw_zgesv_mixed_workspace_size(int64_t n, int64_t nrhs) {
     return al256(mw_cgetrf_workspace_size(n, nrhs)) + al256((size_t)n * nrhs * 16) + al256((size_t)n * nrhs * 8) +
-           al256((size_t)nrhs * 16);
+           al256((size_t)nrhs * 16) + al256(zgemm_split_ws_bytes(n, nrhs));
 }
 
 extern "C" mw_status mw_zgesv_mixed(int64_t n, int64_t nrhs, const double* Z, int64_t ldz, float* Z32, int64_t ldz32,
@@ -148,6 +151,11 @@ extern "C" mw_status mw_zgesv_mixed(int64_t n, int64_t nrhs, const double* Z, in
     cf* R32 = reinterpret_cast<cf*>(w + al256(lu_ws) + al256((size_t)n * nrhs * 16));
     double* norms = reinterpret_cast<double*>(w + al256(lu_ws) + al256((size_t)n * nrhs * 16) +
                                               al256((size_t)n * nrhs * 8));
+    // the residual product's K-split partials (counts zeroed here, reset by
+    // the kernel after each use)
+    void* split_ws = reinterpret_cast<char*>(norms) + al256((size_t)nrhs * 16);
+    const size_t split_bytes = zgemm_split_ws_bytes(n, nrhs);
+    if (mw_status s0 = zgemm_split_ws_init(split_ws, st); s0 != MW_OK) return s0;
     const cd* Zc = reinterpret_cast<const cd*>(Z);
     const cd* Bc = reinterpret_cast<const cd*>(B);
     cd* Xc = reinterpret_cast<cd*>(X);
@@ -254,7 +262,8 @@ extern "C" mw_status mw_zgesv_mixed(int64_t n, int64_t nrhs, const double* Z, in
             // R = B - Z X   (FP64)
             copy_c128_kernel<<<grid_for(tot), 256, 0, st>>>(Bc, ldb, R, n, n, nrhs);
             count_launch();
-            s = zgemm_launch(false, false, n, nrhs, n, cd{-1.0, 0.0}, Zc, ldz, Xc, ldx, cd{1.0, 0.0}, R, n, st, 0);
+            s = zgemm_launch(false, false, n, nrhs, n, cd{-1.0, 0.0}, Zc, ldz, Xc, ldx, cd{1.0, 0.0}, R, n, st, 0,
+                             split_ws, split_bytes);
             if (s != MW_OK) return s;
         }
         if (corr <= tol || !static_pivot) break;

@@ -988,18 +988,35 @@ __global__ void __launch_bounds__(256) zgemm_kernel(int64_t m, int64_t n, int64_
 // FP64 tensor path (sm_100 has no tcgen05 kind for fp64; DMMA
 // mma.sync.m8n8k4.f64 is the fp64 tensor route).  CTA tile 128 x 64
 // complex, 8 warps as 4 (M) x 2 (N), warp tile 32 x 32 complex = 4 x 4
-// blocks of 8 x 8, each block four real MMAs per k-step of 4:
-//   Cr += Ar Br - Ai Bi,  Ci += Ar Bi + Ai Br.
-// K staged 16 complex at a time through a two-slot shared-memory ring.
-constexpr int DM_M = 128, DM_N = 64, DM_K = 16;
-constexpr int DM_PA = DM_M + 2;   // sA[kk][row] row stride (complex)
-constexpr int DM_PB = DM_K + 1;   // sB[col][kk] stride (complex)
-constexpr size_t kDmmaSmem = sizeof(cd) * 2 * (DM_K * DM_PA + DM_N * DM_PB);
+// blocks of 8 x 8.  Each block takes three real MMAs per k-step of 4
+// (the 3M product):
+//   X += Ar Br,  Y += Ai Bi,  W += (Ar + Ai)(Br + Bi);  Cr = X - Y,  Ci = W - X - Y
+// -- a quarter fewer MMAs than the four-product form, at an error bound on
+// each part of a few units of 2^-53 times sum |A||B|, far below what the
+// complex64 refinement needs of its residual.  K is staged 16 complex at a
+// time through a three-slot shared-memory ring filled by cp.async (no
+// staging registers: the three accumulator sets need them).
+constexpr int DM_M = 128, DM_N = 64, DM_K = 16, DM_STAGES = 3;
+constexpr int DM_PA = DM_M + 2;   // sA[kk][row] row stride (complex): the 4 kk rows of a load fall on distinct banks
+constexpr int DM_PB = DM_K + 4;   // sB[col][kk] stride (complex): 8 columns x 4 kk of a load on distinct banks
+constexpr int DM_SA = DM_K * DM_PA, DM_SB = DM_N * DM_PB;  // per slot
+constexpr size_t kDmmaSmem = sizeof(cd) * DM_STAGES * (DM_SA + DM_SB);
 
 __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
     asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
                  : "+d"(d0), "+d"(d1)
                  : "d"(a), "d"(b));
+}
+
+// 16-byte global -> shared copy; zero-filled when !valid (src then unread)
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, bool valid) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(s), "l"(src), "r"(valid ? 16 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
 // The last, partial wave of output tiles may be split along K (chosen by
@@ -1026,13 +1043,13 @@ __global__ void __launch_bounds__(256, 1) zgemm_dmma_kernel(int64_t m, int64_t n
                                                             cd* __restrict__ C, int64_t ldc, DmSplit split) {
     extern __shared__ __align__(16) unsigned char dm_smem[];
     __shared__ int s_last;
-    cd* sA0 = reinterpret_cast<cd*>(dm_smem);  // [2][DM_K][DM_PA]
-    cd* sB0 = sA0 + 2 * DM_K * DM_PA;          // [2][DM_N][DM_PB]
+    cd* sA0 = reinterpret_cast<cd*>(dm_smem);  // [DM_STAGES][DM_K][DM_PA]
+    cd* sB0 = sA0 + DM_STAGES * DM_SA;         // [DM_STAGES][DM_N][DM_PB]
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int wm = warp & 3, wn = warp >> 2;
     const int gid = lane >> 2, tig = lane & 3;
     constexpr int LA = DM_M * DM_K / 256, LB = DM_K * DM_N / 256;
-    // persistent over the output tiles (the grid may be capped to leave SMs
+    // persistent over the work units (the grid may be capped to leave SMs
     // to a concurrent kernel)
     const int64_t n_mt = (m + DM_M - 1) / DM_M;
     const int64_t n_tiles = n_mt * ((n + DM_N - 1) / DM_N);
@@ -1049,21 +1066,26 @@ __global__ void __launch_bounds__(256, 1) zgemm_dmma_kernel(int64_t m, int64_t n
         ke = kb + kchunk < k ? kb + kchunk : k;
     }
     const int64_t m0 = (tile % n_mt) * DM_M, n0 = (tile / n_mt) * DM_N;
-    double cr[4][4][2], ci[4][4][2];
+    double x[4][4][2], y[4][4][2], w[4][4][2];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) cr[i][j][0] = cr[i][j][1] = ci[i][j][0] = ci[i][j][1] = 0.0;
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) x[i][j][h] = y[i][j][h] = w[i][j][h] = 0.0;
 
-    cd ra[LA], rb[LB];
-    auto fetch = [&](int64_t k0) {
+    // stage K columns [k0, k0 + DM_K) of the tile into `slot`
+    auto load = [&](int slot, int64_t k0) {
+        cd* sA = sA0 + slot * DM_SA;
+        cd* sB = sB0 + slot * DM_SB;
 #pragma unroll
         for (int u = 0; u < LA; ++u) {
             const int i = tid + u * 256;
             const int r = TA ? i / DM_K : i % DM_M;
             const int kk = TA ? i % DM_K : i / DM_M;
             const int64_t gr = m0 + r, gk = k0 + kk;
-            ra[u] = (gr < m && gk < ke) ? (TA ? A[gk + gr * lda] : A[gr + gk * lda]) : cd{0.0, 0.0};
+            const bool ok = gr < m && gk < ke;
+            cp_async16(sA + kk * DM_PA + r, ok ? (TA ? A + gk + gr * lda : A + gr + gk * lda) : A, ok);
         }
 #pragma unroll
         for (int u = 0; u < LB; ++u) {
@@ -1071,67 +1093,62 @@ __global__ void __launch_bounds__(256, 1) zgemm_dmma_kernel(int64_t m, int64_t n
             const int kk = TB ? i / DM_N : i % DM_K;
             const int cc = TB ? i % DM_N : i / DM_K;
             const int64_t gk = k0 + kk, gc = n0 + cc;
-            rb[u] = (gk < ke && gc < n) ? (TB ? B[gc + gk * ldb] : B[gk + gc * ldb]) : cd{0.0, 0.0};
-        }
-    };
-    auto stash = [&](int slot) {
-        cd* sA = sA0 + slot * DM_K * DM_PA;
-        cd* sB = sB0 + slot * DM_N * DM_PB;
-#pragma unroll
-        for (int u = 0; u < LA; ++u) {
-            const int i = tid + u * 256;
-            const int r = TA ? i / DM_K : i % DM_M;
-            const int kk = TA ? i % DM_K : i / DM_M;
-            sA[kk * DM_PA + r] = ra[u];
-        }
-#pragma unroll
-        for (int u = 0; u < LB; ++u) {
-            const int i = tid + u * 256;
-            const int kk = TB ? i / DM_N : i % DM_K;
-            const int cc = TB ? i % DM_N : i / DM_K;
-            sB[cc * DM_PB + kk] = rb[u];
+            const bool ok = gk < ke && gc < n;
+            cp_async16(sB + cc * DM_PB + kk, ok ? (TB ? B + gc + gk * ldb : B + gk + gc * ldb) : B, ok);
         }
     };
 
-    fetch(kb);
-    stash(0);
-    __syncthreads();
-    int slot = 0;
-    for (int64_t k0 = kb; k0 < ke; k0 += DM_K) {
-        const bool more = k0 + DM_K < ke;
-        if (more) fetch(k0 + DM_K);
-        const cd* sA = sA0 + slot * DM_K * DM_PA;
-        const cd* sB = sB0 + slot * DM_N * DM_PB;
+    const int64_t nk = kb < ke ? (ke - kb + DM_K - 1) / DM_K : 0;  // K steps of this unit
+#pragma unroll
+    for (int s = 0; s < DM_STAGES - 1; ++s) {
+        if (s < nk) load(s, kb + s * DM_K);
+        cp_async_commit();
+    }
+    for (int64_t t = 0; t < nk; ++t) {
+        cp_async_wait<DM_STAGES - 2>();  // step t has landed
+        __syncthreads();                  // and every warp is done with step t - 1's slot
+        const int64_t tn = t + DM_STAGES - 1;
+        if (tn < nk) load((int)(tn % DM_STAGES), kb + tn * DM_K);
+        cp_async_commit();
+        const int slot = (int)(t % DM_STAGES);
+        const cd* sA = sA0 + slot * DM_SA;
+        const cd* sB = sB0 + slot * DM_SB;
 #pragma unroll
         for (int k4 = 0; k4 < DM_K; k4 += 4) {
-            double ar[4], ai[4], nai[4], br[4], bi[4];
+            double ar[4], ai[4], as[4];
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
                 const cd a = sA[(k4 + tig) * DM_PA + wm * 32 + i * 8 + gid];
                 ar[i] = a.re;
                 ai[i] = a.im;
-                nai[i] = -a.im;
+                as[i] = a.re + a.im;
             }
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 const cd b = sB[(wn * 32 + j * 8 + gid) * DM_PB + k4 + tig];
-                br[j] = b.re;
-                bi[j] = b.im;
-            }
+                const double bs = b.re + b.im;
 #pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    dmma(cr[i][j][0], cr[i][j][1], ar[i], br[j]);
-                    dmma(cr[i][j][0], cr[i][j][1], nai[i], bi[j]);
-                    dmma(ci[i][j][0], ci[i][j][1], ar[i], bi[j]);
-                    dmma(ci[i][j][0], ci[i][j][1], ai[i], br[j]);
+                for (int i = 0; i < 4; ++i) {
+                    dmma(x[i][j][0], x[i][j][1], ar[i], b.re);
+                    dmma(y[i][j][0], y[i][j][1], ai[i], b.im);
+                    dmma(w[i][j][0], w[i][j][1], as[i], bs);
                 }
+            }
         }
-        if (more) stash(slot ^ 1);
-        __syncthreads();
-        slot ^= 1;
     }
+    cp_async_wait<0>();
+    __syncthreads();  // the ring is free for the next unit
+    // Cr = X - Y into x, Ci = W - X - Y into w
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const double xv = x[i][j][h], yv = y[i][j][h];
+                x[i][j][h] = xv - yv;
+                w[i][j][h] -= xv + yv;
+            }
     const bool beta_zero = (beta.re == 0.0 && beta.im == 0.0);
     if (chunk >= 0) {
         // partial sum of a split tile: element e of this thread at e * 256 + tid
@@ -1142,7 +1159,7 @@ __global__ void __launch_bounds__(256, 1) zgemm_dmma_kernel(int64_t m, int64_t n
 #pragma unroll
             for (int j = 0; j < 4; ++j)
 #pragma unroll
-                for (int h = 0; h < 2; ++h) P[((i * 4 + j) * 2 + h) * 256 + tid] = cd{cr[i][j][h], ci[i][j][h]};
+                for (int h = 0; h < 2; ++h) P[((i * 4 + j) * 2 + h) * 256 + tid] = cd{x[i][j][h], w[i][j][h]};
         __threadfence();
         __syncthreads();
         if (tid == 0) s_last = atomicAdd(split.count + st, 1u) == (unsigned)split.splits - 1;
@@ -1163,8 +1180,8 @@ __global__ void __launch_bounds__(256, 1) zgemm_dmma_kernel(int64_t m, int64_t n
                         sr += v.x;
                         si += v.y;
                     }
-                    cr[i][j][h] = sr;
-                    ci[i][j][h] = si;
+                    x[i][j][h] = sr;
+                    w[i][j][h] = si;
                 }
         if (tid == 0) split.count[st] = 0u;
     }
@@ -1178,7 +1195,7 @@ __global__ void __launch_bounds__(256, 1) zgemm_dmma_kernel(int64_t m, int64_t n
             for (int h = 0; h < 2; ++h) {
                 const int64_t gc = n0 + wn * 32 + j * 8 + 2 * tig + h;
                 if (gc >= n) continue;
-                cd v = alpha * cd{cr[i][j][h], ci[i][j][h]};
+                cd v = alpha * cd{x[i][j][h], w[i][j][h]};
                 cd* cp = C + gr + gc * ldc;
                 if (!beta_zero) v = v + beta * (*cp);
                 *cp = v;

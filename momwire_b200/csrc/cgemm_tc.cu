@@ -387,6 +387,26 @@ TcPlanes tc_planes(void* ws, int64_t m_max, int64_t n_max, int64_t k) {
                     reinterpret_cast<float*>(w + 2 * al(ab)), reinterpret_cast<float*>(w + 2 * al(ab) + al(bb))};
 }
 
+// A (m x k complex64, column-major) into the hi / lo A planes of an update
+// with inner dimension k (the B operand is packed elsewhere); `batch`
+// matrices at A + b a_stride into planes at a_hi / a_lo + b p_stride floats.
+mw_status tc_pack_a(int64_t m, int64_t k, const cf* A, int64_t lda, float* a_hi, float* a_lo, cudaStream_t st,
+                    int batch, int64_t a_stride, int64_t p_stride) {
+    if (m <= 0 || k <= 0 || batch <= 0) return MW_OK;
+    MW_REQUIRE(batch <= 65535, "batch too large");
+    const int n_mb = (int)((2 * m + TC_M - 1) / TC_M);
+    const int n_ks = tc_n_ks(k);
+    const int64_t qa = (int64_t)n_mb * n_ks * TC_CHUNKS * TC_M;
+    int64_t blocks = (qa + 255) / 256;
+    if (blocks > 65535) blocks = 65535;  // the kernel strides over the rest
+    ProfileScope ps(PC_MISC, st);
+    pack_a_kernel<<<dim3((unsigned)blocks, (unsigned)batch), 256, 0, st>>>(A, lda, m, k, n_mb, n_ks, a_hi, a_lo,
+                                                                           a_stride, p_stride);
+    MW_CHECK_CUDA(cudaGetLastError());
+    count_launch();
+    return MW_OK;
+}
+
 // C (m x n complex64, column-major) -= A B from operands already packed in
 // the planes (for an inner dimension k): no packing pass.
 mw_status cgemm_tc_prepacked(int64_t m, int64_t n, int64_t k, const TcPlanes& pl, cf* C, int64_t ldc, int* err,

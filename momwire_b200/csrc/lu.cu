@@ -36,6 +36,9 @@ size_t cgemm_tc_workspace(int64_t m, int64_t n, int64_t k);
 TcPlanes tc_planes(void* ws, int64_t m_max, int64_t n_max, int64_t k);
 mw_status cgemm_tc_prepacked(int64_t m, int64_t n, int64_t k, const TcPlanes& pl, cf* C, int64_t ldc, int* err,
                              cudaStream_t st, int max_ctas);
+mw_status tc_pack_a(int64_t m, int64_t k, const cf* A, int64_t lda, float* a_hi, float* a_lo, cudaStream_t st,
+                    int batch = 1, int64_t a_stride = 0, int64_t p_stride = 0);
+size_t tc_pack_a_bytes(int64_t m, int64_t k);
 
 // static-pivot panel of the complex64 path (lu_static.cu)
 mw_status static_panel_c64(cf* A, int64_t lda, int64_t n, int64_t j0, int jb, int32_t* ipiv, int32_t* info,
@@ -614,11 +617,19 @@ struct LeafPack {
     int b_nks = 0;
     int kap0 = 0;
 };
+// A batch of independent solves in one launch (blockIdx.y = member b): the
+// triangle of member b at Tm + b t_step, its right-hand sides at X + b
+// x_step, its order min(jb, n - b L).  n = 0: a single solve.
+struct TrsmBatch {
+    int64_t t_step = 0;
+    int64_t x_step = 0;
+    int64_t n = 0;
+};
 
 template <class T, bool UPPER, int L, int NC>
 __global__ void __launch_bounds__(32 * kTrsmWarps) trsm_kernel(const T* Tm, int64_t ldt, T* X, int64_t ldx, int jb,
                                                                int64_t ncols, const T* Aoff, int64_t ldo, const T* Xp,
-                                                               int K, LeafPack pk) {
+                                                               int K, LeafPack pk, TrsmBatch bt) {
     // Lane l owns rows RP*l .. RP*l+RP-1 of the block, so a RP x RP diagonal
     // block is solved inside one lane; its RP results reach the other lanes
     // in RP independent shuffles and every lane applies the RP x RP update:
@@ -633,6 +644,12 @@ __global__ void __launch_bounds__(32 * kTrsmWarps) trsm_kernel(const T* Tm, int6
     // where its result is consumed.
     constexpr int RP = L / 32;
     static_assert(RP * 32 == L, "leaf order must be a multiple of 32");
+    if (bt.n > 0) {
+        Tm += blockIdx.y * bt.t_step;
+        X += blockIdx.y * bt.x_step;
+        const int64_t left = bt.n - (int64_t)blockIdx.y * L;
+        if (left < jb) jb = (int)left;
+    }
     extern __shared__ __align__(16) unsigned char trsm_smem[];
     T* S = reinterpret_cast<T*>(trsm_smem);
     T* sD = S + L * L;  // U: reciprocals of the diagonal (zero beyond jb)
@@ -850,18 +867,18 @@ static mw_status trsm_setup() {
 template <class T, bool UPPER, int L = kNB>
 static void trsm_launch(const T* Tm, int64_t ldt, T* X, int64_t ldx, int jb, int64_t ncols, cudaStream_t st,
                         const T* Aoff = nullptr, int64_t ldo = 0, const T* Xp = nullptr, int K = 0,
-                        LeafPack pk = LeafPack{}) {
-    ProfileScope ps(PC_TRSM, st, 4.0 * (double)jb * jb * ncols + 8.0 * (double)jb * K * ncols,
-                    2.0 * sizeof(T) * (double)jb * ncols);
-    if (ncols >= kTrsmWide) {
+                        LeafPack pk = LeafPack{}, TrsmBatch bt = TrsmBatch{}, unsigned batch = 1) {
+    ProfileScope ps(PC_TRSM, st, (4.0 * (double)jb * jb * ncols + 8.0 * (double)jb * K * ncols) * batch,
+                    2.0 * sizeof(T) * (double)jb * ncols * batch);
+    if (ncols >= kTrsmWide || batch > 1) {
         const int64_t per_cta = (int64_t)kTrsmWarps * 4;
-        trsm_kernel<T, UPPER, L, 4><<<(unsigned)((ncols + per_cta - 1) / per_cta), 32 * kTrsmWarps,
-                                      trsm_smem_bytes<T, L>(), st>>>(Tm, ldt, X, ldx, jb, ncols, Aoff, ldo, Xp, K,
-                                                                     pk);
+        const dim3 grid((unsigned)((ncols + per_cta - 1) / per_cta), batch);
+        trsm_kernel<T, UPPER, L, 4><<<grid, 32 * kTrsmWarps, trsm_smem_bytes<T, L>(), st>>>(
+            Tm, ldt, X, ldx, jb, ncols, Aoff, ldo, Xp, K, pk, bt);
     } else {
         trsm_kernel<T, UPPER, L, 1><<<(unsigned)((ncols + kTrsmWarps - 1) / kTrsmWarps), 32 * kTrsmWarps,
                                       trsm_smem_bytes<T, L>(), st>>>(Tm, ldt, X, ldx, jb, ncols, Aoff, ldo, Xp, K,
-                                                                     pk);
+                                                                     pk, bt);
     }
     count_launch();
 }
@@ -1855,6 +1872,278 @@ static mw_status trsm_sweep(bool upper, int64_t n, int64_t nrhs, const T* LU, in
     return critical_end(ax, caller);
 }
 
+// ------------------------------------------------ sweeps on block operators
+// The complex64 solves' triangular sweeps with each 128-row leaf turned into
+// one product.  For block b of the triangle T (unit lower L or upper U of
+// the factors) and q the block solved just before it in sweep order (b - 1
+// for L, b + 1 for U; none for the first):
+//     M_b = T_bb^-1 [ I | -T_bq ]                  (128 x 256, column-major)
+// built once per factorisation (sweep_ops_prepare: the right-hand sides
+// [I | -T_bq] of every block, then one batched leaf solve per triangle), so
+// that the leaf of block b is
+//     X_b = M_b [ B_b ; X_q ]
+// -- a 128 x 256 by 256 x nrhs product with no dependent substitution chain.
+// The same preparation packs every block column of the factors as the A
+// operand of the tensor-core update that carries X_b to the blocks further
+// on; the leaf writes X_b as its packed B operand, so the update packs
+// nothing.  The B planes alternate between two sets by step parity: the
+// update of step i reads its set while leaf i + 1 writes the other, and
+// leaf i + 2 waits for that update.
+constexpr int kOpsB = 128;       // block order (the complex64 solve leaf)
+constexpr int kOpsK = 2 * kOpsB;  // columns of an operator
+constexpr int kOpsCols = 4;       // right-hand sides per leaf CTA
+static_assert(kOpsB == GetrsLeaf<cf>::value, "operator blocks are the solve's leaf blocks");
+
+// the packed A operand of one block column, all n rows (one plane, hi or lo)
+static size_t ops_colplane_bytes(int64_t n) { return tc_pack_a_bytes(n, kOpsB); }
+
+size_t sweep_ops_bytes(int64_t n) {
+    const int64_t nblk = (n + kOpsB - 1) / kOpsB;
+    // the L operators, the U operators, then every block column of the
+    // factors as the packed A operand of the sweeps' updates (hi, lo)
+    return 2 * (size_t)nblk * kOpsB * kOpsK * sizeof(cf) + 2 * (size_t)nblk * ops_colplane_bytes(n);
+}
+
+// Every block's [I | -T_bq]: rows past the block's order, and columns past
+// either block's, zero.  One CTA per block.
+__global__ void __launch_bounds__(256) ops_rhs_kernel(const cf* __restrict__ LU, int64_t lda, int64_t n, int upper,
+                                                      cf* __restrict__ M) {
+    const int64_t nblk = (n + kOpsB - 1) / kOpsB;
+    const int64_t b = blockIdx.x;
+    const int64_t q = upper ? b + 1 : b - 1;
+    const int jb = (int)(n - b * kOpsB < kOpsB ? n - b * kOpsB : kOpsB);
+    const int jq = (q >= 0 && q < nblk) ? (int)(n - q * kOpsB < kOpsB ? n - q * kOpsB : kOpsB) : 0;
+    cf* Mb = M + b * kOpsB * kOpsK;
+    for (int i = threadIdx.x; i < kOpsB * kOpsK; i += blockDim.x) {
+        const int r = i % kOpsB, c = i / kOpsB;
+        cf v{0.0f, 0.0f};
+        if (r < jb) {
+            if (c < kOpsB) {
+                if (c == r) v = cf{1.0f, 0.0f};
+            } else if (c - kOpsB < jq) {
+                const cf t = LU[(b * kOpsB + r) + (q * kOpsB + (c - kOpsB)) * lda];
+                v = cf{-t.re, -t.im};
+            }
+        }
+        Mb[i] = v;
+    }
+}
+
+// X_b (rows < jb of this CTA's kOpsCols columns, in place) = M_b [X_b ; X_q]
+// with X_q the jq rows of the block solved before (jq = 0: none); with b_hi
+// set, X_b also as the packed B operand (inner dimension jb, b_nks stages).
+// M_b streams through shared memory in 32-column chunks (32 KB, contiguous
+// in M_b), two in flight by cp.async (two CTAs fit an SM, so the leaf's CTAs
+// take one wave of the SMs the concurrent update leaves); thread (r, g)
+// accumulates row r of
+// columns 2 g, 2 g + 1, reading its M_b row conflict-free and [X_b ; X_q]
+// as broadcasts.
+constexpr int kOpsChunk = 32;
+constexpr size_t kLeafOpsSmem = sizeof(cf) * (2 * (size_t)kOpsChunk * kOpsB + (size_t)kOpsK * kOpsCols +
+                                              (size_t)kOpsCols * (kOpsB + 1));
+__global__ void __launch_bounds__(256, 1) leaf_ops_kernel(const cf* __restrict__ Mb, cf* __restrict__ X, int64_t ldx,
+                                                          int jb, const cf* __restrict__ Xq, int jq, int64_t ncols,
+                                                          float* __restrict__ b_hi, float* __restrict__ b_lo,
+                                                          int b_nks) {
+    extern __shared__ __align__(16) unsigned char lo_smem[];
+    cf* sM = reinterpret_cast<cf*>(lo_smem);                 // [2][kOpsChunk][kOpsB]
+    cf* sR = sM + 2 * kOpsChunk * kOpsB;                      // [kOpsK][kOpsCols]
+    cf* sO = sR + kOpsK * kOpsCols;                           // [kOpsCols][kOpsB + 1]
+    const int tid = threadIdx.x;
+    const int nchunk = (jq > 0 ? kOpsK : kOpsB) / kOpsChunk;
+    // chunk c: columns [c kOpsChunk, (c + 1) kOpsChunk) of M_b, one contiguous
+    // 32 KB run; eight 16-byte copies per thread
+    auto fetch = [&](int c) {
+        const char* src = reinterpret_cast<const char*>(Mb + (size_t)c * kOpsChunk * kOpsB);
+        char* dst = reinterpret_cast<char*>(sM + (size_t)(c & 1) * kOpsChunk * kOpsB);
+        constexpr int n16 = kOpsChunk * kOpsB * (int)sizeof(cf) / 16;
+#pragma unroll
+        for (int u = 0; u < n16 / 256; ++u) {
+            const int q = tid + 256 * u;
+            cp_async16(dst + 16 * q, src + 16 * q, true);
+        }
+        cp_async_commit();
+    };
+    fetch(0);
+    if (nchunk > 1) fetch(1);
+    const int64_t c0 = (int64_t)blockIdx.x * kOpsCols;
+    for (int i = tid; i < kOpsK * kOpsCols; i += blockDim.x) {
+        const int k = i % kOpsK, c = i / kOpsK;
+        const int64_t col = c0 + c;
+        cf v{0.0f, 0.0f};
+        if (col < ncols) {
+            if (k < kOpsB) {
+                if (k < jb) v = X[k + col * ldx];
+            } else if (k - kOpsB < jq) {
+                v = Xq[(k - kOpsB) + col * ldx];
+            }
+        }
+        sR[k * kOpsCols + c] = v;
+    }
+    const int r = tid & (kOpsB - 1), g = tid >> 7;
+    cf acc0{0.0f, 0.0f}, acc1{0.0f, 0.0f};
+    for (int c = 0; c < nchunk; ++c) {
+        if (c + 1 < nchunk) cp_async_wait<1>();
+        else cp_async_wait<0>();
+        __syncthreads();  // chunk c (and, the first time, sR) visible to all
+        const cf* m = sM + (size_t)(c & 1) * kOpsChunk * kOpsB + r;
+        const cf* x = sR + (size_t)c * kOpsChunk * kOpsCols + 2 * g;
+#pragma unroll 16
+        for (int k = 0; k < kOpsChunk; ++k) {
+            const cf mk = m[k * kOpsB];
+            const float4 xx = *reinterpret_cast<const float4*>(x + k * kOpsCols);
+            acc0 = acc0 + mk * cf{xx.x, xx.y};
+            acc1 = acc1 + mk * cf{xx.z, xx.w};
+        }
+        __syncthreads();  // every thread is done with this slot
+        if (c + 2 < nchunk) fetch(c + 2);
+    }
+    sO[(2 * g) * (kOpsB + 1) + r] = r < jb ? acc0 : cf{0.0f, 0.0f};
+    sO[(2 * g + 1) * (kOpsB + 1) + r] = r < jb ? acc1 : cf{0.0f, 0.0f};
+    __syncthreads();
+    for (int i = tid; i < kOpsB * kOpsCols; i += blockDim.x) {
+        const int rr = i % kOpsB, c = i / kOpsB;
+        const int64_t col = c0 + c;
+        if (col < ncols && rr < jb) X[rr + col * ldx] = sO[c * (kOpsB + 1) + rr];
+    }
+    if (b_hi != nullptr) {
+        // real K rows 2 rr (re) and 2 rr + 1 (im): rows 2p and 2p + 1 of the
+        // block make one 16-byte chunk; rows past jb carry zeros
+        for (int i = tid; i < (kOpsB / 2) * kOpsCols; i += blockDim.x) {
+            const int p = i % (kOpsB / 2), c = i / (kOpsB / 2);
+            const int64_t col = c0 + c;
+            const int64_t kap4 = 4 * (int64_t)p;
+            if (col < ncols && kap4 < (int64_t)b_nks * TC_KS) {
+                const cf v0 = sO[c * (kOpsB + 1) + 2 * p], v1 = sO[c * (kOpsB + 1) + 2 * p + 1];
+                tc_store_b4(b_hi, b_lo, b_nks, col, kap4, make_float4(v0.re, v0.im, v1.re, v1.im));
+            }
+        }
+    }
+}
+
+// Both triangles' operators of the factors LU (n x n, complex64) into
+// `ops` (sweep_ops_bytes(n)).
+static mw_status sweep_ops_prepare(int64_t n, const cf* LU, int64_t lda, cf* ops, cudaStream_t st) {
+    if (n <= 0) return MW_OK;
+    {
+        mw_status s0 = trsm_setup<cf>();
+        if (s0 != MW_OK) return s0;
+    }
+    const int64_t nblk = (n + kOpsB - 1) / kOpsB;
+    MW_REQUIRE(nblk <= 65535, "too many blocks for one batched launch");
+    cf* ML = ops;
+    cf* MU = ops + nblk * kOpsB * kOpsK;
+    {
+        ProfileScope ps(PC_MISC, st);
+        ops_rhs_kernel<<<(unsigned)nblk, 256, 0, st>>>(LU, lda, n, 0, ML);
+        ops_rhs_kernel<<<(unsigned)nblk, 256, 0, st>>>(LU, lda, n, 1, MU);
+        count_launch(2);
+    }
+    const TrsmBatch bt{(int64_t)kOpsB * (lda + 1), (int64_t)kOpsB * kOpsK, n};
+    trsm_launch<cf, false, kOpsB>(LU, lda, ML, kOpsB, kOpsB, kOpsK, st, nullptr, 0, nullptr, 0, LeafPack{}, bt,
+                                  (unsigned)nblk);
+    trsm_launch<cf, true, kOpsB>(LU, lda, MU, kOpsB, kOpsB, kOpsK, st, nullptr, 0, nullptr, 0, LeafPack{}, bt,
+                                 (unsigned)nblk);
+    // every block column, all rows, as the packed A operand (inner dimension
+    // its width): the full columns in one launch, a partial last one apart
+    char* cpl = reinterpret_cast<char*>(ops + 2 * nblk * kOpsB * kOpsK);
+    const size_t pa = ops_colplane_bytes(n);
+    const int64_t nfull = n / kOpsB;
+    mw_status s = tc_pack_a(n, kOpsB, LU, lda, reinterpret_cast<float*>(cpl), reinterpret_cast<float*>(cpl + pa), st,
+                            (int)nfull, (int64_t)kOpsB * lda, (int64_t)(2 * pa / sizeof(float)));
+    if (s != MW_OK) return s;
+    if (nblk > nfull) {
+        char* c = cpl + nfull * 2 * pa;
+        s = tc_pack_a(n, n - nfull * kOpsB, LU + nfull * kOpsB * lda, lda, reinterpret_cast<float*>(c),
+                      reinterpret_cast<float*>(c + pa), st);
+        if (s != MW_OK) return s;
+    }
+    MW_CHECK_CUDA(cudaGetLastError());
+    return MW_OK;
+}
+
+// One triangular sweep over the right-hand sides B on the operators: the
+// look-ahead of trsm_sweep (leaf i on the caller's stream, the update of the
+// blocks from i + 2 on the second stream), with product leaves and updates
+// that pack only their A operand.
+static mw_status trsm_sweep_ops(bool upper, int64_t n, int64_t nrhs, const cf* LU, int64_t lda, cf* B, int64_t ldb,
+                                const cf* ops, const Updater& up_main, const Updater& up_rest, cudaStream_t st) {
+    if (n <= 0 || nrhs <= 0) return MW_OK;
+    MW_REQUIRE(nrhs <= up_main.ws_n && nrhs <= up_rest.ws_n, "more right-hand sides than the workspace holds");
+    static bool attr = false;
+    if (!attr) {
+        MW_CHECK_CUDA(cudaFuncSetAttribute(leaf_ops_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)kLeafOpsSmem));
+        attr = true;
+    }
+    AuxStreams* ax = nullptr;
+    {
+        mw_status s0 = aux_streams(&ax);
+        if (s0 != MW_OK) return s0;
+    }
+    cudaStream_t tr = ax->trail;
+    const int64_t nblk = (n + kOpsB - 1) / kOpsB;
+    const cf* M = ops + (upper ? nblk * kOpsB * kOpsK : 0);
+    const char* cpl = reinterpret_cast<const char*>(ops + 2 * nblk * kOpsB * kOpsK);
+    const size_t pa = ops_colplane_bytes(n);
+    // the packed X_b ring: the rest updater's B planes and the main updater's
+    const TcPlanes pr = tc_planes(up_rest.tc_ws, up_rest.ws_m, up_rest.ws_n, kOpsB);
+    const TcPlanes pm = tc_planes(up_main.tc_ws, up_main.ws_m, up_main.ws_n, kOpsB);
+    float* ring_hi[2] = {pr.b_hi, pm.b_hi};
+    float* ring_lo[2] = {pr.b_lo, pm.b_lo};
+    const cudaStream_t caller = st;
+    {
+        mw_status s0 = critical_begin(ax, caller, &st);
+        if (s0 != MW_OK) return s0;
+    }
+    auto blk0 = [&](int64_t b) { return b * kOpsB < n ? b * kOpsB : n; };
+    auto blk1 = [&](int64_t b) { return (b + 1) * kOpsB < n ? (b + 1) * kOpsB : n; };
+    MW_CHECK_CUDA(cudaEventRecord(ax->ev_main, st));
+    MW_CHECK_CUDA(cudaStreamWaitEvent(tr, ax->ev_main, 0));
+    const unsigned leaf_grid = (unsigned)((nrhs + kOpsCols - 1) / kOpsCols);
+    for (int64_t i = 0; i < nblk; ++i) {
+        const int64_t b = upper ? nblk - 1 - i : i;
+        const int64_t r0 = blk0(b), r1 = blk1(b);
+        const int jb = (int)(r1 - r0);
+        // the blocks before i-1 reach this leaf's rows on the second stream
+        if (i >= 2) MW_CHECK_CUDA(cudaStreamWaitEvent(st, ax->ev_trail[(i - 2) & 3], 0));
+        const cf* Xq = nullptr;
+        int jq = 0;
+        if (i >= 1) {
+            const int64_t q = upper ? b + 1 : b - 1;
+            Xq = B + blk0(q);
+            jq = (int)(blk1(q) - blk0(q));
+        }
+        const int slot = (int)(i & 1);
+        {
+            ProfileScope ps(PC_TRSM, st, 8.0 * (double)jb * (jb + jq) * nrhs, 8.0 * (double)(jb + jq) * kOpsB);
+            leaf_ops_kernel<<<leaf_grid, 256, kLeafOpsSmem, st>>>(M + b * kOpsB * kOpsK, B + r0, ldb, jb, Xq, jq,
+                                                                   nrhs, ring_hi[slot], ring_lo[slot], tc_n_ks(jb));
+            count_launch();
+        }
+        MW_CHECK_CUDA(cudaEventRecord(ax->ev_main, st));
+        // blocks i+2.. (lower: rows from f0 down; upper: rows above block b-1)
+        const int64_t f0 = upper ? 0 : blk0(b + 2);
+        const int64_t f1 = upper ? (b >= 2 ? blk0(b - 1) : 0) : n;
+        if (f1 > f0) {
+            MW_CHECK_CUDA(cudaStreamWaitEvent(tr, ax->ev_main, 0));
+            // block column b from row f0: f0 / 64 m-blocks into its planes
+            const int64_t aoff = (2 * f0 / TC_M) * (int64_t)tc_n_ks(jb) * TC_M * TC_KS;
+            float* a_hi = const_cast<float*>(reinterpret_cast<const float*>(cpl + b * 2 * pa)) + aoff;
+            float* a_lo = const_cast<float*>(reinterpret_cast<const float*>(cpl + b * 2 * pa + pa)) + aoff;
+            const TcPlanes pl{a_hi, a_lo, ring_hi[slot], ring_lo[slot]};
+            mw_status s = cgemm_tc_prepacked(f1 - f0, nrhs, jb, pl, B + f0, ldb, up_rest.tc_err, tr,
+                                             up_rest.max_ctas);
+            if (s != MW_OK) return s;
+        }
+        MW_CHECK_CUDA(cudaEventRecord(ax->ev_trail[i & 3], tr));
+    }
+    MW_CHECK_CUDA(cudaEventRecord(ax->ev_main, tr));
+    MW_CHECK_CUDA(cudaStreamWaitEvent(st, ax->ev_main, 0));
+    MW_CHECK_CUDA(cudaGetLastError());
+    return critical_end(ax, caller);
+}
+
 // X <- U^-1 X (the back substitution of a solve).
 template <class T>
 static mw_status getrs_upper(int64_t n, int64_t nrhs, const T* LU, int64_t lda, T* B, int64_t ldb,
@@ -2032,6 +2321,48 @@ mw_status cgetrs_upper(int64_t n, int64_t nrhs, const float* LUd, int64_t lda, f
     up.max_ctas = panel_sms<cf>() - main_sms();
     return getrs_upper<cf>(n, nrhs, reinterpret_cast<const cf*>(LUd), lda, reinterpret_cast<cf*>(Bd), ldb, up_main,
                            up, as_stream(stream));
+}
+
+// The block operators of the complex64 factors in LUd (after every row
+// interchange: the output of cgetrf_forward or mw_cgetrf) into `ops`
+// (cgetrs_ops_bytes(n) bytes), for cgetrs_upper_ops and cgetrs_ops.
+size_t cgetrs_ops_bytes(int64_t n) { return sweep_ops_bytes(n); }
+
+mw_status cgetrs_ops_prepare(int64_t n, const float* LUd, int64_t lda, void* ops, void* stream) {
+    MW_REQUIRE(n >= 0 && lda >= (n > 0 ? n : 1) && LUd && ops, "bad arguments");
+    return sweep_ops_prepare(n, reinterpret_cast<const cf*>(LUd), lda, static_cast<cf*>(ops), as_stream(stream));
+}
+
+// cgetrs_upper on the block operators of the same factors.
+mw_status cgetrs_upper_ops(int64_t n, int64_t nrhs, const float* LUd, int64_t lda, float* Bd, int64_t ldb,
+                           const void* ops, void* workspace, size_t workspace_bytes, void* stream) {
+    MW_REQUIRE(workspace_bytes >= cgetrf_ws_bytes(n, nrhs), "workspace too small");
+    if (n == 0 || nrhs == 0) return MW_OK;
+    char* ws = static_cast<char*>(workspace);
+    Updater up = tc_updater(ws, workspace_bytes, n, nrhs);
+    Updater up_main = tc_updater_main(ws, n, nrhs);
+    up.max_ctas = panel_sms<cf>() - main_sms();
+    return trsm_sweep_ops(true, n, nrhs, reinterpret_cast<const cf*>(LUd), lda, reinterpret_cast<cf*>(Bd), ldb,
+                          static_cast<const cf*>(ops), up_main, up, as_stream(stream));
+}
+
+// mw_cgetrs on the block operators of the same factors: the interchanges,
+// then the forward and the back sweep.
+mw_status cgetrs_ops(int64_t n, int64_t nrhs, const float* LUd, int64_t lda, const int32_t* ipiv, float* Bd,
+                     int64_t ldb, const void* ops, void* workspace, size_t workspace_bytes, void* stream) {
+    MW_REQUIRE(workspace_bytes >= cgetrf_ws_bytes(n, nrhs), "workspace too small");
+    if (n == 0 || nrhs == 0) return MW_OK;
+    char* ws = static_cast<char*>(workspace);
+    Updater up = tc_updater(ws, workspace_bytes, n, nrhs);
+    Updater up_main = tc_updater_main(ws, n, nrhs);
+    up.max_ctas = panel_sms<cf>() - main_sms();
+    cudaStream_t st = as_stream(stream);
+    cf* B = reinterpret_cast<cf*>(Bd);
+    const cf* LU = reinterpret_cast<const cf*>(LUd);
+    laswp_launch<cf>(B, ldb, 0, nrhs, ipiv, 0, n, st);
+    mw_status s = trsm_sweep_ops(false, n, nrhs, LU, lda, B, ldb, static_cast<const cf*>(ops), up_main, up, st);
+    if (s != MW_OK) return s;
+    return trsm_sweep_ops(true, n, nrhs, LU, lda, B, ldb, static_cast<const cf*>(ops), up_main, up, st);
 }
 }  // namespace mw
 

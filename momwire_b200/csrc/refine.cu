@@ -88,6 +88,12 @@ mw_status cgetrf_forward(int64_t n, float* Ad, int64_t lda, int32_t* ipiv, int32
                          void* stream, bool static_pivot);
 mw_status cgetrs_upper(int64_t n, int64_t nrhs, const float* LUd, int64_t lda, float* Bd, int64_t ldb, void* workspace,
                        size_t workspace_bytes, void* stream);
+size_t cgetrs_ops_bytes(int64_t n);
+mw_status cgetrs_ops_prepare(int64_t n, const float* LUd, int64_t lda, void* ops, void* stream);
+mw_status cgetrs_upper_ops(int64_t n, int64_t nrhs, const float* LUd, int64_t lda, float* Bd, int64_t ldb,
+                           const void* ops, void* workspace, size_t workspace_bytes, void* stream);
+mw_status cgetrs_ops(int64_t n, int64_t nrhs, const float* LUd, int64_t lda, const int32_t* ipiv, float* Bd,
+                     int64_t ldb, const void* ops, void* workspace, size_t workspace_bytes, void* stream);
 }  // namespace mw
 
 static size_t al256(size_t x) { return (x + 255) & ~size_t(255); }
@@ -131,7 +137,7 @@ extern "C" int32_t mw_last_mixed_history(double* out, int32_t max_n) {
 
 extern "C" size_t mw_zgesv_mixed_workspace_size(int64_t n, int64_t nrhs) {
     return al256(mw_cgetrf_workspace_size(n, nrhs)) + al256((size_t)n * nrhs * 16) + al256((size_t)n * nrhs * 8) +
-           al256((size_t)nrhs * 16) + al256(zgemm_split_ws_bytes(n, nrhs));
+           al256((size_t)nrhs * 16) + al256(zgemm_split_ws_bytes(n, nrhs)) + al256(cgetrs_ops_bytes(n));
 }
 
 extern "C" mw_status mw_zgesv_mixed(int64_t n, int64_t nrhs, const double* Z, int64_t ldz, float* Z32, int64_t ldz32,
@@ -156,6 +162,8 @@ extern "C" mw_status mw_zgesv_mixed(int64_t n, int64_t nrhs, const double* Z, in
     void* split_ws = reinterpret_cast<char*>(norms) + al256((size_t)nrhs * 16);
     const size_t split_bytes = zgemm_split_ws_bytes(n, nrhs);
     if (mw_status s0 = zgemm_split_ws_init(split_ws, st); s0 != MW_OK) return s0;
+    // the solves' block operators of the factors (rebuilt after each factorisation)
+    void* ops = static_cast<char*>(split_ws) + al256(split_bytes);
     const cd* Zc = reinterpret_cast<const cd*>(Z);
     const cd* Bc = reinterpret_cast<const cd*>(B);
     cd* Xc = reinterpret_cast<cd*>(X);
@@ -221,7 +229,9 @@ extern "C" mw_status mw_zgesv_mixed(int64_t n, int64_t nrhs, const double* Z, in
             if (it == 0) {
                 // R32 holds L^-1 P B from the factorisation
                 ProfileScope ps(PC_SOLVE, st, 4.0 * (double)n * n * nrhs, 0.0);
-                s = cgetrs_upper(n, nrhs, Z32, ldz32, reinterpret_cast<float*>(R32), n, ws_lu, lu_ws, stream);
+                s = cgetrs_ops_prepare(n, Z32, ldz32, ops, stream);
+                if (s != MW_OK) return s;
+                s = cgetrs_upper_ops(n, nrhs, Z32, ldz32, reinterpret_cast<float*>(R32), n, ops, ws_lu, lu_ws, stream);
             } else {
                 {
                     ProfileScope ps(PC_REFINE, st, 0.0, 24.0 * (double)tot);
@@ -229,7 +239,7 @@ extern "C" mw_status mw_zgesv_mixed(int64_t n, int64_t nrhs, const double* Z, in
                     count_launch();
                 }
                 ProfileScope ps(PC_SOLVE, st, 8.0 * (double)n * n * nrhs, 0.0);
-                s = mw_cgetrs(n, nrhs, Z32, ldz32, ipiv, reinterpret_cast<float*>(R32), n, ws_lu, lu_ws, stream);
+                s = cgetrs_ops(n, nrhs, Z32, ldz32, ipiv, reinterpret_cast<float*>(R32), n, ops, ws_lu, lu_ws, stream);
             }
             if (s != MW_OK) return s;
             MW_CHECK_CUDA(cudaMemsetAsync(norms, 0, sizeof(double) * 2 * nrhs, st));

@@ -46,6 +46,8 @@ mw_status static_panel_c64(cf* A, int64_t lda, int64_t n, int64_t j0, int jb, in
 void static_permute_c64(cf* A, int64_t lda, int64_t row0, int jb, int64_t col0, int64_t ncols, const int32_t* perm,
                         cudaStream_t st);
 void static_left_permute_c64(cf* A, int64_t lda, int64_t n, const int32_t* perm_all, cudaStream_t st);
+void static_rows_permute_c64(cf* B, int64_t ldb, int64_t n, int64_t ncols, const int32_t* perm_all,
+                             cudaStream_t st);
 
 constexpr int kNB = 64;         // panel half width (rank-1 work per cooperative panel)
 constexpr int kOuterNB = 128;   // getrf block: panel width and trailing-update k
@@ -2346,10 +2348,13 @@ mw_status cgetrs_upper_ops(int64_t n, int64_t nrhs, const float* LUd, int64_t ld
                           static_cast<const cf*>(ops), up_main, up, as_stream(stream));
 }
 
-// mw_cgetrs on the block operators of the same factors: the interchanges,
-// then the forward and the back sweep.
+// mw_cgetrs on the block operators of the same factors: the interchanges
+// (a static-pivot factorisation's as one parallel block permutation, from
+// the row orders it left in the workspace), then the forward and the back
+// sweep.
 mw_status cgetrs_ops(int64_t n, int64_t nrhs, const float* LUd, int64_t lda, const int32_t* ipiv, float* Bd,
-                     int64_t ldb, const void* ops, void* workspace, size_t workspace_bytes, void* stream) {
+                     int64_t ldb, const void* ops, void* workspace, size_t workspace_bytes, void* stream,
+                     bool static_pivot) {
     MW_REQUIRE(workspace_bytes >= cgetrf_ws_bytes(n, nrhs), "workspace too small");
     if (n == 0 || nrhs == 0) return MW_OK;
     char* ws = static_cast<char*>(workspace);
@@ -2359,7 +2364,12 @@ mw_status cgetrs_ops(int64_t n, int64_t nrhs, const float* LUd, int64_t lda, con
     cudaStream_t st = as_stream(stream);
     cf* B = reinterpret_cast<cf*>(Bd);
     const cf* LU = reinterpret_cast<const cf*>(LUd);
-    laswp_launch<cf>(B, ldb, 0, nrhs, ipiv, 0, n, st);
+    if (static_pivot) {
+        static_rows_permute_c64(B, ldb, n, nrhs, reinterpret_cast<const int32_t*>(ws + cgetrf_perm_offset(n, nrhs)),
+                                st);
+    } else {
+        laswp_launch<cf>(B, ldb, 0, nrhs, ipiv, 0, n, st);
+    }
     mw_status s = trsm_sweep_ops(false, n, nrhs, LU, lda, B, ldb, static_cast<const cf*>(ops), up_main, up, st);
     if (s != MW_OK) return s;
     return trsm_sweep_ops(true, n, nrhs, LU, lda, B, ldb, static_cast<const cf*>(ops), up_main, up, st);

@@ -574,6 +574,43 @@ void static_left_permute_c64(cf* A, int64_t lda, int64_t n, const int32_t* perm_
     count_launch();
 }
 
+// Every block's interchanges applied to columns [0, ncols) of B (n rows, a
+// solve's right-hand sides): the whole row permutation of a static-pivot
+// factorisation in one parallel pass (the interchanges never leave their
+// block).  blockIdx.y is the block, one warp per column.
+__global__ void __launch_bounds__(256) sp_block_permute_kernel(cf* __restrict__ B, int64_t ldb, int64_t n,
+                                                               int64_t ncols, const int32_t* __restrict__ perm_all) {
+    const int64_t j0 = (int64_t)blockIdx.y * kSpB;
+    const int jb = (int)((n - j0) < kSpB ? (n - j0) : kSpB);
+    const int lane = threadIdx.x & 31;
+    const int64_t col = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (col >= ncols) return;
+    const int32_t* perm = perm_all + j0;
+    cf* a = B + col * ldb + j0;
+    cf v[kSpB / 32];
+#pragma unroll
+    for (int u = 0; u < kSpB / 32; ++u) {
+        const int i = lane + 32 * u;
+        v[u] = i < jb ? a[perm[i]] : cf{0.0f, 0.0f};
+    }
+    __syncwarp();
+#pragma unroll
+    for (int u = 0; u < kSpB / 32; ++u) {
+        const int i = lane + 32 * u;
+        if (i < jb) a[i] = v[u];
+    }
+}
+
+void static_rows_permute_c64(cf* B, int64_t ldb, int64_t n, int64_t ncols, const int32_t* perm_all,
+                             cudaStream_t st) {
+    const int64_t nb = (n + kSpB - 1) / kSpB;
+    if (nb < 1 || ncols <= 0) return;
+    ProfileScope ps(PC_LASWP, st, 0.0, 2.0 * sizeof(cf) * (double)n * ncols);
+    dim3 grid((unsigned)((ncols + 7) / 8), (unsigned)nb);
+    sp_block_permute_kernel<<<grid, 256, 0, st>>>(B, ldb, n, ncols, perm_all);
+    count_launch();
+}
+
 // The block's interchanges applied to columns [col0, col0 + ncols).
 void static_permute_c64(cf* A, int64_t lda, int64_t row0, int jb, int64_t col0, int64_t ncols, const int32_t* perm,
                         cudaStream_t st) {

@@ -93,7 +93,8 @@ mw_status cgetrs_ops_prepare(int64_t n, const float* LUd, int64_t lda, void* ops
 mw_status cgetrs_upper_ops(int64_t n, int64_t nrhs, const float* LUd, int64_t lda, float* Bd, int64_t ldb,
                            const void* ops, void* workspace, size_t workspace_bytes, void* stream);
 mw_status cgetrs_ops(int64_t n, int64_t nrhs, const float* LUd, int64_t lda, const int32_t* ipiv, float* Bd,
-                     int64_t ldb, const void* ops, void* workspace, size_t workspace_bytes, void* stream);
+                     int64_t ldb, const void* ops, void* workspace, size_t workspace_bytes, void* stream,
+                     bool static_pivot);
 }  // namespace mw
 
 static size_t al256(size_t x) { return (x + 255) & ~size_t(255); }
@@ -239,7 +240,8 @@ extern "C" mw_status mw_zgesv_mixed(int64_t n, int64_t nrhs, const double* Z, in
                     count_launch();
                 }
                 ProfileScope ps(PC_SOLVE, st, 8.0 * (double)n * n * nrhs, 0.0);
-                s = cgetrs_ops(n, nrhs, Z32, ldz32, ipiv, reinterpret_cast<float*>(R32), n, ops, ws_lu, lu_ws, stream);
+                s = cgetrs_ops(n, nrhs, Z32, ldz32, ipiv, reinterpret_cast<float*>(R32), n, ops, ws_lu, lu_ws, stream,
+                               static_pivot);
             }
             if (s != MW_OK) return s;
             MW_CHECK_CUDA(cudaMemsetAsync(norms, 0, sizeof(double) * 2 * nrhs, st));

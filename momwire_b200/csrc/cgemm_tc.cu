@@ -62,6 +62,14 @@ struct TcArgs {
     int batch;
     int64_t c_stride;
     int64_t a_pstride, b_pstride;
+    // two-part inner dimension: stages [0, n_ks1) from the planes above,
+    // stages [n_ks1, n_ks) from these (each part packed on its own, with its
+    // own stage count); n_ks1 = 0: one part
+    const float* a_hi2 = nullptr;
+    const float* a_lo2 = nullptr;
+    const float* b_hi2 = nullptr;
+    const float* b_lo2 = nullptr;
+    int n_ks1 = 0;
 };
 
 // ---------------------------------------------------------------- kernel
@@ -112,17 +120,22 @@ __global__ void __launch_bounds__(TC_THREADS, 1) cgemm_tc_kernel(TcArgs P) {
             for (int t = blockIdx.x; t < n_tiles && !dead; t += gridDim.x) {
                 const int bt = t / per_mat, tr = t - bt * per_mat;
                 const int mb = tr % P.n_mb, nb = tr / P.n_mb;
+                const int nks1 = P.n_ks1 > 0 ? P.n_ks1 : P.n_ks;
                 for (int ks = 0; ks < P.n_ks; ++ks) {
                     if (!mbar_wait(&bar_empty[slot], (ph_empty >> slot) & 1u, err)) { dead = true; break; }
                     ph_empty ^= 1u << slot;
                     uint8_t* st = tc_smem + (size_t)slot * TC_STAGE_BYTES;
-                    const size_t ao = (size_t)bt * P.a_pstride + ((size_t)mb * P.n_ks + ks) * (TC_A_BYTES / 4);
-                    const size_t bo = (size_t)bt * P.b_pstride + ((size_t)nb * P.n_ks + ks) * (TC_B_BYTES / 4);
+                    const bool second = ks >= nks1;
+                    const int kp = second ? ks - nks1 : ks;             // stage within its part
+                    const int nkp = second ? P.n_ks - nks1 : nks1;      // stages of its part
+                    const size_t ao = (size_t)bt * P.a_pstride + ((size_t)mb * nkp + kp) * (TC_A_BYTES / 4);
+                    const size_t bo = (size_t)bt * P.b_pstride + ((size_t)nb * nkp + kp) * (TC_B_BYTES / 4);
                     mbar_expect_tx(&bar_full[slot], TC_STAGE_BYTES);
-                    bulk_g2s(st, P.a_hi + ao, TC_A_BYTES, &bar_full[slot]);
-                    bulk_g2s(st + TC_A_BYTES, P.a_lo + ao, TC_A_BYTES, &bar_full[slot]);
-                    bulk_g2s(st + 2 * TC_A_BYTES, P.b_hi + bo, TC_B_BYTES, &bar_full[slot]);
-                    bulk_g2s(st + 2 * TC_A_BYTES + TC_B_BYTES, P.b_lo + bo, TC_B_BYTES, &bar_full[slot]);
+                    bulk_g2s(st, (second ? P.a_hi2 : P.a_hi) + ao, TC_A_BYTES, &bar_full[slot]);
+                    bulk_g2s(st + TC_A_BYTES, (second ? P.a_lo2 : P.a_lo) + ao, TC_A_BYTES, &bar_full[slot]);
+                    bulk_g2s(st + 2 * TC_A_BYTES, (second ? P.b_hi2 : P.b_hi) + bo, TC_B_BYTES, &bar_full[slot]);
+                    bulk_g2s(st + 2 * TC_A_BYTES + TC_B_BYTES, (second ? P.b_lo2 : P.b_lo) + bo, TC_B_BYTES,
+                             &bar_full[slot]);
                     issued += 1;
                     slot = (slot + 1) % TC_STAGES;
                 }
@@ -402,6 +415,43 @@ mw_status tc_pack_a(int64_t m, int64_t k, const cf* A, int64_t lda, float* a_hi,
     ProfileScope ps(PC_MISC, st);
     pack_a_kernel<<<dim3((unsigned)blocks, (unsigned)batch), 256, 0, st>>>(A, lda, m, k, n_mb, n_ks, a_hi, a_lo,
                                                                            a_stride, p_stride);
+    MW_CHECK_CUDA(cudaGetLastError());
+    count_launch();
+    return MW_OK;
+}
+
+mw_status cgemm_tc_prepacked(int64_t m, int64_t n, int64_t k, const TcPlanes& pl, cf* C, int64_t ldc, int* err,
+                             cudaStream_t st, int max_ctas);
+
+// C (m x n complex64) -= A1 B1 + A2 B2 from operands already packed, part p
+// in planes pl<p> for an inner dimension k<p>: one launch for both parts.
+mw_status cgemm_tc_prepacked2(int64_t m, int64_t n, int64_t k1, const TcPlanes& pl1, int64_t k2, const TcPlanes& pl2,
+                              cf* C, int64_t ldc, int* err, cudaStream_t st, int max_ctas) {
+    if (m <= 0 || n <= 0 || k1 <= 0) return MW_OK;
+    if (k2 <= 0) return cgemm_tc_prepacked(m, n, k1, pl1, C, ldc, err, st, max_ctas);
+    const int n_mb = (int)((2 * m + TC_M - 1) / TC_M);
+    const int n_nb = (int)((n + TC_N - 1) / TC_N);
+    const int nks1 = tc_n_ks(k1), nks2 = tc_n_ks(k2);
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        MW_CHECK_CUDA(cudaFuncSetAttribute(cgemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           TC_STAGES * TC_STAGE_BYTES));
+    }
+    TcArgs P{pl1.a_hi, pl1.a_lo, pl1.b_hi, pl1.b_lo, reinterpret_cast<float*>(C), ldc, 2 * m, n, n_mb, n_nb,
+             nks1 + nks2, err, 1, 0, 0, 0, pl2.a_hi, pl2.a_lo, pl2.b_hi, pl2.b_lo, nks1};
+    const int64_t tiles = (int64_t)n_mb * n_nb;
+    MW_REQUIRE(tiles < (1ll << 31), "too many tiles");
+    const int cap = (max_ctas > 0 && max_ctas < sms) ? max_ctas : sms;
+    const int grid = tiles < cap ? (int)tiles : cap;
+    {
+        const double k = (double)(k1 + k2);
+        ProfileScope ps(PC_CGEMM_TC, st, 8.0 * (double)m * n * k, 16.0 * (double)m * n + 32.0 * (double)m * k +
+                                                                      16.0 * k * n);
+        cgemm_tc_kernel<<<grid, TC_THREADS, TC_STAGES * TC_STAGE_BYTES, st>>>(P);
+    }
     MW_CHECK_CUDA(cudaGetLastError());
     count_launch();
     return MW_OK;

@@ -39,6 +39,9 @@ mw_status cgemm_tc_prepacked(int64_t m, int64_t n, int64_t k, const TcPlanes& pl
 mw_status tc_pack_a(int64_t m, int64_t k, const cf* A, int64_t lda, float* a_hi, float* a_lo, cudaStream_t st,
                     int batch = 1, int64_t a_stride = 0, int64_t p_stride = 0);
 size_t tc_pack_a_bytes(int64_t m, int64_t k);
+size_t tc_pack_b_bytes(int64_t k, int64_t n);
+mw_status cgemm_tc_prepacked2(int64_t m, int64_t n, int64_t k1, const TcPlanes& pl1, int64_t k2, const TcPlanes& pl2,
+                              cf* C, int64_t ldc, int* err, cudaStream_t st, int max_ctas);
 
 // static-pivot panel of the complex64 path (lu_static.cu)
 mw_status static_panel_c64(cf* A, int64_t lda, int64_t n, int64_t j0, int jb, int32_t* ipiv, int32_t* info,
@@ -1876,83 +1879,103 @@ static mw_status trsm_sweep(bool upper, int64_t n, int64_t nrhs, const T* LU, in
 
 // ------------------------------------------------ sweeps on block operators
 // The complex64 solves' triangular sweeps with each 128-row leaf turned into
-// one product.  For block b of the triangle T (unit lower L or upper U of
-// the factors) and q the block solved just before it in sweep order (b - 1
-// for L, b + 1 for U; none for the first):
-//     M_b = T_bb^-1 [ I | -T_bq ]                  (128 x 256, column-major)
-// built once per factorisation (sweep_ops_prepare: the right-hand sides
-// [I | -T_bq] of every block, then one batched leaf solve per triangle), so
-// that the leaf of block b is
-//     X_b = M_b [ B_b ; X_q ]
-// -- a 128 x 256 by 256 x nrhs product with no dependent substitution chain.
-// The same preparation packs every block column of the factors as the A
-// operand of the tensor-core update that carries X_b to the blocks further
-// on; the leaf writes X_b as its packed B operand, so the update packs
-// nothing.  The B planes alternate between two sets by step parity: the
-// update of step i reads its set while leaf i + 1 writes the other, and
-// leaf i + 2 waits for that update.
-constexpr int kOpsB = 128;       // block order (the complex64 solve leaf)
-constexpr int kOpsK = 2 * kOpsB;  // columns of an operator
+// one product.  Steps s = 0, 1, ... of a sweep take the blocks in order (L:
+// b = s) or in reverse (U: b = nblk - 1 - s).  A second stream applies the
+// solved blocks to the blocks further on two steps at a time: pair k, after
+// the leaf of step 2k + 1, applies steps 2k and 2k + 1 to the blocks of the
+// steps from 2k + 3 on, as one tensor-core update with a two-part inner
+// dimension.  A leaf therefore folds in what no pair has applied yet: the
+// step before it, and at even steps the one before that too.  With T the
+// triangle (unit lower L or upper U of the factors) and q1, q2 the blocks
+// of those steps:
+//     M_b = T_bb^-1 [ I | -T_b,q1 | -T_b,q2 ]           (128 x 384, column-major)
+// built once per factorisation (sweep_ops_prepare: the right-hand sides,
+// zero where a step has no q1 or q2, then one batched leaf solve per
+// triangle), so that the leaf is one product
+//     X_b = M_b [ B_b ; X_q1 ; X_q2 ]
+// with no dependent substitution chain.  The same preparation packs every
+// block column of the factors as the updates' A operand; each leaf writes
+// X_b as the packed B operand of its pair's update, into one of four plane
+// sets by step (mod 4): the update of pair k reads the sets of steps 2k and
+// 2k + 1, which are written again only at steps 2k + 4 and 2k + 5, after
+// leaf 2k + 3 has waited for that update.  Leaf s waits for pair
+// floor((s - 3) / 2), the last one that reaches its rows.
+constexpr int kOpsB = 128;        // block order (the complex64 solve leaf)
+constexpr int kOpsK = 3 * kOpsB;  // columns of an operator
 constexpr int kOpsCols = 4;       // right-hand sides per leaf CTA
 static_assert(kOpsB == GetrsLeaf<cf>::value, "operator blocks are the solve's leaf blocks");
 
 // the packed A operand of one block column, all n rows (one plane, hi or lo)
 static size_t ops_colplane_bytes(int64_t n) { return tc_pack_a_bytes(n, kOpsB); }
+// one packed B plane of a leaf's output (128 rows, nrhs columns)
+static size_t ops_xplane_bytes(int64_t nrhs) { return (tc_pack_b_bytes(kOpsB, nrhs) + 1023) & ~size_t(1023); }
 
-size_t sweep_ops_bytes(int64_t n) {
+size_t sweep_ops_bytes(int64_t n, int64_t nrhs) {
     const int64_t nblk = (n + kOpsB - 1) / kOpsB;
-    // the L operators, the U operators, then every block column of the
-    // factors as the packed A operand of the sweeps' updates (hi, lo)
-    return 2 * (size_t)nblk * kOpsB * kOpsK * sizeof(cf) + 2 * (size_t)nblk * ops_colplane_bytes(n);
+    // the L operators, the U operators, every block column of the factors
+    // as packed A operand (hi, lo), four plane sets of leaf outputs (hi, lo)
+    return 2 * (size_t)nblk * kOpsB * kOpsK * sizeof(cf) + 2 * (size_t)nblk * ops_colplane_bytes(n) +
+           8 * ops_xplane_bytes(nrhs);
 }
 
-// Every block's [I | -T_bq]: rows past the block's order, and columns past
-// either block's, zero.  One CTA per block.
+// Every block's [I | -T_b,q1 | -T_b,q2] (sweep order of the triangle given
+// by `upper`): rows past the block's order, and columns past a block's, zero.
+// One CTA per block.
 __global__ void __launch_bounds__(256) ops_rhs_kernel(const cf* __restrict__ LU, int64_t lda, int64_t n, int upper,
                                                       cf* __restrict__ M) {
     const int64_t nblk = (n + kOpsB - 1) / kOpsB;
     const int64_t b = blockIdx.x;
-    const int64_t q = upper ? b + 1 : b - 1;
-    const int jb = (int)(n - b * kOpsB < kOpsB ? n - b * kOpsB : kOpsB);
-    const int jq = (q >= 0 && q < nblk) ? (int)(n - q * kOpsB < kOpsB ? n - q * kOpsB : kOpsB) : 0;
+    const int64_t s = upper ? nblk - 1 - b : b;  // sweep step
+    auto block_at = [&](int64_t step) { return upper ? nblk - 1 - step : step; };
+    auto order = [&](int64_t blk) { return (int)(n - blk * kOpsB < kOpsB ? n - blk * kOpsB : kOpsB); };
+    const int jb = order(b);
+    const int64_t q1 = s >= 1 ? block_at(s - 1) : -1;
+    const int64_t q2 = (s >= 2 && (s & 1) == 0) ? block_at(s - 2) : -1;
+    const int jq1 = q1 >= 0 ? order(q1) : 0, jq2 = q2 >= 0 ? order(q2) : 0;
     cf* Mb = M + b * kOpsB * kOpsK;
     for (int i = threadIdx.x; i < kOpsB * kOpsK; i += blockDim.x) {
         const int r = i % kOpsB, c = i / kOpsB;
+        const int part = c / kOpsB, cc = c % kOpsB;
         cf v{0.0f, 0.0f};
         if (r < jb) {
-            if (c < kOpsB) {
-                if (c == r) v = cf{1.0f, 0.0f};
-            } else if (c - kOpsB < jq) {
-                const cf t = LU[(b * kOpsB + r) + (q * kOpsB + (c - kOpsB)) * lda];
-                v = cf{-t.re, -t.im};
+            if (part == 0) {
+                if (cc == r) v = cf{1.0f, 0.0f};
+            } else {
+                const int64_t q = part == 1 ? q1 : q2;
+                const int jq = part == 1 ? jq1 : jq2;
+                if (cc < jq) {
+                    const cf t = LU[(b * kOpsB + r) + (q * kOpsB + cc) * lda];
+                    v = cf{-t.re, -t.im};
+                }
             }
         }
         Mb[i] = v;
     }
 }
 
-// X_b (rows < jb of this CTA's kOpsCols columns, in place) = M_b [X_b ; X_q]
-// with X_q the jq rows of the block solved before (jq = 0: none); with b_hi
-// set, X_b also as the packed B operand (inner dimension jb, b_nks stages).
-// M_b streams through shared memory in 32-column chunks (32 KB, contiguous
-// in M_b), two in flight by cp.async (two CTAs fit an SM, so the leaf's CTAs
-// take one wave of the SMs the concurrent update leaves); thread (r, g)
-// accumulates row r of
-// columns 2 g, 2 g + 1, reading its M_b row conflict-free and [X_b ; X_q]
-// as broadcasts.
+// X_b (rows < jb of this CTA's kOpsCols columns, in place) = M_b [X_b ; X_q1 ;
+// X_q2] with X_q1, X_q2 the jq1, jq2 rows of the blocks folded in (0: none);
+// with b_hi set, X_b also as a packed B operand (inner dimension jb, b_nks
+// stages).  M_b streams through shared memory in 32-column chunks (32 KB,
+// contiguous in M_b), two in flight by cp.async, so two CTAs fit an SM and
+// the leaf's CTAs take one wave of the SMs a concurrent update leaves;
+// thread (r, g) accumulates row r of columns 2 g, 2 g + 1, reading its M_b
+// row conflict-free and the right-hand sides as broadcasts.
 constexpr int kOpsChunk = 32;
 constexpr size_t kLeafOpsSmem = sizeof(cf) * (2 * (size_t)kOpsChunk * kOpsB + (size_t)kOpsK * kOpsCols +
                                               (size_t)kOpsCols * (kOpsB + 1));
 __global__ void __launch_bounds__(256, 1) leaf_ops_kernel(const cf* __restrict__ Mb, cf* __restrict__ X, int64_t ldx,
-                                                          int jb, const cf* __restrict__ Xq, int jq, int64_t ncols,
+                                                          int jb, const cf* __restrict__ Xq1, int jq1,
+                                                          const cf* __restrict__ Xq2, int jq2, int64_t ncols,
                                                           float* __restrict__ b_hi, float* __restrict__ b_lo,
                                                           int b_nks) {
     extern __shared__ __align__(16) unsigned char lo_smem[];
-    cf* sM = reinterpret_cast<cf*>(lo_smem);                 // [2][kOpsChunk][kOpsB]
-    cf* sR = sM + 2 * kOpsChunk * kOpsB;                      // [kOpsK][kOpsCols]
-    cf* sO = sR + kOpsK * kOpsCols;                           // [kOpsCols][kOpsB + 1]
+    cf* sM = reinterpret_cast<cf*>(lo_smem);  // [2][kOpsChunk][kOpsB]
+    cf* sR = sM + 2 * kOpsChunk * kOpsB;       // [kOpsK][kOpsCols]
+    cf* sO = sR + kOpsK * kOpsCols;            // [kOpsCols][kOpsB + 1]
     const int tid = threadIdx.x;
-    const int nchunk = (jq > 0 ? kOpsK : kOpsB) / kOpsChunk;
+    const int parts = 1 + (jq1 > 0 ? 1 : 0) + (jq2 > 0 ? 1 : 0);
+    const int nchunk = parts * kOpsB / kOpsChunk;
     // chunk c: columns [c kOpsChunk, (c + 1) kOpsChunk) of M_b, one contiguous
     // 32 KB run; eight 16-byte copies per thread
     auto fetch = [&](int c) {
@@ -1969,15 +1992,18 @@ __global__ void __launch_bounds__(256, 1) leaf_ops_kernel(const cf* __restrict__
     fetch(0);
     if (nchunk > 1) fetch(1);
     const int64_t c0 = (int64_t)blockIdx.x * kOpsCols;
-    for (int i = tid; i < kOpsK * kOpsCols; i += blockDim.x) {
-        const int k = i % kOpsK, c = i / kOpsK;
+    for (int i = tid; i < parts * kOpsB * kOpsCols; i += blockDim.x) {
+        const int k = i % (parts * kOpsB), c = i / (parts * kOpsB);
         const int64_t col = c0 + c;
+        const int part = k / kOpsB, kk = k % kOpsB;
         cf v{0.0f, 0.0f};
         if (col < ncols) {
-            if (k < kOpsB) {
-                if (k < jb) v = X[k + col * ldx];
-            } else if (k - kOpsB < jq) {
-                v = Xq[(k - kOpsB) + col * ldx];
+            if (part == 0) {
+                if (kk < jb) v = X[kk + col * ldx];
+            } else if (part == 1) {
+                if (kk < jq1) v = Xq1[kk + col * ldx];
+            } else if (kk < jq2) {
+                v = Xq2[kk + col * ldx];
             }
         }
         sR[k * kOpsCols + c] = v;
@@ -2023,8 +2049,8 @@ __global__ void __launch_bounds__(256, 1) leaf_ops_kernel(const cf* __restrict__
     }
 }
 
-// Both triangles' operators of the factors LU (n x n, complex64) into
-// `ops` (sweep_ops_bytes(n)).
+// Both triangles' operators and the packed block columns of the factors LU
+// (n x n, complex64) into `ops` (sweep_ops_bytes(n, nrhs)).
 static mw_status sweep_ops_prepare(int64_t n, const cf* LU, int64_t lda, cf* ops, cudaStream_t st) {
     if (n <= 0) return MW_OK;
     {
@@ -2064,14 +2090,14 @@ static mw_status sweep_ops_prepare(int64_t n, const cf* LU, int64_t lda, cf* ops
     return MW_OK;
 }
 
-// One triangular sweep over the right-hand sides B on the operators: the
-// look-ahead of trsm_sweep (leaf i on the caller's stream, the update of the
-// blocks from i + 2 on the second stream), with product leaves and updates
-// that pack only their A operand.
+// One triangular sweep over the right-hand sides B (nrhs columns, at most
+// the nrhs the operator region was sized for) on the operators: leaf s on
+// the caller's stream, the update of pair k on the second stream after
+// leaf 2k + 1.
 static mw_status trsm_sweep_ops(bool upper, int64_t n, int64_t nrhs, const cf* LU, int64_t lda, cf* B, int64_t ldb,
-                                const cf* ops, const Updater& up_main, const Updater& up_rest, cudaStream_t st) {
+                                const cf* ops, int64_t nrhs_ops, const Updater& up_rest, cudaStream_t st) {
     if (n <= 0 || nrhs <= 0) return MW_OK;
-    MW_REQUIRE(nrhs <= up_main.ws_n && nrhs <= up_rest.ws_n, "more right-hand sides than the workspace holds");
+    MW_REQUIRE(nrhs <= nrhs_ops, "more right-hand sides than the operator region holds");
     static bool attr = false;
     if (!attr) {
         MW_CHECK_CUDA(cudaFuncSetAttribute(leaf_ops_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -2088,57 +2114,74 @@ static mw_status trsm_sweep_ops(bool upper, int64_t n, int64_t nrhs, const cf* L
     const cf* M = ops + (upper ? nblk * kOpsB * kOpsK : 0);
     const char* cpl = reinterpret_cast<const char*>(ops + 2 * nblk * kOpsB * kOpsK);
     const size_t pa = ops_colplane_bytes(n);
-    // the packed X_b ring: the rest updater's B planes and the main updater's
-    const TcPlanes pr = tc_planes(up_rest.tc_ws, up_rest.ws_m, up_rest.ws_n, kOpsB);
-    const TcPlanes pm = tc_planes(up_main.tc_ws, up_main.ws_m, up_main.ws_n, kOpsB);
-    float* ring_hi[2] = {pr.b_hi, pm.b_hi};
-    float* ring_lo[2] = {pr.b_lo, pm.b_lo};
+    char* xpl = const_cast<char*>(cpl) + nblk * 2 * pa;  // four plane sets of leaf outputs
+    const size_t px = ops_xplane_bytes(nrhs_ops);
+    auto xhi = [&](int64_t s) { return reinterpret_cast<float*>(xpl + (s & 3) * 2 * px); };
+    auto xlo = [&](int64_t s) { return reinterpret_cast<float*>(xpl + (s & 3) * 2 * px + px); };
     const cudaStream_t caller = st;
     {
         mw_status s0 = critical_begin(ax, caller, &st);
         if (s0 != MW_OK) return s0;
     }
+    auto block_at = [&](int64_t s) { return upper ? nblk - 1 - s : s; };
     auto blk0 = [&](int64_t b) { return b * kOpsB < n ? b * kOpsB : n; };
     auto blk1 = [&](int64_t b) { return (b + 1) * kOpsB < n ? (b + 1) * kOpsB : n; };
     MW_CHECK_CUDA(cudaEventRecord(ax->ev_main, st));
     MW_CHECK_CUDA(cudaStreamWaitEvent(tr, ax->ev_main, 0));
     const unsigned leaf_grid = (unsigned)((nrhs + kOpsCols - 1) / kOpsCols);
-    for (int64_t i = 0; i < nblk; ++i) {
-        const int64_t b = upper ? nblk - 1 - i : i;
-        const int64_t r0 = blk0(b), r1 = blk1(b);
-        const int jb = (int)(r1 - r0);
-        // the blocks before i-1 reach this leaf's rows on the second stream
-        if (i >= 2) MW_CHECK_CUDA(cudaStreamWaitEvent(st, ax->ev_trail[(i - 2) & 3], 0));
-        const cf* Xq = nullptr;
-        int jq = 0;
-        if (i >= 1) {
-            const int64_t q = upper ? b + 1 : b - 1;
-            Xq = B + blk0(q);
-            jq = (int)(blk1(q) - blk0(q));
+    for (int64_t s = 0; s < nblk; ++s) {
+        const int64_t b = block_at(s);
+        const int64_t r0 = blk0(b);
+        const int jb = (int)(blk1(b) - r0);
+        // the last pair that reaches this block's rows
+        if (s >= 3) MW_CHECK_CUDA(cudaStreamWaitEvent(st, ax->ev_trail[((s - 3) / 2) & 3], 0));
+        const cf* X1 = nullptr;
+        const cf* X2 = nullptr;
+        int j1 = 0, j2 = 0;
+        if (s >= 1) {
+            const int64_t q = block_at(s - 1);
+            X1 = B + blk0(q);
+            j1 = (int)(blk1(q) - blk0(q));
         }
-        const int slot = (int)(i & 1);
+        if (s >= 2 && (s & 1) == 0) {
+            const int64_t q = block_at(s - 2);
+            X2 = B + blk0(q);
+            j2 = (int)(blk1(q) - blk0(q));
+        }
         {
-            ProfileScope ps(PC_TRSM, st, 8.0 * (double)jb * (jb + jq) * nrhs, 8.0 * (double)(jb + jq) * kOpsB);
-            leaf_ops_kernel<<<leaf_grid, 256, kLeafOpsSmem, st>>>(M + b * kOpsB * kOpsK, B + r0, ldb, jb, Xq, jq,
-                                                                   nrhs, ring_hi[slot], ring_lo[slot], tc_n_ks(jb));
+            ProfileScope ps(PC_TRSM, st, 8.0 * (double)jb * (jb + j1 + j2) * nrhs, 8.0 * (double)(jb + j1 + j2) * kOpsB);
+            leaf_ops_kernel<<<leaf_grid, 256, kLeafOpsSmem, st>>>(M + b * kOpsB * kOpsK, B + r0, ldb, jb, X1, j1, X2,
+                                                                   j2, nrhs, xhi(s), xlo(s), tc_n_ks(jb));
             count_launch();
         }
+        if ((s & 1) == 0) continue;
+        // pair (s - 1, s) to the blocks of steps s + 2 on: rows from f0 (L)
+        // or below f1 (U)
         MW_CHECK_CUDA(cudaEventRecord(ax->ev_main, st));
-        // blocks i+2.. (lower: rows from f0 down; upper: rows above block b-1)
+        const int64_t bp = block_at(s - 1);
+        const int jp = (int)(blk1(bp) - blk0(bp));
         const int64_t f0 = upper ? 0 : blk0(b + 2);
         const int64_t f1 = upper ? (b >= 2 ? blk0(b - 1) : 0) : n;
         if (f1 > f0) {
             MW_CHECK_CUDA(cudaStreamWaitEvent(tr, ax->ev_main, 0));
-            // block column b from row f0: f0 / 64 m-blocks into its planes
-            const int64_t aoff = (2 * f0 / TC_M) * (int64_t)tc_n_ks(jb) * TC_M * TC_KS;
-            float* a_hi = const_cast<float*>(reinterpret_cast<const float*>(cpl + b * 2 * pa)) + aoff;
-            float* a_lo = const_cast<float*>(reinterpret_cast<const float*>(cpl + b * 2 * pa + pa)) + aoff;
-            const TcPlanes pl{a_hi, a_lo, ring_hi[slot], ring_lo[slot]};
-            mw_status s = cgemm_tc_prepacked(f1 - f0, nrhs, jb, pl, B + f0, ldb, up_rest.tc_err, tr,
-                                             up_rest.max_ctas);
-            if (s != MW_OK) return s;
+            // block columns bp and b from row f0: f0 / 64 m-blocks into their planes
+            auto col = [&](int64_t blk, int k, float** hi, float** lo) {
+                const int64_t off = (2 * f0 / TC_M) * (int64_t)tc_n_ks(k) * TC_M * TC_KS;
+                *hi = const_cast<float*>(reinterpret_cast<const float*>(cpl + blk * 2 * pa)) + off;
+                *lo = const_cast<float*>(reinterpret_cast<const float*>(cpl + blk * 2 * pa + pa)) + off;
+            };
+            TcPlanes p1{}, p2{};
+            col(bp, jp, &p1.a_hi, &p1.a_lo);
+            col(b, jb, &p2.a_hi, &p2.a_lo);
+            p1.b_hi = xhi(s - 1);
+            p1.b_lo = xlo(s - 1);
+            p2.b_hi = xhi(s);
+            p2.b_lo = xlo(s);
+            mw_status rs = cgemm_tc_prepacked2(f1 - f0, nrhs, jp, p1, jb, p2, B + f0, ldb, up_rest.tc_err, tr,
+                                               up_rest.max_ctas);
+            if (rs != MW_OK) return rs;
         }
-        MW_CHECK_CUDA(cudaEventRecord(ax->ev_trail[i & 3], tr));
+        MW_CHECK_CUDA(cudaEventRecord(ax->ev_trail[((s - 1) / 2) & 3], tr));
     }
     MW_CHECK_CUDA(cudaEventRecord(ax->ev_main, tr));
     MW_CHECK_CUDA(cudaStreamWaitEvent(st, ax->ev_main, 0));
@@ -2327,8 +2370,9 @@ mw_status cgetrs_upper(int64_t n, int64_t nrhs, const float* LUd, int64_t lda, f
 
 // The block operators of the complex64 factors in LUd (after every row
 // interchange: the output of cgetrf_forward or mw_cgetrf) into `ops`
-// (cgetrs_ops_bytes(n) bytes), for cgetrs_upper_ops and cgetrs_ops.
-size_t cgetrs_ops_bytes(int64_t n) { return sweep_ops_bytes(n); }
+// (cgetrs_ops_bytes(n, nrhs) bytes), for cgetrs_upper_ops and cgetrs_ops
+// with up to nrhs right-hand sides.
+size_t cgetrs_ops_bytes(int64_t n, int64_t nrhs) { return sweep_ops_bytes(n, nrhs); }
 
 mw_status cgetrs_ops_prepare(int64_t n, const float* LUd, int64_t lda, void* ops, void* stream) {
     MW_REQUIRE(n >= 0 && lda >= (n > 0 ? n : 1) && LUd && ops, "bad arguments");
@@ -2342,10 +2386,9 @@ mw_status cgetrs_upper_ops(int64_t n, int64_t nrhs, const float* LUd, int64_t ld
     if (n == 0 || nrhs == 0) return MW_OK;
     char* ws = static_cast<char*>(workspace);
     Updater up = tc_updater(ws, workspace_bytes, n, nrhs);
-    Updater up_main = tc_updater_main(ws, n, nrhs);
     up.max_ctas = panel_sms<cf>() - main_sms();
     return trsm_sweep_ops(true, n, nrhs, reinterpret_cast<const cf*>(LUd), lda, reinterpret_cast<cf*>(Bd), ldb,
-                          static_cast<const cf*>(ops), up_main, up, as_stream(stream));
+                          static_cast<const cf*>(ops), nrhs, up, as_stream(stream));
 }
 
 // mw_cgetrs on the block operators of the same factors: the interchanges
@@ -2359,7 +2402,6 @@ mw_status cgetrs_ops(int64_t n, int64_t nrhs, const float* LUd, int64_t lda, con
     if (n == 0 || nrhs == 0) return MW_OK;
     char* ws = static_cast<char*>(workspace);
     Updater up = tc_updater(ws, workspace_bytes, n, nrhs);
-    Updater up_main = tc_updater_main(ws, n, nrhs);
     up.max_ctas = panel_sms<cf>() - main_sms();
     cudaStream_t st = as_stream(stream);
     cf* B = reinterpret_cast<cf*>(Bd);
@@ -2370,9 +2412,9 @@ mw_status cgetrs_ops(int64_t n, int64_t nrhs, const float* LUd, int64_t lda, con
     } else {
         laswp_launch<cf>(B, ldb, 0, nrhs, ipiv, 0, n, st);
     }
-    mw_status s = trsm_sweep_ops(false, n, nrhs, LU, lda, B, ldb, static_cast<const cf*>(ops), up_main, up, st);
+    mw_status s = trsm_sweep_ops(false, n, nrhs, LU, lda, B, ldb, static_cast<const cf*>(ops), nrhs, up, st);
     if (s != MW_OK) return s;
-    return trsm_sweep_ops(true, n, nrhs, LU, lda, B, ldb, static_cast<const cf*>(ops), up_main, up, st);
+    return trsm_sweep_ops(true, n, nrhs, LU, lda, B, ldb, static_cast<const cf*>(ops), nrhs, up, st);
 }
 }  // namespace mw
 

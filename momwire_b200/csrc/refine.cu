@@ -88,7 +88,7 @@ mw_status cgetrf_forward(int64_t n, float* Ad, int64_t lda, int32_t* ipiv, int32
                          void* stream, bool static_pivot);
 mw_status cgetrs_upper(int64_t n, int64_t nrhs, const float* LUd, int64_t lda, float* Bd, int64_t ldb, void* workspace,
                        size_t workspace_bytes, void* stream);
-size_t cgetrs_ops_bytes(int64_t n);
+size_t cgetrs_ops_bytes(int64_t n, int64_t nrhs);
 mw_status cgetrs_ops_prepare(int64_t n, const float* LUd, int64_t lda, void* ops, void* stream);
 mw_status cgetrs_upper_ops(int64_t n, int64_t nrhs, const float* LUd, int64_t lda, float* Bd, int64_t ldb,
                            const void* ops, void* workspace, size_t workspace_bytes, void* stream);
@@ -138,7 +138,7 @@ extern "C" int32_t mw_last_mixed_history(double* out, int32_t max_n) {
 
 extern "C" size_t mw_zgesv_mixed_workspace_size(int64_t n, int64_t nrhs) {
     return al256(mw_cgetrf_workspace_size(n, nrhs)) + al256((size_t)n * nrhs * 16) + al256((size_t)n * nrhs * 8) +
-           al256((size_t)nrhs * 16) + al256(zgemm_split_ws_bytes(n, nrhs)) + al256(cgetrs_ops_bytes(n));
+           al256((size_t)nrhs * 16) + al256(zgemm_split_ws_bytes(n, nrhs)) + al256(cgetrs_ops_bytes(n, nrhs));
 }
 
 extern "C" mw_status mw_zgesv_mixed(int64_t n, int64_t nrhs, const double* Z, int64_t ldz, float* Z32, int64_t ldz32,

@@ -653,7 +653,21 @@ class BSplineSolver:
         host = [pr, pc, np.ascontiguousarray(pv).view(np.float64), kr, kc, np.ascontiguousarray(kv).view(np.float64),
                 rr, rc, np.ascontiguousarray(rv).view(np.float64), bt_ptr, bt_col, bt_val.view(np.float64), a_ptr,
                 a_col, a_val.view(np.float64)]
-        ent = [torch.from_numpy(np.ascontiguousarray(a)).to(dev) for a in host]
+        # one page-locked staging buffer and one stream-ordered copy for all
+        # of them (each array 256-byte aligned), device views by offset
+        host = [np.ascontiguousarray(a) for a in host]
+        offs, tot = [], 0
+        for a in host:
+            offs.append(tot)
+            tot += (a.nbytes + 255) & ~255
+        stage = torch.empty(max(tot, 256), dtype=torch.uint8, pin_memory=True)
+        sv = stage.numpy()
+        for a, o in zip(host, offs):
+            sv[o:o + a.nbytes] = a.reshape(-1).view(np.uint8)
+        dbytes = torch.empty(stage.numel(), dtype=torch.uint8, device=dev)
+        dbytes.copy_(stage, non_blocking=True)
+        tdt = {np.dtype(np.int64): torch.int64, np.dtype(np.float64): torch.float64}
+        ent = [dbytes[o:o + a.nbytes].view(tdt[a.dtype]) for a, o in zip(host, offs)]
         lib = _lib.load()
         st = torch.cuda.current_stream(dev).cuda_stream
         m = n_p + n_c
@@ -676,6 +690,7 @@ class BSplineSolver:
             "info": torch.zeros(2, dtype=torch.int32, device=dev),
             "Y": torch.empty((max(n_p, 1), max(n_p, 1)), dtype=torch.complex128, device=dev),
             "kcl": kcl_con,
+            "_stage": stage,  # the staging buffer lives until the copy has run
         }
         buf["RHS"] = torch.empty_like(buf["RHS0"])
         if self.precision == "mixed":

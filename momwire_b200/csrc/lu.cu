@@ -1321,7 +1321,8 @@ mw_status zgemm_launch(bool ta, bool tb, int64_t m, int64_t n, int64_t k, cd alp
     }
 }
 
-// SIMT variant kept for comparison runs (MW_ZGEMM_SIMT=1 selects it).
+// The register-tiled DFMA kernel: the products with k < 128 (the FP64
+// panels' half-width updates, a KCL Schur step with few constraint rows).
 mw_status zgemm_launch_simt(bool ta, bool tb, int64_t m, int64_t n, int64_t k, cd alpha, const cd* A, int64_t lda,
                             const cd* B, int64_t ldb, cd beta, cd* C, int64_t ldc, cudaStream_t st) {
     if (m <= 0 || n <= 0) return MW_OK;
